@@ -1,0 +1,323 @@
+"""Benchmark of the B200 barotropic step.
+
+Workload: the 2048 x 1536 regional basin (1 km, fractal coastline ~40 %
+land, log-normal depth, smooth random wind with a 6-hour cycle, dt = 2 s),
+FP64.  A step is one leap-frog substep that advances the basin by dt: the
+state evolution of barotropic_dynamics(tau=dt, nstep=1) keeping *_e.
+
+  value  grid-cell-steps/s with the state resident in HBM (run_substeps,
+         one fused kernel per step), interior cells (land included) x steps,
+         summed over ranks; timed with CUDA events on the library's stream.
+  e2e    the same metric through the drop-in C-ABI call
+         inmsom_barotropic_dynamics(tau = 50*dt, nstep = 50) with pinned host
+         buffers: every call uploads the forcing, runs the reference's
+         2*nstep substeps with time means, and downloads the time means.
+  cpu_baseline  the CPU oracle (a line-by-line C restatement of the
+         reference loops, OpenMP on all host threads) on a bounded sample.
+
+--impl reference runs only the CPU oracle arm (rank 0) and prints its line.
+Multi-GPU (torchrun): every rank runs its own basin replica (seed + rank);
+the time is the max over ranks and value sums the ranks' cells.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+METRIC = "grid-cell-steps/s"
+BYTES_PER_CELL_STEP = 120          # algorithmic FP64 bytes of one substep
+E2E_NSTEP = 50                     # nstep_barotrop of ocean_run.par:9
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10000)
+    p.add_argument("--warmup", type=int, default=100)
+    p.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    p.add_argument("--nx", type=int, default=2048)
+    p.add_argument("--ny", type=int, default=1536)
+    p.add_argument("--e2e-calls", type=int, default=12)
+    p.add_argument("--cpu-seconds", type=float, default=15.0)
+    p.add_argument("--no-cpu", action="store_true")
+    return p.parse_args()
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    return int(os.environ.get("RANK", "0")), ws, int(os.environ.get("LOCAL_RANK", "0"))
+
+
+def workload(args, rank):
+    from inmsom_elfs_b200 import basins
+    b = basins.regional_basin(nx=args.nx, ny=args.ny, seed=1 + rank)
+    return b
+
+
+def config_dict(b, args, nranks):
+    return {
+        "workload": f"regional_basin {b.bounds.nx}x{b.bounds.ny} 1 km FP64 barotropic leap-frog",
+        "nx": b.bounds.nx, "ny": b.bounds.ny, "spacing_m": 1000.0, "dt_s": b.dt,
+        "land_fraction": round(float(b.info["land_fraction"]), 4),
+        "cells_per_rank": b.cells,
+        "l2": "inputs larger than L2: 6 state + H + 2 forcing FP64 fields = %.0f MB per step"
+              % (9 * 8 * b.cells / 1e6),
+        "parallelism": "replicas" if nranks > 1 else "single",
+        "step": "one advancing leap-frog substep (barotropic_dynamics(dt,1) state evolution)",
+    }
+
+
+# ------------------------------------------------------------------ clocks
+class Clocks:
+    def __init__(self, gpu_index: int):
+        self.proc = None
+        self.lines = []
+        self.gpu = gpu_index
+
+    def __enter__(self):
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "100",
+                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read, daemon=True)
+            self.t.start()
+        except Exception:
+            self.proc = None
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def __exit__(self, *exc):
+        if self.proc:
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, mx, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            f = [x.strip() for x in ln.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx = float(f[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def measured_hbm():
+    p = ROOT / "MEASURED_PEAKS.json"
+    if p.exists():
+        return float(json.loads(p.read_text())["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the fused kernel from the committed ncu
+    summary (scaled to this workload's cells), or None."""
+    p = ROOT / "profiles" / "fused_substep_traffic.json"
+    if not p.exists():
+        return None
+    d = json.loads(p.read_text())
+    return d
+
+
+# ------------------------------------------------------------------ CPU arm
+def cpu_arm(b, nstep, seconds, threads):
+    """Time the oracle's barotropic_dynamics(nstep*dt, nstep) on the host:
+    returns (cell-steps/s, calls, elapsed)."""
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle import oracle as ora
+    from inmsom_elfs_b200 import basins
+    basins.finalize(b, ora.OracleBackend())
+    ora.hh_init_external(b)
+    ora.barotropic_dynamics(b, nstep * b.dt, nstep)   # warm
+    t0 = time.perf_counter()
+    calls = 0
+    while True:
+        ora.barotropic_dynamics(b, nstep * b.dt, nstep)
+        calls += 1
+        el = time.perf_counter() - t0
+        if el >= seconds:
+            break
+    return b.cells * nstep * calls / el, calls, el
+
+
+def run_reference(args):
+    rank, ws, _ = dist_env()
+    if rank != 0:
+        return
+    threads = os.cpu_count() or 1
+    os.environ["OMP_NUM_THREADS"] = str(threads)
+    from oracle import oracle as ora
+    from inmsom_elfs_b200 import basins
+    b = workload(args, 0)
+    basins.finalize(b, ora.OracleBackend())
+    ora.hh_init_external(b)
+    nstep = 5
+    for _ in range(max(args.warmup, 0) and min(args.warmup, 3)):
+        ora.barotropic_dynamics(b, nstep * b.dt, nstep)
+    t0 = time.perf_counter()
+    ksteps = max(1, min(args.steps, 20))
+    for _ in range(ksteps):
+        ora.barotropic_dynamics(b, nstep * b.dt, nstep)
+    el = time.perf_counter() - t0
+    v = b.cells * nstep * ksteps / el
+    cfg = config_dict(b, args, 1)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
+        "steps": ksteps, "warmup": min(args.warmup, 3), "ms_per_step": el / ksteps * 1e3,
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic", "config": cfg,
+        "cpu_baseline": {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
+                         "sample": f"{ksteps} calls of the oracle barotropic_dynamics(tau={nstep}*dt, "
+                                   f"nstep={nstep}) on the full basin ({2*nstep} substeps per call, "
+                                   f"{nstep} advancing steps), OpenMP {threads} threads"},
+        "e2e": {"value": v, "unit": METRIC, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------------------------ GPU arm
+def run_ours(args):
+    import torch
+    rank, ws, local = dist_env()
+    torch.cuda.set_device(local)
+    if ws > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120),
+                                device_id=torch.device("cuda", local))
+    from inmsom_elfs_b200 import basins, solver
+    from inmsom_elfs_b200.grid import MEANS
+
+    b = workload(args, rank)
+    basins.finalize(b, solver.GpuBackend(local))
+    cpu_copy = b.copy() if (rank == 0 and ws == 1 and not args.no_cpu) else None
+
+    def barrier():
+        if ws > 1:
+            import torch.distributed as dist
+            dist.barrier()
+        torch.cuda.synchronize()
+
+    def maxall(x):
+        if ws == 1:
+            return x
+        import torch.distributed as dist
+        t = torch.tensor([x], dtype=torch.float64, device="cuda")
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---- device-resident standalone run (value)
+    s = solver.BarotropicSolver(b, device=local, resident=True)
+    path = s.path()
+    s.load_state()
+    warm = basins.wind_cycle(args.warmup, b.dt)
+    s.run_substeps(args.warmup, b.dt, warm)
+    scale = basins.wind_cycle(args.steps, b.dt, t0=args.warmup * b.dt)
+    barrier()
+    with Clocks(local) as clk:
+        ms = s.run_substeps(args.steps, b.dt, scale)
+        barrier()
+    ms = maxall(ms)
+    nbad = s.guard()
+    s.close()
+    cells = b.cells
+    value = cells * args.steps * ws / (ms / 1e3)
+    per_launch_s = ms / 1e3 / args.steps
+    achieved = BYTES_PER_CELL_STEP * cells / per_launch_s / 1e9
+    peak, peak_kind = measured_hbm()
+
+    # ---- e2e through the drop-in with pinned host buffers
+    pin = {}
+    eb = b.copy()
+    for grp in ("state", "means", "forcing", "scratch"):
+        d = getattr(eb, grp)
+        for k, v in d.items():
+            t = torch.empty(v.shape[::-1], dtype=torch.float64, pin_memory=True)
+            a = t.numpy().T          # Fortran-contiguous view of pinned memory
+            a[...] = v
+            d[k] = a
+            pin[k] = t
+    se = solver.BarotropicSolver(eb, device=local, resident=True)
+    se.barotropic_dynamics(E2E_NSTEP * b.dt, E2E_NSTEP)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_calls):
+        se.barotropic_dynamics(E2E_NSTEP * b.dt, E2E_NSTEP)
+    barrier()
+    e2e_s = maxall(time.perf_counter() - t0)
+    se.close()
+    fb = 8 * b.bounds.shape[0] * b.bounds.shape[1]
+    e2e = {"value": cells * E2E_NSTEP * args.e2e_calls * ws / e2e_s, "unit": METRIC,
+           "h2d_bytes_per_step": 6 * fb / E2E_NSTEP, "d2h_bytes_per_step": 4 * fb / E2E_NSTEP,
+           "call": f"inmsom_barotropic_dynamics(tau={E2E_NSTEP}*dt, nstep={E2E_NSTEP}) from pinned "
+                   f"host arrays: 6 forcing arrays in, 4 time-mean arrays out per call, "
+                   f"{2 * E2E_NSTEP} substeps with time means; h2d/d2h bytes per advancing step"}
+
+    cpu = None
+    if cpu_copy is not None:
+        thr = os.cpu_count() or 1
+        v, calls, el = cpu_arm(cpu_copy, 5, args.cpu_seconds, thr)
+        cpu = {"value": v, "unit": METRIC, "cores": thr, "kind": "port",
+               "sample": f"{calls} calls of the oracle barotropic_dynamics(tau=5*dt, nstep=5) on the "
+                         f"full basin in {el:.1f} s (10 substeps per call, 5 advancing steps), "
+                         f"OpenMP {thr} threads"}
+
+    tr = ncu_traffic()
+    traffic = None
+    if tr and tr.get("cells"):
+        traffic = tr["bytes_per_launch"] * cells / tr["cells"]
+    if rank == 0:
+        line = {
+            "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "config": config_dict(b, args, ws),
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                         "frac": achieved / peak, "traffic": traffic,
+                         "kernel": "k_substep (fused leap-frog substep)",
+                         "bytes_per_cell_step": BYTES_PER_CELL_STEP,
+                         "peak_kind": f"{peak_kind} HBM copy bandwidth"},
+            "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
+            "gpu_launches": args.steps + 1, "path": path[1], "guard_bad_points": nbad,
+        }
+        print(json.dumps(line), flush=True)
+    if ws > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    a = parse()
+    if a.impl == "reference":
+        run_reference(a)
+    else:
+        run_ours(a)

@@ -1,0 +1,219 @@
+/*
+ * inmsom_gpu.h -- C ABI of the B200 barotropic (external-mode) step of INMSOM.
+ *
+ * The Fortran model calls its hot path through implicit-interface external
+ * subroutines with every argument by reference and every array an
+ * explicit-shape, contiguous, column-major real(8) (or real(4) mask) array
+ * with bounds (bnd_x1:bnd_x2, bnd_y1:bnd_y2).  Each entry point below takes
+ * the same arguments in the same order as the routine it replaces, plus a
+ * leading context handle; arrays are passed as base addresses of those host
+ * arrays.  Scalars are passed by value (the ISO_C_BINDING shim adds VALUE).
+ * No torch, CUDA or C++ types appear in any signature.
+ *
+ * Every function returns 0 on success or one of the INMSOM_E* codes;
+ * inmsom_gpu_last_error() gives a one-line description of the last failure
+ * on the calling thread.  The reference has no error returns (it calls
+ * `stop` or `mpi_abort`); the Fortran shim turns a nonzero status into
+ * `stop` with that message.
+ *
+ * Threading: a context is used by one host thread at a time and issues all
+ * work on its own CUDA stream.  Several contexts may coexist.
+ */
+#ifndef INMSOM_GPU_H
+#define INMSOM_GPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* status codes */
+#define INMSOM_OK          0
+#define INMSOM_ECUDA       1  /* a CUDA runtime call failed                       */
+#define INMSOM_EARG        2  /* bad argument: null pointer, bad bounds, nstep<1  */
+#define INMSOM_EGUARD      3  /* state non-finite or out of range (guard tripped) */
+#define INMSOM_ETIMEOUT    4  /* a bounded device-side wait gave up               */
+#define INMSOM_EUNSUPPORTED 5 /* option not supported by the requested path       */
+
+/* context flags (inmsom_gpu_init) */
+#define INMSOM_RESIDENT      0x1u /* state, depths and scratch stay on the device
+                                     between calls; each barotropic_dynamics call
+                                     copies in only the forcing (RHSx, RHSy, wflux,
+                                     mu, mu4, rdis) and copies out only the
+                                     time-mean outputs (ubrtr_i, vbrtr_i,
+                                     ssh4gradx, ssh4grady).  Without it every
+                                     call copies every array argument in and out. */
+#define INMSOM_FORCE_GENERAL 0x2u /* always use the per-loop kernels (exact
+                                     reference rounding) even when the fused
+                                     streaming kernel is eligible               */
+#define INMSOM_GUARD         0x4u /* after every call apply the range/NaN guard of
+                                     Control/dyncall.f90:452-516 to the saved
+                                     state; a trip returns INMSOM_EGUARD        */
+
+/* Domain bounds: Modules/mod_mpi_parallel_tools.f90:7-15 (local interior
+ * nx_start..ny_end and array bounds bnd_x1..bnd_y2), global significant area
+ * mmm..nn and periodicity switches of Inc/basinpar.fi:4-14. */
+typedef struct inmsom_bounds {
+    int nx_start, nx_end, ny_start, ny_end;
+    int bnd_x1, bnd_x2, bnd_y1, bnd_y2;
+    int mmm, mm, nnn, nn;
+    int periodicity_x, periodicity_y;
+} inmsom_bounds;
+
+/* Compile-time constants of the reference, Inc/basinpar.fi:3,46,76-77. */
+typedef struct inmsom_consts {
+    double time_smooth;    /* time_smooth = 0.05 */
+    double free_fall_acc;  /* FreeFallAcc = 9.8  */
+    double ref_den;        /* RefDen = 1025      */
+    int full_free_surface; /* full_free_surface = 1 */
+} inmsom_consts;
+
+typedef struct inmsom_ctx inmsom_ctx;
+
+/* Create a context on CUDA device `device` for one domain.
+ * Replaces the MPI/OpenMP set-up of Control/init_arrays.f90:21-88 for one
+ * GPU: the bounds are the ones that routine (or its serial twin
+ * non_mpi_array_boundary_definition, :2-17) computes. */
+int inmsom_gpu_init(inmsom_ctx **ctx, const inmsom_bounds *bounds,
+                    const inmsom_consts *consts, int device, unsigned flags);
+
+/* Register the basin_grid module arrays that the hot-path routines read
+ * implicitly through `use basin_grid` (Modules/mod_basin_grid.f90:6-63):
+ * the seven real(4) masks, the eight metric arrays, the Coriolis parameter,
+ * the rest depth (Control/init_pars.f90:150-153) and the twelve
+ * external-mode depth arrays (in/out module state).  The grid is uploaded
+ * once; the depth arrays are uploaded here and written back by
+ * inmsom_gpu_sync_to_host(INMSOM_SYNC_DEPTHS) (or after every call without
+ * INMSOM_RESIDENT).  The depth pointers may be NULL, in which case the
+ * depths are initialised on the device by hh_init from the state of the
+ * first call. */
+int inmsom_gpu_register_grid(inmsom_ctx *ctx,
+                             const float *lu, const float *luu, const float *luh,
+                             const float *lcu, const float *lcv,
+                             const float *llu, const float *llv,
+                             const double *dx, const double *dy,
+                             const double *dxt, const double *dyt,
+                             const double *dxh, const double *dyh,
+                             const double *dxb, const double *dyb,
+                             const double *rlh_s, const double *hhq_rest,
+                             double *hhq_e, double *hhqp_e, double *hhqn_e,
+                             double *hhu_e, double *hhup_e, double *hhun_e,
+                             double *hhv_e, double *hhvp_e, double *hhvn_e,
+                             double *hhh_e, double *hhhp_e, double *hhhn_e);
+
+/* Replaces barotropic_dynamics, Function/vel_ssh.f90:379-406 (called at
+ * Control/dyncall.f90:137-164), with the same 28 arguments.  Runs 2*nstep
+ * leap-frog substeps of length tau/nstep, saves the state after substep
+ * nstep into *_e, accumulates the time-mean transports ubrtr_i/vbrtr_i and
+ * pressure gradients ssh4gradx/ssh4grady over all 2*nstep substeps and ends
+ * with hh_init of the external depths. */
+int inmsom_barotropic_dynamics(inmsom_ctx *ctx, double tau, int nstep, int ksw4,
+                               double *ubrtr_e, double *ubrtrp_e,
+                               double *vbrtr_e, double *vbrtrp_e,
+                               double *ssh_e, double *sshp_e,
+                               double *ubrtr_i, double *vbrtr_i,
+                               double *ssh4gradx, double *ssh4grady,
+                               const double *RHSx, const double *RHSy,
+                               const double *wflux, const double *mu,
+                               const double *mu4, double *vort,
+                               double *str_t2d, double *str_s2d,
+                               double *fx, double *fy, const double *rdis,
+                               double *RHSx_adv, double *RHSy_adv,
+                               double *RHSx_dif, double *RHSy_dif);
+
+/* Replaces ssh_internal, Function/vel_ssh.f90:682-751 (called at
+ * Control/dyncall.f90:209-214).  hhqn..hhhn are the internal-mode depth
+ * module arrays that ssh_internal updates through hh_update (:733-735);
+ * copied in and out on every call. */
+int inmsom_ssh_internal(inmsom_ctx *ctx, double tau, double *ssh_i,
+                        double *sshp_i, const double *u, const double *v,
+                        const double *wflux, double *hhqn, double *hhun,
+                        double *hhvn, double *hhhn);
+
+/* Replaces the mask construction of gridcon, Service/grid_construction.f90:
+ * 59-112: luh, luu, llu, llv, lcu, lcv from the T mask lu (all real(4) 0/1
+ * host arrays with the bounds given; outputs must be zero-initialised as
+ * model_grid_allocate does).  Bit-exact. */
+int inmsom_gridcon(const inmsom_bounds *bounds, const float *lu, float *luu,
+                   float *luh, float *llu, float *llv, float *lcu, float *lcv,
+                   int device);
+
+/* Replaces the Rayleigh-friction set-up of Control/init_pars.f90:459-481:
+ * r_diss = r_fric*|grad hhq_rest| on the registered grid. */
+int inmsom_r_diss(inmsom_ctx *ctx, double r_fric, double *r_diss);
+
+/* Replaces the ksw_ssbc=1 wind-stress interpolation of
+ * Function/fluxes.f90:29-37 followed by the barotropic forcing assembly of
+ * Control/dyncall.f90:110-130 for a barotropic-only model (no 3-D
+ * dispersion terms, no bottom stress, no sea-level pressure):
+ * RHSx2d = surf_stress_x*dxt*dyh on lcu, RHSy2d = surf_stress_y*dyt*dxh on
+ * lcv; other points of RHSx2d/RHSy2d are left as passed. */
+int inmsom_wind_forcing(inmsom_ctx *ctx, const double *taux, const double *tauy,
+                        double *RHSx2d, double *RHSy2d);
+
+/* Replaces hh_init, Function/depth.f90:2-105, for the external-mode depths
+ * (its call at Control/init_pars.f90:426-430): recomputes the twelve
+ * registered external depth arrays from ssh_e, sshp_e and hhq_rest and
+ * writes them to the registered host arrays. */
+int inmsom_hh_init_external(inmsom_ctx *ctx, const double *ssh_e,
+                            const double *sshp_e);
+
+/* Guard of Control/dyncall.f90:452-516 on the resident external state:
+ * counts interior points with |ssh_e|>=10 (lu), |ubrtr_e|>=100 (lcu) or
+ * |vbrtr_e|>=100 (lcv), NaN included. */
+int inmsom_guard(inmsom_ctx *ctx, long *nbad);
+
+/* Volume and energy of the resident external state (no reference
+ * counterpart): volume = sum_lu (hhq_rest+ssh)*dx*dy,
+ * energy = sum_lu g/2*ssh^2*dx*dy + sum_lcu hu/2*u^2*dxt*dyh
+ *        + sum_lcv hv/2*v^2*dxh*dyt, with hu, hv the u/v depths of hh_init
+ * from ssh.  FP64, deterministic (fixed reduction order). */
+int inmsom_gpu_diag(inmsom_ctx *ctx, double *volume, double *energy);
+
+/* Residency control for INMSOM_RESIDENT contexts: which host arrays to
+ * refresh (to_host) or re-upload (from_host), using the pointers of the last
+ * inmsom_barotropic_dynamics call and of inmsom_gpu_register_grid. */
+#define INMSOM_SYNC_STATE   0x1u /* ubrtr_e ubrtrp_e vbrtr_e vbrtrp_e ssh_e sshp_e */
+#define INMSOM_SYNC_DEPTHS  0x2u /* the twelve external depth arrays              */
+#define INMSOM_SYNC_SCRATCH 0x4u /* vort str_t2d str_s2d fx fy RHS*_adv RHS*_dif  */
+int inmsom_gpu_sync_to_host(inmsom_ctx *ctx, unsigned what);
+int inmsom_gpu_sync_from_host(inmsom_ctx *ctx, unsigned what);
+
+/* Standalone leap-frog driver (no reference counterpart as one routine;
+ * it is the state evolution of calling barotropic_dynamics(tau=dt,
+ * nstep=1) nsub times and keeping only the saved *_e state).  Each call of
+ * barotropic_dynamics(dt,1) computes two substeps but only the first
+ * advances *_e; the second feeds the time-mean outputs only.  A standalone
+ * barotropic run does not consume those outputs, so this driver computes
+ * only the advancing substep.  Works on the resident state of an
+ * INMSOM_RESIDENT context after one barotropic_dynamics call or
+ * sync_from_host(STATE) has set it.  rhs_scale, if not NULL, holds nsub
+ * factors applied to RHSx/RHSy in the corresponding substep (a
+ * time-varying wind amplitude); the forcing is otherwise the one of the
+ * last call.  The device time of the run (ms) is returned in *ms if ms is
+ * not NULL. */
+int inmsom_run_substeps(inmsom_ctx *ctx, int nsub, double dt,
+                        const double *rhs_scale, float *ms);
+
+/* Upload the external state (*_e, in barotropic_dynamics order) and the
+ * forcing of the standalone driver, and remember these host arrays for
+ * inmsom_gpu_sync_to_host/from_host.  Counterpart of the first half of a
+ * barotropic_dynamics call (its copy-in), without running it.  mu4 may be
+ * NULL when the biharmonic term is off. */
+int inmsom_load_state(inmsom_ctx *ctx, double *ubrtr_e, double *ubrtrp_e,
+                      double *vbrtr_e, double *vbrtrp_e, double *ssh_e,
+                      double *sshp_e, const double *RHSx, const double *RHSy,
+                      const double *wflux, const double *mu, const double *mu4,
+                      const double *rdis);
+
+/* Which kernel path the context uses: 0 = per-loop kernels (exact
+ * reference rounding), 1 = fused streaming kernel.  *reason receives a
+ * static string saying why the fused path is not eligible (or "eligible"). */
+int inmsom_gpu_path(inmsom_ctx *ctx, int *path, const char **reason);
+
+int inmsom_gpu_finalize(inmsom_ctx *ctx);
+const char *inmsom_gpu_last_error(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

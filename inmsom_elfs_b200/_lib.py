@@ -1,0 +1,113 @@
+"""ctypes binding of libinmsom_gpu.so (include/inmsom_gpu.h).
+
+The library is the product: there is no Python or CPU fallback.  Loading
+fails loudly if the shared object has not been built.
+"""
+from __future__ import annotations
+
+import ctypes
+from pathlib import Path
+
+import numpy as np
+
+LIB_PATH = Path(__file__).resolve().with_name("libinmsom_gpu.so")
+
+OK, ECUDA, EARG, EGUARD, ETIMEOUT, EUNSUPPORTED = 0, 1, 2, 3, 4, 5
+RESIDENT, FORCE_GENERAL, GUARD = 0x1, 0x2, 0x4
+SYNC_STATE, SYNC_DEPTHS, SYNC_SCRATCH = 0x1, 0x2, 0x4
+
+# every exported entry point declared in include/inmsom_gpu.h
+EXPORTS = (
+    "inmsom_gpu_init", "inmsom_gpu_register_grid", "inmsom_barotropic_dynamics",
+    "inmsom_ssh_internal", "inmsom_gridcon", "inmsom_r_diss", "inmsom_wind_forcing",
+    "inmsom_hh_init_external", "inmsom_guard", "inmsom_gpu_diag",
+    "inmsom_gpu_sync_to_host", "inmsom_gpu_sync_from_host", "inmsom_run_substeps",
+    "inmsom_gpu_path", "inmsom_gpu_finalize", "inmsom_gpu_last_error", "inmsom_load_state",
+)
+
+
+class InmsomError(RuntimeError):
+    def __init__(self, code: int, message: str):
+        super().__init__(f"[{code}] {message}")
+        self.code = code
+
+
+class CBounds(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in (
+        "nx_start", "nx_end", "ny_start", "ny_end", "bnd_x1", "bnd_x2", "bnd_y1", "bnd_y2",
+        "mmm", "mm", "nnn", "nn", "periodicity_x", "periodicity_y")]
+
+
+class CConsts(ctypes.Structure):
+    _fields_ = [("time_smooth", ctypes.c_double), ("free_fall_acc", ctypes.c_double),
+                ("ref_den", ctypes.c_double), ("full_free_surface", ctypes.c_int)]
+
+
+DP = ctypes.POINTER(ctypes.c_double)
+FP = ctypes.POINTER(ctypes.c_float)
+VP = ctypes.c_void_p
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load the CUDA library (once).  Raises if it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise ImportError(f"{LIB_PATH} is missing: build it with inmsom_elfs_b200.build.build() "
+                          "(there is no CPU fallback)")
+    lib = ctypes.CDLL(str(LIB_PATH))
+    i, d, u = ctypes.c_int, ctypes.c_double, ctypes.c_uint
+    lib.inmsom_gpu_last_error.restype = ctypes.c_char_p
+    lib.inmsom_gpu_init.argtypes = [ctypes.POINTER(VP), ctypes.POINTER(CBounds),
+                                    ctypes.POINTER(CConsts), i, u]
+    lib.inmsom_gpu_register_grid.argtypes = [VP] + [FP] * 7 + [DP] * 10 + [DP] * 12
+    lib.inmsom_barotropic_dynamics.argtypes = [VP, d, i, i] + [DP] * 25
+    lib.inmsom_ssh_internal.argtypes = [VP, d] + [DP] * 9
+    lib.inmsom_gridcon.argtypes = [ctypes.POINTER(CBounds)] + [FP] * 7 + [i]
+    lib.inmsom_r_diss.argtypes = [VP, d, DP]
+    lib.inmsom_wind_forcing.argtypes = [VP, DP, DP, DP, DP]
+    lib.inmsom_hh_init_external.argtypes = [VP, DP, DP]
+    lib.inmsom_guard.argtypes = [VP, ctypes.POINTER(ctypes.c_long)]
+    lib.inmsom_gpu_diag.argtypes = [VP, DP, DP]
+    lib.inmsom_gpu_sync_to_host.argtypes = [VP, u]
+    lib.inmsom_gpu_sync_from_host.argtypes = [VP, u]
+    lib.inmsom_run_substeps.argtypes = [VP, i, d, DP, ctypes.POINTER(ctypes.c_float)]
+    lib.inmsom_load_state.argtypes = [VP] + [DP] * 12
+    lib.inmsom_gpu_path.argtypes = [VP, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_char_p)]
+    lib.inmsom_gpu_finalize.argtypes = [VP]
+    for name in EXPORTS:
+        if name != "inmsom_gpu_last_error":
+            getattr(lib, name).restype = i
+    _lib = lib
+    return lib
+
+
+def check(rc: int) -> None:
+    if rc != OK:
+        raise InmsomError(rc, load().inmsom_gpu_last_error().decode(errors="replace"))
+
+
+def dptr(a):
+    """double* of a Fortran-contiguous float64 array (None -> NULL)."""
+    if a is None:
+        return None
+    if a.dtype != np.float64 or not a.flags.f_contiguous:
+        raise TypeError("expected a Fortran-contiguous float64 array")
+    return a.ctypes.data_as(DP)
+
+
+def fptr(a):
+    if a.dtype != np.float32 or not a.flags.f_contiguous:
+        raise TypeError("expected a Fortran-contiguous float32 array")
+    return a.ctypes.data_as(FP)
+
+
+def cbounds(b) -> CBounds:
+    return CBounds(*b.astuple())
+
+
+def cconsts(c) -> CConsts:
+    return CConsts(c.time_smooth, c.free_fall_acc, c.ref_den, c.full_free_surface)

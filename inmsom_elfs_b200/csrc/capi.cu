@@ -1,0 +1,728 @@
+// C ABI of the barotropic step (include/inmsom_gpu.h): context, device
+// mirrors of the Fortran arrays, host<->device residency, and the drivers
+// that sequence the kernels of general.cu (per-loop, exact rounding) and
+// fused.cu (streaming, one kernel per substep).
+#include "inmsom_gpu.h"
+
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+#include "fused.h"
+#include "general.h"
+
+using namespace inmsom;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+int set_err(int code, const char *fmt, ...)
+{
+    char buf[512];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof buf, fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return code;
+}
+
+#define CK(call)                                                                     \
+    do {                                                                             \
+        cudaError_t e_ = (call);                                                     \
+        if (e_ != cudaSuccess)                                                       \
+            return set_err(INMSOM_ECUDA, "%s failed: %s (%s:%d)", #call,             \
+                           cudaGetErrorString(e_), __FILE__, __LINE__);              \
+    } while (0)
+
+#define CKR(expr)                  \
+    do {                           \
+        int r_ = (expr);           \
+        if (r_ != INMSOM_OK) return r_; \
+    } while (0)
+
+enum { M_LU, M_LUU, M_LUH, M_LCU, M_LCV, M_LLU, M_LLV, NMASK };
+enum { G_DX, G_DY, G_DXT, G_DYT, G_DXH, G_DYH, G_DXB, G_DYB, G_RLH, G_HREST, NMET };
+// external depths, in the argument order of hh_init/hh_shift
+enum { H_Q, H_QP, H_QN, H_U, H_UP, H_UN, H_V, H_VP, H_VN, H_H, H_HP, H_HN, NDEPTH };
+// saved state *_e, in barotropic_dynamics argument order
+enum { S_U, S_UP, S_V, S_VP, S_SSH, S_SSHP, NSTATE };
+enum { W_U, W_V, W_SSH, W_UP, W_VP, W_SSHP, W_UN, W_VN, W_SSHN, NWORK };
+enum { A_UI, A_VI, A_GX, A_GY, NACC };
+enum { F_RHSX, F_RHSY, F_WFLUX, F_MU, F_MU4, F_RDIS, NFORC };
+enum { C_VORT, C_STRT, C_STRS, C_FX, C_FY, C_ADVX, C_ADVY, C_DIFX, C_DIFY, NSCR };
+enum { I_SSH, I_SSHP, I_U, I_V, I_WFLUX, I_NEW, I_HQN, I_HUN, I_HVN, I_HHN, NINT };
+
+}  // namespace
+
+struct inmsom_ctx {
+    Dom dom{};
+    Consts c{};
+    unsigned flags = 0;
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    size_t nbytes = 0;  // one double field on the device
+
+    float *mask[NMASK] = {};
+    double *met[NMET] = {};
+    double *depth[NDEPTH] = {};
+    double *state[NSTATE] = {};
+    double *work[NWORK] = {};
+    double *acc[NACC] = {};
+    double *forc[NFORC] = {};
+    double *scr[NSCR] = {};
+    double *intl[NINT] = {};
+    double *tmp[4] = {};
+    unsigned long long *d_nbad = nullptr;
+    double *d_rows = nullptr, *d_out = nullptr;
+
+    // host arrays registered / last passed
+    double *h_depth[NDEPTH] = {};
+    double *h_state[NSTATE] = {};
+    double *h_scr[NSCR] = {};
+
+    bool grid_ok = false;
+    bool state_on_device = false;   // resident state has been uploaded
+    bool depths_current = false;    // depth[] == hh_init(state) or evolved faithfully
+    bool scratch_on_device = false;
+
+    fused::Plan plan{};              // fused-path layout and eligibility
+    bool fused_ok = false;
+    const char *fused_reason = "grid not registered";
+
+    GridDev gdev() const
+    {
+        GridDev g;
+        g.lu = mask[M_LU]; g.luu = mask[M_LUU]; g.luh = mask[M_LUH];
+        g.lcu = mask[M_LCU]; g.lcv = mask[M_LCV]; g.llu = mask[M_LLU]; g.llv = mask[M_LLV];
+        g.dx = met[G_DX]; g.dy = met[G_DY]; g.dxt = met[G_DXT]; g.dyt = met[G_DYT];
+        g.dxh = met[G_DXH]; g.dyh = met[G_DYH]; g.dxb = met[G_DXB]; g.dyb = met[G_DYB];
+        g.rlh = met[G_RLH]; g.hrest = met[G_HREST];
+        return g;
+    }
+};
+
+namespace {
+
+int check_bounds(const inmsom_bounds *b)
+{
+    if (!b) return set_err(INMSOM_EARG, "bounds is NULL");
+    if (b->nx_start > b->nx_end || b->ny_start > b->ny_end)
+        return set_err(INMSOM_EARG, "empty interior %d..%d x %d..%d", b->nx_start, b->nx_end,
+                       b->ny_start, b->ny_end);
+    if (b->bnd_x1 > b->nx_start - 2 || b->bnd_x2 < b->nx_end + 2 || b->bnd_y1 > b->ny_start - 2 ||
+        b->bnd_y2 < b->ny_end + 2)
+        return set_err(INMSOM_EARG, "array bounds must leave a 2-point halo around the interior");
+    if ((b->periodicity_x && (b->mmm - 1 < b->bnd_x1 || b->mm + 1 > b->bnd_x2)) ||
+        (b->periodicity_y && (b->nnn - 1 < b->bnd_y1 || b->nn + 1 > b->bnd_y2)))
+        return set_err(INMSOM_EARG, "periodic wrap columns/rows outside the arrays");
+    return INMSOM_OK;
+}
+
+Dom make_dom(const inmsom_bounds *b, long long pitch)
+{
+    Dom d;
+    d.nx_start = b->nx_start; d.nx_end = b->nx_end; d.ny_start = b->ny_start; d.ny_end = b->ny_end;
+    d.bnd_x1 = b->bnd_x1; d.bnd_x2 = b->bnd_x2; d.bnd_y1 = b->bnd_y1; d.bnd_y2 = b->bnd_y2;
+    d.mmm = b->mmm; d.mm = b->mm; d.nnn = b->nnn; d.nn = b->nn;
+    d.px = b->periodicity_x; d.py = b->periodicity_y;
+    d.pitch = pitch;
+    return d;
+}
+
+template <typename T>
+int dalloc(inmsom_ctx *c, T **p, size_t elem)
+{
+    size_t bytes = (size_t)c->dom.pitch * (size_t)c->dom.nya() * elem;
+    CK(cudaMalloc((void **)p, bytes));
+    CK(cudaMemsetAsync(*p, 0, bytes, c->stream));
+    return INMSOM_OK;
+}
+
+// host (Fortran, ld = nxa) <-> device (pitched)
+template <typename T>
+int h2d(inmsom_ctx *c, T *dev, const T *host)
+{
+    if (!host) return set_err(INMSOM_EARG, "NULL host array");
+    const size_t w = (size_t)c->dom.nxa() * sizeof(T);
+    CK(cudaMemcpy2DAsync(dev, (size_t)c->dom.pitch * sizeof(T), host, w, w, (size_t)c->dom.nya(),
+                         cudaMemcpyHostToDevice, c->stream));
+    return INMSOM_OK;
+}
+
+template <typename T>
+int d2h(inmsom_ctx *c, T *host, const T *dev)
+{
+    if (!host) return set_err(INMSOM_EARG, "NULL host array");
+    const size_t w = (size_t)c->dom.nxa() * sizeof(T);
+    CK(cudaMemcpy2DAsync(host, w, dev, (size_t)c->dom.pitch * sizeof(T), w, (size_t)c->dom.nya(),
+                         cudaMemcpyDeviceToHost, c->stream));
+    return INMSOM_OK;
+}
+
+int sync_stream(inmsom_ctx *c)
+{
+    CK(cudaStreamSynchronize(c->stream));
+    CK(cudaGetLastError());
+    return INMSOM_OK;
+}
+
+int alloc_set(inmsom_ctx *c, double **arr, int n)
+{
+    for (int k = 0; k < n; k++)
+        if (!arr[k]) CKR(dalloc(c, &arr[k], sizeof(double)));
+    return INMSOM_OK;
+}
+
+// external depths := hh_init(ssh_e, sshp_e), Function/depth.f90:2-105
+void depths_from_state(inmsom_ctx *c)
+{
+    double **h = c->depth;
+    general::hh_init(c->dom, c->gdev(), c->c, h[H_Q], h[H_QP], h[H_QN], h[H_U], h[H_UP], h[H_UN],
+                     h[H_V], h[H_VP], h[H_VN], h[H_H], h[H_HP], h[H_HN], c->state[S_SSH],
+                     c->state[S_SSHP], c->stream);
+    c->depths_current = true;
+}
+
+// One substep of the Function/vel_ssh.f90:484-650 loop body on the work
+// arrays, general path.  acc receives the time-mean sums (may be scratch).
+void general_substep(inmsom_ctx *c, double ti, int nstep, int ksw4, double rhs_scale,
+                     bool shift_depths)
+{
+    const Dom &d = c->dom;
+    const GridDev g = c->gdev();
+    cudaStream_t s = c->stream;
+    double **w = c->work, **h = c->depth, **f = c->forc, **x = c->scr;
+
+    general::continuity(d, g, c->c, ti, w[W_SSHN], w[W_SSHP], w[W_U], w[W_V], h[H_U], h[H_V],
+                        f[F_WFLUX], s);
+    general::halo(d, w[W_SSHN], s);
+    if (c->c.ffs > 0) general::hh_update(d, g, h[H_QN], h[H_UN], h[H_VN], h[H_HN], w[W_SSHN], s);
+    general::stress_components(d, g, w[W_UP], w[W_VP], x[C_STRT], x[C_STRS], s);
+    general::uv_trans(d, g, w[W_U], w[W_V], x[C_VORT], h[H_U], h[H_V], h[H_H], x[C_ADVX],
+                      x[C_ADVY], s);
+    general::uv_diff2(d, g, f[F_MU], x[C_STRT], x[C_STRS], h[H_Q], h[H_H], x[C_DIFX], x[C_DIFY], s);
+    if (ksw4 > 0)
+        general::uv_diff4(d, g, f[F_MU4], x[C_STRT], x[C_STRS], x[C_FX], x[C_FY], h[H_Q], h[H_U],
+                          h[H_V], h[H_H], x[C_DIFX], x[C_DIFY], s);
+    general::MomentumArgs a;
+    a.un = w[W_UN]; a.vn = w[W_VN];
+    a.ubrtr_i = c->acc[A_UI]; a.vbrtr_i = c->acc[A_VI]; a.gx = c->acc[A_GX]; a.gy = c->acc[A_GY];
+    a.u = w[W_U]; a.v = w[W_V]; a.up = w[W_UP]; a.vp = w[W_VP]; a.ssh = w[W_SSH]; a.sshn = w[W_SSHN];
+    a.hu = h[H_U]; a.hup = h[H_UP]; a.hun = h[H_UN]; a.hv = h[H_V]; a.hvp = h[H_VP]; a.hvn = h[H_VN];
+    a.hh = h[H_H];
+    a.rhsx = f[F_RHSX]; a.rhsy = f[F_RHSY]; a.difx = x[C_DIFX]; a.dify = x[C_DIFY];
+    a.advx = x[C_ADVX]; a.advy = x[C_ADVY]; a.rdis = f[F_RDIS]; a.rhs_scale = rhs_scale;
+    general::momentum(d, g, c->c, ti, nstep, a, s);
+    general::halo(d, w[W_UN], s);
+    general::halo(d, w[W_VN], s);
+    general::asselin3(d, g, c->c, (double)nstep, w[W_SSH], w[W_SSHP], w[W_SSHN], w[W_U], w[W_UP],
+                      w[W_UN], w[W_V], w[W_VP], w[W_VN], s);
+    if (c->c.ffs > 0 && shift_depths) general::hh_shift(d, g, c->c, h, nstep, s);
+}
+
+// Function/vel_ssh.f90:465-675 on the device, general path
+void general_dynamics(inmsom_ctx *c, double tau, int nstep, int ksw4)
+{
+    const Dom &d = c->dom;
+    cudaStream_t s = c->stream;
+    double **w = c->work, **st = c->state;
+    const double ti = tau / (double)nstep;
+    general::fill(d, w[W_UN], 0.0, s);
+    general::fill(d, w[W_VN], 0.0, s);
+    general::fill(d, w[W_SSHN], 0.0, s);
+    general::copy(d, w[W_UP], st[S_UP], s);
+    general::copy(d, w[W_VP], st[S_VP], s);
+    general::copy(d, w[W_SSHP], st[S_SSHP], s);
+    general::copy(d, w[W_U], st[S_U], s);
+    general::copy(d, w[W_V], st[S_V], s);
+    general::copy(d, w[W_SSH], st[S_SSH], s);
+    for (int k = 0; k < NACC; k++) general::fill(d, c->acc[k], 0.0, s);
+    for (int step = 1; step <= 2 * nstep; step++) {
+        general_substep(c, ti, nstep, ksw4, 1.0, true);
+        if (step == nstep) {
+            general::copy(d, st[S_UP], w[W_UP], s);
+            general::copy(d, st[S_VP], w[W_VP], s);
+            general::copy(d, st[S_SSHP], w[W_SSHP], s);
+            general::copy(d, st[S_U], w[W_U], s);
+            general::copy(d, st[S_V], w[W_V], s);
+            general::copy(d, st[S_SSH], w[W_SSH], s);
+        }
+    }
+    general::halo(d, c->acc[A_UI], s);
+    general::halo(d, c->acc[A_VI], s);
+    if (c->c.ffs > 0) depths_from_state(c);
+}
+
+int ensure_grid(inmsom_ctx *c)
+{
+    if (!c) return set_err(INMSOM_EARG, "context is NULL");
+    if (!c->grid_ok) return set_err(INMSOM_EARG, "inmsom_gpu_register_grid has not been called");
+    CK(cudaSetDevice(c->device));
+    return INMSOM_OK;
+}
+
+int run_guard(inmsom_ctx *c, long *nbad)
+{
+    CK(cudaMemsetAsync(c->d_nbad, 0, sizeof(unsigned long long), c->stream));
+    general::guard(c->dom, c->gdev(), c->state[S_SSH], c->state[S_U], c->state[S_V], c->d_nbad,
+                   c->stream);
+    unsigned long long h = 0;
+    CK(cudaMemcpyAsync(&h, c->d_nbad, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    CKR(sync_stream(c));
+    *nbad = (long)h;
+    return INMSOM_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+extern "C" {
+
+const char *inmsom_gpu_last_error(void) { return g_last_error.c_str(); }
+
+int inmsom_gpu_init(inmsom_ctx **out, const inmsom_bounds *b, const inmsom_consts *k, int device,
+                    unsigned flags)
+{
+    if (!out || !k) return set_err(INMSOM_EARG, "NULL argument to inmsom_gpu_init");
+    *out = nullptr;
+    CKR(check_bounds(b));
+    int ndev = 0;
+    CK(cudaGetDeviceCount(&ndev));
+    if (device < 0 || device >= ndev) return set_err(INMSOM_EARG, "device %d of %d", device, ndev);
+    CK(cudaSetDevice(device));
+    inmsom_ctx *c = new inmsom_ctx();
+    c->device = device;
+    c->flags = flags;
+    c->c.ts = k->time_smooth;
+    c->c.g = k->free_fall_acc;
+    c->c.rho = k->ref_den;
+    c->c.ffs = k->full_free_surface;
+    const int nxa = b->bnd_x2 - b->bnd_x1 + 1;
+    c->plan = fused::make_plan(*b);
+    long long need = nxa > c->plan.min_pitch ? nxa : c->plan.min_pitch;
+    long long pitch = (need + 31) / 32 * 32;  // 256-byte rows
+    c->dom = make_dom(b, pitch);
+    cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
+    if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+    if (e != cudaSuccess) {
+        delete c;
+        return set_err(INMSOM_ECUDA, "stream/event creation failed: %s", cudaGetErrorString(e));
+    }
+    *out = c;
+    return INMSOM_OK;
+}
+
+int inmsom_gpu_finalize(inmsom_ctx *c)
+{
+    if (!c) return INMSOM_OK;
+    cudaSetDevice(c->device);
+    if (c->stream) cudaStreamSynchronize(c->stream);
+    for (auto &p : c->mask) cudaFree(p);
+    for (auto &p : c->met) cudaFree(p);
+    for (auto &p : c->depth) cudaFree(p);
+    for (auto &p : c->state) cudaFree(p);
+    for (auto &p : c->work) cudaFree(p);
+    for (auto &p : c->acc) cudaFree(p);
+    for (auto &p : c->forc) cudaFree(p);
+    for (auto &p : c->scr) cudaFree(p);
+    for (auto &p : c->intl) cudaFree(p);
+    for (auto &p : c->tmp) cudaFree(p);
+    cudaFree(c->d_nbad);
+    cudaFree(c->d_rows);
+    cudaFree(c->d_out);
+    fused::free_plan(c->plan);
+    if (c->ev0) cudaEventDestroy(c->ev0);
+    if (c->ev1) cudaEventDestroy(c->ev1);
+    if (c->stream) cudaStreamDestroy(c->stream);
+    delete c;
+    return INMSOM_OK;
+}
+
+int inmsom_gpu_register_grid(inmsom_ctx *c, const float *lu, const float *luu, const float *luh,
+                             const float *lcu, const float *lcv, const float *llu, const float *llv,
+                             const double *dx, const double *dy, const double *dxt,
+                             const double *dyt, const double *dxh, const double *dyh,
+                             const double *dxb, const double *dyb, const double *rlh_s,
+                             const double *hhq_rest, double *hhq_e, double *hhqp_e,
+                             double *hhqn_e, double *hhu_e, double *hhup_e, double *hhun_e,
+                             double *hhv_e, double *hhvp_e, double *hhvn_e, double *hhh_e,
+                             double *hhhp_e, double *hhhn_e)
+{
+    if (!c) return set_err(INMSOM_EARG, "context is NULL");
+    CK(cudaSetDevice(c->device));
+    const float *hm[NMASK] = {lu, luu, luh, lcu, lcv, llu, llv};
+    const double *hg[NMET] = {dx, dy, dxt, dyt, dxh, dyh, dxb, dyb, rlh_s, hhq_rest};
+    double *hd[NDEPTH] = {hhq_e, hhqp_e, hhqn_e, hhu_e, hhup_e, hhun_e,
+                          hhv_e, hhvp_e, hhvn_e, hhh_e, hhhp_e, hhhn_e};
+    for (int k = 0; k < NMASK; k++)
+        if (!hm[k]) return set_err(INMSOM_EARG, "mask %d is NULL", k);
+    for (int k = 0; k < NMET; k++)
+        if (!hg[k]) return set_err(INMSOM_EARG, "grid array %d is NULL", k);
+    int ndepth = 0;
+    for (int k = 0; k < NDEPTH; k++) ndepth += hd[k] != nullptr;
+    if (ndepth != 0 && ndepth != NDEPTH)
+        return set_err(INMSOM_EARG, "pass all twelve depth arrays or none");
+
+    for (int k = 0; k < NMASK; k++) {
+        if (!c->mask[k]) CKR(dalloc(c, &c->mask[k], sizeof(float)));
+        CKR(h2d(c, c->mask[k], hm[k]));
+    }
+    CKR(alloc_set(c, c->met, NMET));
+    for (int k = 0; k < NMET; k++) CKR(h2d(c, c->met[k], hg[k]));
+    CKR(alloc_set(c, c->depth, NDEPTH));
+    for (int k = 0; k < NDEPTH; k++) {
+        c->h_depth[k] = hd[k];
+        if (hd[k]) CKR(h2d(c, c->depth[k], (const double *)hd[k]));
+    }
+    c->depths_current = ndepth == NDEPTH;
+    CKR(alloc_set(c, c->state, NSTATE));
+    CKR(alloc_set(c, c->work, NWORK));
+    CKR(alloc_set(c, c->acc, NACC));
+    CKR(alloc_set(c, c->forc, NFORC));
+    CKR(alloc_set(c, c->scr, NSCR));
+    if (!c->d_nbad) CK(cudaMalloc(&c->d_nbad, sizeof(unsigned long long)));
+    const int nrows = c->dom.ny_end - c->dom.ny_start + 1;
+    if (!c->d_rows) CK(cudaMalloc(&c->d_rows, 2 * (size_t)nrows * sizeof(double)));
+    if (!c->d_out) CK(cudaMalloc(&c->d_out, 2 * sizeof(double)));
+    c->grid_ok = true;
+    c->state_on_device = false;
+    c->scratch_on_device = false;
+    // fused-path eligibility and its static tables (host-side checks)
+    c->fused_ok = false;
+    if (c->flags & INMSOM_FORCE_GENERAL) {
+        c->fused_reason = "INMSOM_FORCE_GENERAL";
+    } else {
+        c->fused_reason = fused::check_eligible(c->plan, c->dom, c->c, hm, hg);
+        if (!c->fused_reason) {
+            CKR(fused::setup(c->plan, c->dom, c->c, hm, hg, c->met[G_HREST], c->mask[M_LU], c->stream) == 0
+                    ? INMSOM_OK
+                    : set_err(INMSOM_ECUDA, "fused path set-up failed: %s",
+                              cudaGetErrorString(cudaGetLastError())));
+            c->fused_ok = true;
+            c->fused_reason = "eligible";
+        }
+    }
+    return sync_stream(c);
+}
+
+int inmsom_gpu_path(inmsom_ctx *c, int *path, const char **reason)
+{
+    if (!c || !path) return set_err(INMSOM_EARG, "NULL argument");
+    *path = c->fused_ok ? 1 : 0;
+    if (reason) *reason = c->fused_reason;
+    return INMSOM_OK;
+}
+
+int inmsom_barotropic_dynamics(inmsom_ctx *c, double tau, int nstep, int ksw4, double *ubrtr_e,
+                               double *ubrtrp_e, double *vbrtr_e, double *vbrtrp_e, double *ssh_e,
+                               double *sshp_e, double *ubrtr_i, double *vbrtr_i,
+                               double *ssh4gradx, double *ssh4grady, const double *RHSx,
+                               const double *RHSy, const double *wflux, const double *mu,
+                               const double *mu4, double *vort, double *str_t2d,
+                               double *str_s2d, double *fx, double *fy, const double *rdis,
+                               double *RHSx_adv, double *RHSy_adv, double *RHSx_dif,
+                               double *RHSy_dif)
+{
+    CKR(ensure_grid(c));
+    if (nstep < 1) return set_err(INMSOM_EARG, "nstep = %d < 1", nstep);
+    if (!(tau > 0.0)) return set_err(INMSOM_EARG, "tau must be > 0");
+    double *hs[NSTATE] = {ubrtr_e, ubrtrp_e, vbrtr_e, vbrtrp_e, ssh_e, sshp_e};
+    double *ha[NACC] = {ubrtr_i, vbrtr_i, ssh4gradx, ssh4grady};
+    const double *hf[NFORC] = {RHSx, RHSy, wflux, mu, mu4, rdis};
+    double *hc[NSCR] = {vort, str_t2d, str_s2d, fx, fy, RHSx_adv, RHSy_adv, RHSx_dif, RHSy_dif};
+    const bool resident = (c->flags & INMSOM_RESIDENT) != 0;
+    for (int k = 0; k < NSTATE; k++) c->h_state[k] = hs[k];
+    for (int k = 0; k < NSCR; k++) c->h_scr[k] = hc[k];
+
+    if (!resident || !c->state_on_device) {
+        for (int k = 0; k < NSTATE; k++) CKR(h2d(c, c->state[k], (const double *)hs[k]));
+        c->state_on_device = true;
+        fused::mark_state_changed(c->plan);
+    }
+    if (!resident || !c->scratch_on_device) {
+        for (int k = 0; k < NSCR; k++) CKR(h2d(c, c->scr[k], (const double *)hc[k]));
+        c->scratch_on_device = true;
+    }
+    for (int k = 0; k < NFORC; k++) {
+        if (k == F_MU4 && ksw4 <= 0 && !mu4) continue;
+        CKR(h2d(c, c->forc[k], hf[k]));
+    }
+    if (!resident) {
+        for (int k = 0; k < NDEPTH; k++)
+            if (c->h_depth[k]) CKR(h2d(c, c->depth[k], (const double *)c->h_depth[k]));
+        if (c->h_depth[0]) c->depths_current = true;
+    }
+    if (!c->depths_current) depths_from_state(c);
+
+    int rc = INMSOM_OK;
+    if (c->fused_ok && ksw4 <= 0) {
+        if (fused::dynamics(c->plan, c->dom, c->c, tau, nstep, c->state, c->acc, c->forc,
+                            c->stream))
+            return set_err(INMSOM_ECUDA, "fused dynamics failed: %s",
+                           cudaGetErrorString(cudaGetLastError()));
+        if (c->plan.last_flags & fused::FLAG_TIMEOUT)
+            return set_err(INMSOM_ETIMEOUT, "fused kernel: a bounded TMA wait timed out");
+        if (c->c.ffs > 0) depths_from_state(c);
+    } else {
+        general_dynamics(c, tau, nstep, ksw4);
+    }
+
+    for (int k = 0; k < NACC; k++) CKR(d2h(c, ha[k], c->acc[k]));
+    if (!resident) {
+        for (int k = 0; k < NSTATE; k++) CKR(d2h(c, hs[k], c->state[k]));
+        for (int k = 0; k < NSCR; k++) CKR(d2h(c, hc[k], c->scr[k]));
+        for (int k = 0; k < NDEPTH; k++)
+            if (c->h_depth[k]) CKR(d2h(c, c->h_depth[k], c->depth[k]));
+    }
+    CKR(sync_stream(c));
+    if (c->flags & INMSOM_GUARD) {
+        long nbad = 0;
+        CKR(run_guard(c, &nbad));
+        if (nbad) return set_err(INMSOM_EGUARD, "guard: %ld interior points out of range or NaN", nbad);
+    }
+    return rc;
+}
+
+int inmsom_load_state(inmsom_ctx *c, double *ubrtr_e, double *ubrtrp_e, double *vbrtr_e,
+                      double *vbrtrp_e, double *ssh_e, double *sshp_e, const double *RHSx,
+                      const double *RHSy, const double *wflux, const double *mu, const double *mu4,
+                      const double *rdis)
+{
+    CKR(ensure_grid(c));
+    double *hs[NSTATE] = {ubrtr_e, ubrtrp_e, vbrtr_e, vbrtrp_e, ssh_e, sshp_e};
+    const double *hf[NFORC] = {RHSx, RHSy, wflux, mu, mu4, rdis};
+    for (int k = 0; k < NSTATE; k++) {
+        CKR(h2d(c, c->state[k], (const double *)hs[k]));
+        c->h_state[k] = hs[k];
+    }
+    for (int k = 0; k < NFORC; k++) {
+        if (k == F_MU4 && !mu4) continue;
+        CKR(h2d(c, c->forc[k], hf[k]));
+    }
+    c->state_on_device = true;
+    fused::mark_state_changed(c->plan);
+    if (c->fused_ok || !c->depths_current) depths_from_state(c);
+    return sync_stream(c);
+}
+
+int inmsom_run_substeps(inmsom_ctx *c, int nsub, double dt, const double *rhs_scale, float *ms)
+{
+    CKR(ensure_grid(c));
+    if (nsub < 0) return set_err(INMSOM_EARG, "nsub < 0");
+    if (!(dt > 0.0)) return set_err(INMSOM_EARG, "dt must be > 0");
+    if (!c->state_on_device)
+        return set_err(INMSOM_EARG, "no resident state: call inmsom_load_state or barotropic_dynamics first");
+    CK(cudaEventRecord(c->ev0, c->stream));
+    if (c->fused_ok) {
+        if (fused::run_substeps(c->plan, c->dom, c->c, nsub, dt, rhs_scale, c->state, c->forc,
+                                c->stream))
+            return set_err(INMSOM_ECUDA, "fused substeps failed: %s",
+                           cudaGetErrorString(cudaGetLastError()));
+        c->depths_current = false;
+        if (c->plan.last_flags & fused::FLAG_TIMEOUT)
+            return set_err(INMSOM_ETIMEOUT, "fused kernel: a bounded TMA wait timed out");
+    } else {
+        // nsub calls of barotropic_dynamics(dt, 1) keeping *_e: the first
+        // substep of each call, run in place on the saved state, followed by
+        // the hh_init that ends every call
+        const Dom &d = c->dom;
+        double **w = c->work, **st = c->state;
+        double *saved[NWORK];
+        for (int k = 0; k < NWORK; k++) saved[k] = w[k];
+        w[W_U] = st[S_U]; w[W_UP] = st[S_UP]; w[W_V] = st[S_V]; w[W_VP] = st[S_VP];
+        w[W_SSH] = st[S_SSH]; w[W_SSHP] = st[S_SSHP];
+        general::fill(d, w[W_UN], 0.0, c->stream);
+        general::fill(d, w[W_VN], 0.0, c->stream);
+        general::fill(d, w[W_SSHN], 0.0, c->stream);
+        if (!c->depths_current) depths_from_state(c);
+        for (int k = 0; k < nsub; k++) {
+            general_substep(c, dt, 1, 0, rhs_scale ? rhs_scale[k] : 1.0, false);
+            if (c->c.ffs > 0) depths_from_state(c);
+        }
+        for (int k = 0; k < NWORK; k++) w[k] = saved[k];
+    }
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CKR(sync_stream(c));
+    if (ms) CK(cudaEventElapsedTime(ms, c->ev0, c->ev1));
+    if (c->flags & INMSOM_GUARD) {
+        long nbad = 0;
+        CKR(run_guard(c, &nbad));
+        if (nbad) return set_err(INMSOM_EGUARD, "guard: %ld interior points out of range or NaN", nbad);
+    }
+    return INMSOM_OK;
+}
+
+int inmsom_ssh_internal(inmsom_ctx *c, double tau, double *ssh_i, double *sshp_i, const double *u,
+                        const double *v, const double *wflux, double *hhqn, double *hhun,
+                        double *hhvn, double *hhhn)
+{
+    CKR(ensure_grid(c));
+    CKR(alloc_set(c, c->intl, NINT));
+    double **I = c->intl;
+    CKR(h2d(c, I[I_SSH], (const double *)ssh_i));
+    CKR(h2d(c, I[I_SSHP], (const double *)sshp_i));
+    CKR(h2d(c, I[I_U], u));
+    CKR(h2d(c, I[I_V], v));
+    CKR(h2d(c, I[I_WFLUX], wflux));
+    double *hi[4] = {hhqn, hhun, hhvn, hhhn};
+    for (int k = 0; k < 4; k++) CKR(h2d(c, I[I_HQN + k], (const double *)hi[k]));
+    const Dom &d = c->dom;
+    const GridDev g = c->gdev();
+    general::fill(d, I[I_NEW], 0.0, c->stream);  // vel_ssh.f90:704-705
+    general::continuity(d, g, c->c, tau, I[I_NEW], I[I_SSHP], I[I_U], I[I_V], nullptr, nullptr,
+                        I[I_WFLUX], c->stream);
+    general::halo(d, I[I_NEW], c->stream);
+    if (c->c.ffs > 0)
+        general::hh_update(d, g, I[I_HQN], I[I_HUN], I[I_HVN], I[I_HHN], I[I_NEW], c->stream);
+    general::asselin3(d, g, c->c, 1.0, I[I_SSH], I[I_SSHP], I[I_NEW], nullptr, nullptr, nullptr,
+                      nullptr, nullptr, nullptr, c->stream);
+    CKR(d2h(c, ssh_i, I[I_SSH]));
+    CKR(d2h(c, sshp_i, I[I_SSHP]));
+    for (int k = 0; k < 4; k++) CKR(d2h(c, hi[k], I[I_HQN + k]));
+    return sync_stream(c);
+}
+
+int inmsom_gridcon(const inmsom_bounds *b, const float *lu, float *luu, float *luh, float *llu,
+                   float *llv, float *lcu, float *lcv, int device)
+{
+    CKR(check_bounds(b));
+    if (!lu || !luu || !luh || !llu || !llv || !lcu || !lcv)
+        return set_err(INMSOM_EARG, "NULL mask array");
+    CK(cudaSetDevice(device));
+    const int nxa = b->bnd_x2 - b->bnd_x1 + 1, nya = b->bnd_y2 - b->bnd_y1 + 1;
+    Dom d = make_dom(b, nxa);
+    const size_t bytes = (size_t)nxa * nya * sizeof(float);
+    float *dv[7] = {};
+    const float *src[7] = {lu, luu, luh, llu, llv, lcu, lcv};
+    float *dst[7] = {nullptr, luu, luh, llu, llv, lcu, lcv};
+    int rc = INMSOM_OK;
+    for (int k = 0; k < 7 && rc == INMSOM_OK; k++) {
+        cudaError_t e = cudaMalloc(&dv[k], bytes);
+        if (e == cudaSuccess) e = cudaMemcpy(dv[k], src[k], bytes, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) rc = set_err(INMSOM_ECUDA, "gridcon upload: %s", cudaGetErrorString(e));
+    }
+    if (rc == INMSOM_OK) {
+        general::gridcon(d, dv[0], dv[1], dv[2], dv[3], dv[4], dv[5], dv[6], 0);
+        cudaError_t e = cudaDeviceSynchronize();
+        if (e == cudaSuccess) e = cudaGetLastError();
+        for (int k = 1; k < 7 && e == cudaSuccess; k++)
+            e = cudaMemcpy(dst[k], dv[k], bytes, cudaMemcpyDeviceToHost);
+        if (e != cudaSuccess) rc = set_err(INMSOM_ECUDA, "gridcon: %s", cudaGetErrorString(e));
+    }
+    for (auto p : dv) cudaFree(p);
+    return rc;
+}
+
+int inmsom_r_diss(inmsom_ctx *c, double r_fric, double *r_diss)
+{
+    CKR(ensure_grid(c));
+    if (!c->tmp[0]) CKR(dalloc(c, &c->tmp[0], sizeof(double)));
+    CKR(h2d(c, c->tmp[0], (const double *)r_diss));
+    general::r_diss(c->dom, c->gdev(), r_fric, c->tmp[0], c->stream);
+    CKR(d2h(c, r_diss, c->tmp[0]));
+    return sync_stream(c);
+}
+
+int inmsom_wind_forcing(inmsom_ctx *c, const double *taux, const double *tauy, double *RHSx2d,
+                        double *RHSy2d)
+{
+    CKR(ensure_grid(c));
+    for (int k = 0; k < 4; k++)
+        if (!c->tmp[k]) CKR(dalloc(c, &c->tmp[k], sizeof(double)));
+    CKR(h2d(c, c->tmp[0], taux));
+    CKR(h2d(c, c->tmp[1], tauy));
+    CKR(h2d(c, c->tmp[2], (const double *)RHSx2d));
+    CKR(h2d(c, c->tmp[3], (const double *)RHSy2d));
+    general::wind_forcing(c->dom, c->gdev(), c->c, c->tmp[0], c->tmp[1], c->tmp[2], c->tmp[3],
+                          c->stream);
+    CKR(d2h(c, RHSx2d, c->tmp[2]));
+    CKR(d2h(c, RHSy2d, c->tmp[3]));
+    return sync_stream(c);
+}
+
+int inmsom_hh_init_external(inmsom_ctx *c, const double *ssh_e, const double *sshp_e)
+{
+    CKR(ensure_grid(c));
+    CKR(h2d(c, c->state[S_SSH], ssh_e));
+    CKR(h2d(c, c->state[S_SSHP], sshp_e));
+    fused::mark_state_changed(c->plan);
+    depths_from_state(c);
+    for (int k = 0; k < NDEPTH; k++)
+        if (c->h_depth[k]) CKR(d2h(c, c->h_depth[k], c->depth[k]));
+    // the other state fields are not known here: the next call uploads them
+    c->state_on_device = false;
+    return sync_stream(c);
+}
+
+int inmsom_guard(inmsom_ctx *c, long *nbad)
+{
+    CKR(ensure_grid(c));
+    if (!nbad) return set_err(INMSOM_EARG, "nbad is NULL");
+    if (!c->state_on_device) return set_err(INMSOM_EARG, "no resident state");
+    return run_guard(c, nbad);
+}
+
+int inmsom_gpu_diag(inmsom_ctx *c, double *volume, double *energy)
+{
+    CKR(ensure_grid(c));
+    if (!volume || !energy) return set_err(INMSOM_EARG, "NULL output");
+    if (!c->state_on_device) return set_err(INMSOM_EARG, "no resident state");
+    if (!c->depths_current) depths_from_state(c);
+    const int nrows = c->dom.ny_end - c->dom.ny_start + 1;
+    general::diag_rows(c->dom, c->gdev(), c->c, c->state[S_SSH], c->state[S_U], c->state[S_V],
+                       c->depth[H_U], c->depth[H_V], c->d_rows, c->stream);
+    general::diag_final(nrows, c->d_rows, c->d_out, c->stream);
+    double h[2];
+    CK(cudaMemcpyAsync(h, c->d_out, sizeof h, cudaMemcpyDeviceToHost, c->stream));
+    CKR(sync_stream(c));
+    *volume = h[0];
+    *energy = h[1];
+    return INMSOM_OK;
+}
+
+int inmsom_gpu_sync_to_host(inmsom_ctx *c, unsigned what)
+{
+    CKR(ensure_grid(c));
+    if (what & INMSOM_SYNC_STATE) {
+        if (!c->state_on_device) return set_err(INMSOM_EARG, "no resident state");
+        for (int k = 0; k < NSTATE; k++) CKR(d2h(c, c->h_state[k], c->state[k]));
+    }
+    if (what & INMSOM_SYNC_DEPTHS) {
+        if (!c->depths_current) depths_from_state(c);
+        for (int k = 0; k < NDEPTH; k++)
+            if (c->h_depth[k]) CKR(d2h(c, c->h_depth[k], c->depth[k]));
+    }
+    if (what & INMSOM_SYNC_SCRATCH)
+        for (int k = 0; k < NSCR; k++) CKR(d2h(c, c->h_scr[k], c->scr[k]));
+    return sync_stream(c);
+}
+
+int inmsom_gpu_sync_from_host(inmsom_ctx *c, unsigned what)
+{
+    CKR(ensure_grid(c));
+    if (what & INMSOM_SYNC_STATE) {
+        for (int k = 0; k < NSTATE; k++) CKR(h2d(c, c->state[k], (const double *)c->h_state[k]));
+        c->state_on_device = true;
+        fused::mark_state_changed(c->plan);
+        if (c->fused_ok) c->depths_current = false;
+    }
+    if (what & INMSOM_SYNC_DEPTHS) {
+        for (int k = 0; k < NDEPTH; k++)
+            if (c->h_depth[k]) CKR(h2d(c, c->depth[k], (const double *)c->h_depth[k]));
+        c->depths_current = true;
+    }
+    if (what & INMSOM_SYNC_SCRATCH) {
+        for (int k = 0; k < NSCR; k++) CKR(h2d(c, c->scr[k], (const double *)c->h_scr[k]));
+        c->scratch_on_device = true;
+    }
+    return sync_stream(c);
+}
+
+}  // extern "C"

@@ -1,0 +1,95 @@
+// Fused streaming kernel of the barotropic step ("fused path").
+//
+// One kernel launch performs one whole leap-frog substep of
+// Function/vel_ssh.f90:484-612 (continuity, depth update, stress,
+// advection, viscosity, Coriolis, pressure gradient, drag, momentum,
+// time-mean accumulation and Robert-Asselin filter with time shift) for the
+// whole basin.  Each CTA owns a strip of columns and marches down a chunk of
+// rows; input rows arrive through a ring of shared-memory slots filled by
+// 1-D bulk TMA copies (cp.async.bulk, no multicast) tracked by mbarriers.
+//
+// The fused path derives the external depths from SSH each substep
+// (hq = H + ssh and its mask-weighted averages, which is what hh_init,
+// hh_update and hh_shift produce up to rounding) and the derived masks from
+// a 1-bit T mask, so per cell and substep it reads u, v, ssh at two levels,
+// H and the forcing, and writes the six new state values: the 120 bytes of
+// the algorithmic minimum plus one bit of mask.
+//
+// It is used when the grid allows (make_plan/check_eligible say why not):
+// one domain whose halo is land, metrics and Coriolis constant along rows
+// (every Cartesian or spherical INMSOM grid), no periodic wrap, full free
+// surface, no biharmonic term.
+#pragma once
+
+#include "common.cuh"
+#include "inmsom_gpu.h"
+
+namespace inmsom {
+namespace fused {
+
+// per-row coefficients, row index = device row (n - bnd_y1)
+struct RowCoef {
+    double ku, ku2;           // hu: area(n)/(dxt*dyh)(n), and half of it
+    double wv0, wv1;          // hv: area(n)/(dxh*dyt)(n), area(n+1)/(dxh*dyt)(n)
+    double wh0, wh1;          // hh: area(n)/(dxb*dyb)(n), area(n+1)/(dxb*dyb)(n)
+    double c_u, c_v0, c_v1;   // continuity: dyh(n)/area(n), dxh(n)/area(n), dxh(n-1)/area(n)
+    double fx, fy;            // advection: dyh(n)/4, dxh(n)/4
+    double gx0, gx1;          // GX_h: dyh(n)/4, dyh(n+1)/4
+    double gy0, gy1;          // GY_T: dxh(n-1)/4, dxh(n)/4
+    double cor;               // rlh_s(n)*dxb(n)*dyb(n)
+    double vt0, vt1, vt2;     // vorticity metric terms: dyt-dyb, dxt(n+1)-dxb, dxt-dxb
+    double t1, t2, t3;        // tension: dy/(dx*dyh), dx/(dy*dxh(n)), dx/(dy*dxh(n-1))
+    double s1, s2, s3;        // shear: dxb/(dyb*dxt(n+1)), dxb/(dyb*dxt(n)), dyb/(dxb*dyt)
+    double dux, dus0, dus1;   // u viscosity: dy^2/dyh, dxb^2/dxt, dxb(n-1)^2/dxt
+    double dvt0, dvt1, dvs;   // v viscosity: dx^2/dxh, dx(n+1)^2/dxh, dyb^2/dyt
+    double gdyh, gdxh;        // g*dyh, g*dxh
+    double au, av;            // dxt*dyh, dyt*dxh
+    double rau, rav;          // 1/(dxt*dyh), 1/(dyt*dxh)
+};
+
+struct Plan {
+    int W = 128;              // threads (columns) per CTA
+    int outw = 126;           // output columns per CTA
+    int nstrips = 0, nchunks = 0, chunk_rows = 0;
+    long long min_pitch = 0;  // device row pitch the strips need
+    // device data
+    RowCoef *rows = nullptr;
+    uint32_t *bits = nullptr;       // 1-bit T mask, bm_words per row
+    int bm_words = 0;
+    double *buf[2][6] = {};         // extra state sets (ping-pong)
+    double *d_uniform = nullptr;    // min/max of mu, rdis, wflux (6 doubles)
+    unsigned *d_flags = nullptr;    // [0] status bits (guard / timeout)
+    const double *hrest = nullptr;  // borrowed
+    const float *lu = nullptr;      // borrowed
+    int nsm = 148;
+    bool vort_zero = false;
+    bool buffers_synced = false;    // buf[][] hold the state's land/halo values
+    unsigned last_flags = 0;        // status bits of the last run
+};
+
+enum : unsigned { FLAG_TIMEOUT = 1u, FLAG_GUARD = 2u };
+
+// The fused path writes only ocean points; land and halo points of the
+// ping-pong sets must equal those of the state.  Call after the state was
+// replaced from the host.
+inline void mark_state_changed(Plan &p) { p.buffers_synced = false; }
+
+Plan make_plan(const inmsom_bounds &b);
+// nullptr if the fused path can run this grid, else the reason
+const char *check_eligible(const Plan &p, const Dom &d, const Consts &c,
+                           const float *const masks[7], const double *const grid[10]);
+// build the row table and the bit mask, allocate the ping-pong buffers
+int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7],
+          const double *const grid[10], const double *d_hrest, const float *d_lu,
+          cudaStream_t s);
+// barotropic_dynamics(tau, nstep) on state[6] (in/out) with acc[4] out
+int dynamics(Plan &p, const Dom &d, const Consts &c, double tau, int nstep,
+             double *state[6], double *acc[4], double *forc[6], cudaStream_t s);
+// nsub advancing substeps (the first substep of barotropic_dynamics(dt,1))
+int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt,
+                 const double *rhs_scale, double *state[6], double *forc[6],
+                 cudaStream_t s);
+void free_plan(Plan &p);
+
+}  // namespace fused
+}  // namespace inmsom

@@ -1,0 +1,173 @@
+"""Host-side mirror of the reference's barotropic interface over the C ABI.
+
+``BarotropicSolver`` owns one library context for one basin.  Its methods
+take the reference's arguments in the reference's order
+(Function/vel_ssh.f90:379-406 and :682-687) as Fortran-layout numpy arrays,
+or default to the arrays held by the Basin.
+"""
+from __future__ import annotations
+
+import ctypes
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import InmsomError, cbounds, cconsts, check, dptr, fptr, load
+from .grid import DEPTHS, MASKS, MEANS, METRICS, SCRATCH, STATE, Basin, Bounds
+
+# argument order of barotropic_dynamics after (tau, nstep, ksw4)
+DYN_ARGS = ("ubrtr_e", "ubrtrp_e", "vbrtr_e", "vbrtrp_e", "ssh_e", "sshp_e",
+            "ubrtr_i", "vbrtr_i", "ssh4gradx", "ssh4grady", "RHSx", "RHSy", "wflux",
+            "mu", "mu4", "vort", "str_t2d", "str_s2d", "fx", "fy", "rdis",
+            "RHSx_adv", "RHSy_adv", "RHSx_dif", "RHSy_dif")
+
+
+def gridcon(bounds: Bounds, lu: np.ndarray, device: int = 0) -> dict:
+    """Derived masks of Service/grid_construction.f90:59-112, on the GPU."""
+    lib = load()
+    out = {k: bounds.zeros(np.float32) for k in ("luu", "luh", "llu", "llv", "lcu", "lcv")}
+    cb = cbounds(bounds)
+    check(lib.inmsom_gridcon(ctypes.byref(cb), fptr(lu), fptr(out["luu"]), fptr(out["luh"]),
+                             fptr(out["llu"]), fptr(out["llv"]), fptr(out["lcu"]),
+                             fptr(out["lcv"]), device))
+    return out
+
+
+class BarotropicSolver:
+    def __init__(self, basin: Basin, device: int = 0, resident: bool = True,
+                 force_general: bool = False, guard: bool = False,
+                 register_depths: bool = True):
+        lib = load()
+        self.basin = basin
+        self.device = device
+        flags = (_lib.RESIDENT if resident else 0) | (_lib.FORCE_GENERAL if force_general else 0) \
+            | (_lib.GUARD if guard else 0)
+        self._ctx = ctypes.c_void_p()
+        cb, cc = cbounds(basin.bounds), cconsts(basin.consts)
+        check(lib.inmsom_gpu_init(ctypes.byref(self._ctx), ctypes.byref(cb), ctypes.byref(cc),
+                                  device, flags))
+        m, g = basin.masks, basin.metrics
+        depths = [dptr(basin.depths[k]) if register_depths else None for k in DEPTHS]
+        check(lib.inmsom_gpu_register_grid(self._ctx, *[fptr(m[k]) for k in MASKS],
+                                           *[dptr(g[k]) for k in METRICS], dptr(basin.rlh_s),
+                                           dptr(basin.hhq_rest), *depths))
+
+    # ------------------------------------------------------------------
+    def close(self) -> None:
+        if self._ctx:
+            _lib.load().inmsom_gpu_finalize(self._ctx)
+            self._ctx = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    # ------------------------------------------------------------------
+    def _arrays(self, override: dict) -> list:
+        b = self.basin
+        pools = (b.state, b.means, b.forcing, b.scratch)
+        out = []
+        for k in DYN_ARGS:
+            if k in override:
+                out.append(override[k])
+                continue
+            for p in pools:
+                if k in p:
+                    out.append(p[k])
+                    break
+            else:
+                raise KeyError(k)
+        return out
+
+    def barotropic_dynamics(self, tau: float, nstep: int, ksw4: int = 0, **arrays) -> None:
+        """barotropic_dynamics(tau, nstep, ksw4, ubrtr_e, ..., RHSy_dif);
+        arrays not given are taken from the Basin."""
+        check(load().inmsom_barotropic_dynamics(self._ctx, float(tau), int(nstep), int(ksw4),
+                                                *[dptr(a) for a in self._arrays(arrays)]))
+
+    def ssh_internal(self, tau: float, ssh_i, sshp_i, u, v, wflux, hhqn, hhun, hhvn, hhhn) -> None:
+        check(load().inmsom_ssh_internal(self._ctx, float(tau), dptr(ssh_i), dptr(sshp_i),
+                                         dptr(u), dptr(v), dptr(wflux), dptr(hhqn), dptr(hhun),
+                                         dptr(hhvn), dptr(hhhn)))
+
+    def load_state(self) -> None:
+        """Upload the Basin's *_e state and forcing (inmsom_load_state)."""
+        st, f = self.basin.state, self.basin.forcing
+        check(load().inmsom_load_state(self._ctx, *[dptr(st[k]) for k in STATE],
+                                       *[dptr(f[k]) for k in ("RHSx", "RHSy", "wflux", "mu", "mu4",
+                                                              "rdis")]))
+
+    def run_substeps(self, nsub: int, dt: float, rhs_scale: Optional[Sequence[float]] = None) -> float:
+        """Advance the resident state nsub leap-frog substeps; returns the
+        device time in ms."""
+        ms = ctypes.c_float(0.0)
+        sc = None
+        if rhs_scale is not None:
+            sc = np.ascontiguousarray(rhs_scale, dtype=np.float64)
+            if sc.shape != (nsub,):
+                raise ValueError("rhs_scale needs one value per substep")
+        check(load().inmsom_run_substeps(self._ctx, int(nsub), float(dt),
+                                         None if sc is None else sc.ctypes.data_as(_lib.DP),
+                                         ctypes.byref(ms)))
+        return float(ms.value)
+
+    def wind_forcing(self, taux, tauy, rhsx=None, rhsy=None):
+        b = self.basin.bounds
+        rhsx = b.zeros() if rhsx is None else rhsx
+        rhsy = b.zeros() if rhsy is None else rhsy
+        check(load().inmsom_wind_forcing(self._ctx, dptr(taux), dptr(tauy), dptr(rhsx), dptr(rhsy)))
+        return rhsx, rhsy
+
+    def r_diss(self, r_fric: float, out=None):
+        out = self.basin.bounds.zeros() if out is None else out
+        check(load().inmsom_r_diss(self._ctx, float(r_fric), dptr(out)))
+        return out
+
+    def hh_init_external(self, ssh_e=None, sshp_e=None) -> None:
+        s = self.basin.state
+        check(load().inmsom_hh_init_external(self._ctx, dptr(s["ssh_e"] if ssh_e is None else ssh_e),
+                                             dptr(s["sshp_e"] if sshp_e is None else sshp_e)))
+
+    def guard(self) -> int:
+        n = ctypes.c_long(0)
+        check(load().inmsom_guard(self._ctx, ctypes.byref(n)))
+        return int(n.value)
+
+    def diag(self):
+        v, e = ctypes.c_double(), ctypes.c_double()
+        check(load().inmsom_gpu_diag(self._ctx, ctypes.byref(v), ctypes.byref(e)))
+        return float(v.value), float(e.value)
+
+    def sync_to_host(self, what: int = _lib.SYNC_STATE) -> None:
+        check(load().inmsom_gpu_sync_to_host(self._ctx, what))
+
+    def sync_from_host(self, what: int = _lib.SYNC_STATE) -> None:
+        check(load().inmsom_gpu_sync_from_host(self._ctx, what))
+
+    def path(self):
+        p, r = ctypes.c_int(), ctypes.c_char_p()
+        check(load().inmsom_gpu_path(self._ctx, ctypes.byref(p), ctypes.byref(r)))
+        return int(p.value), (r.value or b"").decode()
+
+
+class GpuBackend:
+    """Basin set-up on the GPU: gridcon and the wind forcing."""
+
+    def __init__(self, device: int = 0):
+        self.device = device
+
+    def gridcon(self, bounds, lu):
+        return gridcon(bounds, lu, self.device)
+
+    def wind_forcing(self, basin: Basin):
+        with BarotropicSolver(basin, self.device, register_depths=False) as s:
+            return s.wind_forcing(basin.taux, basin.tauy)

@@ -1,0 +1,701 @@
+/*
+ * CPU oracle for the INMSOM barotropic step -- TEST INFRASTRUCTURE ONLY.
+ * See oracle.h for what this file is, how it is built and why parity with
+ * the Fortran build is unpinned.  Every function cites the reference lines
+ * it restates; comments mark the places where the Fortran expression order
+ * decides the rounding.
+ */
+#include "oracle.h"
+
+#include <math.h>
+#include <stdlib.h>
+#include <string.h>
+
+#define LD(b) ((b)->bnd_x2 - (b)->bnd_x1 + 1)
+#define NTOT(b) ((size_t)LD(b) * (size_t)((b)->bnd_y2 - (b)->bnd_y1 + 1))
+/* Fortran element (m,n) of an array with the bounds in *B. */
+#define I(m, n) ((size_t)((n) - B->bnd_y1) * (size_t)LDX + (size_t)((m) - B->bnd_x1))
+
+#define SETUP(bptr)                  \
+    const ora_bounds *B = (bptr);    \
+    const int LDX = LD(B);           \
+    (void)LDX
+
+/* ------------------------------------------------------------------ */
+/* Service/grid_construction.f90:59-112 */
+void ora_gridcon(const ora_bounds *b, const float *lu, float *luu, float *luh,
+                 float *llu, float *llv, float *lcu, float *lcv)
+{
+    SETUP(b);
+    /* :59-65 luh: any of the 4 surrounding T points is ocean */
+    for (int n = B->ny_start - 1; n <= B->ny_end; n++)
+        for (int m = B->nx_start - 1; m <= B->nx_end; m++)
+            if (lu[I(m, n)] + lu[I(m + 1, n)] + lu[I(m, n + 1)] + lu[I(m + 1, n + 1)] > 0.5f)
+                luh[I(m, n)] = 1.0f;
+    /* :67-73 luu: all 4 are ocean */
+    for (int n = B->ny_start - 1; n <= B->ny_end; n++)
+        for (int m = B->nx_start - 1; m <= B->nx_end; m++)
+            if (lu[I(m, n)] * lu[I(m + 1, n)] * lu[I(m, n + 1)] * lu[I(m + 1, n + 1)] > 0.5f)
+                luu[I(m, n)] = 1.0f;
+    /* :92-112 llu/llv (either side ocean), lcu/lcv (both sides ocean) */
+    for (int n = B->ny_start - 1; n <= B->ny_end; n++)
+        for (int m = B->nx_start - 1; m <= B->nx_end; m++) {
+            if (lu[I(m, n)] + lu[I(m + 1, n)] > 0.5f) llu[I(m, n)] = 1.0f;
+            if (lu[I(m, n)] + lu[I(m, n + 1)] > 0.5f) llv[I(m, n)] = 1.0f;
+            if (lu[I(m, n)] * lu[I(m + 1, n)] > 0.5f) lcu[I(m, n)] = 1.0f;
+            if (lu[I(m, n)] * lu[I(m, n + 1)] > 0.5f) lcv[I(m, n)] = 1.0f;
+        }
+}
+
+/* ------------------------------------------------------------------ */
+/* Service/oc_algorithms.f90:50-95.  With two or more process columns the
+ * first column receives ff(mm) into ff(mmm-1) and the last receives ff(mmm)
+ * into ff(mm+1): a periodic wrap of one column over the full y extent.
+ * (On a single process column the routine sends to itself and copies
+ * ff(mmm) into ff(mmm-1) instead; the oracle follows the wrap.) */
+void ora_cyclize8_x(const ora_bounds *b, double *f)
+{
+    SETUP(b);
+    for (int n = B->bnd_y1; n <= B->bnd_y2; n++) {
+        double left = f[I(B->mm, n)], right = f[I(B->mmm, n)];
+        f[I(B->mmm - 1, n)] = left;
+        f[I(B->mm + 1, n)] = right;
+    }
+}
+
+/* Service/oc_algorithms.f90:118-135 */
+void ora_cyclize8_y(const ora_bounds *b, double *f)
+{
+    SETUP(b);
+    for (int m = B->bnd_x1; m <= B->bnd_x2; m++) {
+        f[I(m, B->nnn - 1)] = f[I(m, B->nn)];
+        f[I(m, B->nn + 1)] = f[I(m, B->nnn)];
+    }
+}
+
+/* the "syncborder + cyclize" pair that follows every field update; on one
+ * domain syncborder_real8 exchanges nothing (Modules/
+ * mod_mpi_parallel_tools.f90:138-173 with no neighbours). */
+static void halo(const ora_bounds *b, double *f)
+{
+    if (b->periodicity_x) ora_cyclize8_x(b, f);
+    if (b->periodicity_y) ora_cyclize8_y(b, f);
+}
+
+/* ------------------------------------------------------------------ */
+/* interpolations of depth from T points, Function/depth.f90:29-66 */
+static inline double h_on_u(const ora_grid *g, const double *hq, int m, int n)
+{
+    SETUP(&g->b);
+    const float *lu = g->lu;
+    double slu = (double)(lu[I(m, n)] + lu[I(m + 1, n)]);
+    return (hq[I(m, n)] * g->dx[I(m, n)] * g->dy[I(m, n)] * (double)lu[I(m, n)]
+            + hq[I(m + 1, n)] * g->dx[I(m + 1, n)] * g->dy[I(m + 1, n)] * (double)lu[I(m + 1, n)])
+           / slu / g->dxt[I(m, n)] / g->dyh[I(m, n)];
+}
+
+static inline double h_on_v(const ora_grid *g, const double *hq, int m, int n)
+{
+    SETUP(&g->b);
+    const float *lu = g->lu;
+    double slu = (double)(lu[I(m, n)] + lu[I(m, n + 1)]);
+    return (hq[I(m, n)] * g->dx[I(m, n)] * g->dy[I(m, n)] * (double)lu[I(m, n)]
+            + hq[I(m, n + 1)] * g->dx[I(m, n + 1)] * g->dy[I(m, n + 1)] * (double)lu[I(m, n + 1)])
+           / slu / g->dxh[I(m, n)] / g->dyt[I(m, n)];
+}
+
+static inline double h_on_h(const ora_grid *g, const double *hq, int m, int n)
+{
+    SETUP(&g->b);
+    const float *lu = g->lu;
+    /* real(4) sum of the four masks, then dble */
+    double slu = (double)(lu[I(m, n)] + lu[I(m + 1, n)] + lu[I(m, n + 1)] + lu[I(m + 1, n + 1)]);
+    return (hq[I(m, n)] * g->dx[I(m, n)] * g->dy[I(m, n)] * (double)lu[I(m, n)]
+            + hq[I(m + 1, n)] * g->dx[I(m + 1, n)] * g->dy[I(m + 1, n)] * (double)lu[I(m + 1, n)]
+            + hq[I(m, n + 1)] * g->dx[I(m, n + 1)] * g->dy[I(m, n + 1)] * (double)lu[I(m, n + 1)]
+            + hq[I(m + 1, n + 1)] * g->dx[I(m + 1, n + 1)] * g->dy[I(m + 1, n + 1)] * (double)lu[I(m + 1, n + 1)])
+           / slu / g->dxb[I(m, n)] / g->dyb[I(m, n)];
+}
+
+/* Function/depth.f90:2-105 */
+void ora_hh_init(const ora_grid *g,
+                 double *hq, double *hqp, double *hqn,
+                 double *hu, double *hup, double *hun,
+                 double *hv, double *hvp, double *hvn,
+                 double *hh, double *hhp, double *hhn,
+                 const double *sh, const double *shp, const double *h_r)
+{
+    SETUP(&g->b);
+    const size_t nt = NTOT(B);
+    const double ffs = (double)g->full_free_surface;
+    /* :21-23 whole-array assignments */
+    for (size_t i = 0; i < nt; i++) {
+        hq[i] = h_r[i] + sh[i] * ffs;
+        hqp[i] = h_r[i] + shp[i] * ffs;
+        hqn[i] = h_r[i];
+    }
+    /* :25-70 */
+#pragma omp parallel for
+    for (int n = B->ny_start - 1; n <= B->ny_end; n++)
+        for (int m = B->nx_start - 1; m <= B->nx_end; m++) {
+            if (g->llu[I(m, n)] > 0.5f) {
+                hu[I(m, n)] = h_on_u(g, hq, m, n);
+                hup[I(m, n)] = h_on_u(g, hqp, m, n);
+                hun[I(m, n)] = h_on_u(g, hqn, m, n);
+            }
+            if (g->llv[I(m, n)] > 0.5f) {
+                hv[I(m, n)] = h_on_v(g, hq, m, n);
+                hvp[I(m, n)] = h_on_v(g, hqp, m, n);
+                hvn[I(m, n)] = h_on_v(g, hqn, m, n);
+            }
+            if (g->luh[I(m, n)] > 0.5f) {
+                hh[I(m, n)] = h_on_h(g, hq, m, n);
+                hhp[I(m, n)] = h_on_h(g, hqp, m, n);
+                hhn[I(m, n)] = h_on_h(g, hqn, m, n);
+            }
+        }
+    /* :72-104 */
+    double *fs[9] = {hu, hup, hun, hv, hvp, hvn, hh, hhp, hhn};
+    for (int k = 0; k < 9; k++) halo(B, fs[k]);
+}
+
+/* Function/depth.f90:108-170 */
+void ora_hh_update(const ora_grid *g, double *hqn, double *hun, double *hvn,
+                   double *hhn, const double *sh, const double *h_r)
+{
+    SETUP(&g->b);
+    const size_t nt = NTOT(B);
+    for (size_t i = 0; i < nt; i++) hqn[i] = h_r[i] + sh[i]; /* :121 */
+#pragma omp parallel for
+    for (int n = B->ny_start - 1; n <= B->ny_end; n++)
+        for (int m = B->nx_start - 1; m <= B->nx_end; m++) {
+            if (g->llu[I(m, n)] > 0.5f) hun[I(m, n)] = h_on_u(g, hqn, m, n);
+            if (g->llv[I(m, n)] > 0.5f) hvn[I(m, n)] = h_on_v(g, hqn, m, n);
+            if (g->luh[I(m, n)] > 0.5f) hhn[I(m, n)] = h_on_h(g, hqn, m, n);
+        }
+    halo(B, hun);
+    halo(B, hvn);
+    halo(B, hhn);
+}
+
+/* Robert-Asselin step shared by Function/depth.f90:196-211 and
+ * Function/vel_ssh.f90:594-606: f + ts*(fn - 2f + fp)/2/nstep, evaluated as
+ * f + (((ts*((fn - 2f) + fp))/2)/nstep). */
+static inline double asselin(double ts, double f, double fn, double fp, double nstep)
+{
+    return f + ts * (fn - 2.0 * f + fp) / 2.0 / nstep;
+}
+
+/* Function/depth.f90:174-220 */
+void ora_hh_shift(const ora_grid *g,
+                  double *hq, double *hqp, double *hqn,
+                  double *hu, double *hup, double *hun,
+                  double *hv, double *hvp, double *hvn,
+                  double *hh, double *hhp, double *hhn, int nstep)
+{
+    SETUP(&g->b);
+    const double ts = g->time_smooth, ns = (double)nstep;
+#pragma omp parallel for
+    for (int n = B->ny_start - 1; n <= B->ny_end + 1; n++)
+        for (int m = B->nx_start - 1; m <= B->nx_end + 1; m++) {
+            size_t i = I(m, n);
+            if (g->llu[i] > 0.5f) { hup[i] = asselin(ts, hu[i], hun[i], hup[i], ns); hu[i] = hun[i]; }
+            if (g->llv[i] > 0.5f) { hvp[i] = asselin(ts, hv[i], hvn[i], hvp[i], ns); hv[i] = hvn[i]; }
+            if (g->lu[i] > 0.5f)  { hqp[i] = asselin(ts, hq[i], hqn[i], hqp[i], ns); hq[i] = hqn[i]; }
+            if (g->luh[i] > 0.5f) { hhp[i] = asselin(ts, hh[i], hhn[i], hhp[i], ns); hh[i] = hhn[i]; }
+        }
+}
+
+/* ------------------------------------------------------------------ */
+/* Function/mixing.f90:115-168 */
+void ora_stress_components(const ora_grid *g, const double *u, const double *v,
+                           double *str_t, double *str_s)
+{
+    SETUP(&g->b);
+    const double *dx = g->dx, *dy = g->dy, *dxh = g->dxh, *dyh = g->dyh;
+    const double *dxt = g->dxt, *dyt = g->dyt, *dxb = g->dxb, *dyb = g->dyb;
+#pragma omp parallel for
+    for (int n = B->ny_start; n <= B->ny_end; n++)
+        for (int m = B->nx_start; m <= B->nx_end; m++)
+            if (g->lu[I(m, n)] > 0.5f)
+                /* :134-135 */
+                str_t[I(m, n)] = dy[I(m, n)] / dx[I(m, n)] * (u[I(m, n)] / dyh[I(m, n)] - u[I(m - 1, n)] / dyh[I(m - 1, n)])
+                               - dx[I(m, n)] / dy[I(m, n)] * (v[I(m, n)] / dxh[I(m, n)] - v[I(m, n - 1)] / dxh[I(m, n - 1)]);
+#pragma omp parallel for
+    for (int n = B->ny_start; n <= B->ny_end; n++)
+        for (int m = B->nx_start; m <= B->nx_end; m++)
+            if (g->luu[I(m, n)] > 0.5f)
+                /* :147-148 */
+                str_s[I(m, n)] = dxb[I(m, n)] / dyb[I(m, n)] * (u[I(m, n + 1)] / dxt[I(m, n + 1)] - u[I(m, n)] / dxt[I(m, n)])
+                               + dyb[I(m, n)] / dxb[I(m, n)] * (v[I(m + 1, n)] / dyt[I(m + 1, n)] - v[I(m, n)] / dyt[I(m, n)]);
+    halo(B, str_t);
+    halo(B, str_s);
+}
+
+/* Function/mixing.f90:171-219 (one level) */
+void ora_smagorinsky_coeff(const ora_grid *g, double visc2, double dift,
+                           const double *str_t, const double *str_s,
+                           double *amts, double *amuv, double vonkarman,
+                           double pi)
+{
+    SETUP(&g->b);
+    const double prandtl = 0.1; /* :177 */
+#pragma omp parallel for
+    for (int n = B->ny_start; n <= B->ny_end; n++)
+        for (int m = B->nx_start; m <= B->nx_end; m++)
+            if (g->lu[I(m, n)] > 0.5f) {
+                double s0 = str_s[I(m, n)], s1 = str_s[I(m - 1, n)];
+                double s2 = str_s[I(m, n - 1)], s3 = str_s[I(m - 1, n - 1)];
+                double str_s2 = (s0 * s0 + s1 * s1 + s2 * s2 + s3 * s3) / 4.0;
+                double k = vonkarman / pi;
+                double st = str_t[I(m, n)];
+                double mu_smag = k * k * g->dx[I(m, n)] * g->dy[I(m, n)] * sqrt(st * st + str_s2);
+                amuv[I(m, n)] = visc2 + mu_smag;
+                amts[I(m, n)] = dift + mu_smag * prandtl;
+            }
+    halo(B, amuv);
+    halo(B, amts);
+}
+
+/* ------------------------------------------------------------------ */
+/* Function/vel_ssh.f90:2-114 */
+void ora_uv_trans(const ora_grid *g, const double *u, const double *v,
+                  double *vort, const double *hq, const double *hu,
+                  const double *hv, const double *hh, double *rhsx,
+                  double *rhsy)
+{
+    SETUP(&g->b);
+    (void)hq;
+    const double *dxt = g->dxt, *dyt = g->dyt, *dxb = g->dxb, *dyb = g->dyb;
+    const double *dxh = g->dxh, *dyh = g->dyh;
+    /* :30-42 */
+#pragma omp parallel for
+    for (int n = B->ny_start; n <= B->ny_end; n++)
+        for (int m = B->nx_start; m <= B->nx_end; m++)
+            if (g->luu[I(m, n)] > 0.5f)
+                vort[I(m, n)] = (v[I(m + 1, n)] * dyt[I(m + 1, n)] - v[I(m, n)] * dyt[I(m, n)])
+                              - (u[I(m, n + 1)] * dxt[I(m, n + 1)] - u[I(m, n)] * dxt[I(m, n)])
+                              - ((v[I(m + 1, n)] - v[I(m, n)]) * dyb[I(m, n)] - (u[I(m, n + 1)] - u[I(m, n)]) * dxb[I(m, n)]);
+    halo(B, vort); /* :44-52 */
+    /* :54-109 */
+#pragma omp parallel for
+    for (int n = B->ny_start; n <= B->ny_end; n++)
+        for (int m = B->nx_start; m <= B->nx_end; m++) {
+            if (g->lcu[I(m, n)] > 0.5f) {
+                /* :63-77; "(a)/2.0d0*(b)/2.0d0" rounds as ((a/2)*b)/2 */
+                double fx_p = (u[I(m, n)] * dyh[I(m, n)] * hu[I(m, n)] + u[I(m + 1, n)] * dyh[I(m + 1, n)] * hu[I(m + 1, n)]) / 2.0
+                              * (u[I(m, n)] + u[I(m + 1, n)]) / 2.0;
+                double fx_m = (u[I(m, n)] * dyh[I(m, n)] * hu[I(m, n)] + u[I(m - 1, n)] * dyh[I(m - 1, n)] * hu[I(m - 1, n)]) / 2.0
+                              * (u[I(m, n)] + u[I(m - 1, n)]) / 2.0;
+                double fy_p = (v[I(m, n)] * dxh[I(m, n)] * hv[I(m, n)] + v[I(m + 1, n)] * dxh[I(m + 1, n)] * hv[I(m + 1, n)]) / 2.0
+                              * (u[I(m, n + 1)] + u[I(m, n)]) / 2.0 * (double)g->luu[I(m, n)];
+                double fy_m = (v[I(m, n - 1)] * dxh[I(m, n - 1)] * hv[I(m, n - 1)] + v[I(m + 1, n - 1)] * dxh[I(m + 1, n - 1)] * hv[I(m + 1, n - 1)]) / 2.0
+                              * (u[I(m, n - 1)] + u[I(m, n)]) / 2.0 * (double)g->luu[I(m, n - 1)];
+                rhsx[I(m, n)] = -(fx_p - fx_m + fy_p - fy_m)
+                                + (vort[I(m, n)] * hh[I(m, n)] * (v[I(m + 1, n)] + v[I(m, n)])
+                                   + vort[I(m, n - 1)] * hh[I(m, n - 1)] * (v[I(m + 1, n - 1)] + v[I(m, n - 1)])) / 4.0;
+            }
+            if (g->lcv[I(m, n)] > 0.5f) {
+                /* :88-102 */
+                double fy_p = (v[I(m, n)] * dxh[I(m, n)] * hv[I(m, n)] + v[I(m, n + 1)] * dxh[I(m, n + 1)] * hv[I(m, n + 1)]) / 2.0
+                              * (v[I(m, n)] + v[I(m, n + 1)]) / 2.0;
+                double fy_m = (v[I(m, n)] * dxh[I(m, n)] * hv[I(m, n)] + v[I(m, n - 1)] * dxh[I(m, n - 1)] * hv[I(m, n - 1)]) / 2.0
+                              * (v[I(m, n)] + v[I(m, n - 1)]) / 2.0;
+                double fx_p = (u[I(m, n)] * dyh[I(m, n)] * hu[I(m, n)] + u[I(m, n + 1)] * dyh[I(m, n + 1)] * hu[I(m, n + 1)]) / 2.0
+                              * (v[I(m + 1, n)] + v[I(m, n)]) / 2.0;
+                double fx_m = (u[I(m - 1, n)] * dyh[I(m - 1, n)] * hu[I(m - 1, n)] + u[I(m - 1, n + 1)] * dyh[I(m - 1, n + 1)] * hu[I(m - 1, n + 1)]) / 2.0
+                              * (v[I(m - 1, n)] + v[I(m, n)]) / 2.0;
+                rhsy[I(m, n)] = -(fx_p - fx_m + fy_p - fy_m)
+                                - (vort[I(m, n)] * hh[I(m, n)] * (u[I(m, n + 1)] + u[I(m, n)])
+                                   + vort[I(m - 1, n)] * hh[I(m - 1, n)] * (u[I(m - 1, n + 1)] + u[I(m - 1, n)])) / 4.0;
+            }
+        }
+}
+
+/* the stress-divergence expressions of Function/vel_ssh.f90:153-156 and
+ * :169-172 (also :228-231, :245-248, :286-289, :302-305) */
+static inline double diff_x(const ora_grid *g, const double *mu, const double *str_t,
+                            const double *str_s, const double *hq, const double *hh,
+                            int m, int n)
+{
+    SETUP(&g->b);
+    const double *dy = g->dy, *dyh = g->dyh, *dxb = g->dxb, *dxt = g->dxt;
+    double muh_p = (mu[I(m, n)] + mu[I(m + 1, n)] + mu[I(m, n + 1)] + mu[I(m + 1, n + 1)]) / 4.0;
+    double muh_m = (mu[I(m, n)] + mu[I(m + 1, n)] + mu[I(m, n - 1)] + mu[I(m + 1, n - 1)]) / 4.0;
+    double dy1 = dy[I(m + 1, n)], dy0 = dy[I(m, n)], db0 = dxb[I(m, n)], db1 = dxb[I(m, n - 1)];
+    return (dy1 * dy1 * mu[I(m + 1, n)] * hq[I(m + 1, n)] * str_t[I(m + 1, n)]
+            - dy0 * dy0 * mu[I(m, n)] * hq[I(m, n)] * str_t[I(m, n)]) / dyh[I(m, n)]
+           + (db0 * db0 * muh_p * hh[I(m, n)] * str_s[I(m, n)]
+              - db1 * db1 * muh_m * hh[I(m, n - 1)] * str_s[I(m, n - 1)]) / dxt[I(m, n)];
+}
+
+static inline double diff_y_t(const ora_grid *g, const double *mu, const double *str_t,
+                              const double *hq, int m, int n)
+{
+    SETUP(&g->b);
+    const double *dx = g->dx;
+    double dx1 = dx[I(m, n + 1)], dx0 = dx[I(m, n)];
+    return (dx1 * dx1 * mu[I(m, n + 1)] * hq[I(m, n + 1)] * str_t[I(m, n + 1)]
+            - dx0 * dx0 * mu[I(m, n)] * hq[I(m, n)] * str_t[I(m, n)]) / g->dxh[I(m, n)];
+}
+
+static inline double diff_y_s(const ora_grid *g, const double *mu, const double *str_s,
+                              const double *hh, int m, int n)
+{
+    SETUP(&g->b);
+    const double *dyb = g->dyb;
+    double muh_p = (mu[I(m, n)] + mu[I(m + 1, n)] + mu[I(m, n + 1)] + mu[I(m + 1, n + 1)]) / 4.0;
+    double muh_m = (mu[I(m, n)] + mu[I(m - 1, n)] + mu[I(m, n + 1)] + mu[I(m - 1, n + 1)]) / 4.0;
+    double db0 = dyb[I(m, n)], db1 = dyb[I(m - 1, n)];
+    return (db0 * db0 * muh_p * hh[I(m, n)] * str_s[I(m, n)]
+            - db1 * db1 * muh_m * hh[I(m - 1, n)] * str_s[I(m - 1, n)]) / g->dyt[I(m, n)];
+}
+
+/* Function/vel_ssh.f90:117-184 */
+void ora_uv_diff2(const ora_grid *g, const double *mu, const double *str_t,
+                  const double *str_s, const double *hq, const double *hu,
+                  const double *hv, const double *hh, double *rhsx,
+                  double *rhsy)
+{
+    SETUP(&g->b);
+    (void)hu;
+    (void)hv;
+#pragma omp parallel for
+    for (int n = B->ny_start; n <= B->ny_end; n++)
+        for (int m = B->nx_start; m <= B->nx_end; m++) {
+            if (g->lcu[I(m, n)] > 0.5f)
+                rhsx[I(m, n)] = diff_x(g, mu, str_t, str_s, hq, hh, m, n);
+            if (g->lcv[I(m, n)] > 0.5f)
+                /* :169-172: -(A-B)/dxh + (C-D)/dyt */
+                rhsy[I(m, n)] = -diff_y_t(g, mu, str_t, hq, m, n) + diff_y_s(g, mu, str_s, hh, m, n);
+        }
+}
+
+/* Function/vel_ssh.f90:187-317 */
+void ora_uv_diff4(const ora_grid *g, const double *mu, double *str_t,
+                  double *str_s, double *fx, double *fy, const double *hq,
+                  const double *hu, const double *hv, const double *hh,
+                  double *rhsx, double *rhsy)
+{
+    SETUP(&g->b);
+    const size_t nt = NTOT(B);
+    memset(fx, 0, nt * sizeof(double)); /* :213-214 */
+    memset(fy, 0, nt * sizeof(double));
+#pragma omp parallel for
+    for (int n = B->ny_start; n <= B->ny_end; n++)
+        for (int m = B->nx_start; m <= B->nx_end; m++) {
+            size_t i = I(m, n);
+            if (g->lcu[i] > 0.5f) {
+                fx[i] = diff_x(g, mu, str_t, str_s, hq, hh, m, n);
+                fx[i] = -fx[i] / hu[i] / g->dxt[i] / g->dyh[i]; /* :232 */
+            }
+            if (g->lcv[i] > 0.5f) {
+                fy[i] = -diff_y_t(g, mu, str_t, hq, m, n) + diff_y_s(g, mu, str_s, hh, m, n);
+                fy[i] = -fy[i] / hv[i] / g->dxh[i] / g->dyt[i]; /* :249 */
+            }
+        }
+    halo(B, fx); /* :259-270 */
+    halo(B, fy);
+    ora_stress_components(g, fx, fy, str_t, str_s); /* :272 */
+#pragma omp parallel for
+    for (int n = B->ny_start; n <= B->ny_end; n++)
+        for (int m = B->nx_start; m <= B->nx_end; m++) {
+            size_t i = I(m, n);
+            if (g->lcu[i] > 0.5f) {
+                /* :286-289: RHSx + (A-B)/dyh + (C-D)/dxt, left to right */
+                const double *dy = g->dy, *dyh = g->dyh, *dxb = g->dxb, *dxt = g->dxt;
+                double muh_p = (mu[I(m, n)] + mu[I(m + 1, n)] + mu[I(m, n + 1)] + mu[I(m + 1, n + 1)]) / 4.0;
+                double muh_m = (mu[I(m, n)] + mu[I(m + 1, n)] + mu[I(m, n - 1)] + mu[I(m + 1, n - 1)]) / 4.0;
+                double dy1 = dy[I(m + 1, n)], dy0 = dy[I(m, n)], db0 = dxb[I(m, n)], db1 = dxb[I(m, n - 1)];
+                rhsx[i] = rhsx[i]
+                          + (dy1 * dy1 * mu[I(m + 1, n)] * hq[I(m + 1, n)] * str_t[I(m + 1, n)]
+                             - dy0 * dy0 * mu[I(m, n)] * hq[I(m, n)] * str_t[I(m, n)]) / dyh[I(m, n)]
+                          + (db0 * db0 * muh_p * hh[I(m, n)] * str_s[I(m, n)]
+                             - db1 * db1 * muh_m * hh[I(m, n - 1)] * str_s[I(m, n - 1)]) / dxt[I(m, n)];
+            }
+            if (g->lcv[i] > 0.5f)
+                /* :302-305: RHSy - (A-B)/dxh + (C-D)/dyt */
+                rhsy[i] = rhsy[i] - diff_y_t(g, mu, str_t, hq, m, n) + diff_y_s(g, mu, str_s, hh, m, n);
+        }
+}
+
+/* ------------------------------------------------------------------ */
+/* Function/vel_ssh.f90:379-679 */
+void ora_barotropic_dynamics(const ora_grid *g, double tau, int nstep, int ksw4,
+                             double *ubrtr_e, double *ubrtrp_e,
+                             double *vbrtr_e, double *vbrtrp_e,
+                             double *ssh_e, double *sshp_e,
+                             double *ubrtr_i, double *vbrtr_i,
+                             double *ssh4gradx, double *ssh4grady,
+                             const double *rhsx, const double *rhsy,
+                             const double *wflux, const double *mu,
+                             const double *mu4, double *vort,
+                             double *str_t2d, double *str_s2d,
+                             double *fx, double *fy, const double *rdis,
+                             double *rhsx_adv, double *rhsy_adv,
+                             double *rhsx_dif, double *rhsy_dif)
+{
+    SETUP(&g->b);
+    const size_t nt = NTOT(B);
+    const size_t bytes = nt * sizeof(double);
+    const double grav = g->free_fall_acc, rho = g->ref_den, ts = g->time_smooth;
+    const double ffs = (double)g->full_free_surface;
+    const double *dx = g->dx, *dy = g->dy, *dxt = g->dxt, *dyt = g->dyt;
+    const double *dxh = g->dxh, *dyh = g->dyh, *dxb = g->dxb, *dyb = g->dyb;
+    const double *rlh = g->rlh_s;
+
+    /* :454-462 work arrays */
+    double *u = malloc(bytes), *v = malloc(bytes), *ssh = malloc(bytes);
+    double *up = malloc(bytes), *vp = malloc(bytes), *sshp = malloc(bytes);
+    double *un = malloc(bytes), *vn = malloc(bytes), *sshn = malloc(bytes);
+
+    const double tau_inner = tau / (double)nstep; /* :465 */
+    memset(un, 0, bytes); /* :467-469 */
+    memset(vn, 0, bytes);
+    memset(sshn, 0, bytes);
+    memcpy(up, ubrtrp_e, bytes); /* :471-477 */
+    memcpy(vp, vbrtrp_e, bytes);
+    memcpy(sshp, sshp_e, bytes);
+    memcpy(u, ubrtr_e, bytes);
+    memcpy(v, vbrtr_e, bytes);
+    memcpy(ssh, ssh_e, bytes);
+    memset(ubrtr_i, 0, bytes); /* :479-482 */
+    memset(vbrtr_i, 0, bytes);
+    memset(ssh4gradx, 0, bytes);
+    memset(ssh4grady, 0, bytes);
+
+    const double four_nstep = (double)(4 * nstep);
+    for (int step = 1; step <= 2 * nstep; step++) {
+        /* :487-499 continuity */
+#pragma omp parallel for
+        for (int n = B->ny_start; n <= B->ny_end; n++)
+            for (int m = B->nx_start; m <= B->nx_end; m++)
+                if (g->lu[I(m, n)] > 0.5f)
+                    sshn[I(m, n)] = sshp[I(m, n)] + 2.0 * tau_inner * (wflux[I(m, n)] / rho * ffs
+                        - (u[I(m, n)] * g->hhu_e[I(m, n)] * dyh[I(m, n)] - u[I(m - 1, n)] * g->hhu_e[I(m - 1, n)] * dyh[I(m - 1, n)]
+                           + v[I(m, n)] * g->hhv_e[I(m, n)] * dxh[I(m, n)] - v[I(m, n - 1)] * g->hhv_e[I(m, n - 1)] * dxh[I(m, n - 1)])
+                          / (dx[I(m, n)] * dy[I(m, n)]));
+        halo(B, sshn); /* :501-509 */
+        if (g->full_free_surface > 0) /* :511-513 */
+            ora_hh_update(g, g->hhqn_e, g->hhun_e, g->hhvn_e, g->hhhn_e, sshn, g->hhq_rest);
+        ora_stress_components(g, up, vp, str_t2d, str_s2d); /* :516 */
+        ora_uv_trans(g, u, v, vort, g->hhq_e, g->hhu_e, g->hhv_e, g->hhh_e, rhsx_adv, rhsy_adv); /* :518-520 */
+        ora_uv_diff2(g, mu, str_t2d, str_s2d, g->hhq_e, g->hhu_e, g->hhv_e, g->hhh_e, rhsx_dif, rhsy_dif); /* :521-523 */
+        if (ksw4 > 0) /* :525-529 */
+            ora_uv_diff4(g, mu4, str_t2d, str_s2d, fx, fy, g->hhq_e, g->hhu_e, g->hhv_e, g->hhh_e, rhsx_dif, rhsy_dif);
+
+        /* :531-573 momentum */
+#pragma omp parallel for
+        for (int n = B->ny_start; n <= B->ny_end; n++)
+            for (int m = B->nx_start; m <= B->nx_end; m++) {
+                size_t i = I(m, n);
+                if (g->lcu[i] > 0.5f) {
+                    double bp = g->hhun_e[i] * dxt[i] * dyh[i] / 2.0 / tau_inner;
+                    double bp0 = g->hhup_e[i] * dxt[i] * dyh[i] / 2.0 / tau_inner;
+                    double slx = -grav * (ssh[I(m + 1, n)] - ssh[i]) * dyh[i] * g->hhu_e[i];
+                    double slxn = -grav * (sshn[I(m + 1, n)] - sshn[i]) * dyh[i] * g->hhun_e[i];
+                    double grx = rhsx[i] + slx + rhsx_dif[i] + rhsx_adv[i]
+                                 - (rdis[i] + rdis[I(m + 1, n)]) / 2.0 * up[i] * dxt[i] * dyh[i] * g->hhu_e[i]
+                                 + (rlh[i] * g->hhh_e[i] * dxb[i] * dyb[i] * (v[I(m + 1, n)] + v[i])
+                                    + rlh[I(m, n - 1)] * g->hhh_e[I(m, n - 1)] * dxb[I(m, n - 1)] * dyb[I(m, n - 1)]
+                                      * (v[I(m + 1, n - 1)] + v[I(m, n - 1)])) / 4.0;
+                    un[i] = (up[i] * bp0 + grx) / bp;
+                    ubrtr_i[i] = ubrtr_i[i] + (u[i] * g->hhu_e[i] + un[i] * g->hhun_e[i]) / four_nstep;
+                    ssh4gradx[i] = ssh4gradx[i] + (slx + slxn) / four_nstep;
+                }
+                if (g->lcv[i] > 0.5f) {
+                    double bp = g->hhvn_e[i] * dyt[i] * dxh[i] / 2.0 / tau_inner;
+                    double bp0 = g->hhvp_e[i] * dyt[i] * dxh[i] / 2.0 / tau_inner;
+                    double sly = -grav * (ssh[I(m, n + 1)] - ssh[i]) * dxh[i] * g->hhv_e[i];
+                    double slyn = -grav * (sshn[I(m, n + 1)] - sshn[i]) * dxh[i] * g->hhvn_e[i];
+                    double gry = rhsy[i] + sly + rhsy_dif[i] + rhsy_adv[i]
+                                 - (rdis[i] + rdis[I(m, n + 1)]) / 2.0 * vp[i] * dxh[i] * dyt[i] * g->hhv_e[i]
+                                 - (rlh[i] * g->hhh_e[i] * dxb[i] * dyb[i] * (u[I(m, n + 1)] + u[i])
+                                    + rlh[I(m - 1, n)] * g->hhh_e[I(m - 1, n)] * dxb[I(m - 1, n)] * dyb[I(m - 1, n)]
+                                      * (u[I(m - 1, n + 1)] + u[I(m - 1, n)])) / 4.0;
+                    vn[i] = (vp[i] * bp0 + gry) / bp;
+                    vbrtr_i[i] = vbrtr_i[i] + (v[i] * g->hhv_e[i] + vn[i] * g->hhvn_e[i]) / four_nstep;
+                    ssh4grady[i] = ssh4grady[i] + (sly + slyn) / four_nstep;
+                }
+            }
+        halo(B, un); /* :575-586 */
+        halo(B, vn);
+
+        /* :589-612 Robert-Asselin filter and time shift, halo-inclusive */
+        const double ns = (double)nstep;
+#pragma omp parallel for
+        for (int n = B->ny_start - 1; n <= B->ny_end + 1; n++)
+            for (int m = B->nx_start - 1; m <= B->nx_end + 1; m++) {
+                size_t i = I(m, n);
+                if (g->lu[i] > 0.5f) { sshp[i] = asselin(ts, ssh[i], sshn[i], sshp[i], ns); ssh[i] = sshn[i]; }
+                if (g->lcu[i] > 0.5f) { up[i] = asselin(ts, u[i], un[i], up[i], ns); u[i] = un[i]; }
+                if (g->lcv[i] > 0.5f) { vp[i] = asselin(ts, v[i], vn[i], vp[i], ns); v[i] = vn[i]; }
+            }
+        if (g->full_free_surface > 0) /* :614-619 */
+            ora_hh_shift(g, g->hhq_e, g->hhqp_e, g->hhqn_e, g->hhu_e, g->hhup_e, g->hhun_e,
+                         g->hhv_e, g->hhvp_e, g->hhvn_e, g->hhh_e, g->hhhp_e, g->hhhn_e, nstep);
+        if (step == nstep) { /* :638-648 */
+            memcpy(ubrtrp_e, up, bytes);
+            memcpy(vbrtrp_e, vp, bytes);
+            memcpy(sshp_e, sshp, bytes);
+            memcpy(ubrtr_e, u, bytes);
+            memcpy(vbrtr_e, v, bytes);
+            memcpy(ssh_e, ssh, bytes);
+        }
+    }
+    halo(B, ubrtr_i); /* :652-666 */
+    halo(B, vbrtr_i);
+    if (g->full_free_surface > 0) /* :668-675 */
+        ora_hh_init(g, g->hhq_e, g->hhqp_e, g->hhqn_e, g->hhu_e, g->hhup_e, g->hhun_e,
+                    g->hhv_e, g->hhvp_e, g->hhvn_e, g->hhh_e, g->hhhp_e, g->hhhn_e,
+                    ssh_e, sshp_e, g->hhq_rest);
+    (void)ffs;
+    free(sshn); free(vn); free(un); free(sshp); free(vp); free(up); free(ssh); free(v); free(u);
+}
+
+/* Function/vel_ssh.f90:682-751 */
+void ora_ssh_internal(const ora_grid *g, double tau, double *ssh_i,
+                      double *sshp_i, const double *u, const double *v,
+                      const double *wflux, double *hhqn, double *hhun,
+                      double *hhvn, double *hhhn)
+{
+    SETUP(&g->b);
+    const size_t nt = NTOT(B);
+    const double rho = g->ref_den, ffs = (double)g->full_free_surface, ts = g->time_smooth;
+    double *ssh_new = calloc(nt, sizeof(double)); /* :704-705 */
+#pragma omp parallel for
+    for (int n = B->ny_start; n <= B->ny_end; n++)
+        for (int m = B->nx_start; m <= B->nx_end; m++)
+            if (g->lu[I(m, n)] > 0.5f)
+                ssh_new[I(m, n)] = sshp_i[I(m, n)] + 2.0 * tau * (wflux[I(m, n)] / rho * ffs
+                    - (u[I(m, n)] * g->dyh[I(m, n)] - u[I(m - 1, n)] * g->dyh[I(m - 1, n)]
+                       + v[I(m, n)] * g->dxh[I(m, n)] - v[I(m, n - 1)] * g->dxh[I(m, n - 1)])
+                      / (g->dx[I(m, n)] * g->dy[I(m, n)]));
+    halo(B, ssh_new); /* :721-729 */
+    if (g->full_free_surface > 0) /* :733-735 */
+        ora_hh_update(g, hhqn, hhun, hhvn, hhhn, ssh_new, g->hhq_rest);
+#pragma omp parallel for
+    for (int n = B->ny_start - 1; n <= B->ny_end + 1; n++) /* :738-749 */
+        for (int m = B->nx_start - 1; m <= B->nx_end + 1; m++) {
+            size_t i = I(m, n);
+            if (g->lu[i] > 0.5f) {
+                sshp_i[i] = ssh_i[i] + ts * (ssh_new[i] - 2.0 * ssh_i[i] + sshp_i[i]) / 2.0;
+                ssh_i[i] = ssh_new[i];
+            }
+        }
+    free(ssh_new);
+}
+
+/* ------------------------------------------------------------------ */
+/* Control/init_pars.f90:459-481 */
+void ora_r_diss(const ora_grid *g, double r_fric, double *r_diss)
+{
+    SETUP(&g->b);
+    const double *h = g->hhq_rest, *dxt = g->dxt, *dyt = g->dyt;
+    const float *lcu = g->lcu, *lcv = g->lcv;
+#pragma omp parallel for
+    for (int n = B->ny_start; n <= B->ny_end; n++)
+        for (int m = B->nx_start; m <= B->nx_end; m++)
+            if (g->lu[I(m, n)] > 0.5f) {
+                double a = (h[I(m + 1, n)] - h[I(m, n)]) / dxt[I(m, n)];
+                double c = (h[I(m, n)] - h[I(m - 1, n)]) / dxt[I(m - 1, n)];
+                double hx2 = (a * a * (double)lcu[I(m, n)] + c * c * (double)lcu[I(m - 1, n)])
+                             / (double)(lcu[I(m, n)] + lcu[I(m - 1, n)]);
+                double d = (h[I(m, n + 1)] - h[I(m, n)]) / dyt[I(m, n)];
+                double e = (h[I(m, n)] - h[I(m, n - 1)]) / dyt[I(m, n - 1)];
+                double hy2 = (d * d * (double)lcv[I(m, n)] + e * e * (double)lcv[I(m, n - 1)])
+                             / (double)(lcv[I(m, n)] + lcv[I(m, n - 1)]);
+                r_diss[I(m, n)] = r_fric * sqrt(hx2 + hy2);
+            }
+    halo(B, r_diss);
+}
+
+/* Function/fluxes.f90:29-37 */
+void ora_surface_stress(const ora_grid *g, const double *taux,
+                        const double *tauy, double *ssx, double *ssy)
+{
+    SETUP(&g->b);
+    const double *dx = g->dx, *dy = g->dy, rho = g->ref_den;
+#pragma omp parallel for
+    for (int n = B->ny_start; n <= B->ny_end; n++)
+        for (int m = B->nx_start; m <= B->nx_end; m++) {
+            if (g->lcu[I(m, n)] > 0.5f)
+                ssx[I(m, n)] = (taux[I(m, n)] * dx[I(m, n)] * dy[I(m, n)]
+                                + taux[I(m + 1, n)] * dx[I(m + 1, n)] * dy[I(m + 1, n)])
+                               / rho / 2.0 / g->dxt[I(m, n)] / g->dyh[I(m, n)];
+            if (g->lcv[I(m, n)] > 0.5f)
+                ssy[I(m, n)] = (tauy[I(m, n)] * dx[I(m, n)] * dy[I(m, n)]
+                                + tauy[I(m, n + 1)] * dx[I(m, n + 1)] * dy[I(m, n + 1)])
+                               / rho / 2.0 / g->dxh[I(m, n)] / g->dyt[I(m, n)];
+        }
+}
+
+static inline double opt(const double *a, size_t i) { return a ? a[i] : 0.0; }
+
+/* Control/dyncall.f90:110-130 */
+void ora_rhs2d(const ora_grid *g, double *rhsx2d, double *rhsy2d,
+               const double *diff_disp_x, const double *diff_disp_y,
+               const double *tran_x, const double *tran_y,
+               const double *tran_disp_x, const double *tran_disp_y,
+               const double *ssx, const double *ssy, const double *bsx,
+               const double *bsy, const double *slpr, const double *hhu,
+               const double *hhv)
+{
+    SETUP(&g->b);
+    const double rho = g->ref_den;
+#pragma omp parallel for
+    for (int n = B->ny_start; n <= B->ny_end; n++)
+        for (int m = B->nx_start; m <= B->nx_end; m++) {
+            size_t i = I(m, n);
+            if (g->lcu[i] > 0.5f)
+                rhsx2d[i] = rhsx2d[i] - opt(diff_disp_x, i) + opt(tran_x, i) - opt(tran_disp_x, i)
+                            + (opt(ssx, i) + opt(bsx, i)) * g->dxt[i] * g->dyh[i]
+                            - (opt(slpr, I(m + 1, n)) - opt(slpr, i)) * hhu[i] * g->dyh[i] / rho;
+            if (g->lcv[i] > 0.5f)
+                rhsy2d[i] = rhsy2d[i] - opt(diff_disp_y, i) + opt(tran_y, i) - opt(tran_disp_y, i)
+                            + (opt(ssy, i) + opt(bsy, i)) * g->dyt[i] * g->dxh[i]
+                            - (opt(slpr, I(m, n + 1)) - opt(slpr, i)) * hhv[i] * g->dxh[i] / rho;
+        }
+}
+
+/* Control/dyncall.f90:452-516 (barotropic fields only) */
+long ora_guard(const ora_grid *g, const double *ssh, const double *u,
+               const double *v)
+{
+    SETUP(&g->b);
+    long bad = 0;
+    for (int n = B->ny_start; n <= B->ny_end; n++)
+        for (int m = B->nx_start; m <= B->nx_end; m++) {
+            size_t i = I(m, n);
+            if (g->lu[i] > 0.5f && !(ssh[i] < 10.0 && ssh[i] > -10.0)) bad++;
+            if (g->lcu[i] > 0.5f && !(u[i] < 100.0 && u[i] > -100.0)) bad++;
+            if (g->lcv[i] > 0.5f && !(v[i] < 100.0 && v[i] > -100.0)) bad++;
+        }
+    return bad;
+}
+
+void ora_diag(const ora_grid *g, const double *ssh, const double *u,
+              const double *v, const double *hu, const double *hv,
+              double *volume, double *energy)
+{
+    SETUP(&g->b);
+    double vol = 0.0, en = 0.0;
+    const double grav = g->free_fall_acc;
+    for (int n = B->ny_start; n <= B->ny_end; n++) {
+        double rv = 0.0, re = 0.0;
+        for (int m = B->nx_start; m <= B->nx_end; m++) {
+            size_t i = I(m, n);
+            if (g->lu[i] > 0.5f) {
+                double a = g->dx[i] * g->dy[i];
+                rv += (g->hhq_rest[i] + ssh[i]) * a;
+                re += 0.5 * grav * ssh[i] * ssh[i] * a;
+            }
+            if (g->lcu[i] > 0.5f) re += 0.5 * hu[i] * u[i] * u[i] * g->dxt[i] * g->dyh[i];
+            if (g->lcv[i] > 0.5f) re += 0.5 * hv[i] * v[i] * v[i] * g->dxh[i] * g->dyt[i];
+        }
+        vol += rv;
+        en += re;
+    }
+    *volume = vol;
+    *energy = en;
+}

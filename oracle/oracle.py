@@ -1,0 +1,212 @@
+"""ctypes front end of the CPU oracle (liboracle.so) -- TEST INFRASTRUCTURE.
+
+Only tests/, __graft_entry__.smoke() and the CPU-baseline leg of bench.py
+use this module, always as the checker or the timed CPU reference, never as
+the product path.  Functions take the same Basin objects and argument
+orders as inmsom_elfs_b200.solver, so a test can run the same call on both.
+Parity with the Fortran reference itself is unpinned (see oracle.h).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+from pathlib import Path
+
+import numpy as np
+
+HERE = Path(__file__).resolve().parent
+LIB_PATH = HERE / "liboracle.so"
+
+DP = ctypes.POINTER(ctypes.c_double)
+FP = ctypes.POINTER(ctypes.c_float)
+
+MASKS = ("lu", "luu", "luh", "lcu", "lcv", "llu", "llv")
+METRICS = ("dx", "dy", "dxt", "dyt", "dxh", "dyh", "dxb", "dyb")
+DEPTHS = ("hhq_e", "hhqp_e", "hhqn_e", "hhu_e", "hhup_e", "hhun_e",
+          "hhv_e", "hhvp_e", "hhvn_e", "hhh_e", "hhhp_e", "hhhn_e")
+DYN_ARGS = ("ubrtr_e", "ubrtrp_e", "vbrtr_e", "vbrtrp_e", "ssh_e", "sshp_e",
+            "ubrtr_i", "vbrtr_i", "ssh4gradx", "ssh4grady", "RHSx", "RHSy", "wflux",
+            "mu", "mu4", "vort", "str_t2d", "str_s2d", "fx", "fy", "rdis",
+            "RHSx_adv", "RHSy_adv", "RHSx_dif", "RHSy_dif")
+
+
+class OraBounds(ctypes.Structure):
+    _fields_ = [(n, ctypes.c_int) for n in (
+        "nx_start", "nx_end", "ny_start", "ny_end", "bnd_x1", "bnd_x2", "bnd_y1", "bnd_y2",
+        "mmm", "mm", "nnn", "nn", "periodicity_x", "periodicity_y")]
+
+
+class OraGrid(ctypes.Structure):
+    _fields_ = ([("b", OraBounds), ("time_smooth", ctypes.c_double),
+                 ("free_fall_acc", ctypes.c_double), ("ref_den", ctypes.c_double),
+                 ("full_free_surface", ctypes.c_int)]
+                + [(k, FP) for k in MASKS] + [(k, DP) for k in METRICS]
+                + [("rlh_s", DP), ("hhq_rest", DP)] + [(k, DP) for k in DEPTHS])
+
+
+_lib = None
+
+
+def build() -> Path:
+    subprocess.run(["make", "-s", "-C", str(HERE)], check=True)
+    return LIB_PATH
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not LIB_PATH.exists():
+            build()
+        _lib = ctypes.CDLL(str(LIB_PATH))
+        _lib.ora_guard.restype = ctypes.c_long
+    return _lib
+
+
+def _d(a):
+    if a is None:
+        return None
+    assert a.dtype == np.float64 and a.flags.f_contiguous
+    return a.ctypes.data_as(DP)
+
+
+def _f(a):
+    assert a.dtype == np.float32 and a.flags.f_contiguous
+    return a.ctypes.data_as(FP)
+
+
+def bounds_struct(b) -> OraBounds:
+    return OraBounds(*b.astuple())
+
+
+def grid_struct(basin) -> OraGrid:
+    """ora_grid pointing at the basin's arrays (keep the basin alive)."""
+    c = basin.consts
+    g = OraGrid()
+    g.b = bounds_struct(basin.bounds)
+    g.time_smooth, g.free_fall_acc, g.ref_den = c.time_smooth, c.free_fall_acc, c.ref_den
+    g.full_free_surface = c.full_free_surface
+    for k in MASKS:
+        setattr(g, k, _f(basin.masks[k]))
+    for k in METRICS:
+        setattr(g, k, _d(basin.metrics[k]))
+    g.rlh_s, g.hhq_rest = _d(basin.rlh_s), _d(basin.hhq_rest)
+    for k in DEPTHS:
+        setattr(g, k, _d(basin.depths[k]))
+    return g
+
+
+def set_threads(n: int) -> None:
+    os.environ["OMP_NUM_THREADS"] = str(n)
+
+
+# ---------------------------------------------------------------------------
+def gridcon(bounds, lu):
+    out = {k: bounds.zeros(np.float32) for k in ("luu", "luh", "llu", "llv", "lcu", "lcv")}
+    b = bounds_struct(bounds)
+    load().ora_gridcon(ctypes.byref(b), _f(lu), _f(out["luu"]), _f(out["luh"]), _f(out["llu"]),
+                       _f(out["llv"]), _f(out["lcu"]), _f(out["lcv"]))
+    return out
+
+
+def cyclize8_x(bounds, f):
+    b = bounds_struct(bounds)
+    load().ora_cyclize8_x(ctypes.byref(b), _d(f))
+
+
+def cyclize8_y(bounds, f):
+    b = bounds_struct(bounds)
+    load().ora_cyclize8_y(ctypes.byref(b), _d(f))
+
+
+def wind_forcing(basin, taux=None, tauy=None):
+    """surface stress (Function/fluxes.f90:29-37) then the barotropic RHS
+    (Control/dyncall.f90:110-130) with all 3-D terms zero."""
+    b = basin.bounds
+    taux = basin.taux if taux is None else taux
+    tauy = basin.tauy if tauy is None else tauy
+    g = grid_struct(basin)
+    ssx, ssy, rx, ry = b.zeros(), b.zeros(), b.zeros(), b.zeros()
+    hhu, hhv = b.zeros(), b.zeros()
+    lib = load()
+    lib.ora_surface_stress(ctypes.byref(g), _d(taux), _d(tauy), _d(ssx), _d(ssy))
+    lib.ora_rhs2d(ctypes.byref(g), _d(rx), _d(ry), None, None, None, None, None, None,
+                  _d(ssx), _d(ssy), None, None, None, _d(hhu), _d(hhv))
+    return rx, ry
+
+
+def hh_init_external(basin):
+    g = grid_struct(basin)
+    d = basin.depths
+    load().ora_hh_init(ctypes.byref(g), *[_d(d[k]) for k in DEPTHS], _d(basin.state["ssh_e"]),
+                       _d(basin.state["sshp_e"]), _d(basin.hhq_rest))
+
+
+def barotropic_dynamics(basin, tau, nstep, ksw4=0, **override):
+    g = grid_struct(basin)
+    pools = (basin.state, basin.means, basin.forcing, basin.scratch)
+    arrs = []
+    for k in DYN_ARGS:
+        if k in override:
+            arrs.append(override[k])
+        else:
+            arrs.append(next(p[k] for p in pools if k in p))
+    load().ora_barotropic_dynamics(ctypes.byref(g), ctypes.c_double(tau), int(nstep), int(ksw4),
+                                   *[_d(a) for a in arrs])
+
+
+def ssh_internal(basin, tau, ssh_i, sshp_i, u, v, wflux, hhqn, hhun, hhvn, hhhn):
+    g = grid_struct(basin)
+    load().ora_ssh_internal(ctypes.byref(g), ctypes.c_double(tau), _d(ssh_i), _d(sshp_i), _d(u),
+                            _d(v), _d(wflux), _d(hhqn), _d(hhun), _d(hhvn), _d(hhhn))
+
+
+def r_diss(basin, r_fric, out=None):
+    out = basin.bounds.zeros() if out is None else out
+    g = grid_struct(basin)
+    load().ora_r_diss(ctypes.byref(g), ctypes.c_double(r_fric), _d(out))
+    return out
+
+
+def guard(basin, ssh=None, u=None, v=None):
+    s = basin.state
+    g = grid_struct(basin)
+    return int(load().ora_guard(ctypes.byref(g), _d(s["ssh_e"] if ssh is None else ssh),
+                                _d(s["ubrtr_e"] if u is None else u),
+                                _d(s["vbrtr_e"] if v is None else v)))
+
+
+def diag(basin):
+    """volume/energy of the state, with hu/hv from hh_init of that state."""
+    tmp = basin.copy()
+    hh_init_external(tmp)
+    g = grid_struct(tmp)
+    vol, en = ctypes.c_double(), ctypes.c_double()
+    s = tmp.state
+    load().ora_diag(ctypes.byref(g), _d(s["ssh_e"]), _d(s["ubrtr_e"]), _d(s["vbrtr_e"]),
+                    _d(tmp.depths["hhu_e"]), _d(tmp.depths["hhv_e"]), ctypes.byref(vol),
+                    ctypes.byref(en))
+    return vol.value, en.value
+
+
+def run_substeps(basin, nsub, dt, rhs_scale=None):
+    """The standalone integration: nsub calls of barotropic_dynamics(dt, 1),
+    keeping the saved *_e state; RHS multiplied by rhs_scale[k] in call k."""
+    rx0, ry0 = basin.forcing["RHSx"], basin.forcing["RHSy"]
+    for k in range(nsub):
+        if rhs_scale is None:
+            barotropic_dynamics(basin, dt, 1, 0)
+        else:
+            s = float(rhs_scale[k])
+            barotropic_dynamics(basin, dt, 1, 0, RHSx=np.asfortranarray(rx0 * s),
+                                RHSy=np.asfortranarray(ry0 * s))
+
+
+class OracleBackend:
+    """Basin set-up on the CPU oracle (tests only)."""
+
+    def gridcon(self, bounds, lu):
+        return gridcon(bounds, lu)
+
+    def wind_forcing(self, basin):
+        return wind_forcing(basin)
