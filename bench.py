@@ -52,6 +52,7 @@ def parse():
     p.add_argument("--e2e-calls", type=int, default=12)
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu", action="store_true")
+    p.add_argument("--no-e2e", action="store_true")
     return p.parse_args()
 
 
@@ -204,6 +205,40 @@ def run_reference(args):
     print(json.dumps(line), flush=True)
 
 
+def e2e_arm(args, b, local, barrier, maxall, ws):
+    """barotropic_dynamics(E2E_NSTEP*dt, E2E_NSTEP) through the C ABI with
+    pinned host arrays, host<->device copies inside the timed region."""
+    import torch
+    from inmsom_elfs_b200 import solver
+    pin = {}
+    cells = b.cells
+    eb = b.copy()
+    for grp in ("state", "means", "forcing", "scratch"):
+        d = getattr(eb, grp)
+        for k, v in d.items():
+            t = torch.empty(v.shape[::-1], dtype=torch.float64, pin_memory=True)
+            a = t.numpy().T          # Fortran-contiguous view of pinned memory
+            a[...] = v
+            d[k] = a
+            pin[k] = t
+    se = solver.BarotropicSolver(eb, device=local, resident=True)
+    se.barotropic_dynamics(E2E_NSTEP * b.dt, E2E_NSTEP)
+    barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_calls):
+        se.barotropic_dynamics(E2E_NSTEP * b.dt, E2E_NSTEP)
+    barrier()
+    e2e_s = maxall(time.perf_counter() - t0)
+    se.close()
+    fb = 8 * b.bounds.shape[0] * b.bounds.shape[1]
+    return {"value": cells * E2E_NSTEP * args.e2e_calls * ws / e2e_s, "unit": METRIC,
+           "h2d_bytes_per_step": 6 * fb / E2E_NSTEP, "d2h_bytes_per_step": 4 * fb / E2E_NSTEP,
+           "call": f"inmsom_barotropic_dynamics(tau={E2E_NSTEP}*dt, nstep={E2E_NSTEP}) from pinned "
+                   f"host arrays: 6 forcing arrays in, 4 time-mean arrays out per call, "
+                   f"{2 * E2E_NSTEP} substeps with time means; h2d/d2h bytes per advancing step"}
+
+
+
 # ------------------------------------------------------------------ GPU arm
 def run_ours(args):
     import torch
@@ -256,31 +291,9 @@ def run_ours(args):
     peak, peak_kind = measured_hbm()
 
     # ---- e2e through the drop-in with pinned host buffers
-    pin = {}
-    eb = b.copy()
-    for grp in ("state", "means", "forcing", "scratch"):
-        d = getattr(eb, grp)
-        for k, v in d.items():
-            t = torch.empty(v.shape[::-1], dtype=torch.float64, pin_memory=True)
-            a = t.numpy().T          # Fortran-contiguous view of pinned memory
-            a[...] = v
-            d[k] = a
-            pin[k] = t
-    se = solver.BarotropicSolver(eb, device=local, resident=True)
-    se.barotropic_dynamics(E2E_NSTEP * b.dt, E2E_NSTEP)
-    barrier()
-    t0 = time.perf_counter()
-    for _ in range(args.e2e_calls):
-        se.barotropic_dynamics(E2E_NSTEP * b.dt, E2E_NSTEP)
-    barrier()
-    e2e_s = maxall(time.perf_counter() - t0)
-    se.close()
-    fb = 8 * b.bounds.shape[0] * b.bounds.shape[1]
-    e2e = {"value": cells * E2E_NSTEP * args.e2e_calls * ws / e2e_s, "unit": METRIC,
-           "h2d_bytes_per_step": 6 * fb / E2E_NSTEP, "d2h_bytes_per_step": 4 * fb / E2E_NSTEP,
-           "call": f"inmsom_barotropic_dynamics(tau={E2E_NSTEP}*dt, nstep={E2E_NSTEP}) from pinned "
-                   f"host arrays: 6 forcing arrays in, 4 time-mean arrays out per call, "
-                   f"{2 * E2E_NSTEP} substeps with time means; h2d/d2h bytes per advancing step"}
+    e2e = None
+    if not args.no_e2e:
+        e2e = e2e_arm(args, b, local, barrier, maxall, ws)
 
     cpu = None
     if cpu_copy is not None:

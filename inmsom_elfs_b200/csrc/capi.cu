@@ -124,7 +124,7 @@ int check_bounds(const inmsom_bounds *b)
     return INMSOM_OK;
 }
 
-Dom make_dom(const inmsom_bounds *b, long long pitch)
+Dom make_dom(const inmsom_bounds *b, long long pitch, int xoff)
 {
     Dom d;
     d.nx_start = b->nx_start; d.nx_end = b->nx_end; d.ny_start = b->ny_start; d.ny_end = b->ny_end;
@@ -132,6 +132,7 @@ Dom make_dom(const inmsom_bounds *b, long long pitch)
     d.mmm = b->mmm; d.mm = b->mm; d.nnn = b->nnn; d.nn = b->nn;
     d.px = b->periodicity_x; d.py = b->periodicity_y;
     d.pitch = pitch;
+    d.xoff = xoff;
     return d;
 }
 
@@ -150,8 +151,8 @@ int h2d(inmsom_ctx *c, T *dev, const T *host)
 {
     if (!host) return set_err(INMSOM_EARG, "NULL host array");
     const size_t w = (size_t)c->dom.nxa() * sizeof(T);
-    CK(cudaMemcpy2DAsync(dev, (size_t)c->dom.pitch * sizeof(T), host, w, w, (size_t)c->dom.nya(),
-                         cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpy2DAsync(dev + c->dom.xoff, (size_t)c->dom.pitch * sizeof(T), host, w, w,
+                         (size_t)c->dom.nya(), cudaMemcpyHostToDevice, c->stream));
     return INMSOM_OK;
 }
 
@@ -160,8 +161,8 @@ int d2h(inmsom_ctx *c, T *host, const T *dev)
 {
     if (!host) return set_err(INMSOM_EARG, "NULL host array");
     const size_t w = (size_t)c->dom.nxa() * sizeof(T);
-    CK(cudaMemcpy2DAsync(host, w, dev, (size_t)c->dom.pitch * sizeof(T), w, (size_t)c->dom.nya(),
-                         cudaMemcpyDeviceToHost, c->stream));
+    CK(cudaMemcpy2DAsync(host, w, dev + c->dom.xoff, (size_t)c->dom.pitch * sizeof(T), w,
+                         (size_t)c->dom.nya(), cudaMemcpyDeviceToHost, c->stream));
     return INMSOM_OK;
 }
 
@@ -305,9 +306,10 @@ int inmsom_gpu_init(inmsom_ctx **out, const inmsom_bounds *b, const inmsom_const
     c->c.ffs = k->full_free_surface;
     const int nxa = b->bnd_x2 - b->bnd_x1 + 1;
     c->plan = fused::make_plan(*b);
-    long long need = nxa > c->plan.min_pitch ? nxa : c->plan.min_pitch;
+    const int xoff = fused::XOFF;
+    long long need = nxa + xoff > c->plan.min_pitch ? nxa + xoff : c->plan.min_pitch;
     long long pitch = (need + 31) / 32 * 32;  // 256-byte rows
-    c->dom = make_dom(b, pitch);
+    c->dom = make_dom(b, pitch, xoff);
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
@@ -597,7 +599,7 @@ int inmsom_gridcon(const inmsom_bounds *b, const float *lu, float *luu, float *l
         return set_err(INMSOM_EARG, "NULL mask array");
     CK(cudaSetDevice(device));
     const int nxa = b->bnd_x2 - b->bnd_x1 + 1, nya = b->bnd_y2 - b->bnd_y1 + 1;
-    Dom d = make_dom(b, nxa);
+    Dom d = make_dom(b, nxa, 0);
     const size_t bytes = (size_t)nxa * nya * sizeof(float);
     float *dv[7] = {};
     const float *src[7] = {lu, luu, luh, llu, llv, lcu, lcv};

@@ -1,9 +1,10 @@
 // Fused streaming kernel of the barotropic step (see fused.h).
 //
-// Work decomposition.  A CTA of W threads owns device columns
-// [cs, cs+W) (thread t <-> column cs+t) and writes the W-2 columns of
-// threads 1..W-2; strips overlap by two columns.  It marches down a chunk of
-// output rows [r0, r1).  Iteration j computes, for the CTA's columns,
+// Work decomposition.  A CTA is one warp.  Lane l owns the two adjacent
+// device columns k0 = g0+2+2l and k0+1 of a 64-column strip starting at
+// device column g0+2 (g0 = 62*strip, even); strip columns 1..62 are written,
+// so strips overlap by two columns.  The CTA marches down a chunk of output
+// rows [r0, r1).  Iteration j computes, for its columns,
 //   stage 1, row j   : u/v-point depths of the current level and the
 //                      transports U = u*hu, V = v*hv;
 //   stage 2, row j-1 : new SSH (continuity), advective fluxes on T and h
@@ -11,15 +12,18 @@
 //                      tension and shear stresses times viscosity and depth;
 //   stage 3, row j-2 : u and v momentum, time-mean sums, Robert-Asselin
 //                      filter and time shift, stores.
-// Values a stage needs from the neighbouring column pass through a
-// double-buffered shared exchange row; values it needs from earlier rows of
-// its own column stay in registers.  So one __syncthreads per row suffices.
+// A value a stage needs from the neighbouring column is the other column
+// of the same lane or comes from the neighbouring lane by a warp shuffle;
+// values of earlier rows of the same column stay in registers.  There is no
+// CTA-wide barrier.
 //
-// Input rows j-2..j+1 of the ten input fields sit in a ring of RING
-// shared-memory slots; thread 0 refills the slot of row j-2 with row
-// j-2+RING by 1-D bulk TMA copies (cp.async.bulk, no multicast) completing
-// on that slot's mbarrier.  Every wait is bounded: on timeout the CTA sets
-// a status bit, drains its own copies (bounded) and returns.
+// Input rows j-2..j+1 of the input fields (a 68-column segment per field
+// and row, 16-byte aligned), the row's coefficients and the row's T-mask
+// bits sit in a ring of RING shared-memory slots.  Lane 0 refills the slot
+// of row j-2 with row j-2+RING by 1-D bulk TMA copies (cp.async.bulk, no
+// multicast) completing on that slot's mbarrier.  Every wait is bounded: on
+// timeout the CTA sets a status bit, drains its own copies (bounded) and
+// returns.
 #include "fused.h"
 
 #include <algorithm>
@@ -32,18 +36,19 @@ namespace fused {
 
 namespace {
 
-constexpr int W = 128;          // threads per CTA = columns per strip
-constexpr int SEG = W + 2;      // columns per ring row segment: cs-1 .. cs+W
-constexpr int RING = 6;         // ring slots (4 rows in use + 2 in flight)
-constexpr int NXCH = 8;         // doubles per thread in the exchange row
+constexpr int NL = 32;            // lanes = threads per CTA
+constexpr int NCOL = 2 * NL;      // strip columns
+constexpr int OUTW = NCOL - 2;    // written columns per strip
+constexpr int SEG = NCOL + 4;     // ring segment: strip columns -2 .. 65
+constexpr int RING = 6;           // ring slots (4 rows in use + 2 in flight)
+constexpr int CTAS_PER_SM = 7;
+constexpr int COEF_D = (int)(sizeof(RowCoef) / sizeof(double));
 constexpr unsigned WAIT_LIMIT = 1u << 20;
 
 // state order, as the *_e arguments: u, up, v, vp, ssh, sshp
 enum { S_U, S_UP, S_V, S_VP, S_SSH, S_SSHP };
 // ring fields
 enum { R_U, R_V, R_SSH, R_UP, R_VP, R_SSHP, R_H, R_RX, R_RY, R_NBASE, R_MU = R_NBASE, R_RD, R_WF, R_N2D };
-// exchange row slots
-enum { X_U, X_V, X_FX, X_ST, X_SSHN, X_GX, X_QV, X_SS };
 
 struct Params {
     const double *src[6];
@@ -52,6 +57,7 @@ struct Params {
     double *acc[4];
     const uint32_t *bits;
     const RowCoef *rows;
+    RowCoef rc;            // row-invariant coefficients (used when !ROWVAR)
     long long pitch;
     int bm_words;
     int chunk_rows;
@@ -111,50 +117,49 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
 }
 
 template <bool F2D>
-struct Smem {
+struct Layout {
     static constexpr int NF = F2D ? R_N2D : R_NBASE;
-    static constexpr size_t ring_bytes = (size_t)RING * NF * SEG * sizeof(double);
-    static constexpr size_t bits_bytes = (size_t)RING * 8 * sizeof(uint32_t);
-    static constexpr size_t xch_bytes = (size_t)2 * NXCH * W * sizeof(double);
-    static constexpr size_t bar_bytes = (size_t)RING * sizeof(uint64_t);
-    static constexpr size_t total = ring_bytes + bits_bytes + xch_bytes + bar_bytes;
-    static constexpr uint32_t row_tx = (uint32_t)(NF * SEG * sizeof(double) + 8 * sizeof(uint32_t));
+    static constexpr int SLOT_D = NF * SEG + COEF_D + 4;   // doubles per slot
+    static constexpr size_t bytes = (size_t)RING * SLOT_D * sizeof(double) + RING * sizeof(uint64_t);
+    static constexpr uint32_t row_tx = (uint32_t)((NF * SEG + COEF_D + 4) * sizeof(double));
 };
 
-template <bool F2D>
-__global__ void __launch_bounds__(W, 3) k_substep(const Params p)
-{
-    using L = Smem<F2D>;
-    constexpr int NF = L::NF;
-    extern __shared__ __align__(128) unsigned char smem[];
-    double *ring = reinterpret_cast<double *>(smem);
-    uint32_t *rbits = reinterpret_cast<uint32_t *>(smem + L::ring_bytes);
-    double *xch = reinterpret_cast<double *>(smem + L::ring_bytes + L::bits_bytes);
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + L::ring_bytes + L::bits_bytes + L::xch_bytes);
+__device__ __forceinline__ double sel(int m, double x) { return m ? x : 0.0; }
 
-    const int t = threadIdx.x;
-    const int cs = 1 + blockIdx.x * (W - 2);   // device column of thread 0
-    const int c = cs + t;
+// 1 / (number of ocean T points) for the mask-weighted depth averages
+__device__ __forceinline__ double rcount(int n)
+{
+    return n == 4 ? 0.25 : (n == 3 ? 1.0 / 3.0 : (n == 2 ? 0.5 : (n == 1 ? 1.0 : 0.0)));
+}
+
+#define SHFL_UP(x) __shfl_up_sync(0xffffffffu, (x), 1)
+#define SHFL_DN(x) __shfl_down_sync(0xffffffffu, (x), 1)
+
+template <bool F2D, bool ROWVAR>
+__global__ void __launch_bounds__(NL, CTAS_PER_SM) k_substep(const __grid_constant__ Params p)
+{
+    using L = Layout<F2D>;
+    constexpr int NF = L::NF;
+    extern __shared__ __align__(128) double smem[];
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + RING * L::SLOT_D);
+
+    const int l = threadIdx.x;
+    const int g0 = blockIdx.x * OUTW;          // device column of segment offset 0
+    const int k0 = g0 + 2 + 2 * l;             // this lane's columns k0, k0+1
     const int r0 = p.r_first + blockIdx.y * p.chunk_rows;
     const int r1 = min(r0 + p.chunk_rows, p.r_last + 1);   // exclusive
     if (r0 >= r1) return;
     const int row_lo = r0 - 2, row_hi = r1 + 1;             // rows kept in the ring
-    const int wbase = ((cs - 1) >> 7) << 2;                 // first mask word of the window
-    const int bbase = wbase * 32;                           // its first column
-    const long long seg0 = cs - 1;
+    const int wbase = (g0 >> 7) << 2;                       // first mask word of the window
+    const int bsh = k0 - wbase * 32;                        // bit of k0 in the window
+    const int po = 2 * l + 2;                               // segment offset of k0
 
-    auto slot_of = [&](int row) { return (row - row_lo) % RING; };
-    auto fld = [&](int slot, int f) -> const double * { return ring + ((size_t)slot * NF + f) * SEG; };
-    auto bit = [&](int slot, int col) -> int {
-        const int k = col - bbase;
-        return (int)((rbits[slot * 8 + (k >> 5)] >> (k & 31)) & 1u);
-    };
-    auto issue = [&](int row) {
-        const int s = slot_of(row);
+    auto slotp = [&](int s) { return smem + (size_t)s * L::SLOT_D; };
+    auto issue = [&](int row, int s) {
+        double *d = slotp(s);
         uint64_t *bar = &mbar[s];
         mbar_expect_tx(bar, L::row_tx);
-        const long long off = (long long)row * p.pitch + seg0;
-        double *d = ring + (size_t)s * NF * SEG;
+        const long long off = (long long)row * p.pitch + g0;
         const uint32_t nb = SEG * sizeof(double);
         bulk_load(d + R_U * SEG, p.src[S_U] + off, nb, bar);
         bulk_load(d + R_V * SEG, p.src[S_V] + off, nb, bar);
@@ -170,223 +175,313 @@ __global__ void __launch_bounds__(W, 3) k_substep(const Params p)
             bulk_load(d + R_RD * SEG, p.rdis + off, nb, bar);
             bulk_load(d + R_WF * SEG, p.wflux + off, nb, bar);
         }
-        bulk_load(rbits + s * 8, p.bits + (size_t)row * p.bm_words + wbase, 32, bar);
+        bulk_load(d + NF * SEG, p.rows + row, sizeof(RowCoef), bar);
+        bulk_load(d + NF * SEG + COEF_D, p.bits + (size_t)row * p.bm_words + wbase, 32, bar);
     };
+    // field f of a slot: own pair (k0, k0+1), left neighbour (k0-1), right (k0+2)
+    auto pair = [&](int s, int f) {
+        return *reinterpret_cast<const double2 *>(slotp(s) + f * SEG + po);
+    };
+    auto leftv = [&](int s, int f) { return slotp(s)[f * SEG + po - 1]; };
+    auto rightv = [&](int s, int f) { return slotp(s)[f * SEG + po + 2]; };
+    auto coef = [&](int s) { return reinterpret_cast<const RowCoef *>(slotp(s) + NF * SEG); };
+    auto mask3 = [&](int s) -> uint32_t {   // bits: lu(k0), lu(k0+1), lu(k0+2)
+        const uint32_t *w = reinterpret_cast<const uint32_t *>(slotp(s) + NF * SEG + COEF_D);
+        return __funnelshift_r(w[bsh >> 5], w[(bsh >> 5) + 1], bsh & 31) & 7u;
+    };
+#define CF(s, x) (ROWVAR ? coef(s)->x : p.rc.x)
 
-    if (t == 0) {
+    if (l == 0) {
         for (int s = 0; s < RING; s++) mbar_init(&mbar[s], 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     }
-    __syncthreads();
-    int issued = row_lo - 1;   // (meaningful in thread 0 only)
-    if (t == 0)
-        for (int row = row_lo; row < row_lo + RING && row <= row_hi; row++) issue(row), issued = row;
+    __syncwarp();
+    int issued = row_lo - 1;
+    if (l == 0)
+        for (int row = row_lo; row < row_lo + RING && row <= row_hi; row++) issue(row, row - row_lo), issued = row;
 
-    const int tm = max(t - 1, 0), tp = min(t + 1, W - 1);
-    const bool out_col = t >= 1 && t <= W - 2 && c >= p.c_first && c <= p.c_last;
+    const bool out0 = l >= 1 && k0 >= p.c_first && k0 <= p.c_last;
+    const bool out1 = l <= NL - 2 && k0 + 1 >= p.c_first && k0 + 1 <= p.c_last;
 
-    // stage-1 results of earlier rows (own column)
-    double U_cur = 0, V_cur = 0, V_prev = 0;
-    // stage-2 results of earlier rows (own column)
-    double sshn_p = 0, FX_p = 0, GX_p = 0, QV_p = 0, ST_p = 0, SS_p = 0, SS_pp = 0;
-    double FY_p = 0, FY_pp = 0, QU_p = 0, QU_pp = 0, GY_p = 0;
+    // ring slots of rows j-2, j-1, j, j+1: the slot of row r is (r - row_lo) % RING;
+    // for j = r0-1 these are rows r0-3 (none), r0-2, r0-1, r0
+    int s_m2 = RING - 1, s_m1 = 0, s_0 = 1, s_p1 = 2;
+    // T-mask bits, 3 per row: row j+1 in bits 0-2, j in 3-5, j-1 in 6-8, j-2 in 9-11
+    uint32_t mk = 0;
+    // stage-1 windows (two columns each)
+    double hq_m1[3] = {0, 0, 0}, hq_0[3] = {0, 0, 0};      // H+ssh at k0, k0+1, k0+2, rows j-1, j
+    double U_c[2] = {0, 0}, V_c[2] = {0, 0}, V_p[2] = {0, 0};   // U(j-1), V(j-1), V(j-2)
+    double Ul_c = 0, Vr_c = 0;                             // U(k0-1, j-1), V(k0+2, j-1)
+    double hu_w[2][2] = {{0, 0}, {0, 0}}, hv_w[2][2] = {{0, 0}, {0, 0}};   // rows j-2, j-1
+    // stage-2 results: _p row R, _pp row R-1 (own columns) and row-R neighbours
+    double sshn_p[2] = {0, 0}, FX_p[2] = {0, 0}, GX_p[2] = {0, 0}, QV_p[2] = {0, 0};
+    double ST_p[2] = {0, 0}, SS_p[2] = {0, 0}, SS_pp[2] = {0, 0}, FY_p[2] = {0, 0};
+    double FY_pp[2] = {0, 0}, QU_p[2] = {0, 0}, QU_pp[2] = {0, 0}, GY_p[2] = {0, 0};
+    double FXr_p = 0, STr_p = 0, SNr_p = 0, GXl_p = 0, QVl_p = 0, SSl_p = 0;
 
     int waited = row_lo - 1;
     bool abort = false;
     for (int j = r0 - 1; j <= r1 + 1; j++) {
+        // --- rows up to j+1 must have landed ------------------------------
         const int need = min(j + 1, row_hi);
         bool ok = true;
         while (waited < need) {
             const int row = waited + 1;
             const uint32_t par = (uint32_t)(((row - row_lo) / RING) & 1);
-            if (!mbar_wait(&mbar[slot_of(row)], par)) { ok = false; break; }
+            if (!mbar_wait(&mbar[(row - row_lo) % RING], par)) { ok = false; break; }
             waited = row;
+            mk = (mk << 3) | mask3((row - row_lo) % RING);
         }
-        const double *xr = xch + (size_t)((j + 1) & 1) * NXCH * W;   // written at j-1
-        double *xw = xch + (size_t)(j & 1) * NXCH * W;
+        if (j + 1 > row_hi) mk <<= 3;   // keep the row alignment of mk
+        ok = __all_sync(0xffffffffu, ok);   // the shuffles below need every lane
 
-        double U_new = 0, V_new = 0;
-        double sshn_c = 0, FX_c = 0, GX_c = 0, QV_c = 0, ST_c = 0, SS_c = 0, FY_c = 0, QU_c = 0, GY_c = 0;
+        double U_n[2] = {0, 0}, V_n[2] = {0, 0}, Ul_n = 0, Vr_n = 0, hu_n[2] = {0, 0}, hv_n[2] = {0, 0};
+        double hq_p1[3] = {0, 0, 0};
+        double sshn_c[2] = {0, 0}, FX_c[2] = {0, 0}, GX_c[2] = {0, 0}, QV_c[2] = {0, 0};
+        double ST_c[2] = {0, 0}, SS_c[2] = {0, 0}, FY_c[2] = {0, 0}, QU_c[2] = {0, 0}, GY_c[2] = {0, 0};
+        double FXr_c = 0, STr_c = 0, SNr_c = 0, GXl_c = 0, QVl_c = 0, SSl_c = 0;
         if (ok) {
             // ---------------- stage 1: row j ---------------------------------
             if (j <= r1) {
-                const int sj = slot_of(j), sn = slot_of(j + 1);
-                const RowCoef &rc = p.rows[j];
-                const double *Hj = fld(sj, R_H), *Ej = fld(sj, R_SSH);
-                const int l0 = bit(sj, c), l1 = bit(sj, c + 1), ln = bit(sn, c);
-                const double hq0 = Hj[t + 1] + Ej[t + 1];
-                const double hq1 = Hj[t + 2] + Ej[t + 2];
-                const double hqn = fld(sn, R_H)[t + 1] + fld(sn, R_SSH)[t + 1];
-                // Function/depth.f90:127-139: mask-weighted averages onto u and v points
-                const double su = (l0 ? hq0 : 0.0) + (l1 ? hq1 : 0.0);
-                const double hu = su * (l0 + l1 == 2 ? rc.ku2 : (l0 + l1 == 1 ? rc.ku : 0.0));
-                const double sv = (l0 ? hq0 * rc.wv0 : 0.0) + (ln ? hqn * rc.wv1 : 0.0);
-                const double hv = sv * (l0 + ln == 2 ? 0.5 : (l0 + ln == 1 ? 1.0 : 0.0));
-                U_new = fld(sj, R_U)[t + 1] * hu;
-                V_new = fld(sj, R_V)[t + 1] * hv;
-                xw[X_U * W + t] = U_new;
-                xw[X_V * W + t] = V_new;
+                const uint32_t mj = (mk >> 3) & 7u, mn = mk & 7u;
+                {   // H + ssh of row j+1 at k0, k0+1, k0+2
+                    const double2 h = pair(s_p1, R_H), e = pair(s_p1, R_SSH);
+                    hq_p1[0] = h.x + e.x;
+                    hq_p1[1] = h.y + e.y;
+                    hq_p1[2] = rightv(s_p1, R_H) + rightv(s_p1, R_SSH);
+                }
+                if (j == r0 - 1) {   // first iteration: row j itself
+                    const double2 h = pair(s_0, R_H), e = pair(s_0, R_SSH);
+                    hq_0[0] = h.x + e.x;
+                    hq_0[1] = h.y + e.y;
+                    hq_0[2] = rightv(s_0, R_H) + rightv(s_0, R_SSH);
+                }
+                const double ku = CF(s_0, ku), ku2 = CF(s_0, ku2), wv0 = CF(s_0, wv0), wv1 = CF(s_0, wv1);
+                const double2 u = pair(s_0, R_U), v = pair(s_0, R_V);
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    // Function/depth.f90:127-139 mask-weighted averages to u and v points
+                    const int a = (mj >> e) & 1, b = (mj >> (e + 1)) & 1, c = (mn >> e) & 1;
+                    hu_n[e] = (sel(a, hq_0[e]) + sel(b, hq_0[e + 1])) * (a & b ? ku2 : (a | b ? ku : 0.0));
+                    hv_n[e] = (sel(a, hq_0[e] * wv0) + sel(c, hq_p1[e] * wv1)) * (a & c ? 0.5 : (a | c ? 1.0 : 0.0));
+                }
+                U_n[0] = u.x * hu_n[0];
+                U_n[1] = u.y * hu_n[1];
+                V_n[0] = v.x * hv_n[0];
+                V_n[1] = v.y * hv_n[1];
             }
+            Ul_n = SHFL_UP(U_n[1]);
+            Vr_n = SHFL_DN(V_n[0]);
             // ---------------- stage 2: row rho = j-1 -------------------------
             if (j >= r0) {
-                const int rho = j - 1;
-                const int sr = slot_of(rho), sm = slot_of(rho - 1), su_ = slot_of(rho + 1);
-                const RowCoef &rc = p.rows[rho];
-                const double *u_r = fld(sr, R_U), *v_r = fld(sr, R_V), *e_r = fld(sr, R_SSH);
-                const double *h_r = fld(sr, R_H), *up_r = fld(sr, R_UP), *vp_r = fld(sr, R_VP);
-                const double *u_u = fld(su_, R_U), *e_u = fld(su_, R_SSH), *h_u = fld(su_, R_H);
-                const int lc = bit(sr, c), lr = bit(sr, c + 1), lu_ = bit(su_, c), lur = bit(su_, c + 1);
-                const int luu = lc & lr & lu_ & lur;
-                const double U_l = xr[X_U * W + tm];    // U(c-1, rho)
-                const double V_r = xr[X_V * W + tp];    // V(c+1, rho)
-                // vel_ssh.f90:491-494 continuity (leap-frog over 2*tau_inner)
-                const double wq = F2D ? fld(sr, R_WF)[t + 1] * p.inv_rho : p.wq0;
-                const double div = (U_cur - U_l) * rc.c_u + V_cur * rc.c_v0 - V_prev * rc.c_v1;
-                sshn_c = lc ? fld(sr, R_SSHP)[t + 1] + p.two_ti * (wq - div) : 0.0;
-                // vel_ssh.f90:63-73 and :88-98: advective fluxes through T and h faces
-                FX_c = (U_l + U_cur) * (u_r[t] + u_r[t + 1]) * rc.fx;
-                FY_c = luu ? (V_cur + V_r) * (u_r[t + 1] + u_u[t + 1]) * rc.fy : 0.0;
-                GX_c = (U_cur * rc.gx0 + U_new * rc.gx1) * (v_r[t + 1] + v_r[t + 2]);
-                GY_c = (V_prev * rc.gy0 + V_cur * rc.gy1) * (fld(sm, R_V)[t + 1] + v_r[t + 1]);
-                // depth on the h point, depth.f90:141-147
-                const double a0 = h_r[t + 1] + e_r[t + 1], a1 = h_r[t + 2] + e_r[t + 2];
-                const double b0 = h_u[t + 1] + e_u[t + 1], b1 = h_u[t + 2] + e_u[t + 2];
-                const double s0 = (lc ? a0 : 0.0) + (lr ? a1 : 0.0);
-                const double s1 = (lu_ ? b0 : 0.0) + (lur ? b1 : 0.0);
-                const int nl = lc + lr + lu_ + lur;
-                const double rl = nl == 4 ? 0.25 : (nl == 3 ? 1.0 / 3.0 : (nl == 2 ? 0.5 : (nl == 1 ? 1.0 : 0.0)));
-                const double hh = (s0 * rc.wh0 + s1 * rc.wh1) * rl;
-                // vel_ssh.f90:35-37 metric vorticity (zero on uniform grids) + Coriolis
-                double vort = 0.0;
-                if (!p.vort_zero && luu)
-                    vort = (v_r[t + 2] - v_r[t + 1]) * rc.vt0 - u_u[t + 1] * rc.vt1 + u_r[t + 1] * rc.vt2;
-                const double Wh = hh * (rc.cor + vort);
-                QU_c = Wh * (v_r[t + 1] + v_r[t + 2]);
-                QV_c = Wh * (u_r[t + 1] + u_u[t + 1]);
-                // mixing.f90:134-148 stresses from the previous level
-                const double str_t =
-                    lc ? rc.t1 * (up_r[t + 1] - up_r[t]) - (rc.t2 * vp_r[t + 1] - rc.t3 * fld(sm, R_VP)[t + 1])
-                       : 0.0;
-                const double str_s =
-                    luu ? rc.s1 * fld(su_, R_UP)[t + 1] - rc.s2 * up_r[t + 1] + rc.s3 * (vp_r[t + 2] - vp_r[t + 1])
-                        : 0.0;
-                double mu_t = p.mu0, mu_h = p.mu0;
+                const uint32_t mr = (mk >> 6) & 7u, mu_ = (mk >> 3) & 7u;   // rows rho, rho+1
+                const int sr = s_m1, sm = s_m2, su = s_0;
+                const double2 u_r = pair(sr, R_U), u_u = pair(su, R_U), v_r = pair(sr, R_V);
+                const double2 v_m = pair(sm, R_V), up_r = pair(sr, R_UP), up_u = pair(su, R_UP);
+                const double2 vp_r = pair(sr, R_VP), vp_m = pair(sm, R_VP), sp_r = pair(sr, R_SSHP);
+                const double u_l = leftv(sr, R_U), up_l = leftv(sr, R_UP);
+                const double v_rr = rightv(sr, R_V), vp_rr = rightv(sr, R_VP);
+                const double ur[3] = {u_l, u_r.x, u_r.y};           // u at k0-1, k0, k0+1
+                const double vr[3] = {v_r.x, v_r.y, v_rr};           // v at k0, k0+1, k0+2
+                const double vpr[3] = {vp_r.x, vp_r.y, vp_rr};
+                const double upr[3] = {up_l, up_r.x, up_r.y};
+                const double uu[2] = {u_u.x, u_u.y}, vm[2] = {v_m.x, v_m.y};
+                const double upu[2] = {up_u.x, up_u.y}, vpm[2] = {vp_m.x, vp_m.y};
+                const double spr[2] = {sp_r.x, sp_r.y};
+                const double Ur[3] = {Ul_c, U_c[0], U_c[1]};        // U(rho) at k0-1, k0, k0+1
+                const double Vr[3] = {V_c[0], V_c[1], Vr_c};         // V(rho) at k0, k0+1, k0+2
+                double mur[3] = {p.mu0, p.mu0, p.mu0}, muu[3] = {p.mu0, p.mu0, p.mu0}, wf[2] = {p.wq0, p.wq0};
                 if constexpr (F2D) {
-                    const double *m_r = fld(sr, R_MU), *m_u = fld(su_, R_MU);
-                    mu_t = m_r[t + 1];
-                    mu_h = (m_r[t + 1] + m_r[t + 2] + m_u[t + 1] + m_u[t + 2]) * 0.25;
+                    const double2 a = pair(sr, R_MU), b = pair(su, R_MU), w = pair(sr, R_WF);
+                    mur[0] = a.x; mur[1] = a.y; mur[2] = rightv(sr, R_MU);
+                    muu[0] = b.x; muu[1] = b.y; muu[2] = rightv(su, R_MU);
+                    wf[0] = w.x * p.inv_rho; wf[1] = w.y * p.inv_rho;
                 }
-                ST_c = mu_t * a0 * str_t;
-                SS_c = mu_h * hh * str_s;
-                xw[X_FX * W + t] = FX_c;
-                xw[X_ST * W + t] = ST_c;
-                xw[X_SSHN * W + t] = sshn_c;
-                xw[X_GX * W + t] = GX_c;
-                xw[X_QV * W + t] = QV_c;
-                xw[X_SS * W + t] = SS_c;
+                const double c_u = CF(sr, c_u), c_v0 = CF(sr, c_v0), c_v1 = CF(sr, c_v1);
+                const double fx = CF(sr, fx), fy = CF(sr, fy), gx0 = CF(sr, gx0), gx1 = CF(sr, gx1);
+                const double gy0 = CF(sr, gy0), gy1 = CF(sr, gy1), wh0 = CF(sr, wh0), wh1 = CF(sr, wh1);
+                const double t1 = CF(sr, t1), t2 = CF(sr, t2), t3 = CF(sr, t3);
+                const double s1 = CF(sr, s1), s2 = CF(sr, s2), s3 = CF(sr, s3);
+                const double cor = coef(sr)->cor;
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    const int lc = (mr >> e) & 1, lr = (mr >> (e + 1)) & 1;
+                    const int lu = (mu_ >> e) & 1, lur = (mu_ >> (e + 1)) & 1;
+                    const int luu = lc & lr & lu & lur;
+                    // vel_ssh.f90:491-494 continuity over 2*tau_inner
+                    const double div = (Ur[e + 1] - Ur[e]) * c_u + Vr[e] * c_v0 - V_p[e] * c_v1;
+                    sshn_c[e] = lc ? spr[e] + p.two_ti * (wf[e] - div) : 0.0;
+                    // vel_ssh.f90:63-73, :88-98 advective fluxes on T and h faces
+                    FX_c[e] = (Ur[e] + Ur[e + 1]) * (ur[e] + ur[e + 1]) * fx;
+                    FY_c[e] = luu ? (Vr[e] + Vr[e + 1]) * (ur[e + 1] + uu[e]) * fy : 0.0;
+                    GX_c[e] = (Ur[e + 1] * gx0 + U_n[e] * gx1) * (vr[e] + vr[e + 1]);
+                    GY_c[e] = (V_p[e] * gy0 + Vr[e] * gy1) * (vm[e] + vr[e]);
+                    // depth.f90:141-147 depth on the h point
+                    const double s0 = sel(lc, hq_m1[e]) + sel(lr, hq_m1[e + 1]);
+                    const double s1_ = sel(lu, hq_0[e]) + sel(lur, hq_0[e + 1]);
+                    const double hh = (s0 * wh0 + s1_ * wh1) * rcount(lc + lr + lu + lur);
+                    // vel_ssh.f90:35-37 metric vorticity (zero on uniform grids) + Coriolis
+                    double vort = 0.0;
+                    if (!p.vort_zero && luu)
+                        vort = (vr[e + 1] - vr[e]) * CF(sr, vt0) - uu[e] * CF(sr, vt1) + ur[e + 1] * CF(sr, vt2);
+                    const double Wh = hh * (cor + vort);
+                    QU_c[e] = Wh * (vr[e] + vr[e + 1]);
+                    QV_c[e] = Wh * (ur[e + 1] + uu[e]);
+                    // mixing.f90:134-148 stresses from the previous level
+                    const double str_t = lc ? t1 * (upr[e + 1] - upr[e]) - (t2 * vpr[e] - t3 * vpm[e]) : 0.0;
+                    const double str_s = luu ? s1 * upu[e] - s2 * upr[e + 1] + s3 * (vpr[e + 1] - vpr[e]) : 0.0;
+                    double mu_h = p.mu0;
+                    if constexpr (F2D) mu_h = (mur[e] + mur[e + 1] + muu[e] + muu[e + 1]) * 0.25;
+                    ST_c[e] = mur[e] * hq_m1[e] * str_t;
+                    SS_c[e] = mu_h * hh * str_s;
+                }
             }
+            FXr_c = SHFL_DN(FX_c[0]);
+            STr_c = SHFL_DN(ST_c[0]);
+            SNr_c = SHFL_DN(sshn_c[0]);
+            GXl_c = SHFL_UP(GX_c[1]);
+            QVl_c = SHFL_UP(QV_c[1]);
+            SSl_c = SHFL_UP(SS_c[1]);
             // ---------------- stage 3: row R = j-2 ---------------------------
-            if (j >= r0 + 2 && out_col) {
+            if (j >= r0 + 2 && (out0 || out1)) {
                 const int R = j - 2;
-                const int sR = slot_of(R), sU = slot_of(R + 1);
-                const RowCoef &rc = p.rows[R];
-                const int lc = bit(sR, c), lr = bit(sR, c + 1), lup = bit(sU, c);
-                const double *e_R = fld(sR, R_SSH), *h_R = fld(sR, R_H), *ep_R = fld(sR, R_SSHP);
-                const double ssh0 = e_R[t + 1], sshp0 = ep_R[t + 1], H0 = h_R[t + 1];
-                const double sshn0 = sshn_p;
-                const long long idx = (long long)R * p.pitch + c;
-                if (lc & lr) {   // vel_ssh.f90:536-551
-                    const double ssh1 = e_R[t + 2], sshp1 = ep_R[t + 2], H1 = h_R[t + 2];
-                    const double sshn1 = xr[X_SSHN * W + t + 1];
-                    const double u0 = fld(sR, R_U)[t + 1], up0 = fld(sR, R_UP)[t + 1];
-                    const double hu = ((H0 + ssh0) + (H1 + ssh1)) * rc.ku2;
-                    const double hup = ((H0 + sshp0) + (H1 + sshp1)) * rc.ku2;
-                    const double hun = ((H0 + sshn0) + (H1 + sshn1)) * rc.ku2;
-                    const double slx = -(ssh1 - ssh0) * rc.gdyh * hu;
-                    const double slxn = -(sshn1 - sshn0) * rc.gdyh * hun;
-                    const double adv = -((xr[X_FX * W + t + 1] - FX_p) + (FY_p - FY_pp));
-                    const double dif = (xr[X_ST * W + t + 1] - ST_p) * rc.dux + (SS_p * rc.dus0 - SS_pp * rc.dus1);
-                    double rd = p.rd0;
-                    if constexpr (F2D) rd = (fld(sR, R_RD)[t + 1] + fld(sR, R_RD)[t + 2]) * 0.5;
-                    const double grx = fld(sR, R_RX)[t + 1] * p.rhs_scale + slx + dif + adv
-                                       - rd * up0 * rc.au * hu + (QU_p + QU_pp) * 0.25;
-                    const double un = (up0 * hup + grx * p.two_ti * rc.rau) / hun;
-                    if (!(un < 100.0 && un > -100.0)) atomicOr(p.flags, FLAG_GUARD);
-                    if (p.acc_mode) {
-                        double a = (u0 * hu + un * hun) * p.c4, b = (slx + slxn) * p.c4;
-                        if (p.acc_mode == 2) { a += p.acc[0][idx]; b += p.acc[2][idx]; }
-                        p.acc[0][idx] = a;
-                        p.acc[2][idx] = b;
-                    }
-                    if (p.write_state) {
-                        p.dst[S_UP][idx] = u0 + p.gam * (un - 2.0 * u0 + up0);
-                        p.dst[S_U][idx] = un;
-                    }
+                const uint32_t mR = (mk >> 9) & 7u, mU = (mk >> 6) & 7u;   // rows R, R+1
+                const int sR = s_m2, sU = s_m1;
+                const double2 e_R = pair(sR, R_SSH), sp_R = pair(sR, R_SSHP), h_R = pair(sR, R_H);
+                const double2 e_U = pair(sU, R_SSH), sp_U = pair(sU, R_SSHP), h_U = pair(sU, R_H);
+                const double2 u_R = pair(sR, R_U), up_R = pair(sR, R_UP), v_R = pair(sR, R_V);
+                const double2 vp_R = pair(sR, R_VP), rx = pair(sR, R_RX), ry = pair(sR, R_RY);
+                const double e3[3] = {e_R.x, e_R.y, rightv(sR, R_SSH)};
+                const double sp3[3] = {sp_R.x, sp_R.y, rightv(sR, R_SSHP)};
+                const double h3[3] = {h_R.x, h_R.y, rightv(sR, R_H)};
+                const double eU[2] = {e_U.x, e_U.y}, spU[2] = {sp_U.x, sp_U.y}, hU[2] = {h_U.x, h_U.y};
+                const double u0[2] = {u_R.x, u_R.y}, up0[2] = {up_R.x, up_R.y};
+                const double v0[2] = {v_R.x, v_R.y}, vp0[2] = {vp_R.x, vp_R.y};
+                const double rxv[2] = {rx.x, rx.y}, ryv[2] = {ry.x, ry.y};
+                const double sn3[3] = {sshn_p[0], sshn_p[1], SNr_p};   // new SSH, row R
+                const double FX3[3] = {FX_p[0], FX_p[1], FXr_p};
+                const double ST3[3] = {ST_p[0], ST_p[1], STr_p};
+                const double GX3[3] = {GXl_p, GX_p[0], GX_p[1]};
+                const double QV3[3] = {QVl_p, QV_p[0], QV_p[1]};
+                const double SS3[3] = {SSl_p, SS_p[0], SS_p[1]};
+                double rd3[3] = {p.rd0, p.rd0, p.rd0}, rdU[2] = {p.rd0, p.rd0};
+                if constexpr (F2D) {
+                    const double2 a = pair(sR, R_RD), b = pair(sU, R_RD);
+                    rd3[0] = a.x; rd3[1] = a.y; rd3[2] = rightv(sR, R_RD);
+                    rdU[0] = b.x; rdU[1] = b.y;
                 }
-                if (lc & lup) {   // vel_ssh.f90:554-569
-                    const double sshU = fld(sU, R_SSH)[t + 1], sshpU = fld(sU, R_SSHP)[t + 1];
-                    const double HU = fld(sU, R_H)[t + 1];
-                    const double sshnU = sshn_c;
-                    const double v0 = fld(sR, R_V)[t + 1], vp0 = fld(sR, R_VP)[t + 1];
-                    const double hv = ((H0 + ssh0) * rc.wv0 + (HU + sshU) * rc.wv1) * 0.5;
-                    const double hvp = ((H0 + sshp0) * rc.wv0 + (HU + sshpU) * rc.wv1) * 0.5;
-                    const double hvn = ((H0 + sshn0) * rc.wv0 + (HU + sshnU) * rc.wv1) * 0.5;
-                    const double sly = -(sshU - ssh0) * rc.gdxh * hv;
-                    const double slyn = -(sshnU - sshn0) * rc.gdxh * hvn;
-                    const double adv = -((GX_p - xr[X_GX * W + t - 1]) + (GY_c - GY_p));
-                    const double dif = -(ST_c * rc.dvt1 - ST_p * rc.dvt0) + (SS_p - xr[X_SS * W + t - 1]) * rc.dvs;
-                    double rd = p.rd0;
-                    if constexpr (F2D) rd = (fld(sR, R_RD)[t + 1] + fld(sU, R_RD)[t + 1]) * 0.5;
-                    const double gry = fld(sR, R_RY)[t + 1] * p.rhs_scale + sly + dif + adv
-                                       - rd * vp0 * rc.av * hv - (QV_p + xr[X_QV * W + t - 1]) * 0.25;
-                    const double vn = (vp0 * hvp + gry * p.two_ti * rc.rav) / hvn;
-                    if (!(vn < 100.0 && vn > -100.0)) atomicOr(p.flags, FLAG_GUARD);
-                    if (p.acc_mode) {
-                        double a = (v0 * hv + vn * hvn) * p.c4, b = (sly + slyn) * p.c4;
-                        if (p.acc_mode == 2) { a += p.acc[1][idx]; b += p.acc[3][idx]; }
-                        p.acc[1][idx] = a;
-                        p.acc[3][idx] = b;
+                const double ku2 = CF(sR, ku2), wv0 = CF(sR, wv0), wv1 = CF(sR, wv1);
+                const double gdyh = CF(sR, gdyh), gdxh = CF(sR, gdxh), dux = CF(sR, dux);
+                const double dus0 = CF(sR, dus0), dus1 = CF(sR, dus1), dvt0 = CF(sR, dvt0);
+                const double dvt1 = CF(sR, dvt1), dvs = CF(sR, dvs), au = CF(sR, au), av = CF(sR, av);
+                const double cu = p.two_ti * CF(sR, rau), cv = p.two_ti * CF(sR, rav);
+                const long long rowb = (long long)R * p.pitch + k0;
+#pragma unroll
+                for (int e = 0; e < 2; e++) {
+                    if (!(e == 0 ? out0 : out1)) continue;
+                    const int lc = (mR >> e) & 1, lr = (mR >> (e + 1)) & 1, lup = (mU >> e) & 1;
+                    const long long idx = rowb + e;
+                    if (lc & lr) {   // vel_ssh.f90:536-551
+                        const double hu = hu_w[0][e];
+                        const double hup = ((h3[e] + sp3[e]) + (h3[e + 1] + sp3[e + 1])) * ku2;
+                        const double hun = ((h3[e] + sn3[e]) + (h3[e + 1] + sn3[e + 1])) * ku2;
+                        const double slx = -(e3[e + 1] - e3[e]) * gdyh * hu;
+                        const double slxn = -(sn3[e + 1] - sn3[e]) * gdyh * hun;
+                        const double adv = -((FX3[e + 1] - FX3[e]) + (FY_p[e] - FY_pp[e]));
+                        const double dif = (ST3[e + 1] - ST3[e]) * dux + (SS_p[e] * dus0 - SS_pp[e] * dus1);
+                        const double rd = F2D ? (rd3[e] + rd3[e + 1]) * 0.5 : p.rd0;
+                        const double grx = rxv[e] * p.rhs_scale + slx + dif + adv - rd * up0[e] * au * hu
+                                           + (QU_p[e] + QU_pp[e]) * 0.25;
+                        const double un = (up0[e] * hup + grx * cu) / hun;
+                        if (!(un < 100.0 && un > -100.0)) atomicOr(p.flags, FLAG_GUARD);
+                        if (p.acc_mode) {
+                            double a = (u0[e] * hu + un * hun) * p.c4, b = (slx + slxn) * p.c4;
+                            if (p.acc_mode == 2) { a += p.acc[0][idx]; b += p.acc[2][idx]; }
+                            p.acc[0][idx] = a;
+                            p.acc[2][idx] = b;
+                        }
+                        if (p.write_state) {
+                            p.dst[S_UP][idx] = u0[e] + p.gam * (un - 2.0 * u0[e] + up0[e]);
+                            p.dst[S_U][idx] = un;
+                        }
                     }
-                    if (p.write_state) {
-                        p.dst[S_VP][idx] = v0 + p.gam * (vn - 2.0 * v0 + vp0);
-                        p.dst[S_V][idx] = vn;
+                    if (lc & lup) {   // vel_ssh.f90:554-569
+                        const double hv = hv_w[0][e];
+                        const double hvp = ((h3[e] + sp3[e]) * wv0 + (hU[e] + spU[e]) * wv1) * 0.5;
+                        const double hvn = ((h3[e] + sn3[e]) * wv0 + (hU[e] + sshn_c[e]) * wv1) * 0.5;
+                        const double sly = -(eU[e] - e3[e]) * gdxh * hv;
+                        const double slyn = -(sshn_c[e] - sn3[e]) * gdxh * hvn;
+                        const double adv = -((GX3[e + 1] - GX3[e]) + (GY_c[e] - GY_p[e]));
+                        const double dif = -(ST_c[e] * dvt1 - ST3[e] * dvt0) + (SS3[e + 1] - SS3[e]) * dvs;
+                        const double rd = F2D ? (rd3[e] + rdU[e]) * 0.5 : p.rd0;
+                        const double gry = ryv[e] * p.rhs_scale + sly + dif + adv - rd * vp0[e] * av * hv
+                                           - (QV3[e + 1] + QV3[e]) * 0.25;
+                        const double vn = (vp0[e] * hvp + gry * cv) / hvn;
+                        if (!(vn < 100.0 && vn > -100.0)) atomicOr(p.flags, FLAG_GUARD);
+                        if (p.acc_mode) {
+                            double a = (v0[e] * hv + vn * hvn) * p.c4, b = (sly + slyn) * p.c4;
+                            if (p.acc_mode == 2) { a += p.acc[1][idx]; b += p.acc[3][idx]; }
+                            p.acc[1][idx] = a;
+                            p.acc[3][idx] = b;
+                        }
+                        if (p.write_state) {
+                            p.dst[S_VP][idx] = v0[e] + p.gam * (vn - 2.0 * v0[e] + vp0[e]);
+                            p.dst[S_V][idx] = vn;
+                        }
                     }
-                }
-                if (lc) {   // vel_ssh.f90:593-596
-                    if (!(sshn0 < 10.0 && sshn0 > -10.0)) atomicOr(p.flags, FLAG_GUARD);
-                    if (p.write_state) {
-                        p.dst[S_SSHP][idx] = ssh0 + p.gam * (sshn0 - 2.0 * ssh0 + sshp0);
-                        p.dst[S_SSH][idx] = sshn0;
+                    if (lc) {   // vel_ssh.f90:593-596
+                        if (!(sn3[e] < 10.0 && sn3[e] > -10.0)) atomicOr(p.flags, FLAG_GUARD);
+                        if (p.write_state) {
+                            p.dst[S_SSHP][idx] = e3[e] + p.gam * (sn3[e] - 2.0 * e3[e] + sp3[e]);
+                            p.dst[S_SSH][idx] = sn3[e];
+                        }
                     }
                 }
             }
         }
-        // rotate the register pipelines
-        V_prev = V_cur;
-        V_cur = V_new;
-        U_cur = U_new;
-        FY_pp = FY_p; FY_p = FY_c;
-        QU_pp = QU_p; QU_p = QU_c;
-        SS_pp = SS_p; SS_p = SS_c;
-        sshn_p = sshn_c; GY_p = GY_c; ST_p = ST_c; FX_p = FX_c; GX_p = GX_c; QV_p = QV_c;
-
-        if (__syncthreads_or(!ok)) { abort = true; break; }
-        if (t == 0) {
-            const int dead = j - 2;   // last use of row j-2 was stage 3 above
-            if (dead >= row_lo && dead + RING <= row_hi) issue(dead + RING), issued = dead + RING;
+        // ---- rotate the register pipelines and the ring ---------------------
+#pragma unroll
+        for (int e = 0; e < 2; e++) {
+            V_p[e] = V_c[e]; V_c[e] = V_n[e]; U_c[e] = U_n[e];
+            hu_w[0][e] = hu_w[1][e]; hu_w[1][e] = hu_n[e];
+            hv_w[0][e] = hv_w[1][e]; hv_w[1][e] = hv_n[e];
+            FY_pp[e] = FY_p[e]; FY_p[e] = FY_c[e];
+            QU_pp[e] = QU_p[e]; QU_p[e] = QU_c[e];
+            SS_pp[e] = SS_p[e]; SS_p[e] = SS_c[e];
+            sshn_p[e] = sshn_c[e]; GY_p[e] = GY_c[e]; ST_p[e] = ST_c[e];
+            FX_p[e] = FX_c[e]; GX_p[e] = GX_c[e]; QV_p[e] = QV_c[e];
+        }
+#pragma unroll
+        for (int e = 0; e < 3; e++) { hq_m1[e] = hq_0[e]; hq_0[e] = hq_p1[e]; }
+        Ul_c = Ul_n; Vr_c = Vr_n;
+        FXr_p = FXr_c; STr_p = STr_c; SNr_p = SNr_c; GXl_p = GXl_c; QVl_p = QVl_c; SSl_p = SSl_c;
+        s_m2 = s_m1;
+        s_m1 = s_0;
+        s_0 = s_p1;
+        s_p1 = s_p1 + 1 == RING ? 0 : s_p1 + 1;
+        if (__any_sync(0xffffffffu, !ok)) { abort = true; break; }
+        // row j-2 was last read by stage 3 above: once every lane is past it
+        // its slot takes row j-2+RING
+        __syncwarp();
+        if (l == 0) {
+            const int dead = j - 2;
+            if (dead >= row_lo && dead + RING <= row_hi) {
+                issue(dead + RING, (dead - row_lo) % RING);
+                issued = dead + RING;
+            }
         }
     }
-    if (abort && t == 0) {
+#undef CF
+    if (abort && l == 0) {
         atomicOr(p.flags, FLAG_TIMEOUT);
         // drain this CTA's copies still in flight (bounded) before exiting
         for (int row = max(waited + 1, row_lo); row <= issued; row++)
-            (void)mbar_wait(&mbar[slot_of(row)], (uint32_t)(((row - row_lo) / RING) & 1));
+            (void)mbar_wait(&mbar[(row - row_lo) % RING], (uint32_t)(((row - row_lo) / RING) & 1));
     }
 }
 
-// min/max over [m0,m1]x[n0,n1] of three fields, for the uniform-forcing test
-__global__ void k_minmax3(Dom D, const float *lu, const double *a, const double *b, const double *c3,
-                          double *out)
+// min/max over the ocean points of three fields, for the uniform-forcing test
+__global__ void k_minmax3(Dom D, const float *lu, const double *a, const double *b, const double *c3, double *out)
 {
     __shared__ double sh[6][256];
     double mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY};
@@ -416,7 +511,7 @@ __global__ void k_minmax3(Dom D, const float *lu, const double *a, const double 
     }
 }
 
-constexpr int MINMAX_BLOCKS = 64;
+constexpr int MINMAX_BLOCKS = 592;
 
 struct Forcing {
     bool uniform;
@@ -441,6 +536,7 @@ int forcing_mode(Plan &p, const Dom &d, const Consts &c, double *forc[6], cudaSt
             mx[q] = std::max(mx[q], y);
         }
     f.uniform = !nan && mn[0] == mx[0] && mn[1] == mx[1] && mn[2] == mx[2];
+    if (mn[0] > mx[0]) mn[0] = mn[1] = mn[2] = 0.0;   // no ocean at all
     f.mu0 = mn[0];
     f.rd0 = mn[1];
     f.wq0 = mn[2] / c.rho * (double)c.ffs;
@@ -458,13 +554,14 @@ Params base_params(const Plan &p, const Dom &d, const Consts &c, double *forc[6]
     q.rdis = forc[5];
     q.bits = p.bits;
     q.rows = p.rows;
+    q.rc = p.rc;
     q.pitch = d.pitch;
     q.bm_words = p.bm_words;
     q.chunk_rows = p.chunk_rows;
     q.r_first = d.ny_start - d.bnd_y1;
     q.r_last = d.ny_end - d.bnd_y1;
-    q.c_first = d.nx_start - d.bnd_x1;
-    q.c_last = d.nx_end - d.bnd_x1;
+    q.c_first = d.nx_start - d.bnd_x1 + d.xoff;
+    q.c_last = d.nx_end - d.bnd_x1 + d.xoff;
     q.mu0 = f.mu0;
     q.rd0 = f.rd0;
     q.wq0 = f.wq0;
@@ -475,13 +572,20 @@ Params base_params(const Plan &p, const Dom &d, const Consts &c, double *forc[6]
     return q;
 }
 
-void launch(const Plan &p, const Params &q, bool f2d, cudaStream_t s)
+template <bool F2D, bool RV>
+void launch_t(const Plan &p, const Params &q, cudaStream_t s)
 {
     dim3 grid(p.nstrips, p.nchunks);
-    if (f2d)
-        k_substep<true><<<grid, W, Smem<true>::total, s>>>(q);
-    else
-        k_substep<false><<<grid, W, Smem<false>::total, s>>>(q);
+    k_substep<F2D, RV><<<grid, NL, Layout<F2D>::bytes, s>>>(q);
+}
+
+void launch(const Plan &p, const Params &q, bool f2d, cudaStream_t s)
+{
+    if (f2d) {
+        if (p.rowvar) launch_t<true, true>(p, q, s); else launch_t<true, false>(p, q, s);
+    } else {
+        if (p.rowvar) launch_t<false, true>(p, q, s); else launch_t<false, false>(p, q, s);
+    }
 }
 
 int sync_buffers(Plan &p, const Dom &d, double *state[6], cudaStream_t s)
@@ -504,18 +608,25 @@ int read_flags(Plan &p, cudaStream_t s, unsigned *out)
     return 0;
 }
 
+template <bool F2D, bool RV>
+int set_smem()
+{
+    return cudaFuncSetAttribute(k_substep<F2D, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)Layout<F2D>::bytes) != cudaSuccess;
+}
+
 }  // namespace
 
 // ===========================================================================
 Plan make_plan(const inmsom_bounds &b)
 {
     Plan p;
-    p.W = W;
-    p.outw = W - 2;
+    p.ncol = NCOL;
+    p.outw = OUTW;
     const int nx = b.nx_end - b.nx_start + 1;
     p.nstrips = (nx + p.outw - 1) / p.outw;
-    const long long cs_last = 1 + (long long)(p.nstrips - 1) * p.outw;
-    p.min_pitch = cs_last + W + 1;
+    const long long g0_last = (long long)(p.nstrips - 1) * p.outw;
+    p.min_pitch = g0_last + SEG;
     return p;
 }
 
@@ -528,6 +639,7 @@ const char *check_eligible(const Plan &p, const Dom &d, const Consts &c, const f
         return "array bounds are not the interior plus a 2-point halo";
     if (d.px || d.py) return "periodic wrap";
     if (c.ffs != 1) return "full_free_surface != 1";
+    if (d.xoff != XOFF) return "device layout without the fused column offset";
     const int nxa = d.nxa(), nya = d.nya();
     auto at = [&](const float *a, int m, int n) { return a[(size_t)(n - d.bnd_y1) * nxa + (m - d.bnd_x1)]; };
     const float *lu = masks[0];
@@ -573,7 +685,6 @@ const char *check_eligible(const Plan &p, const Dom &d, const Consts &c, const f
 int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], const double *const grid[10],
           const double *d_hrest, const float *d_lu, cudaStream_t s)
 {
-    (void)c;
     const int nxa = d.nxa(), nya = d.nya();
     auto row_of = [&](int k, int n) {
         n = std::min(std::max(n, d.ny_start - 1), d.ny_end + 1);
@@ -586,6 +697,7 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
         const int n = r + d.bnd_y1;
         auto g = [&](int k, int dn) { return row_of(k, n + dn); };
         RowCoef &q = rows[r];
+        q = RowCoef{};
         const double area = g(DX, 0) * g(DY, 0), area1 = g(DX, 1) * g(DY, 1);
         q.ku = area / (g(DXT, 0) * g(DYH, 0));
         q.ku2 = 0.5 * q.ku;
@@ -627,14 +739,26 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
         q.rav = 1.0 / q.av;
     }
     p.vort_zero = vz;
-    // 1-bit T mask, rows padded so that every CTA window (8 words from a
-    // 4-word boundary) is inside the row
+    // rows identical except for cor -> the coefficients go in the kernel
+    // parameters and only cor is read per row
+    p.rowvar = false;
+    for (int r = 1; r < nya && !p.rowvar; r++) {
+        RowCoef a = rows[r], b = rows[0];
+        a.cor = b.cor = 0.0;
+        p.rowvar = std::memcmp(&a, &b, sizeof(RowCoef)) != 0;
+    }
+    p.rc = rows[d.ny_start - d.bnd_y1];
+    // 1-bit T mask indexed by device column, rows padded so that every CTA
+    // window (8 words from a 4-word boundary) lies inside the row
     p.bm_words = (int)(((d.pitch + 31) / 32 + 8 + 3) / 4 * 4);
     std::vector<uint32_t> bits((size_t)p.bm_words * nya, 0u);
     const float *lu = masks[0];
     for (int r = 0; r < nya; r++)
         for (int col = 0; col < nxa; col++)
-            if (lu[(size_t)r * nxa + col] > 0.5f) bits[(size_t)r * p.bm_words + col / 32] |= 1u << (col % 32);
+            if (lu[(size_t)r * nxa + col] > 0.5f) {
+                const int dc = col + d.xoff;
+                bits[(size_t)r * p.bm_words + dc / 32] |= 1u << (dc % 32);
+            }
 
     if (cudaMalloc(&p.rows, rows.size() * sizeof(RowCoef)) != cudaSuccess) return 1;
     if (cudaMemcpyAsync(p.rows, rows.data(), rows.size() * sizeof(RowCoef), cudaMemcpyHostToDevice, s) != cudaSuccess)
@@ -654,26 +778,21 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
     p.hrest = d_hrest;
     p.lu = d_lu;
     p.buffers_synced = false;
-
-    if (cudaFuncSetAttribute(k_substep<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)Smem<false>::total) != cudaSuccess)
-        return 1;
-    if (cudaFuncSetAttribute(k_substep<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                             (int)Smem<true>::total) != cudaSuccess)
+    if (set_smem<false, false>() || set_smem<false, true>() || set_smem<true, false>() || set_smem<true, true>())
         return 1;
     int dev = 0, nsm = 148, occ = 1;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_substep<false>, W, Smem<false>::total) != cudaSuccess ||
-        occ < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_substep<false, false>, NL,
+                                                      Layout<false>::bytes) != cudaSuccess || occ < 1)
         occ = 1;
     p.nsm = nsm;
-    // one wave: strips x chunks <= SMs x resident CTAs, chunks as tall as that allows
+    // one wave: strips x chunks <= SMs x resident CTAs, chunks as tall as
+    // that allows; each chunk re-reads and recomputes three rows of warm-up,
+    // so keep chunks at least 16 rows tall
     const int ny = d.ny_end - d.ny_start + 1;
     const int slots = nsm * occ;
     int nchunks = std::max(1, slots / p.nstrips);
-    // each chunk re-reads and recomputes three rows of warm-up: keep chunks
-    // at least 16 rows tall
     nchunks = std::min(nchunks, std::max(1, (ny + 15) / 16));
     p.chunk_rows = (ny + nchunks - 1) / nchunks;
     p.nchunks = (ny + p.chunk_rows - 1) / p.chunk_rows;

@@ -27,7 +27,10 @@
 namespace inmsom {
 namespace fused {
 
-// per-row coefficients, row index = device row (n - bnd_y1)
+constexpr int XOFF = 1;   // device padding columns before bnd_x1 (see common.cuh)
+
+// per-row coefficients, row index = device row (n - bnd_y1); 38 doubles so
+// that a row is a whole number of 16-byte units for the bulk copies
 struct RowCoef {
     double ku, ku2;           // hu: area(n)/(dxt*dyh)(n), and half of it
     double wv0, wv1;          // hv: area(n)/(dxh*dyt)(n), area(n+1)/(dxh*dyt)(n)
@@ -45,12 +48,16 @@ struct RowCoef {
     double gdyh, gdxh;        // g*dyh, g*dxh
     double au, av;            // dxt*dyh, dyt*dxh
     double rau, rav;          // 1/(dxt*dyh), 1/(dyt*dxh)
+    double pad;
 };
+static_assert(sizeof(RowCoef) % 16 == 0, "RowCoef must be a multiple of 16 bytes");
 
 struct Plan {
-    int W = 128;              // threads (columns) per CTA
-    int outw = 126;           // output columns per CTA
+    int ncol = 64;            // columns per CTA (one warp, two columns per lane)
+    int outw = 62;            // output columns per CTA
     int nstrips = 0, nchunks = 0, chunk_rows = 0;
+    bool rowvar = true;       // coefficients vary along y (else all rows but cor equal)
+    RowCoef rc{};             // the row-invariant coefficients when !rowvar
     long long min_pitch = 0;  // device row pitch the strips need
     // device data
     RowCoef *rows = nullptr;
