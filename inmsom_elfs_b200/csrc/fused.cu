@@ -10,12 +10,16 @@
 //   stage 2, row j-1 : new SSH (continuity), advective fluxes on T and h
 //                      points, Coriolis-plus-metric-vorticity products,
 //                      tension and shear stresses times viscosity and depth;
-//   stage 3, row j-2 : u and v momentum, time-mean sums, Robert-Asselin
-//                      filter and time shift, stores.
+//   stage 3u, row j-1: u momentum, SSH update, their time-mean sums,
+//                      Robert-Asselin filter and time shift, stores;
+//   stage 3v, row j-2: the same for v (it needs stage 2 of the row above).
 // A value a stage needs from the neighbouring column is the other column
 // of the same lane or comes from the neighbouring lane by a warp shuffle;
-// values of earlier rows of the same column stay in registers.  There is no
-// CTA-wide barrier.
+// values of earlier rows of the same column stay in registers, in three
+// instances of each per-row struct that the three-fold unrolled row loop
+// renames instead of copying.  There is no CTA-wide barrier, and the
+// per-column work is branch-free (predicated stores) except for warp-wide
+// skips of rows without ocean.
 //
 // Input rows j-2..j+1 of the input fields (a 68-column segment per field
 // and row, 16-byte aligned), the row's coefficients and the row's T-mask
@@ -135,6 +139,33 @@ __device__ __forceinline__ double rcount(int n)
 #define SHFL_UP(x) __shfl_up_sync(0xffffffffu, (x), 1)
 #define SHFL_DN(x) __shfl_down_sync(0xffffffffu, (x), 1)
 
+// 1/x by two Newton-Raphson steps r <- r + r*(1 - x*r) (quadratic
+// convergence) from the single-precision reciprocal: about 1 ulp of double
+// for a positive normal x inside the float range, such as a water depth.
+__device__ __forceinline__ double rcp_nr(double x)
+{
+    double r = (double)__frcp_rn((float)x);
+    double e = fma(-x, r, 1.0);
+    r = fma(r, e, r);
+    e = fma(-x, r, 1.0);
+    return fma(r, e, r);
+}
+
+// per-row values carried between the stages of the row pipeline
+struct S1 {          // stage 1 of a row: transports and current-level depths
+    double U0, U1, V0, V1;   // U = u*hu at k0, k0+1; V = v*hv
+    double Ul, Vr;           // U(k0-1), V(k0+2) from the neighbouring lanes
+    double hu0, hu1, hv0, hv1;
+};
+struct HQ {          // H + ssh of a row at k0, k0+1, k0+2
+    double a, b, c;
+};
+struct S2 {          // stage 2 of a row
+    double sn0, sn1;         // new SSH
+    double FY0, FY1, QU0, QU1, SS0, SS1;
+    double GX0, GX1, GXl, GY0, GY1, QV0, QV1, QVl, ST0, ST1, SSl;
+};
+
 template <bool F2D, bool ROWVAR>
 __global__ void __launch_bounds__(NL, CTAS_PER_SM) k_substep(const __grid_constant__ Params p)
 {
@@ -155,7 +186,9 @@ __global__ void __launch_bounds__(NL, CTAS_PER_SM) k_substep(const __grid_consta
     const int po = 2 * l + 2;                               // segment offset of k0
 
     auto slotp = [&](int s) { return smem + (size_t)s * L::SLOT_D; };
-    auto issue = [&](int row, int s) {
+    auto slot_of = [&](int row) { return (row - row_lo) % RING; };
+    auto issue = [&](int row) {
+        const int s = slot_of(row);
         double *d = slotp(s);
         uint64_t *bar = &mbar[s];
         mbar_expect_tx(bar, L::row_tx);
@@ -198,285 +231,320 @@ __global__ void __launch_bounds__(NL, CTAS_PER_SM) k_substep(const __grid_consta
     __syncwarp();
     int issued = row_lo - 1;
     if (l == 0)
-        for (int row = row_lo; row < row_lo + RING && row <= row_hi; row++) issue(row, row - row_lo), issued = row;
+        for (int row = row_lo; row < row_lo + RING && row <= row_hi; row++) issue(row), issued = row;
 
     const bool out0 = l >= 1 && k0 >= p.c_first && k0 <= p.c_last;
     const bool out1 = l <= NL - 2 && k0 + 1 >= p.c_first && k0 + 1 <= p.c_last;
+    const double gam = p.gam, two_ti = p.two_ti, rs = p.rhs_scale;
 
-    // ring slots of rows j-2, j-1, j, j+1: the slot of row r is (r - row_lo) % RING;
-    // for j = r0-1 these are rows r0-3 (none), r0-2, r0-1, r0
-    int s_m2 = RING - 1, s_m1 = 0, s_0 = 1, s_p1 = 2;
     // T-mask bits, 3 per row: row j+1 in bits 0-2, j in 3-5, j-1 in 6-8, j-2 in 9-11
     uint32_t mk = 0;
-    // stage-1 windows (two columns each)
-    double hq_m1[3] = {0, 0, 0}, hq_0[3] = {0, 0, 0};      // H+ssh at k0, k0+1, k0+2, rows j-1, j
-    double U_c[2] = {0, 0}, V_c[2] = {0, 0}, V_p[2] = {0, 0};   // U(j-1), V(j-1), V(j-2)
-    double Ul_c = 0, Vr_c = 0;                             // U(k0-1, j-1), V(k0+2, j-1)
-    double hu_w[2][2] = {{0, 0}, {0, 0}}, hv_w[2][2] = {{0, 0}, {0, 0}};   // rows j-2, j-1
-    // stage-2 results: _p row R, _pp row R-1 (own columns) and row-R neighbours
-    double sshn_p[2] = {0, 0}, FX_p[2] = {0, 0}, GX_p[2] = {0, 0}, QV_p[2] = {0, 0};
-    double ST_p[2] = {0, 0}, SS_p[2] = {0, 0}, SS_pp[2] = {0, 0}, FY_p[2] = {0, 0};
-    double FY_pp[2] = {0, 0}, QU_p[2] = {0, 0}, QU_pp[2] = {0, 0}, GY_p[2] = {0, 0};
-    double FXr_p = 0, STr_p = 0, SNr_p = 0, GXl_p = 0, QVl_p = 0, SSl_p = 0;
-
+    uint32_t bad = 0;   // guard: a new value out of range or NaN
     int waited = row_lo - 1;
-    bool abort = false;
-    for (int j = r0 - 1; j <= r1 + 1; j++) {
+    bool ok = true;
+
+    // One row step of the pipeline, for iteration j (see the file comment):
+    //   stage 1 row j      -> s1n (and H+ssh of row j+1 -> hqn)
+    //   stage 2 row j-1    -> s2n, from s1c = S1(j-1), s1p = S1(j-2), s1n,
+    //                         hqp = H+ssh(j-1), hqc = H+ssh(j)
+    //   stage 3u row j-1   u momentum and the SSH update, from s2n, s2o
+    //   stage 3v row j-2   v momentum, from s2o = S2(j-2), s2n, s1p
+    auto step = [&](const int j, S1 &s1n, const S1 &s1c, const S1 &s1p, HQ &hqn, const HQ &hqc,
+                    const HQ &hqp, S2 &s2n, const S2 &s2o) {
         // --- rows up to j+1 must have landed ------------------------------
         const int need = min(j + 1, row_hi);
-        bool ok = true;
-        while (waited < need) {
+        while (waited < need && ok) {
             const int row = waited + 1;
             const uint32_t par = (uint32_t)(((row - row_lo) / RING) & 1);
-            if (!mbar_wait(&mbar[(row - row_lo) % RING], par)) { ok = false; break; }
+            if (!mbar_wait(&mbar[slot_of(row)], par)) { ok = false; break; }
             waited = row;
-            mk = (mk << 3) | mask3((row - row_lo) % RING);
+            mk = (mk << 3) | mask3(slot_of(row));
         }
         if (j + 1 > row_hi) mk <<= 3;   // keep the row alignment of mk
-        ok = __all_sync(0xffffffffu, ok);   // the shuffles below need every lane
+        ok = __all_sync(0xffffffffu, ok);
+        if (!ok) return;
+        const int s_m2 = slot_of(j - 2), s_m1 = slot_of(j - 1), s_0 = slot_of(j), s_p1 = slot_of(j + 1);
 
-        double U_n[2] = {0, 0}, V_n[2] = {0, 0}, Ul_n = 0, Vr_n = 0, hu_n[2] = {0, 0}, hv_n[2] = {0, 0};
-        double hq_p1[3] = {0, 0, 0};
-        double sshn_c[2] = {0, 0}, FX_c[2] = {0, 0}, GX_c[2] = {0, 0}, QV_c[2] = {0, 0};
-        double ST_c[2] = {0, 0}, SS_c[2] = {0, 0}, FY_c[2] = {0, 0}, QU_c[2] = {0, 0}, GY_c[2] = {0, 0};
-        double FXr_c = 0, STr_c = 0, SNr_c = 0, GXl_c = 0, QVl_c = 0, SSl_c = 0;
-        if (ok) {
-            // ---------------- stage 1: row j ---------------------------------
-            if (j <= r1) {
-                const uint32_t mj = (mk >> 3) & 7u, mn = mk & 7u;
-                {   // H + ssh of row j+1 at k0, k0+1, k0+2
-                    const double2 h = pair(s_p1, R_H), e = pair(s_p1, R_SSH);
-                    hq_p1[0] = h.x + e.x;
-                    hq_p1[1] = h.y + e.y;
-                    hq_p1[2] = rightv(s_p1, R_H) + rightv(s_p1, R_SSH);
-                }
-                if (j == r0 - 1) {   // first iteration: row j itself
-                    const double2 h = pair(s_0, R_H), e = pair(s_0, R_SSH);
-                    hq_0[0] = h.x + e.x;
-                    hq_0[1] = h.y + e.y;
-                    hq_0[2] = rightv(s_0, R_H) + rightv(s_0, R_SSH);
-                }
-                const double ku = CF(s_0, ku), ku2 = CF(s_0, ku2), wv0 = CF(s_0, wv0), wv1 = CF(s_0, wv1);
-                const double2 u = pair(s_0, R_U), v = pair(s_0, R_V);
-#pragma unroll
-                for (int e = 0; e < 2; e++) {
-                    // Function/depth.f90:127-139 mask-weighted averages to u and v points
-                    const int a = (mj >> e) & 1, b = (mj >> (e + 1)) & 1, c = (mn >> e) & 1;
-                    hu_n[e] = (sel(a, hq_0[e]) + sel(b, hq_0[e + 1])) * (a & b ? ku2 : (a | b ? ku : 0.0));
-                    hv_n[e] = (sel(a, hq_0[e] * wv0) + sel(c, hq_p1[e] * wv1)) * (a & c ? 0.5 : (a | c ? 1.0 : 0.0));
-                }
-                U_n[0] = u.x * hu_n[0];
-                U_n[1] = u.y * hu_n[1];
-                V_n[0] = v.x * hv_n[0];
-                V_n[1] = v.y * hv_n[1];
+        // ---------------- stage 1: row j ---------------------------------
+        if (j <= r1) {
+            const uint32_t mj = (mk >> 3) & 7u, mn = mk & 7u;
+            {   // H + ssh of row j+1 at k0, k0+1, k0+2
+                const double2 h = pair(s_p1, R_H), e = pair(s_p1, R_SSH);
+                hqn.a = h.x + e.x;
+                hqn.b = h.y + e.y;
+                hqn.c = rightv(s_p1, R_H) + rightv(s_p1, R_SSH);
             }
-            Ul_n = SHFL_UP(U_n[1]);
-            Vr_n = SHFL_DN(V_n[0]);
-            // ---------------- stage 2: row rho = j-1 -------------------------
-            if (j >= r0) {
-                const uint32_t mr = (mk >> 6) & 7u, mu_ = (mk >> 3) & 7u;   // rows rho, rho+1
-                const int sr = s_m1, sm = s_m2, su = s_0;
-                const double2 u_r = pair(sr, R_U), u_u = pair(su, R_U), v_r = pair(sr, R_V);
-                const double2 v_m = pair(sm, R_V), up_r = pair(sr, R_UP), up_u = pair(su, R_UP);
-                const double2 vp_r = pair(sr, R_VP), vp_m = pair(sm, R_VP), sp_r = pair(sr, R_SSHP);
-                const double u_l = leftv(sr, R_U), up_l = leftv(sr, R_UP);
-                const double v_rr = rightv(sr, R_V), vp_rr = rightv(sr, R_VP);
-                const double ur[3] = {u_l, u_r.x, u_r.y};           // u at k0-1, k0, k0+1
-                const double vr[3] = {v_r.x, v_r.y, v_rr};           // v at k0, k0+1, k0+2
-                const double vpr[3] = {vp_r.x, vp_r.y, vp_rr};
-                const double upr[3] = {up_l, up_r.x, up_r.y};
-                const double uu[2] = {u_u.x, u_u.y}, vm[2] = {v_m.x, v_m.y};
-                const double upu[2] = {up_u.x, up_u.y}, vpm[2] = {vp_m.x, vp_m.y};
-                const double spr[2] = {sp_r.x, sp_r.y};
-                const double Ur[3] = {Ul_c, U_c[0], U_c[1]};        // U(rho) at k0-1, k0, k0+1
-                const double Vr[3] = {V_c[0], V_c[1], Vr_c};         // V(rho) at k0, k0+1, k0+2
-                double mur[3] = {p.mu0, p.mu0, p.mu0}, muu[3] = {p.mu0, p.mu0, p.mu0}, wf[2] = {p.wq0, p.wq0};
-                if constexpr (F2D) {
-                    const double2 a = pair(sr, R_MU), b = pair(su, R_MU), w = pair(sr, R_WF);
-                    mur[0] = a.x; mur[1] = a.y; mur[2] = rightv(sr, R_MU);
-                    muu[0] = b.x; muu[1] = b.y; muu[2] = rightv(su, R_MU);
-                    wf[0] = w.x * p.inv_rho; wf[1] = w.y * p.inv_rho;
-                }
-                const double c_u = CF(sr, c_u), c_v0 = CF(sr, c_v0), c_v1 = CF(sr, c_v1);
-                const double fx = CF(sr, fx), fy = CF(sr, fy), gx0 = CF(sr, gx0), gx1 = CF(sr, gx1);
-                const double gy0 = CF(sr, gy0), gy1 = CF(sr, gy1), wh0 = CF(sr, wh0), wh1 = CF(sr, wh1);
-                const double t1 = CF(sr, t1), t2 = CF(sr, t2), t3 = CF(sr, t3);
-                const double s1 = CF(sr, s1), s2 = CF(sr, s2), s3 = CF(sr, s3);
-                const double cor = coef(sr)->cor;
+            const double ku = CF(s_0, ku), ku2 = CF(s_0, ku2), wv0 = CF(s_0, wv0), wv1 = CF(s_0, wv1);
+            const double2 u = pair(s_0, R_U), v = pair(s_0, R_V);
+            const double hq0[3] = {hqc.a, hqc.b, hqc.c}, hq1[2] = {hqn.a, hqn.b};
+            double hu[2], hv[2];
 #pragma unroll
-                for (int e = 0; e < 2; e++) {
-                    const int lc = (mr >> e) & 1, lr = (mr >> (e + 1)) & 1;
-                    const int lu = (mu_ >> e) & 1, lur = (mu_ >> (e + 1)) & 1;
-                    const int luu = lc & lr & lu & lur;
-                    // vel_ssh.f90:491-494 continuity over 2*tau_inner
-                    const double div = (Ur[e + 1] - Ur[e]) * c_u + Vr[e] * c_v0 - V_p[e] * c_v1;
-                    sshn_c[e] = lc ? spr[e] + p.two_ti * (wf[e] - div) : 0.0;
-                    // vel_ssh.f90:63-73, :88-98 advective fluxes on T and h faces
-                    FX_c[e] = (Ur[e] + Ur[e + 1]) * (ur[e] + ur[e + 1]) * fx;
-                    FY_c[e] = luu ? (Vr[e] + Vr[e + 1]) * (ur[e + 1] + uu[e]) * fy : 0.0;
-                    GX_c[e] = (Ur[e + 1] * gx0 + U_n[e] * gx1) * (vr[e] + vr[e + 1]);
-                    GY_c[e] = (V_p[e] * gy0 + Vr[e] * gy1) * (vm[e] + vr[e]);
-                    // depth.f90:141-147 depth on the h point
-                    const double s0 = sel(lc, hq_m1[e]) + sel(lr, hq_m1[e + 1]);
-                    const double s1_ = sel(lu, hq_0[e]) + sel(lur, hq_0[e + 1]);
-                    const double hh = (s0 * wh0 + s1_ * wh1) * rcount(lc + lr + lu + lur);
-                    // vel_ssh.f90:35-37 metric vorticity (zero on uniform grids) + Coriolis
-                    double vort = 0.0;
-                    if (!p.vort_zero && luu)
-                        vort = (vr[e + 1] - vr[e]) * CF(sr, vt0) - uu[e] * CF(sr, vt1) + ur[e + 1] * CF(sr, vt2);
-                    const double Wh = hh * (cor + vort);
-                    QU_c[e] = Wh * (vr[e] + vr[e + 1]);
-                    QV_c[e] = Wh * (ur[e + 1] + uu[e]);
-                    // mixing.f90:134-148 stresses from the previous level
-                    const double str_t = lc ? t1 * (upr[e + 1] - upr[e]) - (t2 * vpr[e] - t3 * vpm[e]) : 0.0;
-                    const double str_s = luu ? s1 * upu[e] - s2 * upr[e + 1] + s3 * (vpr[e + 1] - vpr[e]) : 0.0;
-                    double mu_h = p.mu0;
-                    if constexpr (F2D) mu_h = (mur[e] + mur[e + 1] + muu[e] + muu[e + 1]) * 0.25;
-                    ST_c[e] = mur[e] * hq_m1[e] * str_t;
-                    SS_c[e] = mu_h * hh * str_s;
-                }
+            for (int e = 0; e < 2; e++) {
+                // Function/depth.f90:127-139 mask-weighted averages to u and v points
+                const int a = (mj >> e) & 1, b = (mj >> (e + 1)) & 1, c = (mn >> e) & 1;
+                hu[e] = (sel(a, hq0[e]) + sel(b, hq0[e + 1])) * (a & b ? ku2 : (a | b ? ku : 0.0));
+                hv[e] = (sel(a, hq0[e] * wv0) + sel(c, hq1[e] * wv1)) * (a & c ? 0.5 : (a | c ? 1.0 : 0.0));
             }
-            FXr_c = SHFL_DN(FX_c[0]);
-            STr_c = SHFL_DN(ST_c[0]);
-            SNr_c = SHFL_DN(sshn_c[0]);
-            GXl_c = SHFL_UP(GX_c[1]);
-            QVl_c = SHFL_UP(QV_c[1]);
-            SSl_c = SHFL_UP(SS_c[1]);
-            // ---------------- stage 3: row R = j-2 ---------------------------
-            if (j >= r0 + 2 && (out0 || out1)) {
-                const int R = j - 2;
-                const uint32_t mR = (mk >> 9) & 7u, mU = (mk >> 6) & 7u;   // rows R, R+1
-                const int sR = s_m2, sU = s_m1;
-                const double2 e_R = pair(sR, R_SSH), sp_R = pair(sR, R_SSHP), h_R = pair(sR, R_H);
-                const double2 e_U = pair(sU, R_SSH), sp_U = pair(sU, R_SSHP), h_U = pair(sU, R_H);
-                const double2 u_R = pair(sR, R_U), up_R = pair(sR, R_UP), v_R = pair(sR, R_V);
-                const double2 vp_R = pair(sR, R_VP), rx = pair(sR, R_RX), ry = pair(sR, R_RY);
-                const double e3[3] = {e_R.x, e_R.y, rightv(sR, R_SSH)};
-                const double sp3[3] = {sp_R.x, sp_R.y, rightv(sR, R_SSHP)};
-                const double h3[3] = {h_R.x, h_R.y, rightv(sR, R_H)};
-                const double eU[2] = {e_U.x, e_U.y}, spU[2] = {sp_U.x, sp_U.y}, hU[2] = {h_U.x, h_U.y};
-                const double u0[2] = {u_R.x, u_R.y}, up0[2] = {up_R.x, up_R.y};
-                const double v0[2] = {v_R.x, v_R.y}, vp0[2] = {vp_R.x, vp_R.y};
-                const double rxv[2] = {rx.x, rx.y}, ryv[2] = {ry.x, ry.y};
-                const double sn3[3] = {sshn_p[0], sshn_p[1], SNr_p};   // new SSH, row R
-                const double FX3[3] = {FX_p[0], FX_p[1], FXr_p};
-                const double ST3[3] = {ST_p[0], ST_p[1], STr_p};
-                const double GX3[3] = {GXl_p, GX_p[0], GX_p[1]};
-                const double QV3[3] = {QVl_p, QV_p[0], QV_p[1]};
-                const double SS3[3] = {SSl_p, SS_p[0], SS_p[1]};
-                double rd3[3] = {p.rd0, p.rd0, p.rd0}, rdU[2] = {p.rd0, p.rd0};
-                if constexpr (F2D) {
-                    const double2 a = pair(sR, R_RD), b = pair(sU, R_RD);
-                    rd3[0] = a.x; rd3[1] = a.y; rd3[2] = rightv(sR, R_RD);
-                    rdU[0] = b.x; rdU[1] = b.y;
-                }
-                const double ku2 = CF(sR, ku2), wv0 = CF(sR, wv0), wv1 = CF(sR, wv1);
-                const double gdyh = CF(sR, gdyh), gdxh = CF(sR, gdxh), dux = CF(sR, dux);
-                const double dus0 = CF(sR, dus0), dus1 = CF(sR, dus1), dvt0 = CF(sR, dvt0);
-                const double dvt1 = CF(sR, dvt1), dvs = CF(sR, dvs), au = CF(sR, au), av = CF(sR, av);
-                const double cu = p.two_ti * CF(sR, rau), cv = p.two_ti * CF(sR, rav);
-                const long long rowb = (long long)R * p.pitch + k0;
+            s1n.hu0 = hu[0]; s1n.hu1 = hu[1]; s1n.hv0 = hv[0]; s1n.hv1 = hv[1];
+            s1n.U0 = u.x * hu[0];
+            s1n.U1 = u.y * hu[1];
+            s1n.V0 = v.x * hv[0];
+            s1n.V1 = v.y * hv[1];
+        }
+        s1n.Ul = SHFL_UP(s1n.U1);
+        s1n.Vr = SHFL_DN(s1n.V0);
+
+        // ---------------- stage 2: row rho = j-1 -------------------------
+        const bool st2 = j >= r0 && j <= r1 + 1;
+        double FX0 = 0, FX1 = 0, FXr = 0, ST_r = 0, SNr = 0;
+        if (st2) {
+            const uint32_t mr = (mk >> 6) & 7u, mu_ = (mk >> 3) & 7u;   // rows rho, rho+1
+            const int sr = s_m1, sm = s_m2, su = s_0;
+            const double2 u_r = pair(sr, R_U), u_u = pair(su, R_U), v_r = pair(sr, R_V);
+            const double2 v_m = pair(sm, R_V), up_r = pair(sr, R_UP), up_u = pair(su, R_UP);
+            const double2 vp_r = pair(sr, R_VP), vp_m = pair(sm, R_VP), sp_r = pair(sr, R_SSHP);
+            const double ur[3] = {leftv(sr, R_U), u_r.x, u_r.y};     // u at k0-1, k0, k0+1
+            const double vr[3] = {v_r.x, v_r.y, rightv(sr, R_V)};    // v at k0, k0+1, k0+2
+            const double vpr[3] = {vp_r.x, vp_r.y, rightv(sr, R_VP)};
+            const double upr[3] = {leftv(sr, R_UP), up_r.x, up_r.y};
+            const double uu[2] = {u_u.x, u_u.y}, vm[2] = {v_m.x, v_m.y};
+            const double upu[2] = {up_u.x, up_u.y}, vpm[2] = {vp_m.x, vp_m.y};
+            const double spr[2] = {sp_r.x, sp_r.y};
+            const double Ur[3] = {s1c.Ul, s1c.U0, s1c.U1};           // U(rho) at k0-1, k0, k0+1
+            const double Vr[3] = {s1c.V0, s1c.V1, s1c.Vr};           // V(rho) at k0, k0+1, k0+2
+            const double Un[2] = {s1n.U0, s1n.U1};                   // U(rho+1)
+            const double Vm[2] = {s1p.V0, s1p.V1};                   // V(rho-1)
+            const double hqr[3] = {hqp.a, hqp.b, hqp.c}, hqu[3] = {hqc.a, hqc.b, hqc.c};
+            double mur[3] = {p.mu0, p.mu0, p.mu0}, muu[3] = {p.mu0, p.mu0, p.mu0}, wf[2] = {p.wq0, p.wq0};
+            if constexpr (F2D) {
+                const double2 a = pair(sr, R_MU), b = pair(su, R_MU), w = pair(sr, R_WF);
+                mur[0] = a.x; mur[1] = a.y; mur[2] = rightv(sr, R_MU);
+                muu[0] = b.x; muu[1] = b.y; muu[2] = rightv(su, R_MU);
+                wf[0] = w.x * p.inv_rho; wf[1] = w.y * p.inv_rho;
+            }
+            const double c_u = CF(sr, c_u), c_v0 = CF(sr, c_v0), c_v1 = CF(sr, c_v1);
+            const double fx = CF(sr, fx), fy = CF(sr, fy), gx0 = CF(sr, gx0), gx1 = CF(sr, gx1);
+            const double gy0 = CF(sr, gy0), gy1 = CF(sr, gy1), wh0 = CF(sr, wh0), wh1 = CF(sr, wh1);
+            const double t1 = CF(sr, t1), t2 = CF(sr, t2), t3 = CF(sr, t3);
+            const double s1 = CF(sr, s1), s2 = CF(sr, s2), s3 = CF(sr, s3);
+            const double cor = coef(sr)->cor;
+            double sn[2], FX[2], FY[2], GX[2], GY[2], QU[2], QV[2], ST[2], SS[2];
 #pragma unroll
-                for (int e = 0; e < 2; e++) {
-                    if (!(e == 0 ? out0 : out1)) continue;
-                    const int lc = (mR >> e) & 1, lr = (mR >> (e + 1)) & 1, lup = (mU >> e) & 1;
-                    const long long idx = rowb + e;
-                    if (lc & lr) {   // vel_ssh.f90:536-551
-                        const double hu = hu_w[0][e];
-                        const double hup = ((h3[e] + sp3[e]) + (h3[e + 1] + sp3[e + 1])) * ku2;
-                        const double hun = ((h3[e] + sn3[e]) + (h3[e + 1] + sn3[e + 1])) * ku2;
-                        const double slx = -(e3[e + 1] - e3[e]) * gdyh * hu;
-                        const double slxn = -(sn3[e + 1] - sn3[e]) * gdyh * hun;
-                        const double adv = -((FX3[e + 1] - FX3[e]) + (FY_p[e] - FY_pp[e]));
-                        const double dif = (ST3[e + 1] - ST3[e]) * dux + (SS_p[e] * dus0 - SS_pp[e] * dus1);
-                        const double rd = F2D ? (rd3[e] + rd3[e + 1]) * 0.5 : p.rd0;
-                        const double grx = rxv[e] * p.rhs_scale + slx + dif + adv - rd * up0[e] * au * hu
-                                           + (QU_p[e] + QU_pp[e]) * 0.25;
-                        const double un = (up0[e] * hup + grx * cu) / hun;
-                        if (!(un < 100.0 && un > -100.0)) atomicOr(p.flags, FLAG_GUARD);
-                        if (p.acc_mode) {
-                            double a = (u0[e] * hu + un * hun) * p.c4, b = (slx + slxn) * p.c4;
-                            if (p.acc_mode == 2) { a += p.acc[0][idx]; b += p.acc[2][idx]; }
-                            p.acc[0][idx] = a;
-                            p.acc[2][idx] = b;
-                        }
-                        if (p.write_state) {
-                            p.dst[S_UP][idx] = u0[e] + p.gam * (un - 2.0 * u0[e] + up0[e]);
-                            p.dst[S_U][idx] = un;
-                        }
+            for (int e = 0; e < 2; e++) {
+                const int lc = (mr >> e) & 1, lr = (mr >> (e + 1)) & 1;
+                const int lu = (mu_ >> e) & 1, lur = (mu_ >> (e + 1)) & 1;
+                const int luu = lc & lr & lu & lur;
+                // vel_ssh.f90:491-494 continuity over 2*tau_inner
+                const double div = (Ur[e + 1] - Ur[e]) * c_u + Vr[e] * c_v0 - Vm[e] * c_v1;
+                sn[e] = sel(lc, spr[e] + two_ti * (wf[e] - div));
+                // vel_ssh.f90:63-73, :88-98 advective fluxes on T and h faces
+                FX[e] = (Ur[e] + Ur[e + 1]) * (ur[e] + ur[e + 1]) * fx;
+                FY[e] = sel(luu, (Vr[e] + Vr[e + 1]) * (ur[e + 1] + uu[e]) * fy);
+                GX[e] = (Ur[e + 1] * gx0 + Un[e] * gx1) * (vr[e] + vr[e + 1]);
+                GY[e] = (Vm[e] * gy0 + Vr[e] * gy1) * (vm[e] + vr[e]);
+                // depth.f90:141-147 depth on the h point
+                const double sa = sel(lc, hqr[e]) + sel(lr, hqr[e + 1]);
+                const double sb = sel(lu, hqu[e]) + sel(lur, hqu[e + 1]);
+                const double hh = (sa * wh0 + sb * wh1) * rcount(lc + lr + lu + lur);
+                // vel_ssh.f90:35-37 metric vorticity (zero on uniform grids) + Coriolis
+                double vort = 0.0;
+                if (!p.vort_zero)
+                    vort = sel(luu, (vr[e + 1] - vr[e]) * CF(sr, vt0) - uu[e] * CF(sr, vt1) + ur[e + 1] * CF(sr, vt2));
+                const double Wh = hh * (cor + vort);
+                QU[e] = Wh * (vr[e] + vr[e + 1]);
+                QV[e] = Wh * (ur[e + 1] + uu[e]);
+                // mixing.f90:134-148 stresses from the previous level
+                const double str_t = sel(lc, t1 * (upr[e + 1] - upr[e]) - (t2 * vpr[e] - t3 * vpm[e]));
+                const double str_s = sel(luu, s1 * upu[e] - s2 * upr[e + 1] + s3 * (vpr[e + 1] - vpr[e]));
+                double mu_h = p.mu0;
+                if constexpr (F2D) mu_h = (mur[e] + mur[e + 1] + muu[e] + muu[e + 1]) * 0.25;
+                ST[e] = mur[e] * hqr[e] * str_t;
+                SS[e] = mu_h * hh * str_s;
+            }
+            s2n.sn0 = sn[0]; s2n.sn1 = sn[1];
+            s2n.FY0 = FY[0]; s2n.FY1 = FY[1]; s2n.QU0 = QU[0]; s2n.QU1 = QU[1];
+            s2n.SS0 = SS[0]; s2n.SS1 = SS[1]; s2n.GX0 = GX[0]; s2n.GX1 = GX[1];
+            s2n.GY0 = GY[0]; s2n.GY1 = GY[1]; s2n.QV0 = QV[0]; s2n.QV1 = QV[1];
+            s2n.ST0 = ST[0]; s2n.ST1 = ST[1];
+            FX0 = FX[0]; FX1 = FX[1];
+        }
+        FXr = SHFL_DN(FX0);
+        ST_r = SHFL_DN(s2n.ST0);
+        SNr = SHFL_DN(s2n.sn0);
+        s2n.GXl = SHFL_UP(s2n.GX1);
+        s2n.QVl = SHFL_UP(s2n.QV1);
+        s2n.SSl = SHFL_UP(s2n.SS1);
+
+        // ---------------- stage 3u: row rho = j-1 (u and SSH) -----------
+        const int rho = j - 1;
+        const uint32_t mr = (mk >> 6) & 7u;
+        const bool wr3u = j >= r0 + 1 && j <= r1 && __any_sync(0xffffffffu, (out0 || out1) && (mr & 3u));
+        if (wr3u) {
+            const int sr = s_m1;
+            const double2 e_r = pair(sr, R_SSH), sp_r = pair(sr, R_SSHP), h_r = pair(sr, R_H);
+            const double e3[3] = {e_r.x, e_r.y, rightv(sr, R_SSH)};
+            const double sp3[3] = {sp_r.x, sp_r.y, rightv(sr, R_SSHP)};
+            const double h3[3] = {h_r.x, h_r.y, rightv(sr, R_H)};
+            const double2 u_r = pair(sr, R_U), up_r = pair(sr, R_UP), rx = pair(sr, R_RX);
+            const double u0[2] = {u_r.x, u_r.y}, up0[2] = {up_r.x, up_r.y}, rxv[2] = {rx.x, rx.y};
+            const double sn3[3] = {s2n.sn0, s2n.sn1, SNr};
+            const double FX3[3] = {FX0, FX1, FXr};
+            const double ST3[3] = {s2n.ST0, s2n.ST1, ST_r};
+            const double FYd[2] = {s2n.FY0 - s2o.FY0, s2n.FY1 - s2o.FY1};
+            const double QUs[2] = {s2n.QU0 + s2o.QU0, s2n.QU1 + s2o.QU1};
+            const double SSn[2] = {s2n.SS0, s2n.SS1}, SSo[2] = {s2o.SS0, s2o.SS1};
+            const double hu_c[2] = {s1c.hu0, s1c.hu1};
+            double rd3[3] = {p.rd0, p.rd0, p.rd0};
+            if constexpr (F2D) {
+                const double2 a = pair(sr, R_RD);
+                rd3[0] = a.x; rd3[1] = a.y; rd3[2] = rightv(sr, R_RD);
+            }
+            const double ku2 = CF(sr, ku2), gdyh = CF(sr, gdyh), dux = CF(sr, dux);
+            const double dus0 = CF(sr, dus0), dus1 = CF(sr, dus1), au = CF(sr, au);
+            const double cu = two_ti * CF(sr, rau);
+            const long long rowb = (long long)rho * p.pitch + k0;
+#pragma unroll
+            for (int e = 0; e < 2; e++) {
+                const bool oute = e == 0 ? out0 : out1;
+                const int lc = (mr >> e) & 1, lr = (mr >> (e + 1)) & 1;
+                const bool wu = oute && (lc & lr), wt = oute && lc;
+                // vel_ssh.f90:536-551
+                const double hu = hu_c[e];
+                const double hup = ((h3[e] + sp3[e]) + (h3[e + 1] + sp3[e + 1])) * ku2;
+                const double hun = ((h3[e] + sn3[e]) + (h3[e + 1] + sn3[e + 1])) * ku2;
+                const double slx = -(e3[e + 1] - e3[e]) * gdyh * hu;
+                const double slxn = -(sn3[e + 1] - sn3[e]) * gdyh * hun;
+                const double adv = -((FX3[e + 1] - FX3[e]) + FYd[e]);
+                const double dif = (ST3[e + 1] - ST3[e]) * dux + (SSn[e] * dus0 - SSo[e] * dus1);
+                const double rd = F2D ? (rd3[e] + rd3[e + 1]) * 0.5 : p.rd0;
+                const double grx = rxv[e] * rs + slx + dif + adv - rd * up0[e] * au * hu + QUs[e] * 0.25;
+                const double un = (up0[e] * hup + grx * cu) * rcp_nr(hun);
+                bad |= (uint32_t)(wu && !(un < 100.0 && un > -100.0));
+                bad |= (uint32_t)(wt && !(sn3[e] < 10.0 && sn3[e] > -10.0));
+                const long long idx = rowb + e;
+                if (p.acc_mode && wu) {
+                    double a = (u0[e] * hu + un * hun) * p.c4, b = (slx + slxn) * p.c4;
+                    if (p.acc_mode == 2) { a += p.acc[0][idx]; b += p.acc[2][idx]; }
+                    p.acc[0][idx] = a;
+                    p.acc[2][idx] = b;
+                }
+                if (p.write_state) {
+                    if (wu) {
+                        p.dst[S_UP][idx] = u0[e] + gam * (un - 2.0 * u0[e] + up0[e]);
+                        p.dst[S_U][idx] = un;
                     }
-                    if (lc & lup) {   // vel_ssh.f90:554-569
-                        const double hv = hv_w[0][e];
-                        const double hvp = ((h3[e] + sp3[e]) * wv0 + (hU[e] + spU[e]) * wv1) * 0.5;
-                        const double hvn = ((h3[e] + sn3[e]) * wv0 + (hU[e] + sshn_c[e]) * wv1) * 0.5;
-                        const double sly = -(eU[e] - e3[e]) * gdxh * hv;
-                        const double slyn = -(sshn_c[e] - sn3[e]) * gdxh * hvn;
-                        const double adv = -((GX3[e + 1] - GX3[e]) + (GY_c[e] - GY_p[e]));
-                        const double dif = -(ST_c[e] * dvt1 - ST3[e] * dvt0) + (SS3[e + 1] - SS3[e]) * dvs;
-                        const double rd = F2D ? (rd3[e] + rdU[e]) * 0.5 : p.rd0;
-                        const double gry = ryv[e] * p.rhs_scale + sly + dif + adv - rd * vp0[e] * av * hv
-                                           - (QV3[e + 1] + QV3[e]) * 0.25;
-                        const double vn = (vp0[e] * hvp + gry * cv) / hvn;
-                        if (!(vn < 100.0 && vn > -100.0)) atomicOr(p.flags, FLAG_GUARD);
-                        if (p.acc_mode) {
-                            double a = (v0[e] * hv + vn * hvn) * p.c4, b = (sly + slyn) * p.c4;
-                            if (p.acc_mode == 2) { a += p.acc[1][idx]; b += p.acc[3][idx]; }
-                            p.acc[1][idx] = a;
-                            p.acc[3][idx] = b;
-                        }
-                        if (p.write_state) {
-                            p.dst[S_VP][idx] = v0[e] + p.gam * (vn - 2.0 * v0[e] + vp0[e]);
-                            p.dst[S_V][idx] = vn;
-                        }
-                    }
-                    if (lc) {   // vel_ssh.f90:593-596
-                        if (!(sn3[e] < 10.0 && sn3[e] > -10.0)) atomicOr(p.flags, FLAG_GUARD);
-                        if (p.write_state) {
-                            p.dst[S_SSHP][idx] = e3[e] + p.gam * (sn3[e] - 2.0 * e3[e] + sp3[e]);
-                            p.dst[S_SSH][idx] = sn3[e];
-                        }
+                    if (wt) {   // vel_ssh.f90:593-596
+                        p.dst[S_SSHP][idx] = e3[e] + gam * (sn3[e] - 2.0 * e3[e] + sp3[e]);
+                        p.dst[S_SSH][idx] = sn3[e];
                     }
                 }
             }
         }
-        // ---- rotate the register pipelines and the ring ---------------------
+
+        // ---------------- stage 3v: row R = j-2 (v) ----------------------
+        const int R = j - 2;
+        const uint32_t mR = (mk >> 9) & 7u, mU = (mk >> 6) & 7u;   // rows R, R+1
+        const bool wr3v = j >= r0 + 2 && j <= r1 + 1 &&
+                          __any_sync(0xffffffffu, (out0 && (mR & mU & 1u)) || (out1 && (mR & mU & 2u)));
+        if (wr3v) {
+            const int sR = s_m2, sU = s_m1;
+            const double2 eR = pair(sR, R_SSH), spR = pair(sR, R_SSHP), hR = pair(sR, R_H);
+            const double2 eU = pair(sU, R_SSH), spU = pair(sU, R_SSHP), hU = pair(sU, R_H);
+            const double2 v_R = pair(sR, R_V), vp_R = pair(sR, R_VP), ry = pair(sR, R_RY);
+            const double e0[2] = {eR.x, eR.y}, sp0[2] = {spR.x, spR.y}, h0[2] = {hR.x, hR.y};
+            const double e1[2] = {eU.x, eU.y}, sp1[2] = {spU.x, spU.y}, h1[2] = {hU.x, hU.y};
+            const double v0[2] = {v_R.x, v_R.y}, vp0[2] = {vp_R.x, vp_R.y}, ryv[2] = {ry.x, ry.y};
+            const double sn0[2] = {s2o.sn0, s2o.sn1}, sn1[2] = {s2n.sn0, s2n.sn1};
+            const double GX3[3] = {s2o.GXl, s2o.GX0, s2o.GX1};
+            const double QV3[3] = {s2o.QVl, s2o.QV0, s2o.QV1};
+            const double SS3[3] = {s2o.SSl, s2o.SS0, s2o.SS1};
+            const double GYd[2] = {s2n.GY0 - s2o.GY0, s2n.GY1 - s2o.GY1};
+            const double STo[2] = {s2o.ST0, s2o.ST1}, STn[2] = {s2n.ST0, s2n.ST1};
+            const double hv_c[2] = {s1p.hv0, s1p.hv1};
+            double rdR[2] = {p.rd0, p.rd0}, rdU[2] = {p.rd0, p.rd0};
+            if constexpr (F2D) {
+                const double2 a = pair(sR, R_RD), b = pair(sU, R_RD);
+                rdR[0] = a.x; rdR[1] = a.y; rdU[0] = b.x; rdU[1] = b.y;
+            }
+            const double wv0 = CF(sR, wv0), wv1 = CF(sR, wv1), gdxh = CF(sR, gdxh);
+            const double dvt0 = CF(sR, dvt0), dvt1 = CF(sR, dvt1), dvs = CF(sR, dvs), av = CF(sR, av);
+            const double cv = two_ti * CF(sR, rav);
+            const long long rowb = (long long)R * p.pitch + k0;
 #pragma unroll
-        for (int e = 0; e < 2; e++) {
-            V_p[e] = V_c[e]; V_c[e] = V_n[e]; U_c[e] = U_n[e];
-            hu_w[0][e] = hu_w[1][e]; hu_w[1][e] = hu_n[e];
-            hv_w[0][e] = hv_w[1][e]; hv_w[1][e] = hv_n[e];
-            FY_pp[e] = FY_p[e]; FY_p[e] = FY_c[e];
-            QU_pp[e] = QU_p[e]; QU_p[e] = QU_c[e];
-            SS_pp[e] = SS_p[e]; SS_p[e] = SS_c[e];
-            sshn_p[e] = sshn_c[e]; GY_p[e] = GY_c[e]; ST_p[e] = ST_c[e];
-            FX_p[e] = FX_c[e]; GX_p[e] = GX_c[e]; QV_p[e] = QV_c[e];
+            for (int e = 0; e < 2; e++) {
+                const bool oute = e == 0 ? out0 : out1;
+                const bool wv = oute && ((mR >> e) & (mU >> e) & 1u);
+                // vel_ssh.f90:554-569
+                const double hv = hv_c[e];
+                const double hvp = ((h0[e] + sp0[e]) * wv0 + (h1[e] + sp1[e]) * wv1) * 0.5;
+                const double hvn = ((h0[e] + sn0[e]) * wv0 + (h1[e] + sn1[e]) * wv1) * 0.5;
+                const double sly = -(e1[e] - e0[e]) * gdxh * hv;
+                const double slyn = -(sn1[e] - sn0[e]) * gdxh * hvn;
+                const double adv = -((GX3[e + 1] - GX3[e]) + GYd[e]);
+                const double dif = -(STn[e] * dvt1 - STo[e] * dvt0) + (SS3[e + 1] - SS3[e]) * dvs;
+                const double rd = F2D ? (rdR[e] + rdU[e]) * 0.5 : p.rd0;
+                const double gry = ryv[e] * rs + sly + dif + adv - rd * vp0[e] * av * hv
+                                   - (QV3[e + 1] + QV3[e]) * 0.25;
+                const double vn = (vp0[e] * hvp + gry * cv) * rcp_nr(hvn);
+                bad |= (uint32_t)(wv && !(vn < 100.0 && vn > -100.0));
+                const long long idx = rowb + e;
+                if (p.acc_mode && wv) {
+                    double a = (v0[e] * hv + vn * hvn) * p.c4, b = (sly + slyn) * p.c4;
+                    if (p.acc_mode == 2) { a += p.acc[1][idx]; b += p.acc[3][idx]; }
+                    p.acc[1][idx] = a;
+                    p.acc[3][idx] = b;
+                }
+                if (p.write_state && wv) {
+                    p.dst[S_VP][idx] = v0[e] + gam * (vn - 2.0 * v0[e] + vp0[e]);
+                    p.dst[S_V][idx] = vn;
+                }
+            }
         }
-#pragma unroll
-        for (int e = 0; e < 3; e++) { hq_m1[e] = hq_0[e]; hq_0[e] = hq_p1[e]; }
-        Ul_c = Ul_n; Vr_c = Vr_n;
-        FXr_p = FXr_c; STr_p = STr_c; SNr_p = SNr_c; GXl_p = GXl_c; QVl_p = QVl_c; SSl_p = SSl_c;
-        s_m2 = s_m1;
-        s_m1 = s_0;
-        s_0 = s_p1;
-        s_p1 = s_p1 + 1 == RING ? 0 : s_p1 + 1;
-        if (__any_sync(0xffffffffu, !ok)) { abort = true; break; }
-        // row j-2 was last read by stage 3 above: once every lane is past it
-        // its slot takes row j-2+RING
+        // row j-2 was last read above: once every lane is past it, its slot
+        // takes row j-2+RING
         __syncwarp();
         if (l == 0) {
             const int dead = j - 2;
-            if (dead >= row_lo && dead + RING <= row_hi) {
-                issue(dead + RING, (dead - row_lo) % RING);
-                issued = dead + RING;
-            }
+            if (dead >= row_lo && dead + RING <= row_hi) issue(dead + RING), issued = dead + RING;
+        }
+    };
+
+    // three instances of each carried struct, renamed (not copied) by the
+    // three-fold unrolled loop
+    S1 A{}, B{}, C{};
+    HQ HA{}, HB{}, HC{};
+    S2 X{}, Y{}, Z{};
+    {   // H + ssh of row r0-1 (the stage-1 "current" row of the first step)
+        const int need = row_lo + 1;
+        while (waited < need && ok) {
+            const int row = waited + 1;
+            if (!mbar_wait(&mbar[slot_of(row)], (uint32_t)(((row - row_lo) / RING) & 1))) { ok = false; break; }
+            waited = row;
+            mk = (mk << 3) | mask3(slot_of(row));
+        }
+        ok = __all_sync(0xffffffffu, ok);
+        if (ok) {
+            const int s = slot_of(r0 - 1);
+            const double2 h = pair(s, R_H), e = pair(s, R_SSH);
+            HC.a = h.x + e.x;
+            HC.b = h.y + e.y;
+            HC.c = rightv(s, R_H) + rightv(s, R_SSH);
         }
     }
+    // mk now holds rows r0-2 (bits 3-5) and r0-1 (bits 0-2); the first step
+    // pushes row r0 so that row j+1 = r0 sits in bits 0-2
+    for (int j = r0 - 1; j <= r1 + 1 && ok; j += 3) {
+        step(j, A, C, B, HA, HC, HB, X, Z);
+        step(j + 1, B, A, C, HB, HA, HC, Y, X);
+        step(j + 2, C, B, A, HC, HB, HA, Z, Y);
+    }
 #undef CF
-    if (abort && l == 0) {
+    if (__any_sync(0xffffffffu, bad != 0) && l == 0) atomicOr(p.flags, FLAG_GUARD);
+    if (!ok && l == 0) {
         atomicOr(p.flags, FLAG_TIMEOUT);
         // drain this CTA's copies still in flight (bounded) before exiting
         for (int row = max(waited + 1, row_lo); row <= issued; row++)
-            (void)mbar_wait(&mbar[(row - row_lo) % RING], (uint32_t)(((row - row_lo) / RING) & 1));
+            (void)mbar_wait(&mbar[slot_of(row)], (uint32_t)(((row - row_lo) / RING) & 1));
     }
 }
 
