@@ -1,33 +1,37 @@
 // Fused streaming kernel of the barotropic step (see fused.h).
 //
-// Work decomposition.  A CTA is one warp.  Lane l owns the two adjacent
-// device columns k0 = g0+2+2l and k0+1 of a 64-column strip starting at
-// device column g0+2 (g0 = 62*strip, even); strip columns 1..62 are written,
-// so strips overlap by two columns.  The CTA marches down a chunk of output
-// rows [r0, r1).  Iteration j computes, for its columns,
-//   stage 1, row j   : u/v-point depths of the current level and the
-//                      transports U = u*hu, V = v*hv;
-//   stage 2, row j-1 : new SSH (continuity), advective fluxes on T and h
+// Work decomposition.  A CTA is one warp; lane l owns device column
+// k = g0+2+l of a 32-column strip starting at device column g0+2
+// (g0 = 30*strip, even).  Strip columns 1..30 are written, so strips overlap
+// by two columns.  The CTA marches down a chunk of rows [r0, r1); iteration
+// j of its row loop computes
+//   stage 1,  row j  : u/v-point depths of the current level, the transports
+//                      U = u*hu and V = v*hv, and loads the forcing of row j;
+//   stage 2,  row j-1: new SSH (continuity), advective fluxes on T and h
 //                      points, Coriolis-plus-metric-vorticity products,
 //                      tension and shear stresses times viscosity and depth;
-//   stage 3u, row j-1: u momentum, SSH update, their time-mean sums,
-//                      Robert-Asselin filter and time shift, stores;
+//   stage 3u, row j-1: u momentum and the SSH update (time-mean sums,
+//                      Robert-Asselin filter and time shift, stores);
 //   stage 3v, row j-2: the same for v (it needs stage 2 of the row above).
-// A value a stage needs from the neighbouring column is the other column
-// of the same lane or comes from the neighbouring lane by a warp shuffle;
-// values of earlier rows of the same column stay in registers, in three
+// A value needed from a neighbouring column comes from the neighbouring lane
+// by a warp shuffle; values of earlier rows stay in registers, in three
 // instances of each per-row struct that the three-fold unrolled row loop
-// renames instead of copying.  There is no CTA-wide barrier, and the
-// per-column work is branch-free (predicated stores) except for warp-wide
-// skips of rows without ocean.
+// renames instead of copying.  There is no CTA barrier, and the per-column
+// arithmetic is branch-free (masked selects, predicated stores) except for
+// warp-wide skips of rows without ocean.
 //
-// Input rows j-2..j+1 of the input fields (a 68-column segment per field
-// and row, 16-byte aligned), the row's coefficients and the row's T-mask
-// bits sit in a ring of RING shared-memory slots.  Lane 0 refills the slot
-// of row j-2 with row j-2+RING by 1-D bulk TMA copies (cp.async.bulk, no
-// multicast) completing on that slot's mbarrier.  Every wait is bounded: on
-// timeout the CTA sets a status bit, drains its own copies (bounded) and
-// returns.
+// Input rows j-2..j+1 of the state, the rest depth (and, in the general
+// variant, the 2-D forcing fields and the row's metric coefficients) plus the
+// row's T-mask bits sit in a ring of RING shared-memory slots.  Lane 0 refills
+// the slot of row j-2 with row j-2+RING by 1-D bulk TMA copies
+// (cp.async.bulk, no multicast) completing on that slot's mbarrier.  Every
+// wait is bounded: on timeout the CTA sets a status bit, drains its own
+// copies (bounded) and returns.
+//
+// Two variants: UNI for square uniform grids (every metric array equal to
+// one spacing d; all metric factors fold into a few constants and only the
+// Coriolis parameter varies by row) with spatially uniform viscosity, drag
+// and water flux; GEN for metrics that vary along y and 2-D forcing fields.
 #include "fused.h"
 
 #include <algorithm>
@@ -40,19 +44,17 @@ namespace fused {
 
 namespace {
 
-constexpr int NL = 32;            // lanes = threads per CTA
-constexpr int NCOL = 2 * NL;      // strip columns
-constexpr int OUTW = NCOL - 2;    // written columns per strip
-constexpr int SEG = NCOL + 4;     // ring segment: strip columns -2 .. 65
+constexpr int NL = 32;            // lanes = threads per CTA = strip columns
+constexpr int OUTW = NL - 2;      // written columns per strip
+constexpr int SEG = NL + 4;       // ring segment: strip columns -2 .. 33
 constexpr int RING = 6;           // ring slots (4 rows in use + 2 in flight)
-constexpr int CTAS_PER_SM = 7;
 constexpr int COEF_D = (int)(sizeof(RowCoef) / sizeof(double));
 constexpr unsigned WAIT_LIMIT = 1u << 20;
 
 // state order, as the *_e arguments: u, up, v, vp, ssh, sshp
 enum { S_U, S_UP, S_V, S_VP, S_SSH, S_SSHP };
 // ring fields
-enum { R_U, R_V, R_SSH, R_UP, R_VP, R_SSHP, R_H, R_RX, R_RY, R_NBASE, R_MU = R_NBASE, R_RD, R_WF, R_N2D };
+enum { R_U, R_V, R_SSH, R_UP, R_VP, R_SSHP, R_H, R_NUNI, R_MU = R_NUNI, R_RD, R_WF, R_NGEN };
 
 struct Params {
     const double *src[6];
@@ -61,15 +63,14 @@ struct Params {
     double *acc[4];
     const uint32_t *bits;
     const RowCoef *rows;
-    RowCoef rc;            // row-invariant coefficients (used when !ROWVAR)
+    const double *cor;
     long long pitch;
     int bm_words;
     int chunk_rows;
     int r_first, r_last;   // interior device rows
     int c_first, c_last;   // interior device columns
     double two_ti, gam, c4, rhs_scale, mu0, rd0, wq0, inv_rho;
-    int acc_mode;          // 0 none, 1 write, 2 accumulate
-    int write_state;
+    double d, inv_d, d4, gd, d2, inv_d2;   // UNI metric constants
     int vort_zero;
     unsigned *flags;
 };
@@ -120,12 +121,14 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
         : "memory");
 }
 
-template <bool F2D>
+template <bool GEN>
 struct Layout {
-    static constexpr int NF = F2D ? R_N2D : R_NBASE;
-    static constexpr int SLOT_D = NF * SEG + COEF_D + 4;   // doubles per slot
+    static constexpr int NF = GEN ? R_NGEN : R_NUNI;
+    static constexpr int NCOEF = GEN ? COEF_D : 0;
+    static constexpr int SLOT_D = NF * SEG + NCOEF + 4;   // doubles per slot (4 = 8 mask words)
     static constexpr size_t bytes = (size_t)RING * SLOT_D * sizeof(double) + RING * sizeof(uint64_t);
-    static constexpr uint32_t row_tx = (uint32_t)((NF * SEG + COEF_D + 4) * sizeof(double));
+    static constexpr uint32_t row_tx = (uint32_t)(SLOT_D * sizeof(double));
+    static constexpr int min_ctas = GEN ? 10 : 12;
 };
 
 __device__ __forceinline__ double sel(int m, double x) { return m ? x : 0.0; }
@@ -135,9 +138,6 @@ __device__ __forceinline__ double rcount(int n)
 {
     return n == 4 ? 0.25 : (n == 3 ? 1.0 / 3.0 : (n == 2 ? 0.5 : (n == 1 ? 1.0 : 0.0)));
 }
-
-#define SHFL_UP(x) __shfl_up_sync(0xffffffffu, (x), 1)
-#define SHFL_DN(x) __shfl_down_sync(0xffffffffu, (x), 1)
 
 // 1/x by two Newton-Raphson steps r <- r + r*(1 - x*r) (quadratic
 // convergence) from the single-precision reciprocal: about 1 ulp of double
@@ -151,78 +151,87 @@ __device__ __forceinline__ double rcp_nr(double x)
     return fma(r, e, r);
 }
 
+#define SHFL_UP(x) __shfl_up_sync(0xffffffffu, (x), 1)
+#define SHFL_DN(x) __shfl_down_sync(0xffffffffu, (x), 1)
+
 // per-row values carried between the stages of the row pipeline
-struct S1 {          // stage 1 of a row: transports and current-level depths
-    double U0, U1, V0, V1;   // U = u*hu at k0, k0+1; V = v*hv
-    double Ul, Vr;           // U(k0-1), V(k0+2) from the neighbouring lanes
-    double hu0, hu1, hv0, hv1;
+struct S1 {          // stage 1 of a row
+    double U, V;             // U = u*hu, V = v*hv
+    double Ul, Vr;           // U(k-1), V(k+1) from the neighbouring lanes
+    double hu, hv;           // current-level u/v depths
+    double rx, ry;           // forcing RHSx, RHSy of the row
 };
-struct HQ {          // H + ssh of a row at k0, k0+1, k0+2
-    double a, b, c;
+struct HQ {          // H + ssh of a row at k, k+1
+    double a, b;
 };
 struct S2 {          // stage 2 of a row
-    double sn0, sn1;         // new SSH
-    double FY0, FY1, QU0, QU1, SS0, SS1;
-    double GX0, GX1, GXl, GY0, GY1, QV0, QV1, QVl, ST0, ST1, SSl;
+    double sn;               // new SSH
+    double FY, QU, SS, GX, GXl, GY, QV, QVl, ST, SSl;
 };
 
-template <bool F2D, bool ROWVAR>
-__global__ void __launch_bounds__(NL, CTAS_PER_SM) k_substep(const __grid_constant__ Params p)
+// MODE = acc + 3*write: acc 0 none, 1 first substep (write), 2 accumulate;
+// write 1 stores the new state
+template <bool GEN, int MODE>
+__global__ void __launch_bounds__(NL, Layout<GEN>::min_ctas) k_substep(const __grid_constant__ Params p)
 {
-    using L = Layout<F2D>;
+    using L = Layout<GEN>;
     constexpr int NF = L::NF;
+    constexpr int ACC = MODE % 3;
+    constexpr bool WRITE = MODE / 3 != 0;
     extern __shared__ __align__(128) double smem[];
     uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + RING * L::SLOT_D);
 
     const int l = threadIdx.x;
     const int g0 = blockIdx.x * OUTW;          // device column of segment offset 0
-    const int k0 = g0 + 2 + 2 * l;             // this lane's columns k0, k0+1
+    const int k = g0 + 2 + l;                  // this lane's column
     const int r0 = p.r_first + blockIdx.y * p.chunk_rows;
     const int r1 = min(r0 + p.chunk_rows, p.r_last + 1);   // exclusive
     if (r0 >= r1) return;
     const int row_lo = r0 - 2, row_hi = r1 + 1;             // rows kept in the ring
     const int wbase = (g0 >> 7) << 2;                       // first mask word of the window
-    const int bsh = k0 - wbase * 32;                        // bit of k0 in the window
-    const int po = 2 * l + 2;                               // segment offset of k0
+    const int bsh = k - wbase * 32;                         // bit of k in the window
+    const int po = l + 2;                                   // segment offset of k
 
     auto slotp = [&](int s) { return smem + (size_t)s * L::SLOT_D; };
     auto slot_of = [&](int row) { return (row - row_lo) % RING; };
     auto issue = [&](int row) {
         const int s = slot_of(row);
-        double *d = slotp(s);
+        double *dd = slotp(s);
         uint64_t *bar = &mbar[s];
         mbar_expect_tx(bar, L::row_tx);
         const long long off = (long long)row * p.pitch + g0;
         const uint32_t nb = SEG * sizeof(double);
-        bulk_load(d + R_U * SEG, p.src[S_U] + off, nb, bar);
-        bulk_load(d + R_V * SEG, p.src[S_V] + off, nb, bar);
-        bulk_load(d + R_SSH * SEG, p.src[S_SSH] + off, nb, bar);
-        bulk_load(d + R_UP * SEG, p.src[S_UP] + off, nb, bar);
-        bulk_load(d + R_VP * SEG, p.src[S_VP] + off, nb, bar);
-        bulk_load(d + R_SSHP * SEG, p.src[S_SSHP] + off, nb, bar);
-        bulk_load(d + R_H * SEG, p.H + off, nb, bar);
-        bulk_load(d + R_RX * SEG, p.rhsx + off, nb, bar);
-        bulk_load(d + R_RY * SEG, p.rhsy + off, nb, bar);
-        if constexpr (F2D) {
-            bulk_load(d + R_MU * SEG, p.mu + off, nb, bar);
-            bulk_load(d + R_RD * SEG, p.rdis + off, nb, bar);
-            bulk_load(d + R_WF * SEG, p.wflux + off, nb, bar);
+        bulk_load(dd + R_U * SEG, p.src[S_U] + off, nb, bar);
+        bulk_load(dd + R_V * SEG, p.src[S_V] + off, nb, bar);
+        bulk_load(dd + R_SSH * SEG, p.src[S_SSH] + off, nb, bar);
+        bulk_load(dd + R_UP * SEG, p.src[S_UP] + off, nb, bar);
+        bulk_load(dd + R_VP * SEG, p.src[S_VP] + off, nb, bar);
+        bulk_load(dd + R_SSHP * SEG, p.src[S_SSHP] + off, nb, bar);
+        bulk_load(dd + R_H * SEG, p.H + off, nb, bar);
+        if constexpr (GEN) {
+            bulk_load(dd + R_MU * SEG, p.mu + off, nb, bar);
+            bulk_load(dd + R_RD * SEG, p.rdis + off, nb, bar);
+            bulk_load(dd + R_WF * SEG, p.wflux + off, nb, bar);
+            bulk_load(dd + NF * SEG, p.rows + row, sizeof(RowCoef), bar);
         }
-        bulk_load(d + NF * SEG, p.rows + row, sizeof(RowCoef), bar);
-        bulk_load(d + NF * SEG + COEF_D, p.bits + (size_t)row * p.bm_words + wbase, 32, bar);
+        bulk_load(dd + NF * SEG + L::NCOEF, p.bits + (size_t)row * p.bm_words + wbase, 32, bar);
     };
-    // field f of a slot: own pair (k0, k0+1), left neighbour (k0-1), right (k0+2)
-    auto pair = [&](int s, int f) {
-        return *reinterpret_cast<const double2 *>(slotp(s) + f * SEG + po);
+    auto at = [&](int s, int f, int dk) { return slotp(s)[f * SEG + po + dk]; };
+    auto mask2 = [&](int s) -> uint32_t {   // bits: lu(k), lu(k+1)
+        const uint32_t *w = reinterpret_cast<const uint32_t *>(slotp(s) + NF * SEG + L::NCOEF);
+        return __funnelshift_r(w[bsh >> 5], w[(bsh >> 5) + 1], bsh & 31) & 3u;
     };
-    auto leftv = [&](int s, int f) { return slotp(s)[f * SEG + po - 1]; };
-    auto rightv = [&](int s, int f) { return slotp(s)[f * SEG + po + 2]; };
     auto coef = [&](int s) { return reinterpret_cast<const RowCoef *>(slotp(s) + NF * SEG); };
-    auto mask3 = [&](int s) -> uint32_t {   // bits: lu(k0), lu(k0+1), lu(k0+2)
-        const uint32_t *w = reinterpret_cast<const uint32_t *>(slotp(s) + NF * SEG + COEF_D);
-        return __funnelshift_r(w[bsh >> 5], w[(bsh >> 5) + 1], bsh & 31) & 7u;
-    };
-#define CF(s, x) (ROWVAR ? coef(s)->x : p.rc.x)
+    // metric coefficient of the row in slot s: GEN from the ring, UNI folded
+#define CG(s, x) coef(s)->x
+#define C_KU(s) (GEN ? CG(s, ku) : 1.0)
+#define C_KU2(s) (GEN ? CG(s, ku2) : 0.5)
+#define C_WV0(s) (GEN ? CG(s, wv0) : 1.0)
+#define C_WV1(s) (GEN ? CG(s, wv1) : 1.0)
+#define C_D4(s, x) (GEN ? CG(s, x) : p.d4)
+#define C_GD(s, x) (GEN ? CG(s, x) : p.gd)
+#define C_D2(s, x) (GEN ? CG(s, x) : p.d2)
+#define C_INVD2(s, x) (GEN ? CG(s, x) : p.inv_d2)
 
     if (l == 0) {
         for (int s = 0; s < RING; s++) mbar_init(&mbar[s], 1);
@@ -233,271 +242,189 @@ __global__ void __launch_bounds__(NL, CTAS_PER_SM) k_substep(const __grid_consta
     if (l == 0)
         for (int row = row_lo; row < row_lo + RING && row <= row_hi; row++) issue(row), issued = row;
 
-    const bool out0 = l >= 1 && k0 >= p.c_first && k0 <= p.c_last;
-    const bool out1 = l <= NL - 2 && k0 + 1 >= p.c_first && k0 + 1 <= p.c_last;
+    const bool out = l >= 1 && l <= NL - 2 && k >= p.c_first && k <= p.c_last;
     const double gam = p.gam, two_ti = p.two_ti, rs = p.rhs_scale;
 
-    // T-mask bits, 3 per row: row j+1 in bits 0-2, j in 3-5, j-1 in 6-8, j-2 in 9-11
+    // T-mask bits, 2 per row: row j+1 in bits 0-1, j in 2-3, j-1 in 4-5, j-2 in 6-7
     uint32_t mk = 0;
     uint32_t bad = 0;   // guard: a new value out of range or NaN
     int waited = row_lo - 1;
     bool ok = true;
-
-    // One row step of the pipeline, for iteration j (see the file comment):
-    //   stage 1 row j      -> s1n (and H+ssh of row j+1 -> hqn)
-    //   stage 2 row j-1    -> s2n, from s1c = S1(j-1), s1p = S1(j-2), s1n,
-    //                         hqp = H+ssh(j-1), hqc = H+ssh(j)
-    //   stage 3u row j-1   u momentum and the SSH update, from s2n, s2o
-    //   stage 3v row j-2   v momentum, from s2o = S2(j-2), s2n, s1p
-    auto step = [&](const int j, S1 &s1n, const S1 &s1c, const S1 &s1p, HQ &hqn, const HQ &hqc,
-                    const HQ &hqp, S2 &s2n, const S2 &s2o) {
-        // --- rows up to j+1 must have landed ------------------------------
-        const int need = min(j + 1, row_hi);
+    auto wait_upto = [&](int need) {
         while (waited < need && ok) {
             const int row = waited + 1;
-            const uint32_t par = (uint32_t)(((row - row_lo) / RING) & 1);
-            if (!mbar_wait(&mbar[slot_of(row)], par)) { ok = false; break; }
+            if (!mbar_wait(&mbar[slot_of(row)], (uint32_t)(((row - row_lo) / RING) & 1))) { ok = false; break; }
             waited = row;
-            mk = (mk << 3) | mask3(slot_of(row));
+            mk = (mk << 2) | mask2(slot_of(row));
         }
-        if (j + 1 > row_hi) mk <<= 3;   // keep the row alignment of mk
         ok = __all_sync(0xffffffffu, ok);
+    };
+
+    auto step = [&](const int j, S1 &s1n, const S1 &s1c, const S1 &s1p, HQ &hqn, const HQ &hqc,
+                    const HQ &hqp, S2 &s2n, const S2 &s2o) {
+        wait_upto(min(j + 1, row_hi));
+        if (j + 1 > row_hi) mk <<= 2;   // keep the row alignment of mk
         if (!ok) return;
         const int s_m2 = slot_of(j - 2), s_m1 = slot_of(j - 1), s_0 = slot_of(j), s_p1 = slot_of(j + 1);
 
         // ---------------- stage 1: row j ---------------------------------
         if (j <= r1) {
-            const uint32_t mj = (mk >> 3) & 7u, mn = mk & 7u;
-            {   // H + ssh of row j+1 at k0, k0+1, k0+2
-                const double2 h = pair(s_p1, R_H), e = pair(s_p1, R_SSH);
-                hqn.a = h.x + e.x;
-                hqn.b = h.y + e.y;
-                hqn.c = rightv(s_p1, R_H) + rightv(s_p1, R_SSH);
-            }
-            const double ku = CF(s_0, ku), ku2 = CF(s_0, ku2), wv0 = CF(s_0, wv0), wv1 = CF(s_0, wv1);
-            const double2 u = pair(s_0, R_U), v = pair(s_0, R_V);
-            const double hq0[3] = {hqc.a, hqc.b, hqc.c}, hq1[2] = {hqn.a, hqn.b};
-            double hu[2], hv[2];
-#pragma unroll
-            for (int e = 0; e < 2; e++) {
-                // Function/depth.f90:127-139 mask-weighted averages to u and v points
-                const int a = (mj >> e) & 1, b = (mj >> (e + 1)) & 1, c = (mn >> e) & 1;
-                hu[e] = (sel(a, hq0[e]) + sel(b, hq0[e + 1])) * (a & b ? ku2 : (a | b ? ku : 0.0));
-                hv[e] = (sel(a, hq0[e] * wv0) + sel(c, hq1[e] * wv1)) * (a & c ? 0.5 : (a | c ? 1.0 : 0.0));
-            }
-            s1n.hu0 = hu[0]; s1n.hu1 = hu[1]; s1n.hv0 = hv[0]; s1n.hv1 = hv[1];
-            s1n.U0 = u.x * hu[0];
-            s1n.U1 = u.y * hu[1];
-            s1n.V0 = v.x * hv[0];
-            s1n.V1 = v.y * hv[1];
+            const uint32_t mj = (mk >> 2) & 3u, mn = mk & 3u;
+            hqn.a = at(s_p1, R_H, 0) + at(s_p1, R_SSH, 0);
+            hqn.b = at(s_p1, R_H, 1) + at(s_p1, R_SSH, 1);
+            const int a = mj & 1, b = (mj >> 1) & 1, c = mn & 1;
+            // Function/depth.f90:127-139 mask-weighted averages to u and v points
+            const double hu = (sel(a, hqc.a) + sel(b, hqc.b)) * (a & b ? C_KU2(s_0) : (a | b ? C_KU(s_0) : 0.0));
+            const double hv = (sel(a, hqc.a * C_WV0(s_0)) + sel(c, hqn.a * C_WV1(s_0))) *
+                              (a & c ? 0.5 : (a | c ? 1.0 : 0.0));
+            s1n.hu = hu;
+            s1n.hv = hv;
+            s1n.U = at(s_0, R_U, 0) * hu;
+            s1n.V = at(s_0, R_V, 0) * hv;
+            const long long gi = (long long)j * p.pitch + k;
+            s1n.rx = p.rhsx[gi];
+            s1n.ry = p.rhsy[gi];
         }
-        s1n.Ul = SHFL_UP(s1n.U1);
-        s1n.Vr = SHFL_DN(s1n.V0);
+        s1n.Ul = SHFL_UP(s1n.U);
+        s1n.Vr = SHFL_DN(s1n.V);
 
         // ---------------- stage 2: row rho = j-1 -------------------------
-        const bool st2 = j >= r0 && j <= r1 + 1;
-        double FX0 = 0, FX1 = 0, FXr = 0, ST_r = 0, SNr = 0;
-        if (st2) {
-            const uint32_t mr = (mk >> 6) & 7u, mu_ = (mk >> 3) & 7u;   // rows rho, rho+1
+        double FX = 0.0, u_r = 0.0, up_r = 0.0;
+        if (j >= r0 && j <= r1 + 1) {
+            const uint32_t mr = (mk >> 4) & 3u, mu_ = (mk >> 2) & 3u;   // rows rho, rho+1
             const int sr = s_m1, sm = s_m2, su = s_0;
-            const double2 u_r = pair(sr, R_U), u_u = pair(su, R_U), v_r = pair(sr, R_V);
-            const double2 v_m = pair(sm, R_V), up_r = pair(sr, R_UP), up_u = pair(su, R_UP);
-            const double2 vp_r = pair(sr, R_VP), vp_m = pair(sm, R_VP), sp_r = pair(sr, R_SSHP);
-            const double ur[3] = {leftv(sr, R_U), u_r.x, u_r.y};     // u at k0-1, k0, k0+1
-            const double vr[3] = {v_r.x, v_r.y, rightv(sr, R_V)};    // v at k0, k0+1, k0+2
-            const double vpr[3] = {vp_r.x, vp_r.y, rightv(sr, R_VP)};
-            const double upr[3] = {leftv(sr, R_UP), up_r.x, up_r.y};
-            const double uu[2] = {u_u.x, u_u.y}, vm[2] = {v_m.x, v_m.y};
-            const double upu[2] = {up_u.x, up_u.y}, vpm[2] = {vp_m.x, vp_m.y};
-            const double spr[2] = {sp_r.x, sp_r.y};
-            const double Ur[3] = {s1c.Ul, s1c.U0, s1c.U1};           // U(rho) at k0-1, k0, k0+1
-            const double Vr[3] = {s1c.V0, s1c.V1, s1c.Vr};           // V(rho) at k0, k0+1, k0+2
-            const double Un[2] = {s1n.U0, s1n.U1};                   // U(rho+1)
-            const double Vm[2] = {s1p.V0, s1p.V1};                   // V(rho-1)
-            const double hqr[3] = {hqp.a, hqp.b, hqp.c}, hqu[3] = {hqc.a, hqc.b, hqc.c};
-            double mur[3] = {p.mu0, p.mu0, p.mu0}, muu[3] = {p.mu0, p.mu0, p.mu0}, wf[2] = {p.wq0, p.wq0};
-            if constexpr (F2D) {
-                const double2 a = pair(sr, R_MU), b = pair(su, R_MU), w = pair(sr, R_WF);
-                mur[0] = a.x; mur[1] = a.y; mur[2] = rightv(sr, R_MU);
-                muu[0] = b.x; muu[1] = b.y; muu[2] = rightv(su, R_MU);
-                wf[0] = w.x * p.inv_rho; wf[1] = w.y * p.inv_rho;
+            const int lc = mr & 1, lr = (mr >> 1) & 1, lu = mu_ & 1, lur = (mu_ >> 1) & 1;
+            const int luu = lc & lr & lu & lur;
+            u_r = at(sr, R_U, 0);
+            up_r = at(sr, R_UP, 0);
+            const double u_l = at(sr, R_U, -1), u_u = at(su, R_U, 0);
+            const double v_r = at(sr, R_V, 0), v_rr = at(sr, R_V, 1), v_m = at(sm, R_V, 0);
+            const double up_l = at(sr, R_UP, -1), up_u = at(su, R_UP, 0);
+            const double vp_r = at(sr, R_VP, 0), vp_rr = at(sr, R_VP, 1), vp_m = at(sm, R_VP, 0);
+            double mu_t = p.mu0, mu_h = p.mu0, wq = p.wq0;
+            if constexpr (GEN) {
+                mu_t = at(sr, R_MU, 0);
+                mu_h = (mu_t + at(sr, R_MU, 1) + at(su, R_MU, 0) + at(su, R_MU, 1)) * 0.25;
+                wq = at(sr, R_WF, 0) * p.inv_rho;
             }
-            const double c_u = CF(sr, c_u), c_v0 = CF(sr, c_v0), c_v1 = CF(sr, c_v1);
-            const double fx = CF(sr, fx), fy = CF(sr, fy), gx0 = CF(sr, gx0), gx1 = CF(sr, gx1);
-            const double gy0 = CF(sr, gy0), gy1 = CF(sr, gy1), wh0 = CF(sr, wh0), wh1 = CF(sr, wh1);
-            const double t1 = CF(sr, t1), t2 = CF(sr, t2), t3 = CF(sr, t3);
-            const double s1 = CF(sr, s1), s2 = CF(sr, s2), s3 = CF(sr, s3);
-            const double cor = coef(sr)->cor;
-            double sn[2], FX[2], FY[2], GX[2], GY[2], QU[2], QV[2], ST[2], SS[2];
-#pragma unroll
-            for (int e = 0; e < 2; e++) {
-                const int lc = (mr >> e) & 1, lr = (mr >> (e + 1)) & 1;
-                const int lu = (mu_ >> e) & 1, lur = (mu_ >> (e + 1)) & 1;
-                const int luu = lc & lr & lu & lur;
-                // vel_ssh.f90:491-494 continuity over 2*tau_inner
-                const double div = (Ur[e + 1] - Ur[e]) * c_u + Vr[e] * c_v0 - Vm[e] * c_v1;
-                sn[e] = sel(lc, spr[e] + two_ti * (wf[e] - div));
-                // vel_ssh.f90:63-73, :88-98 advective fluxes on T and h faces
-                FX[e] = (Ur[e] + Ur[e + 1]) * (ur[e] + ur[e + 1]) * fx;
-                FY[e] = sel(luu, (Vr[e] + Vr[e + 1]) * (ur[e + 1] + uu[e]) * fy);
-                GX[e] = (Ur[e + 1] * gx0 + Un[e] * gx1) * (vr[e] + vr[e + 1]);
-                GY[e] = (Vm[e] * gy0 + Vr[e] * gy1) * (vm[e] + vr[e]);
-                // depth.f90:141-147 depth on the h point
-                const double sa = sel(lc, hqr[e]) + sel(lr, hqr[e + 1]);
-                const double sb = sel(lu, hqu[e]) + sel(lur, hqu[e + 1]);
-                const double hh = (sa * wh0 + sb * wh1) * rcount(lc + lr + lu + lur);
-                // vel_ssh.f90:35-37 metric vorticity (zero on uniform grids) + Coriolis
-                double vort = 0.0;
+            // vel_ssh.f90:491-494 continuity over 2*tau_inner
+            const double div = GEN ? (s1c.U - s1c.Ul) * CG(sr, c_u) + s1c.V * CG(sr, c_v0) - s1p.V * CG(sr, c_v1)
+                                   : ((s1c.U - s1c.Ul) + (s1c.V - s1p.V)) * p.inv_d;
+            s2n.sn = sel(lc, at(sr, R_SSHP, 0) + two_ti * (wq - div));
+            // vel_ssh.f90:63-73, :88-98 advective fluxes on T and h faces
+            FX = (s1c.Ul + s1c.U) * (u_l + u_r) * C_D4(sr, fx);
+            s2n.FY = sel(luu, (s1c.V + s1c.Vr) * (u_r + u_u) * C_D4(sr, fy));
+            s2n.GX = (GEN ? s1c.U * CG(sr, gx0) + s1n.U * CG(sr, gx1) : (s1c.U + s1n.U) * p.d4) * (v_r + v_rr);
+            s2n.GY = (GEN ? s1p.V * CG(sr, gy0) + s1c.V * CG(sr, gy1) : (s1p.V + s1c.V) * p.d4) * (v_m + v_r);
+            // depth.f90:141-147 depth on the h point
+            const double sa = sel(lc, hqp.a) + sel(lr, hqp.b);
+            const double sb = sel(lu, hqc.a) + sel(lur, hqc.b);
+            const double hh = (GEN ? sa * CG(sr, wh0) + sb * CG(sr, wh1) : sa + sb) * rcount(lc + lr + lu + lur);
+            // vel_ssh.f90:35-37 metric vorticity (zero on uniform grids) + Coriolis
+            double cor;
+            if constexpr (GEN) {
+                cor = CG(sr, cor);
                 if (!p.vort_zero)
-                    vort = sel(luu, (vr[e + 1] - vr[e]) * CF(sr, vt0) - uu[e] * CF(sr, vt1) + ur[e + 1] * CF(sr, vt2));
-                const double Wh = hh * (cor + vort);
-                QU[e] = Wh * (vr[e] + vr[e + 1]);
-                QV[e] = Wh * (ur[e + 1] + uu[e]);
-                // mixing.f90:134-148 stresses from the previous level
-                const double str_t = sel(lc, t1 * (upr[e + 1] - upr[e]) - (t2 * vpr[e] - t3 * vpm[e]));
-                const double str_s = sel(luu, s1 * upu[e] - s2 * upr[e + 1] + s3 * (vpr[e + 1] - vpr[e]));
-                double mu_h = p.mu0;
-                if constexpr (F2D) mu_h = (mur[e] + mur[e + 1] + muu[e] + muu[e + 1]) * 0.25;
-                ST[e] = mur[e] * hqr[e] * str_t;
-                SS[e] = mu_h * hh * str_s;
+                    cor += sel(luu, (v_rr - v_r) * CG(sr, vt0) - u_u * CG(sr, vt1) + u_r * CG(sr, vt2));
+            } else {
+                cor = p.cor[j - 1];
             }
-            s2n.sn0 = sn[0]; s2n.sn1 = sn[1];
-            s2n.FY0 = FY[0]; s2n.FY1 = FY[1]; s2n.QU0 = QU[0]; s2n.QU1 = QU[1];
-            s2n.SS0 = SS[0]; s2n.SS1 = SS[1]; s2n.GX0 = GX[0]; s2n.GX1 = GX[1];
-            s2n.GY0 = GY[0]; s2n.GY1 = GY[1]; s2n.QV0 = QV[0]; s2n.QV1 = QV[1];
-            s2n.ST0 = ST[0]; s2n.ST1 = ST[1];
-            FX0 = FX[0]; FX1 = FX[1];
+            const double Wh = hh * cor;
+            s2n.QU = Wh * (v_r + v_rr);
+            s2n.QV = Wh * (u_r + u_u);
+            // mixing.f90:134-148 stresses from the previous level
+            const double str_t = GEN ? sel(lc, CG(sr, t1) * (up_r - up_l) - (CG(sr, t2) * vp_r - CG(sr, t3) * vp_m))
+                                     : sel(lc, ((up_r - up_l) - (vp_r - vp_m)) * p.inv_d);
+            const double str_s = GEN ? sel(luu, CG(sr, s1) * up_u - CG(sr, s2) * up_r + CG(sr, s3) * (vp_rr - vp_r))
+                                     : sel(luu, ((up_u - up_r) + (vp_rr - vp_r)) * p.inv_d);
+            s2n.ST = mu_t * hqp.a * str_t;
+            s2n.SS = mu_h * hh * str_s;
         }
-        FXr = SHFL_DN(FX0);
-        ST_r = SHFL_DN(s2n.ST0);
-        SNr = SHFL_DN(s2n.sn0);
-        s2n.GXl = SHFL_UP(s2n.GX1);
-        s2n.QVl = SHFL_UP(s2n.QV1);
-        s2n.SSl = SHFL_UP(s2n.SS1);
+        const double FXr = SHFL_DN(FX);
+        const double STr = SHFL_DN(s2n.ST);
+        const double SNr = SHFL_DN(s2n.sn);
+        s2n.GXl = SHFL_UP(s2n.GX);
+        s2n.QVl = SHFL_UP(s2n.QV);
+        s2n.SSl = SHFL_UP(s2n.SS);
 
         // ---------------- stage 3u: row rho = j-1 (u and SSH) -----------
-        const int rho = j - 1;
-        const uint32_t mr = (mk >> 6) & 7u;
-        const bool wr3u = j >= r0 + 1 && j <= r1 && __any_sync(0xffffffffu, (out0 || out1) && (mr & 3u));
-        if (wr3u) {
+        const uint32_t mr = (mk >> 4) & 3u;
+        if (j >= r0 + 1 && j <= r1 && __any_sync(0xffffffffu, out && (mr & 1u))) {
             const int sr = s_m1;
-            const double2 e_r = pair(sr, R_SSH), sp_r = pair(sr, R_SSHP), h_r = pair(sr, R_H);
-            const double e3[3] = {e_r.x, e_r.y, rightv(sr, R_SSH)};
-            const double sp3[3] = {sp_r.x, sp_r.y, rightv(sr, R_SSHP)};
-            const double h3[3] = {h_r.x, h_r.y, rightv(sr, R_H)};
-            const double2 u_r = pair(sr, R_U), up_r = pair(sr, R_UP), rx = pair(sr, R_RX);
-            const double u0[2] = {u_r.x, u_r.y}, up0[2] = {up_r.x, up_r.y}, rxv[2] = {rx.x, rx.y};
-            const double sn3[3] = {s2n.sn0, s2n.sn1, SNr};
-            const double FX3[3] = {FX0, FX1, FXr};
-            const double ST3[3] = {s2n.ST0, s2n.ST1, ST_r};
-            const double FYd[2] = {s2n.FY0 - s2o.FY0, s2n.FY1 - s2o.FY1};
-            const double QUs[2] = {s2n.QU0 + s2o.QU0, s2n.QU1 + s2o.QU1};
-            const double SSn[2] = {s2n.SS0, s2n.SS1}, SSo[2] = {s2o.SS0, s2o.SS1};
-            const double hu_c[2] = {s1c.hu0, s1c.hu1};
-            double rd3[3] = {p.rd0, p.rd0, p.rd0};
-            if constexpr (F2D) {
-                const double2 a = pair(sr, R_RD);
-                rd3[0] = a.x; rd3[1] = a.y; rd3[2] = rightv(sr, R_RD);
+            const int lc = mr & 1, lr = (mr >> 1) & 1;
+            const bool wu = out && (lc & lr), wt = out && lc;
+            const double e0 = at(sr, R_SSH, 0), e1 = at(sr, R_SSH, 1);
+            const double sp0 = at(sr, R_SSHP, 0), sp1 = at(sr, R_SSHP, 1);
+            const double h0 = at(sr, R_H, 0), h1 = at(sr, R_H, 1);
+            const double sn0 = s2n.sn;
+            // vel_ssh.f90:536-551
+            const double hu = s1c.hu;
+            const double hup = ((h0 + sp0) + (h1 + sp1)) * C_KU2(sr);
+            const double hun = ((h0 + sn0) + (h1 + SNr)) * C_KU2(sr);
+            const double slx = -(e1 - e0) * C_GD(sr, gdyh) * hu;
+            const double slxn = -(SNr - sn0) * C_GD(sr, gdyh) * hun;
+            const double adv = -((FXr - FX) + (s2n.FY - s2o.FY));
+            const double dif = GEN ? (STr - s2n.ST) * CG(sr, dux) + (s2n.SS * CG(sr, dus0) - s2o.SS * CG(sr, dus1))
+                                   : ((STr - s2n.ST) + (s2n.SS - s2o.SS)) * p.d;
+            double rd = p.rd0;
+            if constexpr (GEN) rd = (at(sr, R_RD, 0) + at(sr, R_RD, 1)) * 0.5;
+            const double grx = s1c.rx * rs + slx + dif + adv - rd * up_r * C_D2(sr, au) * hu
+                               + (s2n.QU + s2o.QU) * 0.25;
+            const double un = (up_r * hup + grx * (two_ti * C_INVD2(sr, rau))) * rcp_nr(hun);
+            bad |= (uint32_t)(wu && !(un < 100.0 && un > -100.0));
+            bad |= (uint32_t)(wt && !(sn0 < 10.0 && sn0 > -10.0));
+            const long long idx = (long long)(j - 1) * p.pitch + k;
+            if (ACC && wu) {
+                double a = (u_r * hu + un * hun) * p.c4, b = (slx + slxn) * p.c4;
+                if (ACC == 2) { a += p.acc[0][idx]; b += p.acc[2][idx]; }
+                p.acc[0][idx] = a;
+                p.acc[2][idx] = b;
             }
-            const double ku2 = CF(sr, ku2), gdyh = CF(sr, gdyh), dux = CF(sr, dux);
-            const double dus0 = CF(sr, dus0), dus1 = CF(sr, dus1), au = CF(sr, au);
-            const double cu = two_ti * CF(sr, rau);
-            const long long rowb = (long long)rho * p.pitch + k0;
-#pragma unroll
-            for (int e = 0; e < 2; e++) {
-                const bool oute = e == 0 ? out0 : out1;
-                const int lc = (mr >> e) & 1, lr = (mr >> (e + 1)) & 1;
-                const bool wu = oute && (lc & lr), wt = oute && lc;
-                // vel_ssh.f90:536-551
-                const double hu = hu_c[e];
-                const double hup = ((h3[e] + sp3[e]) + (h3[e + 1] + sp3[e + 1])) * ku2;
-                const double hun = ((h3[e] + sn3[e]) + (h3[e + 1] + sn3[e + 1])) * ku2;
-                const double slx = -(e3[e + 1] - e3[e]) * gdyh * hu;
-                const double slxn = -(sn3[e + 1] - sn3[e]) * gdyh * hun;
-                const double adv = -((FX3[e + 1] - FX3[e]) + FYd[e]);
-                const double dif = (ST3[e + 1] - ST3[e]) * dux + (SSn[e] * dus0 - SSo[e] * dus1);
-                const double rd = F2D ? (rd3[e] + rd3[e + 1]) * 0.5 : p.rd0;
-                const double grx = rxv[e] * rs + slx + dif + adv - rd * up0[e] * au * hu + QUs[e] * 0.25;
-                const double un = (up0[e] * hup + grx * cu) * rcp_nr(hun);
-                bad |= (uint32_t)(wu && !(un < 100.0 && un > -100.0));
-                bad |= (uint32_t)(wt && !(sn3[e] < 10.0 && sn3[e] > -10.0));
-                const long long idx = rowb + e;
-                if (p.acc_mode && wu) {
-                    double a = (u0[e] * hu + un * hun) * p.c4, b = (slx + slxn) * p.c4;
-                    if (p.acc_mode == 2) { a += p.acc[0][idx]; b += p.acc[2][idx]; }
-                    p.acc[0][idx] = a;
-                    p.acc[2][idx] = b;
-                }
-                if (p.write_state) {
-                    if (wu) {
-                        p.dst[S_UP][idx] = u0[e] + gam * (un - 2.0 * u0[e] + up0[e]);
-                        p.dst[S_U][idx] = un;
-                    }
-                    if (wt) {   // vel_ssh.f90:593-596
-                        p.dst[S_SSHP][idx] = e3[e] + gam * (sn3[e] - 2.0 * e3[e] + sp3[e]);
-                        p.dst[S_SSH][idx] = sn3[e];
-                    }
-                }
+            if (WRITE && wu) {
+                p.dst[S_UP][idx] = u_r + gam * (un - 2.0 * u_r + up_r);
+                p.dst[S_U][idx] = un;
+            }
+            if (WRITE && wt) {   // vel_ssh.f90:593-596
+                p.dst[S_SSHP][idx] = e0 + gam * (sn0 - 2.0 * e0 + sp0);
+                p.dst[S_SSH][idx] = sn0;
             }
         }
 
         // ---------------- stage 3v: row R = j-2 (v) ----------------------
-        const int R = j - 2;
-        const uint32_t mR = (mk >> 9) & 7u, mU = (mk >> 6) & 7u;   // rows R, R+1
-        const bool wr3v = j >= r0 + 2 && j <= r1 + 1 &&
-                          __any_sync(0xffffffffu, (out0 && (mR & mU & 1u)) || (out1 && (mR & mU & 2u)));
-        if (wr3v) {
+        const uint32_t mR = (mk >> 6) & 3u, mU = (mk >> 4) & 3u;   // rows R, R+1
+        if (j >= r0 + 2 && j <= r1 + 1 && __any_sync(0xffffffffu, out && (mR & mU & 1u))) {
             const int sR = s_m2, sU = s_m1;
-            const double2 eR = pair(sR, R_SSH), spR = pair(sR, R_SSHP), hR = pair(sR, R_H);
-            const double2 eU = pair(sU, R_SSH), spU = pair(sU, R_SSHP), hU = pair(sU, R_H);
-            const double2 v_R = pair(sR, R_V), vp_R = pair(sR, R_VP), ry = pair(sR, R_RY);
-            const double e0[2] = {eR.x, eR.y}, sp0[2] = {spR.x, spR.y}, h0[2] = {hR.x, hR.y};
-            const double e1[2] = {eU.x, eU.y}, sp1[2] = {spU.x, spU.y}, h1[2] = {hU.x, hU.y};
-            const double v0[2] = {v_R.x, v_R.y}, vp0[2] = {vp_R.x, vp_R.y}, ryv[2] = {ry.x, ry.y};
-            const double sn0[2] = {s2o.sn0, s2o.sn1}, sn1[2] = {s2n.sn0, s2n.sn1};
-            const double GX3[3] = {s2o.GXl, s2o.GX0, s2o.GX1};
-            const double QV3[3] = {s2o.QVl, s2o.QV0, s2o.QV1};
-            const double SS3[3] = {s2o.SSl, s2o.SS0, s2o.SS1};
-            const double GYd[2] = {s2n.GY0 - s2o.GY0, s2n.GY1 - s2o.GY1};
-            const double STo[2] = {s2o.ST0, s2o.ST1}, STn[2] = {s2n.ST0, s2n.ST1};
-            const double hv_c[2] = {s1p.hv0, s1p.hv1};
-            double rdR[2] = {p.rd0, p.rd0}, rdU[2] = {p.rd0, p.rd0};
-            if constexpr (F2D) {
-                const double2 a = pair(sR, R_RD), b = pair(sU, R_RD);
-                rdR[0] = a.x; rdR[1] = a.y; rdU[0] = b.x; rdU[1] = b.y;
+            const bool wv = out && (mR & mU & 1u);
+            const double e0 = at(sR, R_SSH, 0), e1 = at(sU, R_SSH, 0);
+            const double sp0 = at(sR, R_SSHP, 0), sp1 = at(sU, R_SSHP, 0);
+            const double h0 = at(sR, R_H, 0), h1 = at(sU, R_H, 0);
+            const double v0 = at(sR, R_V, 0), vp0 = at(sR, R_VP, 0);
+            const double sn0 = s2o.sn, sn1 = s2n.sn;
+            // vel_ssh.f90:554-569
+            const double hv = s1p.hv;
+            const double hvp = (GEN ? (h0 + sp0) * CG(sR, wv0) + (h1 + sp1) * CG(sR, wv1) : (h0 + sp0) + (h1 + sp1)) * 0.5;
+            const double hvn = (GEN ? (h0 + sn0) * CG(sR, wv0) + (h1 + sn1) * CG(sR, wv1) : (h0 + sn0) + (h1 + sn1)) * 0.5;
+            const double sly = -(e1 - e0) * C_GD(sR, gdxh) * hv;
+            const double slyn = -(sn1 - sn0) * C_GD(sR, gdxh) * hvn;
+            const double adv = -((s2o.GX - s2o.GXl) + (s2n.GY - s2o.GY));
+            const double dif = GEN ? -(s2n.ST * CG(sR, dvt1) - s2o.ST * CG(sR, dvt0)) + (s2o.SS - s2o.SSl) * CG(sR, dvs)
+                                   : (-(s2n.ST - s2o.ST) + (s2o.SS - s2o.SSl)) * p.d;
+            double rd = p.rd0;
+            if constexpr (GEN) rd = (at(sR, R_RD, 0) + at(sU, R_RD, 0)) * 0.5;
+            const double gry = s1p.ry * rs + sly + dif + adv - rd * vp0 * C_D2(sR, av) * hv
+                               - (s2o.QV + s2o.QVl) * 0.25;
+            const double vn = (vp0 * hvp + gry * (two_ti * C_INVD2(sR, rav))) * rcp_nr(hvn);
+            bad |= (uint32_t)(wv && !(vn < 100.0 && vn > -100.0));
+            const long long idx = (long long)(j - 2) * p.pitch + k;
+            if (ACC && wv) {
+                double a = (v0 * hv + vn * hvn) * p.c4, b = (sly + slyn) * p.c4;
+                if (ACC == 2) { a += p.acc[1][idx]; b += p.acc[3][idx]; }
+                p.acc[1][idx] = a;
+                p.acc[3][idx] = b;
             }
-            const double wv0 = CF(sR, wv0), wv1 = CF(sR, wv1), gdxh = CF(sR, gdxh);
-            const double dvt0 = CF(sR, dvt0), dvt1 = CF(sR, dvt1), dvs = CF(sR, dvs), av = CF(sR, av);
-            const double cv = two_ti * CF(sR, rav);
-            const long long rowb = (long long)R * p.pitch + k0;
-#pragma unroll
-            for (int e = 0; e < 2; e++) {
-                const bool oute = e == 0 ? out0 : out1;
-                const bool wv = oute && ((mR >> e) & (mU >> e) & 1u);
-                // vel_ssh.f90:554-569
-                const double hv = hv_c[e];
-                const double hvp = ((h0[e] + sp0[e]) * wv0 + (h1[e] + sp1[e]) * wv1) * 0.5;
-                const double hvn = ((h0[e] + sn0[e]) * wv0 + (h1[e] + sn1[e]) * wv1) * 0.5;
-                const double sly = -(e1[e] - e0[e]) * gdxh * hv;
-                const double slyn = -(sn1[e] - sn0[e]) * gdxh * hvn;
-                const double adv = -((GX3[e + 1] - GX3[e]) + GYd[e]);
-                const double dif = -(STn[e] * dvt1 - STo[e] * dvt0) + (SS3[e + 1] - SS3[e]) * dvs;
-                const double rd = F2D ? (rdR[e] + rdU[e]) * 0.5 : p.rd0;
-                const double gry = ryv[e] * rs + sly + dif + adv - rd * vp0[e] * av * hv
-                                   - (QV3[e + 1] + QV3[e]) * 0.25;
-                const double vn = (vp0[e] * hvp + gry * cv) * rcp_nr(hvn);
-                bad |= (uint32_t)(wv && !(vn < 100.0 && vn > -100.0));
-                const long long idx = rowb + e;
-                if (p.acc_mode && wv) {
-                    double a = (v0[e] * hv + vn * hvn) * p.c4, b = (sly + slyn) * p.c4;
-                    if (p.acc_mode == 2) { a += p.acc[1][idx]; b += p.acc[3][idx]; }
-                    p.acc[1][idx] = a;
-                    p.acc[3][idx] = b;
-                }
-                if (p.write_state && wv) {
-                    p.dst[S_VP][idx] = v0[e] + gam * (vn - 2.0 * v0[e] + vp0[e]);
-                    p.dst[S_V][idx] = vn;
-                }
+            if (WRITE && wv) {
+                p.dst[S_VP][idx] = v0 + gam * (vn - 2.0 * v0 + vp0);
+                p.dst[S_V][idx] = vn;
             }
         }
         // row j-2 was last read above: once every lane is past it, its slot
@@ -509,36 +436,23 @@ __global__ void __launch_bounds__(NL, CTAS_PER_SM) k_substep(const __grid_consta
         }
     };
 
+    // H + ssh of row r0-1, the stage-1 "current" row of the first step
+    HQ HA{}, HB{}, HC{};
+    wait_upto(row_lo + 1);
+    if (ok) {
+        const int s = slot_of(r0 - 1);
+        HC.a = at(s, R_H, 0) + at(s, R_SSH, 0);
+        HC.b = at(s, R_H, 1) + at(s, R_SSH, 1);
+    }
     // three instances of each carried struct, renamed (not copied) by the
     // three-fold unrolled loop
     S1 A{}, B{}, C{};
-    HQ HA{}, HB{}, HC{};
     S2 X{}, Y{}, Z{};
-    {   // H + ssh of row r0-1 (the stage-1 "current" row of the first step)
-        const int need = row_lo + 1;
-        while (waited < need && ok) {
-            const int row = waited + 1;
-            if (!mbar_wait(&mbar[slot_of(row)], (uint32_t)(((row - row_lo) / RING) & 1))) { ok = false; break; }
-            waited = row;
-            mk = (mk << 3) | mask3(slot_of(row));
-        }
-        ok = __all_sync(0xffffffffu, ok);
-        if (ok) {
-            const int s = slot_of(r0 - 1);
-            const double2 h = pair(s, R_H), e = pair(s, R_SSH);
-            HC.a = h.x + e.x;
-            HC.b = h.y + e.y;
-            HC.c = rightv(s, R_H) + rightv(s, R_SSH);
-        }
-    }
-    // mk now holds rows r0-2 (bits 3-5) and r0-1 (bits 0-2); the first step
-    // pushes row r0 so that row j+1 = r0 sits in bits 0-2
     for (int j = r0 - 1; j <= r1 + 1 && ok; j += 3) {
         step(j, A, C, B, HA, HC, HB, X, Z);
         step(j + 1, B, A, C, HB, HA, HC, Y, X);
         step(j + 2, C, B, A, HC, HB, HA, Z, Y);
     }
-#undef CF
     if (__any_sync(0xffffffffu, bad != 0) && l == 0) atomicOr(p.flags, FLAG_GUARD);
     if (!ok && l == 0) {
         atomicOr(p.flags, FLAG_TIMEOUT);
@@ -546,6 +460,15 @@ __global__ void __launch_bounds__(NL, CTAS_PER_SM) k_substep(const __grid_consta
         for (int row = max(waited + 1, row_lo); row <= issued; row++)
             (void)mbar_wait(&mbar[slot_of(row)], (uint32_t)(((row - row_lo) / RING) & 1));
     }
+#undef CG
+#undef C_KU
+#undef C_KU2
+#undef C_WV0
+#undef C_WV1
+#undef C_D4
+#undef C_GD
+#undef C_D2
+#undef C_INVD2
 }
 
 // min/max over the ocean points of three fields, for the uniform-forcing test
@@ -611,7 +534,7 @@ int forcing_mode(Plan &p, const Dom &d, const Consts &c, double *forc[6], cudaSt
     return 0;
 }
 
-Params base_params(const Plan &p, const Dom &d, const Consts &c, double *forc[6], const Forcing &f)
+Params base_params(const Plan &p, const Dom &d, const Consts &c, double *forc[6], const Forcing &f, int gen)
 {
     Params q{};
     q.H = p.hrest;
@@ -622,10 +545,9 @@ Params base_params(const Plan &p, const Dom &d, const Consts &c, double *forc[6]
     q.rdis = forc[5];
     q.bits = p.bits;
     q.rows = p.rows;
-    q.rc = p.rc;
+    q.cor = p.cor;
     q.pitch = d.pitch;
     q.bm_words = p.bm_words;
-    q.chunk_rows = p.chunk_rows;
     q.r_first = d.ny_start - d.bnd_y1;
     q.r_last = d.ny_end - d.bnd_y1;
     q.c_first = d.nx_start - d.bnd_x1 + d.xoff;
@@ -637,23 +559,40 @@ Params base_params(const Plan &p, const Dom &d, const Consts &c, double *forc[6]
     q.rhs_scale = 1.0;
     q.vort_zero = p.vort_zero ? 1 : 0;
     q.flags = p.d_flags;
+    q.d = p.d;
+    q.inv_d = p.d != 0.0 ? 1.0 / p.d : 0.0;
+    q.d4 = p.d / 4.0;
+    q.gd = c.g * p.d;
+    q.d2 = p.d * p.d;
+    q.inv_d2 = p.d != 0.0 ? 1.0 / (p.d * p.d) : 0.0;
+    q.chunk_rows = p.chunk_rows[gen];
     return q;
 }
 
-template <bool F2D, bool RV>
+template <bool GEN, int MODE>
 void launch_t(const Plan &p, const Params &q, cudaStream_t s)
 {
-    dim3 grid(p.nstrips, p.nchunks);
-    k_substep<F2D, RV><<<grid, NL, Layout<F2D>::bytes, s>>>(q);
+    dim3 grid(p.nstrips, p.nchunks[GEN ? 1 : 0]);
+    k_substep<GEN, MODE><<<grid, NL, Layout<GEN>::bytes, s>>>(q);
 }
 
-void launch(const Plan &p, const Params &q, bool f2d, cudaStream_t s)
+// mode = acc + 3*write (acc: 0 none, 1 write, 2 accumulate)
+template <bool GEN>
+void launch_g(const Plan &p, const Params &q, int mode, cudaStream_t s)
 {
-    if (f2d) {
-        if (p.rowvar) launch_t<true, true>(p, q, s); else launch_t<true, false>(p, q, s);
-    } else {
-        if (p.rowvar) launch_t<false, true>(p, q, s); else launch_t<false, false>(p, q, s);
+    switch (mode) {
+    case 3: launch_t<GEN, 3>(p, q, s); break;
+    case 4: launch_t<GEN, 4>(p, q, s); break;
+    case 5: launch_t<GEN, 5>(p, q, s); break;
+    default: launch_t<GEN, 2>(p, q, s); break;
     }
+}
+
+void launch(Plan &p, const Params &q, int gen, int mode, cudaStream_t s)
+{
+    p.last_variant = gen;
+    if (gen) launch_g<true>(p, q, mode, s);
+    else launch_g<false>(p, q, mode, s);
 }
 
 int sync_buffers(Plan &p, const Dom &d, double *state[6], cudaStream_t s)
@@ -676,11 +615,17 @@ int read_flags(Plan &p, cudaStream_t s, unsigned *out)
     return 0;
 }
 
-template <bool F2D, bool RV>
+template <bool GEN, int MODE>
+int set_smem1()
+{
+    return cudaFuncSetAttribute(k_substep<GEN, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                (int)Layout<GEN>::bytes) != cudaSuccess;
+}
+
 int set_smem()
 {
-    return cudaFuncSetAttribute(k_substep<F2D, RV>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)Layout<F2D>::bytes) != cudaSuccess;
+    return set_smem1<false, 2>() | set_smem1<false, 3>() | set_smem1<false, 4>() | set_smem1<false, 5>() |
+           set_smem1<true, 2>() | set_smem1<true, 3>() | set_smem1<true, 4>() | set_smem1<true, 5>();
 }
 
 }  // namespace
@@ -689,7 +634,7 @@ int set_smem()
 Plan make_plan(const inmsom_bounds &b)
 {
     Plan p;
-    p.ncol = NCOL;
+    p.ncol = NL;
     p.outw = OUTW;
     const int nx = b.nx_end - b.nx_start + 1;
     p.nstrips = (nx + p.outw - 1) / p.outw;
@@ -807,15 +752,15 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
         q.rav = 1.0 / q.av;
     }
     p.vort_zero = vz;
-    // rows identical except for cor -> the coefficients go in the kernel
-    // parameters and only cor is read per row
-    p.rowvar = false;
-    for (int r = 1; r < nya && !p.rowvar; r++) {
-        RowCoef a = rows[r], b = rows[0];
-        a.cor = b.cor = 0.0;
-        p.rowvar = std::memcmp(&a, &b, sizeof(RowCoef)) != 0;
-    }
-    p.rc = rows[d.ny_start - d.bnd_y1];
+    // square uniform grid: every metric array equal to one spacing over the
+    // points the step reads -> the UNI variant with folded coefficients
+    p.uni = true;
+    p.d = row_of(DX, d.ny_start);
+    for (int k = 0; k < 8 && p.uni; k++)
+        for (int n = d.ny_start - 1; n <= d.ny_end + 1 && p.uni; n++)
+            if (row_of(k, n) != p.d) p.uni = false;
+    std::vector<double> cor(nya);
+    for (int r = 0; r < nya; r++) cor[r] = row_of(RLH, r + d.bnd_y1) * p.d * p.d;
     // 1-bit T mask indexed by device column, rows padded so that every CTA
     // window (8 words from a 4-word boundary) lies inside the row
     p.bm_words = (int)(((d.pitch + 31) / 32 + 8 + 3) / 4 * 4);
@@ -830,6 +775,9 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
 
     if (cudaMalloc(&p.rows, rows.size() * sizeof(RowCoef)) != cudaSuccess) return 1;
     if (cudaMemcpyAsync(p.rows, rows.data(), rows.size() * sizeof(RowCoef), cudaMemcpyHostToDevice, s) != cudaSuccess)
+        return 1;
+    if (cudaMalloc(&p.cor, cor.size() * sizeof(double)) != cudaSuccess) return 1;
+    if (cudaMemcpyAsync(p.cor, cor.data(), cor.size() * sizeof(double), cudaMemcpyHostToDevice, s) != cudaSuccess)
         return 1;
     if (cudaMalloc(&p.bits, bits.size() * sizeof(uint32_t)) != cudaSuccess) return 1;
     if (cudaMemcpyAsync(p.bits, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s) != cudaSuccess)
@@ -846,24 +794,28 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
     p.hrest = d_hrest;
     p.lu = d_lu;
     p.buffers_synced = false;
-    if (set_smem<false, false>() || set_smem<false, true>() || set_smem<true, false>() || set_smem<true, true>())
-        return 1;
-    int dev = 0, nsm = 148, occ = 1;
+    if (set_smem()) return 1;
+    int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_substep<false, false>, NL,
-                                                      Layout<false>::bytes) != cudaSuccess || occ < 1)
-        occ = 1;
     p.nsm = nsm;
+    int occ[2] = {1, 1};
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], k_substep<false, 3>, NL, Layout<false>::bytes) !=
+            cudaSuccess || occ[0] < 1)
+        occ[0] = 1;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], k_substep<true, 3>, NL, Layout<true>::bytes) !=
+            cudaSuccess || occ[1] < 1)
+        occ[1] = 1;
     // one wave: strips x chunks <= SMs x resident CTAs, chunks as tall as
     // that allows; each chunk re-reads and recomputes three rows of warm-up,
     // so keep chunks at least 16 rows tall
     const int ny = d.ny_end - d.ny_start + 1;
-    const int slots = nsm * occ;
-    int nchunks = std::max(1, slots / p.nstrips);
-    nchunks = std::min(nchunks, std::max(1, (ny + 15) / 16));
-    p.chunk_rows = (ny + nchunks - 1) / nchunks;
-    p.nchunks = (ny + p.chunk_rows - 1) / p.chunk_rows;
+    for (int v = 0; v < 2; v++) {
+        int nchunks = std::max(1, nsm * occ[v] / p.nstrips);
+        nchunks = std::min(nchunks, std::max(1, (ny + 15) / 16));
+        p.chunk_rows[v] = (ny + nchunks - 1) / nchunks;
+        p.nchunks[v] = (ny + p.chunk_rows[v] - 1) / p.chunk_rows[v];
+    }
     return 0;
 }
 
@@ -877,7 +829,8 @@ int dynamics(Plan &p, const Dom &d, const Consts &c, double tau, int nstep, doub
     const size_t fb = (size_t)d.pitch * d.nya() * sizeof(double);
     for (int k = 0; k < 4; k++)
         if (cudaMemsetAsync(acc[k], 0, fb, s) != cudaSuccess) return 1;   // vel_ssh.f90:479-482
-    Params q = base_params(p, d, c, forc, f);
+    const int gen = (p.uni && f.uniform) ? 0 : 1;
+    Params q = base_params(p, d, c, forc, f, gen);
     const double ti = tau / (double)nstep;
     q.two_ti = 2.0 * ti;
     q.gam = c.ts / 2.0 / (double)nstep;
@@ -891,9 +844,7 @@ int dynamics(Plan &p, const Dom &d, const Consts &c, double tau, int nstep, doub
             q.src[k] = odd ? state[k] : p.buf[0][k];
             q.dst[k] = odd ? p.buf[0][k] : state[k];
         }
-        q.acc_mode = step == 1 ? 1 : 2;
-        q.write_state = 1;
-        launch(p, q, !f.uniform, s);
+        launch(p, q, gen, step == 1 ? 4 : 5, s);
         if (cudaGetLastError() != cudaSuccess) return 1;
     }
     if (nstep & 1)
@@ -905,9 +856,7 @@ int dynamics(Plan &p, const Dom &d, const Consts &c, double tau, int nstep, doub
             q.src[k] = k2 == 1 ? state[k] : ((k2 & 1) ? p.buf[1][k] : p.buf[0][k]);
             q.dst[k] = (k2 & 1) ? p.buf[0][k] : p.buf[1][k];
         }
-        q.acc_mode = 2;
-        q.write_state = k2 < nstep ? 1 : 0;
-        launch(p, q, !f.uniform, s);
+        launch(p, q, gen, k2 < nstep ? 5 : 2, s);
         if (cudaGetLastError() != cudaSuccess) return 1;
     }
     unsigned flags = 0;
@@ -923,12 +872,11 @@ int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt, co
     if (forcing_mode(p, d, c, forc, s, f)) return 1;
     if (!p.buffers_synced && sync_buffers(p, d, state, s)) return 1;
     if (cudaMemsetAsync(p.d_flags, 0, sizeof(unsigned), s) != cudaSuccess) return 1;
-    Params q = base_params(p, d, c, forc, f);
+    const int gen = (p.uni && f.uniform) ? 0 : 1;
+    Params q = base_params(p, d, c, forc, f, gen);
     q.two_ti = 2.0 * dt;
     q.gam = c.ts / 2.0;   // nstep = 1
     q.c4 = 0.25;
-    q.acc_mode = 0;
-    q.write_state = 1;
     for (int k = 0; k < 4; k++) q.acc[k] = nullptr;
     for (int step = 0; step < nsub; step++) {
         for (int k = 0; k < 6; k++) {
@@ -936,7 +884,7 @@ int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt, co
             q.dst[k] = (step & 1) ? state[k] : p.buf[0][k];
         }
         q.rhs_scale = rhs_scale ? rhs_scale[step] : 1.0;
-        launch(p, q, !f.uniform, s);
+        launch(p, q, gen, 3, s);
         if (cudaGetLastError() != cudaSuccess) return 1;
     }
     if (nsub & 1)
@@ -950,6 +898,7 @@ int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt, co
 void free_plan(Plan &p)
 {
     cudaFree(p.rows);
+    cudaFree(p.cor);
     cudaFree(p.bits);
     for (auto &b : p.buf)
         for (auto &x : b) cudaFree(x);

@@ -53,18 +53,20 @@ struct RowCoef {
 static_assert(sizeof(RowCoef) % 16 == 0, "RowCoef must be a multiple of 16 bytes");
 
 struct Plan {
-    int ncol = 64;            // columns per CTA (one warp, two columns per lane)
-    int outw = 62;            // output columns per CTA
-    int nstrips = 0, nchunks = 0, chunk_rows = 0;
-    bool rowvar = true;       // coefficients vary along y (else all rows but cor equal)
-    RowCoef rc{};             // the row-invariant coefficients when !rowvar
+    int ncol = 32;            // columns per CTA (one warp, one column per lane)
+    int outw = 30;            // output columns per CTA
+    int nstrips = 0;
+    int nchunks[2] = {0, 0}, chunk_rows[2] = {0, 0};   // per variant: uniform, general
+    bool uni = false;         // metrics all equal one spacing d (square uniform grid)
+    double d = 0.0;           // that spacing
     long long min_pitch = 0;  // device row pitch the strips need
     // device data
-    RowCoef *rows = nullptr;
+    RowCoef *rows = nullptr;        // per-row coefficients (general variant)
+    double *cor = nullptr;          // per-row rlh_s*d*d (uniform variant)
     uint32_t *bits = nullptr;       // 1-bit T mask, bm_words per row
     int bm_words = 0;
     double *buf[2][6] = {};         // extra state sets (ping-pong)
-    double *d_uniform = nullptr;    // min/max of mu, rdis, wflux (6 doubles)
+    double *d_uniform = nullptr;    // per-block min/max of mu, rdis, wflux
     unsigned *d_flags = nullptr;    // [0] status bits (guard / timeout)
     const double *hrest = nullptr;  // borrowed
     const float *lu = nullptr;      // borrowed
@@ -72,6 +74,7 @@ struct Plan {
     bool vort_zero = false;
     bool buffers_synced = false;    // buf[][] hold the state's land/halo values
     unsigned last_flags = 0;        // status bits of the last run
+    int last_variant = -1;          // 0 uniform, 1 general (last launch)
 };
 
 enum : unsigned { FLAG_TIMEOUT = 1u, FLAG_GUARD = 2u };
