@@ -169,6 +169,50 @@ int inmsom_guard(inmsom_ctx *ctx, long *nbad);
  * from ssh.  FP64, deterministic (fixed reduction order). */
 int inmsom_gpu_diag(inmsom_ctx *ctx, double *volume, double *energy);
 
+/* Largest interior row count (ny_end - ny_start + 1) that
+ * inmsom_diag_noalloc accepts.  Its scratch is a fixed array of
+ * 2 * INMSOM_DIAG_NOALLOC_MAX_ROWS doubles (256 KiB) in the library's device
+ * image, which every GPU that loads that image holds until the process
+ * exits. */
+#define INMSOM_DIAG_NOALLOC_MAX_ROWS 16384
+
+/* The volume/energy diagnostic of inmsom_gpu_diag without a context and
+ * without allocating anything.  No counterpart in the reference: it exists
+ * for callers that cannot allocate GPU memory -- a host model that gives all
+ * device memory to its own pool at start-up, or one that must not call
+ * cudaMalloc/cudaFree mid-step because those calls synchronise the device
+ * and stall the model's streams.
+ *
+ * Array arguments are DEVICE pointers to f(bnd_x1:bnd_x2, bnd_y1:bnd_y2),
+ * x fastest, consecutive rows `ld` elements apart (ld >= bnd_x2-bnd_x1+1):
+ * masks lu, lcu, lcv; metrics dx, dy, dxt, dyt, dxh, dyh; rest depth
+ * hhq_rest; state ssh, u, v; u/v-point depths hu, hv (hhu_e, hhv_e of
+ * hh_init for this ssh).  `out` is a device pointer to two doubles that
+ * receive the volume and the energy, defined as for inmsom_gpu_diag; only
+ * free_fall_acc of `c` is used.  The call enqueues its two kernels on
+ * `stream` (a cudaStream_t of the current device, NULL for its default
+ * stream) and returns without waiting; `out` holds the result once the
+ * stream has reached that point.
+ *
+ * It runs on the calling thread's current device and calls no cudaMalloc,
+ * cudaFree or other allocating routine.  Its scratch, the per-row partial
+ * sums, is the fixed array described above, shared by every call on a
+ * device: each call writes every partial it later reads, so nothing is
+ * cleared, but calls whose work overlaps on the GPU (unordered streams)
+ * race on that array and may return wrong sums -- order them on one stream
+ * or with events.  The first call on each device looks up the array's
+ * device address (cudaGetSymbolAddress); make that first call before any
+ * stream capture begins.  More than INMSOM_DIAG_NOALLOC_MAX_ROWS interior
+ * rows returns INMSOM_EARG without touching the device.  An empty interior
+ * gives volume = energy = 0. */
+int inmsom_diag_noalloc(const inmsom_bounds *b, const inmsom_consts *c, long long ld,
+                        const float *lu, const float *lcu, const float *lcv,
+                        const double *dx, const double *dy, const double *dxt,
+                        const double *dyt, const double *dxh, const double *dyh,
+                        const double *hhq_rest, const double *ssh, const double *u,
+                        const double *v, const double *hu, const double *hv,
+                        double *out, void *stream);
+
 /* Residency control for INMSOM_RESIDENT contexts: which host arrays to
  * refresh (to_host) or re-upload (from_host), using the pointers of the last
  * inmsom_barotropic_dynamics call and of inmsom_gpu_register_grid. */

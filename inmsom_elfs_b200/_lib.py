@@ -23,7 +23,11 @@ EXPORTS = (
     "inmsom_hh_init_external", "inmsom_guard", "inmsom_gpu_diag",
     "inmsom_gpu_sync_to_host", "inmsom_gpu_sync_from_host", "inmsom_run_substeps",
     "inmsom_gpu_path", "inmsom_gpu_finalize", "inmsom_gpu_last_error", "inmsom_load_state",
+    "inmsom_diag_noalloc",
 )
+
+# include/inmsom_gpu.h: INMSOM_DIAG_NOALLOC_MAX_ROWS
+DIAG_NOALLOC_MAX_ROWS = 16384
 
 
 class InmsomError(RuntimeError):
@@ -78,6 +82,8 @@ def load() -> ctypes.CDLL:
     lib.inmsom_load_state.argtypes = [VP] + [DP] * 12
     lib.inmsom_gpu_path.argtypes = [VP, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_char_p)]
     lib.inmsom_gpu_finalize.argtypes = [VP]
+    lib.inmsom_diag_noalloc.argtypes = ([ctypes.POINTER(CBounds), ctypes.POINTER(CConsts),
+                                         ctypes.c_longlong] + [VP] * 16 + [VP])
     for name in EXPORTS:
         if name != "inmsom_gpu_last_error":
             getattr(lib, name).restype = i

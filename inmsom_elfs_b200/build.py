@@ -25,6 +25,7 @@ SOURCES = {
     "general.cu": ["--fmad=false"],
     "fused.cu": [],
     "capi.cu": [],
+    "noalloc.cu": [],
 }
 HEADERS = ["common.cuh", "general.h", "fused.h"]
 

@@ -59,6 +59,12 @@ enum { I_SSH, I_SSHP, I_U, I_V, I_WFLUX, I_NEW, I_HQN, I_HUN, I_HVN, I_HHN, NINT
 
 }  // namespace
 
+namespace inmsom {
+// Sets the message of inmsom_gpu_last_error() for entry points defined in
+// other source files of the library.
+int record_error(int code, const char *msg) { return set_err(code, "%s", msg); }
+}  // namespace inmsom
+
 struct inmsom_ctx {
     Dom dom{};
     Consts c{};
