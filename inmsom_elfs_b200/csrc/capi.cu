@@ -179,6 +179,19 @@ int sync_stream(inmsom_ctx *c)
     return INMSOM_OK;
 }
 
+// n fields in ONE allocation, field k at arr[0] + k * pitch * rows (the
+// fused path's tensor maps read a state set as one block)
+int alloc_block(inmsom_ctx *c, double **arr, int n)
+{
+    if (arr[0]) return INMSOM_OK;
+    const size_t f = (size_t)c->dom.pitch * (size_t)c->dom.nya();
+    double *b = nullptr;
+    CK(cudaMalloc((void **)&b, (size_t)n * f * sizeof(double)));
+    CK(cudaMemsetAsync(b, 0, (size_t)n * f * sizeof(double), c->stream));
+    for (int k = 0; k < n; k++) arr[k] = b + k * f;
+    return INMSOM_OK;
+}
+
 int alloc_set(inmsom_ctx *c, double **arr, int n)
 {
     for (int k = 0; k < n; k++)
@@ -335,7 +348,7 @@ int inmsom_gpu_finalize(inmsom_ctx *c)
     for (auto &p : c->mask) cudaFree(p);
     for (auto &p : c->met) cudaFree(p);
     for (auto &p : c->depth) cudaFree(p);
-    for (auto &p : c->state) cudaFree(p);
+    cudaFree(c->state[0]);   // one block (see alloc_block)
     for (auto &p : c->work) cudaFree(p);
     for (auto &p : c->acc) cudaFree(p);
     for (auto &p : c->forc) cudaFree(p);
@@ -390,7 +403,7 @@ int inmsom_gpu_register_grid(inmsom_ctx *c, const float *lu, const float *luu, c
         if (hd[k]) CKR(h2d(c, c->depth[k], (const double *)hd[k]));
     }
     c->depths_current = ndepth == NDEPTH;
-    CKR(alloc_set(c, c->state, NSTATE));
+    CKR(alloc_block(c, c->state, NSTATE));
     CKR(alloc_set(c, c->work, NWORK));
     CKR(alloc_set(c, c->acc, NACC));
     CKR(alloc_set(c, c->forc, NFORC));
@@ -409,7 +422,7 @@ int inmsom_gpu_register_grid(inmsom_ctx *c, const float *lu, const float *luu, c
     } else {
         c->fused_reason = fused::check_eligible(c->plan, c->dom, c->c, hm, hg);
         if (!c->fused_reason) {
-            CKR(fused::setup(c->plan, c->dom, c->c, hm, hg, c->met[G_HREST], c->mask[M_LU], c->stream) == 0
+            CKR(fused::setup(c->plan, c->dom, c->c, hm, hg, c->met[G_HREST], c->mask[M_LU], c->state, c->stream) == 0
                     ? INMSOM_OK
                     : set_err(INMSOM_ECUDA, "fused path set-up failed: %s",
                               cudaGetErrorString(cudaGetLastError())));

@@ -3,30 +3,34 @@
 // Work decomposition.  A CTA is one warp; lane l owns device column
 // k = g0+2+l of a 32-column strip starting at device column g0+2
 // (g0 = 30*strip, even).  Strip columns 1..30 are written, so strips overlap
-// by two columns.  The CTA marches down a chunk of rows [r0, r1); iteration
-// j of its row loop computes
+// by two columns.  The CTA marches down a chunk of rows; iteration j of its
+// row loop computes
 //   stage 1,  row j  : u/v-point depths of the current level, the transports
-//                      U = u*hu and V = v*hv, and loads the forcing of row j;
+//                      U = u*hu and V = v*hv, and the row's forcing, pressure
+//                      gradient and drag terms of the u and v equations;
 //   stage 2,  row j-1: new SSH (continuity), advective fluxes on T and h
 //                      points, Coriolis-plus-metric-vorticity products,
 //                      tension and shear stresses times viscosity and depth;
 //   stage 3u, row j-1: u momentum and the SSH update (time-mean sums,
 //                      Robert-Asselin filter and time shift, stores);
 //   stage 3v, row j-2: the same for v (it needs stage 2 of the row above).
-// A value needed from a neighbouring column comes from the neighbouring lane
-// by a warp shuffle; values of earlier rows stay in registers, in three
-// instances of each per-row struct that the three-fold unrolled row loop
-// renames instead of copying.  There is no CTA barrier, and the per-column
-// arithmetic is branch-free (masked selects, predicated stores) except for
-// warp-wide skips of rows without ocean.
+// Each row's contributions to a later stage are folded into a few partial
+// sums as soon as they are known, so only two instances of the carried
+// values exist; the two-fold unrolled row loop renames them.  A value needed
+// from a neighbouring column comes from the neighbouring lane by a warp
+// shuffle.  There is no CTA barrier, and the per-column arithmetic is
+// branch-free (masked selects, predicated stores) except for warp-wide skips
+// of rows without ocean.
 //
-// Input rows j-2..j+1 of the state, the rest depth (and, in the general
-// variant, the 2-D forcing fields and the row's metric coefficients) plus the
-// row's T-mask bits sit in a ring of RING shared-memory slots.  Lane 0 refills
-// the slot of row j-2 with row j-2+RING by 1-D bulk TMA copies
-// (cp.async.bulk, no multicast) completing on that slot's mbarrier.  Every
-// wait is bounded: on timeout the CTA sets a status bit, drains its own
-// copies (bounded) and returns.
+// Input rows j-2..j+1 sit in a ring of RING shared-memory slots.  A slot
+// holds a 36-column segment of the six state fields and of the static
+// fields (rest depth, forcing; in the general variant also viscosity, drag
+// and water flux), brought by two 3-D tiled TMA loads from field-blocked
+// arrays (cp.async.bulk.tensor, no multicast), plus the row's T-mask bits
+// (and, in the general variant, its metric coefficients) by 1-D bulk copies.
+// Lane 0 refills the slot of row j-2 with row j-2+RING once every lane is
+// past it.  Every wait is bounded: on timeout the CTA sets a status bit,
+// drains its own copies (bounded) and returns.
 //
 // Two variants: UNI for square uniform grids (every metric array equal to
 // one spacing d; all metric factors fold into a few constants and only the
@@ -48,18 +52,12 @@ constexpr int NL = 32;            // lanes = threads per CTA = strip columns
 constexpr int OUTW = NL - 2;      // written columns per strip
 constexpr int SEG = NL + 4;       // ring segment: strip columns -2 .. 33
 constexpr int RING = 6;           // ring slots (4 rows in use + 2 in flight)
-constexpr int COEF_D = (int)(sizeof(RowCoef) / sizeof(double));
 constexpr unsigned WAIT_LIMIT = 1u << 20;
 
-// state order, as the *_e arguments: u, up, v, vp, ssh, sshp
-enum { S_U, S_UP, S_V, S_VP, S_SSH, S_SSHP };
-// ring fields
-enum { R_U, R_V, R_SSH, R_UP, R_VP, R_SSHP, R_H, R_NUNI, R_MU = R_NUNI, R_RD, R_WF, R_NGEN };
-
-struct Params {
-    const double *src[6];
-    double *dst[6];
-    const double *H, *rhsx, *rhsy, *mu, *rdis, *wflux;
+struct alignas(64) Params {
+    CUtensorMap tm_src;    // source state set {pitch, rows, 6 fields}, box {SEG, 1, 6}
+    CUtensorMap tm_stat;   // static block, box {SEG, 1, Layout::NS}
+    double *dst[NSET];
     double *acc[4];
     const uint32_t *bits;
     const RowCoef *rows;
@@ -70,7 +68,7 @@ struct Params {
     int r_first, r_last;   // interior device rows
     int c_first, c_last;   // interior device columns
     double two_ti, gam, c4, rhs_scale, mu0, rd0, wq0, inv_rho;
-    double d, inv_d, d4, gd, d2, inv_d2;   // UNI metric constants
+    double d, inv_d, d4, gd, d2, tt;   // UNI: d, 1/d, d/4, g*d, d*d, two_ti/d^2
     int vort_zero;
     unsigned *flags;
 };
@@ -121,15 +119,31 @@ __device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t b
         : "memory");
 }
 
+// 3-D tiled copy of the box at (x, y, z) of *map into this CTA's shared
+// memory, completion on *bar.  x is even (16-byte aligned for doubles).
+__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar)
+{
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(dst)),
+        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
+        : "memory");
+}
+
 template <bool GEN>
 struct Layout {
-    static constexpr int NF = GEN ? R_NGEN : R_NUNI;
-    static constexpr int NCOEF = GEN ? COEF_D : 0;
-    static constexpr int SLOT_D = NF * SEG + NCOEF + 4;   // doubles per slot (4 = 8 mask words)
-    static constexpr size_t bytes = (size_t)RING * SLOT_D * sizeof(double) + RING * sizeof(uint64_t);
-    static constexpr uint32_t row_tx = (uint32_t)(SLOT_D * sizeof(double));
-    static constexpr int min_ctas = GEN ? 10 : 12;
+    static constexpr int NS = GEN ? NSTAT : 3;                   // static fields in a slot
+    static constexpr int STAT_OFF = 1792;                        // after 6*SEG doubles, 128-aligned
+    static constexpr int COEF_OFF = STAT_OFF + NS * SEG * 8;     // general variant: RowCoef
+    static constexpr int BITS_OFF = COEF_OFF + (GEN ? (int)sizeof(RowCoef) : 0);
+    static constexpr int SLOT_B = (BITS_OFF + 32 + 127) / 128 * 128;
+    static constexpr size_t bytes = 128 + (size_t)RING * SLOT_B + RING * sizeof(uint64_t);
+    static constexpr uint32_t row_tx =
+        (uint32_t)(NSET * SEG * 8 + NS * SEG * 8 + (GEN ? (int)sizeof(RowCoef) : 0) + 32);
+    static constexpr int min_ctas = GEN ? 9 : 13;
 };
+static_assert(NSET * SEG * 8 <= 1792, "state segment overlaps the static segment");
+static_assert(Layout<false>::COEF_OFF % 16 == 0 && Layout<true>::BITS_OFF % 16 == 0, "bulk copy alignment");
 
 __device__ __forceinline__ double sel(int m, double x) { return m ? x : 0.0; }
 
@@ -154,19 +168,26 @@ __device__ __forceinline__ double rcp_nr(double x)
 #define SHFL_UP(x) __shfl_up_sync(0xffffffffu, (x), 1)
 #define SHFL_DN(x) __shfl_down_sync(0xffffffffu, (x), 1)
 
-// per-row values carried between the stages of the row pipeline
-struct S1 {          // stage 1 of a row
-    double U, V;             // U = u*hu, V = v*hv
-    double Ul, Vr;           // U(k-1), V(k+1) from the neighbouring lanes
-    double hu, hv;           // current-level u/v depths
-    double rx, ry;           // forcing RHSx, RHSy of the row
-};
-struct HQ {          // H + ssh of a row at k, k+1
+struct HQ {          // H + ssh of a row at columns k, k+1
     double a, b;
 };
-struct S2 {          // stage 2 of a row
-    double sn;               // new SSH
-    double FY, QU, SS, GX, GXl, GY, QV, QVl, ST, SSl;
+// values of row j from stage 1, carried to the next iteration
+struct S1 {
+    double U, Ul, V, Vr;     // U = u*hu at k, k-1; V = v*hv at k, k+1
+    double Ru;               // u equation of row j: forcing + pressure gradient - drag
+    double Rv;               // v equation of row j: forcing + pressure gradient - drag
+    double cor;              // uniform variant: Coriolis factor of row j
+    double slx, sly;         // pressure-gradient terms (time means only)
+    HQ hq;                   // H + ssh of row j+1
+};
+// values of row j-1 from stage 2 (and of stage 1 routed on), carried on
+struct S2 {
+    double sn;               // new SSH of the row
+    double V;                // V of the row
+    double Cu;               // the row's part of the u equation of the row above
+    double Pv;               // the row's part of its own v equation
+    double sly;              // pressure-gradient term of the row (time means only)
+    HQ hqm;                  // H + ssh of row j
 };
 
 // MODE = acc + 3*write: acc 0 none, 1 first substep (write), 2 accumulate;
@@ -175,11 +196,11 @@ template <bool GEN, int MODE>
 __global__ void __launch_bounds__(NL, Layout<GEN>::min_ctas) k_substep(const __grid_constant__ Params p)
 {
     using L = Layout<GEN>;
-    constexpr int NF = L::NF;
     constexpr int ACC = MODE % 3;
     constexpr bool WRITE = MODE / 3 != 0;
-    extern __shared__ __align__(128) double smem[];
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(smem + RING * L::SLOT_D);
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *ring = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(ring + RING * L::SLOT_B);
 
     const int l = threadIdx.x;
     const int g0 = blockIdx.x * OUTW;          // device column of segment offset 0
@@ -190,48 +211,26 @@ __global__ void __launch_bounds__(NL, Layout<GEN>::min_ctas) k_substep(const __g
     const int row_lo = r0 - 2, row_hi = r1 + 1;             // rows kept in the ring
     const int wbase = (g0 >> 7) << 2;                       // first mask word of the window
     const int bsh = k - wbase * 32;                         // bit of k in the window
-    const int po = l + 2;                                   // segment offset of k
+    const unsigned char *lane = ring + (l + 2) * 8;         // this lane's column in a segment
 
-    auto slotp = [&](int s) { return smem + (size_t)s * L::SLOT_D; };
-    auto slot_of = [&](int row) { return (row - row_lo) % RING; };
-    auto issue = [&](int row) {
-        const int s = slot_of(row);
-        double *dd = slotp(s);
-        uint64_t *bar = &mbar[s];
+    // field f of the state / static segment of the slot at byte offset o
+#define AS(o, f, dk) (*reinterpret_cast<const double *>(lane + (o) + ((f) * SEG + (dk)) * 8))
+#define AT(o, f, dk) (*reinterpret_cast<const double *>(lane + (o) + L::STAT_OFF + ((f) * SEG + (dk)) * 8))
+#define CF(o, x) (reinterpret_cast<const RowCoef *>(ring + (o) + L::COEF_OFF)->x)
+
+    auto issue = [&](int row, int slot) {
+        unsigned char *dd = ring + slot * L::SLOT_B;
+        uint64_t *bar = &mbar[slot];
         mbar_expect_tx(bar, L::row_tx);
-        const long long off = (long long)row * p.pitch + g0;
-        const uint32_t nb = SEG * sizeof(double);
-        bulk_load(dd + R_U * SEG, p.src[S_U] + off, nb, bar);
-        bulk_load(dd + R_V * SEG, p.src[S_V] + off, nb, bar);
-        bulk_load(dd + R_SSH * SEG, p.src[S_SSH] + off, nb, bar);
-        bulk_load(dd + R_UP * SEG, p.src[S_UP] + off, nb, bar);
-        bulk_load(dd + R_VP * SEG, p.src[S_VP] + off, nb, bar);
-        bulk_load(dd + R_SSHP * SEG, p.src[S_SSHP] + off, nb, bar);
-        bulk_load(dd + R_H * SEG, p.H + off, nb, bar);
-        if constexpr (GEN) {
-            bulk_load(dd + R_MU * SEG, p.mu + off, nb, bar);
-            bulk_load(dd + R_RD * SEG, p.rdis + off, nb, bar);
-            bulk_load(dd + R_WF * SEG, p.wflux + off, nb, bar);
-            bulk_load(dd + NF * SEG, p.rows + row, sizeof(RowCoef), bar);
-        }
-        bulk_load(dd + NF * SEG + L::NCOEF, p.bits + (size_t)row * p.bm_words + wbase, 32, bar);
+        tma_load_3d(dd, &p.tm_src, g0, row, 0, bar);
+        tma_load_3d(dd + L::STAT_OFF, &p.tm_stat, g0, row, 0, bar);
+        if constexpr (GEN) bulk_load(dd + L::COEF_OFF, p.rows + row, sizeof(RowCoef), bar);
+        bulk_load(dd + L::BITS_OFF, p.bits + (size_t)row * p.bm_words + wbase, 32, bar);
     };
-    auto at = [&](int s, int f, int dk) { return slotp(s)[f * SEG + po + dk]; };
-    auto mask2 = [&](int s) -> uint32_t {   // bits: lu(k), lu(k+1)
-        const uint32_t *w = reinterpret_cast<const uint32_t *>(slotp(s) + NF * SEG + L::NCOEF);
+    auto mask2 = [&](int o) -> uint32_t {   // bits: lu(k), lu(k+1)
+        const uint32_t *w = reinterpret_cast<const uint32_t *>(ring + o + L::BITS_OFF);
         return __funnelshift_r(w[bsh >> 5], w[(bsh >> 5) + 1], bsh & 31) & 3u;
     };
-    auto coef = [&](int s) { return reinterpret_cast<const RowCoef *>(slotp(s) + NF * SEG); };
-    // metric coefficient of the row in slot s: GEN from the ring, UNI folded
-#define CG(s, x) coef(s)->x
-#define C_KU(s) (GEN ? CG(s, ku) : 1.0)
-#define C_KU2(s) (GEN ? CG(s, ku2) : 0.5)
-#define C_WV0(s) (GEN ? CG(s, wv0) : 1.0)
-#define C_WV1(s) (GEN ? CG(s, wv1) : 1.0)
-#define C_D4(s, x) (GEN ? CG(s, x) : p.d4)
-#define C_GD(s, x) (GEN ? CG(s, x) : p.gd)
-#define C_D2(s, x) (GEN ? CG(s, x) : p.d2)
-#define C_INVD2(s, x) (GEN ? CG(s, x) : p.inv_d2)
 
     if (l == 0) {
         for (int s = 0; s < RING; s++) mbar_init(&mbar[s], 1);
@@ -240,142 +239,171 @@ __global__ void __launch_bounds__(NL, Layout<GEN>::min_ctas) k_substep(const __g
     __syncwarp();
     int issued = row_lo - 1;
     if (l == 0)
-        for (int row = row_lo; row < row_lo + RING && row <= row_hi; row++) issue(row), issued = row;
+        for (int t = 0; t < RING && row_lo + t <= row_hi; t++) issue(row_lo + t, t), issued = row_lo + t;
 
     const bool out = l >= 1 && l <= NL - 2 && k >= p.c_first && k <= p.c_last;
     const double gam = p.gam, two_ti = p.two_ti, rs = p.rhs_scale;
 
+    // slots of rows j-2, j-1, j, j+1 and the fill parity of row j+1
+    int i_m2 = RING - 1, i_m1 = 0, i_0 = 1, i_p1 = 2;
+    uint32_t ph = 0;
     // T-mask bits, 2 per row: row j+1 in bits 0-1, j in 2-3, j-1 in 4-5, j-2 in 6-7
     uint32_t mk = 0;
     uint32_t bad = 0;   // guard: a new value out of range or NaN
     int waited = row_lo - 1;
-    bool ok = true;
-    auto wait_upto = [&](int need) {
-        while (waited < need && ok) {
-            const int row = waited + 1;
-            if (!mbar_wait(&mbar[slot_of(row)], (uint32_t)(((row - row_lo) / RING) & 1))) { ok = false; break; }
-            waited = row;
-            mk = (mk << 2) | mask2(slot_of(row));
-        }
-        ok = __all_sync(0xffffffffu, ok);
-    };
+    bool ok = mbar_wait(&mbar[0], 0);
+    ok = __all_sync(0xffffffffu, ok && mbar_wait(&mbar[1], 0));
+    if (ok) waited = row_lo + 1;
 
-    auto step = [&](const int j, S1 &s1n, const S1 &s1c, const S1 &s1p, HQ &hqn, const HQ &hqc,
-                    const HQ &hqp, S2 &s2n, const S2 &s2o) {
-        wait_upto(min(j + 1, row_hi));
-        if (j + 1 > row_hi) mk <<= 2;   // keep the row alignment of mk
-        if (!ok) return;
-        const int s_m2 = slot_of(j - 2), s_m1 = slot_of(j - 1), s_0 = slot_of(j), s_p1 = slot_of(j + 1);
+    S1 A{}, B{};
+    S2 X{}, Y{};
+    if (ok) {
+        mk = (mask2(0) << 2) | mask2(L::SLOT_B);
+        // H + ssh of row r0-1, the "current" row of the first iteration
+        B.hq.a = AT(L::SLOT_B, T_H, 0) + AS(L::SLOT_B, S_SSH, 0);
+        B.hq.b = AT(L::SLOT_B, T_H, 1) + AS(L::SLOT_B, S_SSH, 1);
+    }
+    long long gi = (long long)(r0 - 1) * p.pitch + k;   // element (row j, column k)
+
+    auto step = [&](const int j, S1 &n, const S1 &c, S2 &q, const S2 &qc) {
+        const int o_m2 = i_m2 * L::SLOT_B, o_m1 = i_m1 * L::SLOT_B, o_0 = i_0 * L::SLOT_B, o_p1 = i_p1 * L::SLOT_B;
+        if (j + 1 <= row_hi) {
+            ok = __all_sync(0xffffffffu, mbar_wait(&mbar[i_p1], ph));
+            if (!ok) return;
+            waited = j + 1;
+            mk = (mk << 2) | mask2(o_p1);
+        } else {
+            mk <<= 2;   // keep the row alignment of mk
+        }
 
         // ---------------- stage 1: row j ---------------------------------
         if (j <= r1) {
             const uint32_t mj = (mk >> 2) & 3u, mn = mk & 3u;
-            hqn.a = at(s_p1, R_H, 0) + at(s_p1, R_SSH, 0);
-            hqn.b = at(s_p1, R_H, 1) + at(s_p1, R_SSH, 1);
-            const int a = mj & 1, b = (mj >> 1) & 1, c = mn & 1;
+            n.hq.a = AT(o_p1, T_H, 0) + AS(o_p1, S_SSH, 0);
+            n.hq.b = AT(o_p1, T_H, 1) + AS(o_p1, S_SSH, 1);
+            const int a = mj & 1, b = (mj >> 1) & 1, cc = mn & 1;
             // Function/depth.f90:127-139 mask-weighted averages to u and v points
-            const double hu = (sel(a, hqc.a) + sel(b, hqc.b)) * (a & b ? C_KU2(s_0) : (a | b ? C_KU(s_0) : 0.0));
-            const double hv = (sel(a, hqc.a * C_WV0(s_0)) + sel(c, hqn.a * C_WV1(s_0))) *
-                              (a & c ? 0.5 : (a | c ? 1.0 : 0.0));
-            s1n.hu = hu;
-            s1n.hv = hv;
-            s1n.U = at(s_0, R_U, 0) * hu;
-            s1n.V = at(s_0, R_V, 0) * hv;
-            const long long gi = (long long)j * p.pitch + k;
-            s1n.rx = p.rhsx[gi];
-            s1n.ry = p.rhsy[gi];
+            double hu, hv;
+            if constexpr (GEN) {
+                hu = (sel(a, c.hq.a) + sel(b, c.hq.b)) * (a & b ? CF(o_0, ku2) : (a | b ? CF(o_0, ku) : 0.0));
+                hv = (sel(a, c.hq.a * CF(o_0, wv0)) + sel(cc, n.hq.a * CF(o_0, wv1))) *
+                     (a & cc ? 0.5 : (a | cc ? 1.0 : 0.0));
+            } else {
+                hu = (sel(a, c.hq.a) + sel(b, c.hq.b)) * (a & b ? 0.5 : (a | b ? 1.0 : 0.0));
+                hv = (sel(a, c.hq.a) + sel(cc, n.hq.a)) * (a & cc ? 0.5 : (a | cc ? 1.0 : 0.0));
+            }
+            n.U = AS(o_0, S_U, 0) * hu;
+            n.V = AS(o_0, S_V, 0) * hv;
+            // vel_ssh.f90:536-545, :554-565: forcing, pressure gradient of
+            // the current level and Rayleigh drag of the previous level
+            const double e0 = AS(o_0, S_SSH, 0), e1 = AS(o_0, S_SSH, 1), e1v = AS(o_p1, S_SSH, 0);
+            double slx, sly, rdu, rdv, au, av;
+            if constexpr (GEN) {
+                slx = -(e1 - e0) * CF(o_0, gdyh) * hu;
+                sly = -(e1v - e0) * CF(o_0, gdxh) * hv;
+                rdu = (AT(o_0, T_RD, 0) + AT(o_0, T_RD, 1)) * 0.5;
+                rdv = (AT(o_0, T_RD, 0) + AT(o_p1, T_RD, 0)) * 0.5;
+                au = CF(o_0, au);
+                av = CF(o_0, av);
+            } else {
+                slx = -(e1 - e0) * p.gd * hu;
+                sly = -(e1v - e0) * p.gd * hv;
+                rdu = rdv = p.rd0;
+                au = av = p.d2;
+                n.cor = p.cor[j];
+            }
+            n.Ru = AT(o_0, T_RX, 0) * rs + slx - rdu * AS(o_0, S_UP, 0) * au * hu;
+            n.Rv = AT(o_0, T_RY, 0) * rs + sly - rdv * AS(o_0, S_VP, 0) * av * hv;
+            if (ACC) {
+                n.slx = slx;
+                n.sly = sly;
+            }
         }
-        s1n.Ul = SHFL_UP(s1n.U);
-        s1n.Vr = SHFL_DN(s1n.V);
+        n.Ul = SHFL_UP(n.U);
+        n.Vr = SHFL_DN(n.V);
 
         // ---------------- stage 2: row rho = j-1 -------------------------
-        double FX = 0.0, u_r = 0.0, up_r = 0.0;
+        double FX = 0.0, FY = 0.0, GY = 0.0, ST = 0.0, SS = 0.0, QU = 0.0, GX = 0.0, QV = 0.0, sn = 0.0;
+        double u_r = 0.0, up_r = 0.0, v_m = 0.0, vp_m = 0.0;
         if (j >= r0 && j <= r1 + 1) {
             const uint32_t mr = (mk >> 4) & 3u, mu_ = (mk >> 2) & 3u;   // rows rho, rho+1
-            const int sr = s_m1, sm = s_m2, su = s_0;
             const int lc = mr & 1, lr = (mr >> 1) & 1, lu = mu_ & 1, lur = (mu_ >> 1) & 1;
             const int luu = lc & lr & lu & lur;
-            u_r = at(sr, R_U, 0);
-            up_r = at(sr, R_UP, 0);
-            const double u_l = at(sr, R_U, -1), u_u = at(su, R_U, 0);
-            const double v_r = at(sr, R_V, 0), v_rr = at(sr, R_V, 1), v_m = at(sm, R_V, 0);
-            const double up_l = at(sr, R_UP, -1), up_u = at(su, R_UP, 0);
-            const double vp_r = at(sr, R_VP, 0), vp_rr = at(sr, R_VP, 1), vp_m = at(sm, R_VP, 0);
+            u_r = AS(o_m1, S_U, 0);
+            up_r = AS(o_m1, S_UP, 0);
+            v_m = AS(o_m2, S_V, 0);
+            vp_m = AS(o_m2, S_VP, 0);
+            const double u_l = AS(o_m1, S_U, -1), u_u = AS(o_0, S_U, 0);
+            const double v_r = AS(o_m1, S_V, 0), v_rr = AS(o_m1, S_V, 1);
+            const double up_l = AS(o_m1, S_UP, -1), up_u = AS(o_0, S_UP, 0);
+            const double vp_r = AS(o_m1, S_VP, 0), vp_rr = AS(o_m1, S_VP, 1);
             double mu_t = p.mu0, mu_h = p.mu0, wq = p.wq0;
             if constexpr (GEN) {
-                mu_t = at(sr, R_MU, 0);
-                mu_h = (mu_t + at(sr, R_MU, 1) + at(su, R_MU, 0) + at(su, R_MU, 1)) * 0.25;
-                wq = at(sr, R_WF, 0) * p.inv_rho;
+                mu_t = AT(o_m1, T_MU, 0);
+                mu_h = (mu_t + AT(o_m1, T_MU, 1) + AT(o_0, T_MU, 0) + AT(o_0, T_MU, 1)) * 0.25;
+                wq = AT(o_m1, T_WF, 0) * p.inv_rho;
             }
             // vel_ssh.f90:491-494 continuity over 2*tau_inner
-            const double div = GEN ? (s1c.U - s1c.Ul) * CG(sr, c_u) + s1c.V * CG(sr, c_v0) - s1p.V * CG(sr, c_v1)
-                                   : ((s1c.U - s1c.Ul) + (s1c.V - s1p.V)) * p.inv_d;
-            s2n.sn = sel(lc, at(sr, R_SSHP, 0) + two_ti * (wq - div));
+            const double div = GEN ? (c.U - c.Ul) * CF(o_m1, c_u) + c.V * CF(o_m1, c_v0) - qc.V * CF(o_m1, c_v1)
+                                   : ((c.U - c.Ul) + (c.V - qc.V)) * p.inv_d;
+            sn = sel(lc, AS(o_m1, S_SSHP, 0) + two_ti * (wq - div));
             // vel_ssh.f90:63-73, :88-98 advective fluxes on T and h faces
-            FX = (s1c.Ul + s1c.U) * (u_l + u_r) * C_D4(sr, fx);
-            s2n.FY = sel(luu, (s1c.V + s1c.Vr) * (u_r + u_u) * C_D4(sr, fy));
-            s2n.GX = (GEN ? s1c.U * CG(sr, gx0) + s1n.U * CG(sr, gx1) : (s1c.U + s1n.U) * p.d4) * (v_r + v_rr);
-            s2n.GY = (GEN ? s1p.V * CG(sr, gy0) + s1c.V * CG(sr, gy1) : (s1p.V + s1c.V) * p.d4) * (v_m + v_r);
+            FX = (c.Ul + c.U) * (u_l + u_r) * (GEN ? CF(o_m1, fx) : p.d4);
+            FY = sel(luu, (c.V + c.Vr) * (u_r + u_u) * (GEN ? CF(o_m1, fy) : p.d4));
+            GX = (GEN ? c.U * CF(o_m1, gx0) + n.U * CF(o_m1, gx1) : (c.U + n.U) * p.d4) * (v_r + v_rr);
+            GY = (GEN ? qc.V * CF(o_m1, gy0) + c.V * CF(o_m1, gy1) : (qc.V + c.V) * p.d4) * (v_m + v_r);
             // depth.f90:141-147 depth on the h point
-            const double sa = sel(lc, hqp.a) + sel(lr, hqp.b);
-            const double sb = sel(lu, hqc.a) + sel(lur, hqc.b);
-            const double hh = (GEN ? sa * CG(sr, wh0) + sb * CG(sr, wh1) : sa + sb) * rcount(lc + lr + lu + lur);
+            const double sa = sel(lc, qc.hqm.a) + sel(lr, qc.hqm.b);
+            const double sb = sel(lu, c.hq.a) + sel(lur, c.hq.b);
+            const double hh = (GEN ? sa * CF(o_m1, wh0) + sb * CF(o_m1, wh1) : sa + sb) * rcount(lc + lr + lu + lur);
             // vel_ssh.f90:35-37 metric vorticity (zero on uniform grids) + Coriolis
             double cor;
             if constexpr (GEN) {
-                cor = CG(sr, cor);
+                cor = CF(o_m1, cor);
                 if (!p.vort_zero)
-                    cor += sel(luu, (v_rr - v_r) * CG(sr, vt0) - u_u * CG(sr, vt1) + u_r * CG(sr, vt2));
+                    cor += sel(luu, (v_rr - v_r) * CF(o_m1, vt0) - u_u * CF(o_m1, vt1) + u_r * CF(o_m1, vt2));
             } else {
-                cor = p.cor[j - 1];
+                cor = c.cor;
             }
             const double Wh = hh * cor;
-            s2n.QU = Wh * (v_r + v_rr);
-            s2n.QV = Wh * (u_r + u_u);
+            QU = Wh * (v_r + v_rr);
+            QV = Wh * (u_r + u_u);
             // mixing.f90:134-148 stresses from the previous level
-            const double str_t = GEN ? sel(lc, CG(sr, t1) * (up_r - up_l) - (CG(sr, t2) * vp_r - CG(sr, t3) * vp_m))
+            const double str_t = GEN ? sel(lc, CF(o_m1, t1) * (up_r - up_l) - (CF(o_m1, t2) * vp_r - CF(o_m1, t3) * vp_m))
                                      : sel(lc, ((up_r - up_l) - (vp_r - vp_m)) * p.inv_d);
-            const double str_s = GEN ? sel(luu, CG(sr, s1) * up_u - CG(sr, s2) * up_r + CG(sr, s3) * (vp_rr - vp_r))
+            const double str_s = GEN ? sel(luu, CF(o_m1, s1) * up_u - CF(o_m1, s2) * up_r + CF(o_m1, s3) * (vp_rr - vp_r))
                                      : sel(luu, ((up_u - up_r) + (vp_rr - vp_r)) * p.inv_d);
-            s2n.ST = mu_t * hqp.a * str_t;
-            s2n.SS = mu_h * hh * str_s;
+            ST = mu_t * qc.hqm.a * str_t;
+            SS = mu_h * hh * str_s;
         }
         const double FXr = SHFL_DN(FX);
-        const double STr = SHFL_DN(s2n.ST);
-        const double SNr = SHFL_DN(s2n.sn);
-        s2n.GXl = SHFL_UP(s2n.GX);
-        s2n.QVl = SHFL_UP(s2n.QV);
-        s2n.SSl = SHFL_UP(s2n.SS);
+        const double STr = SHFL_DN(ST);
+        const double SNr = SHFL_DN(sn);
+        const double GXl = SHFL_UP(GX);
+        const double QVl = SHFL_UP(QV);
+        const double SSl = SHFL_UP(SS);
 
         // ---------------- stage 3u: row rho = j-1 (u and SSH) -----------
         const uint32_t mr = (mk >> 4) & 3u;
         if (j >= r0 + 1 && j <= r1 && __any_sync(0xffffffffu, out && (mr & 1u))) {
-            const int sr = s_m1;
             const int lc = mr & 1, lr = (mr >> 1) & 1;
             const bool wu = out && (lc & lr), wt = out && lc;
-            const double e0 = at(sr, R_SSH, 0), e1 = at(sr, R_SSH, 1);
-            const double sp0 = at(sr, R_SSHP, 0), sp1 = at(sr, R_SSHP, 1);
-            const double h0 = at(sr, R_H, 0), h1 = at(sr, R_H, 1);
-            const double sn0 = s2n.sn;
+            const double e0 = AS(o_m1, S_SSH, 0);
+            const double sp0 = AS(o_m1, S_SSHP, 0), sp1 = AS(o_m1, S_SSHP, 1);
+            const double h0 = AT(o_m1, T_H, 0), h1 = AT(o_m1, T_H, 1);
             // vel_ssh.f90:536-551
-            const double hu = s1c.hu;
-            const double hup = ((h0 + sp0) + (h1 + sp1)) * C_KU2(sr);
-            const double hun = ((h0 + sn0) + (h1 + SNr)) * C_KU2(sr);
-            const double slx = -(e1 - e0) * C_GD(sr, gdyh) * hu;
-            const double slxn = -(SNr - sn0) * C_GD(sr, gdyh) * hun;
-            const double adv = -((FXr - FX) + (s2n.FY - s2o.FY));
-            const double dif = GEN ? (STr - s2n.ST) * CG(sr, dux) + (s2n.SS * CG(sr, dus0) - s2o.SS * CG(sr, dus1))
-                                   : ((STr - s2n.ST) + (s2n.SS - s2o.SS)) * p.d;
-            double rd = p.rd0;
-            if constexpr (GEN) rd = (at(sr, R_RD, 0) + at(sr, R_RD, 1)) * 0.5;
-            const double grx = s1c.rx * rs + slx + dif + adv - rd * up_r * C_D2(sr, au) * hu
-                               + (s2n.QU + s2o.QU) * 0.25;
-            const double un = (up_r * hup + grx * (two_ti * C_INVD2(sr, rau))) * rcp_nr(hun);
-            bad |= (uint32_t)(wu && !(un < 100.0 && un > -100.0));
-            bad |= (uint32_t)(wt && !(sn0 < 10.0 && sn0 > -10.0));
-            const long long idx = (long long)(j - 1) * p.pitch + k;
+            const double ku2 = GEN ? CF(o_m1, ku2) : 0.5;
+            const double hup = ((h0 + sp0) + (h1 + sp1)) * ku2;
+            const double hun = ((h0 + sn) + (h1 + SNr)) * ku2;
+            const double difx = GEN ? (STr - ST) * CF(o_m1, dux) + SS * CF(o_m1, dus0) : ((STr - ST) + SS) * p.d;
+            const double grx = c.Ru + qc.Cu - ((FXr - FX) + FY) + difx + QU * 0.25;
+            const double un = (up_r * hup + grx * (GEN ? two_ti * CF(o_m1, rau) : p.tt)) * rcp_nr(hun);
+            bad |= (uint32_t)(wu && !(fabs(un) < 100.0));
+            bad |= (uint32_t)(wt && !(fabs(sn) < 10.0));
+            const long long idx = gi - p.pitch;
             if (ACC && wu) {
-                double a = (u_r * hu + un * hun) * p.c4, b = (slx + slxn) * p.c4;
+                const double slxn = -(SNr - sn) * (GEN ? CF(o_m1, gdyh) : p.gd) * hun;
+                double a = (c.U + un * hun) * p.c4, b = (c.slx + slxn) * p.c4;
                 if (ACC == 2) { a += p.acc[0][idx]; b += p.acc[2][idx]; }
                 p.acc[0][idx] = a;
                 p.acc[2][idx] = b;
@@ -385,39 +413,35 @@ __global__ void __launch_bounds__(NL, Layout<GEN>::min_ctas) k_substep(const __g
                 p.dst[S_U][idx] = un;
             }
             if (WRITE && wt) {   // vel_ssh.f90:593-596
-                p.dst[S_SSHP][idx] = e0 + gam * (sn0 - 2.0 * e0 + sp0);
-                p.dst[S_SSH][idx] = sn0;
+                p.dst[S_SSHP][idx] = e0 + gam * (sn - 2.0 * e0 + sp0);
+                p.dst[S_SSH][idx] = sn;
             }
         }
 
         // ---------------- stage 3v: row R = j-2 (v) ----------------------
         const uint32_t mR = (mk >> 6) & 3u, mU = (mk >> 4) & 3u;   // rows R, R+1
         if (j >= r0 + 2 && j <= r1 + 1 && __any_sync(0xffffffffu, out && (mR & mU & 1u))) {
-            const int sR = s_m2, sU = s_m1;
             const bool wv = out && (mR & mU & 1u);
-            const double e0 = at(sR, R_SSH, 0), e1 = at(sU, R_SSH, 0);
-            const double sp0 = at(sR, R_SSHP, 0), sp1 = at(sU, R_SSHP, 0);
-            const double h0 = at(sR, R_H, 0), h1 = at(sU, R_H, 0);
-            const double v0 = at(sR, R_V, 0), vp0 = at(sR, R_VP, 0);
-            const double sn0 = s2o.sn, sn1 = s2n.sn;
+            const double sp0 = AS(o_m2, S_SSHP, 0), sp1 = AS(o_m1, S_SSHP, 0);
+            const double h0 = AT(o_m2, T_H, 0), h1 = AT(o_m1, T_H, 0);
+            const double v0 = v_m, vp0 = vp_m;
+            const double sn0 = qc.sn, sn1 = sn;
             // vel_ssh.f90:554-569
-            const double hv = s1p.hv;
-            const double hvp = (GEN ? (h0 + sp0) * CG(sR, wv0) + (h1 + sp1) * CG(sR, wv1) : (h0 + sp0) + (h1 + sp1)) * 0.5;
-            const double hvn = (GEN ? (h0 + sn0) * CG(sR, wv0) + (h1 + sn1) * CG(sR, wv1) : (h0 + sn0) + (h1 + sn1)) * 0.5;
-            const double sly = -(e1 - e0) * C_GD(sR, gdxh) * hv;
-            const double slyn = -(sn1 - sn0) * C_GD(sR, gdxh) * hvn;
-            const double adv = -((s2o.GX - s2o.GXl) + (s2n.GY - s2o.GY));
-            const double dif = GEN ? -(s2n.ST * CG(sR, dvt1) - s2o.ST * CG(sR, dvt0)) + (s2o.SS - s2o.SSl) * CG(sR, dvs)
-                                   : (-(s2n.ST - s2o.ST) + (s2o.SS - s2o.SSl)) * p.d;
-            double rd = p.rd0;
-            if constexpr (GEN) rd = (at(sR, R_RD, 0) + at(sU, R_RD, 0)) * 0.5;
-            const double gry = s1p.ry * rs + sly + dif + adv - rd * vp0 * C_D2(sR, av) * hv
-                               - (s2o.QV + s2o.QVl) * 0.25;
-            const double vn = (vp0 * hvp + gry * (two_ti * C_INVD2(sR, rav))) * rcp_nr(hvn);
-            bad |= (uint32_t)(wv && !(vn < 100.0 && vn > -100.0));
-            const long long idx = (long long)(j - 2) * p.pitch + k;
+            double hvp, hvn;
+            if constexpr (GEN) {
+                hvp = ((h0 + sp0) * CF(o_m2, wv0) + (h1 + sp1) * CF(o_m2, wv1)) * 0.5;
+                hvn = ((h0 + sn0) * CF(o_m2, wv0) + (h1 + sn1) * CF(o_m2, wv1)) * 0.5;
+            } else {
+                hvp = ((h0 + sp0) + (h1 + sp1)) * 0.5;
+                hvn = ((h0 + sn0) + (h1 + sn1)) * 0.5;
+            }
+            const double gry = qc.Pv - GY - ST * (GEN ? CF(o_m2, dvt1) : p.d);
+            const double vn = (vp0 * hvp + gry * (GEN ? two_ti * CF(o_m2, rav) : p.tt)) * rcp_nr(hvn);
+            bad |= (uint32_t)(wv && !(fabs(vn) < 100.0));
+            const long long idx = gi - 2 * p.pitch;
             if (ACC && wv) {
-                double a = (v0 * hv + vn * hvn) * p.c4, b = (sly + slyn) * p.c4;
+                const double slyn = -(sn1 - sn0) * (GEN ? CF(o_m2, gdxh) : p.gd) * hvn;
+                double a = (qc.V + vn * hvn) * p.c4, b = (qc.sly + slyn) * p.c4;
                 if (ACC == 2) { a += p.acc[1][idx]; b += p.acc[3][idx]; }
                 p.acc[1][idx] = a;
                 p.acc[3][idx] = b;
@@ -427,48 +451,49 @@ __global__ void __launch_bounds__(NL, Layout<GEN>::min_ctas) k_substep(const __g
                 p.dst[S_V][idx] = vn;
             }
         }
+
+        // ---------------- carry row rho on ------------------------------
+        // its part of the u equation of row rho+1 (vel_ssh.f90:539-541):
+        // +FY(rho), -SS(rho)*dxb(rho)^2/dxt(rho+1), +QU(rho)/4
+        q.Cu = FY + QU * 0.25 - SS * (GEN ? CF(o_0, dus1) : p.d);
+        // its part of its own v equation (vel_ssh.f90:557-560); the row
+        // above adds -GY(rho+1) and -ST(rho+1)*dx(rho+1)^2/dxh(rho)
+        const double dify = GEN ? ST * CF(o_m1, dvt0) + (SS - SSl) * CF(o_m1, dvs) : (ST + (SS - SSl)) * p.d;
+        q.Pv = c.Rv + (GY - (GX - GXl)) + dify - (QV + QVl) * 0.25;
+        q.sn = sn;
+        q.V = c.V;
+        q.hqm = c.hq;
+        if (ACC) q.sly = c.sly;
+
         // row j-2 was last read above: once every lane is past it, its slot
         // takes row j-2+RING
         __syncwarp();
-        if (l == 0) {
-            const int dead = j - 2;
-            if (dead >= row_lo && dead + RING <= row_hi) issue(dead + RING), issued = dead + RING;
-        }
+        if (l == 0 && j - 2 >= row_lo && j + 4 <= row_hi) issue(j + 4, i_m2), issued = j + 4;
+        i_m2 = i_m1;
+        i_m1 = i_0;
+        i_0 = i_p1;
+        i_p1 = i_p1 == RING - 1 ? 0 : i_p1 + 1;
+        ph ^= i_p1 == 0 ? 1u : 0u;
+        gi += p.pitch;
     };
 
-    // H + ssh of row r0-1, the stage-1 "current" row of the first step
-    HQ HA{}, HB{}, HC{};
-    wait_upto(row_lo + 1);
-    if (ok) {
-        const int s = slot_of(r0 - 1);
-        HC.a = at(s, R_H, 0) + at(s, R_SSH, 0);
-        HC.b = at(s, R_H, 1) + at(s, R_SSH, 1);
-    }
-    // three instances of each carried struct, renamed (not copied) by the
-    // three-fold unrolled loop
-    S1 A{}, B{}, C{};
-    S2 X{}, Y{}, Z{};
-    for (int j = r0 - 1; j <= r1 + 1 && ok; j += 3) {
-        step(j, A, C, B, HA, HC, HB, X, Z);
-        step(j + 1, B, A, C, HB, HA, HC, Y, X);
-        step(j + 2, C, B, A, HC, HB, HA, Z, Y);
+    // two instances of each carried struct, renamed (not copied) by the
+    // two-fold unrolled loop
+    for (int j = r0 - 1; j <= r1 + 1 && ok; j += 2) {
+        step(j, A, B, X, Y);
+        if (!ok) break;
+        step(j + 1, B, A, Y, X);
     }
     if (__any_sync(0xffffffffu, bad != 0) && l == 0) atomicOr(p.flags, FLAG_GUARD);
     if (!ok && l == 0) {
         atomicOr(p.flags, FLAG_TIMEOUT);
         // drain this CTA's copies still in flight (bounded) before exiting
-        for (int row = max(waited + 1, row_lo); row <= issued; row++)
-            (void)mbar_wait(&mbar[slot_of(row)], (uint32_t)(((row - row_lo) / RING) & 1));
+        for (int row = waited + 1; row <= issued; row++)
+            (void)mbar_wait(&mbar[(row - row_lo) % RING], (uint32_t)(((row - row_lo) / RING) & 1));
     }
-#undef CG
-#undef C_KU
-#undef C_KU2
-#undef C_WV0
-#undef C_WV1
-#undef C_D4
-#undef C_GD
-#undef C_D2
-#undef C_INVD2
+#undef AS
+#undef AT
+#undef CF
 }
 
 // min/max over the ocean points of three fields, for the uniform-forcing test
@@ -534,15 +559,22 @@ int forcing_mode(Plan &p, const Dom &d, const Consts &c, double *forc[6], cudaSt
     return 0;
 }
 
-Params base_params(const Plan &p, const Dom &d, const Consts &c, double *forc[6], const Forcing &f, int gen)
+// copy the forcing fields the variant reads into the static block
+int stage_forcing(Plan &p, double *forc[6], int gen, cudaStream_t s)
 {
-    Params q{};
-    q.H = p.hrest;
-    q.rhsx = forc[0];
-    q.rhsy = forc[1];
-    q.wflux = forc[2];
-    q.mu = forc[3];
-    q.rdis = forc[5];
+    const size_t fb = (size_t)p.fstride * sizeof(double);
+    const int src_of[NSTAT] = {-1, 0, 1, 3, 5, 2};   // T_* <- forc index (RHSx RHSy wflux mu mu4 rdis)
+    for (int t = T_RX; t < (gen ? NSTAT : 3); t++)
+        if (cudaMemcpyAsync(p.stat + t * p.fstride, forc[src_of[t]], fb, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+            return 1;
+    return 0;
+}
+
+Params base_params(const Plan &p, const Dom &d, const Consts &c, const Forcing &f, int gen)
+{
+    Params q;
+    std::memset(&q, 0, sizeof q);
+    q.tm_stat = p.tm_stat[gen];
     q.bits = p.bits;
     q.rows = p.rows;
     q.cor = p.cor;
@@ -564,9 +596,26 @@ Params base_params(const Plan &p, const Dom &d, const Consts &c, double *forc[6]
     q.d4 = p.d / 4.0;
     q.gd = c.g * p.d;
     q.d2 = p.d * p.d;
-    q.inv_d2 = p.d != 0.0 ? 1.0 / (p.d * p.d) : 0.0;
     q.chunk_rows = p.chunk_rows[gen];
     return q;
+}
+
+void set_times(Params &q, double two_ti, const Plan &p)
+{
+    q.two_ti = two_ti;
+    q.tt = p.d != 0.0 ? two_ti * (1.0 / (p.d * p.d)) : 0.0;
+}
+
+// source and destination sets of one launch (state order)
+int set_io(const Plan &p, Params &q, double *const src[NSET], double *const dst[NSET])
+{
+    int s = -1;
+    for (int b = 0; b < 3; b++)
+        if (p.set[b] == src[0]) s = b;
+    if (s < 0) return 1;
+    q.tm_src = p.tm_set[s];
+    for (int k = 0; k < NSET; k++) q.dst[k] = dst[k];
+    return 0;
 }
 
 template <bool GEN, int MODE>
@@ -595,13 +644,11 @@ void launch(Plan &p, const Params &q, int gen, int mode, cudaStream_t s)
     else launch_g<false>(p, q, mode, s);
 }
 
-int sync_buffers(Plan &p, const Dom &d, double *state[6], cudaStream_t s)
+int sync_buffers(Plan &p, double *state[6], cudaStream_t s)
 {
-    const size_t bytes = (size_t)d.pitch * d.nya() * sizeof(double);
+    const size_t bytes = (size_t)NSET * p.fstride * sizeof(double);
     for (int b = 0; b < 2; b++)
-        for (int k = 0; k < 6; k++)
-            if (cudaMemcpyAsync(p.buf[b][k], state[k], bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
-                return 1;
+        if (cudaMemcpyAsync(p.buf[b][0], state[0], bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return 1;
     p.buffers_synced = true;
     return 0;
 }
@@ -626,6 +673,42 @@ int set_smem()
 {
     return set_smem1<false, 2>() | set_smem1<false, 3>() | set_smem1<false, 4>() | set_smem1<false, 5>() |
            set_smem1<true, 2>() | set_smem1<true, 3>() | set_smem1<true, 4>() | set_smem1<true, 5>();
+}
+
+using EncodeTiled = decltype(&cuTensorMapEncodeTiled);
+
+// {pitch, rows, nfields} doubles with field stride fstride; box {SEG, 1, box_fields}
+int encode_fields(EncodeTiled enc, CUtensorMap *map, double *base, const Dom &d, long long fstride, int nfields,
+                  int box_fields)
+{
+    const cuuint64_t dims[3] = {(cuuint64_t)d.pitch, (cuuint64_t)d.nya(), (cuuint64_t)nfields};
+    const cuuint64_t strides[2] = {(cuuint64_t)d.pitch * sizeof(double), (cuuint64_t)fstride * sizeof(double)};
+    const cuuint32_t box[3] = {(cuuint32_t)SEG, 1u, (cuuint32_t)box_fields};
+    const cuuint32_t estr[3] = {1u, 1u, 1u};
+    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr,
+               CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
+               CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS;
+}
+
+void release(Plan &p)
+{
+    cudaFree(p.rows);
+    cudaFree(p.cor);
+    cudaFree(p.bits);
+    // the plan owns the two sets that are not the caller's current state
+    cudaFree(p.buf[0][0]);
+    cudaFree(p.buf[1][0]);
+    cudaFree(p.stat);
+    cudaFree(p.d_uniform);
+    cudaFree(p.d_flags);
+    p.rows = nullptr;
+    p.cor = nullptr;
+    p.bits = nullptr;
+    for (auto &b : p.buf)
+        for (auto &x : b) x = nullptr;
+    p.stat = nullptr;
+    p.d_uniform = nullptr;
+    p.d_flags = nullptr;
 }
 
 }  // namespace
@@ -696,8 +779,9 @@ const char *check_eligible(const Plan &p, const Dom &d, const Consts &c, const f
 }
 
 int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], const double *const grid[10],
-          const double *d_hrest, const float *d_lu, cudaStream_t s)
+          const double *d_hrest, const float *d_lu, double *state[NSET], cudaStream_t s)
 {
+    release(p);
     const int nxa = d.nxa(), nya = d.nya();
     auto row_of = [&](int k, int n) {
         n = std::min(std::max(n, d.ny_start - 1), d.ny_end + 1);
@@ -782,16 +866,35 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
     if (cudaMalloc(&p.bits, bits.size() * sizeof(uint32_t)) != cudaSuccess) return 1;
     if (cudaMemcpyAsync(p.bits, bits.data(), bits.size() * sizeof(uint32_t), cudaMemcpyHostToDevice, s) != cudaSuccess)
         return 1;
-    const size_t fb = (size_t)d.pitch * nya * sizeof(double);
-    for (int b = 0; b < 2; b++)
-        for (int k = 0; k < 6; k++) {
-            if (cudaMalloc(&p.buf[b][k], fb) != cudaSuccess) return 1;
-            if (cudaMemsetAsync(p.buf[b][k], 0, fb, s) != cudaSuccess) return 1;
-        }
+    // field-blocked sets: the caller's state block and two ping-pong sets
+    p.fstride = d.pitch * nya;
+    const size_t fb = (size_t)p.fstride * sizeof(double);
+    for (int b = 0; b < 2; b++) {
+        double *blk = nullptr;
+        if (cudaMalloc(&blk, NSET * fb) != cudaSuccess) return 1;
+        if (cudaMemsetAsync(blk, 0, NSET * fb, s) != cudaSuccess) return 1;
+        for (int k = 0; k < NSET; k++) p.buf[b][k] = blk + k * p.fstride;
+    }
+    if (cudaMalloc(&p.stat, NSTAT * fb) != cudaSuccess) return 1;
+    if (cudaMemsetAsync(p.stat, 0, NSTAT * fb, s) != cudaSuccess) return 1;
+    if (cudaMemcpyAsync(p.stat + T_H * p.fstride, d_hrest, fb, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return 1;
+    p.set[0] = state[0];
+    p.set[1] = p.buf[0][0];
+    p.set[2] = p.buf[1][0];
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult qr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &qr) != cudaSuccess ||
+        qr != cudaDriverEntryPointSuccess || !fn)
+        return 1;
+    EncodeTiled enc = reinterpret_cast<EncodeTiled>(fn);
+    for (int b = 0; b < 3; b++)
+        if (encode_fields(enc, &p.tm_set[b], p.set[b], d, p.fstride, NSET, NSET)) return 1;
+    if (encode_fields(enc, &p.tm_stat[0], p.stat, d, p.fstride, NSTAT, Layout<false>::NS)) return 1;
+    if (encode_fields(enc, &p.tm_stat[1], p.stat, d, p.fstride, NSTAT, Layout<true>::NS)) return 1;
+
     if (cudaMalloc(&p.d_uniform, (size_t)MINMAX_BLOCKS * 6 * sizeof(double)) != cudaSuccess) return 1;
     if (cudaMalloc(&p.d_flags, sizeof(unsigned)) != cudaSuccess) return 1;
     if (cudaMemsetAsync(p.d_flags, 0, sizeof(unsigned), s) != cudaSuccess) return 1;
-    p.hrest = d_hrest;
     p.lu = d_lu;
     p.buffers_synced = false;
     if (set_smem()) return 1;
@@ -806,6 +909,8 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
     if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], k_substep<true, 3>, NL, Layout<true>::bytes) !=
             cudaSuccess || occ[1] < 1)
         occ[1] = 1;
+    p.occ[0] = occ[0];
+    p.occ[1] = occ[1];
     // one wave: strips x chunks <= SMs x resident CTAs, chunks as tall as
     // that allows; each chunk re-reads and recomputes three rows of warm-up,
     // so keep chunks at least 16 rows tall
@@ -824,15 +929,16 @@ int dynamics(Plan &p, const Dom &d, const Consts &c, double tau, int nstep, doub
 {
     Forcing f;
     if (forcing_mode(p, d, c, forc, s, f)) return 1;
-    if (!p.buffers_synced && sync_buffers(p, d, state, s)) return 1;
+    if (!p.buffers_synced && sync_buffers(p, state, s)) return 1;
     if (cudaMemsetAsync(p.d_flags, 0, sizeof(unsigned), s) != cudaSuccess) return 1;
     const size_t fb = (size_t)d.pitch * d.nya() * sizeof(double);
     for (int k = 0; k < 4; k++)
         if (cudaMemsetAsync(acc[k], 0, fb, s) != cudaSuccess) return 1;   // vel_ssh.f90:479-482
     const int gen = (p.uni && f.uniform) ? 0 : 1;
-    Params q = base_params(p, d, c, forc, f, gen);
+    if (stage_forcing(p, forc, gen, s)) return 1;
+    Params q = base_params(p, d, c, f, gen);
     const double ti = tau / (double)nstep;
-    q.two_ti = 2.0 * ti;
+    set_times(q, 2.0 * ti, p);
     q.gam = c.ts / 2.0 / (double)nstep;
     q.c4 = 1.0 / (double)(4 * nstep);
     for (int k = 0; k < 4; k++) q.acc[k] = acc[k];
@@ -840,10 +946,7 @@ int dynamics(Plan &p, const Dom &d, const Consts &c, double tau, int nstep, doub
     // after substep nstep (vel_ssh.f90:638-648) is then swapped into state[]
     for (int step = 1; step <= nstep; step++) {
         const bool odd = step & 1;
-        for (int k = 0; k < 6; k++) {
-            q.src[k] = odd ? state[k] : p.buf[0][k];
-            q.dst[k] = odd ? p.buf[0][k] : state[k];
-        }
+        if (set_io(p, q, odd ? state : p.buf[0], odd ? p.buf[0] : state)) return 1;
         launch(p, q, gen, step == 1 ? 4 : 5, s);
         if (cudaGetLastError() != cudaSuccess) return 1;
     }
@@ -852,10 +955,9 @@ int dynamics(Plan &p, const Dom &d, const Consts &c, double tau, int nstep, doub
     // substeps nstep+1..2*nstep feed only the time means: state[] -> buf[0],
     // then buf[0] <-> buf[1]; the last one writes no state
     for (int k2 = 1; k2 <= nstep; k2++) {
-        for (int k = 0; k < 6; k++) {
-            q.src[k] = k2 == 1 ? state[k] : ((k2 & 1) ? p.buf[1][k] : p.buf[0][k]);
-            q.dst[k] = (k2 & 1) ? p.buf[0][k] : p.buf[1][k];
-        }
+        double *const *src = k2 == 1 ? state : ((k2 & 1) ? p.buf[1] : p.buf[0]);
+        double *const *dst = (k2 & 1) ? p.buf[0] : p.buf[1];
+        if (set_io(p, q, src, dst)) return 1;
         launch(p, q, gen, k2 < nstep ? 5 : 2, s);
         if (cudaGetLastError() != cudaSuccess) return 1;
     }
@@ -870,19 +972,17 @@ int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt, co
 {
     Forcing f;
     if (forcing_mode(p, d, c, forc, s, f)) return 1;
-    if (!p.buffers_synced && sync_buffers(p, d, state, s)) return 1;
+    if (!p.buffers_synced && sync_buffers(p, state, s)) return 1;
     if (cudaMemsetAsync(p.d_flags, 0, sizeof(unsigned), s) != cudaSuccess) return 1;
     const int gen = (p.uni && f.uniform) ? 0 : 1;
-    Params q = base_params(p, d, c, forc, f, gen);
-    q.two_ti = 2.0 * dt;
+    if (stage_forcing(p, forc, gen, s)) return 1;
+    Params q = base_params(p, d, c, f, gen);
+    set_times(q, 2.0 * dt, p);
     q.gam = c.ts / 2.0;   // nstep = 1
     q.c4 = 0.25;
     for (int k = 0; k < 4; k++) q.acc[k] = nullptr;
     for (int step = 0; step < nsub; step++) {
-        for (int k = 0; k < 6; k++) {
-            q.src[k] = (step & 1) ? p.buf[0][k] : state[k];
-            q.dst[k] = (step & 1) ? state[k] : p.buf[0][k];
-        }
+        if (set_io(p, q, (step & 1) ? p.buf[0] : state, (step & 1) ? state : p.buf[0])) return 1;
         q.rhs_scale = rhs_scale ? rhs_scale[step] : 1.0;
         launch(p, q, gen, 3, s);
         if (cudaGetLastError() != cudaSuccess) return 1;
@@ -897,13 +997,7 @@ int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt, co
 
 void free_plan(Plan &p)
 {
-    cudaFree(p.rows);
-    cudaFree(p.cor);
-    cudaFree(p.bits);
-    for (auto &b : p.buf)
-        for (auto &x : b) cudaFree(x);
-    cudaFree(p.d_uniform);
-    cudaFree(p.d_flags);
+    release(p);
     p = Plan{};
 }
 

@@ -6,7 +6,15 @@
 // time-mean accumulation and Robert-Asselin filter with time shift) for the
 // whole basin.  Each CTA owns a strip of columns and marches down a chunk of
 // rows; input rows arrive through a ring of shared-memory slots filled by
-// 1-D bulk TMA copies (cp.async.bulk, no multicast) tracked by mbarriers.
+// 3-D tiled TMA copies (cp.async.bulk.tensor, no multicast) of field-blocked
+// arrays, tracked by mbarriers.
+//
+// Device layout of the fused path: a state set is ONE allocation holding the
+// six *_e fields back to back (field stride = pitch * rows), so that one
+// tensor-map box {36 columns, 1 row, 6 fields} brings a row segment of all
+// of them; the static block holds the rest depth and the forcing the same
+// way.  The caller's state must be such a block (state[k] = state[0] + k *
+// pitch * rows).
 //
 // The fused path derives the external depths from SSH each substep
 // (hq = H + ssh and its mask-weighted averages, which is what hh_init,
@@ -21,6 +29,8 @@
 // surface, no biharmonic term.
 #pragma once
 
+#include <cuda.h>
+
 #include "common.cuh"
 #include "inmsom_gpu.h"
 
@@ -28,6 +38,11 @@ namespace inmsom {
 namespace fused {
 
 constexpr int XOFF = 1;   // device padding columns before bnd_x1 (see common.cuh)
+
+// fields of a state set, in memory order (the *_e argument order)
+enum { S_U, S_UP, S_V, S_VP, S_SSH, S_SSHP, NSET };
+// fields of the static block: rest depth, RHSx, RHSy, mu, rdis, wflux
+enum { T_H, T_RX, T_RY, T_MU, T_RD, T_WF, NSTAT };
 
 // per-row coefficients, row index = device row (n - bnd_y1); 38 doubles so
 // that a row is a whole number of 16-byte units for the bulk copies
@@ -65,10 +80,15 @@ struct Plan {
     double *cor = nullptr;          // per-row rlh_s*d*d (uniform variant)
     uint32_t *bits = nullptr;       // 1-bit T mask, bm_words per row
     int bm_words = 0;
-    double *buf[2][6] = {};         // extra state sets (ping-pong)
+    double *buf[2][6] = {};         // the two ping-pong sets (field views)
+    double *set[3] = {};            // base of each state set (field 0)
+    double *stat = nullptr;         // static block, NSTAT fields
+    long long fstride = 0;          // doubles between the fields of a block
+    CUtensorMap tm_set[3];          // box {36, 1, 6} over each state set
+    CUtensorMap tm_stat[2];         // box {36, 1, 3 | 6} over the static block
+    int occ[2] = {0, 0};            // resident CTAs per SM, per variant
     double *d_uniform = nullptr;    // per-block min/max of mu, rdis, wflux
     unsigned *d_flags = nullptr;    // [0] status bits (guard / timeout)
-    const double *hrest = nullptr;  // borrowed
     const float *lu = nullptr;      // borrowed
     int nsm = 148;
     bool vort_zero = false;
@@ -88,10 +108,11 @@ Plan make_plan(const inmsom_bounds &b);
 // nullptr if the fused path can run this grid, else the reason
 const char *check_eligible(const Plan &p, const Dom &d, const Consts &c,
                            const float *const masks[7], const double *const grid[10]);
-// build the row table and the bit mask, allocate the ping-pong buffers
+// build the row table and the bit mask, allocate the ping-pong sets and the
+// static block, encode the tensor maps; state[] is the caller's state set
 int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7],
           const double *const grid[10], const double *d_hrest, const float *d_lu,
-          cudaStream_t s);
+          double *state[NSET], cudaStream_t s);
 // barotropic_dynamics(tau, nstep) on state[6] (in/out) with acc[4] out
 int dynamics(Plan &p, const Dom &d, const Consts &c, double tau, int nstep,
              double *state[6], double *acc[4], double *forc[6], cudaStream_t s);
