@@ -3,8 +3,10 @@
 // Work decomposition.  A CTA is one warp; lane l owns device column
 // k = g0+2+l of a 32-column strip starting at device column g0+2
 // (g0 = 30*strip, even).  Strip columns 1..30 are written, so strips overlap
-// by two columns.  The CTA marches down a chunk of rows; iteration j of its
-// row loop computes
+// by two columns.  The CTA marches down a chunk of rows (a work item; the
+// chunks of a strip are cut so that all items cost about the same and the
+// single wave of CTAs finishes together); iteration j of its row loop
+// computes
 //   stage 1,  row j  : u/v-point depths of the current level, the transports
 //                      U = u*hu and V = v*hv, and the row's forcing, pressure
 //                      gradient and drag terms of the u and v equations;
@@ -28,8 +30,8 @@
 // and water flux), brought by two 3-D tiled TMA loads from field-blocked
 // arrays (cp.async.bulk.tensor, no multicast), plus the row's T-mask bits
 // (and, in the general variant, its metric coefficients) by 1-D bulk copies.
-// Lane 0 refills the slot of row j-2 with row j-2+RING once every lane is
-// past it.  Every wait is bounded: on timeout the CTA sets a status bit,
+// One elected lane refills the slot of row j-2 with row j-2+RING once every
+// lane is past it.  Every wait is bounded: on timeout the CTA sets a status bit,
 // drains its own copies (bounded) and returns.
 //
 // Two variants: UNI for square uniform grids (every metric array equal to
@@ -41,6 +43,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <type_traits>
 #include <vector>
 
 namespace inmsom {
@@ -62,10 +65,9 @@ struct alignas(64) Params {
     const uint32_t *bits;
     const RowCoef *rows;
     const double *cor;
+    const int4 *items;     // work items {g0, first row, end row (exclusive), 0}
     long long pitch;
     int bm_words;
-    int chunk_rows;
-    int r_first, r_last;   // interior device rows
     int c_first, c_last;   // interior device columns
     double two_ti, gam, c4, rhs_scale, mu0, rd0, wq0, inv_rho;
     double d, inv_d, d4, gd, d2, tt;   // UNI: d, 1/d, d/4, g*d, d*d, two_ti/d^2
@@ -81,12 +83,6 @@ __device__ __forceinline__ uint32_t smem_addr(const void *p)
 __device__ __forceinline__ void mbar_init(uint64_t *bar, uint32_t count)
 {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(bar)), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint64_t *bar, uint32_t bytes)
-{
-    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
-                 : "memory");
 }
 
 __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
@@ -109,27 +105,6 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
     return false;
 }
 
-// 1-D bulk copy global -> this CTA's shared memory, completion on *bar
-__device__ __forceinline__ void bulk_load(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
-{
-    asm volatile(
-        "cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
-            smem_addr(dst)),
-        "l"(src), "r"(bytes), "r"(smem_addr(bar))
-        : "memory");
-}
-
-// 3-D tiled copy of the box at (x, y, z) of *map into this CTA's shared
-// memory, completion on *bar.  x is even (16-byte aligned for doubles).
-__device__ __forceinline__ void tma_load_3d(void *dst, const CUtensorMap *map, int x, int y, int z, uint64_t *bar)
-{
-    asm volatile(
-        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
-        " [%0], [%1, {%2, %3, %4}], [%5];" ::"r"(smem_addr(dst)),
-        "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(z), "r"(smem_addr(bar))
-        : "memory");
-}
-
 template <bool GEN>
 struct Layout {
     static constexpr int NS = GEN ? NSTAT : 3;                   // static fields in a slot
@@ -140,10 +115,63 @@ struct Layout {
     static constexpr size_t bytes = 128 + (size_t)RING * SLOT_B + RING * sizeof(uint64_t);
     static constexpr uint32_t row_tx =
         (uint32_t)(NSET * SEG * 8 + NS * SEG * 8 + (GEN ? (int)sizeof(RowCoef) : 0) + 32);
-    static constexpr int min_ctas = GEN ? 9 : 13;
 };
+
+// resident CTAs per SM the register budget is cut for: 13 one-warp CTAs
+// (4 warps per SM sub-partition, 128 registers) for the plain substep,
+// 12 where the time-mean sums need more registers; the general variant's
+// larger ring allows 9
+template <bool GEN, int MODE>
+constexpr int min_ctas() { return GEN ? 9 : (MODE % 3 ? 12 : 13); }
 static_assert(NSET * SEG * 8 <= 1792, "state segment overlaps the static segment");
 static_assert(Layout<false>::COEF_OFF % 16 == 0 && Layout<true>::BITS_OFF % 16 == 0, "bulk copy alignment");
+
+// One lane elected by elect.sync announces the bytes of a row to the slot's
+// mbarrier and starts its copies: the state and static segments (3-D tiled
+// TMA, x = g0 even, so 16-byte aligned), the mask-bit window and, in the
+// general variant, the row's coefficients (1-D bulk copies).  No branch.
+template <bool GEN>
+__device__ __forceinline__ void issue_row(unsigned char *slot, uint64_t *bar, const CUtensorMap *src,
+                                          const CUtensorMap *stat, const void *coef, const void *bits, int x,
+                                          int row)
+{
+    using L = Layout<GEN>;
+    const int z = 0;
+    if constexpr (GEN) {
+        asm volatile(
+            "{\n\t.reg .pred P;\n\t"
+            "elect.sync _|P, 0xffffffff;\n\t"
+            "@P mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n\t"
+            "@P cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+            " [%2], [%3, {%4, %5, %6}], [%0];\n\t"
+            "@P cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+            " [%7], [%8, {%4, %5, %6}], [%0];\n\t"
+            "@P cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%9], [%10], %11, [%0];\n\t"
+            "@P cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%12], [%13], 32, [%0];\n\t"
+            "}" ::"r"(smem_addr(bar)),
+            "r"(L::row_tx), "r"(smem_addr(slot)), "l"(reinterpret_cast<uint64_t>(src)), "r"(x), "r"(row), "r"(z),
+            "r"(smem_addr(slot + L::STAT_OFF)), "l"(reinterpret_cast<uint64_t>(stat)),
+            "r"(smem_addr(slot + L::COEF_OFF)), "l"(coef), "n"((int)sizeof(RowCoef)),
+            "r"(smem_addr(slot + L::BITS_OFF)), "l"(bits)
+            : "memory");
+    } else {
+        (void)coef;
+        asm volatile(
+            "{\n\t.reg .pred P;\n\t"
+            "elect.sync _|P, 0xffffffff;\n\t"
+            "@P mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n\t"
+            "@P cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+            " [%2], [%3, {%4, %5, %6}], [%0];\n\t"
+            "@P cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+            " [%7], [%8, {%4, %5, %6}], [%0];\n\t"
+            "@P cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%9], [%10], 32, [%0];\n\t"
+            "}" ::"r"(smem_addr(bar)),
+            "r"(L::row_tx), "r"(smem_addr(slot)), "l"(reinterpret_cast<uint64_t>(src)), "r"(x), "r"(row), "r"(z),
+            "r"(smem_addr(slot + L::STAT_OFF)), "l"(reinterpret_cast<uint64_t>(stat)),
+            "r"(smem_addr(slot + L::BITS_OFF)), "l"(bits)
+            : "memory");
+    }
+}
 
 __device__ __forceinline__ double sel(int m, double x) { return m ? x : 0.0; }
 
@@ -183,17 +211,21 @@ struct S1 {
 // values of row j-1 from stage 2 (and of stage 1 routed on), carried on
 struct S2 {
     double sn;               // new SSH of the row
-    double V;                // V of the row
+    double V, Uo;            // V and U of the row
+    double vs;               // v(k) + v(k+1) of the row
     double Cu;               // the row's part of the u equation of the row above
-    double Pv;               // the row's part of its own v equation
+    double Pv;               // the row's part of its own v equation, less the GX flux
     double sly;              // pressure-gradient term of the row (time means only)
     HQ hqm;                  // H + ssh of row j
 };
 
+template <bool B>
+using On = std::integral_constant<bool, B>;
+
 // MODE = acc + 3*write: acc 0 none, 1 first substep (write), 2 accumulate;
 // write 1 stores the new state
 template <bool GEN, int MODE>
-__global__ void __launch_bounds__(NL, Layout<GEN>::min_ctas) k_substep(const __grid_constant__ Params p)
+__global__ void __launch_bounds__(NL, min_ctas<GEN, MODE>()) k_substep(const __grid_constant__ Params p)
 {
     using L = Layout<GEN>;
     constexpr int ACC = MODE % 3;
@@ -202,12 +234,11 @@ __global__ void __launch_bounds__(NL, Layout<GEN>::min_ctas) k_substep(const __g
     unsigned char *ring = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
     uint64_t *mbar = reinterpret_cast<uint64_t *>(ring + RING * L::SLOT_B);
 
+    const int4 item = p.items[blockIdx.x];
     const int l = threadIdx.x;
-    const int g0 = blockIdx.x * OUTW;          // device column of segment offset 0
+    const int g0 = item.x;                     // device column of segment offset 0
     const int k = g0 + 2 + l;                  // this lane's column
-    const int r0 = p.r_first + blockIdx.y * p.chunk_rows;
-    const int r1 = min(r0 + p.chunk_rows, p.r_last + 1);   // exclusive
-    if (r0 >= r1) return;
+    const int r0 = item.y, r1 = item.z;        // output rows [r0, r1), r1 > r0
     const int row_lo = r0 - 2, row_hi = r1 + 1;             // rows kept in the ring
     const int wbase = (g0 >> 7) << 2;                       // first mask word of the window
     const int bsh = k - wbase * 32;                         // bit of k in the window
@@ -219,13 +250,8 @@ __global__ void __launch_bounds__(NL, Layout<GEN>::min_ctas) k_substep(const __g
 #define CF(o, x) (reinterpret_cast<const RowCoef *>(ring + (o) + L::COEF_OFF)->x)
 
     auto issue = [&](int row, int slot) {
-        unsigned char *dd = ring + slot * L::SLOT_B;
-        uint64_t *bar = &mbar[slot];
-        mbar_expect_tx(bar, L::row_tx);
-        tma_load_3d(dd, &p.tm_src, g0, row, 0, bar);
-        tma_load_3d(dd + L::STAT_OFF, &p.tm_stat, g0, row, 0, bar);
-        if constexpr (GEN) bulk_load(dd + L::COEF_OFF, p.rows + row, sizeof(RowCoef), bar);
-        bulk_load(dd + L::BITS_OFF, p.bits + (size_t)row * p.bm_words + wbase, 32, bar);
+        issue_row<GEN>(ring + slot * L::SLOT_B, &mbar[slot], &p.tm_src, &p.tm_stat, p.rows + row,
+                       p.bits + (size_t)row * p.bm_words + wbase, g0, row);
     };
     auto mask2 = [&](int o) -> uint32_t {   // bits: lu(k), lu(k+1)
         const uint32_t *w = reinterpret_cast<const uint32_t *>(ring + o + L::BITS_OFF);
@@ -238,8 +264,7 @@ __global__ void __launch_bounds__(NL, Layout<GEN>::min_ctas) k_substep(const __g
     }
     __syncwarp();
     int issued = row_lo - 1;
-    if (l == 0)
-        for (int t = 0; t < RING && row_lo + t <= row_hi; t++) issue(row_lo + t, t), issued = row_lo + t;
+    for (int t = 0; t < RING && row_lo + t <= row_hi; t++) issue(row_lo + t, t), issued = row_lo + t;
 
     const bool out = l >= 1 && l <= NL - 2 && k >= p.c_first && k <= p.c_last;
     const double gam = p.gam, two_ti = p.two_ti, rs = p.rhs_scale;
@@ -265,9 +290,15 @@ __global__ void __launch_bounds__(NL, Layout<GEN>::min_ctas) k_substep(const __g
     }
     long long gi = (long long)(r0 - 1) * p.pitch + k;   // element (row j, column k)
 
-    auto step = [&](const int j, S1 &n, const S1 &c, S2 &q, const S2 &qc) {
+    // One iteration of the row loop; the flags say which stages are valid
+    // for row j (the first three and the last iteration lack some).
+    auto step = [&](const int j, auto on1, auto on2, auto on3u, auto on3v, S1 &n, const S1 &c, S2 &q,
+                    const S2 &qc) {
+        constexpr bool D1 = decltype(on1)::value, D2 = decltype(on2)::value;
+        constexpr bool D3U = decltype(on3u)::value, D3V = decltype(on3v)::value;
+        if (!ok) return;
         const int o_m2 = i_m2 * L::SLOT_B, o_m1 = i_m1 * L::SLOT_B, o_0 = i_0 * L::SLOT_B, o_p1 = i_p1 * L::SLOT_B;
-        if (j + 1 <= row_hi) {
+        if constexpr (D1) {   // stage 1 reads row j+1
             ok = __all_sync(0xffffffffu, mbar_wait(&mbar[i_p1], ph));
             if (!ok) return;
             waited = j + 1;
@@ -276,8 +307,8 @@ __global__ void __launch_bounds__(NL, Layout<GEN>::min_ctas) k_substep(const __g
             mk <<= 2;   // keep the row alignment of mk
         }
 
-        // ---------------- stage 1: row j ---------------------------------
-        if (j <= r1) {
+        // ---------------- stage 1: row j (independent of stage 2) -------
+        if constexpr (D1) {
             const uint32_t mj = (mk >> 2) & 3u, mn = mk & 3u;
             n.hq.a = AT(o_p1, T_H, 0) + AS(o_p1, S_SSH, 0);
             n.hq.b = AT(o_p1, T_H, 1) + AS(o_p1, S_SSH, 1);
@@ -319,13 +350,10 @@ __global__ void __launch_bounds__(NL, Layout<GEN>::min_ctas) k_substep(const __g
                 n.sly = sly;
             }
         }
-        n.Ul = SHFL_UP(n.U);
-        n.Vr = SHFL_DN(n.V);
 
         // ---------------- stage 2: row rho = j-1 -------------------------
-        double FX = 0.0, FY = 0.0, GY = 0.0, ST = 0.0, SS = 0.0, QU = 0.0, GX = 0.0, QV = 0.0, sn = 0.0;
-        double u_r = 0.0, up_r = 0.0, v_m = 0.0, vp_m = 0.0;
-        if (j >= r0 && j <= r1 + 1) {
+        double FX, FY, GY, ST, SS, QU, QV, sn, vs, u_r, up_r, v_m, vp_m;
+        if constexpr (D2) {
             const uint32_t mr = (mk >> 4) & 3u, mu_ = (mk >> 2) & 3u;   // rows rho, rho+1
             const int lc = mr & 1, lr = (mr >> 1) & 1, lu = mu_ & 1, lur = (mu_ >> 1) & 1;
             const int luu = lc & lr & lu & lur;
@@ -348,9 +376,9 @@ __global__ void __launch_bounds__(NL, Layout<GEN>::min_ctas) k_substep(const __g
                                    : ((c.U - c.Ul) + (c.V - qc.V)) * p.inv_d;
             sn = sel(lc, AS(o_m1, S_SSHP, 0) + two_ti * (wq - div));
             // vel_ssh.f90:63-73, :88-98 advective fluxes on T and h faces
+            vs = v_r + v_rr;
             FX = (c.Ul + c.U) * (u_l + u_r) * (GEN ? CF(o_m1, fx) : p.d4);
             FY = sel(luu, (c.V + c.Vr) * (u_r + u_u) * (GEN ? CF(o_m1, fy) : p.d4));
-            GX = (GEN ? c.U * CF(o_m1, gx0) + n.U * CF(o_m1, gx1) : (c.U + n.U) * p.d4) * (v_r + v_rr);
             GY = (GEN ? qc.V * CF(o_m1, gy0) + c.V * CF(o_m1, gy1) : (qc.V + c.V) * p.d4) * (v_m + v_r);
             // depth.f90:141-147 depth on the h point
             const double sa = sel(lc, qc.hqm.a) + sel(lr, qc.hqm.b);
@@ -366,7 +394,7 @@ __global__ void __launch_bounds__(NL, Layout<GEN>::min_ctas) k_substep(const __g
                 cor = c.cor;
             }
             const double Wh = hh * cor;
-            QU = Wh * (v_r + v_rr);
+            QU = Wh * vs;
             QV = Wh * (u_r + u_u);
             // mixing.f90:134-148 stresses from the previous level
             const double str_t = GEN ? sel(lc, CF(o_m1, t1) * (up_r - up_l) - (CF(o_m1, t2) * vp_r - CF(o_m1, t3) * vp_m))
@@ -376,99 +404,121 @@ __global__ void __launch_bounds__(NL, Layout<GEN>::min_ctas) k_substep(const __g
             ST = mu_t * qc.hqm.a * str_t;
             SS = mu_h * hh * str_s;
         }
-        const double FXr = SHFL_DN(FX);
-        const double STr = SHFL_DN(ST);
-        const double SNr = SHFL_DN(sn);
-        const double GXl = SHFL_UP(GX);
-        const double QVl = SHFL_UP(QV);
-        const double SSl = SHFL_UP(SS);
+        double FXr, STr, SNr, QVl, SSl;
+        if constexpr (D2) {
+            FXr = SHFL_DN(FX);
+            STr = SHFL_DN(ST);
+            SNr = SHFL_DN(sn);
+            QVl = SHFL_UP(QV);
+            SSl = SHFL_UP(SS);
+        }
+        if constexpr (D1) {
+            n.Ul = SHFL_UP(n.U);
+            n.Vr = SHFL_DN(n.V);
+        }
 
         // ---------------- stage 3u: row rho = j-1 (u and SSH) -----------
-        const uint32_t mr = (mk >> 4) & 3u;
-        if (j >= r0 + 1 && j <= r1 && __any_sync(0xffffffffu, out && (mr & 1u))) {
-            const int lc = mr & 1, lr = (mr >> 1) & 1;
-            const bool wu = out && (lc & lr), wt = out && lc;
-            const double e0 = AS(o_m1, S_SSH, 0);
-            const double sp0 = AS(o_m1, S_SSHP, 0), sp1 = AS(o_m1, S_SSHP, 1);
-            const double h0 = AT(o_m1, T_H, 0), h1 = AT(o_m1, T_H, 1);
-            // vel_ssh.f90:536-551
-            const double ku2 = GEN ? CF(o_m1, ku2) : 0.5;
-            const double hup = ((h0 + sp0) + (h1 + sp1)) * ku2;
-            const double hun = ((h0 + sn) + (h1 + SNr)) * ku2;
-            const double difx = GEN ? (STr - ST) * CF(o_m1, dux) + SS * CF(o_m1, dus0) : ((STr - ST) + SS) * p.d;
-            const double grx = c.Ru + qc.Cu - ((FXr - FX) + FY) + difx + QU * 0.25;
-            const double un = (up_r * hup + grx * (GEN ? two_ti * CF(o_m1, rau) : p.tt)) * rcp_nr(hun);
-            bad |= (uint32_t)(wu && !(fabs(un) < 100.0));
-            bad |= (uint32_t)(wt && !(fabs(sn) < 10.0));
-            const long long idx = gi - p.pitch;
-            if (ACC && wu) {
-                const double slxn = -(SNr - sn) * (GEN ? CF(o_m1, gdyh) : p.gd) * hun;
-                double a = (c.U + un * hun) * p.c4, b = (c.slx + slxn) * p.c4;
-                if (ACC == 2) { a += p.acc[0][idx]; b += p.acc[2][idx]; }
-                p.acc[0][idx] = a;
-                p.acc[2][idx] = b;
-            }
-            if (WRITE && wu) {
-                p.dst[S_UP][idx] = u_r + gam * (un - 2.0 * u_r + up_r);
-                p.dst[S_U][idx] = un;
-            }
-            if (WRITE && wt) {   // vel_ssh.f90:593-596
-                p.dst[S_SSHP][idx] = e0 + gam * (sn - 2.0 * e0 + sp0);
-                p.dst[S_SSH][idx] = sn;
+        if constexpr (D3U) {
+            const uint32_t mr = (mk >> 4) & 3u;
+            if (__any_sync(0xffffffffu, out && (mr & 1u))) {
+                const int lc = mr & 1, lr = (mr >> 1) & 1;
+                const bool wu = out && (lc & lr), wt = out && lc;
+                const double e0 = AS(o_m1, S_SSH, 0);
+                const double sp0 = AS(o_m1, S_SSHP, 0), sp1 = AS(o_m1, S_SSHP, 1);
+                const double h0 = AT(o_m1, T_H, 0), h1 = AT(o_m1, T_H, 1);
+                // vel_ssh.f90:536-551
+                const double ku2 = GEN ? CF(o_m1, ku2) : 0.5;
+                const double hup = ((h0 + sp0) + (h1 + sp1)) * ku2;
+                const double hun = ((h0 + sn) + (h1 + SNr)) * ku2;
+                const double difx = GEN ? (STr - ST) * CF(o_m1, dux) + SS * CF(o_m1, dus0) : ((STr - ST) + SS) * p.d;
+                const double grx = c.Ru + qc.Cu - ((FXr - FX) + FY) + difx + QU * 0.25;
+                const double un = (up_r * hup + grx * (GEN ? two_ti * CF(o_m1, rau) : p.tt)) * rcp_nr(hun);
+                bad |= (uint32_t)(wu && !(fabs(un) < 100.0));
+                bad |= (uint32_t)(wt && !(fabs(sn) < 10.0));
+                const long long idx = gi - p.pitch;
+                if (ACC && wu) {
+                    const double slxn = -(SNr - sn) * (GEN ? CF(o_m1, gdyh) : p.gd) * hun;
+                    double a = (c.U + un * hun) * p.c4, b = (c.slx + slxn) * p.c4;
+                    if (ACC == 2) { a += p.acc[0][idx]; b += p.acc[2][idx]; }
+                    p.acc[0][idx] = a;
+                    p.acc[2][idx] = b;
+                }
+                if (WRITE && wu) {
+                    p.dst[S_UP][idx] = u_r + gam * (un - 2.0 * u_r + up_r);
+                    p.dst[S_U][idx] = un;
+                }
+                if (WRITE && wt) {   // vel_ssh.f90:593-596
+                    p.dst[S_SSHP][idx] = e0 + gam * (sn - 2.0 * e0 + sp0);
+                    p.dst[S_SSH][idx] = sn;
+                }
             }
         }
 
         // ---------------- stage 3v: row R = j-2 (v) ----------------------
-        const uint32_t mR = (mk >> 6) & 3u, mU = (mk >> 4) & 3u;   // rows R, R+1
-        if (j >= r0 + 2 && j <= r1 + 1 && __any_sync(0xffffffffu, out && (mR & mU & 1u))) {
-            const bool wv = out && (mR & mU & 1u);
-            const double sp0 = AS(o_m2, S_SSHP, 0), sp1 = AS(o_m1, S_SSHP, 0);
-            const double h0 = AT(o_m2, T_H, 0), h1 = AT(o_m1, T_H, 0);
-            const double v0 = v_m, vp0 = vp_m;
-            const double sn0 = qc.sn, sn1 = sn;
-            // vel_ssh.f90:554-569
-            double hvp, hvn;
-            if constexpr (GEN) {
-                hvp = ((h0 + sp0) * CF(o_m2, wv0) + (h1 + sp1) * CF(o_m2, wv1)) * 0.5;
-                hvn = ((h0 + sn0) * CF(o_m2, wv0) + (h1 + sn1) * CF(o_m2, wv1)) * 0.5;
-            } else {
-                hvp = ((h0 + sp0) + (h1 + sp1)) * 0.5;
-                hvn = ((h0 + sn0) + (h1 + sn1)) * 0.5;
-            }
-            const double gry = qc.Pv - GY - ST * (GEN ? CF(o_m2, dvt1) : p.d);
-            const double vn = (vp0 * hvp + gry * (GEN ? two_ti * CF(o_m2, rav) : p.tt)) * rcp_nr(hvn);
-            bad |= (uint32_t)(wv && !(fabs(vn) < 100.0));
-            const long long idx = gi - 2 * p.pitch;
-            if (ACC && wv) {
-                const double slyn = -(sn1 - sn0) * (GEN ? CF(o_m2, gdxh) : p.gd) * hvn;
-                double a = (qc.V + vn * hvn) * p.c4, b = (qc.sly + slyn) * p.c4;
-                if (ACC == 2) { a += p.acc[1][idx]; b += p.acc[3][idx]; }
-                p.acc[1][idx] = a;
-                p.acc[3][idx] = b;
-            }
-            if (WRITE && wv) {
-                p.dst[S_VP][idx] = v0 + gam * (vn - 2.0 * v0 + vp0);
-                p.dst[S_V][idx] = vn;
+        if constexpr (D3V) {
+            // vel_ssh.f90:88-98 the x flux of v on the h point of row R,
+            // from the transports of rows R and R+1
+            const double GX = (GEN ? qc.Uo * CF(o_m2, gx0) + c.U * CF(o_m2, gx1) : (qc.Uo + c.U) * p.d4) * qc.vs;
+            const double GXl = SHFL_UP(GX);
+            const uint32_t mR = (mk >> 6) & 3u, mU = (mk >> 4) & 3u;   // rows R, R+1
+            if (__any_sync(0xffffffffu, out && (mR & mU & 1u))) {
+                const bool wv = out && (mR & mU & 1u);
+                const double sp0 = AS(o_m2, S_SSHP, 0), sp1 = AS(o_m1, S_SSHP, 0);
+                const double h0 = AT(o_m2, T_H, 0), h1 = AT(o_m1, T_H, 0);
+                const double v0 = v_m, vp0 = vp_m;
+                const double sn0 = qc.sn, sn1 = sn;
+                // vel_ssh.f90:554-569
+                double hvp, hvn;
+                if constexpr (GEN) {
+                    hvp = ((h0 + sp0) * CF(o_m2, wv0) + (h1 + sp1) * CF(o_m2, wv1)) * 0.5;
+                    hvn = ((h0 + sn0) * CF(o_m2, wv0) + (h1 + sn1) * CF(o_m2, wv1)) * 0.5;
+                } else {
+                    hvp = ((h0 + sp0) + (h1 + sp1)) * 0.5;
+                    hvn = ((h0 + sn0) + (h1 + sn1)) * 0.5;
+                }
+                const double gry = qc.Pv - (GX - GXl) - GY - ST * (GEN ? CF(o_m2, dvt1) : p.d);
+                const double vn = (vp0 * hvp + gry * (GEN ? two_ti * CF(o_m2, rav) : p.tt)) * rcp_nr(hvn);
+                bad |= (uint32_t)(wv && !(fabs(vn) < 100.0));
+                const long long idx = gi - 2 * p.pitch;
+                if (ACC && wv) {
+                    const double slyn = -(sn1 - sn0) * (GEN ? CF(o_m2, gdxh) : p.gd) * hvn;
+                    double a = (qc.V + vn * hvn) * p.c4, b = (qc.sly + slyn) * p.c4;
+                    if (ACC == 2) { a += p.acc[1][idx]; b += p.acc[3][idx]; }
+                    p.acc[1][idx] = a;
+                    p.acc[3][idx] = b;
+                }
+                if (WRITE && wv) {
+                    p.dst[S_VP][idx] = v0 + gam * (vn - 2.0 * v0 + vp0);
+                    p.dst[S_V][idx] = vn;
+                }
             }
         }
 
         // ---------------- carry row rho on ------------------------------
-        // its part of the u equation of row rho+1 (vel_ssh.f90:539-541):
-        // +FY(rho), -SS(rho)*dxb(rho)^2/dxt(rho+1), +QU(rho)/4
-        q.Cu = FY + QU * 0.25 - SS * (GEN ? CF(o_0, dus1) : p.d);
-        // its part of its own v equation (vel_ssh.f90:557-560); the row
-        // above adds -GY(rho+1) and -ST(rho+1)*dx(rho+1)^2/dxh(rho)
-        const double dify = GEN ? ST * CF(o_m1, dvt0) + (SS - SSl) * CF(o_m1, dvs) : (ST + (SS - SSl)) * p.d;
-        q.Pv = c.Rv + (GY - (GX - GXl)) + dify - (QV + QVl) * 0.25;
-        q.sn = sn;
+        if constexpr (D2) {
+            // its part of the u equation of row rho+1 (vel_ssh.f90:539-541):
+            // +FY(rho), -SS(rho)*dxb(rho)^2/dxt(rho+1), +QU(rho)/4
+            q.Cu = FY + QU * 0.25 - SS * (GEN ? CF(o_0, dus1) : p.d);
+            // its part of its own v equation (vel_ssh.f90:557-560); the
+            // next iteration adds -(GX - GX(k-1)), -GY(rho+1) and
+            // -ST(rho+1)*dx(rho+1)^2/dxh(rho)
+            const double dify = GEN ? ST * CF(o_m1, dvt0) + (SS - SSl) * CF(o_m1, dvs) : (ST + (SS - SSl)) * p.d;
+            q.Pv = c.Rv + GY + dify - (QV + QVl) * 0.25;
+            q.sn = sn;
+            q.vs = vs;
+        }
         q.V = c.V;
+        q.Uo = c.U;
         q.hqm = c.hq;
         if (ACC) q.sly = c.sly;
 
         // row j-2 was last read above: once every lane is past it, its slot
         // takes row j-2+RING
         __syncwarp();
-        if (l == 0 && j - 2 >= row_lo && j + 4 <= row_hi) issue(j + 4, i_m2), issued = j + 4;
+        if (j - 2 >= row_lo && j + 4 <= row_hi) {
+            issue(j + 4, i_m2);
+            issued = j + 4;
+        }
         i_m2 = i_m1;
         i_m1 = i_0;
         i_0 = i_p1;
@@ -478,11 +528,22 @@ __global__ void __launch_bounds__(NL, Layout<GEN>::min_ctas) k_substep(const __g
     };
 
     // two instances of each carried struct, renamed (not copied) by the
-    // two-fold unrolled loop
-    for (int j = r0 - 1; j <= r1 + 1 && ok; j += 2) {
-        step(j, A, B, X, Y);
-        if (!ok) break;
-        step(j + 1, B, A, Y, X);
+    // two-fold unrolled loop; iterations r0-1, r0, r0+1 and r1+1 lack stages
+    const On<true> Y1;
+    const On<false> N0;
+    step(r0 - 1, Y1, N0, N0, N0, A, B, X, Y);
+    step(r0, Y1, Y1, N0, N0, B, A, Y, X);
+    step(r0 + 1, Y1, Y1, Y1, N0, A, B, X, Y);
+    int j = r0 + 2;
+    for (; j + 1 <= r1 && ok; j += 2) {
+        step(j, Y1, Y1, Y1, Y1, B, A, Y, X);
+        step(j + 1, Y1, Y1, Y1, Y1, A, B, X, Y);
+    }
+    if (j <= r1) {
+        step(j, Y1, Y1, Y1, Y1, B, A, Y, X);
+        step(j + 1, N0, Y1, N0, Y1, A, B, X, Y);
+    } else {
+        step(j, N0, Y1, N0, Y1, B, A, Y, X);
     }
     if (__any_sync(0xffffffffu, bad != 0) && l == 0) atomicOr(p.flags, FLAG_GUARD);
     if (!ok && l == 0) {
@@ -580,8 +641,6 @@ Params base_params(const Plan &p, const Dom &d, const Consts &c, const Forcing &
     q.cor = p.cor;
     q.pitch = d.pitch;
     q.bm_words = p.bm_words;
-    q.r_first = d.ny_start - d.bnd_y1;
-    q.r_last = d.ny_end - d.bnd_y1;
     q.c_first = d.nx_start - d.bnd_x1 + d.xoff;
     q.c_last = d.nx_end - d.bnd_x1 + d.xoff;
     q.mu0 = f.mu0;
@@ -596,7 +655,7 @@ Params base_params(const Plan &p, const Dom &d, const Consts &c, const Forcing &
     q.d4 = p.d / 4.0;
     q.gd = c.g * p.d;
     q.d2 = p.d * p.d;
-    q.chunk_rows = p.chunk_rows[gen];
+    q.items = p.items[gen];
     return q;
 }
 
@@ -621,7 +680,7 @@ int set_io(const Plan &p, Params &q, double *const src[NSET], double *const dst[
 template <bool GEN, int MODE>
 void launch_t(const Plan &p, const Params &q, cudaStream_t s)
 {
-    dim3 grid(p.nstrips, p.nchunks[GEN ? 1 : 0]);
+    dim3 grid(p.nitems[GEN ? 1 : 0]);
     k_substep<GEN, MODE><<<grid, NL, Layout<GEN>::bytes, s>>>(q);
 }
 
@@ -690,6 +749,72 @@ int encode_fields(EncodeTiled enc, CUtensorMap *map, double *base, const Dom &d,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS;
 }
 
+// Work items of one variant: each strip's interior rows cut into chunks of
+// about equal cost, as many in all as one wave of resident CTAs holds, so
+// that the wave finishes together.  A row whose written columns are all land
+// skips the momentum stages and costs about LAND_COST of an ocean row; no
+// chunk is shorter than MIN_ROWS rows (each pays three warm-up iterations).
+constexpr double LAND_COST = 0.7;
+constexpr int MIN_ROWS = 16;
+
+std::vector<int4> partition(const Plan &p, const Dom &d, const float *lu, int slots)
+{
+    const int nxa = d.nxa();
+    const int rf = d.ny_start - d.bnd_y1, rl = d.ny_end - d.bnd_y1;   // interior device rows
+    const int cf = d.nx_start - d.bnd_x1 + d.xoff, cl = d.nx_end - d.bnd_x1 + d.xoff;
+    const int ny = rl - rf + 1;
+    std::vector<std::vector<double>> cost(p.nstrips, std::vector<double>(ny));
+    std::vector<double> total(p.nstrips, 0.0);
+    double all = 0.0;
+    for (int s = 0; s < p.nstrips; s++) {
+        const int g0 = s * p.outw;
+        const int c0 = std::max(g0 + 3, cf), c1 = std::min(g0 + 2 + p.outw, cl);   // written columns
+        for (int r = rf; r <= rl; r++) {
+            bool ocean = false;
+            for (int col = c0; col <= c1 && !ocean; col++) ocean = lu[(size_t)r * nxa + (col - d.xoff)] > 0.5f;
+            cost[s][r - rf] = ocean ? 1.0 : LAND_COST;
+            total[s] += cost[s][r - rf];
+        }
+        all += total[s];
+    }
+    // chunks per strip in proportion to its cost (largest remainder)
+    const int maxc = std::max(1, ny / MIN_ROWS);
+    const int want = std::min(std::max(slots, p.nstrips), p.nstrips * maxc);
+    std::vector<int> n(p.nstrips);
+    std::vector<std::pair<double, int>> frac;
+    int used = 0;
+    for (int s = 0; s < p.nstrips; s++) {
+        const double exact = all > 0.0 ? want * total[s] / all : 1.0;
+        n[s] = std::min(maxc, std::max(1, (int)exact));
+        used += n[s];
+        frac.push_back({exact - (int)exact, s});
+    }
+    std::sort(frac.begin(), frac.end(), [](const std::pair<double, int> &a, const std::pair<double, int> &b) {
+        return a.first > b.first;
+    });
+    for (size_t t = 0; used < want && t < frac.size(); t++)
+        if (n[frac[t].second] < maxc) n[frac[t].second]++, used++;
+    // cut each strip at equal shares of its cumulative cost
+    std::vector<int4> items;
+    for (int s = 0; s < p.nstrips; s++) {
+        const double share = total[s] / n[s];
+        double acc = 0.0;
+        int start = rf, made = 0;
+        for (int r = rf; r <= rl; r++) {
+            acc += cost[s][r - rf];
+            const bool last_row = r == rl;
+            const bool cut = made < n[s] - 1 && acc >= share * (made + 1) && r - start + 1 >= 1 &&
+                             rl - r >= n[s] - 1 - made;
+            if (cut || last_row) {
+                items.push_back(make_int4(s * p.outw, start, r + 1, 0));
+                start = r + 1;
+                made++;
+            }
+        }
+    }
+    return items;
+}
+
 void release(Plan &p)
 {
     cudaFree(p.rows);
@@ -701,6 +826,9 @@ void release(Plan &p)
     cudaFree(p.stat);
     cudaFree(p.d_uniform);
     cudaFree(p.d_flags);
+    cudaFree(p.items[0]);
+    cudaFree(p.items[1]);
+    p.items[0] = p.items[1] = nullptr;
     p.rows = nullptr;
     p.cor = nullptr;
     p.bits = nullptr;
@@ -911,16 +1039,17 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
         occ[1] = 1;
     p.occ[0] = occ[0];
     p.occ[1] = occ[1];
-    // one wave: strips x chunks <= SMs x resident CTAs, chunks as tall as
-    // that allows; each chunk re-reads and recomputes three rows of warm-up,
-    // so keep chunks at least 16 rows tall
-    const int ny = d.ny_end - d.ny_start + 1;
+    const float *lu_h = masks[0];
     for (int v = 0; v < 2; v++) {
-        int nchunks = std::max(1, nsm * occ[v] / p.nstrips);
-        nchunks = std::min(nchunks, std::max(1, (ny + 15) / 16));
-        p.chunk_rows[v] = (ny + nchunks - 1) / nchunks;
-        p.nchunks[v] = (ny + p.chunk_rows[v] - 1) / p.chunk_rows[v];
+        std::vector<int4> items = partition(p, d, lu_h, nsm * occ[v]);
+        p.nitems[v] = (int)items.size();
+        if (cudaMalloc(&p.items[v], items.size() * sizeof(int4)) != cudaSuccess) return 1;
+        if (cudaMemcpyAsync(p.items[v], items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, s) !=
+            cudaSuccess)
+            return 1;
     }
+    // the work tables are host vectors: finish their copies before returning
+    if (cudaStreamSynchronize(s) != cudaSuccess) return 1;
     return 0;
 }
 

@@ -71,7 +71,8 @@ struct Plan {
     int ncol = 32;            // columns per CTA (one warp, one column per lane)
     int outw = 30;            // output columns per CTA
     int nstrips = 0;
-    int nchunks[2] = {0, 0}, chunk_rows[2] = {0, 0};   // per variant: uniform, general
+    int nitems[2] = {0, 0};         // work items per variant: uniform, general
+    int4 *items[2] = {nullptr, nullptr};   // {g0, first row, end row, 0} per item
     bool uni = false;         // metrics all equal one spacing d (square uniform grid)
     double d = 0.0;           // that spacing
     long long min_pitch = 0;  // device row pitch the strips need
