@@ -98,6 +98,20 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
+// non-blocking: has the phase with this parity completed?
+__device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.test_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
 __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
 {
     for (unsigned i = 0; i < WAIT_LIMIT; i++)
@@ -118,11 +132,17 @@ struct Layout {
 };
 
 // resident CTAs per SM the register budget is cut for: 13 one-warp CTAs
-// (4 warps per SM sub-partition, 128 registers) for the plain substep,
-// 12 where the time-mean sums need more registers; the general variant's
-// larger ring allows 9
+// (4 warps per SM sub-partition, 128 registers) for the plain substep, 12
+// where the time-mean sums need more registers, 9 for the general variant,
+// and never more than the shared memory holds (228 KB per SM, 1 KB of it
+// reserved per CTA)
 template <bool GEN, int MODE>
-constexpr int min_ctas() { return GEN ? 9 : (MODE % 3 ? 12 : 13); }
+constexpr int min_ctas()
+{
+    constexpr int by_smem = (int)(233472 / (Layout<GEN>::bytes + 1024));
+    constexpr int want = GEN ? 9 : (MODE % 3 ? 12 : 13);
+    return by_smem < want ? by_smem : want;
+}
 static_assert(NSET * SEG * 8 <= 1792, "state segment overlaps the static segment");
 static_assert(Layout<false>::COEF_OFF % 16 == 0 && Layout<true>::BITS_OFF % 16 == 0, "bulk copy alignment");
 
@@ -276,6 +296,7 @@ __global__ void __launch_bounds__(NL, min_ctas<GEN, MODE>()) k_substep(const __g
     uint32_t mk = 0;
     uint32_t bad = 0;   // guard: a new value out of range or NaN
     int waited = row_lo - 1;
+    bool ready = false;   // row j+1 found complete by a test in the previous iteration
     bool ok = mbar_wait(&mbar[0], 0);
     ok = __all_sync(0xffffffffu, ok && mbar_wait(&mbar[1], 0));
     if (ok) waited = row_lo + 1;
@@ -299,8 +320,10 @@ __global__ void __launch_bounds__(NL, min_ctas<GEN, MODE>()) k_substep(const __g
         if (!ok) return;
         const int o_m2 = i_m2 * L::SLOT_B, o_m1 = i_m1 * L::SLOT_B, o_0 = i_0 * L::SLOT_B, o_p1 = i_p1 * L::SLOT_B;
         if constexpr (D1) {   // stage 1 reads row j+1
-            ok = __all_sync(0xffffffffu, mbar_wait(&mbar[i_p1], ph));
-            if (!ok) return;
+            if (!__all_sync(0xffffffffu, ready)) {
+                ok = __all_sync(0xffffffffu, mbar_wait(&mbar[i_p1], ph));
+                if (!ok) return;
+            }
             waited = j + 1;
             mk = (mk << 2) | mask2(o_p1);
         } else {
@@ -416,6 +439,12 @@ __global__ void __launch_bounds__(NL, min_ctas<GEN, MODE>()) k_substep(const __g
             n.Ul = SHFL_UP(n.U);
             n.Vr = SHFL_DN(n.V);
         }
+        // test (without waiting) whether row j+2 has arrived, so that the
+        // next iteration's branch on it does not wait for the test
+        {
+            const int ns = i_p1 == RING - 1 ? 0 : i_p1 + 1;
+            ready = mbar_test(&mbar[ns], ph ^ (ns == 0 ? 1u : 0u));
+        }
 
         // ---------------- stage 3u: row rho = j-1 (u and SSH) -----------
         if constexpr (D3U) {
@@ -515,9 +544,9 @@ __global__ void __launch_bounds__(NL, min_ctas<GEN, MODE>()) k_substep(const __g
         // row j-2 was last read above: once every lane is past it, its slot
         // takes row j-2+RING
         __syncwarp();
-        if (j - 2 >= row_lo && j + 4 <= row_hi) {
-            issue(j + 4, i_m2);
-            issued = j + 4;
+        if (j - 2 >= row_lo && j - 2 + RING <= row_hi) {
+            issue(j - 2 + RING, i_m2);
+            issued = j - 2 + RING;
         }
         i_m2 = i_m1;
         i_m1 = i_0;
