@@ -66,6 +66,7 @@ struct alignas(64) Params {
     const RowCoef *rows;
     const double *cor;
     const int4 *items;     // work items {g0, first row, end row (exclusive), 0}
+    const double *rx, *ry; // RHSx, RHSy (fields of the static block)
     long long pitch;
     int bm_words;
     int c_first, c_last;   // interior device columns
@@ -98,6 +99,11 @@ __device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
+__device__ __forceinline__ void mbar_inval(uint64_t *bar)
+{
+    asm volatile("mbarrier.inval.shared::cta.b64 [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
 // non-blocking: has the phase with this parity completed?
 __device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity)
 {
@@ -121,7 +127,7 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
 
 template <bool GEN>
 struct Layout {
-    static constexpr int NS = GEN ? NSTAT : 3;                   // static fields in a slot
+    static constexpr int NS = GEN ? 4 : 1;                       // static fields in a slot
     static constexpr int STAT_OFF = 1792;                        // after 6*SEG doubles, 128-aligned
     static constexpr int COEF_OFF = STAT_OFF + NS * SEG * 8;     // general variant: RowCoef
     static constexpr int BITS_OFF = COEF_OFF + (GEN ? (int)sizeof(RowCoef) : 0);
@@ -131,16 +137,16 @@ struct Layout {
         (uint32_t)(NSET * SEG * 8 + NS * SEG * 8 + (GEN ? (int)sizeof(RowCoef) : 0) + 32);
 };
 
-// resident CTAs per SM the register budget is cut for: 13 one-warp CTAs
+// resident CTAs per SM the register budget is cut for: 16 one-warp CTAs
 // (4 warps per SM sub-partition, 128 registers) for the plain substep, 12
-// where the time-mean sums need more registers, 9 for the general variant,
+// where the time-mean sums need more registers, 11 for the general variant,
 // and never more than the shared memory holds (228 KB per SM, 1 KB of it
 // reserved per CTA)
 template <bool GEN, int MODE>
 constexpr int min_ctas()
 {
     constexpr int by_smem = (int)(233472 / (Layout<GEN>::bytes + 1024));
-    constexpr int want = GEN ? 9 : (MODE % 3 ? 12 : 13);
+    constexpr int want = GEN ? 11 : (MODE % 3 ? 12 : 16);
     return by_smem < want ? by_smem : want;
 }
 static_assert(NSET * SEG * 8 <= 1792, "state segment overlaps the static segment");
@@ -242,19 +248,22 @@ struct S2 {
 template <bool B>
 using On = std::integral_constant<bool, B>;
 
+// One substep of one work item (a chunk of rows of a strip), by one warp:
+// reads the source set through *tm_src, writes dst[] (and the time-mean
+// sums), RHS scaled by rs.  The ring and its mbarriers are this CTA's
+// shared memory; they are initialised here and left invalidated (ready for
+// the next call) when the item completes.  Returns false after a wait that
+// gave up (FLAG_TIMEOUT is set).
 // MODE = acc + 3*write: acc 0 none, 1 first substep (write), 2 accumulate;
 // write 1 stores the new state
 template <bool GEN, int MODE>
-__global__ void __launch_bounds__(NL, min_ctas<GEN, MODE>()) k_substep(const __grid_constant__ Params p)
+__device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap *tm_src, double *const *dst,
+                                             const double rs, const int4 item, unsigned char *ring, uint64_t *mbar)
 {
     using L = Layout<GEN>;
     constexpr int ACC = MODE % 3;
     constexpr bool WRITE = MODE / 3 != 0;
-    extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char *ring = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
-    uint64_t *mbar = reinterpret_cast<uint64_t *>(ring + RING * L::SLOT_B);
 
-    const int4 item = p.items[blockIdx.x];
     const int l = threadIdx.x;
     const int g0 = item.x;                     // device column of segment offset 0
     const int k = g0 + 2 + l;                  // this lane's column
@@ -270,7 +279,7 @@ __global__ void __launch_bounds__(NL, min_ctas<GEN, MODE>()) k_substep(const __g
 #define CF(o, x) (reinterpret_cast<const RowCoef *>(ring + (o) + L::COEF_OFF)->x)
 
     auto issue = [&](int row, int slot) {
-        issue_row<GEN>(ring + slot * L::SLOT_B, &mbar[slot], &p.tm_src, &p.tm_stat, p.rows + row,
+        issue_row<GEN>(ring + slot * L::SLOT_B, &mbar[slot], tm_src, &p.tm_stat, p.rows + row,
                        p.bits + (size_t)row * p.bm_words + wbase, g0, row);
     };
     auto mask2 = [&](int o) -> uint32_t {   // bits: lu(k), lu(k+1)
@@ -287,7 +296,7 @@ __global__ void __launch_bounds__(NL, min_ctas<GEN, MODE>()) k_substep(const __g
     for (int t = 0; t < RING && row_lo + t <= row_hi; t++) issue(row_lo + t, t), issued = row_lo + t;
 
     const bool out = l >= 1 && l <= NL - 2 && k >= p.c_first && k <= p.c_last;
-    const double gam = p.gam, two_ti = p.two_ti, rs = p.rhs_scale;
+    const double gam = p.gam, two_ti = p.two_ti;
 
     // slots of rows j-2, j-1, j, j+1 and the fill parity of row j+1
     int i_m2 = RING - 1, i_m1 = 0, i_0 = 1, i_p1 = 2;
@@ -366,13 +375,18 @@ __global__ void __launch_bounds__(NL, min_ctas<GEN, MODE>()) k_substep(const __g
                 au = av = p.d2;
                 n.cor = p.cor[j];
             }
-            n.Ru = AT(o_0, T_RX, 0) * rs + slx - rdu * AS(o_0, S_UP, 0) * au * hu;
-            n.Rv = AT(o_0, T_RY, 0) * rs + sly - rdv * AS(o_0, S_VP, 0) * av * hv;
+            n.Ru = slx - rdu * AS(o_0, S_UP, 0) * au * hu;
+            n.Rv = sly - rdv * AS(o_0, S_VP, 0) * av * hv;
             if (ACC) {
                 n.slx = slx;
                 n.sly = sly;
             }
         }
+
+        // forcing of the rows that stage 3 updates, loaded early
+        double rxf = 0.0, ryf = 0.0;
+        if constexpr (D3U) rxf = p.rx[gi - p.pitch];
+        if constexpr (D3V) ryf = p.ry[gi - 2 * p.pitch];
 
         // ---------------- stage 2: row rho = j-1 -------------------------
         double FX, FY, GY, ST, SS, QU, QV, sn, vs, u_r, up_r, v_m, vp_m;
@@ -460,7 +474,7 @@ __global__ void __launch_bounds__(NL, min_ctas<GEN, MODE>()) k_substep(const __g
                 const double hup = ((h0 + sp0) + (h1 + sp1)) * ku2;
                 const double hun = ((h0 + sn) + (h1 + SNr)) * ku2;
                 const double difx = GEN ? (STr - ST) * CF(o_m1, dux) + SS * CF(o_m1, dus0) : ((STr - ST) + SS) * p.d;
-                const double grx = c.Ru + qc.Cu - ((FXr - FX) + FY) + difx + QU * 0.25;
+                const double grx = rxf * rs + c.Ru + qc.Cu - ((FXr - FX) + FY) + difx + QU * 0.25;
                 const double un = (up_r * hup + grx * (GEN ? two_ti * CF(o_m1, rau) : p.tt)) * rcp_nr(hun);
                 bad |= (uint32_t)(wu && !(fabs(un) < 100.0));
                 bad |= (uint32_t)(wt && !(fabs(sn) < 10.0));
@@ -473,12 +487,12 @@ __global__ void __launch_bounds__(NL, min_ctas<GEN, MODE>()) k_substep(const __g
                     p.acc[2][idx] = b;
                 }
                 if (WRITE && wu) {
-                    p.dst[S_UP][idx] = u_r + gam * (un - 2.0 * u_r + up_r);
-                    p.dst[S_U][idx] = un;
+                    dst[S_UP][idx] = u_r + gam * (un - 2.0 * u_r + up_r);
+                    dst[S_U][idx] = un;
                 }
                 if (WRITE && wt) {   // vel_ssh.f90:593-596
-                    p.dst[S_SSHP][idx] = e0 + gam * (sn - 2.0 * e0 + sp0);
-                    p.dst[S_SSH][idx] = sn;
+                    dst[S_SSHP][idx] = e0 + gam * (sn - 2.0 * e0 + sp0);
+                    dst[S_SSH][idx] = sn;
                 }
             }
         }
@@ -505,7 +519,7 @@ __global__ void __launch_bounds__(NL, min_ctas<GEN, MODE>()) k_substep(const __g
                     hvp = ((h0 + sp0) + (h1 + sp1)) * 0.5;
                     hvn = ((h0 + sn0) + (h1 + sn1)) * 0.5;
                 }
-                const double gry = qc.Pv - (GX - GXl) - GY - ST * (GEN ? CF(o_m2, dvt1) : p.d);
+                const double gry = ryf * rs + qc.Pv - (GX - GXl) - GY - ST * (GEN ? CF(o_m2, dvt1) : p.d);
                 const double vn = (vp0 * hvp + gry * (GEN ? two_ti * CF(o_m2, rav) : p.tt)) * rcp_nr(hvn);
                 bad |= (uint32_t)(wv && !(fabs(vn) < 100.0));
                 const long long idx = gi - 2 * p.pitch;
@@ -517,8 +531,8 @@ __global__ void __launch_bounds__(NL, min_ctas<GEN, MODE>()) k_substep(const __g
                     p.acc[3][idx] = b;
                 }
                 if (WRITE && wv) {
-                    p.dst[S_VP][idx] = v0 + gam * (vn - 2.0 * v0 + vp0);
-                    p.dst[S_V][idx] = vn;
+                    dst[S_VP][idx] = v0 + gam * (vn - 2.0 * v0 + vp0);
+                    dst[S_V][idx] = vn;
                 }
             }
         }
@@ -575,15 +589,34 @@ __global__ void __launch_bounds__(NL, min_ctas<GEN, MODE>()) k_substep(const __g
         step(j, N0, Y1, N0, Y1, B, A, Y, X);
     }
     if (__any_sync(0xffffffffu, bad != 0) && l == 0) atomicOr(p.flags, FLAG_GUARD);
-    if (!ok && l == 0) {
-        atomicOr(p.flags, FLAG_TIMEOUT);
-        // drain this CTA's copies still in flight (bounded) before exiting
-        for (int row = waited + 1; row <= issued; row++)
-            (void)mbar_wait(&mbar[(row - row_lo) % RING], (uint32_t)(((row - row_lo) / RING) & 1));
+    if (!ok) {
+        if (l == 0) {
+            atomicOr(p.flags, FLAG_TIMEOUT);
+            // drain this CTA's copies still in flight (bounded) before exiting
+            for (int row = waited + 1; row <= issued; row++)
+                (void)mbar_wait(&mbar[(row - row_lo) % RING], (uint32_t)(((row - row_lo) / RING) & 1));
+        }
+        return false;
     }
+    // every copy issued was waited for: the barriers can be retired
+    __syncwarp();
+    if (l == 0)
+        for (int t = 0; t < RING; t++) mbar_inval(&mbar[t]);
+    __syncwarp();
+    return true;
 #undef AS
 #undef AT
 #undef CF
+}
+
+template <bool GEN, int MODE>
+__global__ void __launch_bounds__(NL, min_ctas<GEN, MODE>()) k_substep(const __grid_constant__ Params p)
+{
+    using L = Layout<GEN>;
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *ring = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+    uint64_t *mbar = reinterpret_cast<uint64_t *>(ring + RING * L::SLOT_B);
+    (void)substep_item<GEN, MODE>(p, &p.tm_src, p.dst, p.rhs_scale, p.items[blockIdx.x], ring, mbar);
 }
 
 // min/max over the ocean points of three fields, for the uniform-forcing test
@@ -653,9 +686,10 @@ int forcing_mode(Plan &p, const Dom &d, const Consts &c, double *forc[6], cudaSt
 int stage_forcing(Plan &p, double *forc[6], int gen, cudaStream_t s)
 {
     const size_t fb = (size_t)p.fstride * sizeof(double);
-    const int src_of[NSTAT] = {-1, 0, 1, 3, 5, 2};   // T_* <- forc index (RHSx RHSy wflux mu mu4 rdis)
-    for (int t = T_RX; t < (gen ? NSTAT : 3); t++)
-        if (cudaMemcpyAsync(p.stat + t * p.fstride, forc[src_of[t]], fb, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
+    const int src_of[NSTAT] = {-1, 3, 5, 2, 0, 1};   // T_* <- forc index (RHSx RHSy wflux mu mu4 rdis)
+    for (int t = 1; t < NSTAT; t++)
+        if ((gen || t >= T_RX) &&
+            cudaMemcpyAsync(p.stat + t * p.fstride, forc[src_of[t]], fb, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
             return 1;
     return 0;
 }
@@ -685,6 +719,8 @@ Params base_params(const Plan &p, const Dom &d, const Consts &c, const Forcing &
     q.gd = c.g * p.d;
     q.d2 = p.d * p.d;
     q.items = p.items[gen];
+    q.rx = p.stat + T_RX * p.fstride;
+    q.ry = p.stat + T_RY * p.fstride;
     return q;
 }
 

@@ -41,8 +41,10 @@ constexpr int XOFF = 1;   // device padding columns before bnd_x1 (see common.cu
 
 // fields of a state set, in memory order (the *_e argument order)
 enum { S_U, S_UP, S_V, S_VP, S_SSH, S_SSHP, NSET };
-// fields of the static block: rest depth, RHSx, RHSy, mu, rdis, wflux
-enum { T_H, T_RX, T_RY, T_MU, T_RD, T_WF, NSTAT };
+// fields of the static block: rest depth, mu, rdis, wflux (those the ring
+// holds: H alone in the uniform variant, all four in the general one),
+// then RHSx, RHSy (read directly where they are used)
+enum { T_H, T_MU, T_RD, T_WF, T_RX, T_RY, NSTAT };
 
 // per-row coefficients, row index = device row (n - bnd_y1); 38 doubles so
 // that a row is a whole number of 16-byte units for the bulk copies
@@ -86,7 +88,7 @@ struct Plan {
     double *stat = nullptr;         // static block, NSTAT fields
     long long fstride = 0;          // doubles between the fields of a block
     CUtensorMap tm_set[3];          // box {36, 1, 6} over each state set
-    CUtensorMap tm_stat[2];         // box {36, 1, 3 | 6} over the static block
+    CUtensorMap tm_stat[2];         // box {36, 1, 1 | 4} over the static block
     int occ[2] = {0, 0};            // resident CTAs per SM, per variant
     double *d_uniform = nullptr;    // per-block min/max of mu, rdis, wflux
     unsigned *d_flags = nullptr;    // [0] status bits (guard / timeout)
