@@ -15,6 +15,13 @@ state evolution of barotropic_dynamics(tau=dt, nstep=1) keeping *_e.
   cpu_baseline  the CPU oracle (a line-by-line C restatement of the
          reference loops, OpenMP on all host threads) on a bounded sample.
 
+--fp32-velocity measures the same workload with u, up, v, vp stored in FP32
+on the device (80 algorithmic bytes per cell and substep; arithmetic, SSH
+and budgets FP64); the e2e arm stays FP64.
+--study fp32 runs the FP32-velocity variant against the FP64 run on the
+4096 x 4096 ridge basin (2 km, dt = 3 s) for --steps substeps and prints the
+per-field max/RMS differences (a study line, not a benchmark line).
+
 --impl reference runs only the CPU oracle arm (rank 0) and prints its line.
 Multi-GPU (torchrun): every rank runs its own basin replica (seed + rank);
 the time is the max over ranks and value sums the ranks' cells.
@@ -38,6 +45,7 @@ sys.path.insert(0, str(ROOT))
 
 METRIC = "grid-cell-steps/s"
 BYTES_PER_CELL_STEP = 120          # algorithmic FP64 bytes of one substep
+BYTES_PER_CELL_STEP_F32V = 80      # ... with u, up, v, vp and RHS in FP32
 E2E_NSTEP = 50                     # nstep_barotrop of ocean_run.par:9
 
 
@@ -53,6 +61,8 @@ def parse():
     p.add_argument("--cpu-seconds", type=float, default=15.0)
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
+    p.add_argument("--fp32-velocity", action="store_true")
+    p.add_argument("--study", default=None, choices=["fp32"])
     return p.parse_args()
 
 
@@ -271,7 +281,7 @@ def run_ours(args):
         return float(t.item())
 
     # ---- device-resident standalone run (value)
-    s = solver.BarotropicSolver(b, device=local, resident=True)
+    s = solver.BarotropicSolver(b, device=local, resident=True, fp32_velocity=args.fp32_velocity)
     path = s.path()
     s.load_state()
     warm = basins.wind_cycle(args.warmup, b.dt)
@@ -287,7 +297,8 @@ def run_ours(args):
     cells = b.cells
     value = cells * args.steps * ws / (ms / 1e3)
     per_launch_s = ms / 1e3 / args.steps
-    achieved = BYTES_PER_CELL_STEP * cells / per_launch_s / 1e9
+    bpc = BYTES_PER_CELL_STEP_F32V if args.fp32_velocity else BYTES_PER_CELL_STEP
+    achieved = bpc * cells / per_launch_s / 1e9
     peak, peak_kind = measured_hbm()
 
     # ---- e2e through the drop-in with pinned host buffers
@@ -304,7 +315,7 @@ def run_ours(args):
                          f"full basin in {el:.1f} s (10 substeps per call, 5 advancing steps), "
                          f"OpenMP {thr} threads"}
 
-    tr = ncu_traffic()
+    tr = None if args.fp32_velocity else ncu_traffic()
     traffic = None
     if tr and tr.get("cells"):
         traffic = tr["bytes_per_launch"] * cells / tr["cells"]
@@ -312,12 +323,13 @@ def run_ours(args):
         line = {
             "metric": METRIC, "value": value, "unit": METRIC, "n_gpus": ws, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True,
-            "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic",
+            "scaling": "weak", "vs_baseline": None,
+            "dtype": "f64 (u, v stored f32)" if args.fp32_velocity else "f64", "data": "synthetic",
             "config": config_dict(b, args, ws),
             "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                          "frac": achieved / peak, "traffic": traffic,
                          "kernel": "k_substep (fused leap-frog substep)",
-                         "bytes_per_cell_step": BYTES_PER_CELL_STEP,
+                         "bytes_per_cell_step": bpc,
                          "peak_kind": f"{peak_kind} HBM copy bandwidth"},
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
             "gpu_launches": args.steps + 1, "path": path[1], "guard_bad_points": nbad,
@@ -328,9 +340,46 @@ def run_ours(args):
         dist.destroy_process_group()
 
 
+def run_study_fp32(args):
+    """FP32 velocity storage against the FP64 run on the ridge basin."""
+    import torch
+    from inmsom_elfs_b200 import basins, solver
+    torch.cuda.set_device(0)
+    n = 4096 if args.nx == 2048 else args.nx
+    b = basins.ridge_basin(n=n)
+    basins.finalize(b, solver.GpuBackend(0))
+    out, ms, vol = {}, {}, {}
+    for fp32 in (False, True):
+        bg = b.copy()
+        with solver.BarotropicSolver(bg, resident=True, fp32_velocity=fp32) as s:
+            s.load_state()
+            v0, _ = s.diag()
+            ms[fp32] = s.run_substeps(args.steps, b.dt, basins.wind_cycle(args.steps, b.dt))
+            v1, e1 = s.diag()
+            s.sync_to_host()
+        out[fp32], vol[fp32] = bg, (v1 - v0) / v0
+    ocean = b.masks["lu"] > 0.5
+    errs = {}
+    for k in out[False].state:
+        a, r = out[True].state[k][ocean], out[False].state[k][ocean]
+        d = a - r
+        errs[k] = {"max_abs": float(np.abs(d).max()), "rms": float(np.sqrt(np.mean(d * d))),
+                   "ref_max_abs": float(np.abs(r).max()), "ref_rms": float(np.sqrt(np.mean(r * r))),
+                   "rel_max": float(np.abs(d).max() / max(np.abs(r).max(), 1e-300))}
+    print(json.dumps({
+        "study": "fp32_velocity", "workload": f"ridge_basin {n}x{n} 2 km dt 3 s, wind with a 6 h cycle",
+        "steps": args.steps, "fields": errs, "relative_volume_change": {"fp64": vol[False], "fp32_velocity": vol[True]},
+        "ms_per_step": {"fp64": ms[False] / args.steps, "fp32_velocity": ms[True] / args.steps},
+        "cell_steps_per_s": {"fp64": b.cells * args.steps / (ms[False] / 1e3),
+                             "fp32_velocity": b.cells * args.steps / (ms[True] / 1e3)},
+    }), flush=True)
+
+
 if __name__ == "__main__":
     a = parse()
-    if a.impl == "reference":
+    if a.study == "fp32":
+        run_study_fp32(a)
+    elif a.impl == "reference":
         run_reference(a)
     else:
         run_ours(a)

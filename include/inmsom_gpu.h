@@ -48,6 +48,16 @@ extern "C" {
 #define INMSOM_GUARD         0x4u /* after every call apply the range/NaN guard of
                                      Control/dyncall.f90:452-516 to the saved
                                      state; a trip returns INMSOM_EGUARD        */
+#define INMSOM_FP32_VELOCITY 0x8u /* inmsom_run_substeps keeps u, up, v, vp in
+                                     FP32 on the device for the run (80 instead
+                                     of 120 bytes per cell and substep); the
+                                     arithmetic, SSH, the rest depth and the
+                                     budgets stay FP64.  The FP64 state gets the
+                                     FP32 velocities back at the end of each
+                                     run.  Needs the fused path on a square
+                                     uniform grid with uniform viscosity, drag
+                                     and water flux (else INMSOM_EUNSUPPORTED);
+                                     barotropic_dynamics stays FP64.           */
 
 /* Domain bounds: Modules/mod_mpi_parallel_tools.f90:7-15 (local interior
  * nx_start..ny_end and array bounds bnd_x1..bnd_y2), global significant area

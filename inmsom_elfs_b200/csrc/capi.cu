@@ -426,6 +426,7 @@ int inmsom_gpu_register_grid(inmsom_ctx *c, const float *lu, const float *luu, c
                     ? INMSOM_OK
                     : set_err(INMSOM_ECUDA, "fused path set-up failed: %s",
                               cudaGetErrorString(cudaGetLastError())));
+            c->plan.f32 = (c->flags & INMSOM_FP32_VELOCITY) != 0;
             c->fused_ok = true;
             c->fused_reason = "eligible";
         }
@@ -540,10 +541,17 @@ int inmsom_run_substeps(inmsom_ctx *c, int nsub, double dt, const double *rhs_sc
     if (!(dt > 0.0)) return set_err(INMSOM_EARG, "dt must be > 0");
     if (!c->state_on_device)
         return set_err(INMSOM_EARG, "no resident state: call inmsom_load_state or barotropic_dynamics first");
+    if ((c->flags & INMSOM_FP32_VELOCITY) && !c->fused_ok)
+        return set_err(INMSOM_EUNSUPPORTED, "FP32 velocity storage needs the fused path (%s)", c->fused_reason);
     CK(cudaEventRecord(c->ev0, c->stream));
     if (c->fused_ok) {
-        if (fused::run_substeps(c->plan, c->dom, c->c, nsub, dt, rhs_scale, c->state, c->forc,
-                                c->stream))
+        const int rc = fused::run_substeps(c->plan, c->dom, c->c, nsub, dt, rhs_scale, c->state, c->forc,
+                                           c->stream);
+        if (rc == 2)
+            return set_err(INMSOM_EUNSUPPORTED,
+                           "FP32 velocity storage needs a square uniform grid with uniform viscosity, drag and "
+                           "water flux");
+        if (rc)
             return set_err(INMSOM_ECUDA, "fused substeps failed: %s",
                            cudaGetErrorString(cudaGetLastError()));
         c->depths_current = false;

@@ -60,7 +60,10 @@ constexpr unsigned WAIT_LIMIT = 1u << 20;
 struct alignas(64) Params {
     CUtensorMap tm_src;    // source state set {pitch, rows, 6 fields}, box {SEG, 1, 6}
     CUtensorMap tm_stat;   // static block, box {SEG, 1, Layout::NS}
+    CUtensorMap tm_ssh;    // FP32-velocity kernel: the source set's SSH fields, box {SEG, 1, 2}
     double *dst[NSET];
+    float *vdst[4];        // FP32-velocity kernel: u, up, v, vp of the destination
+    const float *rx32, *ry32;   // FP32-velocity kernel: RHSx, RHSy
     double *acc[4];
     const uint32_t *bits;
     const RowCoef *rows;
@@ -125,16 +128,24 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
     return false;
 }
 
-template <bool GEN>
+// Ring slot layout.  FP64 state: [6 state fields][static fields][RowCoef]
+// [mask bits].  FP32 velocities (uniform variant only): [u up v vp as FP32,
+// VSEG columns from g0 rounded down to a multiple of 4, so that the TMA
+// x-coordinate is 16-byte aligned for 4-byte elements][ssh sshp][H][bits].
+template <bool GEN, bool F32 = false>
 struct Layout {
-    static constexpr int NS = GEN ? 4 : 1;                       // static fields in a slot
-    static constexpr int STAT_OFF = 1792;                        // after 6*SEG doubles, 128-aligned
-    static constexpr int COEF_OFF = STAT_OFF + NS * SEG * 8;     // general variant: RowCoef
+    static_assert(!(GEN && F32), "FP32 velocities exist in the uniform variant only");
+    static constexpr int VSEG = F32 ? SEG + 4 : 0;                       // FP32 columns per velocity field
+    static constexpr int SSH_OFF = F32 ? (4 * VSEG * 4 + 127) / 128 * 128 : 0;
+    static constexpr int NS = GEN ? 4 : 1;                               // static fields in a slot
+    static constexpr int STAT_OFF = F32 ? (SSH_OFF + 2 * SEG * 8 + 127) / 128 * 128 : 1792;
+    static constexpr int COEF_OFF = STAT_OFF + NS * SEG * 8;             // general variant: RowCoef
     static constexpr int BITS_OFF = COEF_OFF + (GEN ? (int)sizeof(RowCoef) : 0);
     static constexpr int SLOT_B = (BITS_OFF + 32 + 127) / 128 * 128;
     static constexpr size_t bytes = 128 + (size_t)RING * SLOT_B + RING * sizeof(uint64_t);
     static constexpr uint32_t row_tx =
-        (uint32_t)(NSET * SEG * 8 + NS * SEG * 8 + (GEN ? (int)sizeof(RowCoef) : 0) + 32);
+        (uint32_t)((F32 ? 4 * VSEG * 4 + 2 * SEG * 8 : NSET * SEG * 8) + NS * SEG * 8 +
+                   (GEN ? (int)sizeof(RowCoef) : 0) + 32);
 };
 
 // resident CTAs per SM the register budget is cut for: 16 one-warp CTAs
@@ -142,28 +153,51 @@ struct Layout {
 // where the time-mean sums need more registers, 11 for the general variant,
 // and never more than the shared memory holds (228 KB per SM, 1 KB of it
 // reserved per CTA)
-template <bool GEN, int MODE>
+template <bool GEN, int MODE, bool F32 = false>
 constexpr int min_ctas()
 {
-    constexpr int by_smem = (int)(233472 / (Layout<GEN>::bytes + 1024));
+    constexpr int by_smem = (int)(233472 / (Layout<GEN, F32>::bytes + 1024));
     constexpr int want = GEN ? 11 : (MODE % 3 ? 12 : 16);
     return by_smem < want ? by_smem : want;
 }
 static_assert(NSET * SEG * 8 <= 1792, "state segment overlaps the static segment");
 static_assert(Layout<false>::COEF_OFF % 16 == 0 && Layout<true>::BITS_OFF % 16 == 0, "bulk copy alignment");
+static_assert(Layout<false, true>::BITS_OFF % 16 == 0 && (Layout<false, true>::VSEG * 4) % 16 == 0,
+              "FP32 segment alignment");
 
 // One lane elected by elect.sync announces the bytes of a row to the slot's
 // mbarrier and starts its copies: the state and static segments (3-D tiled
 // TMA, x = g0 even, so 16-byte aligned), the mask-bit window and, in the
 // general variant, the row's coefficients (1-D bulk copies).  No branch.
-template <bool GEN>
+template <bool GEN, bool F32 = false>
 __device__ __forceinline__ void issue_row(unsigned char *slot, uint64_t *bar, const CUtensorMap *src,
-                                          const CUtensorMap *stat, const void *coef, const void *bits, int x,
-                                          int row)
+                                          const CUtensorMap *stat, const CUtensorMap *ssh, const void *coef,
+                                          const void *bits, int x, int row)
 {
-    using L = Layout<GEN>;
+    using L = Layout<GEN, F32>;
     const int z = 0;
-    if constexpr (GEN) {
+    if constexpr (F32) {
+        // velocities from x rounded down to a multiple of 4 (16 bytes of
+        // FP32); SSH and SSHP are fields 4 and 5 of the FP64 set
+        const int x4 = x & ~3, zs = S_SSH;
+        asm volatile(
+            "{\n\t.reg .pred P;\n\t"
+            "elect.sync _|P, 0xffffffff;\n\t"
+            "@P mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n\t"
+            "@P cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+            " [%2], [%3, {%4, %5, %6}], [%0];\n\t"
+            "@P cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+            " [%7], [%8, {%9, %5, %10}], [%0];\n\t"
+            "@P cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+            " [%11], [%12, {%9, %5, %6}], [%0];\n\t"
+            "@P cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%13], [%14], 32, [%0];\n\t"
+            "}" ::"r"(smem_addr(bar)),
+            "r"(L::row_tx), "r"(smem_addr(slot)), "l"(reinterpret_cast<uint64_t>(src)), "r"(x4), "r"(row), "r"(z),
+            "r"(smem_addr(slot + L::SSH_OFF)), "l"(reinterpret_cast<uint64_t>(ssh)), "r"(x), "r"(zs),
+            "r"(smem_addr(slot + L::STAT_OFF)), "l"(reinterpret_cast<uint64_t>(stat)),
+            "r"(smem_addr(slot + L::BITS_OFF)), "l"(bits)
+            : "memory");
+    } else if constexpr (GEN) {
         asm volatile(
             "{\n\t.reg .pred P;\n\t"
             "elect.sync _|P, 0xffffffff;\n\t"
@@ -182,6 +216,7 @@ __device__ __forceinline__ void issue_row(unsigned char *slot, uint64_t *bar, co
             : "memory");
     } else {
         (void)coef;
+        (void)ssh;
         asm volatile(
             "{\n\t.reg .pred P;\n\t"
             "elect.sync _|P, 0xffffffff;\n\t"
@@ -217,6 +252,30 @@ __device__ __forceinline__ double rcp_nr(double x)
     r = fma(r, e, r);
     e = fma(-x, r, 1.0);
     return fma(r, e, r);
+}
+
+// state field F of the slot at byte offset o, at the lane's column + dk:
+// FP64, or FP32 velocities widened to FP64
+template <bool GEN, bool F32, int F>
+__device__ __forceinline__ double ld_state(const unsigned char *lane, const unsigned char *lane32, int o, int dk)
+{
+    using L = Layout<GEN, F32>;
+    if constexpr (F32 && F < S_SSH)
+        return (double)*reinterpret_cast<const float *>(lane32 + o + (F * L::VSEG + dk) * 4);
+    else if constexpr (F32)
+        return *reinterpret_cast<const double *>(lane + o + L::SSH_OFF + ((F - S_SSH) * SEG + dk) * 8);
+    else
+        return *reinterpret_cast<const double *>(lane + o + (F * SEG + dk) * 8);
+}
+
+// store a new state value; FP32 velocities are rounded to nearest
+template <bool F32, int F>
+__device__ __forceinline__ void st_state(float *const *vdst, double *const *dst, long long idx, double v)
+{
+    if constexpr (F32 && F < S_SSH)
+        vdst[F][idx] = (float)v;
+    else
+        dst[F][idx] = v;
 }
 
 #define SHFL_UP(x) __shfl_up_sync(0xffffffffu, (x), 1)
@@ -256,11 +315,11 @@ using On = std::integral_constant<bool, B>;
 // gave up (FLAG_TIMEOUT is set).
 // MODE = acc + 3*write: acc 0 none, 1 first substep (write), 2 accumulate;
 // write 1 stores the new state
-template <bool GEN, int MODE>
+template <bool GEN, int MODE, bool F32 = false>
 __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap *tm_src, double *const *dst,
                                              const double rs, const int4 item, unsigned char *ring, uint64_t *mbar)
 {
-    using L = Layout<GEN>;
+    using L = Layout<GEN, F32>;
     constexpr int ACC = MODE % 3;
     constexpr bool WRITE = MODE / 3 != 0;
 
@@ -272,14 +331,15 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
     const int wbase = (g0 >> 7) << 2;                       // first mask word of the window
     const int bsh = k - wbase * 32;                         // bit of k in the window
     const unsigned char *lane = ring + (l + 2) * 8;         // this lane's column in a segment
+    const unsigned char *lane32 = ring + (l + 2 + (g0 & 3)) * 4;   // ... in an FP32 segment (from g0 & ~3)
 
     // field f of the state / static segment of the slot at byte offset o
-#define AS(o, f, dk) (*reinterpret_cast<const double *>(lane + (o) + ((f) * SEG + (dk)) * 8))
+#define AS(o, f, dk) ld_state<GEN, F32, (f)>(lane, lane32, (o), (dk))
 #define AT(o, f, dk) (*reinterpret_cast<const double *>(lane + (o) + L::STAT_OFF + ((f) * SEG + (dk)) * 8))
 #define CF(o, x) (reinterpret_cast<const RowCoef *>(ring + (o) + L::COEF_OFF)->x)
 
     auto issue = [&](int row, int slot) {
-        issue_row<GEN>(ring + slot * L::SLOT_B, &mbar[slot], tm_src, &p.tm_stat, p.rows + row,
+        issue_row<GEN, F32>(ring + slot * L::SLOT_B, &mbar[slot], tm_src, &p.tm_stat, &p.tm_ssh, p.rows + row,
                        p.bits + (size_t)row * p.bm_words + wbase, g0, row);
     };
     auto mask2 = [&](int o) -> uint32_t {   // bits: lu(k), lu(k+1)
@@ -385,8 +445,8 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
 
         // forcing of the rows that stage 3 updates, loaded early
         double rxf = 0.0, ryf = 0.0;
-        if constexpr (D3U) rxf = p.rx[gi - p.pitch];
-        if constexpr (D3V) ryf = p.ry[gi - 2 * p.pitch];
+        if constexpr (D3U) rxf = F32 ? (double)p.rx32[gi - p.pitch] : p.rx[gi - p.pitch];
+        if constexpr (D3V) ryf = F32 ? (double)p.ry32[gi - 2 * p.pitch] : p.ry[gi - 2 * p.pitch];
 
         // ---------------- stage 2: row rho = j-1 -------------------------
         double FX, FY, GY, ST, SS, QU, QV, sn, vs, u_r, up_r, v_m, vp_m;
@@ -487,8 +547,8 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
                     p.acc[2][idx] = b;
                 }
                 if (WRITE && wu) {
-                    dst[S_UP][idx] = u_r + gam * (un - 2.0 * u_r + up_r);
-                    dst[S_U][idx] = un;
+                    st_state<F32, S_UP>(p.vdst, dst, idx, u_r + gam * (un - 2.0 * u_r + up_r));
+                    st_state<F32, S_U>(p.vdst, dst, idx, un);
                 }
                 if (WRITE && wt) {   // vel_ssh.f90:593-596
                     dst[S_SSHP][idx] = e0 + gam * (sn - 2.0 * e0 + sp0);
@@ -531,8 +591,8 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
                     p.acc[3][idx] = b;
                 }
                 if (WRITE && wv) {
-                    dst[S_VP][idx] = v0 + gam * (vn - 2.0 * v0 + vp0);
-                    dst[S_V][idx] = vn;
+                    st_state<F32, S_VP>(p.vdst, dst, idx, v0 + gam * (vn - 2.0 * v0 + vp0));
+                    st_state<F32, S_V>(p.vdst, dst, idx, vn);
                 }
             }
         }
@@ -609,14 +669,14 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
 #undef CF
 }
 
-template <bool GEN, int MODE>
-__global__ void __launch_bounds__(NL, min_ctas<GEN, MODE>()) k_substep(const __grid_constant__ Params p)
+template <bool GEN, int MODE, bool F32 = false>
+__global__ void __launch_bounds__(NL, min_ctas<GEN, MODE, F32>()) k_substep(const __grid_constant__ Params p)
 {
-    using L = Layout<GEN>;
+    using L = Layout<GEN, F32>;
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char *ring = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
     uint64_t *mbar = reinterpret_cast<uint64_t *>(ring + RING * L::SLOT_B);
-    (void)substep_item<GEN, MODE>(p, &p.tm_src, p.dst, p.rhs_scale, p.items[blockIdx.x], ring, mbar);
+    (void)substep_item<GEN, MODE, F32>(p, &p.tm_src, p.dst, p.rhs_scale, p.items[blockIdx.x], ring, mbar);
 }
 
 // min/max over the ocean points of three fields, for the uniform-forcing test
@@ -647,6 +707,35 @@ __global__ void k_minmax3(Dom D, const float *lu, const double *a, const double 
                 mx[q] = (y > mx[q] || y != y) ? y : mx[q];
             }
         for (int q = 0; q < 3; q++) { out[blockIdx.x * 6 + q] = mn[q]; out[blockIdx.x * 6 + 3 + q] = mx[q]; }
+    }
+}
+
+// FP64 -> FP32 (round to nearest), n values
+__global__ void k_to_f32(const double *a, float *b, long long n)
+{
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        b[i] = (float)a[i];
+}
+
+// FP32 velocities back into an FP64 set at the points the FP32 kernel
+// writes: u, up on lcu, v, vp on lcv (interior); every other point of the
+// FP64 set keeps its value
+__global__ void k_vel_from_f32(const float *vs, double *set, const float *lu, long long pitch, long long fs, int r0,
+                               int r1, int c0, int c1)
+{
+    const int w = c1 - c0 + 1;
+    const long long tot = (long long)w * (r1 - r0 + 1);
+    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
+        const long long i = (long long)(r0 + t / w) * pitch + c0 + t % w;
+        const bool o = lu[i] > 0.5f;
+        if (o && lu[i + 1] > 0.5f) {
+            set[S_U * fs + i] = (double)vs[0 * fs + i];
+            set[S_UP * fs + i] = (double)vs[1 * fs + i];
+        }
+        if (o && lu[i + pitch] > 0.5f) {
+            set[S_V * fs + i] = (double)vs[2 * fs + i];
+            set[S_VP * fs + i] = (double)vs[3 * fs + i];
+        }
     }
 }
 
@@ -796,20 +885,24 @@ int set_smem1()
 int set_smem()
 {
     return set_smem1<false, 2>() | set_smem1<false, 3>() | set_smem1<false, 4>() | set_smem1<false, 5>() |
-           set_smem1<true, 2>() | set_smem1<true, 3>() | set_smem1<true, 4>() | set_smem1<true, 5>();
+           set_smem1<true, 2>() | set_smem1<true, 3>() | set_smem1<true, 4>() | set_smem1<true, 5>() |
+           (cudaFuncSetAttribute(k_substep<false, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)Layout<false, true>::bytes) != cudaSuccess);
 }
 
 using EncodeTiled = decltype(&cuTensorMapEncodeTiled);
 
 // {pitch, rows, nfields} doubles with field stride fstride; box {SEG, 1, box_fields}
-int encode_fields(EncodeTiled enc, CUtensorMap *map, double *base, const Dom &d, long long fstride, int nfields,
-                  int box_fields)
+int encode_fields(EncodeTiled enc, CUtensorMap *map, void *base, const Dom &d, long long fstride, int nfields,
+                  int box_fields, bool f32 = false)
 {
+    const cuuint64_t esz = f32 ? sizeof(float) : sizeof(double);
     const cuuint64_t dims[3] = {(cuuint64_t)d.pitch, (cuuint64_t)d.nya(), (cuuint64_t)nfields};
-    const cuuint64_t strides[2] = {(cuuint64_t)d.pitch * sizeof(double), (cuuint64_t)fstride * sizeof(double)};
-    const cuuint32_t box[3] = {(cuuint32_t)SEG, 1u, (cuuint32_t)box_fields};
+    const cuuint64_t strides[2] = {(cuuint64_t)d.pitch * esz, (cuuint64_t)fstride * esz};
+    const cuuint32_t box[3] = {(cuuint32_t)(f32 ? Layout<false, true>::VSEG : SEG), 1u, (cuuint32_t)box_fields};
     const cuuint32_t estr[3] = {1u, 1u, 1u};
-    return enc(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides, box, estr,
+    return enc(map, f32 ? CU_TENSOR_MAP_DATA_TYPE_FLOAT32 : CU_TENSOR_MAP_DATA_TYPE_FLOAT64, 3, base, dims, strides,
+               box, estr,
                CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_256B,
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS;
 }
@@ -894,6 +987,12 @@ void release(Plan &p)
     cudaFree(p.items[0]);
     cudaFree(p.items[1]);
     p.items[0] = p.items[1] = nullptr;
+    for (auto &v : p.vset) {
+        cudaFree(v);
+        v = nullptr;
+    }
+    cudaFree(p.stat32);
+    p.stat32 = nullptr;
     p.rows = nullptr;
     p.cor = nullptr;
     p.bits = nullptr;
@@ -902,6 +1001,42 @@ void release(Plan &p)
     p.stat = nullptr;
     p.d_uniform = nullptr;
     p.d_flags = nullptr;
+}
+
+
+EncodeTiled encoder()
+{
+    void *fn = nullptr;
+    cudaDriverEntryPointQueryResult qr;
+    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &qr) != cudaSuccess ||
+        qr != cudaDriverEntryPointSuccess)
+        return nullptr;
+    return reinterpret_cast<EncodeTiled>(fn);
+}
+
+// FP32 velocity sets (u up v vp per state set), FP32 forcing and their
+// tensor maps, made on the first FP32-velocity run
+int ensure_f32(Plan &p, const Dom &d, cudaStream_t s)
+{
+    if (p.vset[0]) return 0;
+    EncodeTiled enc = encoder();
+    if (!enc) return 1;
+    const size_t fb = (size_t)p.fstride * sizeof(float);
+    for (int b = 0; b < 3; b++) {
+        if (cudaMalloc(&p.vset[b], 4 * fb) != cudaSuccess) return 1;
+        if (cudaMemsetAsync(p.vset[b], 0, 4 * fb, s) != cudaSuccess) return 1;
+        if (encode_fields(enc, &p.tm_vel[b], p.vset[b], d, p.fstride, 4, 4, true)) return 1;
+        if (encode_fields(enc, &p.tm_ssh[b], p.set[b], d, p.fstride, NSET, 2)) return 1;
+    }
+    if (cudaMalloc(&p.stat32, 2 * fb) != cudaSuccess) return 1;
+    return 0;
+}
+
+int set_index(const Plan &p, const double *base)
+{
+    for (int b = 0; b < 3; b++)
+        if (p.set[b] == base) return b;
+    return -1;
 }
 
 }  // namespace
@@ -1074,12 +1209,8 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
     p.set[0] = state[0];
     p.set[1] = p.buf[0][0];
     p.set[2] = p.buf[1][0];
-    void *fn = nullptr;
-    cudaDriverEntryPointQueryResult qr;
-    if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &fn, cudaEnableDefault, &qr) != cudaSuccess ||
-        qr != cudaDriverEntryPointSuccess || !fn)
-        return 1;
-    EncodeTiled enc = reinterpret_cast<EncodeTiled>(fn);
+    EncodeTiled enc = encoder();
+    if (!enc) return 1;
     for (int b = 0; b < 3; b++)
         if (encode_fields(enc, &p.tm_set[b], p.set[b], d, p.fstride, NSET, NSET)) return 1;
     if (encode_fields(enc, &p.tm_stat[0], p.stat, d, p.fstride, NSTAT, Layout<false>::NS)) return 1;
@@ -1175,6 +1306,42 @@ int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt, co
     q.gam = c.ts / 2.0;   // nstep = 1
     q.c4 = 0.25;
     for (int k = 0; k < 4; k++) q.acc[k] = nullptr;
+    if (p.f32) {
+        // FP32 velocity storage: u, up, v, vp of the state and ping-pong
+        // sets in FP32 for the run, SSH in the FP64 sets
+        if (gen) return 2;
+        if (ensure_f32(p, d, s)) return 1;
+        const int blocks = 4 * p.nsm;
+        const int a = set_index(p, state[0]), b = set_index(p, p.buf[0][0]);
+        if (a < 0 || b < 0) return 1;
+        k_to_f32<<<blocks, 256, 0, s>>>(p.set[a], p.vset[a], 4 * p.fstride);
+        k_to_f32<<<blocks, 256, 0, s>>>(p.set[b], p.vset[b], 4 * p.fstride);
+        k_to_f32<<<blocks, 256, 0, s>>>(p.stat + T_RX * p.fstride, p.stat32, 2 * p.fstride);
+        q.rx32 = p.stat32;
+        q.ry32 = p.stat32 + p.fstride;
+        for (int step = 0; step < nsub; step++) {
+            const int si = (step & 1) ? b : a, di = (step & 1) ? a : b;
+            q.tm_src = p.tm_vel[si];
+            q.tm_ssh = p.tm_ssh[si];
+            for (int k = 0; k < NSET; k++) q.dst[k] = p.set[di] + k * p.fstride;
+            for (int k = 0; k < 4; k++) q.vdst[k] = p.vset[di] + k * p.fstride;
+            q.rhs_scale = rhs_scale ? rhs_scale[step] : 1.0;
+            p.last_variant = 2;
+            k_substep<false, 3, true><<<dim3(p.nitems[0]), NL, Layout<false, true>::bytes, s>>>(q);
+            if (cudaGetLastError() != cudaSuccess) return 1;
+        }
+        if (nsub & 1)
+            for (int k = 0; k < 6; k++) std::swap(state[k], p.buf[0][k]);
+        const int fi = set_index(p, state[0]);
+        k_vel_from_f32<<<blocks, 256, 0, s>>>(p.vset[fi], p.set[fi], p.lu, d.pitch, p.fstride,
+                                              d.ny_start - d.bnd_y1, d.ny_end - d.bnd_y1,
+                                              d.nx_start - d.bnd_x1 + d.xoff, d.nx_end - d.bnd_x1 + d.xoff);
+        if (cudaGetLastError() != cudaSuccess) return 1;
+        unsigned flags = 0;
+        if (read_flags(p, s, &flags)) return 1;
+        p.last_flags = flags;
+        return 0;
+    }
     for (int step = 0; step < nsub; step++) {
         if (set_io(p, q, (step & 1) ? p.buf[0] : state, (step & 1) ? state : p.buf[0])) return 1;
         q.rhs_scale = rhs_scale ? rhs_scale[step] : 1.0;

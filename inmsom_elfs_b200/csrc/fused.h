@@ -90,6 +90,13 @@ struct Plan {
     CUtensorMap tm_set[3];          // box {36, 1, 6} over each state set
     CUtensorMap tm_stat[2];         // box {36, 1, 1 | 4} over the static block
     int occ[2] = {0, 0};            // resident CTAs per SM, per variant
+    // FP32 velocity storage for run_substeps (uniform variant): per state
+    // set, u up v vp in FP32 (same field stride), SSH stays in the FP64 set
+    bool f32 = false;
+    float *vset[3] = {};
+    float *stat32 = nullptr;        // RHSx, RHSy in FP32
+    CUtensorMap tm_vel[3];          // box {40, 1, 4} FP32 over each velocity set
+    CUtensorMap tm_ssh[3];          // box {36, 1, 2} over the SSH fields of each state set
     double *d_uniform = nullptr;    // per-block min/max of mu, rdis, wflux
     unsigned *d_flags = nullptr;    // [0] status bits (guard / timeout)
     const float *lu = nullptr;      // borrowed
@@ -97,7 +104,7 @@ struct Plan {
     bool vort_zero = false;
     bool buffers_synced = false;    // buf[][] hold the state's land/halo values
     unsigned last_flags = 0;        // status bits of the last run
-    int last_variant = -1;          // 0 uniform, 1 general (last launch)
+    int last_variant = -1;          // 0 uniform, 1 general, 2 uniform with FP32 velocities (last launch)
 };
 
 enum : unsigned { FLAG_TIMEOUT = 1u, FLAG_GUARD = 2u };
@@ -119,7 +126,9 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7],
 // barotropic_dynamics(tau, nstep) on state[6] (in/out) with acc[4] out
 int dynamics(Plan &p, const Dom &d, const Consts &c, double tau, int nstep,
              double *state[6], double *acc[4], double *forc[6], cudaStream_t s);
-// nsub advancing substeps (the first substep of barotropic_dynamics(dt,1))
+// nsub advancing substeps (the first substep of barotropic_dynamics(dt,1));
+// returns 2 if FP32 velocity storage is asked for a grid that needs the
+// general variant
 int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt,
                  const double *rhs_scale, double *state[6], double *forc[6],
                  cudaStream_t s);

@@ -1,0 +1,89 @@
+"""FP32 velocity storage (INMSOM_FP32_VELOCITY) for inmsom_run_substeps.
+
+u, up, v, vp live in FP32 on the device during a run; every operation and
+SSH stay FP64.  Tolerances against the FP64 fused run (normwise relative,
+max|a-b|/max|b|), written here:
+  * after 300 substeps of the 400 x 300 regional basin: SSH <= 1e-6,
+    u and v (both levels) <= 2e-6 (measured on a B200: 3.4e-7 and 4.4e-7);
+  * the closed-basin volume is conserved to 1e-13 relative, as in FP64:
+    the continuity fluxes are FP64 products shared by both cells of a face;
+  * land and halo points of the FP64 state are never written.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+from inmsom_elfs_b200 import basins
+
+pytestmark = pytest.mark.gpu
+
+TOL_SSH = 1e-6
+TOL_UV = 2e-6
+
+
+def _run(gpu, b, nsub, fp32, scale=None):
+    bg = b.copy()
+    with gpu.BarotropicSolver(bg, resident=True, fp32_velocity=fp32) as s:
+        s.load_state()
+        s.run_substeps(nsub, b.dt, scale)
+        s.sync_to_host()
+        vol, en = s.diag()
+    return bg, vol, en
+
+
+def _prep(gpu, b):
+    basins.finalize(b, gpu.GpuBackend(0))
+    return b
+
+
+def test_fp32_velocity_close_to_fp64(gpu):
+    b = _prep(gpu, basins.regional_basin(nx=400, ny=300, seed=41))
+    scale = basins.wind_cycle(300, b.dt, t0=0.0, period=1800.0)
+    b64, _, _ = _run(gpu, b, 300, False, scale)
+    b32, _, _ = _run(gpu, b, 300, True, scale)
+    errs = {k: rel_err(b32.state[k], b64.state[k]) for k in b64.state}
+    print("fp32 velocity normwise relative errors:", errs)
+    assert errs["ssh_e"] <= TOL_SSH and errs["sshp_e"] <= TOL_SSH, errs
+    for k in ("ubrtr_e", "ubrtrp_e", "vbrtr_e", "vbrtrp_e"):
+        assert errs[k] <= TOL_UV, (k, errs[k])
+    # the velocities came back through FP32
+    u = b32.state["ubrtr_e"]
+    assert np.array_equal(u, u.astype(np.float32).astype(np.float64))
+
+
+def test_fp32_velocity_conserves_volume(gpu):
+    b = _prep(gpu, basins.beta_plane_basin(n=200, seed=42))
+    lu = b.masks["lu"] > 0.5
+    bump = 0.3 * np.exp(-((np.arange(b.bounds.shape[0])[:, None] - 90.0) ** 2 +
+                          (np.arange(b.bounds.shape[1])[None, :] - 110.0) ** 2) / 200.0)
+    b.state["ssh_e"] = np.asfortranarray(np.where(lu, bump, 0.0))
+    b.state["sshp_e"] = b.state["ssh_e"].copy(order="F")
+    with gpu.BarotropicSolver(b, resident=True, fp32_velocity=True) as s:
+        s.load_state()
+        v0, _ = s.diag()
+        s.run_substeps(500, b.dt)
+        v1, e1 = s.diag()
+    assert abs(v1 - v0) / v0 <= 1e-13
+    assert np.isfinite(e1) and e1 > 0.0
+
+
+def test_fp32_velocity_leaves_land_untouched(gpu):
+    b = _prep(gpu, basins.regional_basin(nx=260, ny=200, seed=43))
+    rng = np.random.default_rng(44)
+    land = b.masks["lu"] < 0.5
+    for k in b.state:
+        b.state[k] = np.asfortranarray(np.where(land, rng.standard_normal(b.bounds.shape), b.state[k]))
+    b32, _, _ = _run(gpu, b, 51, True)
+    for k in b.state:
+        assert np.array_equal(b32.state[k][land], b.state[k][land]), k
+
+
+def test_fp32_velocity_needs_uniform_variant(gpu):
+    from inmsom_elfs_b200 import InmsomError
+    from inmsom_elfs_b200 import _lib
+    b = _prep(gpu, basins.spherical_basin(nx=64, ny=48))
+    with gpu.BarotropicSolver(b, resident=True, fp32_velocity=True) as s:
+        s.load_state()
+        with pytest.raises(InmsomError) as e:
+            s.run_substeps(4, b.dt)
+        assert e.value.code == _lib.EUNSUPPORTED
