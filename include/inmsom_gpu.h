@@ -264,6 +264,29 @@ int inmsom_load_state(inmsom_ctx *ctx, double *ubrtr_e, double *ubrtrp_e,
  * static string saying why the fused path is not eligible (or "eligible"). */
 int inmsom_gpu_path(inmsom_ctx *ctx, int *path, const char **reason);
 
+/* Ensemble of independent basins (no counterpart in the reference, which
+ * advances one basin per run).  The members are contexts on one device,
+ * each with its grid registered, the fused path eligible and its state
+ * resident (inmsom_load_state); they may differ in size and in every field.
+ * inmsom_ens_run advances every member by nsub substeps of its own dt[i]
+ * (the state evolution of inmsom_run_substeps), `group` substeps of all
+ * members per launch of one CUDA graph in which each member's kernels run
+ * on its own stream, so that members run concurrently and launch overhead
+ * is paid once per group.  rhs_scale (nsub values, or NULL for 1) scales
+ * every member's RHS at each substep.  group must be even (it keeps each
+ * member's state in its set, so the graph can be replayed).  *ms receives
+ * the device time of the run. */
+typedef struct inmsom_ens inmsom_ens;
+int inmsom_ens_create(inmsom_ens **ens, inmsom_ctx *const *members, int nmembers, int group);
+int inmsom_ens_run(inmsom_ens *ens, int nsub, const double *dt, const double *rhs_scale, float *ms);
+/* Autotuner: for each size class of members (side length rounded to 256),
+ * times `trial_groups` graph launches with each candidate chunk height
+ * (one wave of cost-balanced chunks, or about 96, 64, 48 or 32 rows per
+ * chunk) and keeps the fastest; rows_per_item[i] receives member i's
+ * choice (0 = one wave).  The trial runs advance the members' states. */
+int inmsom_ens_tune(inmsom_ens *ens, const double *dt, int trial_groups, int *rows_per_item);
+int inmsom_ens_destroy(inmsom_ens *ens);
+
 int inmsom_gpu_finalize(inmsom_ctx *ctx);
 const char *inmsom_gpu_last_error(void);
 

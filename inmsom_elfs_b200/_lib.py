@@ -23,7 +23,8 @@ EXPORTS = (
     "inmsom_hh_init_external", "inmsom_guard", "inmsom_gpu_diag",
     "inmsom_gpu_sync_to_host", "inmsom_gpu_sync_from_host", "inmsom_run_substeps",
     "inmsom_gpu_path", "inmsom_gpu_finalize", "inmsom_gpu_last_error", "inmsom_load_state",
-    "inmsom_diag_noalloc",
+    "inmsom_diag_noalloc", "inmsom_ens_create", "inmsom_ens_run", "inmsom_ens_tune",
+    "inmsom_ens_destroy",
 )
 
 # include/inmsom_gpu.h: INMSOM_DIAG_NOALLOC_MAX_ROWS
@@ -82,6 +83,10 @@ def load() -> ctypes.CDLL:
     lib.inmsom_load_state.argtypes = [VP] + [DP] * 12
     lib.inmsom_gpu_path.argtypes = [VP, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_char_p)]
     lib.inmsom_gpu_finalize.argtypes = [VP]
+    lib.inmsom_ens_create.argtypes = [ctypes.POINTER(VP), ctypes.POINTER(VP), i, i]
+    lib.inmsom_ens_run.argtypes = [VP, i, DP, DP, ctypes.POINTER(ctypes.c_float)]
+    lib.inmsom_ens_tune.argtypes = [VP, DP, i, ctypes.POINTER(i)]
+    lib.inmsom_ens_destroy.argtypes = [VP]
     lib.inmsom_diag_noalloc.argtypes = ([ctypes.POINTER(CBounds), ctypes.POINTER(CConsts),
                                          ctypes.c_longlong] + [VP] * 16 + [VP])
     for name in EXPORTS:

@@ -4,6 +4,8 @@
 // fused.cu (streaming, one kernel per substep).
 #include "inmsom_gpu.h"
 
+#include <algorithm>
+#include <cmath>
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
@@ -755,3 +757,242 @@ int inmsom_gpu_sync_from_host(inmsom_ctx *c, unsigned what)
 }
 
 }  // extern "C"
+
+// ===========================================================================
+// Ensemble of contexts advanced by one CUDA graph per group of substeps.
+namespace {
+__global__ void k_advance(int *base, int by) { *base += by; }
+}  // namespace
+
+struct inmsom_ens {
+    std::vector<inmsom_ctx *> m;
+    int device = 0, group = 2;
+    cudaStream_t origin = nullptr;
+    cudaEvent_t fork = nullptr, ev0 = nullptr, ev1 = nullptr;
+    std::vector<cudaEvent_t> join;
+    cudaGraphExec_t exec = nullptr;
+    std::vector<double> graph_dt;          // dt per member the graph was captured with
+    std::vector<unsigned> graph_gen;       // plan generation per member at capture
+    double *d_rs = nullptr;                // RHS scale per substep of the run
+    size_t rs_cap = 0;
+    int *d_base = nullptr;                 // first substep of the next group
+};
+
+namespace {
+
+void ens_drop_graph(inmsom_ens *e)
+{
+    if (e->exec) cudaGraphExecDestroy(e->exec);
+    e->exec = nullptr;
+    e->graph_dt.clear();
+    e->graph_gen.clear();
+}
+
+int ens_capture(inmsom_ens *e, const double *dt)
+{
+    ens_drop_graph(e);
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeThreadLocal));
+    int rc = INMSOM_OK;
+    cudaError_t ce = cudaEventRecord(e->fork, e->origin);
+    for (size_t i = 0; i < e->m.size() && ce == cudaSuccess && rc == INMSOM_OK; i++) {
+        inmsom_ctx *c = e->m[i];
+        ce = cudaStreamWaitEvent(c->stream, e->fork, 0);
+        if (ce == cudaSuccess &&
+            fused::launch_steps(c->plan, c->dom, c->c, dt[i], e->group, e->d_rs, e->d_base, c->state, c->stream))
+            rc = set_err(INMSOM_ECUDA, "ensemble member %zu: launch failed during graph capture", i);
+        if (ce == cudaSuccess && rc == INMSOM_OK) ce = cudaEventRecord(e->join[i], c->stream);
+        if (ce == cudaSuccess && rc == INMSOM_OK) ce = cudaStreamWaitEvent(e->origin, e->join[i], 0);
+    }
+    if (ce == cudaSuccess && rc == INMSOM_OK) {
+        k_advance<<<1, 1, 0, e->origin>>>(e->d_base, e->group);
+        ce = cudaGetLastError();
+    }
+    cudaError_t ee = cudaStreamEndCapture(e->origin, &g);
+    if (rc != INMSOM_OK) {
+        if (g) cudaGraphDestroy(g);
+        return rc;
+    }
+    if (ce != cudaSuccess || ee != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return set_err(INMSOM_ECUDA, "ensemble graph capture failed: %s",
+                       cudaGetErrorString(ce != cudaSuccess ? ce : ee));
+    }
+    ce = cudaGraphInstantiate(&e->exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ce != cudaSuccess) return set_err(INMSOM_ECUDA, "ensemble graph instantiate: %s", cudaGetErrorString(ce));
+    e->graph_dt.assign(dt, dt + e->m.size());
+    for (auto *c : e->m) e->graph_gen.push_back(c->plan.generation);
+    return INMSOM_OK;
+}
+
+bool ens_graph_current(const inmsom_ens *e, const double *dt)
+{
+    if (!e->exec) return false;
+    for (size_t i = 0; i < e->m.size(); i++)
+        if (e->graph_dt[i] != dt[i] || e->graph_gen[i] != e->m[i]->plan.generation) return false;
+    return true;
+}
+
+}  // namespace
+
+int inmsom_ens_create(inmsom_ens **out, inmsom_ctx *const *members, int n, int group)
+{
+    if (!out || !members || n < 1) return set_err(INMSOM_EARG, "inmsom_ens_create: no members");
+    *out = nullptr;
+    if (group < 2 || group % 2) return set_err(INMSOM_EARG, "group = %d must be even and >= 2", group);
+    for (int i = 0; i < n; i++) {
+        inmsom_ctx *c = members[i];
+        if (!c || !c->grid_ok) return set_err(INMSOM_EARG, "member %d: grid not registered", i);
+        if (!c->fused_ok) return set_err(INMSOM_EUNSUPPORTED, "member %d: fused path not eligible (%s)", i, c->fused_reason);
+        if (c->flags & INMSOM_FP32_VELOCITY)
+            return set_err(INMSOM_EUNSUPPORTED, "member %d: the ensemble runs FP64 state only", i);
+        if (c->device != members[0]->device) return set_err(INMSOM_EARG, "member %d on another device", i);
+    }
+    CK(cudaSetDevice(members[0]->device));
+    inmsom_ens *e = new inmsom_ens();
+    e->m.assign(members, members + n);
+    e->device = members[0]->device;
+    e->group = group;
+    cudaError_t ce = cudaStreamCreateWithFlags(&e->origin, cudaStreamNonBlocking);
+    if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&e->ev0);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&e->ev1);
+    e->join.assign(n, nullptr);
+    for (int i = 0; i < n && ce == cudaSuccess; i++) ce = cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming);
+    if (ce == cudaSuccess) ce = cudaMalloc(&e->d_base, sizeof(int));
+    if (ce != cudaSuccess) {
+        inmsom_ens_destroy(e);
+        return set_err(INMSOM_ECUDA, "inmsom_ens_create: %s", cudaGetErrorString(ce));
+    }
+    *out = e;
+    return INMSOM_OK;
+}
+
+int inmsom_ens_run(inmsom_ens *e, int nsub, const double *dt, const double *rhs_scale, float *ms)
+{
+    if (!e || !dt) return set_err(INMSOM_EARG, "NULL argument");
+    if (nsub < 0) return set_err(INMSOM_EARG, "nsub < 0");
+    CK(cudaSetDevice(e->device));
+    const size_t n = e->m.size();
+    for (size_t i = 0; i < n; i++) {
+        inmsom_ctx *c = e->m[i];
+        if (!(dt[i] > 0.0)) return set_err(INMSOM_EARG, "member %zu: dt must be > 0", i);
+        if (!c->state_on_device) return set_err(INMSOM_EARG, "member %zu: no resident state", i);
+        if (fused::prepare_steps(c->plan, c->dom, c->c, c->state, c->forc, c->stream))
+            return set_err(INMSOM_ECUDA, "member %zu: prepare failed: %s", i, cudaGetErrorString(cudaGetLastError()));
+        // the graph orders after the origin stream only: finish the copies
+        // prepare_steps left on the member's stream
+        CK(cudaStreamSynchronize(c->stream));
+    }
+    // RHS scale of every substep on the device, read by the kernels at the
+    // device-side substep counter
+    const size_t need = (size_t)std::max(nsub, 1);
+    if (need > e->rs_cap) {
+        ens_drop_graph(e);   // the graph holds the old buffer
+        cudaFree(e->d_rs);
+        e->d_rs = nullptr;
+        e->rs_cap = 0;
+        CK(cudaMalloc(&e->d_rs, need * sizeof(double)));
+        e->rs_cap = need;
+    }
+    std::vector<double> rs(need, 1.0);
+    if (rhs_scale)
+        for (int k = 0; k < nsub; k++) rs[k] = rhs_scale[k];
+    CK(cudaMemcpyAsync(e->d_rs, rs.data(), need * sizeof(double), cudaMemcpyHostToDevice, e->origin));
+    CK(cudaMemsetAsync(e->d_base, 0, sizeof(int), e->origin));
+    if (!ens_graph_current(e, dt)) CKR(ens_capture(e, dt));
+    CK(cudaEventRecord(e->ev0, e->origin));
+    const int groups = nsub / e->group, rest = nsub % e->group;
+    for (int g = 0; g < groups; g++) CK(cudaGraphLaunch(e->exec, e->origin));
+    if (rest) {
+        // the remaining substeps, launched directly on the member streams
+        CK(cudaEventRecord(e->fork, e->origin));
+        for (size_t i = 0; i < n; i++) {
+            inmsom_ctx *c = e->m[i];
+            CK(cudaStreamWaitEvent(c->stream, e->fork, 0));
+            if (fused::launch_steps(c->plan, c->dom, c->c, dt[i], rest, e->d_rs, e->d_base, c->state, c->stream))
+                return set_err(INMSOM_ECUDA, "member %zu: launch failed", i);
+            CK(cudaEventRecord(e->join[i], c->stream));
+            CK(cudaStreamWaitEvent(e->origin, e->join[i], 0));
+        }
+    }
+    CK(cudaEventRecord(e->ev1, e->origin));
+    CK(cudaStreamSynchronize(e->origin));
+    CK(cudaGetLastError());
+    for (size_t i = 0; i < n; i++) {
+        inmsom_ctx *c = e->m[i];
+        if (fused::finish_steps(c->plan, c->stream))
+            return set_err(INMSOM_ECUDA, "member %zu: %s", i, cudaGetErrorString(cudaGetLastError()));
+        c->depths_current = false;
+        if (c->plan.last_flags & fused::FLAG_TIMEOUT)
+            return set_err(INMSOM_ETIMEOUT, "member %zu: a bounded TMA wait timed out", i);
+    }
+    if (ms) CK(cudaEventElapsedTime(ms, e->ev0, e->ev1));
+    return INMSOM_OK;
+}
+
+int inmsom_ens_tune(inmsom_ens *e, const double *dt, int trial_groups, int *rows_out)
+{
+    if (!e || !dt) return set_err(INMSOM_EARG, "NULL argument");
+    if (trial_groups < 1) return set_err(INMSOM_EARG, "trial_groups < 1");
+    CK(cudaSetDevice(e->device));
+    const int cand[] = {0, 96, 64, 48, 32};
+    const size_t n = e->m.size();
+    // size classes: side length rounded to 256
+    std::vector<int> cls(n);
+    int ncls = 0;
+    for (size_t i = 0; i < n; i++) {
+        const Dom &d = e->m[i]->dom;
+        const double side = std::sqrt((double)(d.nx_end - d.nx_start + 1) * (d.ny_end - d.ny_start + 1));
+        cls[i] = (int)std::lround(side / 256.0);
+        ncls = std::max(ncls, cls[i] + 1);
+    }
+    std::vector<int> chosen(n, 0);
+    for (int k = 0; k < ncls; k++) {
+        bool any = false;
+        for (size_t i = 0; i < n; i++) any |= cls[i] == k;
+        if (!any) continue;
+        float best = INFINITY;
+        int best_c = 0;
+        for (int cnd : cand) {
+            for (size_t i = 0; i < n; i++)
+                if (cls[i] == k && fused::repartition(e->m[i]->plan, e->m[i]->dom, cnd, e->m[i]->stream))
+                    return set_err(INMSOM_ECUDA, "member %zu: repartition failed", i);
+            float ms = 0.0f;
+            CKR(inmsom_ens_run(e, e->group * trial_groups, dt, nullptr, &ms));   // warm-up, captures
+            CKR(inmsom_ens_run(e, e->group * trial_groups, dt, nullptr, &ms));
+            if (ms < best) {
+                best = ms;
+                best_c = cnd;
+            }
+        }
+        for (size_t i = 0; i < n; i++)
+            if (cls[i] == k) {
+                if (fused::repartition(e->m[i]->plan, e->m[i]->dom, best_c, e->m[i]->stream))
+                    return set_err(INMSOM_ECUDA, "member %zu: repartition failed", i);
+                chosen[i] = best_c;
+            }
+    }
+    if (rows_out)
+        for (size_t i = 0; i < n; i++) rows_out[i] = chosen[i];
+    return INMSOM_OK;
+}
+
+int inmsom_ens_destroy(inmsom_ens *e)
+{
+    if (!e) return INMSOM_OK;
+    cudaSetDevice(e->device);
+    if (e->origin) cudaStreamSynchronize(e->origin);
+    ens_drop_graph(e);
+    for (auto ev : e->join)
+        if (ev) cudaEventDestroy(ev);
+    if (e->fork) cudaEventDestroy(e->fork);
+    if (e->ev0) cudaEventDestroy(e->ev0);
+    if (e->ev1) cudaEventDestroy(e->ev1);
+    if (e->origin) cudaStreamDestroy(e->origin);
+    cudaFree(e->d_rs);
+    cudaFree(e->d_base);
+    delete e;
+    return INMSOM_OK;
+}

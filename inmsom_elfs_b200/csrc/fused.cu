@@ -77,6 +77,10 @@ struct alignas(64) Params {
     double d, inv_d, d4, gd, d2, tt;   // UNI: d, 1/d, d/4, g*d, d*d, two_ti/d^2
     int vort_zero;
     unsigned *flags;
+    // RHS scale from device memory (replayable launches): rs_dev[*rs_base + rs_k]
+    const double *rs_dev;
+    const int *rs_base;
+    int rs_k;
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
@@ -676,7 +680,8 @@ __global__ void __launch_bounds__(NL, min_ctas<GEN, MODE, F32>()) k_substep(cons
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char *ring = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
     uint64_t *mbar = reinterpret_cast<uint64_t *>(ring + RING * L::SLOT_B);
-    (void)substep_item<GEN, MODE, F32>(p, &p.tm_src, p.dst, p.rhs_scale, p.items[blockIdx.x], ring, mbar);
+    const double rs = p.rs_dev ? p.rs_dev[*p.rs_base + p.rs_k] : p.rhs_scale;
+    (void)substep_item<GEN, MODE, F32>(p, &p.tm_src, p.dst, rs, p.items[blockIdx.x], ring, mbar);
 }
 
 // min/max over the ocean points of three fields, for the uniform-forcing test
@@ -907,51 +912,73 @@ int encode_fields(EncodeTiled enc, CUtensorMap *map, void *base, const Dom &d, l
                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) != CUDA_SUCCESS;
 }
 
-// Work items of one variant: each strip's interior rows cut into chunks of
-// about equal cost, as many in all as one wave of resident CTAs holds, so
-// that the wave finishes together.  A row whose written columns are all land
-// skips the momentum stages and costs about LAND_COST of an ocean row; no
-// chunk is shorter than MIN_ROWS rows (each pays three warm-up iterations).
 constexpr double LAND_COST = 0.7;
 constexpr int MIN_ROWS = 16;
 
-std::vector<int4> partition(const Plan &p, const Dom &d, const float *lu, int slots)
+// Ocean flags of the written columns of every strip and interior row
+// (strip-major), from the host T mask.
+std::vector<uint8_t> ocean_rows(const Plan &p, const Dom &d, const float *lu)
 {
     const int nxa = d.nxa();
     const int rf = d.ny_start - d.bnd_y1, rl = d.ny_end - d.bnd_y1;   // interior device rows
     const int cf = d.nx_start - d.bnd_x1 + d.xoff, cl = d.nx_end - d.bnd_x1 + d.xoff;
     const int ny = rl - rf + 1;
-    std::vector<std::vector<double>> cost(p.nstrips, std::vector<double>(ny));
-    std::vector<double> total(p.nstrips, 0.0);
-    double all = 0.0;
+    std::vector<uint8_t> oc((size_t)p.nstrips * ny, 0);
     for (int s = 0; s < p.nstrips; s++) {
         const int g0 = s * p.outw;
         const int c0 = std::max(g0 + 3, cf), c1 = std::min(g0 + 2 + p.outw, cl);   // written columns
         for (int r = rf; r <= rl; r++) {
             bool ocean = false;
             for (int col = c0; col <= c1 && !ocean; col++) ocean = lu[(size_t)r * nxa + (col - d.xoff)] > 0.5f;
-            cost[s][r - rf] = ocean ? 1.0 : LAND_COST;
-            total[s] += cost[s][r - rf];
+            oc[(size_t)s * ny + (r - rf)] = ocean;
+        }
+    }
+    return oc;
+}
+
+// Work items of one variant: each strip's interior rows cut into chunks of
+// about equal cost.  rows_per_item = 0: as many items in all as one wave of
+// resident CTAs holds (`slots`), so that the wave finishes together; else
+// about that many rows per item (several waves).  A row whose written
+// columns are all land skips the momentum stages and costs about LAND_COST
+// of an ocean row; no chunk is shorter than MIN_ROWS rows (each pays three
+// warm-up iterations).
+std::vector<int4> partition(const Plan &p, const Dom &d, int slots, int rows_per_item)
+{
+    const int rf = d.ny_start - d.bnd_y1, rl = d.ny_end - d.bnd_y1;
+    const int ny = rl - rf + 1;
+    std::vector<std::vector<double>> cost(p.nstrips, std::vector<double>(ny));
+    std::vector<double> total(p.nstrips, 0.0);
+    double all = 0.0;
+    for (int s = 0; s < p.nstrips; s++) {
+        for (int r = 0; r < ny; r++) {
+            cost[s][r] = p.ocean[(size_t)s * ny + r] ? 1.0 : LAND_COST;
+            total[s] += cost[s][r];
         }
         all += total[s];
     }
-    // chunks per strip in proportion to its cost (largest remainder)
     const int maxc = std::max(1, ny / MIN_ROWS);
-    const int want = std::min(std::max(slots, p.nstrips), p.nstrips * maxc);
     std::vector<int> n(p.nstrips);
-    std::vector<std::pair<double, int>> frac;
-    int used = 0;
-    for (int s = 0; s < p.nstrips; s++) {
-        const double exact = all > 0.0 ? want * total[s] / all : 1.0;
-        n[s] = std::min(maxc, std::max(1, (int)exact));
-        used += n[s];
-        frac.push_back({exact - (int)exact, s});
+    if (rows_per_item > 0) {
+        for (int s = 0; s < p.nstrips; s++)
+            n[s] = std::min(maxc, std::max(1, (ny + rows_per_item / 2) / rows_per_item));
+    } else {
+        // chunks per strip in proportion to its cost (largest remainder)
+        const int want = std::min(std::max(slots, p.nstrips), p.nstrips * maxc);
+        std::vector<std::pair<double, int>> frac;
+        int used = 0;
+        for (int s = 0; s < p.nstrips; s++) {
+            const double exact = all > 0.0 ? want * total[s] / all : 1.0;
+            n[s] = std::min(maxc, std::max(1, (int)exact));
+            used += n[s];
+            frac.push_back({exact - (int)exact, s});
+        }
+        std::sort(frac.begin(), frac.end(), [](const std::pair<double, int> &a, const std::pair<double, int> &b) {
+            return a.first > b.first;
+        });
+        for (size_t t = 0; used < want && t < frac.size(); t++)
+            if (n[frac[t].second] < maxc) n[frac[t].second]++, used++;
     }
-    std::sort(frac.begin(), frac.end(), [](const std::pair<double, int> &a, const std::pair<double, int> &b) {
-        return a.first > b.first;
-    });
-    for (size_t t = 0; used < want && t < frac.size(); t++)
-        if (n[frac[t].second] < maxc) n[frac[t].second]++, used++;
     // cut each strip at equal shares of its cumulative cost
     std::vector<int4> items;
     for (int s = 0; s < p.nstrips; s++) {
@@ -961,8 +988,7 @@ std::vector<int4> partition(const Plan &p, const Dom &d, const float *lu, int sl
         for (int r = rf; r <= rl; r++) {
             acc += cost[s][r - rf];
             const bool last_row = r == rl;
-            const bool cut = made < n[s] - 1 && acc >= share * (made + 1) && r - start + 1 >= 1 &&
-                             rl - r >= n[s] - 1 - made;
+            const bool cut = made < n[s] - 1 && acc >= share * (made + 1) && rl - r >= n[s] - 1 - made;
             if (cut || last_row) {
                 items.push_back(make_int4(s * p.outw, start, r + 1, 0));
                 start = r + 1;
@@ -971,6 +997,20 @@ std::vector<int4> partition(const Plan &p, const Dom &d, const float *lu, int sl
         }
     }
     return items;
+}
+
+int upload_items(Plan &p, int v, const std::vector<int4> &items, cudaStream_t s)
+{
+    p.generation++;
+    cudaFree(p.items[v]);
+    p.items[v] = nullptr;
+    p.nitems[v] = (int)items.size();
+    if (cudaMalloc(&p.items[v], items.size() * sizeof(int4)) != cudaSuccess) return 1;
+    if (cudaMemcpyAsync(p.items[v], items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, s) !=
+        cudaSuccess)
+        return 1;
+    // the item table is a host vector: finish its copy before returning
+    return cudaStreamSynchronize(s) != cudaSuccess;
 }
 
 void release(Plan &p)
@@ -1235,17 +1275,11 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
         occ[1] = 1;
     p.occ[0] = occ[0];
     p.occ[1] = occ[1];
-    const float *lu_h = masks[0];
+    p.ocean = ocean_rows(p, d, masks[0]);
     for (int v = 0; v < 2; v++) {
-        std::vector<int4> items = partition(p, d, lu_h, nsm * occ[v]);
-        p.nitems[v] = (int)items.size();
-        if (cudaMalloc(&p.items[v], items.size() * sizeof(int4)) != cudaSuccess) return 1;
-        if (cudaMemcpyAsync(p.items[v], items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, s) !=
-            cudaSuccess)
-            return 1;
+        p.rows_per_item[v] = 0;
+        if (upload_items(p, v, partition(p, d, nsm * occ[v], 0), s)) return 1;
     }
-    // the work tables are host vectors: finish their copies before returning
-    if (cudaStreamSynchronize(s) != cudaSuccess) return 1;
     return 0;
 }
 
@@ -1350,6 +1384,63 @@ int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt, co
     }
     if (nsub & 1)
         for (int k = 0; k < 6; k++) std::swap(state[k], p.buf[0][k]);
+    unsigned flags = 0;
+    if (read_flags(p, s, &flags)) return 1;
+    p.last_flags = flags;
+    return 0;
+}
+
+int repartition(Plan &p, const Dom &d, int rows_per_item, cudaStream_t s)
+{
+    for (int v = 0; v < 2; v++) {
+        p.rows_per_item[v] = rows_per_item;
+        if (upload_items(p, v, partition(p, d, p.nsm * p.occ[v], rows_per_item), s)) return 1;
+    }
+    return 0;
+}
+
+int prepare_steps(Plan &p, const Dom &d, const Consts &c, double *state[6], double *forc[6], cudaStream_t s)
+{
+    Forcing f;
+    if (forcing_mode(p, d, c, forc, s, f)) return 1;
+    if (!p.buffers_synced && sync_buffers(p, state, s)) return 1;
+    if (cudaMemsetAsync(p.d_flags, 0, sizeof(unsigned), s) != cudaSuccess) return 1;
+    const int gen = (p.uni && f.uniform) ? 0 : 1;
+    if (stage_forcing(p, forc, gen, s)) return 1;
+    p.prep_gen = gen;
+    p.prep_mu0 = f.mu0;
+    p.prep_rd0 = f.rd0;
+    p.prep_wq0 = f.wq0;
+    p.prepared = true;
+    return 0;
+}
+
+int launch_steps(Plan &p, const Dom &d, const Consts &c, double dt, int nsteps, const double *rs_dev,
+                 const int *rs_base, double *state[6], cudaStream_t s)
+{
+    if (!p.prepared) return 1;
+    Forcing f{true, p.prep_mu0, p.prep_rd0, p.prep_wq0};
+    const int gen = p.prep_gen;
+    Params q = base_params(p, d, c, f, gen);
+    set_times(q, 2.0 * dt, p);
+    q.gam = c.ts / 2.0;   // nstep = 1
+    q.c4 = 0.25;
+    for (int k = 0; k < 4; k++) q.acc[k] = nullptr;
+    q.rs_dev = rs_dev;
+    q.rs_base = rs_base;
+    for (int step = 0; step < nsteps; step++) {
+        if (set_io(p, q, (step & 1) ? p.buf[0] : state, (step & 1) ? state : p.buf[0])) return 1;
+        q.rs_k = step;
+        launch(p, q, gen, 3, s);
+        if (cudaGetLastError() != cudaSuccess) return 1;
+    }
+    if (nsteps & 1)
+        for (int k = 0; k < 6; k++) std::swap(state[k], p.buf[0][k]);
+    return 0;
+}
+
+int finish_steps(Plan &p, cudaStream_t s)
+{
     unsigned flags = 0;
     if (read_flags(p, s, &flags)) return 1;
     p.last_flags = flags;

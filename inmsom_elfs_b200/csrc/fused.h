@@ -31,6 +31,9 @@
 
 #include <cuda.h>
 
+#include <cstdint>
+#include <vector>
+
 #include "common.cuh"
 #include "inmsom_gpu.h"
 
@@ -90,6 +93,13 @@ struct Plan {
     CUtensorMap tm_set[3];          // box {36, 1, 6} over each state set
     CUtensorMap tm_stat[2];         // box {36, 1, 1 | 4} over the static block
     int occ[2] = {0, 0};            // resident CTAs per SM, per variant
+    std::vector<uint8_t> ocean;     // per strip and interior row: any written column is ocean
+    int rows_per_item[2] = {0, 0};  // 0: one wave of items by cost; else rows per item
+    unsigned generation = 0;        // bumped whenever buffers or work items change
+    // prepare_steps: classification of the forcing for launch_steps
+    bool prepared = false;
+    int prep_gen = 0;
+    double prep_mu0 = 0.0, prep_rd0 = 0.0, prep_wq0 = 0.0;
     // FP32 velocity storage for run_substeps (uniform variant): per state
     // set, u up v vp in FP32 (same field stride), SSH stays in the FP64 set
     bool f32 = false;
@@ -132,6 +142,19 @@ int dynamics(Plan &p, const Dom &d, const Consts &c, double tau, int nstep,
 int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt,
                  const double *rhs_scale, double *state[6], double *forc[6],
                  cudaStream_t s);
+// Capture-friendly form of run_substeps for CUDA graphs (FP64): prepare_steps
+// classifies the forcing and stages it (it synchronises the stream);
+// launch_steps then only enqueues nsteps kernels, the RHS scale of launch k
+// being rs_dev[*rs_base + k] read on the device (an even nsteps leaves the
+// state in the same set, so the launches can be replayed); finish_steps
+// reads the status bits.
+int prepare_steps(Plan &p, const Dom &d, const Consts &c, double *state[6], double *forc[6],
+                  cudaStream_t s);
+int launch_steps(Plan &p, const Dom &d, const Consts &c, double dt, int nsteps, const double *rs_dev,
+                 const int *rs_base, double *state[6], cudaStream_t s);
+int finish_steps(Plan &p, cudaStream_t s);
+// re-cut the work items: rows_per_item = 0 for one wave of items by cost
+int repartition(Plan &p, const Dom &d, int rows_per_item, cudaStream_t s);
 void free_plan(Plan &p);
 
 }  // namespace fused

@@ -159,6 +159,62 @@ class BarotropicSolver:
         return int(p.value), (r.value or b"").decode()
 
 
+class Ensemble:
+    """Independent basins advanced together (inmsom_ens_*): each member is a
+    BarotropicSolver with its state resident; `group` substeps of all
+    members per CUDA-graph launch."""
+
+    def __init__(self, members: Sequence["BarotropicSolver"], group: int = 10):
+        self.members = list(members)
+        arr = (ctypes.c_void_p * len(self.members))(*[m._ctx.value for m in self.members])
+        self._ens = ctypes.c_void_p()
+        check(load().inmsom_ens_create(ctypes.byref(self._ens), arr, len(self.members), int(group)))
+
+    def _dt(self, dt):
+        a = np.ascontiguousarray(dt, dtype=np.float64)
+        if a.shape != (len(self.members),):
+            raise ValueError("one dt per member")
+        return a
+
+    def run(self, nsub: int, dt, rhs_scale: Optional[Sequence[float]] = None) -> float:
+        """Advance every member nsub substeps of its dt; returns device ms."""
+        d = self._dt(dt)
+        sc = None
+        if rhs_scale is not None:
+            sc = np.ascontiguousarray(rhs_scale, dtype=np.float64)
+            if sc.shape != (nsub,):
+                raise ValueError("rhs_scale needs one value per substep")
+        ms = ctypes.c_float(0.0)
+        check(load().inmsom_ens_run(self._ens, int(nsub), dptr(d), None if sc is None else dptr(sc),
+                                    ctypes.byref(ms)))
+        return float(ms.value)
+
+    def tune(self, dt, trial_groups: int = 2):
+        """Autotune chunk heights per size class; returns rows per item per
+        member (0 = one wave of cost-balanced chunks).  Advances the states."""
+        d = self._dt(dt)
+        out = (ctypes.c_int * len(self.members))()
+        check(load().inmsom_ens_tune(self._ens, dptr(d), int(trial_groups), out))
+        return list(out)
+
+    def close(self) -> None:
+        if self._ens:
+            load().inmsom_ens_destroy(self._ens)
+            self._ens = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class GpuBackend:
     """Basin set-up on the GPU: gridcon and the wind forcing."""
 

@@ -1,0 +1,75 @@
+"""Ensemble runs (inmsom_ens_*): members of different sizes and both fused
+variants advanced by CUDA-graph launches must end bit for bit where each
+member run alone with inmsom_run_substeps ends -- the same kernels on the
+same data; the work partition (changed by the autotuner) does not change
+any value."""
+import numpy as np
+import pytest
+
+from inmsom_elfs_b200 import basins
+
+pytestmark = pytest.mark.gpu
+
+
+def _members(gpu):
+    out = []
+    for k, (nx, ny) in enumerate(((96, 80), (130, 120), (200, 150), (64, 64))):
+        b = basins.regional_basin(nx=nx, ny=ny, seed=60 + k)
+        if k == 2:   # a 2-D viscosity: the general fused variant
+            rng = np.random.default_rng(70)
+            b.forcing["mu"] = np.asfortranarray(700.0 + 500.0 * rng.random(b.bounds.shape))
+        b.taux *= 0.8 + 0.1 * k
+        basins.finalize(b, gpu.GpuBackend(0))
+        out.append(b)
+    return out
+
+
+def _alone(gpu, b, nsub, scale):
+    bg = b.copy()
+    with gpu.BarotropicSolver(bg, resident=True) as s:
+        s.load_state()
+        s.run_substeps(nsub, b.dt, scale)
+        s.sync_to_host()
+    return bg
+
+
+def _ensemble(gpu, bs, nsub, scale, group, tune=False):
+    cps = [b.copy() for b in bs]
+    solvers = [gpu.BarotropicSolver(b, resident=True) for b in cps]
+    for s in solvers:
+        s.load_state()
+    dts = [b.dt for b in cps]
+    with gpu.Ensemble(solvers, group=group) as e:
+        rows = None
+        if tune:
+            rows = e.tune(dts, trial_groups=1)
+            for s in solvers:
+                s.load_state()        # back to the initial state; the tuned partition stays
+        e.run(nsub, dts, scale)
+    for s in solvers:
+        s.sync_to_host()
+        s.close()
+    return cps, rows
+
+
+@pytest.mark.parametrize("tune", [False, True])
+def test_ensemble_matches_members_run_alone(gpu, tune):
+    bs = _members(gpu)
+    nsub = 22                                   # 5 graph launches of 4 and 2 direct substeps
+    scale = basins.wind_cycle(nsub, 2.0, t0=300.0, period=600.0)
+    ref = [_alone(gpu, b, nsub, scale) for b in bs]
+    got, rows = _ensemble(gpu, bs, nsub, scale, group=4, tune=tune)
+    for r, g in zip(ref, got):
+        for k in r.state:
+            assert np.array_equal(r.state[k], g.state[k]), k
+    if tune:
+        assert len(rows) == len(bs) and all(x in (0, 96, 64, 48, 32) for x in rows)
+
+
+def test_ensemble_rejects_odd_group(gpu):
+    from inmsom_elfs_b200 import InmsomError
+    b = _members(gpu)[0]
+    with gpu.BarotropicSolver(b.copy(), resident=True) as s:
+        s.load_state()
+        with pytest.raises(InmsomError):
+            gpu.Ensemble([s], group=3)
