@@ -18,6 +18,10 @@ state evolution of barotropic_dynamics(tau=dt, nstep=1) keeping *_e.
 --fp32-velocity measures the same workload with u, up, v, vp stored in FP32
 on the device (80 algorithmic bytes per cell and substep; arithmetic, SSH
 and budgets FP64); the e2e arm stays FP64.
+--study ensemble advances 64 independent regional basins (sides drawn from
+192, 256, .., 1536, own seeds, wind amplitude +-20 %) for --steps substeps:
+tuned CUDA-graph ensemble, untuned ensemble, and the members one after
+another (a study line).
 --study fp32 runs the FP32-velocity variant against the FP64 run on the
 4096 x 4096 ridge basin (2 km, dt = 3 s) for --steps substeps and prints the
 per-field max/RMS differences (a study line, not a benchmark line).
@@ -62,7 +66,9 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--fp32-velocity", action="store_true")
-    p.add_argument("--study", default=None, choices=["fp32"])
+    p.add_argument("--study", default=None, choices=["fp32", "ensemble"])
+    p.add_argument("--members", type=int, default=64)
+    p.add_argument("--group", type=int, default=20)
     return p.parse_args()
 
 
@@ -375,9 +381,60 @@ def run_study_fp32(args):
     }), flush=True)
 
 
+def run_study_ensemble(args):
+    """64 independent basins: graph ensemble (tuned, untuned) against the
+    members run one after another with inmsom_run_substeps."""
+    import torch
+    from inmsom_elfs_b200 import basins, solver
+    torch.cuda.set_device(0)
+    rng = np.random.default_rng(1234)
+    sides = rng.choice(np.arange(192, 1537, 64), size=args.members)
+    amps = rng.uniform(0.8, 1.2, size=args.members)
+    bs = []
+    for i, (n, a) in enumerate(zip(sides, amps)):
+        b = basins.regional_basin(nx=int(n), ny=int(n), seed=100 + i)
+        b.taux *= a
+        b.tauy *= a
+        basins.finalize(b, solver.GpuBackend(0))
+        bs.append(b)
+    cells = sum(b.cells for b in bs)
+    dts = [b.dt for b in bs]
+    scale = basins.wind_cycle(args.steps, bs[0].dt)
+    solvers = [solver.BarotropicSolver(b, resident=True) for b in bs]
+    res = {}
+    # members one after another (one launch per substep each)
+    for s in solvers:
+        s.load_state()
+    t = 0.0
+    for s, b in zip(solvers, bs):
+        s.run_substeps(10, b.dt)
+        t += s.run_substeps(args.steps, b.dt, scale)
+    res["sequential_members"] = {"ms": t, "cell_steps_per_s": cells * args.steps / (t / 1e3)}
+    with solver.Ensemble(solvers, group=args.group) as e:
+        for tag in ("graph_untuned", "graph_tuned"):
+            if tag == "graph_tuned":
+                rows = e.tune(dts, trial_groups=2)
+            for s in solvers:
+                s.load_state()
+            e.run(2 * args.group, dts)
+            for s in solvers:
+                s.load_state()
+            ms = e.run(args.steps, dts, scale)
+            res[tag] = {"ms": ms, "cell_steps_per_s": cells * args.steps / (ms / 1e3)}
+    for s in solvers:
+        s.close()
+    print(json.dumps({
+        "study": "ensemble", "members": args.members, "sides": [int(x) for x in sides],
+        "wind_amplitude": [round(float(x), 3) for x in amps], "total_cells": cells, "steps": args.steps,
+        "group": args.group, "rows_per_item_chosen": rows, "results": res,
+    }), flush=True)
+
+
 if __name__ == "__main__":
     a = parse()
-    if a.study == "fp32":
+    if a.study == "ensemble":
+        run_study_ensemble(a)
+    elif a.study == "fp32":
         run_study_fp32(a)
     elif a.impl == "reference":
         run_reference(a)
