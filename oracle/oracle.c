@@ -73,11 +73,23 @@ void ora_cyclize8_y(const ora_bounds *b, double *f)
     }
 }
 
-/* the "syncborder + cyclize" pair that follows every field update; on one
- * domain syncborder_real8 exchanges nothing (Modules/
- * mod_mpi_parallel_tools.f90:138-173 with no neighbours). */
+/* syncborder_real8 (Modules/mod_mpi_parallel_tools.f90:179-252): on one
+ * domain it exchanges nothing (check_p_coord, :102-113, skips neighbours
+ * outside the process grid); for a strip of a 1 x P process grid the
+ * caller's hook does the exchanges (rank tests only). */
+static ora_exchange_fn g_exchange = 0;
+static void *g_exchange_user = 0;
+
+void ora_set_exchange(ora_exchange_fn fn, void *user)
+{
+    g_exchange = fn;
+    g_exchange_user = user;
+}
+
+/* the "syncborder + cyclize" pair that follows every field update */
 static void halo(const ora_bounds *b, double *f)
 {
+    if (g_exchange) g_exchange(f, g_exchange_user);
     if (b->periodicity_x) ora_cyclize8_x(b, f);
     if (b->periodicity_y) ora_cyclize8_y(b, f);
 }

@@ -65,6 +65,11 @@ void ora_gridcon(const ora_bounds *b, const float *lu, float *luu, float *luh,
 
 /* Service/oc_algorithms.f90:50-95 (multi-process wrap semantics) and
  * :118-135. */
+/* syncborder_real8 hook: called with every field the reference exchanges
+ * between MPI ranks, at the point it exchanges it (NULL: one domain). */
+typedef void (*ora_exchange_fn)(double *field, void *user);
+void ora_set_exchange(ora_exchange_fn fn, void *user);
+
 void ora_cyclize8_x(const ora_bounds *b, double *f);
 void ora_cyclize8_y(const ora_bounds *b, double *f);
 

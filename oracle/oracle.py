@@ -56,7 +56,8 @@ def build() -> Path:
 def load():
     global _lib
     if _lib is None:
-        if not LIB_PATH.exists():
+        src = Path(__file__).with_name("oracle.c")
+        if not LIB_PATH.exists() or LIB_PATH.stat().st_mtime < src.stat().st_mtime:
             build()
         _lib = ctypes.CDLL(str(LIB_PATH))
         _lib.ora_guard.restype = ctypes.c_long
@@ -210,3 +211,23 @@ class OracleBackend:
 
     def wind_forcing(self, basin):
         return wind_forcing(basin)
+
+
+EXCHANGE_FN = ctypes.CFUNCTYPE(None, ctypes.POINTER(ctypes.c_double), ctypes.c_void_p)
+_exchange_keep = None
+
+
+def set_exchange(fn):
+    """Install fn(field) at every syncborder_real8 point of the oracle
+    (Modules/mod_mpi_parallel_tools.f90:179-252), field being a ctypes
+    pointer to the local array; None removes it.  For rank tests."""
+    global _exchange_keep
+    lib = load()
+    lib.ora_set_exchange.argtypes = [EXCHANGE_FN, ctypes.c_void_p]
+    if fn is None:
+        lib.ora_set_exchange(EXCHANGE_FN(), None)
+        _exchange_keep = None
+        return
+    cb = EXCHANGE_FN(lambda ptr, user: fn(ptr))
+    _exchange_keep = cb
+    lib.ora_set_exchange(cb, None)
