@@ -287,6 +287,25 @@ int inmsom_ens_run(inmsom_ens *ens, int nsub, const double *dt, const double *rh
 int inmsom_ens_tune(inmsom_ens *ens, const double *dt, int trial_groups, int *rows_per_item);
 int inmsom_ens_destroy(inmsom_ens *ens);
 
+/* Row strips of one basin on several contexts (one per GPU, or several on
+ * one GPU); replaces the halo exchange of syncborder_real8
+ * (Modules/mod_mpi_parallel_tools.f90:179-252) for the fused path of a
+ * 1 x n process grid.  ctxs[0..n) hold consecutive strips, south to north,
+ * with the bounds mpi_array_boundary_definition (Control/init_arrays.f90:
+ * 21-88) gives for p_size = (1, n) -- the two halo rows next to another
+ * strip hold that strip's values -- each with its state resident.
+ * inmsom_strips_run advances every strip by nsub substeps of dt (the state
+ * evolution of inmsom_run_substeps on the whole basin); after each substep
+ * the two rows of the six state fields next to every internal boundary are
+ * copied into the neighbour's halo rows (the fused kernel recomputes what
+ * it needs in its halo rows, so one exchange per substep gives the
+ * single-domain result bit for bit).  Contexts on different devices get
+ * peer access. */
+typedef struct inmsom_strips inmsom_strips;
+int inmsom_strips_create(inmsom_strips **strips, inmsom_ctx *const *ctxs, int n);
+int inmsom_strips_run(inmsom_strips *strips, int nsub, double dt, const double *rhs_scale, float *ms);
+int inmsom_strips_destroy(inmsom_strips *strips);
+
 int inmsom_gpu_finalize(inmsom_ctx *ctx);
 const char *inmsom_gpu_last_error(void);
 

@@ -24,7 +24,7 @@ EXPORTS = (
     "inmsom_gpu_sync_to_host", "inmsom_gpu_sync_from_host", "inmsom_run_substeps",
     "inmsom_gpu_path", "inmsom_gpu_finalize", "inmsom_gpu_last_error", "inmsom_load_state",
     "inmsom_diag_noalloc", "inmsom_ens_create", "inmsom_ens_run", "inmsom_ens_tune",
-    "inmsom_ens_destroy",
+    "inmsom_ens_destroy", "inmsom_strips_create", "inmsom_strips_run", "inmsom_strips_destroy",
 )
 
 # include/inmsom_gpu.h: INMSOM_DIAG_NOALLOC_MAX_ROWS
@@ -87,6 +87,9 @@ def load() -> ctypes.CDLL:
     lib.inmsom_ens_run.argtypes = [VP, i, DP, DP, ctypes.POINTER(ctypes.c_float)]
     lib.inmsom_ens_tune.argtypes = [VP, DP, i, ctypes.POINTER(i)]
     lib.inmsom_ens_destroy.argtypes = [VP]
+    lib.inmsom_strips_create.argtypes = [ctypes.POINTER(VP), ctypes.POINTER(VP), i]
+    lib.inmsom_strips_run.argtypes = [VP, i, d, DP, ctypes.POINTER(ctypes.c_float)]
+    lib.inmsom_strips_destroy.argtypes = [VP]
     lib.inmsom_diag_noalloc.argtypes = ([ctypes.POINTER(CBounds), ctypes.POINTER(CConsts),
                                          ctypes.c_longlong] + [VP] * 16 + [VP])
     for name in EXPORTS:

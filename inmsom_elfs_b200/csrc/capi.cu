@@ -996,3 +996,161 @@ int inmsom_ens_destroy(inmsom_ens *e)
     delete e;
     return INMSOM_OK;
 }
+
+// ===========================================================================
+// Row strips of one basin: one fused substep per strip, then the rows next
+// to every internal boundary copied into the neighbour's halo rows.
+struct inmsom_strips {
+    std::vector<inmsom_ctx *> m;
+    std::vector<cudaEvent_t> done;   // per strip: its substep kernel finished
+    cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+};
+
+namespace {
+
+// copy rows [r, r+1] of the six fields of `from`'s current state set into
+// rows [h, h+1] of `to`'s, on `to`'s stream... or the stream given
+int copy_rows(const inmsom_ctx *from, int r, inmsom_ctx *to, int h, cudaStream_t s)
+{
+    const size_t pitch_b = (size_t)from->dom.pitch * sizeof(double);
+    const size_t fs_from = (size_t)from->dom.pitch * from->dom.nya() * sizeof(double);
+    const size_t fs_to = (size_t)to->dom.pitch * to->dom.nya() * sizeof(double);
+    CK(cudaMemcpy2DAsync(to->state[0] + (size_t)h * to->dom.pitch, fs_to, from->state[0] + (size_t)r * from->dom.pitch,
+                         fs_from, 2 * pitch_b, NSTATE, cudaMemcpyDefault, s));
+    return INMSOM_OK;
+}
+
+}  // namespace
+
+int inmsom_strips_create(inmsom_strips **out, inmsom_ctx *const *ctxs, int n)
+{
+    if (!out || !ctxs || n < 1) return set_err(INMSOM_EARG, "inmsom_strips_create: no strips");
+    *out = nullptr;
+    for (int k = 0; k < n; k++) {
+        const inmsom_ctx *c = ctxs[k];
+        if (!c || !c->grid_ok) return set_err(INMSOM_EARG, "strip %d: grid not registered", k);
+        if (!c->fused_ok) return set_err(INMSOM_EUNSUPPORTED, "strip %d: fused path not eligible (%s)", k, c->fused_reason);
+        if (c->flags & INMSOM_FP32_VELOCITY) return set_err(INMSOM_EUNSUPPORTED, "strip %d: FP64 state only", k);
+        if (k > 0) {
+            const Dom &a = ctxs[k - 1]->dom, &b = c->dom;
+            if (a.ny_end + 1 != b.ny_start || a.nx_start != b.nx_start || a.nx_end != b.nx_end ||
+                a.bnd_x1 != b.bnd_x1 || a.bnd_x2 != b.bnd_x2 || a.pitch != b.pitch || a.nnn != b.nnn || a.nn != b.nn)
+                return set_err(INMSOM_EARG, "strips %d and %d are not consecutive row strips of one basin", k - 1, k);
+        }
+    }
+    if (ctxs[0]->dom.ny_start != ctxs[0]->dom.nnn || ctxs[n - 1]->dom.ny_end != ctxs[n - 1]->dom.nn)
+        return set_err(INMSOM_EARG, "the strips do not cover the basin's rows nnn..nn");
+    // peer access between neighbouring strips on different devices
+    for (int k = 0; k + 1 < n; k++) {
+        const int a = ctxs[k]->device, b = ctxs[k + 1]->device;
+        if (a == b) continue;
+        int ok_ab = 0, ok_ba = 0;
+        CK(cudaDeviceCanAccessPeer(&ok_ab, a, b));
+        CK(cudaDeviceCanAccessPeer(&ok_ba, b, a));
+        if (!ok_ab || !ok_ba) return set_err(INMSOM_EUNSUPPORTED, "devices %d and %d lack peer access", a, b);
+        for (int t = 0; t < 2; t++) {
+            CK(cudaSetDevice(t ? b : a));
+            const cudaError_t e = cudaDeviceEnablePeerAccess(t ? a : b, 0);
+            if (e == cudaErrorPeerAccessAlreadyEnabled) (void)cudaGetLastError();
+            else CK(e);
+        }
+    }
+    inmsom_strips *g = new inmsom_strips();
+    g->m.assign(ctxs, ctxs + n);
+    g->done.assign(n, nullptr);
+    cudaError_t ce = cudaSuccess;
+    for (int k = 0; k < n && ce == cudaSuccess; k++) {
+        ce = cudaSetDevice(ctxs[k]->device);
+        if (ce == cudaSuccess) ce = cudaEventCreateWithFlags(&g->done[k], cudaEventDisableTiming);
+    }
+    if (ce == cudaSuccess) ce = cudaSetDevice(ctxs[0]->device);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&g->ev0);
+    if (ce == cudaSuccess) ce = cudaEventCreate(&g->ev1);
+    if (ce != cudaSuccess) {
+        inmsom_strips_destroy(g);
+        return set_err(INMSOM_ECUDA, "inmsom_strips_create: %s", cudaGetErrorString(ce));
+    }
+    *out = g;
+    return INMSOM_OK;
+}
+
+int inmsom_strips_run(inmsom_strips *g, int nsub, double dt, const double *rhs_scale, float *ms)
+{
+    if (!g) return set_err(INMSOM_EARG, "NULL argument");
+    if (nsub < 0) return set_err(INMSOM_EARG, "nsub < 0");
+    if (!(dt > 0.0)) return set_err(INMSOM_EARG, "dt must be > 0");
+    const int n = (int)g->m.size();
+    for (int k = 0; k < n; k++) {
+        inmsom_ctx *c = g->m[k];
+        if (!c->state_on_device) return set_err(INMSOM_EARG, "strip %d: no resident state", k);
+        CK(cudaSetDevice(c->device));
+        if (fused::prepare_steps(c->plan, c->dom, c->c, c->state, c->forc, c->stream))
+            return set_err(INMSOM_ECUDA, "strip %d: prepare failed: %s", k, cudaGetErrorString(cudaGetLastError()));
+    }
+    inmsom_ctx *c0 = g->m[0];
+    CK(cudaSetDevice(c0->device));
+    CK(cudaEventRecord(g->ev0, c0->stream));
+    for (int k = 1; k < n; k++) {   // every strip starts after ev0
+        CK(cudaSetDevice(g->m[k]->device));
+        CK(cudaStreamWaitEvent(g->m[k]->stream, g->ev0, 0));
+    }
+    for (int step = 0; step < nsub; step++) {
+        const double rs = rhs_scale ? rhs_scale[step] : 1.0;
+        for (int k = 0; k < n; k++) {
+            inmsom_ctx *c = g->m[k];
+            CK(cudaSetDevice(c->device));
+            if (fused::launch_steps(c->plan, c->dom, c->c, dt, 1, nullptr, nullptr, c->state, c->stream, rs))
+                return set_err(INMSOM_ECUDA, "strip %d: launch failed", k);
+            CK(cudaEventRecord(g->done[k], c->stream));
+        }
+        // halo rows of the new state: strip k's two northernmost interior
+        // rows into k+1's southern halo rows, k+1's two southernmost into
+        // k's northern halo rows
+        for (int k = 0; k + 1 < n; k++) {
+            inmsom_ctx *a = g->m[k], *b = g->m[k + 1];
+            const int a_last = a->dom.ny_end - a->dom.bnd_y1;   // device row of ny_end
+            CK(cudaSetDevice(b->device));
+            CK(cudaStreamWaitEvent(b->stream, g->done[k], 0));
+            CKR(copy_rows(a, a_last - 1, b, 0, b->stream));
+            CK(cudaSetDevice(a->device));
+            CK(cudaStreamWaitEvent(a->stream, g->done[k + 1], 0));
+            CKR(copy_rows(b, 2, a, a_last + 1, a->stream));
+        }
+    }
+    // ev1 after every strip's last work
+    for (int k = 0; k < n; k++) {
+        CK(cudaSetDevice(g->m[k]->device));
+        CK(cudaEventRecord(g->done[k], g->m[k]->stream));
+    }
+    CK(cudaSetDevice(c0->device));
+    for (int k = 1; k < n; k++) CK(cudaStreamWaitEvent(c0->stream, g->done[k], 0));
+    CK(cudaEventRecord(g->ev1, c0->stream));
+    for (int k = 0; k < n; k++) {
+        inmsom_ctx *c = g->m[k];
+        CK(cudaSetDevice(c->device));
+        if (fused::finish_steps(c->plan, c->stream))
+            return set_err(INMSOM_ECUDA, "strip %d: %s", k, cudaGetErrorString(cudaGetLastError()));
+        c->depths_current = false;
+        if (c->plan.last_flags & fused::FLAG_TIMEOUT)
+            return set_err(INMSOM_ETIMEOUT, "strip %d: a bounded TMA wait timed out", k);
+    }
+    CK(cudaSetDevice(c0->device));
+    CK(cudaEventSynchronize(g->ev1));
+    if (ms) CK(cudaEventElapsedTime(ms, g->ev0, g->ev1));
+    return INMSOM_OK;
+}
+
+int inmsom_strips_destroy(inmsom_strips *g)
+{
+    if (!g) return INMSOM_OK;
+    for (size_t k = 0; k < g->m.size(); k++) {
+        cudaSetDevice(g->m[k]->device);
+        if (g->m[k]->stream) cudaStreamSynchronize(g->m[k]->stream);
+        if (g->done[k]) cudaEventDestroy(g->done[k]);
+    }
+    if (!g->m.empty()) cudaSetDevice(g->m[0]->device);
+    if (g->ev0) cudaEventDestroy(g->ev0);
+    if (g->ev1) cudaEventDestroy(g->ev1);
+    delete g;
+    return INMSOM_OK;
+}

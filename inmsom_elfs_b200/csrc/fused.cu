@@ -1106,12 +1106,17 @@ const char *check_eligible(const Plan &p, const Dom &d, const Consts &c, const f
     if (d.xoff != XOFF) return "device layout without the fused column offset";
     const int nxa = d.nxa(), nya = d.nya();
     auto at = [&](const float *a, int m, int n) { return a[(size_t)(n - d.bnd_y1) * nxa + (m - d.bnd_x1)]; };
+    if (d.nx_start != d.mmm || d.nx_end != d.mm) return "domain split along x (only row strips are supported)";
+    // a row strip of a larger basin: the halo rows next to another strip
+    // hold that strip's values (they may be ocean)
+    const bool open_s = d.ny_start > d.nnn, open_n = d.ny_end < d.nn;
     const float *lu = masks[0];
     for (int n = d.bnd_y1; n <= d.bnd_y2; n++)
         for (int m = d.bnd_x1; m <= d.bnd_x2; m++) {
             float v = at(lu, m, n);
             if (v != 0.0f && v != 1.0f) return "lu is not 0/1";
-            bool interior = m >= d.nx_start && m <= d.nx_end && n >= d.ny_start && n <= d.ny_end;
+            const bool row_ok = (n >= d.ny_start || open_s) && (n <= d.ny_end || open_n);
+            bool interior = m >= d.nx_start && m <= d.nx_end && row_ok;
             if (!interior && v != 0.0f) return "ocean points in the halo ring";
         }
     // derived masks must be gridcon(lu) (Service/grid_construction.f90:59-112)
@@ -1128,9 +1133,14 @@ const char *check_eligible(const Plan &p, const Dom &d, const Consts &c, const f
             if (a + b2 > 0.5f) ref[4][i] = 1.0f;             // llu
             if (a + cc > 0.5f) ref[5][i] = 1.0f;             // llv
         }
+    // rows next to another strip carry that strip's masks: not compared
     for (int k = 0; k < 6; k++)
-        if (std::memcmp(ref[k].data(), masks[k + 1], ref[k].size() * sizeof(float)) != 0)
-            return "derived masks differ from gridcon(lu)";
+        for (int n = d.bnd_y1; n <= d.bnd_y2; n++) {
+            if ((n < d.ny_start - 1 && open_s) || (n > d.ny_end && open_n)) continue;
+            const size_t o = (size_t)(n - d.bnd_y1) * nxa;
+            if (std::memcmp(ref[k].data() + o, masks[k + 1] + o, (size_t)nxa * sizeof(float)) != 0)
+                return "derived masks differ from gridcon(lu)";
+        }
     // metrics and Coriolis constant along rows over the points the step reads
     for (int k = 0; k < 9; k++)
         for (int n = d.ny_start - 1; n <= d.ny_end + 1; n++) {
@@ -1416,7 +1426,7 @@ int prepare_steps(Plan &p, const Dom &d, const Consts &c, double *state[6], doub
 }
 
 int launch_steps(Plan &p, const Dom &d, const Consts &c, double dt, int nsteps, const double *rs_dev,
-                 const int *rs_base, double *state[6], cudaStream_t s)
+                 const int *rs_base, double *state[6], cudaStream_t s, double rs_host)
 {
     if (!p.prepared) return 1;
     Forcing f{true, p.prep_mu0, p.prep_rd0, p.prep_wq0};
@@ -1428,6 +1438,7 @@ int launch_steps(Plan &p, const Dom &d, const Consts &c, double dt, int nsteps, 
     for (int k = 0; k < 4; k++) q.acc[k] = nullptr;
     q.rs_dev = rs_dev;
     q.rs_base = rs_base;
+    q.rhs_scale = rs_host;
     for (int step = 0; step < nsteps; step++) {
         if (set_io(p, q, (step & 1) ? p.buf[0] : state, (step & 1) ? state : p.buf[0])) return 1;
         q.rs_k = step;

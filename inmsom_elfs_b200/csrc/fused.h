@@ -145,13 +145,14 @@ int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt,
 // Capture-friendly form of run_substeps for CUDA graphs (FP64): prepare_steps
 // classifies the forcing and stages it (it synchronises the stream);
 // launch_steps then only enqueues nsteps kernels, the RHS scale of launch k
-// being rs_dev[*rs_base + k] read on the device (an even nsteps leaves the
+// being rs_dev[*rs_base + k] read on the device, or rs_host when rs_dev is
+// NULL (an even nsteps leaves the
 // state in the same set, so the launches can be replayed); finish_steps
 // reads the status bits.
 int prepare_steps(Plan &p, const Dom &d, const Consts &c, double *state[6], double *forc[6],
                   cudaStream_t s);
 int launch_steps(Plan &p, const Dom &d, const Consts &c, double dt, int nsteps, const double *rs_dev,
-                 const int *rs_base, double *state[6], cudaStream_t s);
+                 const int *rs_base, double *state[6], cudaStream_t s, double rs_host = 1.0);
 int finish_steps(Plan &p, cudaStream_t s);
 // re-cut the work items: rows_per_item = 0 for one wave of items by cost
 int repartition(Plan &p, const Dom &d, int rows_per_item, cudaStream_t s);

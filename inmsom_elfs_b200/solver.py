@@ -215,6 +215,46 @@ class Ensemble:
             pass
 
 
+class Strips:
+    """Row strips of one basin advanced together (inmsom_strips_*): each
+    strip is a BarotropicSolver of a Basin from strips.split_basin, south
+    to north, with its state resident."""
+
+    def __init__(self, members: Sequence["BarotropicSolver"]):
+        self.members = list(members)
+        arr = (ctypes.c_void_p * len(self.members))(*[m._ctx.value for m in self.members])
+        self._g = ctypes.c_void_p()
+        check(load().inmsom_strips_create(ctypes.byref(self._g), arr, len(self.members)))
+
+    def run(self, nsub: int, dt: float, rhs_scale: Optional[Sequence[float]] = None) -> float:
+        sc = None
+        if rhs_scale is not None:
+            sc = np.ascontiguousarray(rhs_scale, dtype=np.float64)
+            if sc.shape != (nsub,):
+                raise ValueError("rhs_scale needs one value per substep")
+        ms = ctypes.c_float(0.0)
+        check(load().inmsom_strips_run(self._g, int(nsub), float(dt), None if sc is None else dptr(sc),
+                                       ctypes.byref(ms)))
+        return float(ms.value)
+
+    def close(self) -> None:
+        if self._g:
+            load().inmsom_strips_destroy(self._g)
+            self._g = ctypes.c_void_p()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
 class GpuBackend:
     """Basin set-up on the GPU: gridcon and the wind forcing."""
 
