@@ -69,7 +69,6 @@ struct alignas(64) Params {
     const RowCoef *rows;
     const double *cor;
     const int4 *items;     // work items {g0, first row, end row (exclusive), 0}
-    const double *rx, *ry; // RHSx, RHSy (fields of the static block)
     long long pitch;
     int bm_words;
     int c_first, c_last;   // interior device columns
@@ -141,7 +140,7 @@ struct Layout {
     static_assert(!(GEN && F32), "FP32 velocities exist in the uniform variant only");
     static constexpr int VSEG = F32 ? SEG + 4 : 0;                       // FP32 columns per velocity field
     static constexpr int SSH_OFF = F32 ? (4 * VSEG * 4 + 127) / 128 * 128 : 0;
-    static constexpr int NS = GEN ? 4 : 1;                               // static fields in a slot
+    static constexpr int NS = F32 ? 1 : (GEN ? 6 : 3);                   // static fields in a slot
     static constexpr int STAT_OFF = F32 ? (SSH_OFF + 2 * SEG * 8 + 127) / 128 * 128 : 1792;
     static constexpr int COEF_OFF = STAT_OFF + NS * SEG * 8;             // general variant: RowCoef
     static constexpr int BITS_OFF = COEF_OFF + (GEN ? (int)sizeof(RowCoef) : 0);
@@ -156,7 +155,9 @@ struct Layout {
 // (4 warps per SM sub-partition, 128 registers) for the plain substep, 12
 // where the time-mean sums need more registers, 11 for the general variant,
 // and never more than the shared memory holds (228 KB per SM, 1 KB of it
-// reserved per CTA)
+// reserved per CTA): 13 for the FP64 uniform ring, 9 for the general one.
+// (Reading the forcing from global memory instead of the ring lets 16 fit
+// but exposes the load latency: 5% slower.)
 template <bool GEN, int MODE, bool F32 = false>
 constexpr int min_ctas()
 {
@@ -439,8 +440,11 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
                 au = av = p.d2;
                 n.cor = p.cor[j];
             }
-            n.Ru = slx - rdu * AS(o_0, S_UP, 0) * au * hu;
-            n.Rv = sly - rdv * AS(o_0, S_VP, 0) * av * hv;
+            // RHS: from the ring (FP64 state) or from the FP32 copy
+            const double rx = F32 ? (double)p.rx32[gi] : AT(o_0, T_RX, 0);
+            const double ry = F32 ? (double)p.ry32[gi] : AT(o_0, T_RY, 0);
+            n.Ru = rx * rs + slx - rdu * AS(o_0, S_UP, 0) * au * hu;
+            n.Rv = ry * rs + sly - rdv * AS(o_0, S_VP, 0) * av * hv;
             if (ACC) {
                 n.slx = slx;
                 n.sly = sly;
@@ -448,9 +452,6 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
         }
 
         // forcing of the rows that stage 3 updates, loaded early
-        double rxf = 0.0, ryf = 0.0;
-        if constexpr (D3U) rxf = F32 ? (double)p.rx32[gi - p.pitch] : p.rx[gi - p.pitch];
-        if constexpr (D3V) ryf = F32 ? (double)p.ry32[gi - 2 * p.pitch] : p.ry[gi - 2 * p.pitch];
 
         // ---------------- stage 2: row rho = j-1 -------------------------
         double FX, FY, GY, ST, SS, QU, QV, sn, vs, u_r, up_r, v_m, vp_m;
@@ -538,7 +539,7 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
                 const double hup = ((h0 + sp0) + (h1 + sp1)) * ku2;
                 const double hun = ((h0 + sn) + (h1 + SNr)) * ku2;
                 const double difx = GEN ? (STr - ST) * CF(o_m1, dux) + SS * CF(o_m1, dus0) : ((STr - ST) + SS) * p.d;
-                const double grx = rxf * rs + c.Ru + qc.Cu - ((FXr - FX) + FY) + difx + QU * 0.25;
+                const double grx = c.Ru + qc.Cu - ((FXr - FX) + FY) + difx + QU * 0.25;
                 const double un = (up_r * hup + grx * (GEN ? two_ti * CF(o_m1, rau) : p.tt)) * rcp_nr(hun);
                 bad |= (uint32_t)(wu && !(fabs(un) < 100.0));
                 bad |= (uint32_t)(wt && !(fabs(sn) < 10.0));
@@ -583,7 +584,7 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
                     hvp = ((h0 + sp0) + (h1 + sp1)) * 0.5;
                     hvn = ((h0 + sn0) + (h1 + sn1)) * 0.5;
                 }
-                const double gry = ryf * rs + qc.Pv - (GX - GXl) - GY - ST * (GEN ? CF(o_m2, dvt1) : p.d);
+                const double gry = qc.Pv - (GX - GXl) - GY - ST * (GEN ? CF(o_m2, dvt1) : p.d);
                 const double vn = (vp0 * hvp + gry * (GEN ? two_ti * CF(o_m2, rav) : p.tt)) * rcp_nr(hvn);
                 bad |= (uint32_t)(wv && !(fabs(vn) < 100.0));
                 const long long idx = gi - 2 * p.pitch;
@@ -780,9 +781,9 @@ int forcing_mode(Plan &p, const Dom &d, const Consts &c, double *forc[6], cudaSt
 int stage_forcing(Plan &p, double *forc[6], int gen, cudaStream_t s)
 {
     const size_t fb = (size_t)p.fstride * sizeof(double);
-    const int src_of[NSTAT] = {-1, 3, 5, 2, 0, 1};   // T_* <- forc index (RHSx RHSy wflux mu mu4 rdis)
+    const int src_of[NSTAT] = {-1, 0, 1, 3, 5, 2};   // T_* <- forc index (RHSx RHSy wflux mu mu4 rdis)
     for (int t = 1; t < NSTAT; t++)
-        if ((gen || t >= T_RX) &&
+        if ((gen || t <= T_RY) &&
             cudaMemcpyAsync(p.stat + t * p.fstride, forc[src_of[t]], fb, cudaMemcpyDeviceToDevice, s) != cudaSuccess)
             return 1;
     return 0;
@@ -813,8 +814,6 @@ Params base_params(const Plan &p, const Dom &d, const Consts &c, const Forcing &
     q.gd = c.g * p.d;
     q.d2 = p.d * p.d;
     q.items = p.items[gen];
-    q.rx = p.stat + T_RX * p.fstride;
-    q.ry = p.stat + T_RY * p.fstride;
     return q;
 }
 
@@ -855,11 +854,15 @@ void launch_g(const Plan &p, const Params &q, int mode, cudaStream_t s)
     }
 }
 
-void launch(Plan &p, const Params &q, int gen, int mode, cudaStream_t s)
+// returns nonzero (nothing launched) if the static map does not bring
+// exactly the fields the ring layout holds
+int launch(Plan &p, const Params &q, int gen, int mode, cudaStream_t s)
 {
+    if (p.stat_box[gen] != (gen ? Layout<true>::NS : Layout<false>::NS)) return 1;
     p.last_variant = gen;
     if (gen) launch_g<true>(p, q, mode, s);
     else launch_g<false>(p, q, mode, s);
+    return 0;
 }
 
 int sync_buffers(Plan &p, double *state[6], cudaStream_t s)
@@ -1068,6 +1071,8 @@ int ensure_f32(Plan &p, const Dom &d, cudaStream_t s)
         if (encode_fields(enc, &p.tm_vel[b], p.vset[b], d, p.fstride, 4, 4, true)) return 1;
         if (encode_fields(enc, &p.tm_ssh[b], p.set[b], d, p.fstride, NSET, 2)) return 1;
     }
+    if (encode_fields(enc, &p.tm_stat_f32, p.stat, d, p.fstride, NSTAT, Layout<false, true>::NS)) return 1;
+    p.stat_box_f32 = Layout<false, true>::NS;
     if (cudaMalloc(&p.stat32, 2 * fb) != cudaSuccess) return 1;
     return 0;
 }
@@ -1265,6 +1270,8 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
         if (encode_fields(enc, &p.tm_set[b], p.set[b], d, p.fstride, NSET, NSET)) return 1;
     if (encode_fields(enc, &p.tm_stat[0], p.stat, d, p.fstride, NSTAT, Layout<false>::NS)) return 1;
     if (encode_fields(enc, &p.tm_stat[1], p.stat, d, p.fstride, NSTAT, Layout<true>::NS)) return 1;
+    p.stat_box[0] = Layout<false>::NS;
+    p.stat_box[1] = Layout<true>::NS;
 
     if (cudaMalloc(&p.d_uniform, (size_t)MINMAX_BLOCKS * 6 * sizeof(double)) != cudaSuccess) return 1;
     if (cudaMalloc(&p.d_flags, sizeof(unsigned)) != cudaSuccess) return 1;
@@ -1316,8 +1323,7 @@ int dynamics(Plan &p, const Dom &d, const Consts &c, double tau, int nstep, doub
     for (int step = 1; step <= nstep; step++) {
         const bool odd = step & 1;
         if (set_io(p, q, odd ? state : p.buf[0], odd ? p.buf[0] : state)) return 1;
-        launch(p, q, gen, step == 1 ? 4 : 5, s);
-        if (cudaGetLastError() != cudaSuccess) return 1;
+        if (launch(p, q, gen, step == 1 ? 4 : 5, s) || cudaGetLastError() != cudaSuccess) return 1;
     }
     if (nstep & 1)
         for (int k = 0; k < 6; k++) std::swap(state[k], p.buf[0][k]);
@@ -1327,8 +1333,7 @@ int dynamics(Plan &p, const Dom &d, const Consts &c, double tau, int nstep, doub
         double *const *src = k2 == 1 ? state : ((k2 & 1) ? p.buf[1] : p.buf[0]);
         double *const *dst = (k2 & 1) ? p.buf[0] : p.buf[1];
         if (set_io(p, q, src, dst)) return 1;
-        launch(p, q, gen, k2 < nstep ? 5 : 2, s);
-        if (cudaGetLastError() != cudaSuccess) return 1;
+        if (launch(p, q, gen, k2 < nstep ? 5 : 2, s) || cudaGetLastError() != cudaSuccess) return 1;
     }
     unsigned flags = 0;
     if (read_flags(p, s, &flags)) return 1;
@@ -1363,6 +1368,10 @@ int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt, co
         k_to_f32<<<blocks, 256, 0, s>>>(p.stat + T_RX * p.fstride, p.stat32, 2 * p.fstride);
         q.rx32 = p.stat32;
         q.ry32 = p.stat32 + p.fstride;
+        // the ring's static segment holds Layout<false, true>::NS fields:
+        // the map must bring exactly that many
+        if (p.stat_box_f32 != Layout<false, true>::NS) return 1;
+        q.tm_stat = p.tm_stat_f32;
         for (int step = 0; step < nsub; step++) {
             const int si = (step & 1) ? b : a, di = (step & 1) ? a : b;
             q.tm_src = p.tm_vel[si];
@@ -1389,8 +1398,7 @@ int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt, co
     for (int step = 0; step < nsub; step++) {
         if (set_io(p, q, (step & 1) ? p.buf[0] : state, (step & 1) ? state : p.buf[0])) return 1;
         q.rhs_scale = rhs_scale ? rhs_scale[step] : 1.0;
-        launch(p, q, gen, 3, s);
-        if (cudaGetLastError() != cudaSuccess) return 1;
+        if (launch(p, q, gen, 3, s) || cudaGetLastError() != cudaSuccess) return 1;
     }
     if (nsub & 1)
         for (int k = 0; k < 6; k++) std::swap(state[k], p.buf[0][k]);
@@ -1442,8 +1450,7 @@ int launch_steps(Plan &p, const Dom &d, const Consts &c, double dt, int nsteps, 
     for (int step = 0; step < nsteps; step++) {
         if (set_io(p, q, (step & 1) ? p.buf[0] : state, (step & 1) ? state : p.buf[0])) return 1;
         q.rs_k = step;
-        launch(p, q, gen, 3, s);
-        if (cudaGetLastError() != cudaSuccess) return 1;
+        if (launch(p, q, gen, 3, s) || cudaGetLastError() != cudaSuccess) return 1;
     }
     if (nsteps & 1)
         for (int k = 0; k < 6; k++) std::swap(state[k], p.buf[0][k]);

@@ -44,10 +44,10 @@ constexpr int XOFF = 1;   // device padding columns before bnd_x1 (see common.cu
 
 // fields of a state set, in memory order (the *_e argument order)
 enum { S_U, S_UP, S_V, S_VP, S_SSH, S_SSHP, NSET };
-// fields of the static block: rest depth, mu, rdis, wflux (those the ring
-// holds: H alone in the uniform variant, all four in the general one),
-// then RHSx, RHSy (read directly where they are used)
-enum { T_H, T_MU, T_RD, T_WF, T_RX, T_RY, NSTAT };
+// fields of the static block: rest depth, RHSx, RHSy (the uniform
+// variant's ring holds these three), mu, rdis, wflux (the general variant's
+// holds all six)
+enum { T_H, T_RX, T_RY, T_MU, T_RD, T_WF, NSTAT };
 
 // per-row coefficients, row index = device row (n - bnd_y1); 38 doubles so
 // that a row is a whole number of 16-byte units for the bulk copies
@@ -91,7 +91,7 @@ struct Plan {
     double *stat = nullptr;         // static block, NSTAT fields
     long long fstride = 0;          // doubles between the fields of a block
     CUtensorMap tm_set[3];          // box {36, 1, 6} over each state set
-    CUtensorMap tm_stat[2];         // box {36, 1, 1 | 4} over the static block
+    CUtensorMap tm_stat[2];         // box {36, 1, 3 | 6} over the static block
     int occ[2] = {0, 0};            // resident CTAs per SM, per variant
     std::vector<uint8_t> ocean;     // per strip and interior row: any written column is ocean
     int rows_per_item[2] = {0, 0};  // 0: one wave of items by cost; else rows per item
@@ -107,6 +107,9 @@ struct Plan {
     float *stat32 = nullptr;        // RHSx, RHSy in FP32
     CUtensorMap tm_vel[3];          // box {40, 1, 4} FP32 over each velocity set
     CUtensorMap tm_ssh[3];          // box {36, 1, 2} over the SSH fields of each state set
+    CUtensorMap tm_stat_f32;        // box {36, 1, 1}: H alone, for the FP32-velocity ring
+    int stat_box[2] = {0, 0};       // static fields in tm_stat[v], checked against the ring layout
+    int stat_box_f32 = 0;
     double *d_uniform = nullptr;    // per-block min/max of mu, rdis, wflux
     unsigned *d_flags = nullptr;    // [0] status bits (guard / timeout)
     const float *lu = nullptr;      // borrowed
