@@ -338,7 +338,10 @@ def run_ours(args):
                          "bytes_per_cell_step": bpc,
                          "peak_kind": f"{peak_kind} HBM copy bandwidth"},
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
-            "gpu_launches": args.steps + 1, "path": path[1], "guard_bad_points": nbad,
+            # one fused kernel per step, one k_advance per replayed graph of
+            # 50 steps (runs of 100 steps or more), one k_minmax3 per run
+            "gpu_launches": args.steps + (args.steps // 50 if args.steps >= 100 and not args.fp32_velocity else 0) + 1,
+            "path": path[1], "guard_bad_points": nbad,
         }
         print(json.dumps(line), flush=True)
     if ws > 1:
