@@ -306,6 +306,65 @@ int inmsom_strips_create(inmsom_strips **strips, inmsom_ctx *const *ctxs, int n)
 int inmsom_strips_run(inmsom_strips *strips, int nsub, double dt, const double *rhs_scale, float *ms);
 int inmsom_strips_destroy(inmsom_strips *strips);
 
+/* Learned subgrid momentum closure (no counterpart in the reference; it
+ * stands in for the Laplacian viscosity of uv_diff2 on coarse grids): an
+ * MLP 45 -> 64 -> 64 -> 2 with GELU, BF16 weights and activations on the
+ * tensor cores, FP32 accumulate.  Buffers are the caller's device memory:
+ * params: INMSOM_MLP_NPARAM floats, W1[48][64] b1[64] W2[64][64] b2[64]
+ * W3[64][8] b3[8] (input rows 45..47 and output columns 2..7 zero);
+ * wbf16: INMSOM_MLP_NBF16 BF16 values, W1 W2 W3 in that layout; a sample is
+ * 48 BF16 features (the last 3 zero); targets 2 floats per sample.
+ * `stream` is a cudaStream_t (NULL: default stream); the calls only
+ * enqueue work. */
+#define INMSOM_MLP_NPARAM 7816
+#define INMSOM_MLP_NBF16 7680
+#define INMSOM_MLP_PARTIAL 7817   /* floats per 128-sample tile in `partial` */
+/* wbf16 := BF16(W1, W2, W3 of params) */
+int inmsom_mlp_pack(const float *params, void *wbf16, void *stream);
+/* y[n][0..1] = MLP(x[n]) for n < count */
+int inmsom_mlp_forward(const void *x, long long count, const float *params, const void *wbf16, float *y,
+                       void *stream);
+/* Gradient of the mean squared error over the samples idx[0..batch) (or
+ * 0..batch if idx is NULL), batch a multiple of 128: grad[0..NPARAM) and
+ * grad[NPARAM] = the loss; partial holds batch/128 * INMSOM_MLP_PARTIAL
+ * floats (per-tile sums, added in tile order: deterministic). */
+int inmsom_mlp_grad(const void *x, const float *targets, const int *idx, int batch, const float *params,
+                    const void *wbf16, float *partial, float *grad, void *stream);
+/* One bias-corrected Adam step (step >= 1) on params, then wbf16. */
+int inmsom_mlp_adam(float *params, void *wbf16, float *m, float *v, const float *grad, int step, float lr,
+                    float beta1, float beta2, float eps, void *stream);
+/* idx[i] uniform in [0, n), a function of (seed, step, i) only */
+int inmsom_mlp_batch_indices(int *idx, int batch, long long n, unsigned long long seed, int step, void *stream);
+
+/* The closure on a context's resident state (fused path, FP64 velocities).
+ * Features of cell (m, n): field f of (u, v, ssh, rest depth, rlh_s) at
+ * (m + dx, n + dy), dx, dy in -1..1, is feature 9 f + 3 (dy + 1) + (dx + 1),
+ * normalised as (x - mean[f]) * inv_std[f]; outputs y_u, y_v are velocity
+ * tendencies y * out_scale (m/s^2) at the u and v points of the cell. */
+typedef struct inmsom_closure_norm {
+    float mean[5];
+    float inv_std[5];
+    float out_scale[2];
+} inmsom_closure_norm;
+/* x (device, BF16): 48 features of every interior cell, cell (m, n) at row
+ * (n - ny_start) * nx + (m - nx_start); enqueued on the context's stream
+ * and waited for. */
+int inmsom_closure_features(inmsom_ctx *ctx, const inmsom_closure_norm *norm, void *x);
+/* nsub substeps as inmsom_run_substeps, the network re-evaluated on the
+ * state every `every` substeps (even, dividing nsub): the substeps that
+ * follow read RHSx + y_u * out_scale[0] * hu * dxt * dyh at the ocean u
+ * points (RHSy likewise at the v points), i.e. the tendency is added to the
+ * momentum equation; the registered RHSx, RHSy are not changed.  params and
+ * wbf16 are device buffers as for inmsom_mlp_*.  Replayed as CUDA graphs.
+ * INMSOM_EUNSUPPORTED without the fused path or with FP32 velocities. */
+int inmsom_run_closure(inmsom_ctx *ctx, int nsub, double dt, int every, const float *params, const void *wbf16,
+                       const inmsom_closure_norm *norm, float *ms);
+/* The RHS increment the closure adds on the resident state (host arrays
+ * in the registered layout): y_u * out_scale[0] * hu * dxt * dyh at the
+ * ocean u points, likewise at the v points, 0 elsewhere. */
+int inmsom_closure_tendency(inmsom_ctx *ctx, const float *params, const void *wbf16,
+                            const inmsom_closure_norm *norm, double *rhsx, double *rhsy);
+
 int inmsom_gpu_finalize(inmsom_ctx *ctx);
 const char *inmsom_gpu_last_error(void);
 

@@ -25,7 +25,12 @@ EXPORTS = (
     "inmsom_gpu_path", "inmsom_gpu_finalize", "inmsom_gpu_last_error", "inmsom_load_state",
     "inmsom_diag_noalloc", "inmsom_ens_create", "inmsom_ens_run", "inmsom_ens_tune",
     "inmsom_ens_destroy", "inmsom_strips_create", "inmsom_strips_run", "inmsom_strips_destroy",
+    "inmsom_mlp_pack", "inmsom_mlp_forward", "inmsom_mlp_grad", "inmsom_mlp_adam", "inmsom_mlp_batch_indices",
+    "inmsom_closure_features", "inmsom_run_closure", "inmsom_closure_tendency",
 )
+
+# include/inmsom_gpu.h: INMSOM_MLP_*
+MLP_NPARAM, MLP_NBF16, MLP_PARTIAL = 7816, 7680, 7817
 
 # include/inmsom_gpu.h: INMSOM_DIAG_NOALLOC_MAX_ROWS
 DIAG_NOALLOC_MAX_ROWS = 16384
@@ -41,6 +46,12 @@ class CBounds(ctypes.Structure):
     _fields_ = [(n, ctypes.c_int) for n in (
         "nx_start", "nx_end", "ny_start", "ny_end", "bnd_x1", "bnd_x2", "bnd_y1", "bnd_y2",
         "mmm", "mm", "nnn", "nn", "periodicity_x", "periodicity_y")]
+
+
+class CClosureNorm(ctypes.Structure):
+    """inmsom_closure_norm"""
+    _fields_ = [("mean", ctypes.c_float * 5), ("inv_std", ctypes.c_float * 5),
+                ("out_scale", ctypes.c_float * 2)]
 
 
 class CConsts(ctypes.Structure):
@@ -90,6 +101,18 @@ def load() -> ctypes.CDLL:
     lib.inmsom_strips_create.argtypes = [ctypes.POINTER(VP), ctypes.POINTER(VP), i]
     lib.inmsom_strips_run.argtypes = [VP, i, d, DP, ctypes.POINTER(ctypes.c_float)]
     lib.inmsom_strips_destroy.argtypes = [VP]
+    F = ctypes.POINTER(ctypes.c_float)
+    IP = ctypes.POINTER(ctypes.c_int)
+    lib.inmsom_mlp_pack.argtypes = [VP, VP, VP]
+    lib.inmsom_mlp_forward.argtypes = [VP, ctypes.c_longlong, VP, VP, VP, VP]
+    lib.inmsom_mlp_grad.argtypes = [VP, VP, VP, i, VP, VP, VP, VP, VP]
+    lib.inmsom_mlp_adam.argtypes = [VP, VP, VP, VP, VP, i, ctypes.c_float, ctypes.c_float, ctypes.c_float,
+                                    ctypes.c_float, VP]
+    lib.inmsom_mlp_batch_indices.argtypes = [VP, i, ctypes.c_longlong, ctypes.c_ulonglong, i, VP]
+    NP = ctypes.POINTER(CClosureNorm)
+    lib.inmsom_closure_features.argtypes = [VP, NP, VP]
+    lib.inmsom_run_closure.argtypes = [VP, i, d, i, VP, VP, NP, ctypes.POINTER(ctypes.c_float)]
+    lib.inmsom_closure_tendency.argtypes = [VP, VP, VP, NP, DP, DP]
     lib.inmsom_diag_noalloc.argtypes = ([ctypes.POINTER(CBounds), ctypes.POINTER(CConsts),
                                          ctypes.c_longlong] + [VP] * 16 + [VP])
     for name in EXPORTS:

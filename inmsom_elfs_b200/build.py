@@ -26,6 +26,7 @@ SOURCES = {
     "fused.cu": [],
     "capi.cu": [],
     "noalloc.cu": [],
+    "closure.cu": [],
 }
 HEADERS = ["common.cuh", "general.h", "fused.h"]
 

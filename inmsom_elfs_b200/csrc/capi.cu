@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "closure.h"
 #include "fused.h"
 #include "general.h"
 
@@ -112,6 +113,14 @@ struct inmsom_ctx {
     double *d_rs = nullptr;          // RHS scale per substep of the run
     size_t rs_cap = 0;
     int *d_base = nullptr;           // first substep of the next replay
+    // inmsom_run_closure: per-point tendency factors and the replayed graph
+    double *cl_fac[2] = {};
+    double *cl_tmp[3] = {};          // inmsom_closure_tendency: out u, out v, zero base
+    cudaGraphExec_t cl_exec = nullptr;
+    closure::Args cl_args{};         // the arguments the graph was captured with
+    unsigned cl_gen = 0;
+    double cl_dt = 0.0;
+    int cl_every = 0, cl_groups = 0;
     bool fused_ok = false;
     const char *fused_reason = "grid not registered";
 
@@ -375,11 +384,15 @@ int inmsom_gpu_finalize(inmsom_ctx *c)
     if (c->rs_exec) cudaGraphExecDestroy(c->rs_exec);
     cudaFree(c->d_rs);
     cudaFree(c->d_base);
+    if (c->cl_exec) cudaGraphExecDestroy(c->cl_exec);
+    cudaFree(c->cl_fac[0]);   // one block with cl_fac[1]
+    cudaFree(c->cl_tmp[0]);   // one block
     fused::free_plan(c->plan);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
+    cudaGetLastError();   // nothing from the teardown reaches the next call
     return INMSOM_OK;
 }
 
@@ -659,6 +672,169 @@ int inmsom_run_substeps(inmsom_ctx *c, int nsub, double dt, const double *rhs_sc
     CK(cudaEventRecord(c->ev1, c->stream));
     CKR(sync_stream(c));
     if (ms) CK(cudaEventElapsedTime(ms, c->ev0, c->ev1));
+    if (c->flags & INMSOM_GUARD) {
+        long nbad = 0;
+        CKR(run_guard(c, &nbad));
+        if (nbad) return set_err(INMSOM_EGUARD, "guard: %ld interior points out of range or NaN", nbad);
+    }
+    return INMSOM_OK;
+}
+
+// ===================================================================== closure
+namespace {
+
+// the closure arguments of a context (fields of the resident state)
+int closure_args(inmsom_ctx *c, const inmsom_closure_norm *norm, closure::Args &a)
+{
+    std::memset(&a, 0, sizeof a);
+    const Dom &d = c->dom;
+    a.fld[0] = c->state[S_U];
+    a.fld[1] = c->state[S_V];
+    a.fld[2] = c->state[S_SSH];
+    a.fld[3] = c->met[G_HREST];
+    a.fld[4] = c->met[G_RLH];
+    for (int k = 0; k < 5; k++) {
+        if (!a.fld[k]) return set_err(INMSOM_EARG, "closure: grid or state not on the device");
+        a.mean[k] = norm->mean[k];
+        a.inv_std[k] = norm->inv_std[k];
+    }
+    a.out_scale[0] = norm->out_scale[0];
+    a.out_scale[1] = norm->out_scale[1];
+    a.pitch = d.pitch;
+    a.x1 = d.bnd_x1; a.x2 = d.bnd_x2; a.y1 = d.bnd_y1; a.y2 = d.bnd_y2; a.xoff = d.xoff;
+    a.mx0 = d.nx_start; a.mx1 = d.nx_end; a.ny0 = d.ny_start; a.ny1 = d.ny_end;
+    return INMSOM_OK;
+}
+
+int closure_factors(inmsom_ctx *c, closure::Args &a)
+{
+    if (!c->cl_fac[0]) {
+        double *f[2] = {};
+        CKR(alloc_block(c, f, 2));
+        c->cl_fac[0] = f[0];
+        c->cl_fac[1] = f[1];
+        if (closure::factors(a, c->mask[M_LCU], c->mask[M_LCV], c->met[G_DXT], c->met[G_DYH], c->met[G_DYT],
+                             c->met[G_DXH], c->cl_fac[0], c->cl_fac[1], c->stream))
+            return INMSOM_ECUDA;
+    }
+    a.fac[0] = c->cl_fac[0];
+    a.fac[1] = c->cl_fac[1];
+    return INMSOM_OK;
+}
+
+// one group: the network on the state, then `every` substeps
+int closure_group(inmsom_ctx *c, const closure::Args &a, double dt, int every)
+{
+    if (closure::apply(a, c->plan.nsm, c->stream)) return INMSOM_ECUDA;
+    if (fused::launch_steps(c->plan, c->dom, c->c, dt, every, nullptr, nullptr, c->state, c->stream))
+        return set_err(INMSOM_ECUDA, "closure: substep launch failed");
+    return INMSOM_OK;
+}
+
+}  // namespace
+
+int inmsom_closure_features(inmsom_ctx *c, const inmsom_closure_norm *norm, void *x)
+{
+    CKR(ensure_grid(c));
+    if (!norm || !x) return set_err(INMSOM_EARG, "inmsom_closure_features: NULL argument");
+    if (!c->state_on_device)
+        return set_err(INMSOM_EARG, "no resident state: call inmsom_load_state first");
+    closure::Args a;
+    CKR(closure_args(c, norm, a));
+    a.feat = x;
+    if (closure::features(a, c->plan.nsm, c->stream)) return INMSOM_ECUDA;
+    return sync_stream(c);
+}
+
+int inmsom_closure_tendency(inmsom_ctx *c, const float *params, const void *wbf16, const inmsom_closure_norm *norm,
+                            double *rhsx, double *rhsy)
+{
+    CKR(ensure_grid(c));
+    if (!params || !wbf16 || !norm || !rhsx || !rhsy)
+        return set_err(INMSOM_EARG, "inmsom_closure_tendency: NULL argument");
+    if (!c->state_on_device)
+        return set_err(INMSOM_EARG, "no resident state: call inmsom_load_state first");
+    closure::Args a;
+    CKR(closure_args(c, norm, a));
+    CKR(closure_factors(c, a));
+    CKR(alloc_block(c, c->cl_tmp, 3));   // zeroed once; field 2 stays zero
+    CK(cudaMemsetAsync(c->cl_tmp[0], 0, 2 * c->plan.fstride * sizeof(double), c->stream));
+    a.base[0] = a.base[1] = c->cl_tmp[2];
+    a.out[0] = c->cl_tmp[0];
+    a.out[1] = c->cl_tmp[1];
+    a.prm = params;
+    a.wb = wbf16;
+    if (closure::apply(a, c->plan.nsm, c->stream)) return INMSOM_ECUDA;
+    CKR(d2h(c, rhsx, c->cl_tmp[0]));
+    CKR(d2h(c, rhsy, c->cl_tmp[1]));
+    return sync_stream(c);
+}
+
+int inmsom_run_closure(inmsom_ctx *c, int nsub, double dt, int every, const float *params, const void *wbf16,
+                       const inmsom_closure_norm *norm, float *ms)
+{
+    CKR(ensure_grid(c));
+    if (!params || !wbf16 || !norm) return set_err(INMSOM_EARG, "inmsom_run_closure: NULL argument");
+    if (every < 2 || every % 2 || nsub < 0 || nsub % every)
+        return set_err(INMSOM_EARG, "inmsom_run_closure: every must be even and divide nsub");
+    if (!(dt > 0.0)) return set_err(INMSOM_EARG, "dt must be > 0");
+    if (!c->state_on_device)
+        return set_err(INMSOM_EARG, "no resident state: call inmsom_load_state or barotropic_dynamics first");
+    if (!c->fused_ok) return set_err(INMSOM_EUNSUPPORTED, "the closure needs the fused path (%s)", c->fused_reason);
+    if (c->flags & INMSOM_FP32_VELOCITY)
+        return set_err(INMSOM_EUNSUPPORTED, "the closure runs with FP64 velocities");
+    closure::Args a;
+    CKR(closure_args(c, norm, a));
+    CKR(closure_factors(c, a));
+    fused::Plan &p = c->plan;
+    a.base[0] = c->forc[F_RHSX];
+    a.base[1] = c->forc[F_RHSY];
+    a.out[0] = p.stat + fused::T_RX * p.fstride;
+    a.out[1] = p.stat + fused::T_RY * p.fstride;
+    a.prm = params;
+    a.wb = wbf16;
+    CK(cudaEventRecord(c->ev0, c->stream));
+    // stages RHSx, RHSy into the static block (the closure then overwrites
+    // its ocean u/v points every group) and classifies the forcing
+    if (fused::prepare_steps(p, c->dom, c->c, c->state, c->forc, c->stream))
+        return set_err(INMSOM_ECUDA, "closure: prepare failed: %s", cudaGetErrorString(cudaGetLastError()));
+    const int ngroups = nsub / every;
+    const int per_graph = every >= RS_GROUP ? 1 : RS_GROUP / every;
+    if (ngroups >= 2 * per_graph) {
+        if (!c->cl_exec || c->cl_gen != p.generation || c->cl_dt != dt || c->cl_every != every ||
+            c->cl_groups != per_graph || std::memcmp(&c->cl_args, &a, sizeof a) != 0) {
+            if (c->cl_exec) cudaGraphExecDestroy(c->cl_exec);
+            c->cl_exec = nullptr;
+            cudaGraph_t g = nullptr;
+            CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+            int rc = INMSOM_OK;
+            for (int k = 0; k < per_graph && rc == INMSOM_OK; k++) rc = closure_group(c, a, dt, every);
+            const cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+            if (rc || ce != cudaSuccess) {
+                if (g) cudaGraphDestroy(g);
+                return set_err(INMSOM_ECUDA, "closure: graph capture failed: %s", cudaGetErrorString(ce));
+            }
+            const cudaError_t ie = cudaGraphInstantiate(&c->cl_exec, g, 0);
+            cudaGraphDestroy(g);
+            if (ie != cudaSuccess) return set_err(INMSOM_ECUDA, "closure: %s", cudaGetErrorString(ie));
+            c->cl_gen = p.generation;
+            c->cl_dt = dt;
+            c->cl_every = every;
+            c->cl_groups = per_graph;
+            c->cl_args = a;
+        }
+        for (int k = 0; k < ngroups / per_graph; k++) CK(cudaGraphLaunch(c->cl_exec, c->stream));
+        for (int k = 0; k < ngroups % per_graph; k++) CKR(closure_group(c, a, dt, every));
+    } else {
+        for (int k = 0; k < ngroups; k++) CKR(closure_group(c, a, dt, every));
+    }
+    if (fused::finish_steps(p, c->stream))
+        return set_err(INMSOM_ECUDA, "closure: %s", cudaGetErrorString(cudaGetLastError()));
+    c->depths_current = false;
+    CK(cudaEventRecord(c->ev1, c->stream));
+    CKR(sync_stream(c));
+    if (ms) CK(cudaEventElapsedTime(ms, c->ev0, c->ev1));
+    if (p.last_flags & fused::FLAG_TIMEOUT) return set_err(INMSOM_ETIMEOUT, "fused kernel: a bounded TMA wait timed out");
     if (c->flags & INMSOM_GUARD) {
         long nbad = 0;
         CKR(run_guard(c, &nbad));

@@ -1,0 +1,658 @@
+// Learned subgrid momentum closure: a 45 -> 64 -> 64 -> 2 MLP with GELU,
+// BF16 weights and activations on the tensor cores (mma.sync m16n8k16,
+// FP32 accumulate), FP32 master weights and Adam.  No counterpart in the
+// reference: it stands in for the Laplacian viscosity of uv_diff2
+// (Function/vel_ssh.f90:117-184) on coarse grids.
+//
+// Parameter block (FP32, flat): W1[48][64] b1[64] W2[64][64] b2[64]
+// W3[64][8] b3[8]; rows 45..47 of W1 (padded inputs) and columns 2..7 of
+// W3 and b3 (padded outputs) stay zero.  The BF16 copy holds W1, W2, W3 in
+// the same layout.  A sample is 48 BF16 features (45 used).
+#include "inmsom_gpu.h"
+#include "closure.h"
+
+#include <cuda_bf16.h>
+
+#include <cstdint>
+#include <cstdio>
+
+namespace inmsom {
+int record_error(int code, const char *msg);
+}
+
+namespace {
+
+constexpr int KIN = 48, HID = 64, NOUT = 2, N3 = 8;
+constexpr int OFF_W1 = 0, OFF_B1 = OFF_W1 + KIN * HID, OFF_W2 = OFF_B1 + HID, OFF_B2 = OFF_W2 + HID * HID,
+              OFF_W3 = OFF_B2 + HID, OFF_B3 = OFF_W3 + HID * N3, NPARAM = OFF_B3 + N3;
+constexpr int BOFF_W1 = 0, BOFF_W2 = KIN * HID, BOFF_W3 = BOFF_W2 + HID * HID, NBF = BOFF_W3 + HID * N3;
+static_assert(NPARAM == INMSOM_MLP_NPARAM, "parameter block size");
+constexpr int TILE = 128;     // samples per CTA
+constexpr int WARPS = 8;      // 16 samples per warp in the row-parallel GEMMs
+constexpr int NPART = NPARAM + 1;   // per-CTA partial gradient + loss
+
+// ---------------------------------------------------------------- helpers
+__device__ __forceinline__ uint32_t pack_raw(__nv_bfloat16 lo, __nv_bfloat16 hi)
+{
+    const uint32_t a = *reinterpret_cast<const uint16_t *>(&lo), b = *reinterpret_cast<const uint16_t *>(&hi);
+    return a | (b << 16);
+}
+
+// C[16x8] += A[16x16] * B[16x8], BF16 inputs, FP32 accumulate
+__device__ __forceinline__ void mma16816(float c[4], const uint32_t a[4], const uint32_t b[2])
+{
+    asm volatile(
+        "mma.sync.aligned.m16n8k16.row.col.f32.bf16.bf16.f32 {%0,%1,%2,%3}, {%4,%5,%6,%7}, {%8,%9}, "
+        "{%0,%1,%2,%3};"
+        : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
+        : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
+}
+
+// Fragments of mma.m16n8k16 for lane (g = lane/4, t = lane%4):
+//   A: a0 = A[g][2t,2t+1]  a1 = A[g+8][2t,2t+1]  a2 = A[g][2t+8,2t+9]  a3 = A[g+8][2t+8,2t+9]
+//   B: b0 = B[2t,2t+1][g]  b1 = B[2t+8,2t+9][g]
+//   C: c0 = C[g][2t] c1 = C[g][2t+1] c2 = C[g+8][2t] c3 = C[g+8][2t+1]
+// A(r, k) and B(k, n) are element accessors (BF16).
+template <class FA>
+__device__ __forceinline__ void frag_a(uint32_t a[4], FA A, int m0, int k0)
+{
+    const int l = threadIdx.x & 31, g = l >> 2, t = l & 3;
+    a[0] = pack_raw(A(m0 + g, k0 + 2 * t), A(m0 + g, k0 + 2 * t + 1));
+    a[1] = pack_raw(A(m0 + g + 8, k0 + 2 * t), A(m0 + g + 8, k0 + 2 * t + 1));
+    a[2] = pack_raw(A(m0 + g, k0 + 2 * t + 8), A(m0 + g, k0 + 2 * t + 9));
+    a[3] = pack_raw(A(m0 + g + 8, k0 + 2 * t + 8), A(m0 + g + 8, k0 + 2 * t + 9));
+}
+template <class FB>
+__device__ __forceinline__ void frag_b(uint32_t b[2], FB B, int k0, int n0)
+{
+    const int l = threadIdx.x & 31, g = l >> 2, t = l & 3;
+    b[0] = pack_raw(B(k0 + 2 * t, n0 + g), B(k0 + 2 * t + 1, n0 + g));
+    b[1] = pack_raw(B(k0 + 2 * t + 8, n0 + g), B(k0 + 2 * t + 9, n0 + g));
+}
+// C tile [m0, m0+16) x [n0, n0+8) = sum over K of A * B, handed to out(r, n, value)
+template <class FA, class FB, class FO>
+__device__ __forceinline__ void gemm_tile(FA A, FB B, int K, int m0, int n0, FO out)
+{
+    float c[4] = {0.f, 0.f, 0.f, 0.f};
+    for (int k0 = 0; k0 < K; k0 += 16) {
+        uint32_t a[4], b[2];
+        frag_a(a, A, m0, k0);
+        frag_b(b, B, k0, n0);
+        mma16816(c, a, b);
+    }
+    const int l = threadIdx.x & 31, g = l >> 2, t = l & 3;
+    out(m0 + g, n0 + 2 * t, c[0]);
+    out(m0 + g, n0 + 2 * t + 1, c[1]);
+    out(m0 + g + 8, n0 + 2 * t, c[2]);
+    out(m0 + g + 8, n0 + 2 * t + 1, c[3]);
+}
+
+// GELU in the tanh form of Hendrycks & Gimpel (2016),
+// 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))), with the hardware tanh
+// (tanh.approx.f32, relative error about 2^-11: below the BF16 rounding of
+// the activations); training and inference use this one definition.
+constexpr float GC0 = 0.7978845608028654f, GC1 = 0.7978845608028654f * 0.044715f;
+__device__ __forceinline__ float tanh_hw(float x)
+{
+    float y;
+    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
+    return y;
+}
+__device__ __forceinline__ float gelu(float x)
+{
+    const float h = 0.5f * x;
+    return fmaf(h, tanh_hw(x * fmaf(GC1, x * x, GC0)), h);
+}
+__device__ __forceinline__ float gelu_d(float x)
+{
+    const float x2 = x * x, t = tanh_hw(x * fmaf(GC1, x2, GC0));
+    return fmaf(0.5f, 1.0f + t, 0.5f * x * (1.0f - t * t) * fmaf(3.0f * GC1, x2, GC0));
+}
+
+// shared memory of one 128-sample tile
+struct Smem {
+    __nv_bfloat16 x[TILE][KIN];      // inputs
+    float z1[TILE][HID];             // pre-activations, then their gradients
+    __nv_bfloat16 a1[TILE][HID];     // GELU(z1)
+    float z2[TILE][HID];
+    __nv_bfloat16 a2[TILE][HID];
+    float z3[TILE][N3];              // outputs, then their gradients
+    __nv_bfloat16 d3[TILE][16];      // output gradients (K padded to 16)
+    __nv_bfloat16 d2[TILE][HID];     // gradients of z2
+    __nv_bfloat16 d1[TILE][HID];     // gradients of z1
+    __nv_bfloat16 w1[KIN][HID], w2[HID][HID], w3[HID][16];   // W3 columns padded to 16
+    float b1[HID], b2[HID], b3[N3];
+};
+
+__device__ void load_weights(Smem &s, const float *prm, const __nv_bfloat16 *wb)
+{
+    for (int i = threadIdx.x; i < KIN * HID; i += blockDim.x) s.w1[i / HID][i % HID] = wb[BOFF_W1 + i];
+    for (int i = threadIdx.x; i < HID * HID; i += blockDim.x) s.w2[i / HID][i % HID] = wb[BOFF_W2 + i];
+    for (int i = threadIdx.x; i < HID * 16; i += blockDim.x) {
+        const int r = i / 16, c = i % 16;
+        s.w3[r][c] = c < N3 ? wb[BOFF_W3 + r * N3 + c] : __float2bfloat16(0.f);
+    }
+    for (int i = threadIdx.x; i < HID; i += blockDim.x) {
+        s.b1[i] = prm[OFF_B1 + i];
+        s.b2[i] = prm[OFF_B2 + i];
+    }
+    for (int i = threadIdx.x; i < N3; i += blockDim.x) s.b3[i] = prm[OFF_B3 + i];
+}
+
+// forward pass of the tile in shared memory (x already loaded); z3 holds
+// the outputs (bias included)
+__device__ void forward(Smem &s)
+{
+    const int w = threadIdx.x >> 5;
+    const int m0 = 16 * w;
+    // layer 1: z1 = x W1 + b1, a1 = GELU(z1)
+    for (int n0 = 0; n0 < HID; n0 += 8)
+        gemm_tile([&](int r, int k) { return s.x[r][k]; }, [&](int k, int n) { return s.w1[k][n]; }, KIN, m0, n0,
+                  [&](int r, int n, float v) {
+                      const float z = v + s.b1[n];
+                      s.z1[r][n] = z;
+                      s.a1[r][n] = __float2bfloat16(gelu(z));
+                  });
+    __syncwarp();
+    for (int n0 = 0; n0 < HID; n0 += 8)
+        gemm_tile([&](int r, int k) { return s.a1[r][k]; }, [&](int k, int n) { return s.w2[k][n]; }, HID, m0, n0,
+                  [&](int r, int n, float v) {
+                      const float z = v + s.b2[n];
+                      s.z2[r][n] = z;
+                      s.a2[r][n] = __float2bfloat16(gelu(z));
+                  });
+    __syncwarp();
+    gemm_tile([&](int r, int k) { return s.a2[r][k]; }, [&](int k, int n) { return s.w3[k][n]; }, HID, m0, 0,
+              [&](int r, int n, float v) { s.z3[r][n] = v + s.b3[n]; });
+    __syncthreads();
+}
+
+// One tile of the mean-squared-error loss over `batch` samples and its
+// gradient: partial[cta][0..NPARAM) += d loss / d params, partial[cta][NPARAM]
+// = the tile's loss sum.
+__global__ void __launch_bounds__(WARPS * 32, 1) k_mlp_grad(const __nv_bfloat16 *x, const float *tgt, const int *idx,
+                                                            int batch, const float *prm, const __nv_bfloat16 *wb,
+                                                            float *partial)
+{
+    extern __shared__ __align__(16) unsigned char raw[];
+    Smem &s = *reinterpret_cast<Smem *>(raw);
+    const int tile0 = blockIdx.x * TILE;
+    load_weights(s, prm, wb);
+    for (int i = threadIdx.x; i < TILE * KIN; i += blockDim.x) {
+        const int r = i / KIN, k = i % KIN;
+        const long long row = idx ? idx[tile0 + r] : tile0 + r;
+        s.x[r][k] = x[row * KIN + k];
+    }
+    __syncthreads();
+    forward(s);
+    // loss and output gradient: d/dy of sum (y - t)^2 / (batch * NOUT)
+    __shared__ float lsum[TILE];
+    const float scale = 2.0f / ((float)batch * NOUT);
+    for (int r = threadIdx.x; r < TILE; r += blockDim.x) {
+        const long long row = idx ? idx[tile0 + r] : tile0 + r;
+        float l = 0.f;
+        for (int j = 0; j < 16; j++) {
+            float d = 0.f;
+            if (j < NOUT) {
+                const float e = s.z3[r][j] - tgt[row * NOUT + j];
+                l += e * e;
+                d = scale * e;
+            }
+            if (j < N3) s.z3[r][j] = d;
+            s.d3[r][j] = __float2bfloat16(d);
+        }
+        lsum[r] = l;
+    }
+    __syncthreads();
+    const int w = threadIdx.x >> 5;
+    float *pg = partial + (size_t)blockIdx.x * NPART;
+    // dW3 = a2^T d3   [64 x 8]: warps 0..3 one m-tile each
+    if (w < 4)
+        gemm_tile([&](int r, int k) { return s.a2[k][r]; }, [&](int k, int n) { return s.d3[k][n]; }, TILE, 16 * w, 0,
+                  [&](int r, int n, float v) { pg[OFF_W3 + r * N3 + n] = v; });
+    // d(a2) = d3 W3^T, d(z2) = d(a2) * GELU'(z2)
+    for (int n0 = 0; n0 < HID; n0 += 8)
+        gemm_tile([&](int r, int k) { return s.d3[r][k]; }, [&](int k, int n) { return s.w3[n][k]; }, 16, 16 * w,
+                  n0, [&](int r, int n, float v) {
+                      const float d = v * gelu_d(s.z2[r][n]);
+                      s.d2[r][n] = __float2bfloat16(d);
+                      s.z2[r][n] = d;
+                  });
+    __syncthreads();
+    // dW2 = a1^T d2   [64 x 64]: 4 m-tiles x 8 n-tiles, 4 per warp
+    for (int t = w; t < 32; t += WARPS)
+        gemm_tile([&](int r, int k) { return s.a1[k][r]; }, [&](int k, int n) { return s.d2[k][n]; }, TILE,
+                  16 * (t >> 3), 8 * (t & 7), [&](int r, int n, float v) { pg[OFF_W2 + r * HID + n] = v; });
+    // d(a1) = d2 W2^T, d(z1) = d(a1) * GELU'(z1)
+    for (int n0 = 0; n0 < HID; n0 += 8)
+        gemm_tile([&](int r, int k) { return s.d2[r][k]; }, [&](int k, int n) { return s.w2[n][k]; }, HID, 16 * w,
+                  n0, [&](int r, int n, float v) {
+                      const float d = v * gelu_d(s.z1[r][n]);
+                      s.d1[r][n] = __float2bfloat16(d);
+                      s.z1[r][n] = d;
+                  });
+    __syncthreads();
+    // dW1 = x^T d1   [48 x 64]: 3 m-tiles x 8 n-tiles, 3 per warp
+    for (int t = w; t < 24; t += WARPS)
+        gemm_tile([&](int r, int k) { return s.x[k][r]; }, [&](int k, int n) { return s.d1[k][n]; }, TILE,
+                  16 * (t >> 3), 8 * (t & 7), [&](int r, int n, float v) { pg[OFF_W1 + r * HID + n] = v; });
+    // bias gradients: column sums of the FP32 gradients, and the loss
+    for (int n = threadIdx.x; n < HID; n += blockDim.x) {
+        float a = 0.f, b = 0.f;
+        for (int r = 0; r < TILE; r++) {
+            a += s.z1[r][n];
+            b += s.z2[r][n];
+        }
+        pg[OFF_B1 + n] = a;
+        pg[OFF_B2 + n] = b;
+    }
+    for (int n = threadIdx.x; n < N3; n += blockDim.x) {
+        float a = 0.f;
+        for (int r = 0; r < TILE; r++) a += s.z3[r][n];
+        pg[OFF_B3 + n] = a;
+    }
+    if (threadIdx.x == 0) {
+        float a = 0.f;
+        for (int r = 0; r < TILE; r++) a += lsum[r];
+        pg[NPARAM] = a;
+    }
+}
+
+// grad[p] = sum over tiles of partial[t][p] in tile order (deterministic);
+// grad[NPARAM] = mean squared error
+__global__ void k_mlp_reduce(const float *partial, int ntiles, int batch, float *grad)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p > NPARAM) return;
+    float a = 0.f;
+    for (int t = 0; t < ntiles; t++) a += partial[(size_t)t * NPART + p];
+    grad[p] = p == NPARAM ? a / ((float)batch * NOUT) : a;
+}
+
+// Adam (Kingma & Ba), bias-corrected, then the BF16 weight copy
+__global__ void k_mlp_adam(float *prm, __nv_bfloat16 *wb, float *m, float *v, const float *grad, int step,
+                           float lr, float b1, float b2, float eps)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= NPARAM) return;
+    const bool pad = (p >= OFF_W1 + 45 * HID && p < OFF_B1) || (p >= OFF_W3 && p < OFF_B3 && (p - OFF_W3) % N3 >= NOUT) ||
+                     (p >= OFF_B3 + NOUT);
+    float w = prm[p];
+    if (!pad) {
+        const float g = grad[p];
+        const float mm = b1 * m[p] + (1.f - b1) * g, vv = b2 * v[p] + (1.f - b2) * g * g;
+        m[p] = mm;
+        v[p] = vv;
+        const float mh = mm / (1.f - powf(b1, (float)step)), vh = vv / (1.f - powf(b2, (float)step));
+        w -= lr * mh / (sqrtf(vh) + eps);
+        prm[p] = w;
+    }
+    int bi = -1;
+    if (p < OFF_B1) bi = BOFF_W1 + p;
+    else if (p >= OFF_W2 && p < OFF_B2) bi = BOFF_W2 + (p - OFF_W2);
+    else if (p >= OFF_W3 && p < OFF_B3) bi = BOFF_W3 + (p - OFF_W3);
+    if (bi >= 0) wb[bi] = __float2bfloat16(w);
+}
+
+__global__ void k_mlp_pack(const float *prm, __nv_bfloat16 *wb)
+{
+    const int p = blockIdx.x * blockDim.x + threadIdx.x;
+    if (p < KIN * HID) wb[BOFF_W1 + p] = __float2bfloat16(prm[OFF_W1 + p]);
+    else if (p < KIN * HID + HID * HID) wb[BOFF_W2 + p - KIN * HID] = __float2bfloat16(prm[OFF_W2 + p - KIN * HID]);
+    else if (p < NBF) wb[BOFF_W3 + p - KIN * HID - HID * HID] = __float2bfloat16(prm[OFF_W3 + p - KIN * HID - HID * HID]);
+}
+
+// y[n][0..1] = MLP(x[n]) for n < count (tiles of 128, the last one partial)
+__global__ void __launch_bounds__(WARPS * 32, 1) k_mlp_forward(const __nv_bfloat16 *x, long long count, const float *prm,
+                                                               const __nv_bfloat16 *wb, float *y)
+{
+    extern __shared__ __align__(16) unsigned char raw[];
+    Smem &s = *reinterpret_cast<Smem *>(raw);
+    const long long tile0 = (long long)blockIdx.x * TILE;
+    load_weights(s, prm, wb);
+    for (int i = threadIdx.x; i < TILE * KIN; i += blockDim.x) {
+        const int r = i / KIN, k = i % KIN;
+        s.x[r][k] = tile0 + r < count ? x[(tile0 + r) * KIN + k] : __float2bfloat16(0.f);
+    }
+    __syncthreads();
+    forward(s);
+    for (int i = threadIdx.x; i < TILE * NOUT; i += blockDim.x) {
+        const int r = i / NOUT, j = i % NOUT;
+        if (tile0 + r < count) y[(tile0 + r) * NOUT + j] = s.z3[r][j];
+    }
+}
+
+// splitmix64 of (seed, step, i): uniform sample indices in [0, n)
+__global__ void k_batch_indices(int *idx, int batch, long long n, unsigned long long seed, int step)
+{
+    const int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= batch) return;
+    unsigned long long z = seed + 0x9E3779B97F4A7C15ull * ((unsigned long long)step * 0x100000001ull + i + 1);
+    z = (z ^ (z >> 30)) * 0xBF58476D1CE4E5B9ull;
+    z = (z ^ (z >> 27)) * 0x94D049BB133111EBull;
+    z ^= z >> 31;
+    idx[i] = (int)(z % (unsigned long long)n);
+}
+
+
+// ============================================================ inference
+// Features of cell (m, n): 5 fields x the 3 x 3 stencil around it, feature
+// k = 9 f + 3 (dy + 1) + (dx + 1) for field f (u, v, ssh, H, rlh_s) at
+// (m + dx, n + dy), normalised (x - mean_f) * inv_std_f and rounded to BF16;
+// features 45..47 are zero.  A CTA stages a tile of TCOLS x TROWS cells plus
+// a one-cell ring of the five fields in shared memory; each warp then runs
+// the network on 16-cell row segments, the activations of one layer going
+// to the next as MMA fragments in registers.
+constexpr int TCOLS = 64, TROWS = 8, FW = TCOLS + 2, FH = TROWS + 2, NFLD = 5, NTILE = NFLD * FH * FW;
+constexpr int W1S = KIN + 8, W2S = HID + 8;   // padded rows: conflict-free B fragment loads
+static_assert(TROWS == WARPS, "one tile row per warp");
+
+struct ClSmem {
+    __nv_bfloat16 w1t[HID][W1S];   // W1 transposed, [n][k]
+    __nv_bfloat16 w2t[HID][W2S];
+    __nv_bfloat16 w3t[N3][W2S];
+    float b1[HID], b2[HID], b3[N3];
+    __nv_bfloat16 tile[NTILE];
+    float y[WARPS][16][2];
+};
+
+__device__ __forceinline__ int feat_off(int k)   // tile offset of feature k, cell at ring (0, 0)
+{
+    const int f = k / 9, q = k % 9;
+    return f * FH * FW + (q / 3) * FW + (q % 3);
+}
+
+__device__ void stage_tile(__nv_bfloat16 *tile, const inmsom::closure::Args &a, int m0, int n0)
+{
+    for (int i = threadIdx.x; i < NTILE; i += blockDim.x) {
+        const int f = i / (FH * FW), rem = i - f * (FH * FW), r = rem / FW, cidx = rem - r * FW;
+        const int m = m0 - 1 + cidx, n = n0 - 1 + r;
+        float v = 0.f;
+        if (m >= a.x1 && m <= a.x2 && n >= a.y1 && n <= a.y2)
+            v = (float)a.fld[f][(long long)(n - a.y1) * a.pitch + (m - a.x1 + a.xoff)];
+        tile[i] = __float2bfloat16((v - a.mean[f]) * a.inv_std[f]);
+    }
+}
+
+__device__ __forceinline__ uint32_t lds32(const __nv_bfloat16 *p) { return *reinterpret_cast<const uint32_t *>(p); }
+__device__ __forceinline__ uint32_t pack2(float lo, float hi)
+{
+    const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
+    return *reinterpret_cast<const uint32_t *>(&v);
+}
+
+// y (outputs 0, 1 of cells g and g+8 in o[0..3] of lanes t == 0) of the
+// 16 cells whose layer-1 A fragments are a1
+__device__ __forceinline__ void mlp16(const ClSmem &s, const uint32_t a1[3][4], float o[4])
+{
+    const int l = threadIdx.x & 31, g = l >> 2, t = l & 3;
+    float acc[8][4];
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+        acc[nt][0] = acc[nt][2] = s.b1[8 * nt + 2 * t];
+        acc[nt][1] = acc[nt][3] = s.b1[8 * nt + 2 * t + 1];
+    }
+#pragma unroll
+    for (int kb = 0; kb < 3; kb++)
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            const uint32_t b[2] = {lds32(&s.w1t[8 * nt + g][16 * kb + 2 * t]), lds32(&s.w1t[8 * nt + g][16 * kb + 2 * t + 8])};
+            mma16816(acc[nt], a1[kb], b);
+        }
+    uint32_t a2[4][4];
+#pragma unroll
+    for (int kb = 0; kb < 4; kb++) {
+        a2[kb][0] = pack2(gelu(acc[2 * kb][0]), gelu(acc[2 * kb][1]));
+        a2[kb][1] = pack2(gelu(acc[2 * kb][2]), gelu(acc[2 * kb][3]));
+        a2[kb][2] = pack2(gelu(acc[2 * kb + 1][0]), gelu(acc[2 * kb + 1][1]));
+        a2[kb][3] = pack2(gelu(acc[2 * kb + 1][2]), gelu(acc[2 * kb + 1][3]));
+    }
+#pragma unroll
+    for (int nt = 0; nt < 8; nt++) {
+        acc[nt][0] = acc[nt][2] = s.b2[8 * nt + 2 * t];
+        acc[nt][1] = acc[nt][3] = s.b2[8 * nt + 2 * t + 1];
+    }
+#pragma unroll
+    for (int kb = 0; kb < 4; kb++)
+#pragma unroll
+        for (int nt = 0; nt < 8; nt++) {
+            const uint32_t b[2] = {lds32(&s.w2t[8 * nt + g][16 * kb + 2 * t]), lds32(&s.w2t[8 * nt + g][16 * kb + 2 * t + 8])};
+            mma16816(acc[nt], a2[kb], b);
+        }
+#pragma unroll
+    for (int kb = 0; kb < 4; kb++) {
+        a2[kb][0] = pack2(gelu(acc[2 * kb][0]), gelu(acc[2 * kb][1]));
+        a2[kb][1] = pack2(gelu(acc[2 * kb][2]), gelu(acc[2 * kb][3]));
+        a2[kb][2] = pack2(gelu(acc[2 * kb + 1][0]), gelu(acc[2 * kb + 1][1]));
+        a2[kb][3] = pack2(gelu(acc[2 * kb + 1][2]), gelu(acc[2 * kb + 1][3]));
+    }
+    o[0] = o[2] = s.b3[2 * t];
+    o[1] = o[3] = s.b3[2 * t + 1];
+#pragma unroll
+    for (int kb = 0; kb < 4; kb++) {
+        const uint32_t b[2] = {lds32(&s.w3t[g][16 * kb + 2 * t]), lds32(&s.w3t[g][16 * kb + 2 * t + 8])};
+        mma16816(o, a2[kb], b);
+    }
+}
+
+// Persistent over tiles: out[c] = base[c] + MLP(features)_c * out_scale[c] * fac[c]
+__global__ void __launch_bounds__(WARPS * 32, 2) k_closure_apply(const __grid_constant__ inmsom::closure::Args a)
+{
+    __shared__ __align__(16) ClSmem s;
+    const __nv_bfloat16 *wb = (const __nv_bfloat16 *)a.wb;
+    for (int i = threadIdx.x; i < KIN * HID; i += blockDim.x) s.w1t[i % HID][i / HID] = wb[BOFF_W1 + i];
+    for (int i = threadIdx.x; i < HID * HID; i += blockDim.x) s.w2t[i % HID][i / HID] = wb[BOFF_W2 + i];
+    for (int i = threadIdx.x; i < HID * N3; i += blockDim.x) s.w3t[i % N3][i / N3] = wb[BOFF_W3 + i];
+    for (int i = threadIdx.x; i < HID; i += blockDim.x) {
+        s.b1[i] = a.prm[OFF_B1 + i];
+        s.b2[i] = a.prm[OFF_B2 + i];
+    }
+    if (threadIdx.x < N3) s.b3[threadIdx.x] = a.prm[OFF_B3 + threadIdx.x];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, g = l >> 2, t = l & 3;
+    // this lane's 12 feature offsets of the layer-1 A fragments (k >= 45: zero)
+    int koff[3][4];
+#pragma unroll
+    for (int kb = 0; kb < 3; kb++)
+#pragma unroll
+        for (int q = 0; q < 4; q++) {
+            const int k = 16 * kb + 2 * t + (q & 1) + 8 * (q >> 1);
+            koff[kb][q] = k < 45 ? feat_off(k) : -1;
+        }
+    const int nx = a.mx1 - a.mx0 + 1, ny = a.ny1 - a.ny0 + 1;
+    const int ntx = (nx + TCOLS - 1) / TCOLS, nty = (ny + TROWS - 1) / TROWS;
+    const __nv_bfloat16 zero = __float2bfloat16(0.f);
+    for (int tix = blockIdx.x; tix < ntx * nty; tix += gridDim.x) {
+        const int m0 = a.mx0 + (tix % ntx) * TCOLS, n0 = a.ny0 + (tix / ntx) * TROWS;
+        __syncthreads();   // the previous tile's reads are done (and the weights are in)
+        stage_tile(s.tile, a, m0, n0);
+        __syncthreads();
+        const int n = n0 + w;
+        if (n > a.ny1) continue;
+        for (int c0 = 0; c0 < TCOLS && m0 + c0 <= a.mx1; c0 += 16) {
+            uint32_t a1[3][4];
+            const int base_g = w * FW + c0 + g, base_h = base_g + 8;   // cells g, g+8 at ring offset
+#pragma unroll
+            for (int kb = 0; kb < 3; kb++)
+#pragma unroll
+                for (int h = 0; h < 2; h++) {   // h: features 2t.. (h = 0) or 2t+8.. (h = 1)
+                    const int ka = koff[kb][2 * h], kc = koff[kb][2 * h + 1];
+                    const __nv_bfloat16 xg0 = ka >= 0 ? s.tile[ka + base_g] : zero, xg1 = kc >= 0 ? s.tile[kc + base_g] : zero;
+                    const __nv_bfloat16 xh0 = ka >= 0 ? s.tile[ka + base_h] : zero, xh1 = kc >= 0 ? s.tile[kc + base_h] : zero;
+                    a1[kb][2 * h] = pack_raw(xg0, xg1);
+                    a1[kb][2 * h + 1] = pack_raw(xh0, xh1);
+                }
+            float o[4];
+            mlp16(s, a1, o);
+            if (t == 0) {
+                s.y[w][g][0] = o[0];
+                s.y[w][g][1] = o[1];
+                s.y[w][g + 8][0] = o[2];
+                s.y[w][g + 8][1] = o[3];
+            }
+            __syncwarp();
+            const int cell = l >> 1, comp = l & 1, m = m0 + c0 + cell;
+            if (m <= a.mx1) {
+                const long long idx = (long long)(n - a.y1) * a.pitch + (m - a.x1 + a.xoff);
+                const double f = a.fac[comp][idx];
+                if (f != 0.0) a.out[comp][idx] = a.base[comp][idx] + (double)(s.y[w][cell][comp] * a.out_scale[comp]) * f;
+            }
+            __syncwarp();
+        }
+    }
+}
+
+// the 48 BF16 features of every interior cell, row-major over (n, m)
+__global__ void __launch_bounds__(WARPS * 32) k_closure_features(const __grid_constant__ inmsom::closure::Args a)
+{
+    __shared__ __align__(16) __nv_bfloat16 tile[NTILE];
+    __shared__ int koff[KIN];
+    if (threadIdx.x < KIN) koff[threadIdx.x] = threadIdx.x < 45 ? feat_off(threadIdx.x) : -1;
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+    const int nx = a.mx1 - a.mx0 + 1, ny = a.ny1 - a.ny0 + 1;
+    const int ntx = (nx + TCOLS - 1) / TCOLS, nty = (ny + TROWS - 1) / TROWS;
+    uint32_t *feat = (uint32_t *)a.feat;
+    for (int tix = blockIdx.x; tix < ntx * nty; tix += gridDim.x) {
+        const int m0 = a.mx0 + (tix % ntx) * TCOLS, n0 = a.ny0 + (tix / ntx) * TROWS;
+        __syncthreads();
+        stage_tile(tile, a, m0, n0);
+        __syncthreads();
+        const int n = n0 + w;
+        if (n > a.ny1) continue;
+        for (int j = l; j < TCOLS * (KIN / 2); j += 32) {
+            const int cell = j / (KIN / 2), p = j - cell * (KIN / 2), m = m0 + cell;
+            if (m > a.mx1) continue;
+            const int b = w * FW + cell, k0 = koff[2 * p], k1 = koff[2 * p + 1];
+            const __nv_bfloat16 z = __float2bfloat16(0.f);
+            const uint32_t v = pack_raw(k0 >= 0 ? tile[k0 + b] : z, k1 >= 0 ? tile[k1 + b] : z);
+            feat[((long long)(n - a.ny0) * nx + (m - a.mx0)) * (KIN / 2) + p] = v;
+        }
+    }
+}
+
+__global__ void k_closure_factors(inmsom::closure::Args a, const float *lcu, const float *lcv, const double *dxt,
+                                  const double *dyh, const double *dyt, const double *dxh, double *fu, double *fv)
+{
+    const int nx = a.mx1 - a.mx0 + 1, ny = a.ny1 - a.ny0 + 1;
+    const double *H = a.fld[3];
+    for (long long k = blockIdx.x * (long long)blockDim.x + threadIdx.x; k < (long long)nx * ny;
+         k += (long long)gridDim.x * blockDim.x) {
+        const int m = a.mx0 + (int)(k % nx), n = a.ny0 + (int)(k / nx);
+        const long long i = (long long)(n - a.y1) * a.pitch + (m - a.x1 + a.xoff);
+        fu[i] = lcu[i] > 0.5f ? 0.5 * (H[i] + H[i + 1]) * dxt[i] * dyh[i] : 0.0;
+        fv[i] = lcv[i] > 0.5f ? 0.5 * (H[i] + H[i + a.pitch]) * dyt[i] * dxh[i] : 0.0;
+    }
+}
+
+int fail(int code, const char *msg) { return inmsom::record_error(code, msg); }
+
+int check_launch(const char *what)
+{
+    const cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) {
+        char buf[256];
+        snprintf(buf, sizeof buf, "%s: %s", what, cudaGetErrorString(e));
+        return fail(INMSOM_ECUDA, buf);
+    }
+    return INMSOM_OK;
+}
+
+bool smem_ready = false;
+
+int ensure_smem()
+{
+    if (smem_ready) return INMSOM_OK;
+    if (cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem)) !=
+            cudaSuccess ||
+        cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem)) !=
+            cudaSuccess)
+        return fail(INMSOM_ECUDA, "MLP kernels: shared memory attribute");
+    smem_ready = true;
+    return INMSOM_OK;
+}
+
+}  // namespace
+
+namespace inmsom {
+namespace closure {
+
+int apply(const Args &a, int nsm, cudaStream_t s)
+{
+    const int nx = a.mx1 - a.mx0 + 1, ny = a.ny1 - a.ny0 + 1;
+    const int tiles = ((nx + TCOLS - 1) / TCOLS) * ((ny + TROWS - 1) / TROWS);
+    const int grid = tiles < 2 * nsm ? tiles : 2 * nsm;
+    k_closure_apply<<<grid, WARPS * 32, 0, s>>>(a);
+    return check_launch("closure apply");
+}
+
+int features(const Args &a, int nsm, cudaStream_t s)
+{
+    const int nx = a.mx1 - a.mx0 + 1, ny = a.ny1 - a.ny0 + 1;
+    const int tiles = ((nx + TCOLS - 1) / TCOLS) * ((ny + TROWS - 1) / TROWS);
+    const int grid = tiles < 4 * nsm ? tiles : 4 * nsm;
+    k_closure_features<<<grid, WARPS * 32, 0, s>>>(a);
+    return check_launch("closure features");
+}
+
+int factors(const Args &a, const float *lcu, const float *lcv, const double *dxt, const double *dyh,
+            const double *dyt, const double *dxh, double *fac_u, double *fac_v, cudaStream_t s)
+{
+    k_closure_factors<<<592, 256, 0, s>>>(a, lcu, lcv, dxt, dyh, dyt, dxh, fac_u, fac_v);
+    return check_launch("closure factors");
+}
+
+}  // namespace closure
+}  // namespace inmsom
+
+extern "C" {
+
+int inmsom_mlp_pack(const float *params, void *wbf16, void *stream)
+{
+    if (!params || !wbf16) return fail(INMSOM_EARG, "inmsom_mlp_pack: NULL argument");
+    k_mlp_pack<<<(NBF + 255) / 256, 256, 0, (cudaStream_t)stream>>>(params, (__nv_bfloat16 *)wbf16);
+    return check_launch("inmsom_mlp_pack");
+}
+
+int inmsom_mlp_forward(const void *x, long long count, const float *params, const void *wbf16, float *y,
+                       void *stream)
+{
+    if (!x || !params || !wbf16 || !y || count < 0) return fail(INMSOM_EARG, "inmsom_mlp_forward: bad argument");
+    if (count == 0) return INMSOM_OK;
+    if (ensure_smem()) return INMSOM_ECUDA;
+    const long long tiles = (count + TILE - 1) / TILE;
+    k_mlp_forward<<<(unsigned)tiles, WARPS * 32, sizeof(Smem), (cudaStream_t)stream>>>(
+        (const __nv_bfloat16 *)x, count, params, (const __nv_bfloat16 *)wbf16, y);
+    return check_launch("inmsom_mlp_forward");
+}
+
+int inmsom_mlp_grad(const void *x, const float *targets, const int *idx, int batch, const float *params,
+                    const void *wbf16, float *partial, float *grad, void *stream)
+{
+    if (!x || !targets || !params || !wbf16 || !partial || !grad)
+        return fail(INMSOM_EARG, "inmsom_mlp_grad: NULL argument");
+    if (batch <= 0 || batch % TILE) return fail(INMSOM_EARG, "inmsom_mlp_grad: batch must be a positive multiple of 128");
+    if (ensure_smem()) return INMSOM_ECUDA;
+    const int tiles = batch / TILE;
+    k_mlp_grad<<<tiles, WARPS * 32, sizeof(Smem), (cudaStream_t)stream>>>(
+        (const __nv_bfloat16 *)x, targets, idx, batch, params, (const __nv_bfloat16 *)wbf16, partial);
+    if (check_launch("inmsom_mlp_grad")) return INMSOM_ECUDA;
+    k_mlp_reduce<<<(NPARAM + 1 + 255) / 256, 256, 0, (cudaStream_t)stream>>>(partial, tiles, batch, grad);
+    return check_launch("inmsom_mlp_grad reduce");
+}
+
+int inmsom_mlp_adam(float *params, void *wbf16, float *m, float *v, const float *grad, int step, float lr,
+                    float beta1, float beta2, float eps, void *stream)
+{
+    if (!params || !wbf16 || !m || !v || !grad || step < 1) return fail(INMSOM_EARG, "inmsom_mlp_adam: bad argument");
+    k_mlp_adam<<<(NPARAM + 255) / 256, 256, 0, (cudaStream_t)stream>>>(params, (__nv_bfloat16 *)wbf16, m, v, grad,
+                                                                       step, lr, beta1, beta2, eps);
+    return check_launch("inmsom_mlp_adam");
+}
+
+int inmsom_mlp_batch_indices(int *idx, int batch, long long n, unsigned long long seed, int step, void *stream)
+{
+    if (!idx || batch <= 0 || n <= 0) return fail(INMSOM_EARG, "inmsom_mlp_batch_indices: bad argument");
+    k_batch_indices<<<(batch + 255) / 256, 256, 0, (cudaStream_t)stream>>>(idx, batch, n, seed, step);
+    return check_launch("inmsom_mlp_batch_indices");
+}
+
+}  // extern "C"

@@ -120,6 +120,27 @@ class BarotropicSolver:
                                          ctypes.byref(ms)))
         return float(ms.value)
 
+    def closure_features(self, norm, x_ptr: int) -> None:
+        """48 BF16 features of every interior cell of the resident state into
+        the device buffer at x_ptr (nx * ny * 48 values)."""
+        check(load().inmsom_closure_features(self._ctx, ctypes.byref(norm), ctypes.c_void_p(x_ptr)))
+
+    def run_closure(self, nsub: int, dt: float, every: int, params_ptr: int, wbf16_ptr: int, norm) -> float:
+        """nsub substeps with the learned closure re-evaluated every `every`
+        substeps (inmsom_run_closure); returns the device time in ms."""
+        ms = ctypes.c_float(0.0)
+        check(load().inmsom_run_closure(self._ctx, int(nsub), float(dt), int(every), ctypes.c_void_p(params_ptr),
+                                        ctypes.c_void_p(wbf16_ptr), ctypes.byref(norm), ctypes.byref(ms)))
+        return float(ms.value)
+
+    def closure_tendency(self, params_ptr: int, wbf16_ptr: int, norm):
+        """(RHSx, RHSy) increments of the closure on the resident state."""
+        b = self.basin.bounds
+        fx, fy = b.zeros(), b.zeros()
+        check(load().inmsom_closure_tendency(self._ctx, ctypes.c_void_p(params_ptr), ctypes.c_void_p(wbf16_ptr),
+                                             ctypes.byref(norm), dptr(fx), dptr(fy)))
+        return fx, fy
+
     def wind_forcing(self, taux, tauy, rhsx=None, rhsy=None):
         b = self.basin.bounds
         rhsx = b.zeros() if rhsx is None else rhsx

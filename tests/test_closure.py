@@ -1,0 +1,198 @@
+"""The learned closure on the solver state.
+
+CPU: coarse graining keeps the fine fluxes and block means; the fine and
+coarse closure basins share their land mask block by block.
+GPU (tolerances written here):
+  * features of the resident state equal the oracle's restatement bit for
+    bit (FP32 normalisation, BF16 rounding);
+  * the RHS increments of the fused inference kernel equal the oracle
+    network on those features times out_scale * hu * area, normwise
+    relative <= 5e-3 (BF16 MMA with FP32 accumulation against FP64 with
+    BF16 rounding emulated);
+  * a network whose output is zero leaves run_closure bit-identical to
+    run_substeps; a constant output equals run_substeps with the RHS
+    increased by that tendency, normwise relative <= 1e-12.
+"""
+import numpy as np
+import pytest
+
+from conftest import rel_err
+
+
+def _cfg(n=32):
+    from inmsom_elfs_b200.closure import ClosureConfig
+    return ClosureConfig(n_coarse=n, factor=4, spacing_fine=4.0e3, dt_fine=6.0, visc_fine=200.0,
+                         visc_plain=1000.0, visc_base=100.0)
+
+
+def test_coarsen_block_means_and_fluxes():
+    from inmsom_elfs_b200.closure import coarsen
+    from inmsom_elfs_b200.grid import Bounds
+    r, nc = 4, 6
+    fb, cb = Bounds.serial(nc * r, nc * r), Bounds.serial(nc, nc)
+    rng = np.random.default_rng(3)
+    u, v, s = (np.asfortranarray(rng.standard_normal(fb.shape)) for _ in range(3))
+    cu, cv, cs = coarsen(fb, cb, r, u, v, s)
+    U, V, S = u[fb.interior], v[fb.interior], s[fb.interior]
+    for M in range(nc):
+        for N in range(nc):
+            blk = (slice(r * M, r * M + r), slice(r * N, r * N + r))
+            assert np.isclose(cs[cb.interior][M, N], S[blk].mean())
+            assert np.isclose(cu[cb.interior][M, N], U[r * M + r - 1, r * N:r * N + r].mean())
+            assert np.isclose(cv[cb.interior][M, N], V[r * M:r * M + r, r * N + r - 1].mean())
+    assert np.all(cu[:, 0] == 0) and np.all(cs[0, :] == 0)
+
+
+def test_closure_basins_share_the_mask(ora):
+    from inmsom_elfs_b200.closure import closure_basins
+    cfg = _cfg(16)
+    b = closure_basins(cfg, ora.OracleBackend())
+    fb, cb = b["fine"].bounds, b["plain"].bounds
+    lf = b["fine"].masks["lu"][fb.interior]
+    lc = b["plain"].masks["lu"][cb.interior]
+    assert np.array_equal(np.kron(lc, np.ones((4, 4), np.float32)), lf)
+    hf, hc = b["fine"].hhq_rest[fb.interior], b["plain"].hhq_rest[cb.interior]
+    assert np.allclose(hf.reshape(16, 4, 16, 4).mean(axis=(1, 3)), hc)
+    assert b["fine"].dt * 4 == b["plain"].dt == b["base"].dt
+    assert b["plain"].forcing["mu"][0, 0] == 1000.0 and b["base"].forcing["mu"][0, 0] == 100.0
+
+
+def _spun_up(gpu, nc=32, days=1.0):
+    """The coarse base basin with a coarse-grained state of a short fine run."""
+    from inmsom_elfs_b200.closure import closure_basins, coarsen, _set_state
+    cfg = _cfg(nc)
+    bs = closure_basins(cfg, gpu.GpuBackend(0))
+    with gpu.BarotropicSolver(bs["fine"]) as f:
+        f.load_state()
+        f.run_substeps(int(days * 86400 / cfg.dt_fine) // 100 * 100, cfg.dt_fine)
+        f.sync_to_host()
+        st = bs["fine"].state
+        prev = coarsen(bs["fine"].bounds, bs["base"].bounds, 4, st["ubrtrp_e"], st["vbrtrp_e"], st["sshp_e"])
+        cur = coarsen(bs["fine"].bounds, bs["base"].bounds, 4, st["ubrtr_e"], st["vbrtr_e"], st["ssh_e"])
+    _set_state(bs["base"], cur, prev)
+    return cfg, bs["base"], cur
+
+
+def _net(seed):
+    from oracle import mlp_oracle as mo
+    from inmsom_elfs_b200.mlp import MLP, init_params
+    p = init_params(seed)
+    rng = np.random.default_rng(seed)
+    p[mo.OFF_B1:mo.OFF_W2] = rng.uniform(-0.3, 0.3, 64)   # exercise the bias paths
+    p[mo.OFF_B2:mo.OFF_W3] = rng.uniform(-0.3, 0.3, 64)
+    p[mo.OFF_B3:mo.OFF_B3 + 2] = rng.uniform(-0.3, 0.3, 2)
+    return MLP(params=p)
+
+
+@pytest.mark.gpu
+def test_features_match_oracle(gpu):
+    import torch
+    from oracle import mlp_oracle as mo
+    from inmsom_elfs_b200.closure import make_norm
+    cfg, b, cur = _spun_up(gpu)
+    norm = make_norm(b, *cur, out_scale=(1e-6, 1e-6))
+    x = torch.empty((b.bounds.nx * b.bounds.ny, 48), dtype=torch.bfloat16, device="cuda")
+    with gpu.BarotropicSolver(b) as s:
+        s.load_state()
+        s.closure_features(norm, x.data_ptr())
+    got = x.float().cpu().numpy().astype(np.float64)
+    st = b.state
+    want = mo.features((st["ubrtr_e"], st["vbrtr_e"], st["ssh_e"], b.hhq_rest, b.rlh_s), b.bounds,
+                       list(norm.mean), list(norm.inv_std))
+    assert np.array_equal(got, want)
+
+
+@pytest.mark.gpu
+def test_inference_kernel_matches_oracle(gpu):
+    import torch
+    from oracle import mlp_oracle as mo
+    from inmsom_elfs_b200.closure import make_norm
+    cfg, b, cur = _spun_up(gpu)
+    norm = make_norm(b, *cur, out_scale=(2e-6, 3e-6))
+    net = _net(11)
+    with gpu.BarotropicSolver(b) as s:
+        s.load_state()
+        fx, fy = s.closure_tendency(net.params.data_ptr(), net.wbf16.data_ptr(), norm)
+    st, bb = b.state, b.bounds
+    X = mo.features((st["ubrtr_e"], st["vbrtr_e"], st["ssh_e"], b.hhq_rest, b.rlh_s), bb,
+                    list(norm.mean), list(norm.inv_std))
+    y, _ = mo.forward(net.host_params(), X, emulate=True)
+    H, d = b.hhq_rest, b.metrics["dxt"]
+    i = bb.interior
+    hu = 0.5 * (H + np.roll(H, -1, axis=0))
+    hv = 0.5 * (H + np.roll(H, -1, axis=1))
+    fu = np.where(b.masks["lcu"] > 0.5, hu * b.metrics["dxt"] * b.metrics["dyh"], 0.0)[i]
+    fv = np.where(b.masks["lcv"] > 0.5, hv * b.metrics["dyt"] * b.metrics["dxh"], 0.0)[i]
+    wu = y[:, 0].reshape(bb.ny, bb.nx).T * norm.out_scale[0] * fu
+    wv = y[:, 1].reshape(bb.ny, bb.nx).T * norm.out_scale[1] * fv
+    assert np.all(fx[i][fu == 0] == 0) and np.all(fy[i][fv == 0] == 0)
+    assert rel_err(fx[i], wu) <= 5e-3, rel_err(fx[i], wu)
+    assert rel_err(fy[i], wv) <= 5e-3, rel_err(fy[i], wv)
+    assert np.abs(fx).max() > 0 and np.abs(fy).max() > 0
+
+
+@pytest.mark.gpu
+def test_run_closure_zero_and_constant_network(gpu):
+    from inmsom_elfs_b200.closure import make_norm
+    from inmsom_elfs_b200.mlp import MLP
+    cfg, b, cur = _spun_up(gpu)
+    norm = make_norm(b, *cur, out_scale=(1e-6, -2e-6))
+    nsub, every = 248, 4   # 5 graphs of 12 groups and 2 groups launched alone
+    # zero network: bit-identical to the plain substeps
+    zero = MLP(params=np.zeros(7816, np.float32))
+    ref = b.copy()
+    with gpu.BarotropicSolver(ref) as s:
+        s.load_state()
+        s.run_substeps(nsub, cfg.dt_coarse)
+        s.sync_to_host()
+    got = b.copy()
+    with gpu.BarotropicSolver(got) as s:
+        s.load_state()
+        s.run_closure(nsub, cfg.dt_coarse, every, zero.params.data_ptr(), zero.wbf16.data_ptr(), norm)
+        s.sync_to_host()
+    for k in ref.state:
+        assert np.array_equal(got.state[k], ref.state[k]), k
+    # constant output (0.7, -0.4): the RHS raised by y * out_scale * hu * area
+    p = np.zeros(7816, np.float32)
+    p[7808], p[7809] = 0.7, -0.4   # b3
+    const = MLP(params=p)
+    H = b.hhq_rest
+    ref = b.copy()
+    yu = np.float64(np.float32(np.float32(0.7) * np.float32(norm.out_scale[0])))
+    yv = np.float64(np.float32(np.float32(-0.4) * np.float32(norm.out_scale[1])))
+    fu = np.where(b.masks["lcu"] > 0.5, 0.5 * (H + np.roll(H, -1, 0)) * b.metrics["dxt"] * b.metrics["dyh"], 0.0)
+    fv = np.where(b.masks["lcv"] > 0.5, 0.5 * (H + np.roll(H, -1, 1)) * b.metrics["dyt"] * b.metrics["dxh"], 0.0)
+    ref.forcing["RHSx"] = np.asfortranarray(np.where(fu != 0, ref.forcing["RHSx"] + yu * fu, ref.forcing["RHSx"]))
+    ref.forcing["RHSy"] = np.asfortranarray(np.where(fv != 0, ref.forcing["RHSy"] + yv * fv, ref.forcing["RHSy"]))
+    with gpu.BarotropicSolver(ref) as s:
+        s.load_state()
+        s.run_substeps(nsub, cfg.dt_coarse)
+        s.sync_to_host()
+    got = b.copy()
+    with gpu.BarotropicSolver(got) as s:
+        s.load_state()
+        s.run_closure(nsub, cfg.dt_coarse, every, const.params.data_ptr(), const.wbf16.data_ptr(), norm)
+        s.sync_to_host()
+    for k in ref.state:
+        assert rel_err(got.state[k], ref.state[k]) <= 1e-12, (k, rel_err(got.state[k], ref.state[k]))
+
+
+@pytest.mark.gpu
+def test_run_closure_rejects_bad_arguments(gpu):
+    from inmsom_elfs_b200 import InmsomError, _lib
+    from inmsom_elfs_b200.closure import make_norm
+    from inmsom_elfs_b200.mlp import MLP
+    cfg, b, cur = _spun_up(gpu, days=0.1)
+    norm = make_norm(b, *cur, out_scale=(1e-6, 1e-6))
+    net = MLP(seed=1)
+    with gpu.BarotropicSolver(b) as s:
+        s.load_state()
+        for nsub, every in ((10, 3), (10, 4), (8, 0)):
+            with pytest.raises(InmsomError) as e:
+                s.run_closure(nsub, cfg.dt_coarse, every, net.params.data_ptr(), net.wbf16.data_ptr(), norm)
+            assert e.value.code == _lib.EARG
+    with gpu.BarotropicSolver(b.copy(), fp32_velocity=True) as s:
+        s.load_state()
+        with pytest.raises(InmsomError) as e:
+            s.run_closure(8, cfg.dt_coarse, 4, net.params.data_ptr(), net.wbf16.data_ptr(), norm)
+        assert e.value.code == _lib.EUNSUPPORTED
