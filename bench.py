@@ -22,6 +22,15 @@ and budgets FP64); the e2e arm stays FP64.
 192, 256, .., 1536, own seeds, wind amplitude +-20 %) for --steps substeps:
 tuned CUDA-graph ensemble, untuned ensemble, and the members one after
 another (a study line).
+--study closure trains the learned momentum closure on a 2048^2 double-gyre
+ridge basin (2 km) coarse-grained to 512^2 (8 km) and compares the
+closure-equipped 512^2 run with the plain one (A = 1000 m^2/s) and with
+lower plain viscosities: SSH and KE RMSE against the coarse-grained truth
+and device time (a study line).
+--study closure-kernels times the closure's kernels on the 512^2 coarse basin
+with a seeded synthetic state: run_closure against run_substeps (the fused
+inference kernel's cost per evaluation) and the training step (gradient +
+Adam, batch 65536) (a study line; the ncu summaries use it).
 --study fp32 runs the FP32-velocity variant against the FP64 run on the
 4096 x 4096 ridge basin (2 km, dt = 3 s) for --steps substeps and prints the
 per-field max/RMS differences (a study line, not a benchmark line).
@@ -66,7 +75,11 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--fp32-velocity", action="store_true")
-    p.add_argument("--study", default=None, choices=["fp32", "ensemble"])
+    p.add_argument("--study", default=None, choices=["fp32", "ensemble", "closure", "closure-kernels"])
+    p.add_argument("--closure-days", type=float, default=40.0, help="fine spin-up before the training states")
+    p.add_argument("--closure-every", type=int, default=10, help="coarse substeps per network evaluation")
+    p.add_argument("--closure-tau", type=float, default=0.3, help="wind stress amplitude, N/m^2")
+    p.add_argument("--closure-eval", type=int, default=60000, help="coarse substeps of the comparison")
     p.add_argument("--members", type=int, default=64)
     p.add_argument("--group", type=int, default=20)
     return p.parse_args()
@@ -433,9 +446,83 @@ def run_study_ensemble(args):
     }), flush=True)
 
 
+def run_study_closure(args):
+    """Learned closure against the plain viscosity on 512^2 coarse-grained
+    from 2048^2 (inmsom_elfs_b200.closure.run_study)."""
+    import torch
+    from inmsom_elfs_b200.closure import ClosureConfig, run_study
+    torch.cuda.set_device(0)
+    cfg = ClosureConfig(n_coarse=512, factor=4, tau0=args.closure_tau)
+    res = run_study(cfg, spinup_days=args.closure_days, snapshots=200, gap=1200, train_steps=20000,
+                    eval_gap=20000, eval_steps=args.closure_eval, records=20, every=args.closure_every,
+                    extra_plain={"plain_A250": 250.0, "plain_A500": 500.0},
+                    log=lambda m: print(m, file=sys.stderr, flush=True))
+    print(json.dumps({"study": "closure", "data": "synthetic", **res}), flush=True)
+
+
+def run_study_closure_kernels(args):
+    """Timing of the closure kernels (inference fused into the step forcing,
+    training step) on the 512^2 coarse basin; synthetic state and data."""
+    import torch
+    from inmsom_elfs_b200 import _lib, solver
+    from inmsom_elfs_b200.closure import ClosureConfig, closure_basins, make_norm
+    from inmsom_elfs_b200.mlp import MLP
+    torch.cuda.set_device(0)
+    cfg = ClosureConfig(n_coarse=512, factor=4)
+    b = closure_basins(cfg, solver.GpuBackend(0), which=("base",))["base"]
+    bb = b.bounds
+    rng = np.random.default_rng(7)
+    ocean = b.masks["lu"] > 0.5
+    for k, amp in (("ssh_e", 0.02), ("ubrtr_e", 0.1), ("vbrtr_e", 0.1)):
+        f = bb.zeros()
+        f[bb.interior] = amp * rng.standard_normal((bb.nx, bb.ny))
+        b.state[k] = np.asfortranarray(np.where(ocean, f, 0.0))
+    b.state["sshp_e"] = b.state["ssh_e"].copy(order="F")
+    b.state["ubrtrp_e"] = b.state["ubrtr_e"].copy(order="F")
+    b.state["vbrtrp_e"] = b.state["vbrtr_e"].copy(order="F")
+    norm = make_norm(b, b.state["ubrtr_e"], b.state["vbrtr_e"], b.state["ssh_e"], out_scale=(1e-9, 1e-9))
+    net = MLP(seed=1)
+    nsub, res = args.steps - args.steps % 100, {}
+    with solver.BarotropicSolver(b) as s:
+        s.load_state()
+        s.run_substeps(200, cfg.dt_coarse)
+        s.run_closure(200, cfg.dt_coarse, 10, net.params.data_ptr(), net.wbf16.data_ptr(), norm)
+        t_plain = s.run_substeps(nsub, cfg.dt_coarse)
+        res["plain_ms_per_substep"] = t_plain / nsub
+        for every in (10, 2):
+            s.load_state()
+            t = s.run_closure(nsub, cfg.dt_coarse, every, net.params.data_ptr(), net.wbf16.data_ptr(), norm)
+            res[f"closure_every{every}_ms_per_substep"] = t / nsub
+        per_eval = (res["closure_every2_ms_per_substep"] - res["plain_ms_per_substep"]) * 2
+        res["inference_ms_per_evaluation"] = per_eval
+        cells = bb.nx * bb.ny
+        flop = 2 * (45 * 64 + 64 * 64 + 64 * 2) * cells
+        res["inference_cells_per_s"] = cells / (per_eval / 1e3)
+        res["inference_tflops"] = flop / (per_eval / 1e3) / 1e12
+    n, batch = 1 << 21, 65536
+    x = torch.from_numpy(rng.standard_normal((n, 48)).astype(np.float32)).to("cuda").to(torch.bfloat16)
+    t = torch.from_numpy(rng.standard_normal((n, 2)).astype(np.float32)).to("cuda")
+    net.train(x, t, 20, batch=batch)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    e0.record()
+    net.train(x, t, 200, batch=batch)
+    e1.record()
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / 200
+    res["train_ms_per_step"] = ms
+    res["train_tflops"] = 3 * 2 * (45 * 64 + 64 * 64 + 64 * 2) * batch / (ms / 1e3) / 1e12
+    print(json.dumps({"study": "closure-kernels", "workload": "closure base basin 512x512 8 km, synthetic state",
+                      "steps": nsub, "results": res}), flush=True)
+
+
 if __name__ == "__main__":
     a = parse()
-    if a.study == "ensemble":
+    if a.study == "closure-kernels":
+        run_study_closure_kernels(a)
+    elif a.study == "closure":
+        run_study_closure(a)
+    elif a.study == "ensemble":
         run_study_ensemble(a)
     elif a.study == "fp32":
         run_study_fp32(a)

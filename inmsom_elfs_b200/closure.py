@@ -73,10 +73,10 @@ def _ridge_depth(cfg: ClosureConfig, x: np.ndarray, y: np.ndarray, L: float) -> 
     return crest * np.exp(-0.5 * ((x - axis) / w) ** 2)
 
 
-def closure_basins(cfg: ClosureConfig, backend) -> Dict[str, Basin]:
+def closure_basins(cfg: ClosureConfig, backend, which=("fine", "plain", "base")) -> Dict[str, Basin]:
     """The fine basin and the coarse basins (plain viscosity and the
     closure run's base viscosity), derived masks and wind forcing by
-    `backend` (finalize)."""
+    `backend` (finalize); `which` selects the ones built."""
     r, nc = cfg.factor, cfg.n_coarse
     nf = nc * r
     dxf, dxc = cfg.spacing_fine, cfg.spacing_fine * r
@@ -98,6 +98,8 @@ def closure_basins(cfg: ClosureConfig, backend) -> Dict[str, Basin]:
     for name, b, dx, lu, h, visc, dt in (("fine", fb, dxf, lu_f, hf, cfg.visc_fine, cfg.dt_fine),
                                           ("plain", cb, dxc, lu_c, hc, cfg.visc_plain, cfg.dt_coarse),
                                           ("base", cb, dxc, lu_c, hc, cfg.visc_base, cfg.dt_coarse)):
+        if name not in which:
+            continue
         basin = Basin(b, Consts())
         basin.masks["lu"] = lu.copy(order="F")
         uniform_metrics(basin, dx)
