@@ -258,13 +258,17 @@ def e2e_arm(args, b, local, barrier, maxall, ws):
         se.barotropic_dynamics(E2E_NSTEP * b.dt, E2E_NSTEP)
     barrier()
     e2e_s = maxall(time.perf_counter() - t0)
+    up, comp, down = se.last_phases()
     se.close()
     fb = 8 * b.bounds.shape[0] * b.bounds.shape[1]
     return {"value": cells * E2E_NSTEP * args.e2e_calls * ws / e2e_s, "unit": METRIC,
-           "h2d_bytes_per_step": 6 * fb / E2E_NSTEP, "d2h_bytes_per_step": 4 * fb / E2E_NSTEP,
+           "h2d_bytes_per_step": 5 * fb / E2E_NSTEP, "d2h_bytes_per_step": 4 * fb / E2E_NSTEP,
+           "ms_per_call": e2e_s / args.e2e_calls * 1e3,
+           "last_call_device_ms": {"upload": up, "substeps": comp, "download": down},
            "call": f"inmsom_barotropic_dynamics(tau={E2E_NSTEP}*dt, nstep={E2E_NSTEP}) from pinned "
-                   f"host arrays: 6 forcing arrays in, 4 time-mean arrays out per call, "
-                   f"{2 * E2E_NSTEP} substeps with time means; h2d/d2h bytes per advancing step"}
+                   f"host arrays: RHSx, RHSy, wflux, mu, rdis in (mu4 is read only with ksw4 > 0), "
+                   f"4 time-mean arrays out per call, {2 * E2E_NSTEP} substeps with time means; "
+                   f"h2d/d2h bytes per advancing step"}
 
 
 

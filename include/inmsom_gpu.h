@@ -263,6 +263,12 @@ int inmsom_load_state(inmsom_ctx *ctx, double *ubrtr_e, double *ubrtrp_e,
  * reference rounding), 1 = fused streaming kernel.  *reason receives a
  * static string saying why the fused path is not eligible (or "eligible"). */
 int inmsom_gpu_path(inmsom_ctx *ctx, int *path, const char **reason);
+/* Device time of the phases of the last completed
+ * inmsom_barotropic_dynamics call (CUDA events on the context's stream):
+ * host->device copies, the substeps (with the depth and time-mean work),
+ * device->host copies.  The reference times the whole call
+ * (Control/dyncall.f90:135,165-167 start_timer/end_timer). */
+int inmsom_gpu_last_phases(inmsom_ctx *ctx, float *upload_ms, float *compute_ms, float *download_ms);
 
 /* Ensemble of independent basins (no counterpart in the reference, which
  * advances one basin per run).  The members are contexts on one device,

@@ -26,7 +26,7 @@ EXPORTS = (
     "inmsom_diag_noalloc", "inmsom_ens_create", "inmsom_ens_run", "inmsom_ens_tune",
     "inmsom_ens_destroy", "inmsom_strips_create", "inmsom_strips_run", "inmsom_strips_destroy",
     "inmsom_mlp_pack", "inmsom_mlp_forward", "inmsom_mlp_grad", "inmsom_mlp_adam", "inmsom_mlp_batch_indices",
-    "inmsom_closure_features", "inmsom_run_closure", "inmsom_closure_tendency",
+    "inmsom_closure_features", "inmsom_run_closure", "inmsom_closure_tendency", "inmsom_gpu_last_phases",
 )
 
 # include/inmsom_gpu.h: INMSOM_MLP_*
@@ -113,6 +113,8 @@ def load() -> ctypes.CDLL:
     lib.inmsom_closure_features.argtypes = [VP, NP, VP]
     lib.inmsom_run_closure.argtypes = [VP, i, d, i, VP, VP, NP, ctypes.POINTER(ctypes.c_float)]
     lib.inmsom_closure_tendency.argtypes = [VP, VP, VP, NP, DP, DP]
+    FPP = ctypes.POINTER(ctypes.c_float)
+    lib.inmsom_gpu_last_phases.argtypes = [VP, FPP, FPP, FPP]
     lib.inmsom_diag_noalloc.argtypes = ([ctypes.POINTER(CBounds), ctypes.POINTER(CConsts),
                                          ctypes.c_longlong] + [VP] * 16 + [VP])
     for name in EXPORTS:

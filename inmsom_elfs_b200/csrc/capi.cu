@@ -80,6 +80,8 @@ struct inmsom_ctx {
     int device = 0;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev0 = nullptr, ev1 = nullptr;
+    cudaEvent_t ph[4] = {};          // barotropic_dynamics phases: start, uploaded, computed, downloaded
+    bool ph_valid = false;
     size_t nbytes = 0;  // one double field on the device
 
     float *mask[NMASK] = {};
@@ -355,6 +357,7 @@ int inmsom_gpu_init(inmsom_ctx **out, const inmsom_bounds *b, const inmsom_const
     cudaError_t e = cudaStreamCreateWithFlags(&c->stream, cudaStreamNonBlocking);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev0);
     if (e == cudaSuccess) e = cudaEventCreate(&c->ev1);
+    for (int k = 0; k < 4 && e == cudaSuccess; k++) e = cudaEventCreate(&c->ph[k]);
     if (e != cudaSuccess) {
         delete c;
         return set_err(INMSOM_ECUDA, "stream/event creation failed: %s", cudaGetErrorString(e));
@@ -390,6 +393,8 @@ int inmsom_gpu_finalize(inmsom_ctx *c)
     fused::free_plan(c->plan);
     if (c->ev0) cudaEventDestroy(c->ev0);
     if (c->ev1) cudaEventDestroy(c->ev1);
+    for (auto &e : c->ph)
+        if (e) cudaEventDestroy(e);
     if (c->stream) cudaStreamDestroy(c->stream);
     delete c;
     cudaGetLastError();   // nothing from the teardown reaches the next call
@@ -492,6 +497,8 @@ int inmsom_barotropic_dynamics(inmsom_ctx *c, double tau, int nstep, int ksw4, d
     const bool resident = (c->flags & INMSOM_RESIDENT) != 0;
     for (int k = 0; k < NSTATE; k++) c->h_state[k] = hs[k];
     for (int k = 0; k < NSCR; k++) c->h_scr[k] = hc[k];
+    c->ph_valid = false;
+    CK(cudaEventRecord(c->ph[0], c->stream));
 
     if (!resident || !c->state_on_device) {
         for (int k = 0; k < NSTATE; k++) CKR(h2d(c, c->state[k], (const double *)hs[k]));
@@ -503,7 +510,7 @@ int inmsom_barotropic_dynamics(inmsom_ctx *c, double tau, int nstep, int ksw4, d
         c->scratch_on_device = true;
     }
     for (int k = 0; k < NFORC; k++) {
-        if (k == F_MU4 && ksw4 <= 0 && !mu4) continue;
+        if (k == F_MU4 && ksw4 <= 0) continue;   // read only by uv_diff4
         CKR(h2d(c, c->forc[k], hf[k]));
     }
     if (!resident) {
@@ -511,21 +518,31 @@ int inmsom_barotropic_dynamics(inmsom_ctx *c, double tau, int nstep, int ksw4, d
             if (c->h_depth[k]) CKR(h2d(c, c->depth[k], (const double *)c->h_depth[k]));
         if (c->h_depth[0]) c->depths_current = true;
     }
-    if (!c->depths_current) depths_from_state(c);
+    CK(cudaEventRecord(c->ph[1], c->stream));
+    const bool fused_run = c->fused_ok && ksw4 <= 0;
+    // the fused path derives the depths from SSH; the per-loop path reads them
+    if (!c->depths_current && !fused_run) depths_from_state(c);
 
     int rc = INMSOM_OK;
-    if (c->fused_ok && ksw4 <= 0) {
+    if (fused_run) {
         if (fused::dynamics(c->plan, c->dom, c->c, tau, nstep, c->state, c->acc, c->forc,
                             c->stream))
             return set_err(INMSOM_ECUDA, "fused dynamics failed: %s",
                            cudaGetErrorString(cudaGetLastError()));
         if (c->plan.last_flags & fused::FLAG_TIMEOUT)
             return set_err(INMSOM_ETIMEOUT, "fused kernel: a bounded TMA wait timed out");
-        if (c->c.ffs > 0) depths_from_state(c);
+        // the call ends with hh_init(ssh_e, sshp_e) (vel_ssh.f90:668-675):
+        // resident depths are derived when next read (per-loop path, diag,
+        // sync_to_host), host depths now
+        if (c->c.ffs > 0) {
+            if (resident) c->depths_current = false;
+            else depths_from_state(c);
+        }
     } else {
         general_dynamics(c, tau, nstep, ksw4);
     }
 
+    CK(cudaEventRecord(c->ph[2], c->stream));
     for (int k = 0; k < NACC; k++) CKR(d2h(c, ha[k], c->acc[k]));
     if (!resident) {
         for (int k = 0; k < NSTATE; k++) CKR(d2h(c, hs[k], c->state[k]));
@@ -533,13 +550,25 @@ int inmsom_barotropic_dynamics(inmsom_ctx *c, double tau, int nstep, int ksw4, d
         for (int k = 0; k < NDEPTH; k++)
             if (c->h_depth[k]) CKR(d2h(c, c->h_depth[k], c->depth[k]));
     }
+    CK(cudaEventRecord(c->ph[3], c->stream));
     CKR(sync_stream(c));
+    c->ph_valid = true;
     if (c->flags & INMSOM_GUARD) {
         long nbad = 0;
         CKR(run_guard(c, &nbad));
         if (nbad) return set_err(INMSOM_EGUARD, "guard: %ld interior points out of range or NaN", nbad);
     }
     return rc;
+}
+
+int inmsom_gpu_last_phases(inmsom_ctx *c, float *upload_ms, float *compute_ms, float *download_ms)
+{
+    if (!c || !upload_ms || !compute_ms || !download_ms) return set_err(INMSOM_EARG, "NULL argument");
+    if (!c->ph_valid) return set_err(INMSOM_EARG, "no completed inmsom_barotropic_dynamics call");
+    CK(cudaEventElapsedTime(upload_ms, c->ph[0], c->ph[1]));
+    CK(cudaEventElapsedTime(compute_ms, c->ph[1], c->ph[2]));
+    CK(cudaEventElapsedTime(download_ms, c->ph[2], c->ph[3]));
+    return INMSOM_OK;
 }
 
 int inmsom_load_state(inmsom_ctx *c, double *ubrtr_e, double *ubrtrp_e, double *vbrtr_e,

@@ -307,6 +307,8 @@ struct S2 {
     double Pv;               // the row's part of its own v equation, less the GX flux
     double sly;              // pressure-gradient term of the row (time means only)
     HQ hqm;                  // H + ssh of row j
+    double au0, au2;         // time-mean sums (u, pgrx) of row j, for the next iteration's stage 3u
+    double av1, av3;         // time-mean sums (v, pgry) of row j-1, for its stage 3v
 };
 
 template <bool B>
@@ -402,6 +404,19 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
             mk = (mk << 2) | mask2(o_p1);
         } else {
             mk <<= 2;   // keep the row alignment of mk
+        }
+        if constexpr (ACC == 2 && D1) {
+            // the sums the next iteration's stage 3 adds to, loaded one
+            // iteration ahead; exactly where it will write them
+            const uint32_t mj = (mk >> 2) & 3u, mj1 = (mk >> 4) & 3u;   // rows j, j-1
+            if (out && j >= r0 && j < r1 && mj == 3u) {
+                q.au0 = p.acc[0][gi];
+                q.au2 = p.acc[2][gi];
+            }
+            if (out && j - 1 >= r0 && j - 1 < r1 && (mj & mj1 & 1u)) {
+                q.av1 = p.acc[1][gi - p.pitch];
+                q.av3 = p.acc[3][gi - p.pitch];
+            }
         }
 
         // ---------------- stage 1: row j (independent of stage 2) -------
@@ -547,7 +562,7 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
                 if (ACC && wu) {
                     const double slxn = -(SNr - sn) * (GEN ? CF(o_m1, gdyh) : p.gd) * hun;
                     double a = (c.U + un * hun) * p.c4, b = (c.slx + slxn) * p.c4;
-                    if (ACC == 2) { a += p.acc[0][idx]; b += p.acc[2][idx]; }
+                    if (ACC == 2) { a += qc.au0; b += qc.au2; }
                     p.acc[0][idx] = a;
                     p.acc[2][idx] = b;
                 }
@@ -591,7 +606,7 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
                 if (ACC && wv) {
                     const double slyn = -(sn1 - sn0) * (GEN ? CF(o_m2, gdxh) : p.gd) * hvn;
                     double a = (qc.V + vn * hvn) * p.c4, b = (qc.sly + slyn) * p.c4;
-                    if (ACC == 2) { a += p.acc[1][idx]; b += p.acc[3][idx]; }
+                    if (ACC == 2) { a += qc.av1; b += qc.av3; }
                     p.acc[1][idx] = a;
                     p.acc[3][idx] = b;
                 }

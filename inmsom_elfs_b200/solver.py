@@ -174,6 +174,13 @@ class BarotropicSolver:
     def sync_from_host(self, what: int = _lib.SYNC_STATE) -> None:
         check(load().inmsom_gpu_sync_from_host(self._ctx, what))
 
+    def last_phases(self):
+        """(upload, compute, download) device ms of the last
+        barotropic_dynamics call."""
+        a, b, c = ctypes.c_float(), ctypes.c_float(), ctypes.c_float()
+        check(load().inmsom_gpu_last_phases(self._ctx, ctypes.byref(a), ctypes.byref(b), ctypes.byref(c)))
+        return float(a.value), float(b.value), float(c.value)
+
     def path(self):
         p, r = ctypes.c_int(), ctypes.c_char_p()
         check(load().inmsom_gpu_path(self._ctx, ctypes.byref(p), ctypes.byref(r)))
