@@ -28,7 +28,7 @@ SOURCES = {
     "noalloc.cu": [],
     "closure.cu": [],
 }
-HEADERS = ["common.cuh", "general.h", "fused.h"]
+HEADERS = ["common.cuh", "general.h", "fused.h", "closure.h"]
 
 
 def nvcc() -> str:

@@ -54,7 +54,6 @@ namespace {
 constexpr int NL = 32;            // lanes = threads per CTA = strip columns
 constexpr int OUTW = NL - 2;      // written columns per strip
 constexpr int SEG = NL + 4;       // ring segment: strip columns -2 .. 33
-constexpr int RING = 6;           // ring slots (4 rows in use + 2 in flight)
 constexpr unsigned WAIT_LIMIT = 1u << 20;
 
 struct alignas(64) Params {
@@ -145,23 +144,37 @@ struct Layout {
     static constexpr int COEF_OFF = STAT_OFF + NS * SEG * 8;             // general variant: RowCoef
     static constexpr int BITS_OFF = COEF_OFF + (GEN ? (int)sizeof(RowCoef) : 0);
     static constexpr int SLOT_B = (BITS_OFF + 32 + 127) / 128 * 128;
-    static constexpr size_t bytes = 128 + (size_t)RING * SLOT_B + RING * sizeof(uint64_t);
     static constexpr uint32_t row_tx =
         (uint32_t)((F32 ? 4 * VSEG * 4 + 2 * SEG * 8 : NSET * SEG * 8) + NS * SEG * 8 +
                    (GEN ? (int)sizeof(RowCoef) : 0) + 32);
 };
 
+// ring slots: rows j-2..j+1 in use plus one row in flight for the plain
+// substep (15 CTAs per SM fit), two in flight where the registers hold the
+// CTAs per SM to 12 (time-mean sums) or the slots are small (FP32 velocities)
+template <bool GEN, int MODE, bool F32 = false>
+__host__ __device__ constexpr int ring_slots()
+{
+    return (MODE % 3 != 0 || F32) ? 6 : 5;
+}
+template <bool GEN, int MODE, bool F32 = false>
+constexpr size_t ring_bytes()
+{
+    return 128 + (size_t)ring_slots<GEN, MODE, F32>() * (Layout<GEN, F32>::SLOT_B + sizeof(uint64_t));
+}
+
 // resident CTAs per SM the register budget is cut for: 16 one-warp CTAs
 // (4 warps per SM sub-partition, 128 registers) for the plain substep, 12
 // where the time-mean sums need more registers, 11 for the general variant,
 // and never more than the shared memory holds (228 KB per SM, 1 KB of it
-// reserved per CTA): 13 for the FP64 uniform ring, 9 for the general one.
-// (Reading the forcing from global memory instead of the ring lets 16 fit
-// but exposes the load latency: 5% slower.)
+// reserved per CTA): 15 for the FP64 uniform ring of 5 slots, 11 for the
+// general one.  (A 6-slot ring holds 13 uniform CTAs: 4.5 % slower on the
+// 2048 x 1536 basin; reading the forcing from global memory instead of the
+// ring lets 16 fit but exposes the load latency: 5 % slower.)
 template <bool GEN, int MODE, bool F32 = false>
 constexpr int min_ctas()
 {
-    constexpr int by_smem = (int)(233472 / (Layout<GEN, F32>::bytes + 1024));
+    constexpr int by_smem = (int)(233472 / (ring_bytes<GEN, MODE, F32>() + 1024));
     constexpr int want = GEN ? 11 : (MODE % 3 ? 12 : 16);
     return by_smem < want ? by_smem : want;
 }
@@ -329,6 +342,7 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
     using L = Layout<GEN, F32>;
     constexpr int ACC = MODE % 3;
     constexpr bool WRITE = MODE / 3 != 0;
+    constexpr int RING = ring_slots<GEN, MODE, F32>();
 
     const int l = threadIdx.x;
     const int g0 = item.x;                     // device column of segment offset 0
@@ -693,6 +707,7 @@ template <bool GEN, int MODE, bool F32 = false>
 __global__ void __launch_bounds__(NL, min_ctas<GEN, MODE, F32>()) k_substep(const __grid_constant__ Params p)
 {
     using L = Layout<GEN, F32>;
+    constexpr int RING = ring_slots<GEN, MODE, F32>();
     extern __shared__ __align__(128) unsigned char smem_raw[];
     unsigned char *ring = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
     uint64_t *mbar = reinterpret_cast<uint64_t *>(ring + RING * L::SLOT_B);
@@ -853,8 +868,10 @@ int set_io(const Plan &p, Params &q, double *const src[NSET], double *const dst[
 template <bool GEN, int MODE>
 void launch_t(const Plan &p, const Params &q, cudaStream_t s)
 {
-    dim3 grid(p.nitems[GEN ? 1 : 0]);
-    k_substep<GEN, MODE><<<grid, NL, Layout<GEN>::bytes, s>>>(q);
+    const int v = item_table(GEN, MODE);
+    Params r = q;
+    r.items = p.items[v];
+    k_substep<GEN, MODE><<<dim3(p.nitems[v]), NL, ring_bytes<GEN, MODE>(), s>>>(r);
 }
 
 // mode = acc + 3*write (acc: 0 none, 1 write, 2 accumulate)
@@ -902,7 +919,7 @@ template <bool GEN, int MODE>
 int set_smem1()
 {
     return cudaFuncSetAttribute(k_substep<GEN, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                (int)Layout<GEN>::bytes) != cudaSuccess;
+                                (int)ring_bytes<GEN, MODE>()) != cudaSuccess;
 }
 
 int set_smem()
@@ -910,7 +927,7 @@ int set_smem()
     return set_smem1<false, 2>() | set_smem1<false, 3>() | set_smem1<false, 4>() | set_smem1<false, 5>() |
            set_smem1<true, 2>() | set_smem1<true, 3>() | set_smem1<true, 4>() | set_smem1<true, 5>() |
            (cudaFuncSetAttribute(k_substep<false, 3, true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)Layout<false, true>::bytes) != cudaSuccess);
+                                 (int)ring_bytes<false, 3, true>()) != cudaSuccess);
 }
 
 using EncodeTiled = decltype(&cuTensorMapEncodeTiled);
@@ -1042,9 +1059,10 @@ void release(Plan &p)
     cudaFree(p.stat);
     cudaFree(p.d_uniform);
     cudaFree(p.d_flags);
-    cudaFree(p.items[0]);
-    cudaFree(p.items[1]);
-    p.items[0] = p.items[1] = nullptr;
+    for (auto &it : p.items) {
+        cudaFree(it);
+        it = nullptr;
+    }
     for (auto &v : p.vset) {
         cudaFree(v);
         v = nullptr;
@@ -1298,20 +1316,24 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
     p.nsm = nsm;
-    int occ[2] = {1, 1};
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], k_substep<false, 3>, NL, Layout<false>::bytes) !=
-            cudaSuccess || occ[0] < 1)
-        occ[0] = 1;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], k_substep<true, 3>, NL, Layout<true>::bytes) !=
-            cudaSuccess || occ[1] < 1)
-        occ[1] = 1;
-    p.occ[0] = occ[0];
-    p.occ[1] = occ[1];
+    // one item table per variant for the plain substep and one for the
+    // time-mean substeps, each one wave of the kernel's resident CTAs
+    int occ[NTABLE] = {1, 1, 1, 1};
+    cudaError_t oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], k_substep<false, 3>, NL,
+                                                                   ring_bytes<false, 3>());
+    if (oe == cudaSuccess)
+        oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[1], k_substep<true, 3>, NL, ring_bytes<true, 3>());
+    if (oe == cudaSuccess)
+        oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], k_substep<false, 5>, NL, ring_bytes<false, 5>());
+    if (oe == cudaSuccess)
+        oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[3], k_substep<true, 5>, NL, ring_bytes<true, 5>());
+    if (oe != cudaSuccess) return 1;
     p.ocean = ocean_rows(p, d, masks[0]);
-    for (int v = 0; v < 2; v++) {
-        p.rows_per_item[v] = 0;
-        if (upload_items(p, v, partition(p, d, nsm * occ[v], 0), s)) return 1;
+    for (int v = 0; v < NTABLE; v++) {
+        p.occ[v] = occ[v] < 1 ? 1 : occ[v];
+        if (upload_items(p, v, partition(p, d, nsm * p.occ[v], 0), s)) return 1;
     }
+    p.rows_per_item[0] = p.rows_per_item[1] = 0;
     return 0;
 }
 
@@ -1395,7 +1417,7 @@ int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt, co
             for (int k = 0; k < 4; k++) q.vdst[k] = p.vset[di] + k * p.fstride;
             q.rhs_scale = rhs_scale ? rhs_scale[step] : 1.0;
             p.last_variant = 2;
-            k_substep<false, 3, true><<<dim3(p.nitems[0]), NL, Layout<false, true>::bytes, s>>>(q);
+            k_substep<false, 3, true><<<dim3(p.nitems[0]), NL, ring_bytes<false, 3, true>(), s>>>(q);
             if (cudaGetLastError() != cudaSuccess) return 1;
         }
         if (nsub & 1)
@@ -1425,8 +1447,8 @@ int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt, co
 
 int repartition(Plan &p, const Dom &d, int rows_per_item, cudaStream_t s)
 {
-    for (int v = 0; v < 2; v++) {
-        p.rows_per_item[v] = rows_per_item;
+    for (int v = 0; v < NTABLE; v++) {
+        p.rows_per_item[v & 1] = rows_per_item;
         if (upload_items(p, v, partition(p, d, p.nsm * p.occ[v], rows_per_item), s)) return 1;
     }
     return 0;

@@ -76,8 +76,10 @@ struct Plan {
     int ncol = 32;            // columns per CTA (one warp, one column per lane)
     int outw = 30;            // output columns per CTA
     int nstrips = 0;
-    int nitems[2] = {0, 0};         // work items per variant: uniform, general
-    int4 *items[2] = {nullptr, nullptr};   // {g0, first row, end row, 0} per item
+    // work-item tables (item_table): uniform and general variant, plain and
+    // time-mean substeps (their kernels hold different numbers of CTAs per SM)
+    int nitems[4] = {0, 0, 0, 0};
+    int4 *items[4] = {nullptr, nullptr, nullptr, nullptr};   // {g0, first row, end row, 0} per item
     bool uni = false;         // metrics all equal one spacing d (square uniform grid)
     double d = 0.0;           // that spacing
     long long min_pitch = 0;  // device row pitch the strips need
@@ -92,7 +94,7 @@ struct Plan {
     long long fstride = 0;          // doubles between the fields of a block
     CUtensorMap tm_set[3];          // box {36, 1, 6} over each state set
     CUtensorMap tm_stat[2];         // box {36, 1, 3 | 6} over the static block
-    int occ[2] = {0, 0};            // resident CTAs per SM, per variant
+    int occ[4] = {0, 0, 0, 0};      // resident CTAs per SM, per item table
     std::vector<uint8_t> ocean;     // per strip and interior row: any written column is ocean
     int rows_per_item[2] = {0, 0};  // 0: one wave of items by cost; else rows per item
     unsigned generation = 0;        // bumped whenever buffers or work items change
@@ -121,6 +123,11 @@ struct Plan {
 };
 
 enum : unsigned { FLAG_TIMEOUT = 1u, FLAG_GUARD = 2u };
+
+constexpr int NTABLE = 4;
+// item table of a launch: variant (0 uniform, 1 general) + 2 for the
+// substeps that accumulate time means (mode % 3 != 0)
+inline int item_table(bool gen, int mode) { return (gen ? 1 : 0) + (mode % 3 != 0 ? 2 : 0); }
 
 // The fused path writes only ocean points; land and halo points of the
 // ping-pong sets must equal those of the state.  Call after the state was
