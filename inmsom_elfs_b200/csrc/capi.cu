@@ -312,6 +312,14 @@ int ensure_grid(inmsom_ctx *c)
     return INMSOM_OK;
 }
 
+// the error of the fused kernel's status bits (the last run's flags)
+int fused_flag_error(const inmsom_ctx *c, const char *who)
+{
+    if (c->plan.last_flags & fused::FLAG_SMEM)
+        return set_err(INMSOM_ECUDA, "%s: dynamic shared memory not 128-byte aligned, nothing computed", who);
+    return set_err(INMSOM_ETIMEOUT, "%s: a bounded TMA wait timed out", who);
+}
+
 int run_guard(inmsom_ctx *c, long *nbad)
 {
     CK(cudaMemsetAsync(c->d_nbad, 0, sizeof(unsigned long long), c->stream));
@@ -529,8 +537,7 @@ int inmsom_barotropic_dynamics(inmsom_ctx *c, double tau, int nstep, int ksw4, d
                             c->stream))
             return set_err(INMSOM_ECUDA, "fused dynamics failed: %s",
                            cudaGetErrorString(cudaGetLastError()));
-        if (c->plan.last_flags & fused::FLAG_TIMEOUT)
-            return set_err(INMSOM_ETIMEOUT, "fused kernel: a bounded TMA wait timed out");
+        if (c->plan.last_flags & (fused::FLAG_TIMEOUT | fused::FLAG_SMEM)) return fused_flag_error(c, "fused kernel");
         // the call ends with hh_init(ssh_e, sshp_e) (vel_ssh.f90:668-675):
         // resident depths are derived when next read (per-loop path, diag,
         // sync_to_host), host depths now
@@ -663,8 +670,7 @@ int inmsom_run_substeps(inmsom_ctx *c, int nsub, double dt, const double *rhs_sc
     if (c->fused_ok && !(c->flags & INMSOM_FP32_VELOCITY) && nsub >= 2 * RS_GROUP) {
         CKR(run_substeps_graph(c, nsub, dt, rhs_scale));
         c->depths_current = false;
-        if (c->plan.last_flags & fused::FLAG_TIMEOUT)
-            return set_err(INMSOM_ETIMEOUT, "fused kernel: a bounded TMA wait timed out");
+        if (c->plan.last_flags & (fused::FLAG_TIMEOUT | fused::FLAG_SMEM)) return fused_flag_error(c, "fused kernel");
     } else if (c->fused_ok) {
         const int rc = fused::run_substeps(c->plan, c->dom, c->c, nsub, dt, rhs_scale, c->state, c->forc,
                                            c->stream);
@@ -676,8 +682,7 @@ int inmsom_run_substeps(inmsom_ctx *c, int nsub, double dt, const double *rhs_sc
             return set_err(INMSOM_ECUDA, "fused substeps failed: %s",
                            cudaGetErrorString(cudaGetLastError()));
         c->depths_current = false;
-        if (c->plan.last_flags & fused::FLAG_TIMEOUT)
-            return set_err(INMSOM_ETIMEOUT, "fused kernel: a bounded TMA wait timed out");
+        if (c->plan.last_flags & (fused::FLAG_TIMEOUT | fused::FLAG_SMEM)) return fused_flag_error(c, "fused kernel");
     } else {
         // nsub calls of barotropic_dynamics(dt, 1) keeping *_e: the first
         // substep of each call, run in place on the saved state, followed by
@@ -863,7 +868,7 @@ int inmsom_run_closure(inmsom_ctx *c, int nsub, double dt, int every, const floa
     CK(cudaEventRecord(c->ev1, c->stream));
     CKR(sync_stream(c));
     if (ms) CK(cudaEventElapsedTime(ms, c->ev0, c->ev1));
-    if (p.last_flags & fused::FLAG_TIMEOUT) return set_err(INMSOM_ETIMEOUT, "fused kernel: a bounded TMA wait timed out");
+    if (p.last_flags & (fused::FLAG_TIMEOUT | fused::FLAG_SMEM)) return fused_flag_error(c, "fused kernel");
     if (c->flags & INMSOM_GUARD) {
         long nbad = 0;
         CKR(run_guard(c, &nbad));
@@ -1203,8 +1208,7 @@ int inmsom_ens_run(inmsom_ens *e, int nsub, const double *dt, const double *rhs_
         if (fused::finish_steps(c->plan, c->stream))
             return set_err(INMSOM_ECUDA, "member %zu: %s", i, cudaGetErrorString(cudaGetLastError()));
         c->depths_current = false;
-        if (c->plan.last_flags & fused::FLAG_TIMEOUT)
-            return set_err(INMSOM_ETIMEOUT, "member %zu: a bounded TMA wait timed out", i);
+        if (c->plan.last_flags & (fused::FLAG_TIMEOUT | fused::FLAG_SMEM)) return fused_flag_error(c, "ensemble member");
     }
     if (ms) CK(cudaEventElapsedTime(ms, e->ev0, e->ev1));
     return INMSOM_OK;
@@ -1409,8 +1413,7 @@ int inmsom_strips_run(inmsom_strips *g, int nsub, double dt, const double *rhs_s
         if (fused::finish_steps(c->plan, c->stream))
             return set_err(INMSOM_ECUDA, "strip %d: %s", k, cudaGetErrorString(cudaGetLastError()));
         c->depths_current = false;
-        if (c->plan.last_flags & fused::FLAG_TIMEOUT)
-            return set_err(INMSOM_ETIMEOUT, "strip %d: a bounded TMA wait timed out", k);
+        if (c->plan.last_flags & (fused::FLAG_TIMEOUT | fused::FLAG_SMEM)) return fused_flag_error(c, "strip");
     }
     CK(cudaSetDevice(c0->device));
     CK(cudaEventSynchronize(g->ev1));

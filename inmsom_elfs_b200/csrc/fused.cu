@@ -150,7 +150,7 @@ struct Layout {
 };
 
 // ring slots: rows j-2..j+1 in use plus one row in flight for the plain
-// substep (15 CTAs per SM fit), two in flight where the registers hold the
+// substep (16 CTAs per SM fit), two in flight where the registers hold the
 // CTAs per SM to 12 (time-mean sums) or the slots are small (FP32 velocities)
 template <bool GEN, int MODE, bool F32 = false>
 __host__ __device__ constexpr int ring_slots()
@@ -160,17 +160,18 @@ __host__ __device__ constexpr int ring_slots()
 template <bool GEN, int MODE, bool F32 = false>
 constexpr size_t ring_bytes()
 {
-    return 128 + (size_t)ring_slots<GEN, MODE, F32>() * (Layout<GEN, F32>::SLOT_B + sizeof(uint64_t));
+    return (size_t)ring_slots<GEN, MODE, F32>() * (Layout<GEN, F32>::SLOT_B + sizeof(uint64_t));
 }
 
 // resident CTAs per SM the register budget is cut for: 16 one-warp CTAs
 // (4 warps per SM sub-partition, 128 registers) for the plain substep, 12
 // where the time-mean sums need more registers, 11 for the general variant,
 // and never more than the shared memory holds (228 KB per SM, 1 KB of it
-// reserved per CTA): 15 for the FP64 uniform ring of 5 slots, 11 for the
-// general one.  (A 6-slot ring holds 13 uniform CTAs: 4.5 % slower on the
-// 2048 x 1536 basin; reading the forcing from global memory instead of the
-// ring lets 16 fit but exposes the load latency: 5 % slower.)
+// reserved per CTA): 16 for the FP64 uniform ring of 5 slots, 11 for the
+// general one.  (A 6-slot ring holds 13 uniform CTAs: 6 % slower on the
+// 2048 x 1536 basin; 128 bytes of alignment slack per CTA leave room for 15:
+// 2 % slower; reading the forcing from global memory instead of the ring
+// exposes the load latency: 5 % slower.)
 template <bool GEN, int MODE, bool F32 = false>
 constexpr int min_ctas()
 {
@@ -709,7 +710,13 @@ __global__ void __launch_bounds__(NL, min_ctas<GEN, MODE, F32>()) k_substep(cons
     using L = Layout<GEN, F32>;
     constexpr int RING = ring_slots<GEN, MODE, F32>();
     extern __shared__ __align__(128) unsigned char smem_raw[];
-    unsigned char *ring = smem_raw + ((128u - (smem_addr(smem_raw) & 127u)) & 127u);
+    // the dynamic shared memory is the ring itself (no alignment slack, so
+    // that 16 uniform CTAs fit per SM): its TMA slots need a 128-byte base
+    unsigned char *ring = smem_raw;
+    if (smem_addr(smem_raw) & 127u) {
+        if (threadIdx.x == 0) atomicOr(p.flags, FLAG_SMEM);
+        return;
+    }
     uint64_t *mbar = reinterpret_cast<uint64_t *>(ring + RING * L::SLOT_B);
     const double rs = p.rs_dev ? p.rs_dev[*p.rs_base + p.rs_k] : p.rhs_scale;
     (void)substep_item<GEN, MODE, F32>(p, &p.tm_src, p.dst, rs, p.items[blockIdx.x], ring, mbar);

@@ -122,7 +122,10 @@ struct Plan {
     int last_variant = -1;          // 0 uniform, 1 general, 2 uniform with FP32 velocities (last launch)
 };
 
-enum : unsigned { FLAG_TIMEOUT = 1u, FLAG_GUARD = 2u };
+// status bits the fused kernel sets: a bounded wait gave up; a new value out
+// of range; the dynamic shared memory did not start on a 128-byte boundary
+// (the ring's TMA slots need it; the kernel then does nothing)
+enum : unsigned { FLAG_TIMEOUT = 1u, FLAG_GUARD = 2u, FLAG_SMEM = 4u };
 
 constexpr int NTABLE = 4;
 // item table of a launch: variant (0 uniform, 1 general) + 2 for the
