@@ -1041,6 +1041,11 @@ std::vector<int4> partition(const Plan &p, const Dom &d, int slots, int rows_per
     return items;
 }
 
+// waves of work items per table: one for the plain substep (measured on the
+// 2048 x 1536 basin: 2 waves +5.6 %, 1.5 waves +15 %), two for the
+// time-mean substeps (-1.9 % against one)
+int item_waves(int table) { return table >= 2 ? 2 : 1; }
+
 int upload_items(Plan &p, int v, const std::vector<int4> &items, cudaStream_t s)
 {
     p.generation++;
@@ -1338,7 +1343,7 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
     p.ocean = ocean_rows(p, d, masks[0]);
     for (int v = 0; v < NTABLE; v++) {
         p.occ[v] = occ[v] < 1 ? 1 : occ[v];
-        if (upload_items(p, v, partition(p, d, nsm * p.occ[v], 0), s)) return 1;
+        if (upload_items(p, v, partition(p, d, item_waves(v) * nsm * p.occ[v], 0), s)) return 1;
     }
     p.rows_per_item[0] = p.rows_per_item[1] = 0;
     return 0;
@@ -1456,7 +1461,7 @@ int repartition(Plan &p, const Dom &d, int rows_per_item, cudaStream_t s)
 {
     for (int v = 0; v < NTABLE; v++) {
         p.rows_per_item[v & 1] = rows_per_item;
-        if (upload_items(p, v, partition(p, d, p.nsm * p.occ[v], rows_per_item), s)) return 1;
+        if (upload_items(p, v, partition(p, d, item_waves(v) * p.nsm * p.occ[v], rows_per_item), s)) return 1;
     }
     return 0;
 }
