@@ -111,6 +111,7 @@ struct inmsom_ctx {
     // run_substeps as replays of a graph of RS_GROUP substeps
     cudaGraphExec_t rs_exec = nullptr;
     unsigned rs_gen = 0;
+    const double *rs_src = nullptr;  // state set the graph reads first (an odd run moves the state)
     double rs_dt = 0.0;
     double *d_rs = nullptr;          // RHS scale per substep of the run
     size_t rs_cap = 0;
@@ -607,11 +608,27 @@ constexpr int RS_GROUP = 50;   // substeps per graph replay (even: the state sta
 // inmsom_run_substeps on the fused path as replays of one captured graph of
 // RS_GROUP launches (launch gaps removed: 2-3 % on the 2048 x 1536 basin);
 // the RHS scale of every substep is read on the device at a counter the
-// graph advances.  The graph is recaptured when dt or the work items change.
+// graph advances.  The graph is recaptured when dt, the work items or the
+// state's set change.  FP32 velocity storage: the same with its kernel,
+// between the conversions to and from FP32.
 int run_substeps_graph(inmsom_ctx *c, int nsub, double dt, const double *rhs_scale)
 {
-    if (fused::prepare_steps(c->plan, c->dom, c->c, c->state, c->forc, c->stream))
+    const bool f32 = (c->flags & INMSOM_FP32_VELOCITY) != 0;
+    if (f32) {
+        const int rc = fused::prepare_steps_f32(c->plan, c->dom, c->c, c->state, c->forc, c->stream);
+        if (rc == 2)
+            return set_err(INMSOM_EUNSUPPORTED,
+                           "FP32 velocity storage needs a square uniform grid with uniform viscosity, drag and "
+                           "water flux");
+        if (rc) return set_err(INMSOM_ECUDA, "fused substeps: prepare failed: %s", cudaGetErrorString(cudaGetLastError()));
+    } else if (fused::prepare_steps(c->plan, c->dom, c->c, c->state, c->forc, c->stream)) {
         return set_err(INMSOM_ECUDA, "fused substeps: prepare failed: %s", cudaGetErrorString(cudaGetLastError()));
+    }
+    auto launch = [&](int n) {
+        return f32 ? fused::launch_steps_f32(c->plan, c->dom, c->c, dt, n, c->d_rs, c->d_base, nullptr, c->state,
+                                             c->stream)
+                   : fused::launch_steps(c->plan, c->dom, c->c, dt, n, c->d_rs, c->d_base, c->state, c->stream);
+    };
     if (!c->d_base) CK(cudaMalloc(&c->d_base, sizeof(int)));
     if ((size_t)nsub > c->rs_cap) {
         if (c->rs_exec) cudaGraphExecDestroy(c->rs_exec);
@@ -627,13 +644,12 @@ int run_substeps_graph(inmsom_ctx *c, int nsub, double dt, const double *rhs_sca
         for (int k = 0; k < nsub; k++) rs[k] = rhs_scale[k];
     CK(cudaMemcpyAsync(c->d_rs, rs.data(), (size_t)nsub * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(c->d_base, 0, sizeof(int), c->stream));
-    if (!c->rs_exec || c->rs_gen != c->plan.generation || c->rs_dt != dt) {
+    if (!c->rs_exec || c->rs_gen != c->plan.generation || c->rs_dt != dt || c->rs_src != c->state[0]) {
         if (c->rs_exec) cudaGraphExecDestroy(c->rs_exec);
         c->rs_exec = nullptr;
         cudaGraph_t g = nullptr;
         CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        const int lrc = fused::launch_steps(c->plan, c->dom, c->c, dt, RS_GROUP, c->d_rs, c->d_base, c->state,
-                                            c->stream);
+        const int lrc = launch(RS_GROUP);
         if (lrc == 0) k_advance<<<1, 1, 0, c->stream>>>(c->d_base, RS_GROUP);
         const cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
         if (lrc || ce != cudaSuccess) {
@@ -645,13 +661,14 @@ int run_substeps_graph(inmsom_ctx *c, int nsub, double dt, const double *rhs_sca
         if (ie != cudaSuccess) return set_err(INMSOM_ECUDA, "fused substeps: %s", cudaGetErrorString(ie));
         c->rs_gen = c->plan.generation;
         c->rs_dt = dt;
+        c->rs_src = c->state[0];
     }
     const int groups = nsub / RS_GROUP, rest = nsub % RS_GROUP;
     for (int gi = 0; gi < groups; gi++) CK(cudaGraphLaunch(c->rs_exec, c->stream));
-    if (rest && fused::launch_steps(c->plan, c->dom, c->c, dt, rest, c->d_rs, c->d_base, c->state, c->stream))
-        return set_err(INMSOM_ECUDA, "fused substeps: launch failed");
-    if (fused::finish_steps(c->plan, c->stream))
-        return set_err(INMSOM_ECUDA, "fused substeps: %s", cudaGetErrorString(cudaGetLastError()));
+    if (rest && launch(rest)) return set_err(INMSOM_ECUDA, "fused substeps: launch failed");
+    const int frc = f32 ? fused::finish_steps_f32(c->plan, c->dom, c->state, c->stream)
+                        : fused::finish_steps(c->plan, c->stream);
+    if (frc) return set_err(INMSOM_ECUDA, "fused substeps: %s", cudaGetErrorString(cudaGetLastError()));
     return INMSOM_OK;
 }
 
@@ -667,7 +684,7 @@ int inmsom_run_substeps(inmsom_ctx *c, int nsub, double dt, const double *rhs_sc
     if ((c->flags & INMSOM_FP32_VELOCITY) && !c->fused_ok)
         return set_err(INMSOM_EUNSUPPORTED, "FP32 velocity storage needs the fused path (%s)", c->fused_reason);
     CK(cudaEventRecord(c->ev0, c->stream));
-    if (c->fused_ok && !(c->flags & INMSOM_FP32_VELOCITY) && nsub >= 2 * RS_GROUP) {
+    if (c->fused_ok && nsub >= 2 * RS_GROUP) {
         CKR(run_substeps_graph(c, nsub, dt, rhs_scale));
         c->depths_current = false;
         if (c->plan.last_flags & (fused::FLAG_TIMEOUT | fused::FLAG_SMEM)) return fused_flag_error(c, "fused kernel");
@@ -1056,6 +1073,7 @@ struct inmsom_ens {
     cudaGraphExec_t exec = nullptr;
     std::vector<double> graph_dt;          // dt per member the graph was captured with
     std::vector<unsigned> graph_gen;       // plan generation per member at capture
+    std::vector<const double *> graph_src; // state set per member at capture (an odd run moves the state)
     double *d_rs = nullptr;                // RHS scale per substep of the run
     size_t rs_cap = 0;
     int *d_base = nullptr;                 // first substep of the next group
@@ -1069,6 +1087,7 @@ void ens_drop_graph(inmsom_ens *e)
     e->exec = nullptr;
     e->graph_dt.clear();
     e->graph_gen.clear();
+    e->graph_src.clear();
 }
 
 int ens_capture(inmsom_ens *e, const double *dt)
@@ -1106,6 +1125,7 @@ int ens_capture(inmsom_ens *e, const double *dt)
     if (ce != cudaSuccess) return set_err(INMSOM_ECUDA, "ensemble graph instantiate: %s", cudaGetErrorString(ce));
     e->graph_dt.assign(dt, dt + e->m.size());
     for (auto *c : e->m) e->graph_gen.push_back(c->plan.generation);
+    for (auto *c : e->m) e->graph_src.push_back(c->state[0]);
     return INMSOM_OK;
 }
 
@@ -1113,7 +1133,9 @@ bool ens_graph_current(const inmsom_ens *e, const double *dt)
 {
     if (!e->exec) return false;
     for (size_t i = 0; i < e->m.size(); i++)
-        if (e->graph_dt[i] != dt[i] || e->graph_gen[i] != e->m[i]->plan.generation) return false;
+        if (e->graph_dt[i] != dt[i] || e->graph_gen[i] != e->m[i]->plan.generation ||
+            e->graph_src[i] != e->m[i]->state[0])
+            return false;
     return true;
 }
 

@@ -60,9 +60,9 @@ struct alignas(64) Params {
     CUtensorMap tm_src;    // source state set {pitch, rows, 6 fields}, box {SEG, 1, 6}
     CUtensorMap tm_stat;   // static block, box {SEG, 1, Layout::NS}
     CUtensorMap tm_ssh;    // FP32-velocity kernel: the source set's SSH fields, box {SEG, 1, 2}
+    CUtensorMap tm_rhs;    // FP32-velocity kernel: RHSx, RHSy in FP32, box {VSEG, 1, 2}
     double *dst[NSET];
     float *vdst[4];        // FP32-velocity kernel: u, up, v, vp of the destination
-    const float *rx32, *ry32;   // FP32-velocity kernel: RHSx, RHSy
     double *acc[4];
     const uint32_t *bits;
     const RowCoef *rows;
@@ -133,7 +133,8 @@ __device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
 // Ring slot layout.  FP64 state: [6 state fields][static fields][RowCoef]
 // [mask bits].  FP32 velocities (uniform variant only): [u up v vp as FP32,
 // VSEG columns from g0 rounded down to a multiple of 4, so that the TMA
-// x-coordinate is 16-byte aligned for 4-byte elements][ssh sshp][H][bits].
+// x-coordinate is 16-byte aligned for 4-byte elements][ssh sshp][H][RHSx
+// RHSy as FP32, the same columns as the velocities][bits].
 template <bool GEN, bool F32 = false>
 struct Layout {
     static_assert(!(GEN && F32), "FP32 velocities exist in the uniform variant only");
@@ -142,10 +143,11 @@ struct Layout {
     static constexpr int NS = F32 ? 1 : (GEN ? 6 : 3);                   // static fields in a slot
     static constexpr int STAT_OFF = F32 ? (SSH_OFF + 2 * SEG * 8 + 127) / 128 * 128 : 1792;
     static constexpr int COEF_OFF = STAT_OFF + NS * SEG * 8;             // general variant: RowCoef
-    static constexpr int BITS_OFF = COEF_OFF + (GEN ? (int)sizeof(RowCoef) : 0);
+    static constexpr int RHS_OFF = F32 ? (COEF_OFF + 127) / 128 * 128 : COEF_OFF;   // FP32 RHSx, RHSy
+    static constexpr int BITS_OFF = F32 ? RHS_OFF + 2 * VSEG * 4 : COEF_OFF + (GEN ? (int)sizeof(RowCoef) : 0);
     static constexpr int SLOT_B = (BITS_OFF + 32 + 127) / 128 * 128;
     static constexpr uint32_t row_tx =
-        (uint32_t)((F32 ? 4 * VSEG * 4 + 2 * SEG * 8 : NSET * SEG * 8) + NS * SEG * 8 +
+        (uint32_t)((F32 ? 4 * VSEG * 4 + 2 * SEG * 8 + 2 * VSEG * 4 : NSET * SEG * 8) + NS * SEG * 8 +
                    (GEN ? (int)sizeof(RowCoef) : 0) + 32);
 };
 
@@ -181,6 +183,9 @@ constexpr int min_ctas()
 }
 static_assert(NSET * SEG * 8 <= 1792, "state segment overlaps the static segment");
 static_assert(Layout<false>::COEF_OFF % 16 == 0 && Layout<true>::BITS_OFF % 16 == 0, "bulk copy alignment");
+static_assert(Layout<false, true>::RHS_OFF % 128 == 0 && Layout<false, true>::SSH_OFF % 128 == 0 &&
+                  Layout<false, true>::STAT_OFF % 128 == 0,
+              "TMA destinations of the FP32 slot");
 static_assert(Layout<false, true>::BITS_OFF % 16 == 0 && (Layout<false, true>::VSEG * 4) % 16 == 0,
               "FP32 segment alignment");
 
@@ -190,8 +195,8 @@ static_assert(Layout<false, true>::BITS_OFF % 16 == 0 && (Layout<false, true>::V
 // general variant, the row's coefficients (1-D bulk copies).  No branch.
 template <bool GEN, bool F32 = false>
 __device__ __forceinline__ void issue_row(unsigned char *slot, uint64_t *bar, const CUtensorMap *src,
-                                          const CUtensorMap *stat, const CUtensorMap *ssh, const void *coef,
-                                          const void *bits, int x, int row)
+                                          const CUtensorMap *stat, const CUtensorMap *ssh, const CUtensorMap *rhs,
+                                          const void *coef, const void *bits, int x, int row)
 {
     using L = Layout<GEN, F32>;
     const int z = 0;
@@ -209,12 +214,15 @@ __device__ __forceinline__ void issue_row(unsigned char *slot, uint64_t *bar, co
             " [%7], [%8, {%9, %5, %10}], [%0];\n\t"
             "@P cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
             " [%11], [%12, {%9, %5, %6}], [%0];\n\t"
+            "@P cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes"
+            " [%15], [%16, {%4, %5, %6}], [%0];\n\t"
             "@P cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%13], [%14], 32, [%0];\n\t"
             "}" ::"r"(smem_addr(bar)),
             "r"(L::row_tx), "r"(smem_addr(slot)), "l"(reinterpret_cast<uint64_t>(src)), "r"(x4), "r"(row), "r"(z),
             "r"(smem_addr(slot + L::SSH_OFF)), "l"(reinterpret_cast<uint64_t>(ssh)), "r"(x), "r"(zs),
             "r"(smem_addr(slot + L::STAT_OFF)), "l"(reinterpret_cast<uint64_t>(stat)),
-            "r"(smem_addr(slot + L::BITS_OFF)), "l"(bits)
+            "r"(smem_addr(slot + L::BITS_OFF)), "l"(bits),
+            "r"(smem_addr(slot + L::RHS_OFF)), "l"(reinterpret_cast<uint64_t>(rhs))
             : "memory");
     } else if constexpr (GEN) {
         asm volatile(
@@ -361,7 +369,7 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
 #define CF(o, x) (reinterpret_cast<const RowCoef *>(ring + (o) + L::COEF_OFF)->x)
 
     auto issue = [&](int row, int slot) {
-        issue_row<GEN, F32>(ring + slot * L::SLOT_B, &mbar[slot], tm_src, &p.tm_stat, &p.tm_ssh, p.rows + row,
+        issue_row<GEN, F32>(ring + slot * L::SLOT_B, &mbar[slot], tm_src, &p.tm_stat, &p.tm_ssh, &p.tm_rhs, p.rows + row,
                        p.bits + (size_t)row * p.bm_words + wbase, g0, row);
     };
     auto mask2 = [&](int o) -> uint32_t {   // bits: lu(k), lu(k+1)
@@ -471,8 +479,10 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
                 n.cor = p.cor[j];
             }
             // RHS: from the ring (FP64 state) or from the FP32 copy
-            const double rx = F32 ? (double)p.rx32[gi] : AT(o_0, T_RX, 0);
-            const double ry = F32 ? (double)p.ry32[gi] : AT(o_0, T_RY, 0);
+            const double rx = F32 ? (double)*reinterpret_cast<const float *>(lane32 + o_0 + L::RHS_OFF)
+                                  : AT(o_0, T_RX, 0);
+            const double ry = F32 ? (double)*reinterpret_cast<const float *>(lane32 + o_0 + L::RHS_OFF + L::VSEG * 4)
+                                  : AT(o_0, T_RY, 0);
             n.Ru = rx * rs + slx - rdu * AS(o_0, S_UP, 0) * au * hu;
             n.Rv = ry * rs + sly - rdv * AS(o_0, S_VP, 0) * av * hv;
             if (ACC) {
@@ -1044,7 +1054,7 @@ std::vector<int4> partition(const Plan &p, const Dom &d, int slots, int rows_per
 // waves of work items per table: one for the plain substep (measured on the
 // 2048 x 1536 basin: 2 waves +5.6 %, 1.5 waves +15 %), two for the
 // time-mean substeps (-1.9 % against one)
-int item_waves(int table) { return table >= 2 ? 2 : 1; }
+int item_waves(int table) { return table == 2 || table == 3 ? 2 : 1; }
 
 int upload_items(Plan &p, int v, const std::vector<int4> &items, cudaStream_t s)
 {
@@ -1119,6 +1129,9 @@ int ensure_f32(Plan &p, const Dom &d, cudaStream_t s)
     if (encode_fields(enc, &p.tm_stat_f32, p.stat, d, p.fstride, NSTAT, Layout<false, true>::NS)) return 1;
     p.stat_box_f32 = Layout<false, true>::NS;
     if (cudaMalloc(&p.stat32, 2 * fb) != cudaSuccess) return 1;
+    if (cudaMemsetAsync(p.stat32, 0, 2 * fb, s) != cudaSuccess) return 1;
+    // RHSx, RHSy in FP32: the box brings both fields, as the slot layout holds
+    if (encode_fields(enc, &p.tm_rhs32, p.stat32, d, p.fstride, 2, 2, true)) return 1;
     return 0;
 }
 
@@ -1330,7 +1343,7 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
     p.nsm = nsm;
     // one item table per variant for the plain substep and one for the
     // time-mean substeps, each one wave of the kernel's resident CTAs
-    int occ[NTABLE] = {1, 1, 1, 1};
+    int occ[NTABLE] = {1, 1, 1, 1, 1};
     cudaError_t oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[0], k_substep<false, 3>, NL,
                                                                    ring_bytes<false, 3>());
     if (oe == cudaSuccess)
@@ -1339,6 +1352,9 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
         oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[2], k_substep<false, 5>, NL, ring_bytes<false, 5>());
     if (oe == cudaSuccess)
         oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[3], k_substep<true, 5>, NL, ring_bytes<true, 5>());
+    if (oe == cudaSuccess)
+        oe = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ[4], k_substep<false, 3, true>, NL,
+                                                           ring_bytes<false, 3, true>());
     if (oe != cudaSuccess) return 1;
     p.ocean = ocean_rows(p, d, masks[0]);
     for (int v = 0; v < NTABLE; v++) {
@@ -1393,6 +1409,14 @@ int dynamics(Plan &p, const Dom &d, const Consts &c, double tau, int nstep, doub
 int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt, const double *rhs_scale,
                  double *state[6], double *forc[6], cudaStream_t s)
 {
+    if (p.f32) {
+        // FP32 velocity storage: u, up, v, vp of the state and ping-pong
+        // sets in FP32 for the run, SSH in the FP64 sets
+        const int rc = prepare_steps_f32(p, d, c, state, forc, s);
+        if (rc) return rc;
+        if (launch_steps_f32(p, d, c, dt, nsub, nullptr, nullptr, rhs_scale, state, s)) return 1;
+        return finish_steps_f32(p, d, state, s);
+    }
     Forcing f;
     if (forcing_mode(p, d, c, forc, s, f)) return 1;
     if (!p.buffers_synced && sync_buffers(p, state, s)) return 1;
@@ -1404,46 +1428,6 @@ int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt, co
     q.gam = c.ts / 2.0;   // nstep = 1
     q.c4 = 0.25;
     for (int k = 0; k < 4; k++) q.acc[k] = nullptr;
-    if (p.f32) {
-        // FP32 velocity storage: u, up, v, vp of the state and ping-pong
-        // sets in FP32 for the run, SSH in the FP64 sets
-        if (gen) return 2;
-        if (ensure_f32(p, d, s)) return 1;
-        const int blocks = 4 * p.nsm;
-        const int a = set_index(p, state[0]), b = set_index(p, p.buf[0][0]);
-        if (a < 0 || b < 0) return 1;
-        k_to_f32<<<blocks, 256, 0, s>>>(p.set[a], p.vset[a], 4 * p.fstride);
-        k_to_f32<<<blocks, 256, 0, s>>>(p.set[b], p.vset[b], 4 * p.fstride);
-        k_to_f32<<<blocks, 256, 0, s>>>(p.stat + T_RX * p.fstride, p.stat32, 2 * p.fstride);
-        q.rx32 = p.stat32;
-        q.ry32 = p.stat32 + p.fstride;
-        // the ring's static segment holds Layout<false, true>::NS fields:
-        // the map must bring exactly that many
-        if (p.stat_box_f32 != Layout<false, true>::NS) return 1;
-        q.tm_stat = p.tm_stat_f32;
-        for (int step = 0; step < nsub; step++) {
-            const int si = (step & 1) ? b : a, di = (step & 1) ? a : b;
-            q.tm_src = p.tm_vel[si];
-            q.tm_ssh = p.tm_ssh[si];
-            for (int k = 0; k < NSET; k++) q.dst[k] = p.set[di] + k * p.fstride;
-            for (int k = 0; k < 4; k++) q.vdst[k] = p.vset[di] + k * p.fstride;
-            q.rhs_scale = rhs_scale ? rhs_scale[step] : 1.0;
-            p.last_variant = 2;
-            k_substep<false, 3, true><<<dim3(p.nitems[0]), NL, ring_bytes<false, 3, true>(), s>>>(q);
-            if (cudaGetLastError() != cudaSuccess) return 1;
-        }
-        if (nsub & 1)
-            for (int k = 0; k < 6; k++) std::swap(state[k], p.buf[0][k]);
-        const int fi = set_index(p, state[0]);
-        k_vel_from_f32<<<blocks, 256, 0, s>>>(p.vset[fi], p.set[fi], p.lu, d.pitch, p.fstride,
-                                              d.ny_start - d.bnd_y1, d.ny_end - d.bnd_y1,
-                                              d.nx_start - d.bnd_x1 + d.xoff, d.nx_end - d.bnd_x1 + d.xoff);
-        if (cudaGetLastError() != cudaSuccess) return 1;
-        unsigned flags = 0;
-        if (read_flags(p, s, &flags)) return 1;
-        p.last_flags = flags;
-        return 0;
-    }
     for (int step = 0; step < nsub; step++) {
         if (set_io(p, q, (step & 1) ? p.buf[0] : state, (step & 1) ? state : p.buf[0])) return 1;
         q.rhs_scale = rhs_scale ? rhs_scale[step] : 1.0;
@@ -1455,6 +1439,68 @@ int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt, co
     if (read_flags(p, s, &flags)) return 1;
     p.last_flags = flags;
     return 0;
+}
+
+int prepare_steps_f32(Plan &p, const Dom &d, const Consts &c, double *state[6], double *forc[6], cudaStream_t s)
+{
+    if (prepare_steps(p, d, c, state, forc, s)) return 1;
+    if (p.prep_gen) return 2;
+    if (ensure_f32(p, d, s)) return 1;
+    const int blocks = 4 * p.nsm;
+    const int a = set_index(p, state[0]), b = set_index(p, p.buf[0][0]);
+    if (a < 0 || b < 0) return 1;
+    k_to_f32<<<blocks, 256, 0, s>>>(p.set[a], p.vset[a], 4 * p.fstride);
+    k_to_f32<<<blocks, 256, 0, s>>>(p.set[b], p.vset[b], 4 * p.fstride);
+    k_to_f32<<<blocks, 256, 0, s>>>(p.stat + T_RX * p.fstride, p.stat32, 2 * p.fstride);
+    return cudaGetLastError() != cudaSuccess;
+}
+
+int launch_steps_f32(Plan &p, const Dom &d, const Consts &c, double dt, int nsteps, const double *rs_dev,
+                     const int *rs_base, const double *rs_host, double *state[6], cudaStream_t s)
+{
+    if (!p.prepared || p.prep_gen) return 1;
+    // the ring's static segment holds Layout<false, true>::NS fields: the
+    // map must bring exactly that many
+    if (p.stat_box_f32 != Layout<false, true>::NS) return 1;
+    Forcing f{true, p.prep_mu0, p.prep_rd0, p.prep_wq0};
+    Params q = base_params(p, d, c, f, 0);
+    set_times(q, 2.0 * dt, p);
+    q.gam = c.ts / 2.0;   // nstep = 1
+    q.c4 = 0.25;
+    for (int k = 0; k < 4; k++) q.acc[k] = nullptr;
+    q.tm_rhs = p.tm_rhs32;
+    q.tm_stat = p.tm_stat_f32;
+    q.items = p.items[TABLE_F32];
+    q.rs_dev = rs_dev;
+    q.rs_base = rs_base;
+    const int a = set_index(p, state[0]), b = set_index(p, p.buf[0][0]);
+    if (a < 0 || b < 0) return 1;
+    for (int step = 0; step < nsteps; step++) {
+        const int si = (step & 1) ? b : a, di = (step & 1) ? a : b;
+        q.tm_src = p.tm_vel[si];
+        q.tm_ssh = p.tm_ssh[si];
+        for (int k = 0; k < NSET; k++) q.dst[k] = p.set[di] + k * p.fstride;
+        for (int k = 0; k < 4; k++) q.vdst[k] = p.vset[di] + k * p.fstride;
+        q.rhs_scale = rs_host ? rs_host[step] : 1.0;
+        q.rs_k = step;
+        p.last_variant = 2;
+        k_substep<false, 3, true><<<dim3(p.nitems[TABLE_F32]), NL, ring_bytes<false, 3, true>(), s>>>(q);
+        if (cudaGetLastError() != cudaSuccess) return 1;
+    }
+    if (nsteps & 1)
+        for (int k = 0; k < 6; k++) std::swap(state[k], p.buf[0][k]);
+    return 0;
+}
+
+int finish_steps_f32(Plan &p, const Dom &d, double *state[6], cudaStream_t s)
+{
+    const int fi = set_index(p, state[0]);
+    if (fi < 0) return 1;
+    k_vel_from_f32<<<4 * p.nsm, 256, 0, s>>>(p.vset[fi], p.set[fi], p.lu, d.pitch, p.fstride,
+                                             d.ny_start - d.bnd_y1, d.ny_end - d.bnd_y1,
+                                             d.nx_start - d.bnd_x1 + d.xoff, d.nx_end - d.bnd_x1 + d.xoff);
+    if (cudaGetLastError() != cudaSuccess) return 1;
+    return finish_steps(p, s);
 }
 
 int repartition(Plan &p, const Dom &d, int rows_per_item, cudaStream_t s)

@@ -77,9 +77,10 @@ struct Plan {
     int outw = 30;            // output columns per CTA
     int nstrips = 0;
     // work-item tables (item_table): uniform and general variant, plain and
-    // time-mean substeps (their kernels hold different numbers of CTAs per SM)
-    int nitems[4] = {0, 0, 0, 0};
-    int4 *items[4] = {nullptr, nullptr, nullptr, nullptr};   // {g0, first row, end row, 0} per item
+    // time-mean substeps, and the FP32-velocity substep (their kernels hold
+    // different numbers of CTAs per SM)
+    int nitems[5] = {0, 0, 0, 0, 0};
+    int4 *items[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};   // {g0, first row, end row, 0} per item
     bool uni = false;         // metrics all equal one spacing d (square uniform grid)
     double d = 0.0;           // that spacing
     long long min_pitch = 0;  // device row pitch the strips need
@@ -94,7 +95,7 @@ struct Plan {
     long long fstride = 0;          // doubles between the fields of a block
     CUtensorMap tm_set[3];          // box {36, 1, 6} over each state set
     CUtensorMap tm_stat[2];         // box {36, 1, 3 | 6} over the static block
-    int occ[4] = {0, 0, 0, 0};      // resident CTAs per SM, per item table
+    int occ[5] = {0, 0, 0, 0, 0};   // resident CTAs per SM, per item table
     std::vector<uint8_t> ocean;     // per strip and interior row: any written column is ocean
     int rows_per_item[2] = {0, 0};  // 0: one wave of items by cost; else rows per item
     unsigned generation = 0;        // bumped whenever buffers or work items change
@@ -110,6 +111,7 @@ struct Plan {
     CUtensorMap tm_vel[3];          // box {40, 1, 4} FP32 over each velocity set
     CUtensorMap tm_ssh[3];          // box {36, 1, 2} over the SSH fields of each state set
     CUtensorMap tm_stat_f32;        // box {36, 1, 1}: H alone, for the FP32-velocity ring
+    CUtensorMap tm_rhs32;           // box {40, 1, 2} FP32 over stat32: RHSx, RHSy
     int stat_box[2] = {0, 0};       // static fields in tm_stat[v], checked against the ring layout
     int stat_box_f32 = 0;
     double *d_uniform = nullptr;    // per-block min/max of mu, rdis, wflux
@@ -127,8 +129,9 @@ struct Plan {
 // (the ring's TMA slots need it; the kernel then does nothing)
 enum : unsigned { FLAG_TIMEOUT = 1u, FLAG_GUARD = 2u, FLAG_SMEM = 4u };
 
-constexpr int NTABLE = 4;
-// item table of a launch: variant (0 uniform, 1 general) + 2 for the
+constexpr int NTABLE = 5;
+constexpr int TABLE_F32 = 4;   // the FP32-velocity substep's items
+// item table of an FP64 launch: variant (0 uniform, 1 general) + 2 for the
 // substeps that accumulate time means (mode % 3 != 0)
 inline int item_table(bool gen, int mode) { return (gen ? 1 : 0) + (mode % 3 != 0 ? 2 : 0); }
 
@@ -167,6 +170,17 @@ int prepare_steps(Plan &p, const Dom &d, const Consts &c, double *state[6], doub
 int launch_steps(Plan &p, const Dom &d, const Consts &c, double dt, int nsteps, const double *rs_dev,
                  const int *rs_base, double *state[6], cudaStream_t s, double rs_host = 1.0);
 int finish_steps(Plan &p, cudaStream_t s);
+// The FP32-velocity run in the same parts: prepare_steps_f32 also converts
+// the state, the other ping-pong set and RHSx/RHSy to FP32 (returns 2 if the
+// grid needs the general variant); launch_steps_f32 enqueues nsteps
+// substeps, the RHS scale of launch k being rs_dev[*rs_base + k] or
+// rs_host[k] (or 1); finish_steps_f32 writes the velocities back to the
+// FP64 state and reads the status bits.
+int prepare_steps_f32(Plan &p, const Dom &d, const Consts &c, double *state[6], double *forc[6],
+                      cudaStream_t s);
+int launch_steps_f32(Plan &p, const Dom &d, const Consts &c, double dt, int nsteps, const double *rs_dev,
+                     const int *rs_base, const double *rs_host, double *state[6], cudaStream_t s);
+int finish_steps_f32(Plan &p, const Dom &d, double *state[6], cudaStream_t s);
 // re-cut the work items: rows_per_item = 0 for one wave of items by cost
 int repartition(Plan &p, const Dom &d, int rows_per_item, cudaStream_t s);
 void free_plan(Plan &p);

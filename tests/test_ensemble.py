@@ -73,3 +73,25 @@ def test_ensemble_rejects_odd_group(gpu):
         s.load_state()
         with pytest.raises(InmsomError):
             gpu.Ensemble([s], group=3)
+
+
+def test_ensemble_odd_runs_back_to_back(gpu):
+    """An odd run moves each member's state to its other ping-pong set; the
+    next run must notice (recapture) and continue from there."""
+    bs = _members(gpu)
+    scale = basins.wind_cycle(10, 2.0, t0=100.0, period=600.0)
+    ref = [_alone(gpu, b, 10, scale) for b in bs]
+    cps = [b.copy() for b in bs]
+    solvers = [gpu.BarotropicSolver(b, resident=True) for b in cps]
+    for s in solvers:
+        s.load_state()
+    dts = [b.dt for b in cps]
+    with gpu.Ensemble(solvers, group=4) as e:
+        e.run(5, dts, scale[:5])       # one graph launch and one direct substep
+        e.run(5, dts, scale[5:])
+    for s in solvers:
+        s.sync_to_host()
+        s.close()
+    for r, g in zip(ref, cps):
+        for k in r.state:
+            assert np.array_equal(r.state[k], g.state[k]), k
