@@ -38,10 +38,11 @@ extern "C" {
 #define INMSOM_RESIDENT      0x1u /* state, depths and scratch stay on the device
                                      between calls; each barotropic_dynamics call
                                      copies in only the forcing (RHSx, RHSy, wflux,
-                                     mu, mu4, rdis) and copies out only the
-                                     time-mean outputs (ubrtr_i, vbrtr_i,
-                                     ssh4gradx, ssh4grady).  Without it every
-                                     call copies every array argument in and out. */
+                                     mu, rdis, and mu4 when ksw4 > 0) and copies
+                                     out only the time-mean outputs (ubrtr_i,
+                                     vbrtr_i, ssh4gradx, ssh4grady).  Without it
+                                     every call copies every array argument in
+                                     and out. */
 #define INMSOM_FORCE_GENERAL 0x2u /* always use the per-loop kernels (exact
                                      reference rounding) even when the fused
                                      streaming kernel is eligible               */
@@ -311,6 +312,36 @@ typedef struct inmsom_strips inmsom_strips;
 int inmsom_strips_create(inmsom_strips **strips, inmsom_ctx *const *ctxs, int n);
 int inmsom_strips_run(inmsom_strips *strips, int nsub, double dt, const double *rhs_scale, float *ms);
 int inmsom_strips_destroy(inmsom_strips *strips);
+
+/* Row strips with one process (rank) per GPU, replacing syncborder_real8's
+ * MPI exchange (Modules/mod_mpi_parallel_tools.f90:179-252) for a 1 x P
+ * process grid: each rank owns the context of its strip (its local bounds
+ * from mpi_array_boundary_definition, Control/init_arrays.f90:21-88, with
+ * two halo rows each side) and, per substep, calls inmsom_step_launch, packs
+ * the two rows each neighbour needs, moves them with its own transport
+ * (NCCL send/recv of the device buffers, ordered on inmsom_gpu_stream) and
+ * unpacks what it received into its halo rows.  One exchange per substep
+ * gives the single-domain result bit for bit (the fused kernel recomputes
+ * its halo rows' intermediates).  FP64 state, fused path only.
+ *   inmsom_step_begin: classify and stage the forcing for a run of substeps
+ *     (synchronises the stream);
+ *   inmsom_step_launch: enqueue one substep with RHS scale rhs_scale;
+ *   inmsom_halo_pack: side 0 the two southernmost interior rows, side 1 the
+ *     two northernmost, of the six state fields into buf (device,
+ *     INMSOM_HALO_DOUBLES(pitch) doubles, field-major, rows of `pitch`
+ *     doubles; pitch from inmsom_gpu_pitch);
+ *   inmsom_halo_unpack: buf into the two southern (side 0) or northern
+ *     (side 1) halo rows;
+ *   inmsom_step_end: wait for the stream and read the kernel status. */
+#define INMSOM_HALO_DOUBLES(pitch) (12LL * (long long)(pitch))
+int inmsom_step_begin(inmsom_ctx *ctx);
+int inmsom_step_launch(inmsom_ctx *ctx, double dt, double rhs_scale);
+int inmsom_halo_pack(inmsom_ctx *ctx, int side, void *buf);
+int inmsom_halo_unpack(inmsom_ctx *ctx, int side, const void *buf);
+int inmsom_step_end(inmsom_ctx *ctx);
+/* the context's cudaStream_t, and its device row pitch in doubles */
+void *inmsom_gpu_stream(inmsom_ctx *ctx);
+long long inmsom_gpu_pitch(inmsom_ctx *ctx);
 
 /* Learned subgrid momentum closure (no counterpart in the reference; it
  * stands in for the Laplacian viscosity of uv_diff2 on coarse grids): an

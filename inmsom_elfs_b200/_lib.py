@@ -27,6 +27,8 @@ EXPORTS = (
     "inmsom_ens_destroy", "inmsom_strips_create", "inmsom_strips_run", "inmsom_strips_destroy",
     "inmsom_mlp_pack", "inmsom_mlp_forward", "inmsom_mlp_grad", "inmsom_mlp_adam", "inmsom_mlp_batch_indices",
     "inmsom_closure_features", "inmsom_run_closure", "inmsom_closure_tendency", "inmsom_gpu_last_phases",
+    "inmsom_step_begin", "inmsom_step_launch", "inmsom_halo_pack", "inmsom_halo_unpack", "inmsom_step_end",
+    "inmsom_gpu_stream", "inmsom_gpu_pitch",
 )
 
 # include/inmsom_gpu.h: INMSOM_MLP_*
@@ -115,11 +117,20 @@ def load() -> ctypes.CDLL:
     lib.inmsom_closure_tendency.argtypes = [VP, VP, VP, NP, DP, DP]
     FPP = ctypes.POINTER(ctypes.c_float)
     lib.inmsom_gpu_last_phases.argtypes = [VP, FPP, FPP, FPP]
+    lib.inmsom_step_begin.argtypes = [VP]
+    lib.inmsom_step_launch.argtypes = [VP, d, d]
+    lib.inmsom_halo_pack.argtypes = [VP, i, VP]
+    lib.inmsom_halo_unpack.argtypes = [VP, i, VP]
+    lib.inmsom_step_end.argtypes = [VP]
+    lib.inmsom_gpu_stream.argtypes = [VP]
+    lib.inmsom_gpu_pitch.argtypes = [VP]
     lib.inmsom_diag_noalloc.argtypes = ([ctypes.POINTER(CBounds), ctypes.POINTER(CConsts),
                                          ctypes.c_longlong] + [VP] * 16 + [VP])
     for name in EXPORTS:
-        if name != "inmsom_gpu_last_error":
+        if name not in ("inmsom_gpu_last_error", "inmsom_gpu_stream", "inmsom_gpu_pitch"):
             getattr(lib, name).restype = i
+    lib.inmsom_gpu_stream.restype = VP
+    lib.inmsom_gpu_pitch.restype = ctypes.c_longlong
     _lib = lib
     return lib
 

@@ -1443,6 +1443,75 @@ int inmsom_strips_run(inmsom_strips *g, int nsub, double dt, const double *rhs_s
     return INMSOM_OK;
 }
 
+int inmsom_step_begin(inmsom_ctx *c)
+{
+    CKR(ensure_grid(c));
+    if (!c->state_on_device) return set_err(INMSOM_EARG, "no resident state: call inmsom_load_state first");
+    if (!c->fused_ok) return set_err(INMSOM_EUNSUPPORTED, "fused path not eligible (%s)", c->fused_reason);
+    if (c->flags & INMSOM_FP32_VELOCITY) return set_err(INMSOM_EUNSUPPORTED, "row strips keep an FP64 state");
+    if (fused::prepare_steps(c->plan, c->dom, c->c, c->state, c->forc, c->stream))
+        return set_err(INMSOM_ECUDA, "prepare failed: %s", cudaGetErrorString(cudaGetLastError()));
+    return INMSOM_OK;
+}
+
+int inmsom_step_launch(inmsom_ctx *c, double dt, double rhs_scale)
+{
+    if (!c) return set_err(INMSOM_EARG, "context is NULL");
+    if (!c->plan.prepared) return set_err(INMSOM_EARG, "inmsom_step_begin has not been called");
+    if (!(dt > 0.0)) return set_err(INMSOM_EARG, "dt must be > 0");
+    CK(cudaSetDevice(c->device));
+    if (fused::launch_steps(c->plan, c->dom, c->c, dt, 1, nullptr, nullptr, c->state, c->stream, rhs_scale))
+        return set_err(INMSOM_ECUDA, "substep launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    c->depths_current = false;
+    return INMSOM_OK;
+}
+
+namespace {
+// device row of the first of the two rows a side packs (interior) or
+// unpacks (halo): south 2 / 0, north ny_end-1 / ny_end+1 (relative to bnd_y1)
+int halo_row(const inmsom_ctx *c, int side, bool pack)
+{
+    const int last = c->dom.ny_end - c->dom.bnd_y1;
+    if (side == 0) return pack ? 2 : 0;
+    return pack ? last - 1 : last + 1;
+}
+}  // namespace
+
+int inmsom_halo_pack(inmsom_ctx *c, int side, void *buf)
+{
+    CKR(ensure_grid(c));
+    if (!buf || (side != 0 && side != 1)) return set_err(INMSOM_EARG, "inmsom_halo_pack: bad argument");
+    const size_t row_b = (size_t)c->dom.pitch * sizeof(double);
+    const size_t fs = row_b * c->dom.nya();
+    CK(cudaMemcpy2DAsync(buf, 2 * row_b, c->state[0] + (size_t)halo_row(c, side, true) * c->dom.pitch, fs,
+                         2 * row_b, NSTATE, cudaMemcpyDeviceToDevice, c->stream));
+    return INMSOM_OK;
+}
+
+int inmsom_halo_unpack(inmsom_ctx *c, int side, const void *buf)
+{
+    CKR(ensure_grid(c));
+    if (!buf || (side != 0 && side != 1)) return set_err(INMSOM_EARG, "inmsom_halo_unpack: bad argument");
+    const size_t row_b = (size_t)c->dom.pitch * sizeof(double);
+    const size_t fs = row_b * c->dom.nya();
+    CK(cudaMemcpy2DAsync(c->state[0] + (size_t)halo_row(c, side, false) * c->dom.pitch, fs, buf, 2 * row_b,
+                         2 * row_b, NSTATE, cudaMemcpyDeviceToDevice, c->stream));
+    return INMSOM_OK;
+}
+
+int inmsom_step_end(inmsom_ctx *c)
+{
+    CKR(ensure_grid(c));
+    if (fused::finish_steps(c->plan, c->stream))
+        return set_err(INMSOM_ECUDA, "substeps: %s", cudaGetErrorString(cudaGetLastError()));
+    if (c->plan.last_flags & (fused::FLAG_TIMEOUT | fused::FLAG_SMEM)) return fused_flag_error(c, "fused kernel");
+    return INMSOM_OK;
+}
+
+void *inmsom_gpu_stream(inmsom_ctx *c) { return c ? (void *)c->stream : nullptr; }
+
+long long inmsom_gpu_pitch(inmsom_ctx *c) { return c ? c->dom.pitch : 0; }
+
 int inmsom_strips_destroy(inmsom_strips *g)
 {
     if (!g) return INMSOM_OK;

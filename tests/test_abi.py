@@ -11,7 +11,7 @@ def declared_functions():
     names = set()
     for h in (ROOT / "include").glob("*.h"):
         text = re.sub(r"/\*.*?\*/", "", h.read_text(), flags=re.S)
-        for m in re.finditer(r"\b(?:int|const char \*)\s*(inmsom_\w+)\s*\(", text):
+        for m in re.finditer(r"\b(?:int|const char \*|void \*|long long)\s*(inmsom_\w+)\s*\(", text):
             names.add(m.group(1))
     return names
 

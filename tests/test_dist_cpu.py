@@ -1,0 +1,70 @@
+"""One process per strip (inmsom_elfs_b200.dist): the per-substep halo
+exchange between gloo ranks on CPU, with a radius-2 numpy stencil standing
+in for the GPU substep, must reproduce the single-domain run bit for bit
+(2 and 3 ranks).  The GPU side of the same exchange is tested in
+test_dist_gpu.py."""
+import os
+import socket
+
+import numpy as np
+import pytest
+import torch.multiprocessing as mp
+
+NX, ROWS, NSUB = 19, 41, 7      # global rows incl. 2 halo rows each side
+
+
+def _port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _fields():
+    rng = np.random.default_rng(5)
+    return rng.standard_normal((6, NX, ROWS))
+
+
+def _split(world):
+    """interior rows [2, ROWS-3] cut into `world` strips: (first, last) global rows"""
+    ny = ROWS - 4
+    locn = ny // world
+    out = []
+    for k in range(world):
+        a = 2 + k * locn
+        b = a + locn - 1 if k < world - 1 else ROWS - 3
+        out.append((a, b))
+    return out
+
+
+def _rank(rank, world, port, q):
+    import torch.distributed as dist
+    from inmsom_elfs_b200.dist import NumpyStripStepper, run_strip
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        a, b = _split(world)[rank]
+        f = _fields()[:, :, a - 2:b + 3]
+        st = NumpyStripStepper(f, (None, None), (2, b - a + 2))
+        run_strip(st, rank, world, NSUB, 0.5, np.linspace(0.5, 1.5, NSUB))
+        q.put((rank, st.f[:, :, 2:b - a + 3]))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_gloo_ranks_reproduce_one_domain(world):
+    from inmsom_elfs_b200.dist import NumpyStripStepper, run_strip
+    ref = NumpyStripStepper(_fields(), (None, None), (2, ROWS - 3))
+    run_strip(ref, 0, 1, NSUB, 0.5, np.linspace(0.5, 1.5, NSUB))
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    port = _port()
+    procs = [ctx.Process(target=_rank, args=(r, world, port, q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=300) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    merged = np.concatenate([got[r] for r in range(world)], axis=2)
+    assert np.array_equal(merged, ref.f[:, :, 2:ROWS - 2])
