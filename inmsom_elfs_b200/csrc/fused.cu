@@ -393,7 +393,6 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
     uint32_t ph = 0;
     // T-mask bits, 2 per row: row j+1 in bits 0-1, j in 2-3, j-1 in 4-5, j-2 in 6-7
     uint32_t mk = 0;
-    uint32_t bad = 0;   // guard: a new value out of range or NaN
     int waited = row_lo - 1;
     bool ready = false;   // row j+1 found complete by a test in the previous iteration
     bool ok = mbar_wait(&mbar[0], 0);
@@ -581,8 +580,6 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
                 const double difx = GEN ? (STr - ST) * CF(o_m1, dux) + SS * CF(o_m1, dus0) : ((STr - ST) + SS) * p.d;
                 const double grx = c.Ru + qc.Cu - ((FXr - FX) + FY) + difx + QU * 0.25;
                 const double un = (up_r * hup + grx * (GEN ? two_ti * CF(o_m1, rau) : p.tt)) * rcp_nr(hun);
-                bad |= (uint32_t)(wu && !(fabs(un) < 100.0));
-                bad |= (uint32_t)(wt && !(fabs(sn) < 10.0));
                 const long long idx = gi - p.pitch;
                 if (ACC && wu) {
                     const double slxn = -(SNr - sn) * (GEN ? CF(o_m1, gdyh) : p.gd) * hun;
@@ -626,7 +623,6 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
                 }
                 const double gry = qc.Pv - (GX - GXl) - GY - ST * (GEN ? CF(o_m2, dvt1) : p.d);
                 const double vn = (vp0 * hvp + gry * (GEN ? two_ti * CF(o_m2, rav) : p.tt)) * rcp_nr(hvn);
-                bad |= (uint32_t)(wv && !(fabs(vn) < 100.0));
                 const long long idx = gi - 2 * p.pitch;
                 if (ACC && wv) {
                     const double slyn = -(sn1 - sn0) * (GEN ? CF(o_m2, gdxh) : p.gd) * hvn;
@@ -693,7 +689,6 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
     } else {
         step(j, N0, Y1, N0, Y1, B, A, Y, X);
     }
-    if (__any_sync(0xffffffffu, bad != 0) && l == 0) atomicOr(p.flags, FLAG_GUARD);
     if (!ok) {
         if (l == 0) {
             atomicOr(p.flags, FLAG_TIMEOUT);

@@ -124,10 +124,11 @@ struct Plan {
     int last_variant = -1;          // 0 uniform, 1 general, 2 uniform with FP32 velocities (last launch)
 };
 
-// status bits the fused kernel sets: a bounded wait gave up; a new value out
-// of range; the dynamic shared memory did not start on a 128-byte boundary
-// (the ring's TMA slots need it; the kernel then does nothing)
-enum : unsigned { FLAG_TIMEOUT = 1u, FLAG_GUARD = 2u, FLAG_SMEM = 4u };
+// status bits the fused kernel sets: a bounded wait gave up; the dynamic
+// shared memory did not start on a 128-byte boundary (the ring's TMA slots
+// need it; the kernel then does nothing).  The range/NaN guard is the
+// separate k_guard pass (INMSOM_GUARD).
+enum : unsigned { FLAG_TIMEOUT = 1u, FLAG_SMEM = 4u };
 
 constexpr int NTABLE = 5;
 constexpr int TABLE_F32 = 4;   // the FP32-velocity substep's items
