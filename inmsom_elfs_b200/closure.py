@@ -49,7 +49,7 @@ class ClosureConfig:
     f0: float = 1.0e-4
     beta: float = 2.0e-11
     drag: float = 1.0e-6           # 1/s
-    visc_fine: float = 100.0       # m^2/s, the truth
+    visc_fine: float = 50.0        # m^2/s, the truth
     visc_plain: float = 1000.0     # m^2/s, the plain coarse run
     visc_base: float = 0.0         # m^2/s, kept by the closure run
     dt_fine: float = 3.0           # s

@@ -124,9 +124,8 @@ class NumpyStripStepper:
     row/column stencil that, like the fused kernel, needs only the state's
     halo rows.  Rows outside the global interior are never written."""
 
-    def __init__(self, fields: np.ndarray, global_rows: tuple, local_rows: tuple):
+    def __init__(self, fields: np.ndarray, local_rows: tuple):
         self.f = fields.copy()                       # [6, nx, rows]
-        self.g0, self.g1 = global_rows               # first/last interior rows of the basin (local index)
         self.l0, self.l1 = local_rows                # first/last interior rows of this strip (local index)
         self.buf = [np.zeros((6, self.f.shape[1], 2)) for _ in range(4)]
 
@@ -165,3 +164,17 @@ class NumpyStripStepper:
 
     def end(self):
         pass
+
+
+def diag(solver, group=None, device_tensor: bool = False):
+    """Volume and energy of the whole basin: each rank's inmsom_gpu_diag
+    over its strip's interior rows, summed over the ranks by an FP64
+    all-reduce (two scalars; NCCL with device_tensor, else on the host)."""
+    import torch
+    import torch.distributed as dist
+    v, e = solver.diag()
+    t = torch.tensor([v, e], dtype=torch.float64)
+    if device_tensor:
+        t = t.to(torch.device("cuda", solver.device))
+    dist.all_reduce(t, op=dist.ReduceOp.SUM, group=group)
+    return float(t[0].item()), float(t[1].item())

@@ -44,7 +44,7 @@ def _rank(rank, world, port, q):
     try:
         a, b = _split(world)[rank]
         f = _fields()[:, :, a - 2:b + 3]
-        st = NumpyStripStepper(f, (None, None), (2, b - a + 2))
+        st = NumpyStripStepper(f, (2, b - a + 2))
         run_strip(st, rank, world, NSUB, 0.5, np.linspace(0.5, 1.5, NSUB))
         q.put((rank, st.f[:, :, 2:b - a + 3]))
     finally:
@@ -54,7 +54,7 @@ def _rank(rank, world, port, q):
 @pytest.mark.parametrize("world", [2, 3])
 def test_gloo_ranks_reproduce_one_domain(world):
     from inmsom_elfs_b200.dist import NumpyStripStepper, run_strip
-    ref = NumpyStripStepper(_fields(), (None, None), (2, ROWS - 3))
+    ref = NumpyStripStepper(_fields(), (2, ROWS - 3))
     run_strip(ref, 0, 1, NSUB, 0.5, np.linspace(0.5, 1.5, NSUB))
     ctx = mp.get_context("spawn")
     q = ctx.Queue()

@@ -3,7 +3,8 @@ inmsom_elfs_b200.dist): two ranks, each with its own context for its strip,
 advance with one halo exchange per substep (gloo, staged through host
 memory; both ranks on the one GPU this test gets -- their kernels never
 wait for each other, the host exchange orders them) and must end bit for
-bit where the single-domain fused run ends."""
+bit where the single-domain fused run ends; the all-reduced volume and
+energy equal the single-domain diagnostics to 1e-13 / 1e-12 relative."""
 import os
 import socket
 
@@ -41,11 +42,13 @@ def _rank(rank, world, port, q):
         b = _basin()
         loc = split_basin(b, world)[rank]
         scale = basins.wind_cycle(NSUB, b.dt, t0=50.0, period=900.0)
+        from inmsom_elfs_b200.dist import diag
         with solver.BarotropicSolver(loc, resident=True) as s:
             s.load_state()
             run_strip(GpuStripStepper(s, host_staging=True), rank, world, NSUB, b.dt, scale)
             s.sync_to_host()
-        q.put((rank, {k: v for k, v in loc.state.items()}))
+            vol, en = diag(s)
+        q.put((rank, {k: v for k, v in loc.state.items()}, (vol, en)))
     finally:
         dist.destroy_process_group()
 
@@ -59,7 +62,10 @@ def test_two_ranks_match_single_domain(gpu):
     procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
     for p in procs:
         p.start()
-    got = dict(q.get(timeout=300) for _ in range(2))
+    got, dg = {}, {}
+    for _ in range(2):
+        r, st, d = q.get(timeout=300)
+        got[r], dg[r] = st, d
     for p in procs:
         p.join(timeout=60)
         assert p.exitcode == 0
@@ -70,6 +76,11 @@ def test_two_ranks_match_single_domain(gpu):
         s.load_state()
         s.run_substeps(NSUB, b.dt, scale)
         s.sync_to_host()
+        vol, en = s.diag()
+    # the all-reduced diagnostics: the same on both ranks, the single-domain
+    # sums up to the order of the additions
+    assert dg[0] == dg[1]
+    assert abs(dg[0][0] - vol) <= 1e-13 * abs(vol) and abs(dg[0][1] - en) <= 1e-12 * abs(en)
     parts = split_basin(b, 2)
     for r in range(2):
         parts[r].state.update(got[r])
