@@ -355,7 +355,7 @@ long long inmsom_gpu_pitch(inmsom_ctx *ctx);
  * enqueue work. */
 #define INMSOM_MLP_NPARAM 7816
 #define INMSOM_MLP_NBF16 7680
-#define INMSOM_MLP_PARTIAL 7817   /* floats per 128-sample tile in `partial` */
+#define INMSOM_MLP_PARTIAL 7817   /* floats per 128 samples in `partial` */
 /* wbf16 := BF16(W1, W2, W3 of params) */
 int inmsom_mlp_pack(const float *params, void *wbf16, void *stream);
 /* y[n][0..1] = MLP(x[n]) for n < count */
@@ -364,7 +364,8 @@ int inmsom_mlp_forward(const void *x, long long count, const float *params, cons
 /* Gradient of the mean squared error over the samples idx[0..batch) (or
  * 0..batch if idx is NULL), batch a multiple of 128: grad[0..NPARAM) and
  * grad[NPARAM] = the loss; partial holds batch/128 * INMSOM_MLP_PARTIAL
- * floats (per-tile sums, added in tile order: deterministic). */
+ * floats (at most one CTA per 128 samples writes its sums there; they are
+ * added in CTA order: deterministic for a given device). */
 int inmsom_mlp_grad(const void *x, const float *targets, const int *idx, int batch, const float *params,
                     const void *wbf16, float *partial, float *grad, void *stream);
 /* One bias-corrected Adam step (step >= 1) on params, then wbf16. */
