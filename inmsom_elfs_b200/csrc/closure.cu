@@ -170,13 +170,22 @@ __device__ void forward(Smem &s)
 
 // grad[p] = sum over CTAs of partial[c][p] in CTA order (deterministic);
 // grad[NPARAM] = mean squared error
-__global__ void k_mlp_reduce(const float *partial, int ntiles, int batch, float *grad)
+// 32 parameters per block of 8 warps: warp w sums CTAs w, w+8, ... (each a
+// coalesced 128-byte row piece), then warp 0 adds the 8 sums in order
+__global__ void __launch_bounds__(256) k_mlp_reduce(const float *partial, int ntiles, int batch, float *grad)
 {
-    const int p = blockIdx.x * blockDim.x + threadIdx.x;
-    if (p > NPARAM) return;
+    __shared__ float part[8][32];
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, p = 32 * blockIdx.x + l;
     float a = 0.f;
-    for (int t = 0; t < ntiles; t++) a += partial[(size_t)t * NPART + p];
-    grad[p] = p == NPARAM ? a / ((float)batch * NOUT) : a;
+    if (p <= NPARAM)
+        for (int t = w; t < ntiles; t += 8) a += partial[(size_t)t * NPART + p];
+    part[w][l] = a;
+    __syncthreads();
+    if (w == 0 && p <= NPARAM) {
+        float v = 0.f;
+        for (int k = 0; k < 8; k++) v += part[k][l];
+        grad[p] = p == NPARAM ? v / ((float)batch * NOUT) : v;
+    }
 }
 
 // Adam (Kingma & Ba), bias-corrected, then the BF16 weight copy
@@ -472,7 +481,8 @@ struct GSmem {
     alignas(16) __nv_bfloat16 w2t[HID][HS];   // W2^T
     alignas(16) __nv_bfloat16 w3t[16][HS];             // W3^T, outputs padded to 16 (rows 8..15 zero)
     float b1[HID], b2[HID], b3[N3];
-    alignas(16) __nv_bfloat16 x[GT][XS];
+    alignas(16) __nv_bfloat16 x[2][GT][XS];   // this tile's inputs and the next one's
+    alignas(16) float tg[2][GT][NOUT];       // targets, likewise
     alignas(16) __nv_bfloat16 a1[GT][HS], a2[GT][HS];
     alignas(16) __nv_bfloat16 d1[GT][HS], d2[GT][HS];
     alignas(16) __nv_bfloat16 d3[GT][OS];              // output gradients, columns 8..15 zero
@@ -485,6 +495,17 @@ __device__ __forceinline__ uint32_t smem_addr(const void *p)
 {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
+__device__ __forceinline__ void cp_async16(void *dst, const void *src)
+{
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async8(void *dst, const void *src)
+{
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
+
 __device__ __forceinline__ void ldsm4(uint32_t r[4], const void *p)
 {
     asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
@@ -585,15 +606,25 @@ __global__ void __launch_bounds__(GW * 32) k_mlp_grad(const __nv_bfloat16 *x, co
     const float scale = 2.0f / ((float)batch * NOUT);
     const int m0 = 16 * w;
     const int ntiles = batch / GT;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
-        __syncthreads();   // the previous tile's shared arrays are no longer read
-        // the tile's inputs: 64 rows of 48 BF16 (6 x 16 bytes each)
-        for (int i = threadIdx.x; i < GT * 6; i += blockDim.x) {
-            const int r = i / 6, q = i % 6;
-            const long long row = idx ? idx[tile * GT + r] : (long long)tile * GT + r;
-            *reinterpret_cast<uint4 *>(&s.x[r][8 * q]) = reinterpret_cast<const uint4 *>(x + row * KIN)[q];
+    // the inputs (64 rows of 6 x 16 bytes) and targets of a tile into buffer b
+    auto fetch = [&](int tile, int b) {
+        if (tile < ntiles) {
+            for (int i = threadIdx.x; i < GT * 7; i += blockDim.x) {
+                const int r = i / 7, q = i % 7;
+                const long long row = idx ? idx[tile * GT + r] : (long long)tile * GT + r;
+                if (q < 6) cp_async16(&s.x[b][r][8 * q], x + row * KIN + 8 * q);
+                else cp_async8(&s.tg[b][r][0], tgt + row * NOUT);
+            }
         }
-        __syncthreads();
+        cp_async_commit();   // an empty group past the last tile keeps the count
+    };
+    fetch(blockIdx.x, 0);
+    int cur = 0;
+    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, cur ^= 1) {
+        __syncthreads();   // the previous tile's shared arrays are no longer read
+        fetch(tile + gridDim.x, cur ^ 1);
+        cp_async_wait1();  // this tile's group has landed (for this thread)
+        __syncthreads();   // ... and for every thread
         // ---- forward (this warp's 16 samples)
         float z1[8][4], z2[8][4], acc[8][4];
         uint32_t a[4][4];
@@ -605,7 +636,7 @@ __global__ void __launch_bounds__(GW * 32) k_mlp_grad(const __nv_bfloat16 *x, co
 #pragma unroll
         for (int kb = 0; kb < 3; kb++) {
             uint32_t af[4];
-            ldsm4(af, &s.x[m0 + (l & 7) + 8 * ((l >> 3) & 1)][16 * kb + 8 * (l >> 4)]);
+            ldsm4(af, &s.x[cur][m0 + (l & 7) + 8 * ((l >> 3) & 1)][16 * kb + 8 * (l >> 4)]);
 #pragma unroll
             for (int np = 0; np < 4; np++) {
                 uint32_t b[4];
@@ -655,11 +686,9 @@ __global__ void __launch_bounds__(GW * 32) k_mlp_grad(const __nv_bfloat16 *x, co
         if (t == 0) {
 #pragma unroll
             for (int h = 0; h < 2; h++) {
-                const int r = tile * GT + m0 + g + 8 * h;
-                const long long row = idx ? idx[r] : (long long)r;
 #pragma unroll
                 for (int j = 0; j < NOUT; j++) {
-                    const float e = o[2 * h + j] - tgt[row * NOUT + j];
+                    const float e = o[2 * h + j] - s.tg[cur][m0 + g + 8 * h][j];
                     lsum += e * e;
                     d3[2 * h + j] = scale * e;
                 }
@@ -730,7 +759,7 @@ __global__ void __launch_bounds__(GW * 32) k_mlp_grad(const __nv_bfloat16 *x, co
             const __nv_bfloat16 *A, *B;
             int sa, sb, m0w, n0w, off, ldw;
             if (q < 24) {
-                A = &s.x[0][0], sa = XS, B = &s.d1[0][0], sb = HS;
+                A = &s.x[cur][0][0], sa = XS, B = &s.d1[0][0], sb = HS;
                 m0w = 16 * (q >> 3), n0w = 8 * (q & 7), off = OFF_W1, ldw = HID;
             } else if (q < 56) {
                 const int r = q - 24;
@@ -873,7 +902,7 @@ int inmsom_mlp_grad(const void *x, const float *targets, const int *idx, int bat
     k_mlp_grad<<<grid, GW * 32, sizeof(GSmem), (cudaStream_t)stream>>>(
         (const __nv_bfloat16 *)x, targets, idx, batch, params, (const __nv_bfloat16 *)wbf16, partial);
     if (check_launch("inmsom_mlp_grad")) return INMSOM_ECUDA;
-    k_mlp_reduce<<<(NPARAM + 1 + 255) / 256, 256, 0, (cudaStream_t)stream>>>(partial, grid, batch, grad);
+    k_mlp_reduce<<<(NPARAM + 1 + 31) / 32, 256, 0, (cudaStream_t)stream>>>(partial, grid, batch, grad);
     return check_launch("inmsom_mlp_grad reduce");
 }
 
