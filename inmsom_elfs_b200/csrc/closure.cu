@@ -28,8 +28,8 @@ constexpr int OFF_W1 = 0, OFF_B1 = OFF_W1 + KIN * HID, OFF_W2 = OFF_B1 + HID, OF
               OFF_W3 = OFF_B2 + HID, OFF_B3 = OFF_W3 + HID * N3, NPARAM = OFF_B3 + N3;
 constexpr int BOFF_W1 = 0, BOFF_W2 = KIN * HID, BOFF_W3 = BOFF_W2 + HID * HID, NBF = BOFF_W3 + HID * N3;
 static_assert(NPARAM == INMSOM_MLP_NPARAM, "parameter block size");
-constexpr int TILE = 128;     // samples per CTA
-constexpr int WARPS = 8;      // 16 samples per warp in the row-parallel GEMMs
+constexpr int TILE = 128;     // batch unit of inmsom_mlp_grad (one partial sum set per TILE samples)
+constexpr int WARPS = 8;      // warps per CTA of the inference kernels (one per tile row)
 constexpr int NPART = NPARAM + 1;   // per-CTA partial gradient + loss
 
 // ---------------------------------------------------------------- helpers
@@ -47,45 +47,6 @@ __device__ __forceinline__ void mma16816(float c[4], const uint32_t a[4], const 
         "{%0,%1,%2,%3};"
         : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
-// Fragments of mma.m16n8k16 for lane (g = lane/4, t = lane%4):
-//   A: a0 = A[g][2t,2t+1]  a1 = A[g+8][2t,2t+1]  a2 = A[g][2t+8,2t+9]  a3 = A[g+8][2t+8,2t+9]
-//   B: b0 = B[2t,2t+1][g]  b1 = B[2t+8,2t+9][g]
-//   C: c0 = C[g][2t] c1 = C[g][2t+1] c2 = C[g+8][2t] c3 = C[g+8][2t+1]
-// A(r, k) and B(k, n) are element accessors (BF16).
-template <class FA>
-__device__ __forceinline__ void frag_a(uint32_t a[4], FA A, int m0, int k0)
-{
-    const int l = threadIdx.x & 31, g = l >> 2, t = l & 3;
-    a[0] = pack_raw(A(m0 + g, k0 + 2 * t), A(m0 + g, k0 + 2 * t + 1));
-    a[1] = pack_raw(A(m0 + g + 8, k0 + 2 * t), A(m0 + g + 8, k0 + 2 * t + 1));
-    a[2] = pack_raw(A(m0 + g, k0 + 2 * t + 8), A(m0 + g, k0 + 2 * t + 9));
-    a[3] = pack_raw(A(m0 + g + 8, k0 + 2 * t + 8), A(m0 + g + 8, k0 + 2 * t + 9));
-}
-template <class FB>
-__device__ __forceinline__ void frag_b(uint32_t b[2], FB B, int k0, int n0)
-{
-    const int l = threadIdx.x & 31, g = l >> 2, t = l & 3;
-    b[0] = pack_raw(B(k0 + 2 * t, n0 + g), B(k0 + 2 * t + 1, n0 + g));
-    b[1] = pack_raw(B(k0 + 2 * t + 8, n0 + g), B(k0 + 2 * t + 9, n0 + g));
-}
-// C tile [m0, m0+16) x [n0, n0+8) = sum over K of A * B, handed to out(r, n, value)
-template <class FA, class FB, class FO>
-__device__ __forceinline__ void gemm_tile(FA A, FB B, int K, int m0, int n0, FO out)
-{
-    float c[4] = {0.f, 0.f, 0.f, 0.f};
-    for (int k0 = 0; k0 < K; k0 += 16) {
-        uint32_t a[4], b[2];
-        frag_a(a, A, m0, k0);
-        frag_b(b, B, k0, n0);
-        mma16816(c, a, b);
-    }
-    const int l = threadIdx.x & 31, g = l >> 2, t = l & 3;
-    out(m0 + g, n0 + 2 * t, c[0]);
-    out(m0 + g, n0 + 2 * t + 1, c[1]);
-    out(m0 + g + 8, n0 + 2 * t, c[2]);
-    out(m0 + g + 8, n0 + 2 * t + 1, c[3]);
 }
 
 // GELU in the tanh form of Hendrycks & Gimpel (2016),
@@ -108,64 +69,6 @@ __device__ __forceinline__ float gelu_d(float x)
 {
     const float x2 = x * x, t = tanh_hw(x * fmaf(GC1, x2, GC0));
     return fmaf(0.5f, 1.0f + t, 0.5f * x * (1.0f - t * t) * fmaf(3.0f * GC1, x2, GC0));
-}
-
-// shared memory of one 128-sample tile
-struct Smem {
-    __nv_bfloat16 x[TILE][KIN];      // inputs
-    float z1[TILE][HID];             // pre-activations, then their gradients
-    __nv_bfloat16 a1[TILE][HID];     // GELU(z1)
-    float z2[TILE][HID];
-    __nv_bfloat16 a2[TILE][HID];
-    float z3[TILE][N3];              // outputs, then their gradients
-    __nv_bfloat16 d3[TILE][16];      // output gradients (K padded to 16)
-    __nv_bfloat16 d2[TILE][HID];     // gradients of z2
-    __nv_bfloat16 d1[TILE][HID];     // gradients of z1
-    __nv_bfloat16 w1[KIN][HID], w2[HID][HID], w3[HID][16];   // W3 columns padded to 16
-    float b1[HID], b2[HID], b3[N3];
-};
-
-__device__ void load_weights(Smem &s, const float *prm, const __nv_bfloat16 *wb)
-{
-    for (int i = threadIdx.x; i < KIN * HID; i += blockDim.x) s.w1[i / HID][i % HID] = wb[BOFF_W1 + i];
-    for (int i = threadIdx.x; i < HID * HID; i += blockDim.x) s.w2[i / HID][i % HID] = wb[BOFF_W2 + i];
-    for (int i = threadIdx.x; i < HID * 16; i += blockDim.x) {
-        const int r = i / 16, c = i % 16;
-        s.w3[r][c] = c < N3 ? wb[BOFF_W3 + r * N3 + c] : __float2bfloat16(0.f);
-    }
-    for (int i = threadIdx.x; i < HID; i += blockDim.x) {
-        s.b1[i] = prm[OFF_B1 + i];
-        s.b2[i] = prm[OFF_B2 + i];
-    }
-    for (int i = threadIdx.x; i < N3; i += blockDim.x) s.b3[i] = prm[OFF_B3 + i];
-}
-
-// forward pass of the tile in shared memory (x already loaded); z3 holds
-// the outputs (bias included)
-__device__ void forward(Smem &s)
-{
-    const int w = threadIdx.x >> 5;
-    const int m0 = 16 * w;
-    // layer 1: z1 = x W1 + b1, a1 = GELU(z1)
-    for (int n0 = 0; n0 < HID; n0 += 8)
-        gemm_tile([&](int r, int k) { return s.x[r][k]; }, [&](int k, int n) { return s.w1[k][n]; }, KIN, m0, n0,
-                  [&](int r, int n, float v) {
-                      const float z = v + s.b1[n];
-                      s.z1[r][n] = z;
-                      s.a1[r][n] = __float2bfloat16(gelu(z));
-                  });
-    __syncwarp();
-    for (int n0 = 0; n0 < HID; n0 += 8)
-        gemm_tile([&](int r, int k) { return s.a1[r][k]; }, [&](int k, int n) { return s.w2[k][n]; }, HID, m0, n0,
-                  [&](int r, int n, float v) {
-                      const float z = v + s.b2[n];
-                      s.z2[r][n] = z;
-                      s.a2[r][n] = __float2bfloat16(gelu(z));
-                  });
-    __syncwarp();
-    gemm_tile([&](int r, int k) { return s.a2[r][k]; }, [&](int k, int n) { return s.w3[k][n]; }, HID, m0, 0,
-              [&](int r, int n, float v) { s.z3[r][n] = v + s.b3[n]; });
-    __syncthreads();
 }
 
 // grad[p] = sum over CTAs of partial[c][p] in CTA order (deterministic);
@@ -219,26 +122,6 @@ __global__ void k_mlp_pack(const float *prm, __nv_bfloat16 *wb)
     if (p < KIN * HID) wb[BOFF_W1 + p] = __float2bfloat16(prm[OFF_W1 + p]);
     else if (p < KIN * HID + HID * HID) wb[BOFF_W2 + p - KIN * HID] = __float2bfloat16(prm[OFF_W2 + p - KIN * HID]);
     else if (p < NBF) wb[BOFF_W3 + p - KIN * HID - HID * HID] = __float2bfloat16(prm[OFF_W3 + p - KIN * HID - HID * HID]);
-}
-
-// y[n][0..1] = MLP(x[n]) for n < count (tiles of 128, the last one partial)
-__global__ void __launch_bounds__(WARPS * 32, 1) k_mlp_forward(const __nv_bfloat16 *x, long long count, const float *prm,
-                                                               const __nv_bfloat16 *wb, float *y)
-{
-    extern __shared__ __align__(16) unsigned char raw[];
-    Smem &s = *reinterpret_cast<Smem *>(raw);
-    const long long tile0 = (long long)blockIdx.x * TILE;
-    load_weights(s, prm, wb);
-    for (int i = threadIdx.x; i < TILE * KIN; i += blockDim.x) {
-        const int r = i / KIN, k = i % KIN;
-        s.x[r][k] = tile0 + r < count ? x[(tile0 + r) * KIN + k] : __float2bfloat16(0.f);
-    }
-    __syncthreads();
-    forward(s);
-    for (int i = threadIdx.x; i < TILE * NOUT; i += blockDim.x) {
-        const int r = i / NOUT, j = i % NOUT;
-        if (tile0 + r < count) y[(tile0 + r) * NOUT + j] = s.z3[r][j];
-    }
 }
 
 // splitmix64 of (seed, step, i): uniform sample indices in [0, n)
@@ -302,7 +185,8 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi)
 
 // y (outputs 0, 1 of cells g and g+8 in o[0..3] of lanes t == 0) of the
 // 16 cells whose layer-1 A fragments are a1
-__device__ __forceinline__ void mlp16(const ClSmem &s, const uint32_t a1[3][4], float o[4])
+template <class S>
+__device__ __forceinline__ void mlp16(const S &s, const uint32_t a1[3][4], float o[4])
 {
     const int l = threadIdx.x & 31, g = l >> 2, t = l & 3;
     float acc[8][4];
@@ -803,6 +687,63 @@ __global__ void __launch_bounds__(GW * 32) k_mlp_grad(const __nv_bfloat16 *x, co
     }
 }
 
+// y[n][0..1] = MLP(x[n]) for n < count: the network of k_closure_apply
+// (mlp16) on feature rows, 64 per tile, one warp per 16
+struct FSmem {
+    alignas(16) __nv_bfloat16 w1t[HID][XS];
+    alignas(16) __nv_bfloat16 w2t[HID][HS];
+    alignas(16) __nv_bfloat16 w3t[16][HS];
+    float b1[HID], b2[HID], b3[N3];
+    alignas(16) __nv_bfloat16 x[GT][XS];
+};
+
+__global__ void __launch_bounds__(GW * 32) k_mlp_forward(const __nv_bfloat16 *x, long long count, const float *prm,
+                                                        const __nv_bfloat16 *wb, float *y)
+{
+    __shared__ FSmem s;
+    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, g = l >> 2, t = l & 3;
+    for (int i = threadIdx.x; i < KIN * HID; i += blockDim.x) s.w1t[i % HID][i / HID] = wb[BOFF_W1 + i];
+    for (int i = threadIdx.x; i < HID * HID; i += blockDim.x) s.w2t[i % HID][i / HID] = wb[BOFF_W2 + i];
+    for (int i = threadIdx.x; i < 16 * HS; i += blockDim.x) {
+        const int o = i / HS, c = i % HS;
+        s.w3t[o][c] = o < N3 && c < HID ? wb[BOFF_W3 + c * N3 + o] : __float2bfloat16(0.f);
+    }
+    for (int i = threadIdx.x; i < HID; i += blockDim.x) {
+        s.b1[i] = prm[OFF_B1 + i];
+        s.b2[i] = prm[OFF_B2 + i];
+    }
+    if (threadIdx.x < N3) s.b3[threadIdx.x] = prm[OFF_B3 + threadIdx.x];
+    const int m0 = 16 * w;
+    const long long ntiles = (count + GT - 1) / GT;
+    for (long long tile = blockIdx.x; tile < ntiles; tile += gridDim.x) {
+        __syncthreads();
+        for (int i = threadIdx.x; i < GT * 6; i += blockDim.x) {
+            const int r = i / 6, q = i % 6;
+            const long long row = tile * GT + r;
+            uint4 v = make_uint4(0u, 0u, 0u, 0u);
+            if (row < count) v = reinterpret_cast<const uint4 *>(x + row * KIN)[q];
+            *reinterpret_cast<uint4 *>(&s.x[r][8 * q]) = v;
+        }
+        __syncthreads();
+        uint32_t a1[3][4];
+#pragma unroll
+        for (int kb = 0; kb < 3; kb++) ldsm4(a1[kb], &s.x[m0 + (l & 7) + 8 * ((l >> 3) & 1)][16 * kb + 8 * (l >> 4)]);
+        float o[4];
+        mlp16(s, a1, o);
+        if (t == 0) {
+            const long long r0 = tile * GT + m0 + g, r1 = r0 + 8;
+            if (r0 < count) {
+                y[r0 * NOUT] = o[0];
+                y[r0 * NOUT + 1] = o[1];
+            }
+            if (r1 < count) {
+                y[r1 * NOUT] = o[2];
+                y[r1 * NOUT + 1] = o[3];
+            }
+        }
+    }
+}
+
 int fail(int code, const char *msg) { return inmsom::record_error(code, msg); }
 
 int check_launch(const char *what)
@@ -822,9 +763,7 @@ int ensure_smem()
 {
     if (smem_ready) return INMSOM_OK;
     if (cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GSmem)) !=
-            cudaSuccess ||
-        cudaFuncSetAttribute(k_mlp_forward, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(Smem)) !=
-            cudaSuccess)
+        cudaSuccess)
         return fail(INMSOM_ECUDA, "MLP kernels: shared memory attribute");
     smem_ready = true;
     return INMSOM_OK;
@@ -877,10 +816,13 @@ int inmsom_mlp_forward(const void *x, long long count, const float *params, cons
 {
     if (!x || !params || !wbf16 || !y || count < 0) return fail(INMSOM_EARG, "inmsom_mlp_forward: bad argument");
     if (count == 0) return INMSOM_OK;
-    if (ensure_smem()) return INMSOM_ECUDA;
-    const long long tiles = (count + TILE - 1) / TILE;
-    k_mlp_forward<<<(unsigned)tiles, WARPS * 32, sizeof(Smem), (cudaStream_t)stream>>>(
-        (const __nv_bfloat16 *)x, count, params, (const __nv_bfloat16 *)wbf16, y);
+    int dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    const long long tiles = (count + GT - 1) / GT;
+    const int grid = (int)std::min<long long>(tiles, 8LL * nsm);
+    k_mlp_forward<<<grid, GW * 32, 0, (cudaStream_t)stream>>>((const __nv_bfloat16 *)x, count, params,
+                                                              (const __nv_bfloat16 *)wbf16, y);
     return check_launch("inmsom_mlp_forward");
 }
 
