@@ -266,3 +266,23 @@ def test_guard_trips_and_context_survives(gpu, ora):
             bad.state[k][...] = b.state[k]
         s.sync_from_host()       # resident context: re-upload the sane state
         s.barotropic_dynamics(b.dt, 1)
+
+
+def test_last_phases_cover_the_call(gpu, ora):
+    """inmsom_gpu_last_phases: upload, substeps and download of the last
+    barotropic_dynamics call, each positive, together within the call's
+    wall time; before any call it is an argument error."""
+    import time
+    from inmsom_elfs_b200 import InmsomError, _lib
+    b = prep(basins.regional_basin(nx=200, ny=150, seed=17), ora)
+    with gpu.BarotropicSolver(b, resident=True) as s:
+        with pytest.raises(InmsomError) as e:
+            s.last_phases()
+        assert e.value.code == _lib.EARG
+        s.barotropic_dynamics(4 * b.dt, 4)
+        t0 = time.perf_counter()
+        s.barotropic_dynamics(4 * b.dt, 4)
+        wall = (time.perf_counter() - t0) * 1e3
+        up, comp, down = s.last_phases()
+        assert up > 0 and comp > 0 and down > 0
+        assert up + comp + down <= wall * 1.05 + 0.05
