@@ -161,6 +161,21 @@ int inmsom_r_diss(inmsom_ctx *ctx, double r_fric, double *r_diss);
 int inmsom_wind_forcing(inmsom_ctx *ctx, const double *taux, const double *tauy,
                         double *RHSx2d, double *RHSy2d);
 
+/* The barotropic RHS of Control/dyncall.f90:110-130 (the mode-split caller
+ * of barotropic_dynamics), at the ocean u (v) points, in the reference's
+ * order of operations:
+ *   RHSx2d = RHSx2d - RHSx2d_diff_disp + RHSx2d_tran - RHSx2d_tran_disp
+ *          + (surf_stress_x + bot_stress_x)*dxt*dyh
+ *          - (slpr(m+1,n) - slpr(m,n))*hhu*dyh/RefDen
+ * and likewise for RHSy2d (dyt*dxh, slpr(m,n+1), hhv, dxh).  Host arrays
+ * in the registered layout; any input may be NULL (that term is zero);
+ * hhu and hhv are needed with slpr. */
+int inmsom_rhs2d(inmsom_ctx *ctx, double *RHSx2d, double *RHSy2d, const double *RHSx2d_diff_disp,
+                 const double *RHSy2d_diff_disp, const double *RHSx2d_tran, const double *RHSy2d_tran,
+                 const double *RHSx2d_tran_disp, const double *RHSy2d_tran_disp, const double *surf_stress_x,
+                 const double *surf_stress_y, const double *bot_stress_x, const double *bot_stress_y,
+                 const double *slpr, const double *hhu, const double *hhv);
+
 /* Replaces hh_init, Function/depth.f90:2-105, for the external-mode depths
  * (its call at Control/init_pars.f90:426-430): recomputes the twelve
  * registered external depth arrays from ssh_e, sshp_e and hhq_rest and

@@ -94,6 +94,7 @@ struct inmsom_ctx {
     double *scr[NSCR] = {};
     double *intl[NINT] = {};
     double *tmp[4] = {};
+    double *r2d[7] = {};             // inmsom_rhs2d: RHSx, RHSy, four inputs, a zero field (one block)
     unsigned long long *d_nbad = nullptr;
     double *d_rows = nullptr, *d_out = nullptr;
 
@@ -390,6 +391,7 @@ int inmsom_gpu_finalize(inmsom_ctx *c)
     for (auto &p : c->scr) cudaFree(p);
     for (auto &p : c->intl) cudaFree(p);
     for (auto &p : c->tmp) cudaFree(p);
+    cudaFree(c->r2d[0]);   // one block
     cudaFree(c->d_nbad);
     cudaFree(c->d_rows);
     cudaFree(c->d_out);
@@ -979,6 +981,53 @@ int inmsom_wind_forcing(inmsom_ctx *c, const double *taux, const double *tauy, d
                           c->stream);
     CKR(d2h(c, RHSx2d, c->tmp[2]));
     CKR(d2h(c, RHSy2d, c->tmp[3]));
+    return sync_stream(c);
+}
+
+int inmsom_rhs2d(inmsom_ctx *c, double *RHSx2d, double *RHSy2d, const double *RHSx2d_diff_disp,
+                 const double *RHSy2d_diff_disp, const double *RHSx2d_tran, const double *RHSy2d_tran,
+                 const double *RHSx2d_tran_disp, const double *RHSy2d_tran_disp, const double *surf_stress_x,
+                 const double *surf_stress_y, const double *bot_stress_x, const double *bot_stress_y,
+                 const double *slpr, const double *hhu, const double *hhv)
+{
+    CKR(ensure_grid(c));
+    if (!RHSx2d || !RHSy2d) return set_err(INMSOM_EARG, "inmsom_rhs2d: NULL RHSx2d or RHSy2d");
+    if (slpr && (!hhu || !hhv)) return set_err(INMSOM_EARG, "inmsom_rhs2d: slpr needs hhu and hhv");
+    CKR(alloc_block(c, c->r2d, 7));   // zeroed once; field 6 stays zero
+    double **r = c->r2d, *zero = c->r2d[6];
+    // an input on the device, or the zero field for a NULL argument (a
+    // missing term adds or subtracts 0, as in the reference with the term zero)
+    auto in = [&](double *dev, const double *host, int *rc) -> const double * {
+        if (!host) return zero;
+        *rc = h2d(c, dev, host);
+        return dev;
+    };
+    int rc = INMSOM_OK;
+    CKR(h2d(c, r[0], (const double *)RHSx2d));
+    CKR(h2d(c, r[1], (const double *)RHSy2d));
+    const GridDev g = c->gdev();
+    const double *pairs[3][2] = {{RHSx2d_diff_disp, RHSy2d_diff_disp}, {RHSx2d_tran, RHSy2d_tran},
+                                 {RHSx2d_tran_disp, RHSy2d_tran_disp}};
+    const int term_of[3] = {0, 1, 0};
+    for (int t = 0; t < 3; t++) {
+        const double *ax = in(r[2], pairs[t][0], &rc), *ay = in(r[3], pairs[t][1], &rc);
+        CKR(rc);
+        general::rhs2d_term(c->dom, g, c->c, term_of[t], r[0], r[1], ax, ay, nullptr, nullptr, c->stream);
+    }
+    {
+        const double *ax = in(r[2], surf_stress_x, &rc), *bx = in(r[3], bot_stress_x, &rc);
+        const double *ay = in(r[4], surf_stress_y, &rc), *by = in(r[5], bot_stress_y, &rc);
+        CKR(rc);
+        general::rhs2d_term(c->dom, g, c->c, 2, r[0], r[1], ax, ay, bx, by, c->stream);
+    }
+    {
+        const double *a = in(r[2], slpr, &rc), *bx = in(r[3], hhu, &rc), *by = in(r[4], hhv, &rc);
+        CKR(rc);
+        general::rhs2d_term(c->dom, g, c->c, 3, r[0], r[1], a, a, bx, by, c->stream);
+    }
+    CK(cudaGetLastError());
+    CKR(d2h(c, RHSx2d, r[0]));
+    CKR(d2h(c, RHSy2d, r[1]));
     return sync_stream(c);
 }
 

@@ -374,6 +374,34 @@ __global__ void k_wind(int m0, int m1, int n0, int n1, Dom D, GridDev g, double 
     }
 }
 
+// ---- Control/dyncall.f90:110-130: the barotropic RHS, one term per launch
+// in the reference's left-to-right order, so that every step rounds where
+// the Fortran expression rounds (this file: --fmad=false, no reassociation):
+// term 0: r - a; 1: r + a; 2: r + (a + b) * area; 3: r - dslpr * b * d / rho
+__global__ void k_rhs2d_term(int m0, int m1, int n0, int n1, Dom D, GridDev g, double rho, int term,
+                             double *rx, double *ry, const double *ax, const double *ay, const double *bx,
+                             const double *by)
+{
+    RANGE_GUARD
+    const long long i = X(m, n);
+    if (g.lcu[i] > 0.5f) {
+        double r = rx[i];
+        if (term == 0) r = r - ax[i];
+        else if (term == 1) r = r + ax[i];
+        else if (term == 2) r = r + (ax[i] + bx[i]) * g.dxt[i] * g.dyh[i];
+        else r = r - (ax[X(m + 1, n)] - ax[i]) * bx[i] * g.dyh[i] / rho;
+        rx[i] = r;
+    }
+    if (g.lcv[i] > 0.5f) {
+        double r = ry[i];
+        if (term == 0) r = r - ay[i];
+        else if (term == 1) r = r + ay[i];
+        else if (term == 2) r = r + (ay[i] + by[i]) * g.dyt[i] * g.dxh[i];
+        else r = r - (ay[X(m, n + 1)] - ay[i]) * by[i] * g.dxh[i] / rho;
+        ry[i] = r;
+    }
+}
+
 // ---- Service/grid_construction.f90:59-112 -----------------------------------
 __global__ void k_gridcon(int m0, int m1, int n0, int n1, Dom D, const float *lu, float *luu,
                           float *luh, float *llu, float *llv, float *lcu, float *lcv)
@@ -592,6 +620,13 @@ void wind_forcing(const Dom &d, const GridDev &g, const Consts &c,
 {
     launch2d(k_wind, d.nx_start, d.nx_end, d.ny_start, d.ny_end, s, d, g, c.rho, taux, tauy,
              rhsx, rhsy);
+}
+
+void rhs2d_term(const Dom &d, const GridDev &g, const Consts &c, int term, double *rx, double *ry,
+                const double *ax, const double *ay, const double *bx, const double *by, cudaStream_t s)
+{
+    launch2d(k_rhs2d_term, d.nx_start, d.nx_end, d.ny_start, d.ny_end, s, d, g, c.rho, term, rx, ry, ax, ay,
+             bx, by);
 }
 
 void gridcon(const Dom &d, const float *lu, float *luu, float *luh, float *llu,

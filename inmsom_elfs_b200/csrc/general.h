@@ -77,6 +77,11 @@ void r_diss(const Dom &d, const GridDev &g, double r_fric, double *r, cudaStream
 void wind_forcing(const Dom &d, const GridDev &g, const Consts &c,
                   const double *taux, const double *tauy, double *rhsx,
                   double *rhsy, cudaStream_t s);
+// Control/dyncall.f90:110-130, one term of the barotropic RHS in the
+// reference's order: 0 r -= a, 1 r += a, 2 r += (a + b) * (dxt*dyh | dyt*dxh),
+// 3 r -= (a(next) - a) * b * (dyh | dxh) / rho (a = slpr, b = hhu | hhv)
+void rhs2d_term(const Dom &d, const GridDev &g, const Consts &c, int term, double *rx, double *ry,
+                const double *ax, const double *ay, const double *bx, const double *by, cudaStream_t s);
 // Service/grid_construction.f90:59-112
 void gridcon(const Dom &d, const float *lu, float *luu, float *luh, float *llu,
              float *llv, float *lcu, float *lcv, cudaStream_t s);

@@ -148,6 +148,15 @@ class BarotropicSolver:
         check(load().inmsom_wind_forcing(self._ctx, dptr(taux), dptr(tauy), dptr(rhsx), dptr(rhsy)))
         return rhsx, rhsy
 
+    def rhs2d(self, rhsx, rhsy, diff_disp=(None, None), tran=(None, None), tran_disp=(None, None),
+              surf_stress=(None, None), bot_stress=(None, None), slpr=None, hhu=None, hhv=None):
+        """Control/dyncall.f90:110-130 on (rhsx, rhsy) in place (inmsom_rhs2d)."""
+        check(load().inmsom_rhs2d(self._ctx, dptr(rhsx), dptr(rhsy), dptr(diff_disp[0]), dptr(diff_disp[1]),
+                                  dptr(tran[0]), dptr(tran[1]), dptr(tran_disp[0]), dptr(tran_disp[1]),
+                                  dptr(surf_stress[0]), dptr(surf_stress[1]), dptr(bot_stress[0]),
+                                  dptr(bot_stress[1]), dptr(slpr), dptr(hhu), dptr(hhv)))
+        return rhsx, rhsy
+
     def r_diss(self, r_fric: float, out=None):
         out = self.basin.bounds.zeros() if out is None else out
         check(load().inmsom_r_diss(self._ctx, float(r_fric), dptr(out)))

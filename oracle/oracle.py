@@ -136,6 +136,19 @@ def wind_forcing(basin, taux=None, tauy=None):
     return rx, ry
 
 
+def rhs2d(basin, rhsx, rhsy, diff_disp=(None, None), tran=(None, None), tran_disp=(None, None),
+          surf_stress=(None, None), bot_stress=(None, None), slpr=None, hhu=None, hhv=None):
+    """Control/dyncall.f90:110-130 on (rhsx, rhsy) in place (ora_rhs2d)."""
+    b = basin.bounds
+    g = grid_struct(basin)
+    hhu = b.zeros() if hhu is None else hhu
+    hhv = b.zeros() if hhv is None else hhv
+    load().ora_rhs2d(ctypes.byref(g), _d(rhsx), _d(rhsy), _d(diff_disp[0]), _d(diff_disp[1]), _d(tran[0]),
+                     _d(tran[1]), _d(tran_disp[0]), _d(tran_disp[1]), _d(surf_stress[0]), _d(surf_stress[1]),
+                     _d(bot_stress[0]), _d(bot_stress[1]), _d(slpr), _d(hhu), _d(hhv))
+    return rhsx, rhsy
+
+
 def hh_init_external(basin):
     g = grid_struct(basin)
     d = basin.depths

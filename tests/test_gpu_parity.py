@@ -286,3 +286,22 @@ def test_last_phases_cover_the_call(gpu, ora):
         up, comp, down = s.last_phases()
         assert up > 0 and comp > 0 and down > 0
         assert up + comp + down <= wall * 1.05 + 0.05
+
+
+@pytest.mark.parametrize("with_all", [True, False])
+def test_rhs2d_bitexact(gpu, ora, with_all):
+    """inmsom_rhs2d (Control/dyncall.f90:110-130) against the oracle's
+    restatement, bit for bit, with every term given or with some absent."""
+    b = prep(basins.regional_basin(nx=180, ny=130, seed=18), ora)
+    rng = np.random.default_rng(19)
+    f = lambda: np.asfortranarray(rng.standard_normal(b.bounds.shape))
+    args = dict(diff_disp=(f(), f()), tran=(f(), f()), tran_disp=(f(), f()), surf_stress=(f(), f()),
+                bot_stress=(f(), f()), slpr=f(), hhu=np.abs(f()) * 100.0, hhv=np.abs(f()) * 100.0)
+    if not with_all:
+        args.update(tran=(None, None), bot_stress=(f(), None), slpr=None)
+    rx, ry = f(), f()
+    ox, oy = ora.rhs2d(b, rx.copy(order="F"), ry.copy(order="F"), **args)
+    with gpu.BarotropicSolver(b, resident=True) as s:
+        gx, gy = s.rhs2d(rx.copy(order="F"), ry.copy(order="F"), **args)
+    assert np.array_equal(gx, ox) and np.array_equal(gy, oy)
+    assert not np.array_equal(gx, rx)
