@@ -161,6 +161,15 @@ int inmsom_r_diss(inmsom_ctx *ctx, double r_fric, double *r_diss);
 int inmsom_wind_forcing(inmsom_ctx *ctx, const double *taux, const double *tauy,
                         double *RHSx2d, double *RHSy2d);
 
+/* After barotropic_dynamics, Control/dyncall.f90:186-201 (the 2-D part of
+ * the mode-split step): at the ocean u points of the interior and its
+ * one-point ring uu2d = ubrtr_i/hhu and pgrx = pgrx - (slpr(m+1,n) -
+ * slpr(m,n))*hhu*dyh/RefDen; likewise vv2d, pgry at v points.  Host arrays;
+ * uu2d, vv2d, pgrx, pgry are updated in place. */
+int inmsom_velocity2d(inmsom_ctx *ctx, double *uu2d, double *vv2d, double *pgrx, double *pgry,
+                      const double *ubrtr_i, const double *vbrtr_i, const double *slpr, const double *hhu,
+                      const double *hhv);
+
 /* The barotropic RHS of Control/dyncall.f90:110-130 (the mode-split caller
  * of barotropic_dynamics), at the ocean u (v) points, in the reference's
  * order of operations:

@@ -28,7 +28,7 @@ EXPORTS = (
     "inmsom_mlp_pack", "inmsom_mlp_forward", "inmsom_mlp_grad", "inmsom_mlp_adam", "inmsom_mlp_batch_indices",
     "inmsom_closure_features", "inmsom_run_closure", "inmsom_closure_tendency", "inmsom_gpu_last_phases",
     "inmsom_step_begin", "inmsom_step_launch", "inmsom_halo_pack", "inmsom_halo_unpack", "inmsom_step_end",
-    "inmsom_gpu_stream", "inmsom_gpu_pitch", "inmsom_rhs2d",
+    "inmsom_gpu_stream", "inmsom_gpu_pitch", "inmsom_rhs2d", "inmsom_velocity2d",
 )
 
 # include/inmsom_gpu.h: INMSOM_MLP_*
@@ -118,6 +118,7 @@ def load() -> ctypes.CDLL:
     FPP = ctypes.POINTER(ctypes.c_float)
     lib.inmsom_gpu_last_phases.argtypes = [VP, FPP, FPP, FPP]
     lib.inmsom_rhs2d.argtypes = [VP] + [DP] * 15
+    lib.inmsom_velocity2d.argtypes = [VP] + [DP] * 9
     lib.inmsom_step_begin.argtypes = [VP]
     lib.inmsom_step_launch.argtypes = [VP, d, d]
     lib.inmsom_halo_pack.argtypes = [VP, i, VP]

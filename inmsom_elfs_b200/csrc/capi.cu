@@ -95,6 +95,7 @@ struct inmsom_ctx {
     double *intl[NINT] = {};
     double *tmp[4] = {};
     double *r2d[7] = {};             // inmsom_rhs2d: RHSx, RHSy, four inputs, a zero field (one block)
+    double *v2d[9] = {};             // inmsom_velocity2d: its nine arrays (one block)
     unsigned long long *d_nbad = nullptr;
     double *d_rows = nullptr, *d_out = nullptr;
 
@@ -392,6 +393,7 @@ int inmsom_gpu_finalize(inmsom_ctx *c)
     for (auto &p : c->intl) cudaFree(p);
     for (auto &p : c->tmp) cudaFree(p);
     cudaFree(c->r2d[0]);   // one block
+    cudaFree(c->v2d[0]);   // one block
     cudaFree(c->d_nbad);
     cudaFree(c->d_rows);
     cudaFree(c->d_out);
@@ -1028,6 +1030,27 @@ int inmsom_rhs2d(inmsom_ctx *c, double *RHSx2d, double *RHSy2d, const double *RH
     CK(cudaGetLastError());
     CKR(d2h(c, RHSx2d, r[0]));
     CKR(d2h(c, RHSy2d, r[1]));
+    return sync_stream(c);
+}
+
+int inmsom_velocity2d(inmsom_ctx *c, double *uu2d, double *vv2d, double *pgrx, double *pgry,
+                      const double *ubrtr_i, const double *vbrtr_i, const double *slpr, const double *hhu,
+                      const double *hhv)
+{
+    CKR(ensure_grid(c));
+    double *const out[4] = {uu2d, vv2d, pgrx, pgry};
+    const double *in[5] = {ubrtr_i, vbrtr_i, slpr, hhu, hhv};
+    for (auto *p : out)
+        if (!p) return set_err(INMSOM_EARG, "inmsom_velocity2d: NULL argument");
+    for (auto *p : in)
+        if (!p) return set_err(INMSOM_EARG, "inmsom_velocity2d: NULL argument");
+    CKR(alloc_block(c, c->v2d, 9));
+    double **v = c->v2d;
+    for (int k = 0; k < 4; k++) CKR(h2d(c, v[k], (const double *)out[k]));
+    for (int k = 0; k < 5; k++) CKR(h2d(c, v[4 + k], in[k]));
+    general::velocity2d(c->dom, c->gdev(), c->c, v[0], v[1], v[2], v[3], v[4], v[5], v[6], v[7], v[8], c->stream);
+    CK(cudaGetLastError());
+    for (int k = 0; k < 4; k++) CKR(d2h(c, out[k], v[k]));
     return sync_stream(c);
 }
 

@@ -402,6 +402,24 @@ __global__ void k_rhs2d_term(int m0, int m1, int n0, int n1, Dom D, GridDev g, d
     }
 }
 
+// ---- Control/dyncall.f90:186-201: corrected 2-D velocity and the slpr part
+// of the time-mean pressure gradient (interior and its one-point ring)
+__global__ void k_velocity2d(int m0, int m1, int n0, int n1, Dom D, GridDev g, double rho, double *uu2d,
+                             double *vv2d, double *pgrx, double *pgry, const double *ubrtr_i,
+                             const double *vbrtr_i, const double *slpr, const double *hhu, const double *hhv)
+{
+    RANGE_GUARD
+    const long long i = X(m, n);
+    if (g.lcu[i] > 0.5f) {
+        uu2d[i] = ubrtr_i[i] / hhu[i];
+        pgrx[i] = pgrx[i] - (slpr[X(m + 1, n)] - slpr[i]) * hhu[i] * g.dyh[i] / rho;
+    }
+    if (g.lcv[i] > 0.5f) {
+        vv2d[i] = vbrtr_i[i] / hhv[i];
+        pgry[i] = pgry[i] - (slpr[X(m, n + 1)] - slpr[i]) * hhv[i] * g.dxh[i] / rho;
+    }
+}
+
 // ---- Service/grid_construction.f90:59-112 -----------------------------------
 __global__ void k_gridcon(int m0, int m1, int n0, int n1, Dom D, const float *lu, float *luu,
                           float *luh, float *llu, float *llv, float *lcu, float *lcv)
@@ -620,6 +638,14 @@ void wind_forcing(const Dom &d, const GridDev &g, const Consts &c,
 {
     launch2d(k_wind, d.nx_start, d.nx_end, d.ny_start, d.ny_end, s, d, g, c.rho, taux, tauy,
              rhsx, rhsy);
+}
+
+void velocity2d(const Dom &d, const GridDev &g, const Consts &c, double *uu2d, double *vv2d, double *pgrx,
+                double *pgry, const double *ubrtr_i, const double *vbrtr_i, const double *slpr, const double *hhu,
+                const double *hhv, cudaStream_t s)
+{
+    launch2d(k_velocity2d, d.nx_start - 1, d.nx_end + 1, d.ny_start - 1, d.ny_end + 1, s, d, g, c.rho, uu2d, vv2d,
+             pgrx, pgry, ubrtr_i, vbrtr_i, slpr, hhu, hhv);
 }
 
 void rhs2d_term(const Dom &d, const GridDev &g, const Consts &c, int term, double *rx, double *ry,

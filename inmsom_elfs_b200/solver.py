@@ -157,6 +157,12 @@ class BarotropicSolver:
                                   dptr(bot_stress[1]), dptr(slpr), dptr(hhu), dptr(hhv)))
         return rhsx, rhsy
 
+    def velocity2d(self, uu2d, vv2d, pgrx, pgry, ubrtr_i, vbrtr_i, slpr, hhu, hhv):
+        """Control/dyncall.f90:186-201 in place (inmsom_velocity2d)."""
+        check(load().inmsom_velocity2d(self._ctx, dptr(uu2d), dptr(vv2d), dptr(pgrx), dptr(pgry), dptr(ubrtr_i),
+                                       dptr(vbrtr_i), dptr(slpr), dptr(hhu), dptr(hhv)))
+        return uu2d, vv2d, pgrx, pgry
+
     def r_diss(self, r_fric: float, out=None):
         out = self.basin.bounds.zeros() if out is None else out
         check(load().inmsom_r_diss(self._ctx, float(r_fric), dptr(out)))

@@ -670,6 +670,30 @@ void ora_rhs2d(const ora_grid *g, double *rhsx2d, double *rhsy2d,
         }
 }
 
+/* Control/dyncall.f90:186-201: the corrected 2-D velocity from the time
+ * means and the sea-level-pressure part of the time-mean pressure gradient,
+ * over nx_start-1..nx_end+1 x ny_start-1..ny_end+1 */
+void ora_velocity2d(const ora_grid *g, double *uu2d, double *vv2d, double *pgrx, double *pgry,
+                    const double *ubrtr_i, const double *vbrtr_i, const double *slpr, const double *hhu,
+                    const double *hhv)
+{
+    SETUP(&g->b);
+    const double rho = g->ref_den;
+#pragma omp parallel for
+    for (int n = B->ny_start - 1; n <= B->ny_end + 1; n++)
+        for (int m = B->nx_start - 1; m <= B->nx_end + 1; m++) {
+            size_t i = I(m, n);
+            if (g->lcu[i] > 0.5f) {
+                uu2d[i] = ubrtr_i[i] / hhu[i];
+                pgrx[i] = pgrx[i] - (slpr[I(m + 1, n)] - slpr[i]) * hhu[i] * g->dyh[i] / rho;
+            }
+            if (g->lcv[i] > 0.5f) {
+                vv2d[i] = vbrtr_i[i] / hhv[i];
+                pgry[i] = pgry[i] - (slpr[I(m, n + 1)] - slpr[i]) * hhv[i] * g->dxh[i] / rho;
+            }
+        }
+}
+
 /* Control/dyncall.f90:452-516 (barotropic fields only) */
 long ora_guard(const ora_grid *g, const double *ssh, const double *u,
                const double *v)

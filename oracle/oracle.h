@@ -144,6 +144,11 @@ void ora_r_diss(const ora_grid *g, double r_fric, double *r_diss);
 void ora_surface_stress(const ora_grid *g, const double *taux,
                         const double *tauy, double *ssx, double *ssy);
 
+/* Control/dyncall.f90:186-201: uu2d = ubrtr_i/hhu, pgrx -= slpr gradient
+ * (and v), on the interior and its one-point ring. */
+void ora_velocity2d(const ora_grid *g, double *uu2d, double *vv2d, double *pgrx, double *pgry,
+                    const double *ubrtr_i, const double *vbrtr_i, const double *slpr, const double *hhu,
+                    const double *hhv);
 /* Control/dyncall.f90:110-130: barotropic forcing assembly.  Any of the
  * optional 3-D-coupling inputs may be NULL, meaning an all-zero field. */
 void ora_rhs2d(const ora_grid *g, double *rhsx2d, double *rhsy2d,

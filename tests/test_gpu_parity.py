@@ -305,3 +305,24 @@ def test_rhs2d_bitexact(gpu, ora, with_all):
         gx, gy = s.rhs2d(rx.copy(order="F"), ry.copy(order="F"), **args)
     assert np.array_equal(gx, ox) and np.array_equal(gy, oy)
     assert not np.array_equal(gx, rx)
+
+
+def test_velocity2d_bitexact(gpu, ora):
+    """inmsom_velocity2d (Control/dyncall.f90:186-201) against the oracle's
+    restatement, bit for bit, after a call of barotropic_dynamics."""
+    b = prep(basins.regional_basin(nx=170, ny=140, seed=20), ora)
+    with gpu.BarotropicSolver(b, resident=True) as s:
+        s.barotropic_dynamics(4 * b.dt, 4)
+        s.sync_to_host(0x1 | 0x2)
+        rng = np.random.default_rng(21)
+        f = lambda: np.asfortranarray(rng.standard_normal(b.bounds.shape))
+        slpr = f()
+        hhu = np.asfortranarray(b.depths["hhu_e"] + 1.0)   # no zero depth at masked points
+        hhv = np.asfortranarray(b.depths["hhv_e"] + 1.0)
+        args = [b.means["ubrtr_i"], b.means["vbrtr_i"], slpr, hhu, hhv]
+        outs = [f(), f(), f(), f()]
+        got = s.velocity2d(*[o.copy(order="F") for o in outs], *args)
+    ref = ora.velocity2d(b, *[o.copy(order="F") for o in outs], *args)
+    for g_, r_ in zip(got, ref):
+        assert np.array_equal(g_, r_)
+    assert not np.array_equal(got[0], outs[0])
