@@ -31,6 +31,13 @@ and device time (a study line).
 with a seeded synthetic state: run_closure against run_substeps (the fused
 inference kernel's cost per evaluation) and the training step (gradient +
 Adam, batch 65536) (a study line; the ncu summaries use it).
+--study baroclinic times the 3-D velocity block of the mode-split step,
+inmsom_baroclinic_dynamics (per-column implicit vertical viscosity solve and
+Robert-Asselin filter) on the regional basin with --nz s-levels (20) and
+seeded synthetic 3-D fields: device time of its kernels with the inputs in
+HBM, the end-to-end call with pinned host arrays, the roofline of the
+column kernel, a full-size bit-exact check against the CPU oracle and the
+oracle's time on the host cores (a study line).
 --study fp32 runs the FP32-velocity variant against the FP64 run on the
 4096 x 4096 ridge basin (2 km, dt = 3 s) for --steps substeps and prints the
 per-field max/RMS differences (a study line, not a benchmark line).
@@ -75,7 +82,9 @@ def parse():
     p.add_argument("--no-cpu", action="store_true")
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--fp32-velocity", action="store_true")
-    p.add_argument("--study", default=None, choices=["fp32", "ensemble", "closure", "closure-kernels"])
+    p.add_argument("--study", default=None,
+                   choices=["fp32", "ensemble", "closure", "closure-kernels", "baroclinic"])
+    p.add_argument("--nz", type=int, default=20, help="s-levels of the baroclinic study")
     p.add_argument("--closure-days", type=float, default=40.0, help="fine spin-up before the training states")
     p.add_argument("--closure-every", type=int, default=10, help="coarse substeps per network evaluation")
     p.add_argument("--closure-tau", type=float, default=0.3, help="wind stress amplitude, N/m^2")
@@ -520,9 +529,91 @@ def run_study_closure_kernels(args):
                       "steps": nsub, "results": res}), flush=True)
 
 
+BARO_BYTES_PER_CELL_LEVEL = 14 * 8     # 10 nz-level fields read, 4 written (FP64)
+BARO_BYTES_PER_COLUMN = 23 * 8 + 2 * 4  # 2-D fields, metrics and the lcu/lcv masks read once
+
+
+def _pinned_like(a):
+    """A pinned host copy of a Fortran-ordered array (same shape and order)."""
+    import torch
+    t = torch.empty(tuple(reversed(a.shape)), dtype=torch.float64, pin_memory=True)
+    out = t.numpy().T
+    out[...] = a
+    return out
+
+
+def run_study_baroclinic(args):
+    """inmsom_baroclinic_dynamics on the regional basin with nz s-levels."""
+    import torch
+    from inmsom_elfs_b200 import basins, solver
+    torch.cuda.set_device(0)
+    b = workload(args, 0)
+    basins.finalize(b, solver.GpuBackend(0))
+    nz, tau = args.nz, 60.0
+    dz, hzt = basins.vertical_grid(nz, 0)
+    f = basins.column_fields(b, nz, seed=1, tau=tau)
+    names = ("uu", "uup", "vv", "vvp")
+    host = {k: _pinned_like(v) for k, v in f.items() if k != "wflux"}
+    first = None
+    comp, tot = [], []
+    clk = Clocks(0)
+    with solver.BarotropicSolver(b, resident=False) as s, clk:
+        flds = {k: host[k] for k in s.BAROCLINIC_FIELDS}
+        st = [host[k] for k in names]
+        calls = max(args.steps, 1)
+        for it in range(args.warmup + calls):
+            for k in names:                       # the same inputs every call
+                st[names.index(k)][...] = f[k]
+            s.baroclinic_dynamics(dz, hzt, tau, *st, **flds)
+            if first is None:
+                first = [a.copy(order="F") for a in st]
+            if it >= args.warmup:
+                up, cm, dn = s.last_phases()
+                comp.append(cm)
+                tot.append(up + cm + dn)
+    cells = b.bounds.nx * b.bounds.ny
+    units = cells * nz
+    ms = statistics.median(comp)
+    ms_e2e = statistics.median(tot)
+    alg = units * BARO_BYTES_PER_CELL_LEVEL + cells * BARO_BYTES_PER_COLUMN
+    peak, src = measured_hbm()
+    h2d = sum(f[k].nbytes for k in f if k != "wflux") + dz.nbytes + hzt.nbytes
+    d2h = sum(f[k].nbytes for k in names)
+    line = {
+        "study": "baroclinic", "metric": "cell-level-steps/s", "unit": "cell-level-steps/s",
+        "value": units / (ms / 1e3), "ms_per_call": ms, "calls": len(comp), "warmup": args.warmup,
+        "dtype": "f64", "data": "synthetic (seeded 3-D fields on the regional basin)",
+        "config": {"workload": f"baroclinic_dynamics on regional_basin {b.bounds.nx}x{b.bounds.ny}, nz={nz}",
+                   "nz": nz, "tau_s": tau, "cells": cells, "land_fraction": round(float(b.info["land_fraction"]), 4),
+                   "l2": "inputs larger than L2 (%.1f GB on the device)" % (h2d / 1e9)},
+        "e2e": {"value": units / (ms_e2e / 1e3), "unit": "cell-level-steps/s", "ms_per_call": ms_e2e,
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / (ms / 1e3) / 1e9 / peak, "traffic": None, "peak_source": src,
+                     "algorithmic_bytes_per_call": int(alg),
+                     "kernels_timed": "k_columns + k_border (the compute phase of the call)"},
+        "gpu_launches": 2 * len(comp),
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu:
+        from oracle import oracle as ora
+        threads = os.cpu_count() or 1
+        ora.set_threads(threads)
+        ref = [f[k].copy(order="F") for k in names]
+        t0 = time.perf_counter()
+        ora.baroclinic_dynamics(b, dz, hzt, tau, *ref, **{k: f[k] for k in ora.BAROCLINIC_FIELDS})
+        el = time.perf_counter() - t0
+        line["parity_full_size"] = all(np.array_equal(x, y) for x, y in zip(first, ref))
+        line["cpu_baseline"] = {"value": units / el, "unit": "cell-level-steps/s", "cores": threads, "kind": "port",
+                                "sample": f"one baroclinic_dynamics call of the same workload ({el:.2f} s)"}
+    print(json.dumps(line), flush=True)
+
+
 if __name__ == "__main__":
     a = parse()
-    if a.study == "closure-kernels":
+    if a.study == "baroclinic":
+        run_study_baroclinic(a)
+    elif a.study == "closure-kernels":
         run_study_closure_kernels(a)
     elif a.study == "closure":
         run_study_closure(a)

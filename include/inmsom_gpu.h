@@ -170,6 +170,40 @@ int inmsom_velocity2d(inmsom_ctx *ctx, double *uu2d, double *vv2d, double *pgrx,
                       const double *ubrtr_i, const double *vbrtr_i, const double *slpr, const double *hhu,
                       const double *hhv);
 
+/* Replaces baroclinic_dynamics, Function/vel_ssh.f90:794-1027: the 3-D
+ * horizontal velocity after the implicit vertical viscosity solve of each
+ * water column (the tridiagonal sweep factor8,
+ * Service/oc_algorithms.f90:494-524) with vertical advection, Coriolis,
+ * the pressure gradient, drag and surface/bottom stress, then the
+ * Robert-Asselin filter on the interior and its one-point ring.  Same
+ * arguments as the reference routine (Control/dyncall.f90:349-366 passes
+ * anzu as nu, r_diss as rdis, the surface/bottom stresses as tx_*, ty_*),
+ * plus what it reads from its modules: nz and the vertical grid dz (nz),
+ * hzt (nz + 1) of main_basin_pars, and the internal-mode depths hhu, hhup,
+ * hhun, hhv, hhvp, hhvn, hhh of basin_grid.  3-D host arrays are
+ * (bnd_x1:bnd_x2, bnd_y1:bnd_y2, levels) in Fortran order with nz levels
+ * (ww and nu nz + 1), the rest 2-D in the registered layout.  uu, uup, vv,
+ * vvp are updated in place.  2 <= nz <= 200 (the reference's surface point
+ * reads level 2), else INMSOM_EARG; a periodic wrap column inside the
+ * interior gives INMSOM_EUNSUPPORTED.  inmsom_gpu_last_phases times it. */
+int inmsom_baroclinic_dynamics(inmsom_ctx *ctx, int nz, const double *dz, const double *hzt, double tau,
+                               double *uu, double *uup, double *vv, double *vvp, const double *ww,
+                               const double *nu, const double *RHSx, const double *RHSy,
+                               const double *RHSx_tran, const double *RHSy_tran, const double *pgrx,
+                               const double *pgry, const double *rdis, const double *tx_surf,
+                               const double *ty_surf, const double *tx_bot, const double *ty_bot,
+                               const double *hhu, const double *hhup, const double *hhun, const double *hhv,
+                               const double *hhvp, const double *hhvn, const double *hhh);
+
+/* Replaces vertical_velocity, Function/vel_ssh.f90:1030-1076 (called at
+ * Control/dyncall.f90:186): w from the continuity equation, integrated up
+ * from w(nz+1) = 0 at the ocean T points of the interior, then the periodic
+ * wrap.  u, v have nz levels, w nz + 1 (updated in place; other points keep
+ * their values); hu, hv, wflux are 2-D; dz (nz) is the vertical grid.
+ * inmsom_gpu_last_phases times it. */
+int inmsom_vertical_velocity(inmsom_ctx *ctx, int nz, const double *dz, const double *u, const double *v,
+                             double *w, const double *hu, const double *hv, const double *wflux);
+
 /* The barotropic RHS of Control/dyncall.f90:110-130 (the mode-split caller
  * of barotropic_dynamics), at the ocean u (v) points, in the reference's
  * order of operations:
@@ -289,10 +323,12 @@ int inmsom_load_state(inmsom_ctx *ctx, double *ubrtr_e, double *ubrtrp_e,
  * static string saying why the fused path is not eligible (or "eligible"). */
 int inmsom_gpu_path(inmsom_ctx *ctx, int *path, const char **reason);
 /* Device time of the phases of the last completed
- * inmsom_barotropic_dynamics call (CUDA events on the context's stream):
- * host->device copies, the substeps (with the depth and time-mean work),
- * device->host copies.  The reference times the whole call
- * (Control/dyncall.f90:135,165-167 start_timer/end_timer). */
+ * inmsom_barotropic_dynamics, inmsom_baroclinic_dynamics or
+ * inmsom_vertical_velocity call (CUDA events on the context's stream):
+ * host->device copies, the computation (for the barotropic call the
+ * substeps with the depth and time-mean work), device->host copies.  The
+ * reference times the whole calls (Control/dyncall.f90:135,165-167 and
+ * :348,367-368 start_timer/end_timer). */
 int inmsom_gpu_last_phases(inmsom_ctx *ctx, float *upload_ms, float *compute_ms, float *download_ms);
 
 /* Ensemble of independent basins (no counterpart in the reference, which

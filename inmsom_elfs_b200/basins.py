@@ -336,3 +336,53 @@ def finalize(basin: Basin, backend) -> Basin:
         rx, ry = backend.wind_forcing(basin)
         basin.forcing["RHSx"], basin.forcing["RHSy"] = rx, ry
     return basin
+
+
+def vertical_grid(nz: int, seed: int = 0):
+    """Sigma-level thicknesses dz (nz, summing to 1) and interface spacings
+    hzt (nz + 1: half layers at the surface and the bottom, the mean of the
+    two layers between), the steps Service/basin_parameters.f90:113-121
+    (vgrid) derives from the level depths; the thicknesses are seeded and
+    uneven."""
+    rng = np.random.default_rng(seed)
+    dz = rng.uniform(0.5, 1.5, nz)
+    dz /= dz.sum()
+    hzt = np.empty(nz + 1)
+    hzt[0], hzt[-1] = dz[0] / 2.0, dz[-1] / 2.0
+    hzt[1:-1] = (dz[:-1] + dz[1:]) / 2.0
+    return dz, hzt
+
+
+def column_fields(basin: Basin, nz: int, seed: int = 0, depth: float = 50.0, tau: float = 60.0) -> dict:
+    """Seeded synthetic inputs of the 3-D velocity block of the mode-split
+    step (Function/vel_ssh.f90:794-1076) on `basin`: the velocity time
+    levels uu, uup, vv, vvp (nz levels), the vertical velocity ww and
+    viscosity nu (nz + 1 levels), the 3-D RHS terms, the 2-D pressure
+    gradient, drag and stresses, and the internal-mode depths (positive
+    everywhere).  Magnitudes follow a shelf sea of `depth` metres: the
+    velocities are O(0.1 m/s) and every RHS term is a fraction of the time
+    term bp*u, so each term moves the solution."""
+    rng = np.random.default_rng(seed)
+    shp = basin.bounds.shape
+    area = float(np.median(basin.metrics["dxt"]) * np.median(basin.metrics["dyh"]))
+    scale = depth * area / tau * 0.1          # bp * 0.1 m/s, the RHS unit
+
+    def f3(s, lev=nz):
+        return np.asfortranarray(s * rng.standard_normal((*shp, lev)))
+
+    def f2(s):
+        return np.asfortranarray(s * rng.standard_normal(shp))
+
+    def pos(lo, hi, lev=None):
+        return np.asfortranarray(rng.uniform(lo, hi, shp if lev is None else (*shp, lev)))
+
+    out = dict(uu=f3(0.1), uup=f3(0.1), vv=f3(0.1), vvp=f3(0.1),
+               ww=f3(1.0e-3, nz + 1), nu=pos(1.0e-4, 1.0e-2, nz + 1),
+               rhsx=f3(0.05 * scale), rhsy=f3(0.05 * scale), rhsx_tran=f3(0.05 * scale),
+               rhsy_tran=f3(0.05 * scale), pgrx=f2(0.05 * scale), pgry=f2(0.05 * scale),
+               rdis=pos(0.0, 2.0e-5), tx_surf=f2(1.0e-4), ty_surf=f2(1.0e-4), tx_bot=f2(1.0e-4),
+               ty_bot=f2(1.0e-4))
+    for k in ("hhu", "hhup", "hhun", "hhv", "hhvp", "hhvn", "hhh"):
+        out[k] = pos(0.8 * depth, 1.2 * depth)
+    out["wflux"] = f2(1.0e-5 * basin.consts.ref_den)
+    return out

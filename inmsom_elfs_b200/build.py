@@ -1,8 +1,9 @@
 """Build recipe of the CUDA library libinmsom_gpu.so (sm_100a only).
 
 The library is built in-tree, next to this file, so that it travels with
-the repository.  general.cu is compiled with --fmad=false (per-loop kernels
-that round exactly like the Fortran expressions); the fused streaming
+the repository.  general.cu and column.cu are compiled with --fmad=false
+(per-loop and per-column kernels that round exactly like the Fortran
+expressions); the fused streaming
 kernel and the C ABI layer use the default contraction.
 """
 from __future__ import annotations
@@ -27,8 +28,9 @@ SOURCES = {
     "capi.cu": [],
     "noalloc.cu": [],
     "closure.cu": [],
+    "column.cu": ["--fmad=false"],
 }
-HEADERS = ["common.cuh", "general.h", "fused.h", "closure.h"]
+HEADERS = ["common.cuh", "general.h", "fused.h", "closure.h", "column.h"]
 
 
 def nvcc() -> str:

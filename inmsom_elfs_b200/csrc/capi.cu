@@ -14,6 +14,7 @@
 
 #include "common.cuh"
 #include "closure.h"
+#include "column.h"
 #include "fused.h"
 #include "general.h"
 
@@ -96,6 +97,10 @@ struct inmsom_ctx {
     double *tmp[4] = {};
     double *r2d[7] = {};             // inmsom_rhs2d: RHSx, RHSy, four inputs, a zero field (one block)
     double *v2d[9] = {};             // inmsom_velocity2d: its nine arrays (one block)
+    // inmsom_baroclinic_dynamics / inmsom_vertical_velocity: fields of col_nz
+    // levels in one block (col3, colw, col2) and dz, hzt
+    double *col = nullptr, *col_lev = nullptr;
+    int col_nz = 0;
     unsigned long long *d_nbad = nullptr;
     double *d_rows = nullptr, *d_out = nullptr;
 
@@ -394,6 +399,8 @@ int inmsom_gpu_finalize(inmsom_ctx *c)
     for (auto &p : c->tmp) cudaFree(p);
     cudaFree(c->r2d[0]);   // one block
     cudaFree(c->v2d[0]);   // one block
+    cudaFree(c->col);
+    cudaFree(c->col_lev);
     cudaFree(c->d_nbad);
     cudaFree(c->d_rows);
     cudaFree(c->d_out);
@@ -576,7 +583,7 @@ int inmsom_barotropic_dynamics(inmsom_ctx *c, double tau, int nstep, int ksw4, d
 int inmsom_gpu_last_phases(inmsom_ctx *c, float *upload_ms, float *compute_ms, float *download_ms)
 {
     if (!c || !upload_ms || !compute_ms || !download_ms) return set_err(INMSOM_EARG, "NULL argument");
-    if (!c->ph_valid) return set_err(INMSOM_EARG, "no completed inmsom_barotropic_dynamics call");
+    if (!c->ph_valid) return set_err(INMSOM_EARG, "no completed timed call");
     CK(cudaEventElapsedTime(upload_ms, c->ph[0], c->ph[1]));
     CK(cudaEventElapsedTime(compute_ms, c->ph[1], c->ph[2]));
     CK(cudaEventElapsedTime(download_ms, c->ph[2], c->ph[3]));
@@ -1052,6 +1059,154 @@ int inmsom_velocity2d(inmsom_ctx *c, double *uu2d, double *vv2d, double *pgrx, d
     CK(cudaGetLastError());
     for (int k = 0; k < 4; k++) CKR(d2h(c, out[k], v[k]));
     return sync_stream(c);
+}
+
+namespace {
+
+// the block of the 3-D velocity calls: NC3 fields of nz levels, ww and nu
+// (nz + 1 levels each), then NC2 2-D fields
+enum { C3_UU, C3_UUP, C3_VV, C3_VVP, C3_RHSX, C3_RHSY, C3_RHSXT, C3_RHSYT, C3_UUO, C3_UUPO, C3_VVO, C3_VVPO, NC3 };
+constexpr int NC2 = 14;
+
+size_t col_plane(const inmsom_ctx *c) { return (size_t)c->dom.pitch * (size_t)c->dom.nya(); }
+double *col3(inmsom_ctx *c, int f) { return c->col + (size_t)f * c->col_nz * col_plane(c); }
+double *colw(inmsom_ctx *c, int f) { return c->col + ((size_t)NC3 * c->col_nz + (size_t)f * (c->col_nz + 1)) * col_plane(c); }
+double *col2(inmsom_ctx *c, int f)
+{
+    return c->col + ((size_t)NC3 * c->col_nz + 2 * (size_t)(c->col_nz + 1) + f) * col_plane(c);
+}
+
+int col_alloc(inmsom_ctx *c, int nz)
+{
+    if (c->col && c->col_nz == nz) return INMSOM_OK;
+    cudaFree(c->col);
+    cudaFree(c->col_lev);
+    c->col = c->col_lev = nullptr;
+    c->col_nz = 0;
+    const size_t planes = (size_t)NC3 * nz + 2 * (size_t)(nz + 1) + NC2;
+    CK(cudaMalloc((void **)&c->col, planes * col_plane(c) * sizeof(double)));
+    CK(cudaMemsetAsync(c->col, 0, planes * col_plane(c) * sizeof(double), c->stream));
+    CK(cudaMalloc((void **)&c->col_lev, (2 * (size_t)nz + 1) * sizeof(double)));
+    c->col_nz = nz;
+    return INMSOM_OK;
+}
+
+// nlev levels of a host array (bnd_x1:bnd_x2, bnd_y1:bnd_y2, nlev): the
+// host rows of consecutive levels follow each other, as do the device rows
+int h2d3(inmsom_ctx *c, double *dev, const double *host, int nlev)
+{
+    if (!host) return set_err(INMSOM_EARG, "NULL host array");
+    const size_t w = (size_t)c->dom.nxa() * sizeof(double);
+    CK(cudaMemcpy2DAsync(dev + c->dom.xoff, (size_t)c->dom.pitch * sizeof(double), host, w, w,
+                         (size_t)c->dom.nya() * nlev, cudaMemcpyHostToDevice, c->stream));
+    return INMSOM_OK;
+}
+
+int d2h3(inmsom_ctx *c, double *host, const double *dev, int nlev)
+{
+    const size_t w = (size_t)c->dom.nxa() * sizeof(double);
+    CK(cudaMemcpy2DAsync(host, w, dev + c->dom.xoff, (size_t)c->dom.pitch * sizeof(double), w,
+                         (size_t)c->dom.nya() * nlev, cudaMemcpyDeviceToHost, c->stream));
+    return INMSOM_OK;
+}
+
+column::Levels col_levels(inmsom_ctx *c)
+{
+    column::Levels L;
+    L.nz = c->col_nz;
+    L.plane = (long long)col_plane(c);
+    L.dz = c->col_lev;
+    L.hzt = c->col_lev + c->col_nz;
+    return L;
+}
+
+}  // namespace
+
+int inmsom_baroclinic_dynamics(inmsom_ctx *c, int nz, const double *dz, const double *hzt, double tau,
+                               double *uu, double *uup, double *vv, double *vvp, const double *ww,
+                               const double *nu, const double *RHSx, const double *RHSy,
+                               const double *RHSx_tran, const double *RHSy_tran, const double *pgrx,
+                               const double *pgry, const double *rdis, const double *tx_surf,
+                               const double *ty_surf, const double *tx_bot, const double *ty_bot,
+                               const double *hhu, const double *hhup, const double *hhun, const double *hhv,
+                               const double *hhvp, const double *hhvn, const double *hhh)
+{
+    CKR(ensure_grid(c));
+    if (nz < 2 || nz > column::max_levels())
+        return set_err(INMSOM_EARG, "inmsom_baroclinic_dynamics: nz = %d outside 2..%d", nz, column::max_levels());
+    if (!(tau > 0.0)) return set_err(INMSOM_EARG, "tau must be > 0");
+    double *const io[4] = {uu, uup, vv, vvp};
+    const double *in3[4] = {RHSx, RHSy, RHSx_tran, RHSy_tran};
+    const double *in2[NC2] = {pgrx, pgry, rdis, tx_surf, ty_surf, tx_bot, ty_bot,
+                              hhu,  hhup, hhun, hhv,     hhvp,    hhvn,   hhh};
+    bool null = !dz || !hzt || !ww || !nu;
+    for (auto *p : io) null = null || !p;
+    for (auto *p : in3) null = null || !p;
+    for (auto *p : in2) null = null || !p;
+    if (null) return set_err(INMSOM_EARG, "inmsom_baroclinic_dynamics: NULL argument");
+    const Dom &d = c->dom;
+    if (column::wrap_inside(d)) return set_err(INMSOM_EUNSUPPORTED, "inmsom_baroclinic_dynamics: a periodic wrap column/row lies in the interior");
+    CKR(col_alloc(c, nz));
+    c->ph_valid = false;
+    CK(cudaEventRecord(c->ph[0], c->stream));
+    for (int k = 0; k < 4; k++) CKR(h2d3(c, col3(c, C3_UU + k), io[k], nz));
+    for (int k = 0; k < 4; k++) CKR(h2d3(c, col3(c, C3_RHSX + k), in3[k], nz));
+    CKR(h2d3(c, colw(c, 0), ww, nz + 1));
+    CKR(h2d3(c, colw(c, 1), nu, nz + 1));
+    for (int k = 0; k < NC2; k++) CKR(h2d(c, col2(c, k), in2[k]));
+    CK(cudaMemcpyAsync(c->col_lev, dz, nz * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->col_lev + nz, hzt, (nz + 1) * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaEventRecord(c->ph[1], c->stream));
+    column::BaroclinicArgs a;
+    a.tau = tau;
+    a.uu = col3(c, C3_UU); a.uup = col3(c, C3_UUP); a.vv = col3(c, C3_VV); a.vvp = col3(c, C3_VVP);
+    a.ww = colw(c, 0); a.nu = colw(c, 1);
+    a.rhsx = col3(c, C3_RHSX); a.rhsy = col3(c, C3_RHSY);
+    a.rhsx_tran = col3(c, C3_RHSXT); a.rhsy_tran = col3(c, C3_RHSYT);
+    a.pgrx = col2(c, 0); a.pgry = col2(c, 1); a.rdis = col2(c, 2);
+    a.tx_surf = col2(c, 3); a.ty_surf = col2(c, 4); a.tx_bot = col2(c, 5); a.ty_bot = col2(c, 6);
+    a.hhu = col2(c, 7); a.hhup = col2(c, 8); a.hhun = col2(c, 9);
+    a.hhv = col2(c, 10); a.hhvp = col2(c, 11); a.hhvn = col2(c, 12); a.hhh = col2(c, 13);
+    a.uu_out = col3(c, C3_UUO); a.uup_out = col3(c, C3_UUPO); a.vv_out = col3(c, C3_VVO); a.vvp_out = col3(c, C3_VVPO);
+    if (column::baroclinic_dynamics(d, c->gdev(), c->c, col_levels(c), a, c->stream))
+        return set_err(INMSOM_ECUDA, "inmsom_baroclinic_dynamics: launch failed: %s",
+                       cudaGetErrorString(cudaGetLastError()));
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ph[2], c->stream));
+    for (int k = 0; k < 4; k++) CKR(d2h3(c, io[k], col3(c, C3_UUO + k), nz));
+    CK(cudaEventRecord(c->ph[3], c->stream));
+    CKR(sync_stream(c));
+    c->ph_valid = true;
+    return INMSOM_OK;
+}
+
+int inmsom_vertical_velocity(inmsom_ctx *c, int nz, const double *dz, const double *u, const double *v, double *w,
+                             const double *hu, const double *hv, const double *wflux)
+{
+    CKR(ensure_grid(c));
+    if (nz < 1) return set_err(INMSOM_EARG, "inmsom_vertical_velocity: nz = %d < 1", nz);
+    if (!dz || !u || !v || !w || !hu || !hv || !wflux)
+        return set_err(INMSOM_EARG, "inmsom_vertical_velocity: NULL argument");
+    CKR(col_alloc(c, nz));
+    c->ph_valid = false;
+    CK(cudaEventRecord(c->ph[0], c->stream));
+    CKR(h2d3(c, col3(c, C3_UU), u, nz));
+    CKR(h2d3(c, col3(c, C3_VV), v, nz));
+    CKR(h2d3(c, colw(c, 0), w, nz + 1));
+    CKR(h2d(c, col2(c, 0), hu));
+    CKR(h2d(c, col2(c, 1), hv));
+    CKR(h2d(c, col2(c, 2), wflux));
+    CK(cudaMemcpyAsync(c->col_lev, dz, nz * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaEventRecord(c->ph[1], c->stream));
+    column::vertical_velocity(c->dom, c->gdev(), c->c, col_levels(c), col3(c, C3_UU), col3(c, C3_VV), colw(c, 0),
+                              col2(c, 0), col2(c, 1), col2(c, 2), c->stream);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ph[2], c->stream));
+    CKR(d2h3(c, w, colw(c, 0), nz + 1));
+    CK(cudaEventRecord(c->ph[3], c->stream));
+    CKR(sync_stream(c));
+    c->ph_valid = true;
+    return INMSOM_OK;
 }
 
 int inmsom_hh_init_external(inmsom_ctx *c, const double *ssh_e, const double *sshp_e)

@@ -1,0 +1,53 @@
+// Per-water-column kernels of the 3-D velocity block: the implicit vertical
+// viscosity solve of baroclinic_dynamics (Function/vel_ssh.f90:794-1027,
+// tridiagonal sweep factor8 of Service/oc_algorithms.f90:494-524) and the
+// continuity integral of vertical_velocity (Function/vel_ssh.f90:1030-1076).
+//
+// 3-D fields are stacks of pitched 2-D levels: level k (0-based) of a field
+// starts plane * k doubles after level 0, and element (m, n) of a level sits
+// where ix(d, m, n) puts it.  column.cu is compiled with --fmad=false and
+// follows the Fortran expression order, so the results are bit-exact with
+// a non-contracting build of the reference.
+#pragma once
+
+#include "common.cuh"
+
+namespace inmsom {
+namespace column {
+
+struct Levels {
+    int nz;                 // s-levels; ww and nu have nz + 1
+    long long plane;        // doubles per level
+    const double *dz;       // nz layer thicknesses (device)
+    const double *hzt;      // nz + 1 interface spacings (device)
+};
+
+struct BaroclinicArgs {
+    double tau;
+    // nz levels (ww, nu: nz + 1), read only
+    const double *uu, *uup, *vv, *vvp, *ww, *nu, *rhsx, *rhsy, *rhsx_tran, *rhsy_tran;
+    // 2-D
+    const double *pgrx, *pgry, *rdis, *tx_surf, *ty_surf, *tx_bot, *ty_bot;
+    const double *hhu, *hhup, *hhun, *hhv, *hhvp, *hhvn, *hhh;
+    // nz levels: uu, uup, vv, vvp after the step (every point of the arrays)
+    double *uu_out, *uup_out, *vv_out, *vvp_out;
+};
+
+// largest nz the solve supports (its sweep coefficients live in shared memory)
+int max_levels();
+// true when a periodic wrap column/row lies inside the interior (the filter
+// would then need the wrapped value at an interior point; not supported)
+bool wrap_inside(const Dom &d);
+
+// Function/vel_ssh.f90:794-1027 on one domain.  Returns 0, or -1 when nz is
+// out of range or a periodic wrap column/row lies inside the interior.
+int baroclinic_dynamics(const Dom &d, const GridDev &g, const Consts &c, const Levels &L,
+                        const BaroclinicArgs &a, cudaStream_t s);
+
+// Function/vel_ssh.f90:1030-1076: w (nz + 1 levels) in place.
+int vertical_velocity(const Dom &d, const GridDev &g, const Consts &c, const Levels &L, const double *u,
+                      const double *v, double *w, const double *hu, const double *hv, const double *wflux,
+                      cudaStream_t s);
+
+}  // namespace column
+}  // namespace inmsom

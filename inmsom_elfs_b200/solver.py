@@ -163,6 +163,47 @@ class BarotropicSolver:
                                        dptr(vbrtr_i), dptr(slpr), dptr(hhu), dptr(hhv)))
         return uu2d, vv2d, pgrx, pgry
 
+    BAROCLINIC_FIELDS = ("ww", "nu", "rhsx", "rhsy", "rhsx_tran", "rhsy_tran", "pgrx", "pgry", "rdis",
+                         "tx_surf", "ty_surf", "tx_bot", "ty_bot", "hhu", "hhup", "hhun", "hhv", "hhvp",
+                         "hhvn", "hhh")
+
+    def baroclinic_dynamics(self, dz, hzt, tau: float, uu, uup, vv, vvp, **fields):
+        """Function/vel_ssh.f90:794-1027 in place on uu, uup, vv, vvp
+        (inmsom_baroclinic_dynamics).  3-D arrays are (bnd_x, bnd_y, nz) in
+        Fortran order, ww and nu with nz + 1 levels; `fields` holds
+        BAROCLINIC_FIELDS by name (hh*: the internal-mode depths)."""
+        dz = np.ascontiguousarray(dz, dtype=np.float64)
+        hzt = np.ascontiguousarray(hzt, dtype=np.float64)
+        nz = len(dz)
+        if len(hzt) != nz + 1:
+            raise ValueError("hzt needs nz + 1 values")
+        shp = self.basin.bounds.shape
+        for name, a in (("uu", uu), ("uup", uup), ("vv", vv), ("vvp", vvp)):
+            if a.shape != (*shp, nz):
+                raise ValueError(f"{name}: expected shape {(*shp, nz)}")
+        for name in ("ww", "nu"):
+            if fields[name].shape != (*shp, nz + 1):
+                raise ValueError(f"{name}: expected shape {(*shp, nz + 1)}")
+        for name in ("rhsx", "rhsy", "rhsx_tran", "rhsy_tran"):
+            if fields[name].shape != (*shp, nz):
+                raise ValueError(f"{name}: expected shape {(*shp, nz)}")
+        check(load().inmsom_baroclinic_dynamics(self._ctx, nz, dz.ctypes.data_as(_lib.DP), hzt.ctypes.data_as(_lib.DP),
+                                                float(tau), dptr(uu), dptr(uup), dptr(vv), dptr(vvp),
+                                                *[dptr(fields[k]) for k in self.BAROCLINIC_FIELDS]))
+        return uu, uup, vv, vvp
+
+    def vertical_velocity(self, dz, u, v, w, hu, hv, wflux):
+        """Function/vel_ssh.f90:1030-1076: w (nz + 1 levels) in place
+        (inmsom_vertical_velocity)."""
+        dz = np.ascontiguousarray(dz, dtype=np.float64)
+        nz = len(dz)
+        shp = self.basin.bounds.shape
+        if u.shape != (*shp, nz) or v.shape != (*shp, nz) or w.shape != (*shp, nz + 1):
+            raise ValueError("u, v need nz levels and w nz + 1")
+        check(load().inmsom_vertical_velocity(self._ctx, nz, dz.ctypes.data_as(_lib.DP), dptr(u), dptr(v), dptr(w),
+                                              dptr(hu), dptr(hv), dptr(wflux)))
+        return w
+
     def r_diss(self, r_fric: float, out=None):
         out = self.basin.bounds.zeros() if out is None else out
         check(load().inmsom_r_diss(self._ctx, float(r_fric), dptr(out)))

@@ -670,6 +670,191 @@ void ora_rhs2d(const ora_grid *g, double *rhsx2d, double *rhsy2d,
         }
 }
 
+/* Service/oc_algorithms.f90:494-524 factor8: the tridiagonal system
+ * a(n) f(n-1) + b(n) f(n) + c(n) f(n+1) = eta(n), n = 1..nd (0-based here),
+ * forward elimination then back substitution, in the reference's order. */
+static void factor8(int nd, const double *a, const double *b, const double *c, const double *eta,
+                    double *rksi, double *x, double *y)
+{
+    x[0] = -c[0] / b[0];
+    y[0] = eta[0] / b[0];
+    for (int j = 1; j < nd; j++) {
+        const double scr = 1.0 / (a[j] * x[j - 1] + b[j]);
+        x[j] = -c[j] * scr;
+        y[j] = (eta[j] - a[j] * y[j - 1]) * scr;
+    }
+    rksi[nd - 1] = y[nd - 1];
+    for (int j = nd - 2; j >= 0; j--) rksi[j] = x[j] * rksi[j + 1] + y[j];
+}
+
+/* Function/vel_ssh.f90:794-1027 baroclinic_dynamics: implicit vertical
+ * viscosity per water column (factor8), vertical advection, Coriolis, drag,
+ * surface and bottom stress, then the Robert-Asselin filter.  3-D arrays
+ * are (bnd_x1:bnd_x2, bnd_y1:bnd_y2, levels), levels nz (nz+1 for ww, nu);
+ * dz(nz), hzt(nz+1); hh* are the internal-mode depths of basin_grid. */
+void ora_baroclinic_dynamics(const ora_grid *g, int nz, const double *dz, const double *hzt, double tau,
+                             double *uu, double *uup, double *vv, double *vvp, const double *ww,
+                             const double *nu, const double *rhsx, const double *rhsy,
+                             const double *rhsx_tran, const double *rhsy_tran, const double *pgrx,
+                             const double *pgry, const double *rdis, const double *tx_surf,
+                             const double *ty_surf, const double *tx_bot, const double *ty_bot,
+                             const double *hhu, const double *hhup, const double *hhun, const double *hhv,
+                             const double *hhvp, const double *hhvn, const double *hhh)
+{
+    SETUP(&g->b);
+    const size_t nt = NTOT(B);
+#define I3(m, n, k) (I(m, n) + (size_t)((k) - 1) * nt)
+    double *un = calloc(nt * (size_t)nz, sizeof(double));
+    double *vn = calloc(nt * (size_t)nz, sizeof(double));
+    /* :847-983 */
+#pragma omp parallel for
+    for (int n = B->ny_start; n <= B->ny_end; n++) {
+        double *a = malloc(6 * (size_t)nz * sizeof(double));
+        double *bb = a + nz, *c = bb + nz, *eta = c + nz, *x = eta + nz, *y = x + nz;
+        double *rksi = malloc((size_t)nz * sizeof(double));
+        for (int m = B->nx_start; m <= B->nx_end; m++) {
+            const size_t i = I(m, n);
+            if (g->lcu[i] > 0.5f) {
+                const double bp = hhun[i] * g->dxt[i] * g->dyh[i] / tau / 2.0;
+                const double bp0 = hhup[i] * g->dxt[i] * g->dyh[i] / tau / 2.0;
+                double dp = 0.0, dm = 0.0, fz_p = 0.0, fz_m = 0.0;
+                for (int k = 1; k <= nz; k++) {
+                    dm = dp;
+                    fz_m = fz_p;
+                    if (k < nz) {
+                        dp = (nu[I3(m, n, k + 1)] + nu[I3(m + 1, n, k + 1)]) / 2.0 / hhun[i] / hzt[k] * g->dxt[i] *
+                             g->dyh[i];
+                        fz_p = (ww[I3(m, n, k + 1)] * g->dx[i] * g->dy[i] +
+                                ww[I3(m + 1, n, k + 1)] * g->dx[I(m + 1, n)] * g->dy[I(m + 1, n)]) /
+                               2.0 * (uu[I3(m, n, k)] + uu[I3(m, n, k + 1)]) / 2.0;
+                    } else {
+                        dp = 0.0;
+                        fz_p = 0.0;
+                    }
+                    const int q = k - 1;
+                    c[q] = k < nz ? -dp / dz[q] : 0.0;
+                    a[q] = k > 1 ? -dm / dz[q] : 0.0;
+                    bb[q] = k == 1 ? bp + dp / dz[q] : (k < nz ? bp + (dp + dm) / dz[q] : bp + dm / dz[q]);
+                    double e = bp0 * uup[I3(m, n, k)] + rhsx[I3(m, n, k)] + rhsx_tran[I3(m, n, k)] + pgrx[i] -
+                               (fz_p - fz_m) / dz[q] +
+                               (g->rlh_s[i] * hhh[i] * g->dxb[i] * g->dyb[i] *
+                                    (vv[I3(m + 1, n, k)] + vv[I3(m, n, k)]) +
+                                g->rlh_s[I(m, n - 1)] * hhh[I(m, n - 1)] * g->dxb[I(m, n - 1)] *
+                                    g->dyb[I(m, n - 1)] * (vv[I3(m + 1, n - 1, k)] + vv[I3(m, n - 1, k)])) /
+                                   4.0 -
+                               (rdis[i] + rdis[I(m + 1, n)]) / 2.0 * uup[I3(m, n, k)] * g->dxt[i] * g->dyh[i] *
+                                   hhu[i];
+                    if (k == 1) e = e + tx_surf[i] / dz[q] * g->dxt[i] * g->dyh[i];
+                    if (k == nz) e = e + tx_bot[i] / dz[q] * g->dxt[i] * g->dyh[i];
+                    eta[q] = e;
+                }
+                factor8(nz, a, bb, c, eta, rksi, x, y);
+                for (int k = 1; k <= nz; k++) un[I3(m, n, k)] = rksi[k - 1];
+            }
+            if (g->lcv[i] > 0.5f) {
+                const double bp = hhvn[i] * g->dxh[i] * g->dyt[i] / tau / 2.0;
+                const double bp0 = hhvp[i] * g->dxh[i] * g->dyt[i] / tau / 2.0;
+                double dp = 0.0, dm = 0.0, fz_p = 0.0, fz_m = 0.0;
+                for (int k = 1; k <= nz; k++) {
+                    dm = dp;
+                    fz_m = fz_p;
+                    if (k < nz) {
+                        dp = (nu[I3(m, n, k + 1)] + nu[I3(m, n + 1, k + 1)]) / 2.0 / hhvn[i] / hzt[k] * g->dxh[i] *
+                             g->dyt[i];
+                        fz_p = (ww[I3(m, n, k + 1)] * g->dx[i] * g->dy[i] +
+                                ww[I3(m, n + 1, k + 1)] * g->dx[I(m, n + 1)] * g->dy[I(m, n + 1)]) /
+                               2.0 * (vv[I3(m, n, k)] + vv[I3(m, n, k + 1)]) / 2.0;
+                    } else {
+                        dp = 0.0;
+                        fz_p = 0.0;
+                    }
+                    const int q = k - 1;
+                    c[q] = k < nz ? -dp / dz[q] : 0.0;
+                    a[q] = k > 1 ? -dm / dz[q] : 0.0;
+                    bb[q] = k == 1 ? bp + dp / dz[q] : (k < nz ? bp + (dp + dm) / dz[q] : bp + dm / dz[q]);
+                    double e = bp0 * vvp[I3(m, n, k)] + rhsy[I3(m, n, k)] + rhsy_tran[I3(m, n, k)] + pgry[i] -
+                               (fz_p - fz_m) / dz[q] -
+                               (g->rlh_s[i] * hhh[i] * g->dxb[i] * g->dyb[i] *
+                                    (uu[I3(m, n + 1, k)] + uu[I3(m, n, k)]) +
+                                g->rlh_s[I(m - 1, n)] * hhh[I(m - 1, n)] * g->dxb[I(m - 1, n)] *
+                                    g->dyb[I(m - 1, n)] * (uu[I3(m - 1, n + 1, k)] + uu[I3(m - 1, n, k)])) /
+                                   4.0 -
+                               (rdis[i] + rdis[I(m, n + 1)]) / 2.0 * vvp[I3(m, n, k)] * g->dxh[i] * g->dyt[i] *
+                                   hhv[i];
+                    if (k == 1) e = e + ty_surf[i] / dz[q] * g->dxh[i] * g->dyt[i];
+                    if (k == nz) e = e + ty_bot[i] / dz[q] * g->dxh[i] * g->dyt[i];
+                    eta[q] = e;
+                }
+                factor8(nz, a, bb, c, eta, rksi, x, y);
+                for (int k = 1; k <= nz; k++) vn[I3(m, n, k)] = rksi[k - 1];
+            }
+        }
+        free(a);
+        free(rksi);
+    }
+    /* :988-998 halo: no exchange on one domain; periodic wrap per level */
+    for (int k = 1; k <= nz; k++) {
+        if (B->periodicity_x) {
+            ora_cyclize8_x(B, un + (size_t)(k - 1) * nt);
+            ora_cyclize8_x(B, vn + (size_t)(k - 1) * nt);
+        }
+        if (B->periodicity_y) {
+            ora_cyclize8_y(B, un + (size_t)(k - 1) * nt);
+            ora_cyclize8_y(B, vn + (size_t)(k - 1) * nt);
+        }
+    }
+    /* :1002-1024 Robert-Asselin filter with time shift */
+    const double ts = g->time_smooth;
+#pragma omp parallel for
+    for (int n = B->ny_start - 1; n <= B->ny_end + 1; n++)
+        for (int m = B->nx_start - 1; m <= B->nx_end + 1; m++) {
+            const size_t i = I(m, n);
+            if (g->lcu[i] > 0.5f)
+                for (int k = 1; k <= nz; k++) {
+                    const size_t j = I3(m, n, k);
+                    uup[j] = uu[j] + ts * (un[j] - 2.0 * uu[j] + uup[j]) / 2.0;
+                    uu[j] = un[j];
+                }
+            if (g->lcv[i] > 0.5f)
+                for (int k = 1; k <= nz; k++) {
+                    const size_t j = I3(m, n, k);
+                    vvp[j] = vv[j] + ts * (vn[j] - 2.0 * vv[j] + vvp[j]) / 2.0;
+                    vv[j] = vn[j];
+                }
+        }
+    free(un);
+    free(vn);
+}
+
+/* Function/vel_ssh.f90:1030-1076 vertical_velocity: w from the continuity
+ * equation, integrated from the bottom (w(nz+1) = 0), on lu points */
+void ora_vertical_velocity(const ora_grid *g, int nz, const double *dz, const double *u, const double *v,
+                           double *w, const double *hu, const double *hv, const double *wflux)
+{
+    SETUP(&g->b);
+    const size_t nt = NTOT(B);
+    const double ffs = (double)g->full_free_surface;
+#pragma omp parallel for
+    for (int n = B->ny_start; n <= B->ny_end; n++)
+        for (int m = B->nx_start; m <= B->nx_end; m++) {
+            const size_t i = I(m, n);
+            if (!(g->lu[i] > 0.5f)) continue;
+            w[I3(m, n, nz + 1)] = 0.0;
+            for (int k = nz; k >= 1; k--)
+                w[I3(m, n, k)] = w[I3(m, n, k + 1)] + dz[k - 1] / (g->dx[i] * g->dy[i]) *
+                                                          (u[I3(m, n, k)] * hu[i] * g->dyh[i] -
+                                                           u[I3(m - 1, n, k)] * hu[I(m - 1, n)] * g->dyh[I(m - 1, n)] +
+                                                           v[I3(m, n, k)] * hv[i] * g->dxh[i] -
+                                                           v[I3(m, n - 1, k)] * hv[I(m, n - 1)] * g->dxh[I(m, n - 1)] +
+                                                           wflux[i] / g->ref_den * ffs);
+        }
+    for (int k = 1; k <= nz + 1; k++) {
+        if (B->periodicity_x) ora_cyclize8_x(B, w + (size_t)(k - 1) * nt);
+        if (B->periodicity_y) ora_cyclize8_y(B, w + (size_t)(k - 1) * nt);
+    }
+#undef I3
+}
+
 /* Control/dyncall.f90:186-201: the corrected 2-D velocity from the time
  * means and the sea-level-pressure part of the time-mean pressure gradient,
  * over nx_start-1..nx_end+1 x ny_start-1..ny_end+1 */

@@ -144,6 +144,19 @@ void ora_r_diss(const ora_grid *g, double r_fric, double *r_diss);
 void ora_surface_stress(const ora_grid *g, const double *taux,
                         const double *tauy, double *ssx, double *ssy);
 
+/* Function/vel_ssh.f90:794-1027 baroclinic_dynamics (with factor8,
+ * Service/oc_algorithms.f90:494-524) and :1030-1076 vertical_velocity.
+ * 3-D arrays (bnd_x1:bnd_x2, bnd_y1:bnd_y2, levels); dz[nz], hzt[nz+1]. */
+void ora_baroclinic_dynamics(const ora_grid *g, int nz, const double *dz, const double *hzt, double tau,
+                             double *uu, double *uup, double *vv, double *vvp, const double *ww,
+                             const double *nu, const double *rhsx, const double *rhsy,
+                             const double *rhsx_tran, const double *rhsy_tran, const double *pgrx,
+                             const double *pgry, const double *rdis, const double *tx_surf,
+                             const double *ty_surf, const double *tx_bot, const double *ty_bot,
+                             const double *hhu, const double *hhup, const double *hhun, const double *hhv,
+                             const double *hhvp, const double *hhvn, const double *hhh);
+void ora_vertical_velocity(const ora_grid *g, int nz, const double *dz, const double *u, const double *v,
+                           double *w, const double *hu, const double *hv, const double *wflux);
 /* Control/dyncall.f90:186-201: uu2d = ubrtr_i/hhu, pgrx -= slpr gradient
  * (and v), on the interior and its one-point ring. */
 void ora_velocity2d(const ora_grid *g, double *uu2d, double *vv2d, double *pgrx, double *pgry,

@@ -157,6 +157,33 @@ def velocity2d(basin, uu2d, vv2d, pgrx, pgry, ubrtr_i, vbrtr_i, slpr, hhu, hhv):
     return uu2d, vv2d, pgrx, pgry
 
 
+BAROCLINIC_FIELDS = ("ww", "nu", "rhsx", "rhsy", "rhsx_tran", "rhsy_tran", "pgrx", "pgry", "rdis",
+                     "tx_surf", "ty_surf", "tx_bot", "ty_bot", "hhu", "hhup", "hhun", "hhv", "hhvp", "hhvn",
+                     "hhh")
+
+
+def baroclinic_dynamics(basin, dz, hzt, tau, uu, uup, vv, vvp, **f):
+    """Function/vel_ssh.f90:794-1027 in place on uu, uup, vv, vvp: arrays of
+    shape (bnd_x, bnd_y, nz) in Fortran order, ww and nu with nz + 1 levels,
+    the rest 2-D; f holds the BAROCLINIC_FIELDS by name."""
+    g = grid_struct(basin)
+    dz = np.ascontiguousarray(dz, dtype=np.float64)
+    hzt = np.ascontiguousarray(hzt, dtype=np.float64)
+    load().ora_baroclinic_dynamics(ctypes.byref(g), int(len(dz)), dz.ctypes.data_as(DP), hzt.ctypes.data_as(DP),
+                                   ctypes.c_double(tau), _d(uu), _d(uup), _d(vv), _d(vvp),
+                                   *[_d(f[k]) for k in BAROCLINIC_FIELDS])
+    return uu, uup, vv, vvp
+
+
+def vertical_velocity(basin, dz, u, v, w, hu, hv, wflux):
+    """Function/vel_ssh.f90:1030-1076: w (nz + 1 levels) in place."""
+    g = grid_struct(basin)
+    dz = np.ascontiguousarray(dz, dtype=np.float64)
+    load().ora_vertical_velocity(ctypes.byref(g), int(len(dz)), dz.ctypes.data_as(DP), _d(u), _d(v), _d(w),
+                                 _d(hu), _d(hv), _d(wflux))
+    return w
+
+
 def hh_init_external(basin):
     g = grid_struct(basin)
     d = basin.depths
