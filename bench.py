@@ -577,6 +577,8 @@ def run_study_baroclinic(args):
     ms_e2e = statistics.median(tot)
     alg = units * BARO_BYTES_PER_CELL_LEVEL + cells * BARO_BYTES_PER_COLUMN
     peak, src = measured_hbm()
+    tp = ROOT / "profiles" / "k_columns_traffic.json"
+    traffic = int(json.loads(tp.read_text())["bytes_per_cell_level"] * units) if tp.exists() else None
     h2d = sum(f[k].nbytes for k in f if k != "wflux") + dz.nbytes + hzt.nbytes
     d2h = sum(f[k].nbytes for k in names)
     line = {
@@ -589,7 +591,8 @@ def run_study_baroclinic(args):
         "e2e": {"value": units / (ms_e2e / 1e3), "unit": "cell-level-steps/s", "ms_per_call": ms_e2e,
                 "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
         "roofline": {"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
-                     "frac": alg / (ms / 1e3) / 1e9 / peak, "traffic": None, "peak_source": src,
+                     "frac": alg / (ms / 1e3) / 1e9 / peak, "traffic": traffic, "peak_source": src,
+                     "traffic_source": "ncu dram bytes of a 512x512x20 launch scaled by cell-levels",
                      "algorithmic_bytes_per_call": int(alg),
                      "kernels_timed": "k_columns + k_border (the compute phase of the call)"},
         "gpu_launches": 2 * len(comp),

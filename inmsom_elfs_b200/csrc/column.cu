@@ -150,7 +150,7 @@ __device__ __forceinline__ double new_at(const Dom &D, const float *mask, const 
     return mask[j] > 0.5f ? out[lev + j] : 0.0;
 }
 
-// Function/vel_ssh.f90:1002-1024 outside the interior
+// Function/vel_ssh.f90:1002-1024 outside the interior, one level per grid row
 __global__ void k_border(Dom D, GridDev g, Levels L, BaroclinicArgs a, double ts, int count)
 {
     const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
@@ -174,8 +174,8 @@ __global__ void k_border(Dom D, GridDev g, Levels L, BaroclinicArgs a, double ts
     const long long i = X(m, n);
     const bool ring = m >= D.nx_start - 1 && m <= D.nx_end + 1 && n >= D.ny_start - 1 && n <= D.ny_end + 1;
     const bool fu = ring && g.lcu[i] > 0.5f, fv = ring && g.lcv[i] > 0.5f;
-    for (int k = 0; k < L.nz; k++) {
-        const long long lev = (long long)k * L.plane, o = lev + i;
+    {
+        const long long lev = (long long)blockIdx.y * L.plane, o = lev + i;
         if (fu) {
             const double un = new_at(D, g.lcu, a.uu_out, lev, m, n), cu = a.uu[o];
             a.uup_out[o] = cu + ts * (un - 2.0 * cu + a.uup[o]) / 2.0;
@@ -272,7 +272,7 @@ int baroclinic_dynamics(const Dom &d, const GridDev &g, const Consts &c, const L
     const int nxi = d.nx_end - d.nx_start + 1, nyi = d.ny_end - d.ny_start + 1;
     k_columns<<<dim3((nxi + TB - 1) / TB, nyi, 2), TB, smem, s>>>(d, g, L, a, c.ts);
     const int count = d.nxa() * d.nya() - nxi * nyi;
-    if (count > 0) k_border<<<(count + 127) / 128, 128, 0, s>>>(d, g, L, a, c.ts, count);
+    if (count > 0) k_border<<<dim3((count + 127) / 128, L.nz), 128, 0, s>>>(d, g, L, a, c.ts, count);
     return 0;
 }
 
