@@ -204,6 +204,24 @@ int inmsom_baroclinic_dynamics(inmsom_ctx *ctx, int nz, const double *dz, const 
 int inmsom_vertical_velocity(inmsom_ctx *ctx, int nz, const double *dz, const double *u, const double *v,
                              double *w, const double *hu, const double *hv, const double *wflux);
 
+/* Replaces depth_ave, Function/depth.f90:223-254 (called at
+ * Control/dyncall.f90:101-105 to take the barotropic RHS out of the 3-D
+ * one): at the points where mask > 0.5 (all but the arrays' outermost ring)
+ * utr = sum over k of u(k)*dz(k), then u = u - kbcl*utr.  u has nz levels
+ * (in place), utr and the real(4) mask are 2-D; other points of utr keep
+ * their values. */
+int inmsom_depth_ave(inmsom_ctx *ctx, int nz, const double *dz, double *u, double *utr, const float *mask,
+                     int kbcl);
+
+/* The two loops of Control/dyncall.f90 that move the barotropic velocity
+ * in and out of the 3-D velocity around vertical_velocity and
+ * ssh_internal: sign = -1 is :170-183 (uu = uu - uu2d), sign = +1 is
+ * :215-229 (uu = uu + uu2d); likewise vv with vv2d; at the ocean u (v)
+ * points of the interior and its one-point ring, every one of the nz
+ * levels.  uu, vv in place. */
+int inmsom_shift_barotropic(inmsom_ctx *ctx, int nz, double *uu, double *vv, const double *uu2d,
+                            const double *vv2d, int sign);
+
 /* The barotropic RHS of Control/dyncall.f90:110-130 (the mode-split caller
  * of barotropic_dynamics), at the ocean u (v) points, in the reference's
  * order of operations:

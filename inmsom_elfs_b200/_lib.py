@@ -29,7 +29,7 @@ EXPORTS = (
     "inmsom_closure_features", "inmsom_run_closure", "inmsom_closure_tendency", "inmsom_gpu_last_phases",
     "inmsom_step_begin", "inmsom_step_launch", "inmsom_halo_pack", "inmsom_halo_unpack", "inmsom_step_end",
     "inmsom_gpu_stream", "inmsom_gpu_pitch", "inmsom_rhs2d", "inmsom_velocity2d",
-    "inmsom_baroclinic_dynamics", "inmsom_vertical_velocity",
+    "inmsom_baroclinic_dynamics", "inmsom_vertical_velocity", "inmsom_depth_ave", "inmsom_shift_barotropic",
 )
 
 # include/inmsom_gpu.h: INMSOM_MLP_*
@@ -122,6 +122,8 @@ def load() -> ctypes.CDLL:
     lib.inmsom_velocity2d.argtypes = [VP] + [DP] * 9
     lib.inmsom_baroclinic_dynamics.argtypes = [VP, i, DP, DP, d] + [DP] * 24
     lib.inmsom_vertical_velocity.argtypes = [VP, i] + [DP] * 7
+    lib.inmsom_depth_ave.argtypes = [VP, i, DP, DP, DP, FP, i]
+    lib.inmsom_shift_barotropic.argtypes = [VP, i, DP, DP, DP, DP, i]
     lib.inmsom_step_begin.argtypes = [VP]
     lib.inmsom_step_launch.argtypes = [VP, d, d]
     lib.inmsom_halo_pack.argtypes = [VP, i, VP]

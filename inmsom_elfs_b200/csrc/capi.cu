@@ -1086,7 +1086,7 @@ int col_alloc(inmsom_ctx *c, int nz)
     const size_t planes = (size_t)NC3 * nz + 2 * (size_t)(nz + 1) + NC2;
     CK(cudaMalloc((void **)&c->col, planes * col_plane(c) * sizeof(double)));
     CK(cudaMemsetAsync(c->col, 0, planes * col_plane(c) * sizeof(double), c->stream));
-    CK(cudaMalloc((void **)&c->col_lev, (2 * (size_t)nz + 1) * sizeof(double)));
+    CK(cudaMalloc((void **)&c->col_lev, (2 * (size_t)nz + 2) * sizeof(double)));   // + the staged kernel's flag
     c->col_nz = nz;
     return INMSOM_OK;
 }
@@ -1168,14 +1168,19 @@ int inmsom_baroclinic_dynamics(inmsom_ctx *c, int nz, const double *dz, const do
     a.hhu = col2(c, 7); a.hhup = col2(c, 8); a.hhun = col2(c, 9);
     a.hhv = col2(c, 10); a.hhvp = col2(c, 11); a.hhvn = col2(c, 12); a.hhh = col2(c, 13);
     a.uu_out = col3(c, C3_UUO); a.uup_out = col3(c, C3_UUPO); a.vv_out = col3(c, C3_VVO); a.vvp_out = col3(c, C3_VVPO);
+    a.flag = reinterpret_cast<int *>(c->col_lev + 2 * nz + 1);
+    CK(cudaMemsetAsync(a.flag, 0, sizeof(int), c->stream));
     if (column::baroclinic_dynamics(d, c->gdev(), c->c, col_levels(c), a, c->stream))
         return set_err(INMSOM_ECUDA, "inmsom_baroclinic_dynamics: launch failed: %s",
                        cudaGetErrorString(cudaGetLastError()));
     CK(cudaGetLastError());
     CK(cudaEventRecord(c->ph[2], c->stream));
+    int flag = 0;
+    CK(cudaMemcpyAsync(&flag, a.flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     for (int k = 0; k < 4; k++) CKR(d2h3(c, io[k], col3(c, C3_UUO + k), nz));
     CK(cudaEventRecord(c->ph[3], c->stream));
     CKR(sync_stream(c));
+    if (flag) return set_err(INMSOM_ETIMEOUT, "inmsom_baroclinic_dynamics: a bounded wait of the column kernel gave up");
     c->ph_valid = true;
     return INMSOM_OK;
 }
@@ -1207,6 +1212,44 @@ int inmsom_vertical_velocity(inmsom_ctx *c, int nz, const double *dz, const doub
     CKR(sync_stream(c));
     c->ph_valid = true;
     return INMSOM_OK;
+}
+
+int inmsom_depth_ave(inmsom_ctx *c, int nz, const double *dz, double *u, double *utr, const float *mask, int kbcl)
+{
+    CKR(ensure_grid(c));
+    if (nz < 1) return set_err(INMSOM_EARG, "inmsom_depth_ave: nz = %d < 1", nz);
+    if (!dz || !u || !utr || !mask) return set_err(INMSOM_EARG, "inmsom_depth_ave: NULL argument");
+    CKR(col_alloc(c, nz));
+    float *dmask = (float *)col2(c, 1);     // a float plane fits in a double one
+    CKR(h2d3(c, col3(c, C3_UU), u, nz));
+    CKR(h2d(c, col2(c, 0), (const double *)utr));
+    CKR(h2d(c, dmask, mask));
+    CK(cudaMemcpyAsync(c->col_lev, dz, nz * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    column::depth_ave(c->dom, col_levels(c), col3(c, C3_UU), col2(c, 0), dmask, kbcl, c->stream);
+    CK(cudaGetLastError());
+    CKR(d2h3(c, u, col3(c, C3_UU), nz));
+    CKR(d2h(c, utr, col2(c, 0)));
+    return sync_stream(c);
+}
+
+int inmsom_shift_barotropic(inmsom_ctx *c, int nz, double *uu, double *vv, const double *uu2d, const double *vv2d,
+                            int sign)
+{
+    CKR(ensure_grid(c));
+    if (nz < 1) return set_err(INMSOM_EARG, "inmsom_shift_barotropic: nz = %d < 1", nz);
+    if (sign != 1 && sign != -1) return set_err(INMSOM_EARG, "inmsom_shift_barotropic: sign must be +1 or -1");
+    if (!uu || !vv || !uu2d || !vv2d) return set_err(INMSOM_EARG, "inmsom_shift_barotropic: NULL argument");
+    CKR(col_alloc(c, nz));
+    CKR(h2d3(c, col3(c, C3_UU), uu, nz));
+    CKR(h2d3(c, col3(c, C3_VV), vv, nz));
+    CKR(h2d(c, col2(c, 0), uu2d));
+    CKR(h2d(c, col2(c, 1), vv2d));
+    column::shift_barotropic(c->dom, c->gdev(), col_levels(c), col3(c, C3_UU), col3(c, C3_VV), col2(c, 0),
+                             col2(c, 1), sign, c->stream);
+    CK(cudaGetLastError());
+    CKR(d2h3(c, uu, col3(c, C3_UU), nz));
+    CKR(d2h3(c, vv, col3(c, C3_VV), nz));
+    return sync_stream(c);
 }
 
 int inmsom_hh_init_external(inmsom_ctx *c, const double *ssh_e, const double *sshp_e)

@@ -2,13 +2,17 @@
 // expression keeps the left-to-right order of the Fortran line it cites.
 //
 // baroclinic_dynamics runs as two kernels:
-//  1. k_columns, one thread per interior water column and velocity component
-//     (grid z: 0 = u, 1 = v).  The thread builds the tridiagonal system level
-//     by level, runs factor8's forward elimination as it goes (x, y of the
-//     sweep kept in shared memory), then back-substitutes from the bottom and
-//     applies the Robert-Asselin filter to the new velocity at once, writing
-//     uu/uup (vv/vvp) to the output arrays.  The inputs stay untouched, so the
-//     neighbouring columns' Coriolis and advection reads see the old state.
+//  1. k_columns (k_columns_direct above 96 levels): every interior water
+//     column and velocity component is one thread, which builds the
+//     tridiagonal system level by level, runs factor8's forward elimination
+//     as it goes (x, y of the sweep kept in shared memory), then
+//     back-substitutes from the bottom and applies the Robert-Asselin filter
+//     to the new velocity at once, writing uu/uup (vv/vvp) to the output
+//     arrays.  The inputs stay untouched, so the neighbouring columns'
+//     Coriolis and advection reads see the old state.  k_columns stages
+//     every level's rows in shared memory with bulk asynchronous copies (a
+//     copy warp runs ahead of the compute warps through a ring of mbarrier
+//     slots); k_columns_direct loads them per thread.
 //  2. k_border, over every point of the arrays outside the interior: the
 //     filter on the one-point ring with the new velocity the periodic wrap
 //     brings there (zero without a wrap, as the reference's un = 0), a copy
@@ -20,15 +24,122 @@ namespace column {
 
 namespace {
 
-constexpr int TB = 64;          // threads (water columns) per block of k_columns
+constexpr int TB = 64;          // threads (water columns) per block of k_columns_direct
 constexpr int MAX_NZ = 200;     // 2 * MAX_NZ * TB doubles of shared memory
 constexpr int BX = 32, BY = 8;
 
 #define X(m_, n_) ix(D, (m_), (n_))
 
-// Function/vel_ssh.f90:847-983 (V = false: the u block :852-915, true: the v
-// block :917-979), factor8 (Service/oc_algorithms.f90:494-524), then the
-// filter of :1002-1024 at this point.
+// ---- Function/vel_ssh.f90:847-983: one water column's system --------------
+// V = false: the u block (:852-915), true: the v block (:917-979).
+
+// what the column's equations take from 2-D fields, in the Fortran order of
+// their products
+struct ColConst {
+    double f1, f2;            // u: dxt, dyh; v: dxh, dyt
+    double hn, bp, bp0, hc, pg, tsurf, tbot;
+    double dx0, dy0, dx1, dy1, cor0, cor1, drag;
+};
+
+// the values of level k the equations read (nu, ww, s1 at level k + 1)
+struct LevelIn {
+    double sp, r1, r2, oe, o0, ope, op, nu0, nu1, w0, w1, s1;
+};
+
+// the far end of the velocity point (u: m+1, v: n+1) and the partner of the
+// Coriolis average (u: n-1, v: m-1), as offsets in a pitched level
+template <bool V>
+__device__ __forceinline__ long long far_off(const Dom &D) { return V ? D.pitch : 1; }
+template <bool V>
+__device__ __forceinline__ long long partner_off(const Dom &D) { return V ? -1 : -D.pitch; }
+
+template <bool V>
+__device__ __forceinline__ ColConst col_const(const Dom &D, const GridDev &g, const BaroclinicArgs &a, long long i)
+{
+    const long long e = far_off<V>(D), p = partner_off<V>(D);
+    ColConst c;
+    c.f1 = V ? g.dxh[i] : g.dxt[i];
+    c.f2 = V ? g.dyt[i] : g.dyh[i];
+    c.hn = (V ? a.hhvn : a.hhun)[i];
+    c.bp = c.hn * c.f1 * c.f2 / a.tau / 2.0;
+    c.bp0 = (V ? a.hhvp : a.hhup)[i] * c.f1 * c.f2 / a.tau / 2.0;
+    c.hc = (V ? a.hhv : a.hhu)[i];
+    c.pg = (V ? a.pgry : a.pgrx)[i];
+    c.tsurf = (V ? a.ty_surf : a.tx_surf)[i];
+    c.tbot = (V ? a.ty_bot : a.tx_bot)[i];
+    c.dx0 = g.dx[i];
+    c.dy0 = g.dy[i];
+    c.dx1 = g.dx[i + e];
+    c.dy1 = g.dy[i + e];
+    c.cor0 = g.rlh[i] * a.hhh[i] * g.dxb[i] * g.dyb[i];
+    c.cor1 = g.rlh[i + p] * a.hhh[i + p] * g.dxb[i + p] * g.dyb[i + p];
+    c.drag = (a.rdis[i] + a.rdis[i + e]) / 2.0;
+    return c;
+}
+
+// Level k (1-based) of the column: its row of the tridiagonal system
+// (:862-911 surface, internal and bottom points) and factor8's forward step
+// (Service/oc_algorithms.f90:510-516).  dp, fz_p carry the level above,
+// xm, ym the sweep, s0 the velocity at level k.
+template <bool V>
+__device__ __forceinline__ void level_step(const ColConst &c, const LevelIn &v, int k, int nz, double dzk,
+                                           double hztk1, double &dp, double &fz_p, double &xm, double &ym,
+                                           double &s0)
+{
+    const double dm = dp, fz_m = fz_p;
+    if (k < nz) {
+        dp = (v.nu0 + v.nu1) / 2.0 / c.hn / hztk1 * c.f1 * c.f2;
+        fz_p = (v.w0 * c.dx0 * c.dy0 + v.w1 * c.dx1 * c.dy1) / 2.0 * (s0 + v.s1) / 2.0;
+    } else {
+        dp = 0.0;
+        fz_p = 0.0;
+    }
+    const double cor = (c.cor0 * (v.oe + v.o0) + c.cor1 * (v.ope + v.op)) / 4.0;
+    double eta = c.bp0 * v.sp + v.r1 + v.r2 + c.pg - (fz_p - fz_m) / dzk;
+    eta = V ? eta - cor : eta + cor;
+    eta = eta - c.drag * v.sp * c.f1 * c.f2 * c.hc;
+    if (k == 1) eta = eta + c.tsurf / dzk * c.f1 * c.f2;
+    if (k == nz) eta = eta + c.tbot / dzk * c.f1 * c.f2;
+    const double cc = k < nz ? -dp / dzk : 0.0;
+    const double bb = k == 1 ? c.bp + dp / dzk : (k < nz ? c.bp + (dp + dm) / dzk : c.bp + dm / dzk);
+    if (k == 1) {
+        xm = -cc / bb;
+        ym = eta / bb;
+    } else {
+        const double aa = -dm / dzk;
+        const double scr = 1.0 / (aa * xm + bb);
+        ym = (eta - aa * ym) * scr;
+        xm = -cc * scr;
+    }
+    s0 = v.s1;
+}
+
+// factor8's back substitution (:517-520) from the bottom, with the filter
+// of :1002-1024 at this point: uup = uu + ts*(un - 2 uu + uup)/2, uu = un.
+// xs, ys: the sweep of levels 1..nz at stride `stride`; r starts as y(nz).
+__device__ __forceinline__ void back_filter(const double *xs, const double *ys, int stride, int nz, long long P,
+                                            long long i, double r, double ts, const double *self,
+                                            const double *selfp, double *out, double *outp)
+{
+    long long o = (long long)(nz - 1) * P + i;
+    double cu = self[o], cp = selfp[o];
+    for (int k = nz; k >= 1; k--) {
+        double cu1 = 0.0, cp1 = 0.0;
+        if (k > 1) {                                      // next level up, one iteration ahead
+            cu1 = self[o - P];
+            cp1 = selfp[o - P];
+        }
+        if (k < nz) r = xs[(k - 1) * stride] * r + ys[(k - 1) * stride];
+        outp[o] = cu + ts * (r - 2.0 * cu + cp) / 2.0;
+        out[o] = r;
+        cu = cu1;
+        cp = cp1;
+        o -= P;
+    }
+}
+
+// ---- the direct kernel (any nz up to MAX_NZ): each thread loads its
+// column's values from global memory level by level ----------------------
 template <bool V>
 __device__ __forceinline__ void solve_column(const Dom &D, const GridDev &g, const Levels &L,
                                              const BaroclinicArgs &a, double ts, int m, int n, double *xs,
@@ -37,10 +148,7 @@ __device__ __forceinline__ void solve_column(const Dom &D, const GridDev &g, con
     const long long i = X(m, n);
     const long long P = L.plane;
     const int nz = L.nz;
-    // the far end of the velocity point (u: m+1, v: n+1) and the partner of
-    // the Coriolis average (u: n-1, v: m-1)
-    const long long e = V ? D.pitch : 1;
-    const long long p = V ? -1 : -D.pitch;
+    const long long e = far_off<V>(D), p = partner_off<V>(D);
     const double *self = V ? a.vv : a.uu, *selfp = V ? a.vvp : a.uup, *other = V ? a.uu : a.vv;
     double *out = V ? a.vv_out : a.uu_out, *outp = V ? a.vvp_out : a.uup_out;
     const float mask = V ? g.lcv[i] : g.lcu[i];
@@ -52,72 +160,38 @@ __device__ __forceinline__ void solve_column(const Dom &D, const GridDev &g, con
         }
         return;
     }
-    const double f1 = V ? g.dxh[i] : g.dxt[i];   // u: dxt*dyh, v: dxh*dyt
-    const double f2 = V ? g.dyt[i] : g.dyh[i];
-    const double hn = (V ? a.hhvn : a.hhun)[i];
-    const double bp = hn * f1 * f2 / a.tau / 2.0;
-    const double bp0 = (V ? a.hhvp : a.hhup)[i] * f1 * f2 / a.tau / 2.0;
-    const double hc = (V ? a.hhv : a.hhu)[i];
-    const double pg = (V ? a.pgry : a.pgrx)[i];
-    const double tsurf = (V ? a.ty_surf : a.tx_surf)[i], tbot = (V ? a.ty_bot : a.tx_bot)[i];
+    const ColConst c = col_const<V>(D, g, a, i);
     const double *rhs = V ? a.rhsy : a.rhsx, *rhst = V ? a.rhsy_tran : a.rhsx_tran;
-    const double dx0 = g.dx[i], dy0 = g.dy[i], dx1 = g.dx[i + e], dy1 = g.dy[i + e];
-    const double cor0 = g.rlh[i] * a.hhh[i] * g.dxb[i] * g.dyb[i];
-    const double cor1 = g.rlh[i + p] * a.hhh[i + p] * g.dxb[i + p] * g.dyb[i + p];
-    const double drag = (a.rdis[i] + a.rdis[i + e]) / 2.0;
-
     double dp = 0.0, fz_p = 0.0, xm = 0.0, ym = 0.0;
-    double s0 = self[i];                                  // self at level k
+    double s0 = self[i];
     for (int k = 1; k <= nz; k++) {
         const long long o = (long long)(k - 1) * P + i;
-        const double dm = dp, fz_m = fz_p;
-        const double dzk = L.dz[k - 1];
-        double s1 = 0.0;
+        LevelIn v;
+        v.sp = selfp[o];
+        v.r1 = rhs[o];
+        v.r2 = rhst[o];
+        v.oe = other[o + e];
+        v.o0 = other[o];
+        v.ope = other[o + p + e];
+        v.op = other[o + p];
         if (k < nz) {
             const long long o1 = o + P;
-            dp = (a.nu[o1] + a.nu[o1 + e]) / 2.0 / hn / L.hzt[k] * f1 * f2;
-            s1 = self[o1];
-            fz_p = (a.ww[o1] * dx0 * dy0 + a.ww[o1 + e] * dx1 * dy1) / 2.0 * (s0 + s1) / 2.0;
+            v.nu0 = a.nu[o1];
+            v.nu1 = a.nu[o1 + e];
+            v.w0 = a.ww[o1];
+            v.w1 = a.ww[o1 + e];
+            v.s1 = self[o1];
         } else {
-            dp = 0.0;
-            fz_p = 0.0;
+            v.nu0 = v.nu1 = v.w0 = v.w1 = v.s1 = 0.0;
         }
-        const double sp = selfp[o];
-        const double cor = (cor0 * (other[o + e] + other[o]) + cor1 * (other[o + p + e] + other[o + p])) / 4.0;
-        double eta = bp0 * sp + rhs[o] + rhst[o] + pg - (fz_p - fz_m) / dzk;
-        eta = V ? eta - cor : eta + cor;
-        eta = eta - drag * sp * f1 * f2 * hc;
-        if (k == 1) eta = eta + tsurf / dzk * f1 * f2;
-        if (k == nz) eta = eta + tbot / dzk * f1 * f2;
-        const double cc = k < nz ? -dp / dzk : 0.0;
-        const double bb = k == 1 ? bp + dp / dzk : (k < nz ? bp + (dp + dm) / dzk : bp + dm / dzk);
-        double x, y;
-        if (k == 1) {
-            x = -cc / bb;
-            y = eta / bb;
-        } else {
-            const double aa = -dm / dzk;
-            const double scr = 1.0 / (aa * xm + bb);
-            x = -cc * scr;
-            y = (eta - aa * ym) * scr;
-        }
-        xs[(k - 1) * TB] = x;
-        ys[(k - 1) * TB] = y;
-        xm = x;
-        ym = y;
-        s0 = s1;
+        level_step<V>(c, v, k, nz, L.dz[k - 1], k < nz ? L.hzt[k] : 1.0, dp, fz_p, xm, ym, s0);
+        xs[(k - 1) * TB] = xm;
+        ys[(k - 1) * TB] = ym;
     }
-    double r = ym;                                        // rksi(nz) = y(nz)
-    for (int k = nz; k >= 1; k--) {
-        const long long o = (long long)(k - 1) * P + i;
-        if (k < nz) r = xs[(k - 1) * TB] * r + ys[(k - 1) * TB];
-        const double cu = self[o];
-        outp[o] = cu + ts * (r - 2.0 * cu + selfp[o]) / 2.0;
-        out[o] = r;
-    }
+    back_filter(xs, ys, TB, nz, P, i, ym, ts, self, selfp, out, outp);
 }
 
-__global__ void __launch_bounds__(TB) k_columns(Dom D, GridDev g, Levels L, BaroclinicArgs a, double ts)
+__global__ void __launch_bounds__(TB) k_columns_direct(Dom D, GridDev g, Levels L, BaroclinicArgs a, double ts)
 {
     extern __shared__ double sm[];
     const int m = D.nx_start + blockIdx.x * TB + threadIdx.x;
@@ -126,6 +200,234 @@ __global__ void __launch_bounds__(TB) k_columns(Dom D, GridDev g, Levels L, Baro
     double *xs = sm + threadIdx.x, *ys = sm + (size_t)L.nz * TB + threadIdx.x;
     if (blockIdx.z == 0) solve_column<false>(D, g, L, a, ts, m, n, xs, ys);
     else solve_column<true>(D, g, L, a, ts, m, n, xs, ys);
+}
+
+// ---- the staged kernel (nz up to NZ_STAGED) -------------------------------
+// A CTA owns CW consecutive columns of one row n for both components: warps
+// 0-1 the u columns, warps 2-3 the v columns, warp 4 the copies.  For every
+// level j the copy warp brings the fourteen row segments the level's
+// equations read (CW + 4 columns each, 16-byte aligned) into a ring slot
+// with 1-D bulk asynchronous copies completing on the slot's mbarrier; the
+// compute warps read the slot of level k and of level k + 1, then release
+// slot k.  The sweep's x, y stay in shared memory for the back
+// substitution, which re-reads uu/uup (vv/vvp) from global memory (L2).
+
+constexpr int CW = 64;                   // columns per CTA
+constexpr int NCW = 4;                   // compute warps
+constexpr int NS = 4;                    // ring slots (levels)
+constexpr int NROW = 14;                 // row segments per level
+constexpr int RW = CW + 4;               // doubles per staged segment
+constexpr int SLOT_D = NROW * RW;        // doubles per slot
+constexpr int NZ_STAGED = 96;
+constexpr unsigned WAIT_LIMIT = 1u << 20;
+
+// the row segments of a slot: field (level j), row
+enum { R_UU0, R_UU1, R_VVM, R_VV0, R_UUP, R_VVP, R_RX, R_RY, R_RXT, R_RYT, R_NU0, R_NU1, R_WW0, R_WW1 };
+
+size_t staged_smem(int nz)
+{
+    return ((size_t)NS * SLOT_D + 2 * (size_t)nz * NCW * 32 + 2 * (size_t)nz + 1) * sizeof(double) +
+           2 * NS * sizeof(uint64_t);
+}
+
+__device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
+
+__device__ __forceinline__ bool mbar_try_wait(uint64_t *bar, uint32_t parity)
+{
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_addr(bar)), "r"(parity)
+        : "memory");
+    return ok != 0;
+}
+
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+{
+    for (unsigned t = 0; t < WAIT_LIMIT; t++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar)
+{
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_addr(bar)) : "memory");
+}
+
+__device__ __forceinline__ void mbar_expect(uint64_t *bar, uint32_t bytes)
+{
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_addr(bar)), "r"(bytes)
+                 : "memory");
+}
+
+__device__ __forceinline__ void bulk_copy(void *dst, const void *src, uint32_t bytes, uint64_t *bar)
+{
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_addr(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_addr(bar))
+                 : "memory");
+}
+
+template <bool V>
+__device__ __forceinline__ LevelIn staged_level(const double *st, const double *sn, int cs, bool last)
+{
+    LevelIn v;
+    if (!V) {
+        v.sp = st[R_UUP * RW + cs];
+        v.r1 = st[R_RX * RW + cs];
+        v.r2 = st[R_RXT * RW + cs];
+        v.oe = st[R_VV0 * RW + cs + 1];                   // vv(m+1, n)
+        v.o0 = st[R_VV0 * RW + cs];                       // vv(m, n)
+        v.ope = st[R_VVM * RW + cs + 1];                  // vv(m+1, n-1)
+        v.op = st[R_VVM * RW + cs];                       // vv(m, n-1)
+    } else {
+        v.sp = st[R_VVP * RW + cs];
+        v.r1 = st[R_RY * RW + cs];
+        v.r2 = st[R_RYT * RW + cs];
+        v.oe = st[R_UU1 * RW + cs];                       // uu(m, n+1)
+        v.o0 = st[R_UU0 * RW + cs];                       // uu(m, n)
+        v.ope = st[R_UU1 * RW + cs - 1];                  // uu(m-1, n+1)
+        v.op = st[R_UU0 * RW + cs - 1];                   // uu(m-1, n)
+    }
+    if (!last) {
+        v.nu0 = sn[R_NU0 * RW + cs];
+        v.nu1 = V ? sn[R_NU1 * RW + cs] : sn[R_NU0 * RW + cs + 1];
+        v.w0 = sn[R_WW0 * RW + cs];
+        v.w1 = V ? sn[R_WW1 * RW + cs] : sn[R_WW0 * RW + cs + 1];
+        v.s1 = V ? sn[R_VV0 * RW + cs] : sn[R_UU0 * RW + cs];
+    } else {
+        v.nu0 = v.nu1 = v.w0 = v.w1 = v.s1 = 0.0;
+    }
+    return v;
+}
+
+template <bool V>
+__device__ __forceinline__ bool staged_column(const Dom &D, const GridDev &g, const Levels &L,
+                                              const BaroclinicArgs &a, double ts, int m, int n, int cs,
+                                              const double *ring, const double *sdz, uint64_t *full,
+                                              uint64_t *empty, double *xs, double *ys, int lane)
+{
+    const int nz = L.nz;
+    const long long P = L.plane;
+    const bool act = m <= D.nx_end;
+    const long long i = act ? X(m, n) : 0;
+    const bool ocean = act && (V ? g.lcv[i] : g.lcu[i]) > 0.5f;
+    const double *self = V ? a.vv : a.uu, *selfp = V ? a.vvp : a.uup;
+    double *out = V ? a.vv_out : a.uu_out, *outp = V ? a.vvp_out : a.uup_out;
+    ColConst c{};
+    if (ocean) c = col_const<V>(D, g, a, i);
+    double dp = 0.0, fz_p = 0.0, xm = 0.0, ym = 0.0, s0 = 0.0;
+    bool ok = true;
+    for (int k = 1; k <= nz && ok; k++) {
+        const int sk = (k - 1) % NS, sn = k % NS;
+        ok = mbar_wait(&full[sk], (uint32_t)(((k - 1) / NS) & 1));
+        if (ok && k < nz) ok = mbar_wait(&full[sn], (uint32_t)((k / NS) & 1));
+        ok = __all_sync(0xffffffffu, ok);
+        if (!ok) break;
+        const double *st = ring + (size_t)sk * SLOT_D, *snx = ring + (size_t)sn * SLOT_D;
+        const int rself = V ? R_VV0 : R_UU0, rselfp = V ? R_VVP : R_UUP;
+        if (ocean) {
+            if (k == 1) s0 = st[rself * RW + cs];
+            const LevelIn v = staged_level<V>(st, snx, cs, k == nz);
+            level_step<V>(c, v, k, nz, sdz[k - 1], k < nz ? sdz[nz + k] : 1.0, dp, fz_p, xm, ym, s0);
+            xs[(k - 1) * NCW * 32] = xm;
+            ys[(k - 1) * NCW * 32] = ym;
+        } else if (act) {
+            const long long o = (long long)(k - 1) * P + i;
+            out[o] = st[rself * RW + cs];
+            outp[o] = st[rselfp * RW + cs];
+        }
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[sk]);
+    }
+    if (ok && ocean) back_filter(xs, ys, NCW * 32, nz, P, i, ym, ts, self, selfp, out, outp);
+    return ok;
+}
+
+__global__ void __launch_bounds__((NCW + 1) * 32) k_columns(Dom D, GridDev g, Levels L, BaroclinicArgs a, double ts)
+{
+    extern __shared__ __align__(128) double sm[];
+    const int nz = L.nz;
+    double *ring = sm;
+    double *xs0 = ring + (size_t)NS * SLOT_D;
+    double *ys0 = xs0 + (size_t)nz * NCW * 32;
+    double *sdz = ys0 + (size_t)nz * NCW * 32;            // dz (nz), hzt (nz + 1)
+    uint64_t *full = reinterpret_cast<uint64_t *>(sdz + 2 * nz + 1);
+    uint64_t *empty = full + NS;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = D.nx_start + blockIdx.x * CW, n = D.ny_start + blockIdx.y;
+
+    for (int t = threadIdx.x; t < 2 * nz + 1; t += blockDim.x) sdz[t] = L.dz[t];
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NS; s++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&full[s])), "r"(1) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&empty[s])), "r"(NCW)
+                         : "memory");
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+
+    // the staged segments: device columns c0 .. c0 + cnt - 1, c0 even, from
+    // m0 - 1 (or m0 - 2) to at least the last column + 1
+    const int cm0 = m0 - D.bnd_x1 + D.xoff;
+    const int mlast = min(m0 + CW - 1, D.nx_end);
+    const int c0 = (cm0 - 1) & ~1;
+    const int cnt = ((mlast - D.bnd_x1 + D.xoff + 2 - c0) + 1) & ~1;
+
+    if (warp == NCW) {
+        if (lane != 0) return;
+        const long long P = L.plane;
+        const long long rb = (long long)(n - D.bnd_y1) * D.pitch + c0;   // row n, column c0
+        const long long pt = D.pitch;
+        const uint32_t seg = (uint32_t)cnt * 8u;
+        int armed = 0;
+        bool ok = true;
+        for (int j = 1; j <= nz; j++) {
+            const int s = (j - 1) % NS;
+            if (j > NS && !mbar_wait(&empty[s], (uint32_t)(((j - 1) / NS - 1) & 1))) {
+                ok = false;
+                break;
+            }
+            double *slot = ring + (size_t)s * SLOT_D;
+            const long long lv = (long long)(j - 1) * P + rb;
+            const int nrow = j == 1 ? R_NU0 : NROW;       // nu, ww of level 1 are not read
+            mbar_expect(&full[s], seg * (uint32_t)nrow);
+            bulk_copy(slot + R_UU0 * RW, a.uu + lv, seg, &full[s]);
+            bulk_copy(slot + R_UU1 * RW, a.uu + lv + pt, seg, &full[s]);
+            bulk_copy(slot + R_VVM * RW, a.vv + lv - pt, seg, &full[s]);
+            bulk_copy(slot + R_VV0 * RW, a.vv + lv, seg, &full[s]);
+            bulk_copy(slot + R_UUP * RW, a.uup + lv, seg, &full[s]);
+            bulk_copy(slot + R_VVP * RW, a.vvp + lv, seg, &full[s]);
+            bulk_copy(slot + R_RX * RW, a.rhsx + lv, seg, &full[s]);
+            bulk_copy(slot + R_RY * RW, a.rhsy + lv, seg, &full[s]);
+            bulk_copy(slot + R_RXT * RW, a.rhsx_tran + lv, seg, &full[s]);
+            bulk_copy(slot + R_RYT * RW, a.rhsy_tran + lv, seg, &full[s]);
+            if (j > 1) {
+                bulk_copy(slot + R_NU0 * RW, a.nu + lv, seg, &full[s]);
+                bulk_copy(slot + R_NU1 * RW, a.nu + lv + pt, seg, &full[s]);
+                bulk_copy(slot + R_WW0 * RW, a.ww + lv, seg, &full[s]);
+                bulk_copy(slot + R_WW1 * RW, a.ww + lv + pt, seg, &full[s]);
+            }
+            armed = j;
+        }
+        if (!ok) atomicOr(a.flag, 1);
+        // no copy of this CTA may be in flight when it exits
+        for (int j = max(1, armed - NS + 1); j <= armed; j++)
+            (void)mbar_wait(&full[(j - 1) % NS], (uint32_t)(((j - 1) / NS) & 1));
+        return;
+    }
+    const bool V = warp >= 2;
+    const int col = (warp & 1) * 32 + lane;
+    const int m = m0 + col;
+    const int cs = (m - D.bnd_x1 + D.xoff) - c0;
+    double *xs = xs0 + warp * 32 + lane, *ys = ys0 + warp * 32 + lane;
+    const bool ok = V ? staged_column<true>(D, g, L, a, ts, m, n, cs, ring, sdz, full, empty, xs, ys, lane)
+                      : staged_column<false>(D, g, L, a, ts, m, n, cs, ring, sdz, full, empty, xs, ys, lane);
+    if (!ok && lane == 0) atomicOr(a.flag, 1);
 }
 
 __device__ __forceinline__ int wrap(int i, bool on, int lo, int hi)
@@ -222,6 +524,48 @@ __global__ void k_vertical_velocity(Dom D, GridDev g, Levels L, double rho, int 
     }
 }
 
+// Function/depth.f90:231-250 at one point
+__global__ void k_depth_ave(Dom D, Levels L, double *u, double *utr, const float *mask, int kbcl)
+{
+    const int m = D.bnd_x1 + 1 + blockIdx.x * BX + threadIdx.x;
+    const int n = D.bnd_y1 + 1 + blockIdx.y * BY + threadIdx.y;
+    if (m > D.bnd_x2 - 1 || n > D.bnd_y2 - 1) return;
+    const long long i = X(m, n);
+    if (!(mask[i] > 0.5f)) return;
+    double ff0 = 0.0;
+    for (int k = 0; k < L.nz; k++) ff0 = ff0 + u[(long long)k * L.plane + i] * L.dz[k];
+    utr[i] = ff0;
+    const double kb = (double)kbcl;
+    for (int k = 0; k < L.nz; k++) {
+        const long long o = (long long)k * L.plane + i;
+        u[o] = u[o] - kb * ff0;
+    }
+}
+
+// Control/dyncall.f90:170-183 / :215-229 at one point of the interior and its ring
+__global__ void k_shift_barotropic(Dom D, GridDev g, Levels L, double *uu, double *vv, const double *uu2d,
+                                   const double *vv2d, int sign)
+{
+    const int m = D.nx_start - 1 + blockIdx.x * BX + threadIdx.x;
+    const int n = D.ny_start - 1 + blockIdx.y * BY + threadIdx.y;
+    if (m > D.nx_end + 1 || n > D.ny_end + 1) return;
+    const long long i = X(m, n);
+    if (g.lcu[i] > 0.5f) {
+        const double s = uu2d[i];
+        for (int k = 0; k < L.nz; k++) {
+            const long long o = (long long)k * L.plane + i;
+            uu[o] = sign < 0 ? uu[o] - s : uu[o] + s;
+        }
+    }
+    if (g.lcv[i] > 0.5f) {
+        const double s = vv2d[i];
+        for (int k = 0; k < L.nz; k++) {
+            const long long o = (long long)k * L.plane + i;
+            vv[o] = sign < 0 ? vv[o] - s : vv[o] + s;
+        }
+    }
+}
+
 // Service/oc_algorithms.f90:50-95 and :118-135 on every level (grid y)
 __global__ void k_cyclize_x3(Dom D, long long plane, double *f)
 {
@@ -265,14 +609,42 @@ int baroclinic_dynamics(const Dom &d, const GridDev &g, const Consts &c, const L
                         const BaroclinicArgs &a, cudaStream_t s)
 {
     if (L.nz < 2 || L.nz > MAX_NZ || wrap_inside(d)) return -1;
-    const size_t smem = 2 * (size_t)L.nz * TB * sizeof(double);
-    // per device: set on every call (the context's device is current)
-    if (cudaFuncSetAttribute(k_columns, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-        return -1;
     const int nxi = d.nx_end - d.nx_start + 1, nyi = d.ny_end - d.ny_start + 1;
-    k_columns<<<dim3((nxi + TB - 1) / TB, nyi, 2), TB, smem, s>>>(d, g, L, a, c.ts);
+    // the staged kernel's 16-byte segments need even row pitch and level stride
+    if (L.nz <= NZ_STAGED && d.pitch % 2 == 0 && L.plane % 2 == 0 && a.flag) {
+        const size_t smem = staged_smem(L.nz);
+        // per device: set on every call (the context's device is current)
+        if (cudaFuncSetAttribute(k_columns, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+            return -1;
+        k_columns<<<dim3((nxi + CW - 1) / CW, nyi), (NCW + 1) * 32, smem, s>>>(d, g, L, a, c.ts);
+    } else {
+        const size_t smem = 2 * (size_t)L.nz * TB * sizeof(double);
+        if (cudaFuncSetAttribute(k_columns_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
+            cudaSuccess)
+            return -1;
+        k_columns_direct<<<dim3((nxi + TB - 1) / TB, nyi, 2), TB, smem, s>>>(d, g, L, a, c.ts);
+    }
     const int count = d.nxa() * d.nya() - nxi * nyi;
     if (count > 0) k_border<<<dim3((count + 127) / 128, L.nz), 128, 0, s>>>(d, g, L, a, c.ts, count);
+    return 0;
+}
+
+int depth_ave(const Dom &d, const Levels &L, double *u, double *utr, const float *mask, int kbcl, cudaStream_t s)
+{
+    if (L.nz < 1) return -1;
+    const int w = d.nxa() - 2, h = d.nya() - 2;
+    if (w < 1 || h < 1) return 0;
+    k_depth_ave<<<dim3((w + BX - 1) / BX, (h + BY - 1) / BY), dim3(BX, BY), 0, s>>>(d, L, u, utr, mask, kbcl);
+    return 0;
+}
+
+int shift_barotropic(const Dom &d, const GridDev &g, const Levels &L, double *uu, double *vv, const double *uu2d,
+                     const double *vv2d, int sign, cudaStream_t s)
+{
+    if (L.nz < 1) return -1;
+    const int w = d.nx_end - d.nx_start + 3, h = d.ny_end - d.ny_start + 3;
+    k_shift_barotropic<<<dim3((w + BX - 1) / BX, (h + BY - 1) / BY), dim3(BX, BY), 0, s>>>(d, g, L, uu, vv, uu2d,
+                                                                                            vv2d, sign);
     return 0;
 }
 

@@ -31,9 +31,13 @@ struct BaroclinicArgs {
     const double *hhu, *hhup, *hhun, *hhv, *hhvp, *hhvn, *hhh;
     // nz levels: uu, uup, vv, vvp after the step (every point of the arrays)
     double *uu_out, *uup_out, *vv_out, *vvp_out;
+    // set to nonzero when a bounded wait of the staged kernel gave up (its
+    // outputs are then incomplete); must be zero before the launch
+    int *flag;
 };
 
-// largest nz the solve supports (its sweep coefficients live in shared memory)
+// largest nz the solve supports (its sweep coefficients live in shared
+// memory; up to 96 levels the staged kernel runs, above it the direct one)
 int max_levels();
 // true when a periodic wrap column/row lies inside the interior (the filter
 // would then need the wrapped value at an interior point; not supported)
@@ -48,6 +52,15 @@ int baroclinic_dynamics(const Dom &d, const GridDev &g, const Consts &c, const L
 int vertical_velocity(const Dom &d, const GridDev &g, const Consts &c, const Levels &L, const double *u,
                       const double *v, double *w, const double *hu, const double *hv, const double *wflux,
                       cudaStream_t s);
+
+// Function/depth.f90:223-254: utr = sum_k u(k)*dz(k) at the points of mask
+// (all but the arrays' outermost ring), u = u - kbcl*utr there; L.dz only.
+int depth_ave(const Dom &d, const Levels &L, double *u, double *utr, const float *mask, int kbcl, cudaStream_t s);
+
+// Control/dyncall.f90:170-183 (sign < 0: uu - uu2d) and :215-229 (sign > 0:
+// uu + uu2d) at the ocean u (v) points of the interior and its ring.
+int shift_barotropic(const Dom &d, const GridDev &g, const Levels &L, double *uu, double *vv, const double *uu2d,
+                     const double *vv2d, int sign, cudaStream_t s);
 
 }  // namespace column
 }  // namespace inmsom

@@ -204,6 +204,25 @@ class BarotropicSolver:
                                               dptr(hu), dptr(hv), dptr(wflux)))
         return w
 
+    def depth_ave(self, dz, u, utr, mask, kbcl: int):
+        """Function/depth.f90:223-254 in place on u (nz levels) and utr
+        (inmsom_depth_ave)."""
+        dz = np.ascontiguousarray(dz, dtype=np.float64)
+        if u.shape != (*self.basin.bounds.shape, len(dz)):
+            raise ValueError("u needs nz levels")
+        check(load().inmsom_depth_ave(self._ctx, len(dz), dz.ctypes.data_as(_lib.DP), dptr(u), dptr(utr),
+                                      fptr(mask), int(kbcl)))
+        return u, utr
+
+    def shift_barotropic(self, uu, vv, uu2d, vv2d, sign: int):
+        """Control/dyncall.f90:170-183 (sign -1) / :215-229 (sign +1) in
+        place on uu, vv (inmsom_shift_barotropic)."""
+        nz = uu.shape[2]
+        if uu.shape != vv.shape or uu.shape[:2] != self.basin.bounds.shape:
+            raise ValueError("uu, vv need the array shape and nz levels")
+        check(load().inmsom_shift_barotropic(self._ctx, nz, dptr(uu), dptr(vv), dptr(uu2d), dptr(vv2d), int(sign)))
+        return uu, vv
+
     def r_diss(self, r_fric: float, out=None):
         out = self.basin.bounds.zeros() if out is None else out
         check(load().inmsom_r_diss(self._ctx, float(r_fric), dptr(out)))

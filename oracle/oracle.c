@@ -826,6 +826,48 @@ void ora_baroclinic_dynamics(const ora_grid *g, int nz, const double *dz, const 
     free(vn);
 }
 
+/* Function/depth.f90:223-254 depth_ave: utr = sum_k u(k)*dz(k) over the
+ * points of mask, and u = u - kbcl*utr there; the loop covers the arrays
+ * but their outermost ring */
+void ora_depth_ave(const ora_grid *g, int nz, const double *dz, double *u, double *utr, const float *mask,
+                   int kbcl)
+{
+    SETUP(&g->b);
+    const size_t nt = NTOT(B);
+#pragma omp parallel for
+    for (int n = B->bnd_y1 + 1; n <= B->bnd_y2 - 1; n++)
+        for (int m = B->bnd_x1 + 1; m <= B->bnd_x2 - 1; m++) {
+            const size_t i = I(m, n);
+            if (!(mask[i] > 0.5f)) continue;
+            double ff0 = 0.0;
+            for (int k = 1; k <= nz; k++) ff0 = ff0 + u[I3(m, n, k)] * dz[k - 1];
+            utr[i] = ff0;
+            for (int k = 1; k <= nz; k++) u[I3(m, n, k)] = u[I3(m, n, k)] - (double)kbcl * ff0;
+        }
+}
+
+/* Control/dyncall.f90:170-183 (sign < 0: uu = uu - uu2d, the barotropic
+ * component removed before vertical_velocity) and :215-229 (sign > 0:
+ * uu = uu + uu2d, restored after ssh_internal), at the ocean u (v) points of
+ * the interior and its one-point ring, every level */
+void ora_shift_barotropic(const ora_grid *g, int nz, double *uu, double *vv, const double *uu2d,
+                          const double *vv2d, int sign)
+{
+    SETUP(&g->b);
+    const size_t nt = NTOT(B);
+#pragma omp parallel for
+    for (int n = B->ny_start - 1; n <= B->ny_end + 1; n++)
+        for (int m = B->nx_start - 1; m <= B->nx_end + 1; m++) {
+            const size_t i = I(m, n);
+            if (g->lcu[i] > 0.5f)
+                for (int k = 1; k <= nz; k++)
+                    uu[I3(m, n, k)] = sign < 0 ? uu[I3(m, n, k)] - uu2d[i] : uu[I3(m, n, k)] + uu2d[i];
+            if (g->lcv[i] > 0.5f)
+                for (int k = 1; k <= nz; k++)
+                    vv[I3(m, n, k)] = sign < 0 ? vv[I3(m, n, k)] - vv2d[i] : vv[I3(m, n, k)] + vv2d[i];
+        }
+}
+
 /* Function/vel_ssh.f90:1030-1076 vertical_velocity: w from the continuity
  * equation, integrated from the bottom (w(nz+1) = 0), on lu points */
 void ora_vertical_velocity(const ora_grid *g, int nz, const double *dz, const double *u, const double *v,

@@ -157,6 +157,12 @@ void ora_baroclinic_dynamics(const ora_grid *g, int nz, const double *dz, const 
                              const double *hhvp, const double *hhvn, const double *hhh);
 void ora_vertical_velocity(const ora_grid *g, int nz, const double *dz, const double *u, const double *v,
                            double *w, const double *hu, const double *hv, const double *wflux);
+/* Function/depth.f90:223-254 depth_ave */
+void ora_depth_ave(const ora_grid *g, int nz, const double *dz, double *u, double *utr, const float *mask,
+                   int kbcl);
+/* Control/dyncall.f90:170-183 (sign < 0) and :215-229 (sign > 0) */
+void ora_shift_barotropic(const ora_grid *g, int nz, double *uu, double *vv, const double *uu2d,
+                          const double *vv2d, int sign);
 /* Control/dyncall.f90:186-201: uu2d = ubrtr_i/hhu, pgrx -= slpr gradient
  * (and v), on the interior and its one-point ring. */
 void ora_velocity2d(const ora_grid *g, double *uu2d, double *vv2d, double *pgrx, double *pgry,

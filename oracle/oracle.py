@@ -184,6 +184,21 @@ def vertical_velocity(basin, dz, u, v, w, hu, hv, wflux):
     return w
 
 
+def depth_ave(basin, dz, u, utr, mask, kbcl):
+    """Function/depth.f90:223-254 in place on u (nz levels) and utr."""
+    g = grid_struct(basin)
+    dz = np.ascontiguousarray(dz, dtype=np.float64)
+    load().ora_depth_ave(ctypes.byref(g), int(len(dz)), dz.ctypes.data_as(DP), _d(u), _d(utr), _f(mask), int(kbcl))
+    return u, utr
+
+
+def shift_barotropic(basin, nz, uu, vv, uu2d, vv2d, sign):
+    """Control/dyncall.f90:170-183 (sign -1) / :215-229 (sign +1) in place."""
+    g = grid_struct(basin)
+    load().ora_shift_barotropic(ctypes.byref(g), int(nz), _d(uu), _d(vv), _d(uu2d), _d(vv2d), int(sign))
+    return uu, vv
+
+
 def hh_init_external(basin):
     g = grid_struct(basin)
     d = basin.depths

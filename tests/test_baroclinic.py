@@ -273,9 +273,10 @@ def _gpu_run(gpu, basin, dz, hzt, f, tau=TAU):
 
 
 @pytest.mark.gpu
-@pytest.mark.parametrize("case,nz", [("coastline", NZ), ("coastline", 2), ("coastline", 57),
-                                     ("periodic_xy", NZ), ("channel_x", 7)])
+@pytest.mark.parametrize("case,nz", [("coastline", NZ), ("coastline", 2), ("coastline", 57), ("coastline", 96),
+                                     ("coastline", 97), ("coastline", 150), ("periodic_xy", NZ), ("channel_x", 7)])
 def test_baroclinic_bitexact(gpu, ora, case, nz):
+    """Up to 96 levels the staged kernel runs, above it the direct one."""
     b = {"coastline": lambda: coastline(ora), "periodic_xy": lambda: periodic(ora),
          "channel_x": lambda: periodic(ora, px=1, py=0)}[case]()
     dz, hzt, f = inputs(b, nz=nz, seed=nz)
@@ -324,3 +325,81 @@ def test_repeated_calls_and_level_change(gpu, ora):
             s.baroclinic_dynamics(dz, hzt, TAU, *st, **{k: f[k] for k in s.BAROCLINIC_FIELDS})
             for g_, w_ in zip(st, want):
                 assert np.array_equal(g_, w_)
+
+
+# ---- the 2-D/3-D coupling loops of the mode-split step ----------------------
+
+def np_depth_ave(basin, dz, u, utr, mask, kbcl):
+    B = basin.bounds
+    u, utr = u.copy(order="F"), utr.copy(order="F")
+    inner = (slice(1, -1), slice(1, -1))
+    m = mask[inner] > 0.5
+    ff0 = np.zeros(m.shape)
+    for k in range(len(dz)):
+        ff0 = ff0 + u[inner][..., k] * dz[k]
+    utr[inner] = np.where(m, ff0, utr[inner])
+    sub = u[inner]
+    sub[...] = np.where(m[..., None], sub - float(kbcl) * ff0[..., None], sub)
+    return u, utr
+
+
+@pytest.mark.parametrize("kbcl", [0, 1])
+def test_depth_ave_oracle_matches_numpy(ora, kbcl):
+    b = coastline(ora)
+    dz, _, f = inputs(b)
+    for mname, field in (("llu", "rhsx"), ("llv", "rhsy")):
+        utr0 = basins.column_fields(b, 1, seed=4)["pgrx"]
+        got = ora.depth_ave(b, dz, f[field].copy(order="F"), utr0.copy(order="F"), b.masks[mname], kbcl)
+        want = np_depth_ave(b, dz, f[field], utr0, b.masks[mname], kbcl)
+        for g_, w_ in zip(got, want):
+            assert np.array_equal(g_, w_)
+    # the depth mean of a level-independent field is the field (sum dz = 1)
+    u = np.repeat(f["pgrx"][..., None], NZ, axis=2).copy(order="F")
+    _, utr = ora.depth_ave(b, dz, u, b.bounds.zeros(), b.masks["llu"], 0)
+    m = b.masks["llu"][1:-1, 1:-1] > 0.5
+    assert np.allclose(utr[1:-1, 1:-1][m], f["pgrx"][1:-1, 1:-1][m], rtol=1e-14, atol=0)
+
+
+def test_shift_barotropic_oracle_round_trip(ora):
+    """Removing then restoring uu2d returns uu up to the rounding of x - s + s;
+    the ring's ocean points are shifted, land points are not."""
+    b = periodic(ora)
+    _, _, f = inputs(b)
+    s2 = {k: np.asfortranarray(0.1 * v / np.abs(v).max()) for k, v in basins.column_fields(b, 1, seed=6).items()
+          if k in ("pgrx", "pgry")}            # velocities of the same size as uu
+    uu, vv = f["uu"].copy(order="F"), f["vv"].copy(order="F")
+    ora.shift_barotropic(b, NZ, uu, vv, s2["pgrx"], s2["pgry"], -1)
+    B = b.bounds
+    x0, y0 = B.bnd_x1, B.bnd_y1
+    ring = (slice(B.nx_start - 1 - x0, B.nx_end + 2 - x0), slice(B.ny_start - 1 - y0, B.ny_end + 2 - y0))
+    m = (b.masks["lcu"][ring] > 0.5)[..., None]
+    want = np.where(m, f["uu"][ring] - s2["pgrx"][ring][..., None], f["uu"][ring])
+    assert np.array_equal(uu[ring], want)
+    ora.shift_barotropic(b, NZ, uu, vv, s2["pgrx"], s2["pgry"], 1)
+    assert rel_err(uu, f["uu"]) < 1e-15 * 8 and rel_err(vv, f["vv"]) < 1e-15 * 8
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("kbcl", [0, 1])
+def test_depth_ave_bitexact(gpu, ora, kbcl):
+    b = coastline(ora)
+    dz, _, f = inputs(b)
+    utr0 = basins.column_fields(b, 1, seed=4)["pgrx"]
+    want = ora.depth_ave(b, dz, f["rhsx"].copy(order="F"), utr0.copy(order="F"), b.masks["llu"], kbcl)
+    with gpu.BarotropicSolver(b, resident=False) as s:
+        got = s.depth_ave(dz, f["rhsx"].copy(order="F"), utr0.copy(order="F"), b.masks["llu"], kbcl)
+    for g_, w_ in zip(got, want):
+        assert np.array_equal(g_, w_)
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("sign", [-1, 1])
+def test_shift_barotropic_bitexact(gpu, ora, sign):
+    b = periodic(ora)
+    _, _, f = inputs(b, nz=9)
+    s2 = basins.column_fields(b, 1, seed=6)
+    want = ora.shift_barotropic(b, 9, f["uu"].copy(order="F"), f["vv"].copy(order="F"), s2["pgrx"], s2["pgry"], sign)
+    with gpu.BarotropicSolver(b, resident=False) as s:
+        got = s.shift_barotropic(f["uu"].copy(order="F"), f["vv"].copy(order="F"), s2["pgrx"], s2["pgry"], sign)
+    for g_, w_ in zip(got, want):
+        assert np.array_equal(g_, w_)
