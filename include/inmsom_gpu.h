@@ -33,6 +33,7 @@ extern "C" {
 #define INMSOM_EGUARD      3  /* state non-finite or out of range (guard tripped) */
 #define INMSOM_ETIMEOUT    4  /* a bounded device-side wait gave up               */
 #define INMSOM_EUNSUPPORTED 5 /* option not supported by the requested path       */
+#define INMSOM_EIO         6  /* a file could not be opened, read or written      */
 
 /* context flags (inmsom_gpu_init) */
 #define INMSOM_RESIDENT      0x1u /* state, depths and scratch stay on the device
@@ -348,6 +349,73 @@ int inmsom_gpu_path(inmsom_ctx *ctx, int *path, const char **reason);
  * reference times the whole calls (Control/dyncall.f90:135,165-167 and
  * :348,367-368 start_timer/end_timer). */
 int inmsom_gpu_last_phases(inmsom_ctx *ctx, float *upload_ms, float *compute_ms, float *download_ms);
+
+/* ---- On-disk formats (host code, no GPU work) ------------------------- */
+
+/* The reference's DIOGIN-standard direct-access files
+ * (Service/input_output_data.f90:117-534, Inc/reclen.fi), same arguments
+ * (the Fortran ierr becomes the return value): field(nx, ny, nz) and
+ * lu(nx, ny) are column-major host arrays with 1-based positions; the box
+ * nxb..nxe x nyb..nye of levels nzb..nze is stored as one record per level
+ * (x fastest), record (nfield-1)*(nze-nzb+1) + (k-nzb+1), FP64 for the *8
+ * forms and FP32 otherwise, in the host's byte order.  Writing puts undef
+ * = -1.0e32 at the points with |lu| < 0.5 and, as the reference does, leaves
+ * those points of `field` at 0 afterwards; an existing file is not
+ * truncated.  Reading sets the |lu| < 0.5 points of the box to 0.  Errors:
+ * INMSOM_EARG (box outside the field, no file name), INMSOM_EIO. */
+int inmsom_wdstd8(const char *path, const char *fname, int nfield, double *field, const float *lu, int nx, int ny,
+                  int nz, int nxb, int nxe, int nyb, int nye, int nzb, int nze);
+int inmsom_wdstd(const char *path, const char *fname, int nfield, float *field, const float *lu, int nx, int ny,
+                 int nz, int nxb, int nxe, int nyb, int nye, int nzb, int nze);
+int inmsom_rdstd8(const char *path, const char *fname, int nfield, double *field, const float *lu, int nx, int ny,
+                  int nz, int nxb, int nxe, int nyb, int nye, int nzb, int nze);
+int inmsom_rdstd(const char *path, const char *fname, int nfield, float *field, const float *lu, int nx, int ny,
+                 int nz, int nxb, int nxe, int nyb, int nye, int nzb, int nze);
+
+/* The GrADS descriptor of Service/rw_ctl_file.f90:1-139 ctl_file_write,
+ * same arguments: writes <fname with .ctl> describing <fname with .dat>,
+ * line by line as the reference's formatted WRITE statements (e12.5,
+ * g15.8, i6, i2.2, i4.4 editing). */
+int inmsom_ctl_file_write(const char *fname, float undef, int nx, int ny, int nz, int nt, int xtype, const double *x0,
+                          double hx, int ytype, const double *y0, double hy, int ztype, const double *z0, double hz,
+                          int yr_type, int year0, int month0, int day0, int hour0, int minute0, float ht,
+                          const char *title, const char *varname);
+
+/* The grid and calendar that the checkpoint's descriptors state
+ * (basin_grid's xt, xu, yt, yv, dxst, dyst, xgr_type, ygr_type and the
+ * model time of Control/output.f90:1454-1463): for a LINEAR axis (type 0)
+ * the pointers give the first value only. */
+typedef struct inmsom_ctl_axes {
+    int xgr_type, ygr_type;
+    const double *xt;   /* x of T points from mmm (nx_glob values if LEVELS)      */
+    const double *xu;   /* x of u points from mmm-1 (nx_glob+1 values if LEVELS)  */
+    const double *yt;   /* y of T points from nnn                                  */
+    const double *yv;   /* y of v points from nnn-1                                */
+    double dxst, dyst;
+    int calendar, year, month, day, hour, minute;
+    float tstep;
+} inmsom_ctl_axes;
+
+/* The barotropic part of the reference's checkpoint ocpwrite
+ * (Control/output.f90:1736-1847) from the context's resident state: in
+ * `path`, cpsshe8.dat (ssh_e, sshp_e over mmm..mm x nnn..nn, mask lu),
+ * cpube8.dat (ubrtr_e, ubrtrp_e from mmm-1, mask llu), cpvbe8.dat (vbrtr_e,
+ * vbrtrp_e from nnn-1, mask llv), their FP32 copies cpsshe.dat, cpubi.dat,
+ * cpvbe.dat and the descriptors cpsshe.ctl, cpube.ctl, cpvbe.ctl (file
+ * names as the reference writes them: the u descriptor names cpube.dat).
+ * Needs a resident state (inmsom_load_state or a resident
+ * barotropic_dynamics call). */
+int inmsom_write_checkpoint(inmsom_ctx *ctx, const char *path, const inmsom_ctl_axes *axes);
+
+/* Restart of the barotropic state from such a checkpoint (the reads that
+ * Control/init_pars.f90:384-411 lists for start_type > 0, which the
+ * reference leaves unimplemented): rdstd8 of cpsshe8.dat, cpube8.dat and
+ * cpvbe8.dat (land points 0), the periodic wrap, then the context's
+ * resident state and, with full_free_surface, its external depths
+ * (hh_init) are set from them.  With the host arrays given (else NULL),
+ * the six fields are also returned there. */
+int inmsom_read_checkpoint(inmsom_ctx *ctx, const char *path, double *ubrtr_e, double *ubrtrp_e, double *vbrtr_e,
+                           double *vbrtrp_e, double *ssh_e, double *sshp_e);
 
 /* Ensemble of independent basins (no counterpart in the reference, which
  * advances one basin per run).  The members are contexts on one device,

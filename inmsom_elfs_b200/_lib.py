@@ -30,6 +30,8 @@ EXPORTS = (
     "inmsom_step_begin", "inmsom_step_launch", "inmsom_halo_pack", "inmsom_halo_unpack", "inmsom_step_end",
     "inmsom_gpu_stream", "inmsom_gpu_pitch", "inmsom_rhs2d", "inmsom_velocity2d",
     "inmsom_baroclinic_dynamics", "inmsom_vertical_velocity", "inmsom_depth_ave", "inmsom_shift_barotropic",
+    "inmsom_wdstd8", "inmsom_wdstd", "inmsom_rdstd8", "inmsom_rdstd", "inmsom_ctl_file_write",
+    "inmsom_write_checkpoint", "inmsom_read_checkpoint",
 )
 
 # include/inmsom_gpu.h: INMSOM_MLP_*
@@ -37,6 +39,16 @@ MLP_NPARAM, MLP_NBF16, MLP_PARTIAL = 7816, 7680, 7817
 
 # include/inmsom_gpu.h: INMSOM_DIAG_NOALLOC_MAX_ROWS
 DIAG_NOALLOC_MAX_ROWS = 16384
+
+
+class CCtlAxes(ctypes.Structure):
+    """include/inmsom_gpu.h: inmsom_ctl_axes."""
+    _fields_ = [("xgr_type", ctypes.c_int), ("ygr_type", ctypes.c_int),
+                ("xt", ctypes.POINTER(ctypes.c_double)), ("xu", ctypes.POINTER(ctypes.c_double)),
+                ("yt", ctypes.POINTER(ctypes.c_double)), ("yv", ctypes.POINTER(ctypes.c_double)),
+                ("dxst", ctypes.c_double), ("dyst", ctypes.c_double),
+                ("calendar", ctypes.c_int), ("year", ctypes.c_int), ("month", ctypes.c_int), ("day", ctypes.c_int),
+                ("hour", ctypes.c_int), ("minute", ctypes.c_int), ("tstep", ctypes.c_float)]
 
 
 class InmsomError(RuntimeError):
@@ -124,6 +136,13 @@ def load() -> ctypes.CDLL:
     lib.inmsom_vertical_velocity.argtypes = [VP, i] + [DP] * 7
     lib.inmsom_depth_ave.argtypes = [VP, i, DP, DP, DP, FP, i]
     lib.inmsom_shift_barotropic.argtypes = [VP, i, DP, DP, DP, DP, i]
+    cp = ctypes.c_char_p
+    for nm, ptr in (("inmsom_wdstd8", DP), ("inmsom_wdstd", FP), ("inmsom_rdstd8", DP), ("inmsom_rdstd", FP)):
+        getattr(lib, nm).argtypes = [cp, cp, i, ptr, FP] + [i] * 9
+    lib.inmsom_ctl_file_write.argtypes = [cp, ctypes.c_float, i, i, i, i, i, DP, d, i, DP, d, i, DP, d,
+                                          i, i, i, i, i, i, ctypes.c_float, cp, cp]
+    lib.inmsom_write_checkpoint.argtypes = [VP, cp, ctypes.POINTER(CCtlAxes)]
+    lib.inmsom_read_checkpoint.argtypes = [VP, cp] + [DP] * 6
     lib.inmsom_step_begin.argtypes = [VP]
     lib.inmsom_step_launch.argtypes = [VP, d, d]
     lib.inmsom_halo_pack.argtypes = [VP, i, VP]

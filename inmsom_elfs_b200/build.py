@@ -29,6 +29,7 @@ SOURCES = {
     "noalloc.cu": [],
     "closure.cu": [],
     "column.cu": ["--fmad=false"],
+    "dstd.cu": [],
 }
 HEADERS = ["common.cuh", "general.h", "fused.h", "closure.h", "column.h"]
 

@@ -1,0 +1,70 @@
+"""The reference's on-disk formats through the C ABI.
+
+DIOGIN-standard direct-access files (Service/input_output_data.f90:117-534):
+one record per level of a box of a field, x fastest, FP64 (wdstd8/rdstd8)
+or FP32 (wdstd/rdstd), land points written as undef = -1.0e32 and read as 0.
+GrADS descriptors (Service/rw_ctl_file.f90:1-139 ctl_file_write).  Arrays
+are Fortran-ordered numpy arrays (nx, ny[, nz]); boxes are 1-based inclusive
+(nxb, nxe, nyb, nye, nzb, nze) as in the reference's argument lists.
+"""
+from __future__ import annotations
+
+import ctypes
+
+import numpy as np
+
+from ._lib import DP, FP, check, load
+
+UNDEF = np.float32(-1.0e32)
+
+
+def _dims(field):
+    nx, ny = field.shape[:2]
+    nz = field.shape[2] if field.ndim == 3 else 1
+    return nx, ny, nz
+
+
+def _box(field, box):
+    nx, ny, nz = _dims(field)
+    return tuple(box) if box is not None else (1, nx, 1, ny, 1, nz)
+
+
+def _call(name, ptr, dtype, path, fname, nfield, field, lu, box):
+    if field.dtype != dtype or not field.flags.f_contiguous:
+        raise TypeError(f"{name}: expected a Fortran-ordered {np.dtype(dtype).name} array")
+    lu = np.asfortranarray(lu, dtype=np.float32)
+    nx, ny, nz = _dims(field)
+    if lu.shape != (nx, ny):
+        raise ValueError(f"{name}: lu must have the field's first two dimensions")
+    check(getattr(load(), name)(path.encode(), fname.encode(), int(nfield), field.ctypes.data_as(ptr),
+                                lu.ctypes.data_as(FP), nx, ny, nz, *_box(field, box)))
+    return field
+
+
+def wdstd8(path, fname, nfield, field, lu, box=None):
+    """inmsom_wdstd8; like the reference, leaves the box's land points of
+    `field` at 0."""
+    return _call("inmsom_wdstd8", DP, np.float64, path, fname, nfield, field, lu, box)
+
+
+def wdstd(path, fname, nfield, field, lu, box=None):
+    return _call("inmsom_wdstd", FP, np.float32, path, fname, nfield, field, lu, box)
+
+
+def rdstd8(path, fname, nfield, field, lu, box=None):
+    return _call("inmsom_rdstd8", DP, np.float64, path, fname, nfield, field, lu, box)
+
+
+def rdstd(path, fname, nfield, field, lu, box=None):
+    return _call("inmsom_rdstd", FP, np.float32, path, fname, nfield, field, lu, box)
+
+
+def ctl_file_write(fname, undef, nx, ny, nz, nt, xtype, x0, hx, ytype, y0, hy, ztype, z0, hz, yr_type, year0,
+                   month0, day0, hour0, minute0, ht, title, varname):
+    """inmsom_ctl_file_write: x0, y0, z0 are sequences (one value for a
+    LINEAR axis, nx/ny/nz values for LEVELS)."""
+    arrs = [np.ascontiguousarray(np.atleast_1d(v), dtype=np.float64) for v in (x0, y0, z0)]
+    check(load().inmsom_ctl_file_write(fname.encode(), float(undef), nx, ny, nz, nt, xtype,
+                                       arrs[0].ctypes.data_as(DP), float(hx), ytype, arrs[1].ctypes.data_as(DP),
+                                       float(hy), ztype, arrs[2].ctypes.data_as(DP), float(hz), yr_type, year0,
+                                       month0, day0, hour0, minute0, float(ht), title.encode(), varname.encode()))

@@ -223,6 +223,25 @@ class BarotropicSolver:
         check(load().inmsom_shift_barotropic(self._ctx, nz, dptr(uu), dptr(vv), dptr(uu2d), dptr(vv2d), int(sign)))
         return uu, vv
 
+    def write_checkpoint(self, path: str, xt, xu, yt, yv, dxst: float, dyst: float, xgr_type: int = 0,
+                         ygr_type: int = 0, calendar: int = 1, date=(2000, 1, 1, 0, 0), tstep: float = 86400.0):
+        """The barotropic checkpoint of Control/output.f90:1736-1847 from
+        the resident state into `path` (inmsom_write_checkpoint); xt, xu,
+        yt, yv: the first coordinate (LINEAR axes) or all of them (LEVELS)."""
+        keep = [np.ascontiguousarray(np.atleast_1d(v), dtype=np.float64) for v in (xt, xu, yt, yv)]
+        ax = _lib.CCtlAxes(xgr_type, ygr_type, *[k.ctypes.data_as(_lib.DP) for k in keep], float(dxst), float(dyst),
+                           calendar, *[int(x) for x in date], float(tstep))
+        check(load().inmsom_write_checkpoint(self._ctx, path.encode(), ctypes.byref(ax)))
+
+    def read_checkpoint(self, path: str, into_basin: bool = True) -> None:
+        """Restart the resident state from cp*8.dat files in `path`
+        (inmsom_read_checkpoint); with into_basin, the basin's state arrays
+        receive the fields too."""
+        st = self.basin.state
+        arrs = [st[k] if into_basin else None for k in ("ubrtr_e", "ubrtrp_e", "vbrtr_e", "vbrtrp_e", "ssh_e",
+                                                         "sshp_e")]
+        check(load().inmsom_read_checkpoint(self._ctx, path.encode(), *[dptr(a) for a in arrs]))
+
     def r_diss(self, r_fric: float, out=None):
         out = self.basin.bounds.zeros() if out is None else out
         check(load().inmsom_r_diss(self._ctx, float(r_fric), dptr(out)))

@@ -1,0 +1,194 @@
+"""On-disk formats: the DIOGIN-standard direct-access files and GrADS
+descriptors of the reference (Service/input_output_data.f90:117-534,
+Service/rw_ctl_file.f90:1-183) through the C ABI, against the oracle's
+restatement (oracle/dstd_oracle.py), byte for byte; the barotropic
+checkpoint and restart (Control/output.f90:1736-1847,
+Control/init_pars.f90:384-411) on the GPU.
+"""
+import numpy as np
+import pytest
+
+from inmsom_elfs_b200 import dstd
+from inmsom_elfs_b200._lib import InmsomError
+from oracle import dstd_oracle as od
+
+
+def _case(seed=0, nx=13, ny=9, nz=4):
+    rng = np.random.default_rng(seed)
+    field = np.asfortranarray(rng.standard_normal((nx, ny, nz)))
+    lu = np.asfortranarray((rng.random((nx, ny)) > 0.3).astype(np.float32))
+    lu[0, 0] = -1.0                       # |lu| >= 0.5 is ocean
+    return field, lu
+
+
+def _expected_file(fields, lu, box, dtype):
+    size = 0
+    chunks = []
+    for nfield, f in fields:
+        for kr, rec in enumerate(od.records(f, lu, box, dtype), start=1):
+            off = od.record_offset(nfield, box, kr, np.dtype(dtype).itemsize)
+            chunks.append((off, rec))
+            size = max(size, off + len(rec))
+    buf = bytearray(size)
+    for off, rec in chunks:
+        buf[off:off + len(rec)] = rec
+    return bytes(buf)
+
+
+@pytest.mark.parametrize("kind", ["8", "4"])
+def test_write_records_match_oracle(tmp_path, kind):
+    dtype = np.float64 if kind == "8" else np.float32
+    write = dstd.wdstd8 if kind == "8" else dstd.wdstd
+    f1, lu = _case(1)
+    f2, _ = _case(2)
+    f1, f2 = f1.astype(dtype, order="F"), f2.astype(dtype, order="F")
+    box = (2, 12, 3, 8, 2, 4)
+    want = _expected_file([(1, f1), (2, f2)], lu, box, dtype)
+    g1, g2 = f1.copy(order="F"), f2.copy(order="F")
+    write(str(tmp_path), "cpx.dat", 1, g1, lu, box)
+    write(str(tmp_path), "cpx.dat", 2, g2, lu, box)
+    assert (tmp_path / "cpx.dat").read_bytes() == want
+    # the reference leaves the written land points of the field at zero
+    land = np.zeros(f1.shape, bool)
+    land[1:12, 2:8, 1:4] = (np.abs(lu[1:12, 2:8]) < 0.5)[..., None]
+    assert np.all(g1[land] == 0) and np.array_equal(g1[~land], f1[~land])
+
+
+def test_undef_value_and_record_length(tmp_path):
+    f, lu = _case(3, nx=6, ny=5, nz=1)
+    lu[:] = 0.0
+    dstd.wdstd8(str(tmp_path), "u8.dat", 1, f.copy(order="F"), lu)
+    data = np.frombuffer((tmp_path / "u8.dat").read_bytes(), dtype=np.float64)
+    assert data.size == 30 and np.all(data == np.float64(np.float32(-1.0e32)))
+    dstd.wdstd(str(tmp_path), "u4.dat", 1, f.astype(np.float32, order="F"), lu)
+    data = np.frombuffer((tmp_path / "u4.dat").read_bytes(), dtype=np.float32)
+    assert data.size == 30 and np.all(data == np.float32(-1.0e32))
+
+
+@pytest.mark.parametrize("kind", ["8", "4"])
+def test_read_matches_oracle(tmp_path, kind):
+    dtype = np.float64 if kind == "8" else np.float32
+    write, read = (dstd.wdstd8, dstd.rdstd8) if kind == "8" else (dstd.wdstd, dstd.rdstd)
+    f, lu = _case(4)
+    f = f.astype(dtype, order="F")
+    box = (1, 13, 2, 9, 1, 3)
+    write(str(tmp_path), "r.dat", 2, f.copy(order="F"), lu, box)
+    got = np.full(f.shape, np.nan, dtype=dtype, order="F")
+    read(str(tmp_path), "r.dat", 2, got, lu, box)
+    want = od.read_field((tmp_path / "r.dat").read_bytes(), 2, box, dtype, lu,
+                         np.full(f.shape, np.nan, dtype=dtype, order="F"))
+    assert np.array_equal(got, want, equal_nan=True)
+    inbox = np.zeros(f.shape, bool)
+    inbox[:, 1:9, 0:3] = True
+    ocean = (np.abs(lu) >= 0.5)[..., None] & inbox
+    assert np.array_equal(got[ocean], f[ocean])
+    assert np.all(got[inbox & ~ocean] == 0) and np.all(np.isnan(got[~inbox]))
+
+
+def test_existing_file_is_not_truncated(tmp_path):
+    p = tmp_path / "keep.dat"
+    p.write_bytes(b"\xab" * 4096)
+    f, lu = _case(5, nx=4, ny=3, nz=1)
+    dstd.wdstd8(str(tmp_path), "keep.dat", 1, f.copy(order="F"), lu)
+    data = p.read_bytes()
+    assert len(data) == 4096 and data[96:] == b"\xab" * (4096 - 96)
+
+
+def test_path_joining_and_errors(tmp_path):
+    f, lu = _case(6, nx=4, ny=3, nz=1)
+    dstd.wdstd8(f"  {tmp_path}/  ", "  j.dat  ", 1, f.copy(order="F"), lu)     # blanks around, one '/'
+    assert (tmp_path / "j.dat").exists()
+    with pytest.raises(InmsomError) as e:
+        dstd.wdstd8(str(tmp_path), "j.dat", 1, f.copy(order="F"), lu, (0, 4, 1, 3, 1, 1))
+    assert e.value.code == 2
+    with pytest.raises(InmsomError) as e:
+        dstd.rdstd8(str(tmp_path), "missing.dat", 1, f.copy(order="F"), lu)
+    assert e.value.code == 6
+
+
+CTL_CASES = [
+    dict(nx=256, ny=256, nz=1, nt=2, xtype=0, x0=[27.5], hx=0.5, ytype=0, y0=[40.9], hy=0.25, ztype=0, z0=[0.0],
+         hz=1.0, yr_type=1, date=(2000, 1, 1, 0, 0), ht=86400.0, title="External SSH, m", var="ssh"),
+    dict(nx=9, ny=3, nz=20, nt=12, xtype=1, x0=list(np.linspace(-1500.0, 1.0e9, 9)), hx=0.0, ytype=1,
+         y0=[0.001, 0.05, 123456789.0], hy=0.0, ztype=1, z0=list(np.linspace(2.5, 997.5, 20)), hz=1.0,
+         yr_type=0, date=(1957, 12, 31, 23, 59), ht=6 * 3600.0, title="Potential temperature, C", var="tt"),
+    dict(nx=2049, ny=1537, nz=1, nt=1, xtype=0, x0=[-0.5], hx=1000.0, ytype=0, y0=[0.0], hy=1.0e-9, ztype=0,
+         z0=[0.0], hz=1.0, yr_type=1, date=(2024, 6, 15, 12, 30), ht=30.0 * 86400.0, title="External UB, m/s",
+         var="ub"),
+    dict(nx=4, ny=4, nz=1, nt=3, xtype=0, x0=[1.0], hx=1.0, ytype=0, y0=[1.0], hy=1.0, ztype=0, z0=[0.0], hz=1.0,
+         yr_type=1, date=(1, 2, 3, 4, 5), ht=90.0, title="t", var="v"),
+    # a step under a minute: no unit, k left from the file-name search
+    dict(nx=4, ny=4, nz=1, nt=3, xtype=0, x0=[1.0], hx=1.0, ytype=0, y0=[1.0], hy=1.0, ztype=0, z0=[0.0], hz=1.0,
+         yr_type=1, date=(1, 2, 3, 4, 5), ht=30.0, title="t", var="v"),
+]
+
+
+@pytest.mark.parametrize("case", range(len(CTL_CASES)))
+def test_ctl_file_matches_oracle(tmp_path, case):
+    c = CTL_CASES[case]
+    fname = str(tmp_path / "cpsshe.dat")
+    args = (fname, -1.0e32, c["nx"], c["ny"], c["nz"], c["nt"], c["xtype"], c["x0"], c["hx"], c["ytype"], c["y0"],
+            c["hy"], c["ztype"], c["z0"], c["hz"], c["yr_type"], *c["date"][:1], c["date"][1], c["date"][2],
+            c["date"][3], c["date"][4], c["ht"], c["title"], c["var"])
+    dstd.ctl_file_write(*args)
+    name, text = od.ctl_text(*args)
+    assert name == str(tmp_path / "cpsshe.ctl")
+    assert (tmp_path / "cpsshe.ctl").read_text() == text
+
+
+def test_ctl_lines_by_hand(tmp_path):
+    """A few lines worked out from the edit descriptors by hand."""
+    c = CTL_CASES[0]
+    dstd.ctl_file_write(str(tmp_path / "a.dat"), -1.0e32, 256, 256, 1, 2, 0, [27.5], 0.5, 0, [40.9], 0.25, 0, [0.0],
+                        1.0, 1, 2000, 1, 1, 0, 0, 86400.0, c["title"], "ssh")
+    lines = (tmp_path / "a.ctl").read_text().split("\n")
+    assert lines[0] == "DSET    ^a.dat" + " " * 123
+    assert lines[1] == "TITLE    External SSH, m"
+    assert lines[2] == "UNDEF   -0.10000E+33  ! gap value"
+    # a6 i6 a11, g15.8 (F11.6 + 4 blanks), 5x, g15.8 (F11.8 + 4 blanks); the
+    # final 5x writes nothing
+    assert lines[3] == "XDEF  " + "   256" + "  LINEAR   " + "  27.500000" + " " * 9 + " 0.50000000" + " " * 4
+    # g15.8 of zero: F11.7 + 4 blanks
+    assert lines[5] == "ZDEF  " + "     1" + "  LINEAR   " + "  0.0000000" + " " * 9 + "  1.0000000" + " " * 4
+    assert lines[6] == "TDEF       2  LINEAR  00:00Z01JAN2000        1dy"
+    assert lines[7:11] == ["VARS 1  ! Number of variables", "ssh" + " " * 8 + "    1" + "  1 VARIABLES ", "ENDVARS", ""]
+
+
+# ---- the barotropic checkpoint on the GPU -----------------------------------
+
+@pytest.mark.gpu
+def test_checkpoint_restart_continues_bit_for_bit(gpu, tmp_path):
+    from inmsom_elfs_b200 import basins
+    from oracle import oracle as ora
+    b = basins.regional_basin(nx=150, ny=110, seed=12)
+    basins.finalize(b, ora.OracleBackend())
+    fresh = b.copy()
+    ax = dict(xt=[0.5], xu=[0.0], yt=[0.5], yv=[0.0], dxst=1.0, dyst=1.0)
+    with gpu.BarotropicSolver(b, resident=True) as s:
+        s.load_state()
+        s.run_substeps(40, b.dt)
+        s.write_checkpoint(str(tmp_path), **ax)
+        s.sync_to_host(0x1)
+        saved = {k: v.copy(order="F") for k, v in b.state.items()}
+        s.run_substeps(30, b.dt)
+        s.sync_to_host(0x1)
+        cont = {k: v.copy(order="F") for k, v in b.state.items()}
+    B = b.bounds
+    box = (B.mmm - B.bnd_x1 + 1, B.mm - B.bnd_x1 + 1, B.nnn - B.bnd_y1 + 1, B.nn - B.bnd_y1 + 1, 1, 1)
+    for name, k0, k1, mask, dx, dy in (("cpsshe8.dat", "ssh_e", "sshp_e", "lu", 0, 0),
+                                       ("cpube8.dat", "ubrtr_e", "ubrtrp_e", "llu", 1, 0),
+                                       ("cpvbe8.dat", "vbrtr_e", "vbrtrp_e", "llv", 0, 1)):
+        bx = (box[0] - dx, box[1], box[2] - dy, box[3], 1, 1)
+        want = _expected_file([(1, saved[k0]), (2, saved[k1])], b.masks[mask], bx, np.float64)
+        assert (tmp_path / name).read_bytes() == want, name
+    for name in ("cpsshe.dat", "cpubi.dat", "cpvbe.dat", "cpsshe.ctl", "cpube.ctl", "cpvbe.ctl"):
+        assert (tmp_path / name).exists(), name
+    with gpu.BarotropicSolver(fresh, resident=True) as s:
+        s.load_state()
+        s.read_checkpoint(str(tmp_path))
+        for k in saved:
+            assert np.array_equal(fresh.state[k], saved[k]), k
+        s.run_substeps(30, b.dt)
+        s.sync_to_host(0x1)
+    for k in cont:
+        assert np.array_equal(fresh.state[k], cont[k]), k
