@@ -38,6 +38,9 @@ seeded synthetic 3-D fields: device time of its kernels with the inputs in
 HBM, the end-to-end call with pinned host arrays, the roofline of the
 column kernel, a full-size bit-exact check against the CPU oracle and the
 oracle's time on the host cores (a study line).
+--study tracer times inmsom_tracer_tran_diff (one tracer's transport,
+isoneutral/GM diffusion and implicit vertical diffusion) the same way on the
+same basin and levels (a study line).
 --study fp32 runs the FP32-velocity variant against the FP64 run on the
 4096 x 4096 ridge basin (2 km, dt = 3 s) for --steps substeps and prints the
 per-field max/RMS differences (a study line, not a benchmark line).
@@ -83,7 +86,7 @@ def parse():
     p.add_argument("--no-e2e", action="store_true")
     p.add_argument("--fp32-velocity", action="store_true")
     p.add_argument("--study", default=None,
-                   choices=["fp32", "ensemble", "closure", "closure-kernels", "baroclinic"])
+                   choices=["fp32", "ensemble", "closure", "closure-kernels", "baroclinic", "tracer"])
     p.add_argument("--nz", type=int, default=20, help="s-levels of the baroclinic study")
     p.add_argument("--closure-days", type=float, default=40.0, help="fine spin-up before the training states")
     p.add_argument("--closure-every", type=int, default=10, help="coarse substeps per network evaluation")
@@ -612,10 +615,82 @@ def run_study_baroclinic(args):
     print(json.dumps(line), flush=True)
 
 
+TRACER_BYTES_PER_CELL_LEVEL = 14 * 8       # ff ffp uu vv mu src, ww nu and 4 slopes read; ff ffp written
+TRACER_BYTES_PER_COLUMN = 15 * 8 + 2 * 4 + 8 * 8   # 2-D inputs and metrics, ig_top/bot, the 8 flux diagnostics
+
+
+def run_study_tracer(args):
+    """inmsom_tracer_tran_diff on the regional basin with nz s-levels."""
+    import torch
+    from inmsom_elfs_b200 import basins, solver
+    torch.cuda.set_device(0)
+    b = workload(args, 0)
+    basins.finalize(b, solver.GpuBackend(0))
+    nz, tau = args.nz, 60.0
+    dz, hzt = basins.vertical_grid(nz, 0)
+    f = basins.tracer_fields(b, nz, seed=1)
+    host = {k: (_pinned_like(v) if isinstance(v, np.ndarray) and v.dtype == np.float64 else v) for k, v in f.items()}
+    shp4 = (*b.bounds.shape, 4)
+    fx, fy = _pinned_like(np.zeros(shp4, order="F")), _pinned_like(np.zeros(shp4, order="F"))
+    first = None
+    comp, tot = [], []
+    clk = Clocks(0)
+    with solver.BarotropicSolver(b, resident=False) as s, clk:
+        for it in range(args.warmup + max(args.steps, 1)):
+            host["ff"][...] = f["ff"]
+            host["ffp"][...] = f["ffp"]
+            s.tracer_tran_diff(dz, hzt, tau, host["ff"], host["ffp"], fx, fy, host)
+            if first is None:
+                first = [host["ff"].copy(order="F"), host["ffp"].copy(order="F"), fx.copy(order="F"),
+                         fy.copy(order="F")]
+            if it >= args.warmup:
+                up, cm, dn = s.last_phases()
+                comp.append(cm)
+                tot.append(up + cm + dn)
+    cells = b.bounds.nx * b.bounds.ny
+    units = cells * nz
+    ms, ms_e2e = statistics.median(comp), statistics.median(tot)
+    alg = units * TRACER_BYTES_PER_CELL_LEVEL + cells * TRACER_BYTES_PER_COLUMN
+    peak, src = measured_hbm()
+    h2d = sum(v.nbytes for k, v in f.items() if isinstance(v, np.ndarray)) + dz.nbytes + hzt.nbytes
+    d2h = 2 * f["ff"].nbytes + fx.nbytes + fy.nbytes
+    line = {
+        "study": "tracer", "metric": "cell-level-steps/s", "unit": "cell-level-steps/s",
+        "value": units / (ms / 1e3), "ms_per_call": ms, "calls": len(comp), "warmup": args.warmup,
+        "dtype": "f64", "data": "synthetic (seeded 3-D fields on the regional basin)",
+        "config": {"workload": f"tracer_tran_diff on regional_basin {b.bounds.nx}x{b.bounds.ny}, nz={nz}",
+                   "nz": nz, "tau_s": tau, "cells": cells,
+                   "l2": "inputs larger than L2 (%.1f GB on the device)" % (h2d / 1e9)},
+        "e2e": {"value": units / (ms_e2e / 1e3), "unit": "cell-level-steps/s", "ms_per_call": ms_e2e,
+                "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+        "roofline": {"bound": "hbm", "achieved": alg / (ms / 1e3) / 1e9, "peak": peak, "unit": "GB/s",
+                     "frac": alg / (ms / 1e3) / 1e9 / peak, "traffic": None, "peak_source": src,
+                     "algorithmic_bytes_per_call": int(alg),
+                     "kernels_timed": "k_tracer_flux, wraps, k_tracer_solve, k_tracer_border (the compute phase)"},
+        "gpu_launches": 3 * len(comp),
+        "clocks": clk.summary(),
+    }
+    if not args.no_cpu:
+        from oracle import oracle as ora
+        threads = os.cpu_count() or 1
+        ora.set_threads(threads)
+        ff, ffp = f["ff"].copy(order="F"), f["ffp"].copy(order="F")
+        ox, oy = np.zeros(shp4, order="F"), np.zeros(shp4, order="F")
+        t0 = time.perf_counter()
+        ora.tracer_tran_diff(b, dz, hzt, tau, ff, ffp, ox, oy, f)
+        el = time.perf_counter() - t0
+        line["parity_full_size"] = all(np.array_equal(x, y) for x, y in zip(first, (ff, ffp, ox, oy)))
+        line["cpu_baseline"] = {"value": units / el, "unit": "cell-level-steps/s", "cores": threads, "kind": "port",
+                                "sample": f"one tracer_tran_diff call of the same workload ({el:.2f} s)"}
+    print(json.dumps(line), flush=True)
+
+
 if __name__ == "__main__":
     a = parse()
     if a.study == "baroclinic":
         run_study_baroclinic(a)
+    elif a.study == "tracer":
+        run_study_tracer(a)
     elif a.study == "closure-kernels":
         run_study_closure_kernels(a)
     elif a.study == "closure":

@@ -205,6 +205,34 @@ int inmsom_baroclinic_dynamics(inmsom_ctx *ctx, int nz, const double *dz, const 
 int inmsom_vertical_velocity(inmsom_ctx *ctx, int nz, const double *dz, const double *u, const double *v,
                              double *w, const double *hu, const double *hv, const double *wflux);
 
+/* Replaces tracer_tran_diff, Function/tem_sal.f90:1-422 (called for
+ * temperature and salinity at Control/dyncall.f90:262-332): one tracer's
+ * leap-frog step with lateral advection, isoneutral diffusion and
+ * Gent-McWilliams fluxes, implicit vertical diffusion per water column
+ * (factor8) with the surface/bottom conditions of types 1 and 2, the
+ * periodic wrap and the Robert-Asselin filter.  Same arguments as the
+ * reference routine, plus what it reads from its modules: nz, dz (nz), hzt
+ * (nz + 1) and the internal-mode depths hhu, hhv, hhqn, hhqp (hhq_rest is
+ * the registered rest depth).  3-D host arrays are (bnd_x1:bnd_x2,
+ * bnd_y1:bnd_y2, levels) in Fortran order: ff, ffp, uu, vv, mu, src with nz
+ * levels, ww, nu, slrx, slry, slzx, slzy with nz + 1; flux_f_x, flux_f_y
+ * are (bnd_x1:bnd_x2, bnd_y1:bnd_y2, 4) outputs (total, advective,
+ * diffusive, GM depth-integrated fluxes; zero outside the ocean u/v points
+ * of the interior); ig_top, ig_bot are integer arrays with 1 or 2 at the
+ * ocean points (else INMSOM_EARG).  ff, ffp are updated in place.  The
+ * lateral-boundary arguments (ksw_lbc .. flbc) are accepted and, as in the
+ * reference's body, not read.  2 <= nz <= 200.  inmsom_gpu_last_phases
+ * times it. */
+int inmsom_tracer_tran_diff(inmsom_ctx *ctx, int nz, const double *dz, const double *hzt, double *ff, double *ffp,
+                            double tau, const double *uu, const double *vv, const double *ww, const double *mu,
+                            double factor_mu, const double *nu, double factor_nu, const double *slrx,
+                            const double *slry, const double *slzx, const double *slzy, double az, double ar,
+                            double alpha_gm, const double *ff_top, const double *ff_bot, const int *ig_top,
+                            const int *ig_bot, double *flux_f_x, double *flux_f_y, const double *swbal, int ksw_lbc,
+                            int numlbc, const int *lqpx, const int *lqpy, const char *ind_lbc, const float *flbc,
+                            const double *src, double src_factor, const double *hhu, const double *hhv,
+                            const double *hhqn, const double *hhqp);
+
 /* Replaces depth_ave, Function/depth.f90:223-254 (called at
  * Control/dyncall.f90:101-105 to take the barotropic RHS out of the 3-D
  * one): at the points where mask > 0.5 (all but the arrays' outermost ring)
@@ -342,8 +370,8 @@ int inmsom_load_state(inmsom_ctx *ctx, double *ubrtr_e, double *ubrtrp_e,
  * static string saying why the fused path is not eligible (or "eligible"). */
 int inmsom_gpu_path(inmsom_ctx *ctx, int *path, const char **reason);
 /* Device time of the phases of the last completed
- * inmsom_barotropic_dynamics, inmsom_baroclinic_dynamics or
- * inmsom_vertical_velocity call (CUDA events on the context's stream):
+ * inmsom_barotropic_dynamics, inmsom_baroclinic_dynamics,
+ * inmsom_vertical_velocity or inmsom_tracer_tran_diff call (CUDA events on the context's stream):
  * host->device copies, the computation (for the barotropic call the
  * substeps with the depth and time-mean work), device->host copies.  The
  * reference times the whole calls (Control/dyncall.f90:135,165-167 and

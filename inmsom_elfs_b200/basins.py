@@ -386,3 +386,33 @@ def column_fields(basin: Basin, nz: int, seed: int = 0, depth: float = 50.0, tau
         out[k] = pos(0.8 * depth, 1.2 * depth)
     out["wflux"] = f2(1.0e-5 * basin.consts.ref_den)
     return out
+
+
+def tracer_fields(basin: Basin, nz: int, seed: int = 0, depth: float = 50.0) -> dict:
+    """Seeded synthetic inputs of one tracer's step (Function/tem_sal.f90):
+    a temperature-like tracer ff, ffp (nz levels, about 10 +- 3), the
+    transporting velocities uu, vv (nz) and ww (nz + 1), lateral diffusivity
+    mu (nz) and vertical nu (nz + 1) with their factors, isopycnal and
+    z-level slopes (nz + 1), the isoneutral/GM weights, surface and bottom
+    values with boundary-condition types 1 or 2, the short-wave balance and
+    source, and the internal-mode depths hhu, hhv, hhqn, hhqp."""
+    rng = np.random.default_rng(seed)
+    shp = basin.bounds.shape
+
+    def f3(lev, s, loc=0.0):
+        return np.asfortranarray(loc + s * rng.standard_normal((*shp, lev)))
+
+    def pos(lo, hi, lev=None):
+        return np.asfortranarray(rng.uniform(lo, hi, shp if lev is None else (*shp, lev)))
+
+    out = dict(ff=f3(nz, 3.0, 10.0), ffp=f3(nz, 3.0, 10.0), uu=f3(nz, 0.1), vv=f3(nz, 0.1),
+               ww=f3(nz + 1, 1.0e-3), mu=pos(50.0, 500.0, nz), nu=pos(1.0e-5, 1.0e-3, nz + 1),
+               slrx=f3(nz + 1, 1.0e-3), slry=f3(nz + 1, 1.0e-3), slzx=f3(nz + 1, 1.0e-3), slzy=f3(nz + 1, 1.0e-3),
+               ff_top=f3(1, 2.0, 15.0)[..., 0].copy(order="F"), ff_bot=f3(1, 1.0, 4.0)[..., 0].copy(order="F"),
+               ig_top=np.asfortranarray(rng.integers(1, 3, shp, dtype=np.int32)),
+               ig_bot=np.asfortranarray(rng.integers(1, 3, shp, dtype=np.int32)),
+               swbal=pos(0.0, 1.0), src=f3(nz, 1.0e-6), factor_mu=1.0, factor_nu=1.0, az=0.3, ar=0.7,
+               alpha_gm=1.0, src_factor=1.0)
+    for k in ("hhu", "hhv", "hhqn", "hhqp"):
+        out[k] = pos(0.8 * depth, 1.2 * depth)
+    return out

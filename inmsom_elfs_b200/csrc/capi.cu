@@ -101,6 +101,10 @@ struct inmsom_ctx {
     // levels in one block (col3, colw, col2) and dz, hzt
     double *col = nullptr, *col_lev = nullptr;
     int col_nz = 0;
+    // inmsom_tracer_tran_diff: fields of trc_nz levels in one block and dz, hzt
+    double *trc = nullptr, *trc_lev = nullptr;
+    int trc_nz = 0;
+    std::vector<float> h_lu;          // the registered lu (argument checks)
     unsigned long long *d_nbad = nullptr;
     double *d_rows = nullptr, *d_out = nullptr;
 
@@ -401,6 +405,8 @@ int inmsom_gpu_finalize(inmsom_ctx *c)
     cudaFree(c->v2d[0]);   // one block
     cudaFree(c->col);
     cudaFree(c->col_lev);
+    cudaFree(c->trc);
+    cudaFree(c->trc_lev);
     cudaFree(c->d_nbad);
     cudaFree(c->d_rows);
     cudaFree(c->d_out);
@@ -450,6 +456,7 @@ int inmsom_gpu_register_grid(inmsom_ctx *c, const float *lu, const float *luu, c
         if (!c->mask[k]) CKR(dalloc(c, &c->mask[k], sizeof(float)));
         CKR(h2d(c, c->mask[k], hm[k]));
     }
+    c->h_lu.assign(lu, lu + (size_t)c->dom.nxa() * c->dom.nya());
     CKR(alloc_set(c, c->met, NMET));
     for (int k = 0; k < NMET; k++) CKR(h2d(c, c->met[k], hg[k]));
     CKR(alloc_set(c, c->depth, NDEPTH));
@@ -1081,6 +1088,8 @@ int col_alloc(inmsom_ctx *c, int nz)
     if (c->col && c->col_nz == nz) return INMSOM_OK;
     cudaFree(c->col);
     cudaFree(c->col_lev);
+    cudaFree(c->trc);
+    cudaFree(c->trc_lev);
     c->col = c->col_lev = nullptr;
     c->col_nz = 0;
     const size_t planes = (size_t)NC3 * nz + 2 * (size_t)(nz + 1) + NC2;
@@ -1181,6 +1190,122 @@ int inmsom_baroclinic_dynamics(inmsom_ctx *c, int nz, const double *dz, const do
     CK(cudaEventRecord(c->ph[3], c->stream));
     CKR(sync_stream(c));
     if (flag) return set_err(INMSOM_ETIMEOUT, "inmsom_baroclinic_dynamics: a bounded wait of the column kernel gave up");
+    c->ph_valid = true;
+    return INMSOM_OK;
+}
+
+namespace {
+
+// the tracer block: TN3 fields of nz levels, TN31 of nz + 1, then TN2 2-D planes
+enum { T_FF, T_FFP, T_UU, T_VV, T_MU, T_SRC, T_FFO, T_FFPO, T_FLX, T_FLY, TN3 };
+enum { T_WW, T_NU, T_SLRX, T_SLRY, T_SLZX, T_SLZY, T_FZX, T_FZY, T_COX, T_COY, T_SGX, T_SGY, TN31 };
+enum { T_TOP, T_BOT, T_SWB, T_HU, T_HV, T_HQN, T_HQP, T_IGT, T_IGB, T_FFX, T_FFY = T_FFX + 4, TN2 = T_FFY + 4 };
+
+double *trc3(inmsom_ctx *c, int f) { return c->trc + (size_t)f * c->trc_nz * col_plane(c); }
+double *trc31(inmsom_ctx *c, int f)
+{
+    return c->trc + ((size_t)TN3 * c->trc_nz + (size_t)f * (c->trc_nz + 1)) * col_plane(c);
+}
+double *trc2(inmsom_ctx *c, int f)
+{
+    return c->trc + ((size_t)TN3 * c->trc_nz + (size_t)TN31 * (c->trc_nz + 1) + f) * col_plane(c);
+}
+
+int trc_alloc(inmsom_ctx *c, int nz)
+{
+    if (c->trc && c->trc_nz == nz) return INMSOM_OK;
+    cudaFree(c->trc);
+    cudaFree(c->trc_lev);
+    c->trc = c->trc_lev = nullptr;
+    c->trc_nz = 0;
+    const size_t planes = (size_t)TN3 * nz + (size_t)TN31 * (nz + 1) + TN2;
+    CK(cudaMalloc((void **)&c->trc, planes * col_plane(c) * sizeof(double)));
+    CK(cudaMemsetAsync(c->trc, 0, planes * col_plane(c) * sizeof(double), c->stream));
+    CK(cudaMalloc((void **)&c->trc_lev, (2 * (size_t)nz + 1) * sizeof(double)));
+    c->trc_nz = nz;
+    return INMSOM_OK;
+}
+
+}  // namespace
+
+int inmsom_tracer_tran_diff(inmsom_ctx *c, int nz, const double *dz, const double *hzt, double *ff, double *ffp,
+                            double tau, const double *uu, const double *vv, const double *ww, const double *mu,
+                            double factor_mu, const double *nu, double factor_nu, const double *slrx,
+                            const double *slry, const double *slzx, const double *slzy, double az, double ar,
+                            double alpha_gm, const double *ff_top, const double *ff_bot, const int *ig_top,
+                            const int *ig_bot, double *flux_f_x, double *flux_f_y, const double *swbal, int ksw_lbc,
+                            int numlbc, const int *lqpx, const int *lqpy, const char *ind_lbc, const float *flbc,
+                            const double *src, double src_factor, const double *hhu, const double *hhv,
+                            const double *hhqn, const double *hhqp)
+{
+    (void)ksw_lbc; (void)numlbc; (void)lqpx; (void)lqpy; (void)ind_lbc; (void)flbc;   // unread by the reference too
+    CKR(ensure_grid(c));
+    if (nz < 2 || nz > column::max_levels())
+        return set_err(INMSOM_EARG, "inmsom_tracer_tran_diff: nz = %d outside 2..%d", nz, column::max_levels());
+    if (!(tau > 0.0)) return set_err(INMSOM_EARG, "tau must be > 0");
+    const double *in3[6] = {ff, ffp, uu, vv, mu, src};
+    const double *in31[6] = {ww, nu, slrx, slry, slzx, slzy};
+    const double *in2[7] = {ff_top, ff_bot, swbal, hhu, hhv, hhqn, hhqp};
+    bool null = !dz || !hzt || !ig_top || !ig_bot || !flux_f_x || !flux_f_y;
+    for (auto *p : in3) null = null || !p;
+    for (auto *p : in31) null = null || !p;
+    for (auto *p : in2) null = null || !p;
+    if (null) return set_err(INMSOM_EARG, "inmsom_tracer_tran_diff: NULL argument");
+    const Dom &d = c->dom;
+    if (column::wrap_inside(d))
+        return set_err(INMSOM_EUNSUPPORTED, "inmsom_tracer_tran_diff: a periodic wrap column/row lies in the interior");
+    // the reference sets b(1), eta(1) (b(nz), eta(nz)) only for types 1 and 2
+    const int nxa = d.nxa();
+    for (int n = d.ny_start; n <= d.ny_end; n++)
+        for (int m = d.nx_start; m <= d.nx_end; m++) {
+            const size_t i = (size_t)(n - d.bnd_y1) * nxa + (size_t)(m - d.bnd_x1);
+            if (c->h_lu[i] > 0.5f && ((ig_top[i] != 1 && ig_top[i] != 2) || (ig_bot[i] != 1 && ig_bot[i] != 2)))
+                return set_err(INMSOM_EARG, "inmsom_tracer_tran_diff: ig_top/ig_bot must be 1 or 2 at ocean point (%d,%d)",
+                               m, n);
+        }
+    CKR(trc_alloc(c, nz));
+    c->ph_valid = false;
+    CK(cudaEventRecord(c->ph[0], c->stream));
+    const int f3[6] = {T_FF, T_FFP, T_UU, T_VV, T_MU, T_SRC};
+    const int f31[6] = {T_WW, T_NU, T_SLRX, T_SLRY, T_SLZX, T_SLZY};
+    for (int k = 0; k < 6; k++) CKR(h2d3(c, trc3(c, f3[k]), in3[k], nz));
+    for (int k = 0; k < 6; k++) CKR(h2d3(c, trc31(c, f31[k]), in31[k], nz + 1));
+    for (int k = 0; k < 7; k++) CKR(h2d(c, trc2(c, T_TOP + k), in2[k]));
+    CKR(h2d(c, reinterpret_cast<int *>(trc2(c, T_IGT)), ig_top));
+    CKR(h2d(c, reinterpret_cast<int *>(trc2(c, T_IGB)), ig_bot));
+    CK(cudaMemcpyAsync(c->trc_lev, dz, nz * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaMemcpyAsync(c->trc_lev + nz, hzt, (nz + 1) * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    CK(cudaEventRecord(c->ph[1], c->stream));
+    column::TracerArgs a;
+    a.tau = tau; a.factor_mu = factor_mu; a.factor_nu = factor_nu; a.az = az; a.ar = ar; a.alpha_gm = alpha_gm;
+    a.src_factor = src_factor;
+    a.ff = trc3(c, T_FF); a.ffp = trc3(c, T_FFP); a.uu = trc3(c, T_UU); a.vv = trc3(c, T_VV);
+    a.mu = trc3(c, T_MU); a.src = trc3(c, T_SRC);
+    a.ww = trc31(c, T_WW); a.nu = trc31(c, T_NU); a.slrx = trc31(c, T_SLRX); a.slry = trc31(c, T_SLRY);
+    a.slzx = trc31(c, T_SLZX); a.slzy = trc31(c, T_SLZY);
+    a.ff_top = trc2(c, T_TOP); a.ff_bot = trc2(c, T_BOT); a.swbal = trc2(c, T_SWB); a.hhu = trc2(c, T_HU);
+    a.hhv = trc2(c, T_HV); a.hhqn = trc2(c, T_HQN); a.hhqp = trc2(c, T_HQP);
+    a.ig_top = reinterpret_cast<const int *>(trc2(c, T_IGT)); a.ig_bot = reinterpret_cast<const int *>(trc2(c, T_IGB));
+    a.ff_out = trc3(c, T_FFO); a.ffp_out = trc3(c, T_FFPO);
+    a.flux_f_x = trc2(c, T_FFX); a.flux_f_y = trc2(c, T_FFY);
+    a.flux_x = trc3(c, T_FLX); a.flux_y = trc3(c, T_FLY);
+    a.flux_zx = trc31(c, T_FZX); a.flux_zy = trc31(c, T_FZY); a.coef_zx = trc31(c, T_COX); a.coef_zy = trc31(c, T_COY);
+    a.sfgm_zx = trc31(c, T_SGX); a.sfgm_zy = trc31(c, T_SGY);
+    column::Levels L;
+    L.nz = nz;
+    L.plane = (long long)col_plane(c);
+    L.dz = c->trc_lev;
+    L.hzt = c->trc_lev + nz;
+    if (column::tracer_tran_diff(d, c->gdev(), c->c, L, a, c->stream))
+        return set_err(INMSOM_ECUDA, "inmsom_tracer_tran_diff: launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(c->ph[2], c->stream));
+    CKR(d2h3(c, ff, trc3(c, T_FFO), nz));
+    CKR(d2h3(c, ffp, trc3(c, T_FFPO), nz));
+    CKR(d2h3(c, flux_f_x, trc2(c, T_FFX), 4));
+    CKR(d2h3(c, flux_f_y, trc2(c, T_FFY), 4));
+    CK(cudaEventRecord(c->ph[3], c->stream));
+    CKR(sync_stream(c));
     c->ph_valid = true;
     return INMSOM_OK;
 }

@@ -524,6 +524,227 @@ __global__ void k_vertical_velocity(Dom D, GridDev g, Levels L, double rho, int 
     }
 }
 
+// ---- Function/tem_sal.f90: one tracer's step ---------------------------
+
+// :101-253 at one u (V = false) or v (V = true) point of the interior: the
+// lateral advective, diffusive and GM fluxes of every level, the vertical
+// parts and coefficients of the isoneutral flux (levels 2..nz; levels 1 and
+// nz + 1 are zero), and the depth-integrated diagnostics.
+template <bool V>
+__device__ __forceinline__ void tracer_flux_point(const Dom &D, const GridDev &g, const Levels &L,
+                                                  const TracerArgs &a, int m, int n)
+{
+    const long long i = X(m, n);
+    const long long P = L.plane;
+    const int nz = L.nz;
+    const long long e = V ? D.pitch : 1;                 // the far point: u m+1, v n+1
+    double *flux = V ? a.flux_y : a.flux_x, *fz = V ? a.flux_zy : a.flux_zx;
+    double *coef = V ? a.coef_zy : a.coef_zx, *sfgm = V ? a.sfgm_zy : a.sfgm_zx;
+    double *ffo = V ? a.flux_f_y : a.flux_f_x;
+    const bool wet = (V ? g.lcv[i] : g.lcu[i]) > 0.5f;
+    if (!wet) {
+        for (int k = 0; k < nz; k++) flux[(long long)k * P + i] = 0.0;
+        for (int k = 0; k <= nz; k++) {
+            const long long o = (long long)k * P + i;
+            fz[o] = 0.0;
+            coef[o] = 0.0;
+            sfgm[o] = 0.0;
+        }
+        for (int c = 0; c < 4; c++) ffo[(long long)c * P + i] = 0.0;
+        return;
+    }
+    const double hh = (V ? a.hhv : a.hhu)[i];
+    const double *slr = V ? a.slry : a.slrx, *slz = V ? a.slzy : a.slzx, *vel = V ? a.vv : a.uu;
+    const double dside = V ? g.dxh[i] : g.dyh[i], dnorm = V ? g.dyt[i] : g.dxt[i];
+    double f1d = 0.0, sg = 0.0;                          // flux_1d(k), sfgm(k) of the level in hand
+    double acc1 = 0.0, acc2 = 0.0, acc3 = 0.0, acc4 = 0.0;
+    fz[i] = 0.0;
+    coef[i] = 0.0;
+    sfgm[i] = 0.0;
+    for (int k = 1; k <= nz; k++) {
+        const long long o = (long long)(k - 1) * P + i;  // level k
+        double f1d1 = 0.0, sg1 = 0.0;                     // level k + 1
+        if (k < nz) {
+            const long long o1 = o + P;
+            const double dfdz = (a.ffp[o1] - a.ffp[o] + a.ffp[o1 + e] - a.ffp[o + e]) / 2.0;
+            const double dfdh = (a.ffp[o1 + e] - a.ffp[o1] + a.ffp[o + e] - a.ffp[o]) / 2.0;
+            const double mu1 = (a.mu[o1] + a.mu[o] + a.mu[o1 + e] + a.mu[o + e]) / 4.0 * a.factor_mu * dside / dnorm;
+            const double slope = a.ar * slr[o1] + a.az * slz[o1];
+            f1d1 = mu1 * (hh * dfdh * L.hzt[k] - slope * dfdz);
+            fz[o1] = mu1 * slope * dfdh;
+            coef[o1] = mu1 * (slope * slope) / hh / L.hzt[k];
+            sg1 = mu1 * (slr[o1] - slz[o1]) * a.alpha_gm;
+            sfgm[o1] = sg1;
+        }
+        const double dzk = L.dz[k - 1];
+        double fd;
+        if (k == 1) fd = f1d1 / L.hzt[1];
+        else if (k < nz) fd = (f1d + f1d1) / dzk / 2.0;
+        else fd = f1d / L.hzt[k - 1];
+        const double s2 = a.ff[o] + a.ff[o + e];
+        const double fa = -(vel[o] * hh * dside * s2 / 2.0);
+        const double vg = (sg1 - sg) / dzk;
+        const double fg = -(vg * s2 / 2.0);
+        flux[o] = fa + fd + fg;
+        acc1 = acc1 + dzk * (fa + fd + fg);
+        acc2 = acc2 + dzk * fa;
+        acc3 = acc3 + dzk * fd;
+        acc4 = acc4 + dzk * fg;
+        f1d = f1d1;
+        sg = sg1;
+    }
+    const long long ot = (long long)nz * P + i;            // level nz + 1
+    fz[ot] = 0.0;
+    coef[ot] = 0.0;
+    sfgm[ot] = 0.0;
+    ffo[i] = acc1;
+    ffo[P + i] = acc2;
+    ffo[2 * P + i] = acc3;
+    ffo[3 * P + i] = acc4;
+}
+
+__global__ void __launch_bounds__(TB) k_tracer_flux(Dom D, GridDev g, Levels L, TracerArgs a)
+{
+    const int m = D.nx_start + blockIdx.x * TB + threadIdx.x;
+    const int n = D.ny_start + blockIdx.y;
+    if (m > D.nx_end) return;
+    if (blockIdx.z == 0) tracer_flux_point<false>(D, g, L, a, m, n);
+    else tracer_flux_point<true>(D, g, L, a, m, n);
+}
+
+// :279-403 at one T point of the interior (the vertical diffusion system,
+// factor8), then the filter of :415-429 there
+__global__ void __launch_bounds__(TB) k_tracer_solve(Dom D, GridDev g, Levels L, TracerArgs a, double ts)
+{
+    extern __shared__ double sm[];
+    const int m = D.nx_start + blockIdx.x * TB + threadIdx.x;
+    const int n = D.ny_start + blockIdx.y;
+    if (m > D.nx_end) return;
+    const long long i = X(m, n);
+    const long long P = L.plane;
+    const int nz = L.nz;
+    if (!(g.lu[i] > 0.5f)) {
+        for (int k = 0; k < nz; k++) {
+            const long long o = (long long)k * P + i;
+            a.ff_out[o] = a.ff[o];
+            a.ffp_out[o] = a.ffp[o];
+        }
+        return;
+    }
+    double *xs = sm + threadIdx.x, *ys = sm + (size_t)nz * TB + threadIdx.x;
+    const long long w = X(m - 1, n) - i, s_ = X(m, n - 1) - i, e = 1, nn = D.pitch;
+    const double dx = g.dx[i], dy = g.dy[i];
+    const double hn = a.hhqn[i];
+    const double bp = hn * dx * dy / a.tau / 2.0;
+    const double bp0 = a.hhqp[i] * dx * dy / a.tau / 2.0;
+    const double cu = (double)fmaxf(g.lcu[i] + g.lcu[i + w], 1e-10f);
+    const double cv = (double)fmaxf(g.lcv[i] + g.lcv[i + s_], 1e-10f);
+    const double hq = g.hrest[i], swb = a.swbal[i];
+    const int igt = a.ig_top[i], igb = a.ig_bot[i];
+    double fz_p = 0.0, dp = 0.0, xm = 0.0, ym = 0.0;
+    for (int k = 1; k <= nz; k++) {
+        const int q = k - 1;
+        const long long o = (long long)q * P + i;
+        const double dzk = L.dz[q];
+        const double fz_m = fz_p;
+        if (k < nz) {
+            const long long o1 = o + P;
+            const double vel_gm = -(a.sfgm_zx[o1] - a.sfgm_zx[o1 + w] + a.sfgm_zy[o1] - a.sfgm_zy[o1 + s_]);
+            fz_p = -((a.flux_zx[o1] + a.flux_zx[o1 + w]) / cu) - (a.flux_zy[o1] + a.flux_zy[o1 + s_]) / cv +
+                   (a.coef_zx[o1] * (a.ffp[o1 + e] - a.ffp[o + e]) + a.coef_zx[o1 + w] * (a.ffp[o1 + w] - a.ffp[o + w])) /
+                       cu / 2.0 +
+                   (a.coef_zy[o1] * (a.ffp[o1 + nn] - a.ffp[o + nn]) +
+                    a.coef_zy[o1 + s_] * (a.ffp[o1 + s_] - a.ffp[o + s_])) /
+                       cv / 2.0 -
+                   (a.ww[o1] * dx * dy + vel_gm) * (a.ff[o] + a.ff[o1]) / 2.0;
+        } else {
+            fz_p = 0.0;
+        }
+        const double nu_p = a.nu[o + P] * a.factor_nu;
+        const double dm = k == 1 ? a.nu[o] * a.factor_nu * dx * dy / hn / L.hzt[0] : dp;
+        if (k < nz)
+            dp = (a.coef_zx[o + P] + a.coef_zx[o + P + w]) / cu / 2.0 +
+                 (a.coef_zy[o + P] + a.coef_zy[o + P + s_]) / cv / 2.0 + nu_p * dx * dy / hn / L.hzt[k];
+        else
+            dp = nu_p * dx * dy / hn / L.hzt[k];
+        const double rhs = a.flux_x[o] - a.flux_x[o + w] + a.flux_y[o] - a.flux_y[o + s_] + (fz_p - fz_m) / dzk +
+                           a.src[o] * hq * swb * a.src_factor * dx * dy;
+        const double base = a.ffp[o];
+        double cc, aa = 0.0, bb, eta;
+        if (k == 1) {
+            cc = -dp / dzk;
+            if (igt == 1) {
+                bb = bp + (dp + dm) / dzk;
+                eta = bp0 * base + rhs + dm * a.ff_top[i] / dzk;
+            } else {
+                bb = bp + dp / dzk;
+                eta = bp0 * base + rhs + a.ff_top[i] / dzk * dx * dy;
+            }
+        } else if (k < nz) {
+            cc = -dp / dzk;
+            aa = -dm / dzk;
+            bb = bp + (dp + dm) / dzk;
+            eta = bp0 * base + rhs;
+        } else {
+            cc = 0.0;
+            aa = -dm / dzk;
+            if (igb == 1) {
+                bb = bp + (dp + dm) / dzk;
+                eta = bp0 * base + rhs + dp * a.ff_bot[i] / dzk;
+            } else {
+                bb = bp + dm / dzk;
+                eta = bp0 * base + rhs + a.ff_bot[i] / dzk * dx * dy;
+            }
+        }
+        if (k == 1) {
+            xm = -cc / bb;
+            ym = eta / bb;
+        } else {
+            const double scr = 1.0 / (aa * xm + bb);
+            ym = (eta - aa * ym) * scr;
+            xm = -cc * scr;
+        }
+        xs[q * TB] = xm;
+        ys[q * TB] = ym;
+    }
+    back_filter(xs, ys, TB, nz, P, i, ym, ts, a.ff, a.ffp, a.ff_out, a.ffp_out);
+}
+
+// :415-429 outside the interior (the ring with the wrapped new tracer,
+// copies elsewhere), one level per grid row
+__global__ void k_tracer_border(Dom D, GridDev g, Levels L, TracerArgs a, double ts, int count)
+{
+    const int t0 = blockIdx.x * blockDim.x + threadIdx.x;
+    if (t0 >= count) return;
+    const int nxa = D.bnd_x2 - D.bnd_x1 + 1;
+    const int h0 = D.ny_start - D.bnd_y1, h1 = D.bnd_y2 - D.ny_end;
+    const int w0 = D.nx_start - D.bnd_x1, w1 = D.bnd_x2 - D.nx_end;
+    int m, n, t = t0;
+    if (t < h0 * nxa) {
+        n = D.bnd_y1 + t / nxa;
+        m = D.bnd_x1 + t % nxa;
+    } else if ((t -= h0 * nxa) < h1 * nxa) {
+        n = D.ny_end + 1 + t / nxa;
+        m = D.bnd_x1 + t % nxa;
+    } else {
+        t -= h1 * nxa;
+        n = D.ny_start + t / (w0 + w1);
+        const int c = t % (w0 + w1);
+        m = c < w0 ? D.bnd_x1 + c : D.nx_end + 1 + (c - w0);
+    }
+    const long long i = X(m, n);
+    const bool ring = m >= D.nx_start - 1 && m <= D.nx_end + 1 && n >= D.ny_start - 1 && n <= D.ny_end + 1;
+    const long long lev = (long long)blockIdx.y * L.plane, o = lev + i;
+    if (ring && g.lu[i] > 0.5f) {
+        const double fnew = new_at(D, g.lu, a.ff_out, lev, m, n), cf = a.ff[o];
+        a.ffp_out[o] = cf + ts * (fnew - 2.0 * cf + a.ffp[o]) / 2.0;
+        a.ff_out[o] = fnew;
+    } else {
+        a.ff_out[o] = a.ff[o];
+        a.ffp_out[o] = a.ffp[o];
+    }
+}
+
 // Function/depth.f90:231-250 at one point
 __global__ void k_depth_ave(Dom D, Levels L, double *u, double *utr, const float *mask, int kbcl)
 {
@@ -626,6 +847,32 @@ int baroclinic_dynamics(const Dom &d, const GridDev &g, const Consts &c, const L
     }
     const int count = d.nxa() * d.nya() - nxi * nyi;
     if (count > 0) k_border<<<dim3((count + 127) / 128, L.nz), 128, 0, s>>>(d, g, L, a, c.ts, count);
+    return 0;
+}
+
+int tracer_tran_diff(const Dom &d, const GridDev &g, const Consts &c, const Levels &L, const TracerArgs &a,
+                     cudaStream_t s)
+{
+    if (L.nz < 2 || L.nz > MAX_NZ || wrap_inside(d)) return -1;
+    const int nxi = d.nx_end - d.nx_start + 1, nyi = d.ny_end - d.ny_start + 1;
+    k_tracer_flux<<<dim3((nxi + TB - 1) / TB, nyi, 2), TB, 0, s>>>(d, g, L, a);
+    // the x-fluxes wrap in x, the y-fluxes in y (Function/tem_sal.f90:265-277)
+    if (d.px) {
+        k_cyclize_x3<<<dim3((d.nya() + 127) / 128, L.nz), 128, 0, s>>>(d, L.plane, a.flux_x);
+        for (double *f : {a.flux_zx, a.coef_zx, a.sfgm_zx})
+            k_cyclize_x3<<<dim3((d.nya() + 127) / 128, L.nz + 1), 128, 0, s>>>(d, L.plane, f);
+    }
+    if (d.py) {
+        k_cyclize_y3<<<dim3((d.nxa() + 127) / 128, L.nz), 128, 0, s>>>(d, L.plane, a.flux_y);
+        for (double *f : {a.flux_zy, a.coef_zy, a.sfgm_zy})
+            k_cyclize_y3<<<dim3((d.nxa() + 127) / 128, L.nz + 1), 128, 0, s>>>(d, L.plane, f);
+    }
+    const size_t smem = 2 * (size_t)L.nz * TB * sizeof(double);
+    if (cudaFuncSetAttribute(k_tracer_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return -1;
+    k_tracer_solve<<<dim3((nxi + TB - 1) / TB, nyi), TB, smem, s>>>(d, g, L, a, c.ts);
+    const int count = d.nxa() * d.nya() - nxi * nyi;
+    if (count > 0) k_tracer_border<<<dim3((count + 127) / 128, L.nz), 128, 0, s>>>(d, g, L, a, c.ts, count);
     return 0;
 }
 

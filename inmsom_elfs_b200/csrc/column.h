@@ -53,6 +53,27 @@ int vertical_velocity(const Dom &d, const GridDev &g, const Consts &c, const Lev
                       const double *v, double *w, const double *hu, const double *hv, const double *wflux,
                       cudaStream_t s);
 
+struct TracerArgs {
+    double tau, factor_mu, factor_nu, az, ar, alpha_gm, src_factor;
+    // nz levels (ww, nu and the slopes nz + 1), read only
+    const double *ff, *ffp, *uu, *vv, *ww, *mu, *nu, *slrx, *slry, *slzx, *slzy, *src;
+    // 2-D
+    const double *ff_top, *ff_bot, *swbal, *hhu, *hhv, *hhqn, *hhqp;
+    const int *ig_top, *ig_bot;
+    // outputs: ff, ffp after the step (every point); the flux diagnostics
+    // (4 planes each: total, advection, diffusion, GM)
+    double *ff_out, *ffp_out, *flux_f_x, *flux_f_y;
+    // work: lateral fluxes (nz), their vertical parts, coefficients and GM
+    // stream functions (nz + 1); zero outside the interior
+    double *flux_x, *flux_y, *flux_zx, *flux_zy, *coef_zx, *coef_zy, *sfgm_zx, *sfgm_zy;
+};
+
+// Function/tem_sal.f90:1-422 on one domain (hhq_rest from the grid's rest
+// depth).  Returns 0, or -1 when nz is out of range or a periodic wrap
+// column/row lies inside the interior.
+int tracer_tran_diff(const Dom &d, const GridDev &g, const Consts &c, const Levels &L, const TracerArgs &a,
+                     cudaStream_t s);
+
 // Function/depth.f90:223-254: utr = sum_k u(k)*dz(k) at the points of mask
 // (all but the arrays' outermost ring), u = u - kbcl*utr there; L.dz only.
 int depth_ave(const Dom &d, const Levels &L, double *u, double *utr, const float *mask, int kbcl, cudaStream_t s);

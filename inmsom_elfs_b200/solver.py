@@ -204,6 +204,33 @@ class BarotropicSolver:
                                               dptr(hu), dptr(hv), dptr(wflux)))
         return w
 
+    def tracer_tran_diff(self, dz, hzt, tau: float, ff, ffp, flux_f_x, flux_f_y, f: dict):
+        """Function/tem_sal.f90:1-422 in place on ff, ffp (nz levels) and the
+        diagnostics flux_f_x, flux_f_y (bnd_x, bnd_y, 4)
+        (inmsom_tracer_tran_diff); f holds the other arguments by the
+        reference's names (basins.tracer_fields)."""
+        dz = np.ascontiguousarray(dz, dtype=np.float64)
+        hzt = np.ascontiguousarray(hzt, dtype=np.float64)
+        nz = len(dz)
+        shp = self.basin.bounds.shape
+        for name, a, lev in (("ff", ff, nz), ("ffp", ffp, nz), ("flux_f_x", flux_f_x, 4), ("flux_f_y", flux_f_y, 4),
+                             *[(k, f[k], nz) for k in ("uu", "vv", "mu", "src")],
+                             *[(k, f[k], nz + 1) for k in ("ww", "nu", "slrx", "slry", "slzx", "slzy")]):
+            if a.shape != (*shp, lev):
+                raise ValueError(f"{name}: expected shape {(*shp, lev)}")
+        ip = ctypes.POINTER(ctypes.c_int)
+        igt = np.asfortranarray(f["ig_top"], dtype=np.int32)
+        igb = np.asfortranarray(f["ig_bot"], dtype=np.int32)
+        check(load().inmsom_tracer_tran_diff(
+            self._ctx, nz, dz.ctypes.data_as(_lib.DP), hzt.ctypes.data_as(_lib.DP), dptr(ff), dptr(ffp), float(tau),
+            dptr(f["uu"]), dptr(f["vv"]), dptr(f["ww"]), dptr(f["mu"]), float(f["factor_mu"]), dptr(f["nu"]),
+            float(f["factor_nu"]), dptr(f["slrx"]), dptr(f["slry"]), dptr(f["slzx"]), dptr(f["slzy"]),
+            float(f["az"]), float(f["ar"]), float(f["alpha_gm"]), dptr(f["ff_top"]), dptr(f["ff_bot"]),
+            igt.ctypes.data_as(ip), igb.ctypes.data_as(ip), dptr(flux_f_x), dptr(flux_f_y), dptr(f["swbal"]),
+            0, 0, None, None, None, None, dptr(f["src"]), float(f["src_factor"]), dptr(f["hhu"]), dptr(f["hhv"]),
+            dptr(f["hhqn"]), dptr(f["hhqp"])))
+        return ff, ffp, flux_f_x, flux_f_y
+
     def depth_ave(self, dz, u, utr, mask, kbcl: int):
         """Function/depth.f90:223-254 in place on u (nz levels) and utr
         (inmsom_depth_ave)."""

@@ -868,6 +868,204 @@ void ora_shift_barotropic(const ora_grid *g, int nz, double *uu, double *vv, con
         }
 }
 
+/* Function/tem_sal.f90:1-422 tracer_tran_diff: one tracer's step —
+ * lateral advection, isoneutral diffusion and Gent-McWilliams fluxes on u
+ * and v points (:101-253), the periodic wrap of those fluxes (:255-277),
+ * the implicit vertical diffusion per water column with vertical
+ * advection and the fluxes' vertical parts (:279-403, factor8), and the
+ * Robert-Asselin filter (:415-429).  The lateral-boundary arguments of the
+ * reference (ksw_lbc, numlbc, lqpx, lqpy, ind_lbc, flbc) are not read by
+ * its body and are not taken here.  ig_top/ig_bot must be 1 or 2 at the
+ * ocean points (other values leave the reference's b(1)/eta(1) unset). */
+void ora_tracer_tran_diff(const ora_grid *g, int nz, const double *dz, const double *hzt, double *ff, double *ffp,
+                          double tau, const double *uu, const double *vv, const double *ww, const double *mu,
+                          double factor_mu, const double *nu, double factor_nu, const double *slrx,
+                          const double *slry, const double *slzx, const double *slzy, double az, double ar,
+                          double alpha_gm, const double *ff_top, const double *ff_bot, const int *ig_top,
+                          const int *ig_bot, double *flux_f_x, double *flux_f_y, const double *swbal,
+                          const double *src, double src_factor, const double *hhu, const double *hhv,
+                          const double *hhqn, const double *hhqp)
+{
+    SETUP(&g->b);
+    const size_t nt = NTOT(B);
+    const size_t n3 = nt * (size_t)nz, n31 = nt * (size_t)(nz + 1);
+    double *flux_x = calloc(n3, sizeof(double)), *flux_y = calloc(n3, sizeof(double));
+    double *flux_zx = calloc(n31, sizeof(double)), *flux_zy = calloc(n31, sizeof(double));
+    double *coef_zx = calloc(n31, sizeof(double)), *coef_zy = calloc(n31, sizeof(double));
+    double *sfgm_zx = calloc(n31, sizeof(double)), *sfgm_zy = calloc(n31, sizeof(double));
+    double *fn = calloc(n3, sizeof(double));
+    memset(flux_f_x, 0, 4 * nt * sizeof(double));
+    memset(flux_f_y, 0, 4 * nt * sizeof(double));
+#define F4(a, m, n, c) (a)[I(m, n) + (size_t)((c) - 1) * nt]
+    /* :101-253 */
+#pragma omp parallel for
+    for (int n = B->ny_start; n <= B->ny_end; n++) {
+        double *flux_1d = malloc((size_t)(nz + 2) * sizeof(double)), *mu_1d = malloc((size_t)(nz + 2) * sizeof(double));
+        for (int m = B->nx_start; m <= B->nx_end; m++) {
+            const size_t i = I(m, n);
+            for (int V = 0; V < 2; V++) {
+                const float *mk = V ? g->lcv : g->lcu;
+                if (!(mk[i] > 0.5f)) continue;
+                /* the far point (u: m+1, v: n+1) and the u/v-specific metrics */
+                const int mf = V ? m : m + 1, nf = V ? n + 1 : n;
+                const double *hh = V ? hhv : hhu, *slr = V ? slry : slrx, *slz = V ? slzy : slzx;
+                const double *vel = V ? vv : uu;
+                const double dside = V ? g->dxh[i] : g->dyh[i];             /* dyh (u), dxh (v) */
+                const double dnorm = V ? g->dyt[i] : g->dxt[i];             /* dxt (u), dyt (v) */
+                double *flux = V ? flux_y : flux_x, *fz = V ? flux_zy : flux_zx;
+                double *coef = V ? coef_zy : coef_zx, *sfgm = V ? sfgm_zy : sfgm_zx;
+                double *ffo = V ? flux_f_y : flux_f_x;
+                for (int k = 1; k <= nz + 1; k++) flux_1d[k] = 0.0, mu_1d[k] = 0.0;
+                for (int k = 2; k <= nz; k++) {
+                    const double dfdz = (ffp[I3(m, n, k)] - ffp[I3(m, n, k - 1)] + ffp[I3(mf, nf, k)] -
+                                         ffp[I3(mf, nf, k - 1)]) / 2.0;
+                    const double dfdh = (ffp[I3(mf, nf, k)] - ffp[I3(m, n, k)] + ffp[I3(mf, nf, k - 1)] -
+                                         ffp[I3(m, n, k - 1)]) / 2.0;
+                    mu_1d[k] = (mu[I3(m, n, k)] + mu[I3(m, n, k - 1)] + mu[I3(mf, nf, k)] + mu[I3(mf, nf, k - 1)]) /
+                               4.0 * factor_mu * dside / dnorm;
+                    const double slope = ar * slr[I3(m, n, k)] + az * slz[I3(m, n, k)];
+                    flux_1d[k] = mu_1d[k] * (hh[i] * dfdh * hzt[k - 1] - slope * dfdz);
+                    fz[I3(m, n, k)] = mu_1d[k] * slope * dfdh;
+                    coef[I3(m, n, k)] = mu_1d[k] * (slope * slope) / hh[i] / hzt[k - 1];
+                    sfgm[I3(m, n, k)] = mu_1d[k] * (slr[I3(m, n, k)] - slz[I3(m, n, k)]) * alpha_gm;
+                }
+                for (int k = 1; k <= nz; k++) {
+                    double flux_diff;
+                    if (k == 1) flux_diff = flux_1d[k + 1] / hzt[k];
+                    else if (k < nz) flux_diff = (flux_1d[k] + flux_1d[k + 1]) / dz[k - 1] / 2.0;
+                    else flux_diff = flux_1d[k] / hzt[k - 1];
+                    const double flux_adv =
+                        -(vel[I3(m, n, k)] * hh[i] * dside * (ff[I3(m, n, k)] + ff[I3(mf, nf, k)]) / 2.0);
+                    const double vel_gm = (sfgm[I3(m, n, k + 1)] - sfgm[I3(m, n, k)]) / dz[k - 1];
+                    const double flux_gm = -(vel_gm * (ff[I3(m, n, k)] + ff[I3(mf, nf, k)]) / 2.0);
+                    flux[I3(m, n, k)] = flux_adv + flux_diff + flux_gm;
+                    F4(ffo, m, n, 1) = F4(ffo, m, n, 1) + dz[k - 1] * (flux_adv + flux_diff + flux_gm);
+                    F4(ffo, m, n, 2) = F4(ffo, m, n, 2) + dz[k - 1] * flux_adv;
+                    F4(ffo, m, n, 3) = F4(ffo, m, n, 3) + dz[k - 1] * flux_diff;
+                    F4(ffo, m, n, 4) = F4(ffo, m, n, 4) + dz[k - 1] * flux_gm;
+                }
+            }
+        }
+        free(flux_1d);
+        free(mu_1d);
+    }
+    /* :255-277: x-fluxes wrap in x, y-fluxes in y */
+    for (int k = 1; k <= nz + 1; k++) {
+        const size_t o = (size_t)(k - 1) * nt;
+        if (B->periodicity_x) {
+            if (k <= nz) ora_cyclize8_x(B, flux_x + o);
+            ora_cyclize8_x(B, flux_zx + o);
+            ora_cyclize8_x(B, coef_zx + o);
+            ora_cyclize8_x(B, sfgm_zx + o);
+        }
+        if (B->periodicity_y) {
+            if (k <= nz) ora_cyclize8_y(B, flux_y + o);
+            ora_cyclize8_y(B, flux_zy + o);
+            ora_cyclize8_y(B, coef_zy + o);
+            ora_cyclize8_y(B, sfgm_zy + o);
+        }
+    }
+    /* :279-403 */
+#pragma omp parallel for
+    for (int n = B->ny_start; n <= B->ny_end; n++) {
+        double *a = malloc(6 * (size_t)nz * sizeof(double));
+        double *bb = a + nz, *c = bb + nz, *eta = c + nz, *x = eta + nz, *y = x + nz;
+        double *rksi = malloc((size_t)nz * sizeof(double));
+        for (int m = B->nx_start; m <= B->nx_end; m++) {
+            const size_t i = I(m, n);
+            if (!(g->lu[i] > 0.5f)) continue;
+            const double dxy_x = g->dx[i], dxy_y = g->dy[i];
+            const double bp = hhqn[i] * dxy_x * dxy_y / tau / 2.0;
+            const double bp0 = hhqp[i] * dxy_x * dxy_y / tau / 2.0;
+            const double cu = (double)fmaxf(g->lcu[i] + g->lcu[I(m - 1, n)], 1e-10f);
+            const double cv = (double)fmaxf(g->lcv[i] + g->lcv[I(m, n - 1)], 1e-10f);
+            double fz_p = 0.0, fz_m, dp = 0.0, dm;
+            for (int k = 1; k <= nz; k++) {
+                const int q = k - 1;
+                fz_m = fz_p;
+                if (k < nz) {
+                    const double vel_gm = -(sfgm_zx[I3(m, n, k + 1)] - sfgm_zx[I3(m - 1, n, k + 1)] +
+                                            sfgm_zy[I3(m, n, k + 1)] - sfgm_zy[I3(m, n - 1, k + 1)]);
+                    fz_p = -((flux_zx[I3(m, n, k + 1)] + flux_zx[I3(m - 1, n, k + 1)]) / cu) -
+                           (flux_zy[I3(m, n, k + 1)] + flux_zy[I3(m, n - 1, k + 1)]) / cv +
+                           (coef_zx[I3(m, n, k + 1)] * (ffp[I3(m + 1, n, k + 1)] - ffp[I3(m + 1, n, k)]) +
+                            coef_zx[I3(m - 1, n, k + 1)] * (ffp[I3(m - 1, n, k + 1)] - ffp[I3(m - 1, n, k)])) /
+                               cu / 2.0 +
+                           (coef_zy[I3(m, n, k + 1)] * (ffp[I3(m, n + 1, k + 1)] - ffp[I3(m, n + 1, k)]) +
+                            coef_zy[I3(m, n - 1, k + 1)] * (ffp[I3(m, n - 1, k + 1)] - ffp[I3(m, n - 1, k)])) /
+                               cv / 2.0 -
+                           (ww[I3(m, n, k + 1)] * dxy_x * dxy_y + vel_gm) * (ff[I3(m, n, k)] + ff[I3(m, n, k + 1)]) /
+                               2.0;
+                } else {
+                    fz_p = 0.0;
+                }
+                const double nu_p = nu[I3(m, n, k + 1)] * factor_nu;
+                if (k == 1) dm = nu[I3(m, n, k)] * factor_nu * dxy_x * dxy_y / hhqn[i] / hzt[0];
+                else dm = dp;
+                if (k < nz)
+                    dp = (coef_zx[I3(m, n, k + 1)] + coef_zx[I3(m - 1, n, k + 1)]) / cu / 2.0 +
+                         (coef_zy[I3(m, n, k + 1)] + coef_zy[I3(m, n - 1, k + 1)]) / cv / 2.0 +
+                         nu_p * dxy_x * dxy_y / hhqn[i] / hzt[k];
+                else
+                    dp = nu_p * dxy_x * dxy_y / hhqn[i] / hzt[k];
+                const double rhs = flux_x[I3(m, n, k)] - flux_x[I3(m - 1, n, k)] + flux_y[I3(m, n, k)] -
+                                   flux_y[I3(m, n - 1, k)] + (fz_p - fz_m) / dz[q] +
+                                   src[I3(m, n, k)] * g->hhq_rest[i] * swbal[i] * src_factor * dxy_x * dxy_y;
+                if (k == 1) {
+                    c[q] = -dp / dz[q];
+                    a[q] = 0.0;
+                    if (ig_top[i] == 1) {
+                        bb[q] = bp + (dp + dm) / dz[q];
+                        eta[q] = bp0 * ffp[I3(m, n, k)] + rhs + dm * ff_top[i] / dz[q];
+                    } else {
+                        bb[q] = bp + dp / dz[q];
+                        eta[q] = bp0 * ffp[I3(m, n, k)] + rhs + ff_top[i] / dz[q] * dxy_x * dxy_y;
+                    }
+                } else if (k < nz) {
+                    c[q] = -dp / dz[q];
+                    a[q] = -dm / dz[q];
+                    bb[q] = bp + (dp + dm) / dz[q];
+                    eta[q] = bp0 * ffp[I3(m, n, k)] + rhs;
+                } else {
+                    c[q] = 0.0;
+                    a[q] = -dm / dz[q];
+                    if (ig_bot[i] == 1) {
+                        bb[q] = bp + (dp + dm) / dz[q];
+                        eta[q] = bp0 * ffp[I3(m, n, k)] + rhs + dp * ff_bot[i] / dz[q];
+                    } else {
+                        bb[q] = bp + dm / dz[q];
+                        eta[q] = bp0 * ffp[I3(m, n, k)] + rhs + ff_bot[i] / dz[q] * dxy_x * dxy_y;
+                    }
+                }
+            }
+            factor8(nz, a, bb, c, eta, rksi, x, y);
+            for (int k = 1; k <= nz; k++) fn[I3(m, n, k)] = rksi[k - 1];
+        }
+        free(a);
+        free(rksi);
+    }
+    /* :405-413 */
+    for (int k = 1; k <= nz; k++) {
+        if (B->periodicity_x) ora_cyclize8_x(B, fn + (size_t)(k - 1) * nt);
+        if (B->periodicity_y) ora_cyclize8_y(B, fn + (size_t)(k - 1) * nt);
+    }
+    /* :415-429 */
+    const double ts = g->time_smooth;
+#pragma omp parallel for
+    for (int n = B->ny_start - 1; n <= B->ny_end + 1; n++)
+        for (int m = B->nx_start - 1; m <= B->nx_end + 1; m++) {
+            if (!(g->lu[I(m, n)] > 0.5f)) continue;
+            for (int k = 1; k <= nz; k++) {
+                const size_t j = I3(m, n, k);
+                ffp[j] = ff[j] + ts * (fn[j] - 2.0 * ff[j] + ffp[j]) / 2.0;
+                ff[j] = fn[j];
+            }
+        }
+#undef F4
+    free(flux_x); free(flux_y); free(flux_zx); free(flux_zy);
+    free(coef_zx); free(coef_zy); free(sfgm_zx); free(sfgm_zy); free(fn);
+}
+
 /* Function/vel_ssh.f90:1030-1076 vertical_velocity: w from the continuity
  * equation, integrated from the bottom (w(nz+1) = 0), on lu points */
 void ora_vertical_velocity(const ora_grid *g, int nz, const double *dz, const double *u, const double *v,

@@ -157,6 +157,16 @@ void ora_baroclinic_dynamics(const ora_grid *g, int nz, const double *dz, const 
                              const double *hhvp, const double *hhvn, const double *hhh);
 void ora_vertical_velocity(const ora_grid *g, int nz, const double *dz, const double *u, const double *v,
                            double *w, const double *hu, const double *hv, const double *wflux);
+/* Function/tem_sal.f90:1-422 tracer_tran_diff (without its unused
+ * lateral-boundary arguments); hhu, hhv, hhqn, hhqp: internal-mode depths */
+void ora_tracer_tran_diff(const ora_grid *g, int nz, const double *dz, const double *hzt, double *ff, double *ffp,
+                          double tau, const double *uu, const double *vv, const double *ww, const double *mu,
+                          double factor_mu, const double *nu, double factor_nu, const double *slrx,
+                          const double *slry, const double *slzx, const double *slzy, double az, double ar,
+                          double alpha_gm, const double *ff_top, const double *ff_bot, const int *ig_top,
+                          const int *ig_bot, double *flux_f_x, double *flux_f_y, const double *swbal,
+                          const double *src, double src_factor, const double *hhu, const double *hhv,
+                          const double *hhqn, const double *hhqp);
 /* Function/depth.f90:223-254 depth_ave */
 void ora_depth_ave(const ora_grid *g, int nz, const double *dz, double *u, double *utr, const float *mask,
                    int kbcl);

@@ -184,6 +184,30 @@ def vertical_velocity(basin, dz, u, v, w, hu, hv, wflux):
     return w
 
 
+TRACER_3D = ("uu", "vv", "ww", "mu", "nu", "slrx", "slry", "slzx", "slzy", "src")
+
+
+def tracer_tran_diff(basin, dz, hzt, tau, ff, ffp, flux_f_x, flux_f_y, f):
+    """Function/tem_sal.f90:1-422 in place on ff, ffp (nz levels) and the
+    flux diagnostics flux_f_x, flux_f_y (bnd_x, bnd_y, 4); f holds the other
+    arguments by name (see ora_tracer_tran_diff)."""
+    g = grid_struct(basin)
+    dz = np.ascontiguousarray(dz, dtype=np.float64)
+    hzt = np.ascontiguousarray(hzt, dtype=np.float64)
+    ip = ctypes.POINTER(ctypes.c_int)
+    igt = np.asfortranarray(f["ig_top"], dtype=np.int32)
+    igb = np.asfortranarray(f["ig_bot"], dtype=np.int32)
+    c = ctypes.c_double
+    load().ora_tracer_tran_diff(
+        ctypes.byref(g), int(len(dz)), dz.ctypes.data_as(DP), hzt.ctypes.data_as(DP), _d(ff), _d(ffp), c(tau),
+        _d(f["uu"]), _d(f["vv"]), _d(f["ww"]), _d(f["mu"]), c(f["factor_mu"]), _d(f["nu"]), c(f["factor_nu"]),
+        _d(f["slrx"]), _d(f["slry"]), _d(f["slzx"]), _d(f["slzy"]), c(f["az"]), c(f["ar"]), c(f["alpha_gm"]),
+        _d(f["ff_top"]), _d(f["ff_bot"]), igt.ctypes.data_as(ip), igb.ctypes.data_as(ip), _d(flux_f_x),
+        _d(flux_f_y), _d(f["swbal"]), _d(f["src"]), c(f["src_factor"]), _d(f["hhu"]), _d(f["hhv"]), _d(f["hhqn"]),
+        _d(f["hhqp"]))
+    return ff, ffp, flux_f_x, flux_f_y
+
+
 def depth_ave(basin, dz, u, utr, mask, kbcl):
     """Function/depth.f90:223-254 in place on u (nz levels) and utr."""
     g = grid_struct(basin)
