@@ -206,7 +206,7 @@ int inmsom_vertical_velocity(inmsom_ctx *ctx, int nz, const double *dz, const do
                              double *w, const double *hu, const double *hv, const double *wflux);
 
 /* Replaces tracer_tran_diff, Function/tem_sal.f90:1-422 (called for
- * temperature and salinity at Control/dyncall.f90:262-332): one tracer's
+ * temperature and salinity at Control/dyncall.f90:265-338): one tracer's
  * leap-frog step with lateral advection, isoneutral diffusion and
  * Gent-McWilliams fluxes, implicit vertical diffusion per water column
  * (factor8) with the surface/bottom conditions of types 1 and 2, the
