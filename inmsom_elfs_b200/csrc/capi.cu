@@ -1221,7 +1221,7 @@ int trc_alloc(inmsom_ctx *c, int nz)
     const size_t planes = (size_t)TN3 * nz + (size_t)TN31 * (nz + 1) + TN2;
     CK(cudaMalloc((void **)&c->trc, planes * col_plane(c) * sizeof(double)));
     CK(cudaMemsetAsync(c->trc, 0, planes * col_plane(c) * sizeof(double), c->stream));
-    CK(cudaMalloc((void **)&c->trc_lev, (2 * (size_t)nz + 1) * sizeof(double)));
+    CK(cudaMalloc((void **)&c->trc_lev, (2 * (size_t)nz + 2) * sizeof(double)));   // + the solve's flag
     c->trc_nz = nz;
     return INMSOM_OK;
 }
@@ -1291,6 +1291,8 @@ int inmsom_tracer_tran_diff(inmsom_ctx *c, int nz, const double *dz, const doubl
     a.flux_x = trc3(c, T_FLX); a.flux_y = trc3(c, T_FLY);
     a.flux_zx = trc31(c, T_FZX); a.flux_zy = trc31(c, T_FZY); a.coef_zx = trc31(c, T_COX); a.coef_zy = trc31(c, T_COY);
     a.sfgm_zx = trc31(c, T_SGX); a.sfgm_zy = trc31(c, T_SGY);
+    a.flag = reinterpret_cast<int *>(c->trc_lev + 2 * nz + 1);
+    CK(cudaMemsetAsync(a.flag, 0, sizeof(int), c->stream));
     column::Levels L;
     L.nz = nz;
     L.plane = (long long)col_plane(c);
@@ -1300,12 +1302,15 @@ int inmsom_tracer_tran_diff(inmsom_ctx *c, int nz, const double *dz, const doubl
         return set_err(INMSOM_ECUDA, "inmsom_tracer_tran_diff: launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     CK(cudaGetLastError());
     CK(cudaEventRecord(c->ph[2], c->stream));
+    int flag = 0;
+    CK(cudaMemcpyAsync(&flag, a.flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
     CKR(d2h3(c, ff, trc3(c, T_FFO), nz));
     CKR(d2h3(c, ffp, trc3(c, T_FFPO), nz));
     CKR(d2h3(c, flux_f_x, trc2(c, T_FFX), 4));
     CKR(d2h3(c, flux_f_y, trc2(c, T_FFY), 4));
     CK(cudaEventRecord(c->ph[3], c->stream));
     CKR(sync_stream(c));
+    if (flag) return set_err(INMSOM_ETIMEOUT, "inmsom_tracer_tran_diff: a bounded wait of the solve gave up");
     c->ph_valid = true;
     return INMSOM_OK;
 }

@@ -138,6 +138,35 @@ __device__ __forceinline__ void back_filter(const double *xs, const double *ys, 
     }
 }
 
+// The same with the sweep kept in the output arrays: x(k) in outp, y(k) in
+// out at level k, written by this thread in the forward sweep and
+// overwritten here with the filtered values (one level ahead loaded first;
+// no other thread touches these addresses, and the lines stay in L2).
+__device__ __forceinline__ void back_filter_inplace(int nz, long long P, long long i, double r, double ts,
+                                                    const double *self, const double *selfp, double *out,
+                                                    double *outp)
+{
+    long long o = (long long)(nz - 1) * P + i;
+    double cu = self[o], cp = selfp[o], xk = 0.0, yk = 0.0;
+    for (int k = nz; k >= 1; k--) {
+        double cu1 = 0.0, cp1 = 0.0, x1 = 0.0, y1 = 0.0;
+        if (k > 1) {
+            cu1 = self[o - P];
+            cp1 = selfp[o - P];
+            x1 = outp[o - P];
+            y1 = out[o - P];
+        }
+        if (k < nz) r = xk * r + yk;
+        outp[o] = cu + ts * (r - 2.0 * cu + cp) / 2.0;
+        out[o] = r;
+        cu = cu1;
+        cp = cp1;
+        xk = x1;
+        yk = y1;
+        o -= P;
+    }
+}
+
 // ---- the direct kernel (any nz up to MAX_NZ): each thread loads its
 // column's values from global memory level by level ----------------------
 template <bool V>
@@ -218,7 +247,7 @@ constexpr int NS = 4;                    // ring slots (levels)
 constexpr int NROW = 14;                 // row segments per level
 constexpr int RW = CW + 4;               // doubles per staged segment
 constexpr int SLOT_D = NROW * RW;        // doubles per slot
-constexpr int NZ_STAGED = 96;
+constexpr int NZ_STAGED = MAX_NZ;
 constexpr unsigned WAIT_LIMIT = 1u << 20;
 
 // the row segments of a slot: field (level j), row
@@ -226,8 +255,7 @@ enum { R_UU0, R_UU1, R_VVM, R_VV0, R_UUP, R_VVP, R_RX, R_RY, R_RXT, R_RYT, R_NU0
 
 size_t staged_smem(int nz)
 {
-    return ((size_t)NS * SLOT_D + 2 * (size_t)nz * NCW * 32 + 2 * (size_t)nz + 1) * sizeof(double) +
-           2 * NS * sizeof(uint64_t);
+    return ((size_t)NS * SLOT_D + 2 * (size_t)nz + 1) * sizeof(double) + 2 * NS * sizeof(uint64_t);
 }
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p) { return (uint32_t)__cvta_generic_to_shared(p); }
@@ -308,7 +336,7 @@ template <bool V>
 __device__ __forceinline__ bool staged_column(const Dom &D, const GridDev &g, const Levels &L,
                                               const BaroclinicArgs &a, double ts, int m, int n, int cs,
                                               const double *ring, const double *sdz, uint64_t *full,
-                                              uint64_t *empty, double *xs, double *ys, int lane)
+                                              uint64_t *empty, int lane)
 {
     const int nz = L.nz;
     const long long P = L.plane;
@@ -333,8 +361,9 @@ __device__ __forceinline__ bool staged_column(const Dom &D, const GridDev &g, co
             if (k == 1) s0 = st[rself * RW + cs];
             const LevelIn v = staged_level<V>(st, snx, cs, k == nz);
             level_step<V>(c, v, k, nz, sdz[k - 1], k < nz ? sdz[nz + k] : 1.0, dp, fz_p, xm, ym, s0);
-            xs[(k - 1) * NCW * 32] = xm;
-            ys[(k - 1) * NCW * 32] = ym;
+            const long long o = (long long)(k - 1) * P + i;
+            outp[o] = xm;
+            out[o] = ym;
         } else if (act) {
             const long long o = (long long)(k - 1) * P + i;
             out[o] = st[rself * RW + cs];
@@ -343,18 +372,16 @@ __device__ __forceinline__ bool staged_column(const Dom &D, const GridDev &g, co
         __syncwarp();
         if (lane == 0) mbar_arrive(&empty[sk]);
     }
-    if (ok && ocean) back_filter(xs, ys, NCW * 32, nz, P, i, ym, ts, self, selfp, out, outp);
+    if (ok && ocean) back_filter_inplace(nz, P, i, ym, ts, self, selfp, out, outp);
     return ok;
 }
 
-__global__ void __launch_bounds__((NCW + 1) * 32) k_columns(Dom D, GridDev g, Levels L, BaroclinicArgs a, double ts)
+__global__ void __launch_bounds__((NCW + 1) * 32, 4) k_columns(Dom D, GridDev g, Levels L, BaroclinicArgs a, double ts)
 {
     extern __shared__ __align__(128) double sm[];
     const int nz = L.nz;
     double *ring = sm;
-    double *xs0 = ring + (size_t)NS * SLOT_D;
-    double *ys0 = xs0 + (size_t)nz * NCW * 32;
-    double *sdz = ys0 + (size_t)nz * NCW * 32;            // dz (nz), hzt (nz + 1)
+    double *sdz = ring + (size_t)NS * SLOT_D;             // dz (nz), hzt (nz + 1)
     uint64_t *full = reinterpret_cast<uint64_t *>(sdz + 2 * nz + 1);
     uint64_t *empty = full + NS;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
@@ -424,9 +451,8 @@ __global__ void __launch_bounds__((NCW + 1) * 32) k_columns(Dom D, GridDev g, Le
     const int col = (warp & 1) * 32 + lane;
     const int m = m0 + col;
     const int cs = (m - D.bnd_x1 + D.xoff) - c0;
-    double *xs = xs0 + warp * 32 + lane, *ys = ys0 + warp * 32 + lane;
-    const bool ok = V ? staged_column<true>(D, g, L, a, ts, m, n, cs, ring, sdz, full, empty, xs, ys, lane)
-                      : staged_column<false>(D, g, L, a, ts, m, n, cs, ring, sdz, full, empty, xs, ys, lane);
+    const bool ok = V ? staged_column<true>(D, g, L, a, ts, m, n, cs, ring, sdz, full, empty, lane)
+                      : staged_column<false>(D, g, L, a, ts, m, n, cs, ring, sdz, full, empty, lane);
     if (!ok && lane == 0) atomicOr(a.flag, 1);
 }
 
@@ -612,102 +638,208 @@ __global__ void __launch_bounds__(TB) k_tracer_flux(Dom D, GridDev g, Levels L, 
     else tracer_flux_point<true>(D, g, L, a, m, n);
 }
 
-// :279-403 at one T point of the interior (the vertical diffusion system,
-// factor8), then the filter of :415-429 there
-__global__ void __launch_bounds__(TB) k_tracer_solve(Dom D, GridDev g, Levels L, TracerArgs a, double ts)
+// :279-403 at the T points of the interior (the vertical diffusion system,
+// factor8), then the filter of :415-429 there.  Staged like k_columns: a CTA
+// owns CW columns of row n (warps 0-1) and a copy warp (2) brings, for
+// every level j, the nineteen row segments the equations of levels j - 1
+// and j read into a 3-slot mbarrier ring; stage nz + 1 holds nu only.  The
+// sweep's x, y go to ffp_out, ff_out (back_filter_inplace).
+constexpr int TNS = 3;                    // ring slots of the tracer solve
+constexpr int TNROW = 19;
+constexpr int TSLOT_D = TNROW * RW;
+enum {
+    Q_FF, Q_FFPM, Q_FFP0, Q_FFPP, Q_FLX, Q_FLY0, Q_FLYM, Q_SRC, Q_NU,          // levels 1..nz (nu: 1..nz+1)
+    Q_WW, Q_FZX, Q_FZY0, Q_FZYM, Q_COX, Q_COY0, Q_COYM, Q_SGX, Q_SGY0, Q_SGYM  // levels 2..nz
+};
+
+size_t tracer_smem(int nz)
 {
-    extern __shared__ double sm[];
-    const int m = D.nx_start + blockIdx.x * TB + threadIdx.x;
-    const int n = D.ny_start + blockIdx.y;
-    if (m > D.nx_end) return;
-    const long long i = X(m, n);
-    const long long P = L.plane;
+    return ((size_t)TNS * TSLOT_D + 2 * (size_t)nz + 1) * sizeof(double) + 2 * TNS * sizeof(uint64_t);
+}
+
+__global__ void __launch_bounds__(3 * 32) k_tracer_solve(Dom D, GridDev g, Levels L, TracerArgs a, double ts)
+{
+    extern __shared__ __align__(128) double sm[];
     const int nz = L.nz;
-    if (!(g.lu[i] > 0.5f)) {
-        for (int k = 0; k < nz; k++) {
-            const long long o = (long long)k * P + i;
-            a.ff_out[o] = a.ff[o];
-            a.ffp_out[o] = a.ffp[o];
+    double *ring = sm;
+    double *sdz = ring + (size_t)TNS * TSLOT_D;           // dz (nz), hzt (nz + 1)
+    uint64_t *full = reinterpret_cast<uint64_t *>(sdz + 2 * nz + 1);
+    uint64_t *empty = full + TNS;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = D.nx_start + blockIdx.x * CW, n = D.ny_start + blockIdx.y;
+    for (int t = threadIdx.x; t < 2 * nz + 1; t += blockDim.x) sdz[t] = L.dz[t];
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < TNS; s++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&full[s])), "r"(1) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&empty[s])), "r"(2) : "memory");
         }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const int cm0 = m0 - D.bnd_x1 + D.xoff;
+    const int mlast = min(m0 + CW - 1, D.nx_end);
+    const int c0 = (cm0 - 1) & ~1;
+    const int cnt = ((mlast - D.bnd_x1 + D.xoff + 2 - c0) + 1) & ~1;
+    const long long P = L.plane;
+
+    if (warp == 2) {
+        if (lane != 0) return;
+        const long long rb = (long long)(n - D.bnd_y1) * D.pitch + c0, pt = D.pitch;
+        const uint32_t seg = (uint32_t)cnt * 8u;
+        int armed = 0;
+        bool ok = true;
+        for (int j = 1; j <= nz + 1; j++) {
+            const int s = (j - 1) % TNS;
+            if (j > TNS && !mbar_wait(&empty[s], (uint32_t)(((j - 1) / TNS - 1) & 1))) {
+                ok = false;
+                break;
+            }
+            double *slot = ring + (size_t)s * TSLOT_D;
+            const long long lv = (long long)(j - 1) * P + rb;
+            const int nrow = j == nz + 1 ? 1 : (j == 1 ? Q_NU + 1 : TNROW);
+            mbar_expect(&full[s], seg * (uint32_t)nrow);
+            bulk_copy(slot + Q_NU * RW, a.nu + lv, seg, &full[s]);
+            if (j <= nz) {
+                bulk_copy(slot + Q_FF * RW, a.ff + lv, seg, &full[s]);
+                bulk_copy(slot + Q_FFPM * RW, a.ffp + lv - pt, seg, &full[s]);
+                bulk_copy(slot + Q_FFP0 * RW, a.ffp + lv, seg, &full[s]);
+                bulk_copy(slot + Q_FFPP * RW, a.ffp + lv + pt, seg, &full[s]);
+                bulk_copy(slot + Q_FLX * RW, a.flux_x + lv, seg, &full[s]);
+                bulk_copy(slot + Q_FLY0 * RW, a.flux_y + lv, seg, &full[s]);
+                bulk_copy(slot + Q_FLYM * RW, a.flux_y + lv - pt, seg, &full[s]);
+                bulk_copy(slot + Q_SRC * RW, a.src + lv, seg, &full[s]);
+            }
+            if (j > 1 && j <= nz) {
+                bulk_copy(slot + Q_WW * RW, a.ww + lv, seg, &full[s]);
+                bulk_copy(slot + Q_FZX * RW, a.flux_zx + lv, seg, &full[s]);
+                bulk_copy(slot + Q_FZY0 * RW, a.flux_zy + lv, seg, &full[s]);
+                bulk_copy(slot + Q_FZYM * RW, a.flux_zy + lv - pt, seg, &full[s]);
+                bulk_copy(slot + Q_COX * RW, a.coef_zx + lv, seg, &full[s]);
+                bulk_copy(slot + Q_COY0 * RW, a.coef_zy + lv, seg, &full[s]);
+                bulk_copy(slot + Q_COYM * RW, a.coef_zy + lv - pt, seg, &full[s]);
+                bulk_copy(slot + Q_SGX * RW, a.sfgm_zx + lv, seg, &full[s]);
+                bulk_copy(slot + Q_SGY0 * RW, a.sfgm_zy + lv, seg, &full[s]);
+                bulk_copy(slot + Q_SGYM * RW, a.sfgm_zy + lv - pt, seg, &full[s]);
+            }
+            armed = j;
+        }
+        if (!ok) atomicOr(a.flag, 1);
+        for (int j = max(1, armed - TNS + 1); j <= armed; j++)
+            (void)mbar_wait(&full[(j - 1) % TNS], (uint32_t)(((j - 1) / TNS) & 1));
         return;
     }
-    double *xs = sm + threadIdx.x, *ys = sm + (size_t)nz * TB + threadIdx.x;
-    const long long w = X(m - 1, n) - i, s_ = X(m, n - 1) - i, e = 1, nn = D.pitch;
-    const double dx = g.dx[i], dy = g.dy[i];
-    const double hn = a.hhqn[i];
-    const double bp = hn * dx * dy / a.tau / 2.0;
-    const double bp0 = a.hhqp[i] * dx * dy / a.tau / 2.0;
-    const double cu = (double)fmaxf(g.lcu[i] + g.lcu[i + w], 1e-10f);
-    const double cv = (double)fmaxf(g.lcv[i] + g.lcv[i + s_], 1e-10f);
-    const double hq = g.hrest[i], swb = a.swbal[i];
-    const int igt = a.ig_top[i], igb = a.ig_bot[i];
+
+    const int m = m0 + warp * 32 + lane;
+    const bool act = m <= D.nx_end;
+    const long long i = act ? X(m, n) : 0;
+    const bool ocean = act && g.lu[i] > 0.5f;
+    const int cs = (m - D.bnd_x1 + D.xoff) - c0;
+    double dx = 0.0, dy = 0.0, hn = 0.0, bp = 0.0, bp0 = 0.0, cu = 0.0, cv = 0.0, hq = 0.0, swb = 0.0;
+    double ftop = 0.0, fbot = 0.0;
+    int igt = 0, igb = 0;
+    if (ocean) {
+        dx = g.dx[i];
+        dy = g.dy[i];
+        hn = a.hhqn[i];
+        bp = hn * dx * dy / a.tau / 2.0;
+        bp0 = a.hhqp[i] * dx * dy / a.tau / 2.0;
+        cu = (double)fmaxf(g.lcu[i] + g.lcu[i - 1], 1e-10f);
+        cv = (double)fmaxf(g.lcv[i] + g.lcv[i - D.pitch], 1e-10f);
+        hq = g.hrest[i];
+        swb = a.swbal[i];
+        ftop = a.ff_top[i];
+        fbot = a.ff_bot[i];
+        igt = a.ig_top[i];
+        igb = a.ig_bot[i];
+    }
     double fz_p = 0.0, dp = 0.0, xm = 0.0, ym = 0.0;
-    for (int k = 1; k <= nz; k++) {
+    bool ok = true;
+    for (int k = 1; k <= nz && ok; k++) {
+        const int sk = (k - 1) % TNS, sn = k % TNS;
+        ok = mbar_wait(&full[sk], (uint32_t)(((k - 1) / TNS) & 1)) && mbar_wait(&full[sn], (uint32_t)((k / TNS) & 1));
+        ok = __all_sync(0xffffffffu, ok);
+        if (!ok) break;
+        const double *st = ring + (size_t)sk * TSLOT_D, *nx = ring + (size_t)sn * TSLOT_D;
         const int q = k - 1;
         const long long o = (long long)q * P + i;
-        const double dzk = L.dz[q];
-        const double fz_m = fz_p;
-        if (k < nz) {
-            const long long o1 = o + P;
-            const double vel_gm = -(a.sfgm_zx[o1] - a.sfgm_zx[o1 + w] + a.sfgm_zy[o1] - a.sfgm_zy[o1 + s_]);
-            fz_p = -((a.flux_zx[o1] + a.flux_zx[o1 + w]) / cu) - (a.flux_zy[o1] + a.flux_zy[o1 + s_]) / cv +
-                   (a.coef_zx[o1] * (a.ffp[o1 + e] - a.ffp[o + e]) + a.coef_zx[o1 + w] * (a.ffp[o1 + w] - a.ffp[o + w])) /
-                       cu / 2.0 +
-                   (a.coef_zy[o1] * (a.ffp[o1 + nn] - a.ffp[o + nn]) +
-                    a.coef_zy[o1 + s_] * (a.ffp[o1 + s_] - a.ffp[o + s_])) /
-                       cv / 2.0 -
-                   (a.ww[o1] * dx * dy + vel_gm) * (a.ff[o] + a.ff[o1]) / 2.0;
-        } else {
-            fz_p = 0.0;
-        }
-        const double nu_p = a.nu[o + P] * a.factor_nu;
-        const double dm = k == 1 ? a.nu[o] * a.factor_nu * dx * dy / hn / L.hzt[0] : dp;
-        if (k < nz)
-            dp = (a.coef_zx[o + P] + a.coef_zx[o + P + w]) / cu / 2.0 +
-                 (a.coef_zy[o + P] + a.coef_zy[o + P + s_]) / cv / 2.0 + nu_p * dx * dy / hn / L.hzt[k];
-        else
-            dp = nu_p * dx * dy / hn / L.hzt[k];
-        const double rhs = a.flux_x[o] - a.flux_x[o + w] + a.flux_y[o] - a.flux_y[o + s_] + (fz_p - fz_m) / dzk +
-                           a.src[o] * hq * swb * a.src_factor * dx * dy;
-        const double base = a.ffp[o];
-        double cc, aa = 0.0, bb, eta;
-        if (k == 1) {
-            cc = -dp / dzk;
-            if (igt == 1) {
-                bb = bp + (dp + dm) / dzk;
-                eta = bp0 * base + rhs + dm * a.ff_top[i] / dzk;
+        if (ocean) {
+            const double dzk = sdz[q];
+            const double fz_m = fz_p;
+            if (k < nz) {
+                const double vel_gm = -(nx[Q_SGX * RW + cs] - nx[Q_SGX * RW + cs - 1] + nx[Q_SGY0 * RW + cs] -
+                                        nx[Q_SGYM * RW + cs]);
+                fz_p = -((nx[Q_FZX * RW + cs] + nx[Q_FZX * RW + cs - 1]) / cu) -
+                       (nx[Q_FZY0 * RW + cs] + nx[Q_FZYM * RW + cs]) / cv +
+                       (nx[Q_COX * RW + cs] * (nx[Q_FFP0 * RW + cs + 1] - st[Q_FFP0 * RW + cs + 1]) +
+                        nx[Q_COX * RW + cs - 1] * (nx[Q_FFP0 * RW + cs - 1] - st[Q_FFP0 * RW + cs - 1])) /
+                           cu / 2.0 +
+                       (nx[Q_COY0 * RW + cs] * (nx[Q_FFPP * RW + cs] - st[Q_FFPP * RW + cs]) +
+                        nx[Q_COYM * RW + cs] * (nx[Q_FFPM * RW + cs] - st[Q_FFPM * RW + cs])) /
+                           cv / 2.0 -
+                       (nx[Q_WW * RW + cs] * dx * dy + vel_gm) * (st[Q_FF * RW + cs] + nx[Q_FF * RW + cs]) / 2.0;
             } else {
-                bb = bp + dp / dzk;
-                eta = bp0 * base + rhs + a.ff_top[i] / dzk * dx * dy;
+                fz_p = 0.0;
             }
-        } else if (k < nz) {
-            cc = -dp / dzk;
-            aa = -dm / dzk;
-            bb = bp + (dp + dm) / dzk;
-            eta = bp0 * base + rhs;
-        } else {
-            cc = 0.0;
-            aa = -dm / dzk;
-            if (igb == 1) {
+            const double nu_p = nx[Q_NU * RW + cs] * a.factor_nu;
+            const double dm = k == 1 ? st[Q_NU * RW + cs] * a.factor_nu * dx * dy / hn / sdz[nz] : dp;
+            if (k < nz)
+                dp = (nx[Q_COX * RW + cs] + nx[Q_COX * RW + cs - 1]) / cu / 2.0 +
+                     (nx[Q_COY0 * RW + cs] + nx[Q_COYM * RW + cs]) / cv / 2.0 + nu_p * dx * dy / hn / sdz[nz + k];
+            else
+                dp = nu_p * dx * dy / hn / sdz[nz + k];
+            const double rhs = st[Q_FLX * RW + cs] - st[Q_FLX * RW + cs - 1] + st[Q_FLY0 * RW + cs] -
+                               st[Q_FLYM * RW + cs] + (fz_p - fz_m) / dzk +
+                               st[Q_SRC * RW + cs] * hq * swb * a.src_factor * dx * dy;
+            const double base = st[Q_FFP0 * RW + cs];
+            double cc, aa = 0.0, bb, eta;
+            if (k == 1) {
+                cc = -dp / dzk;
+                if (igt == 1) {
+                    bb = bp + (dp + dm) / dzk;
+                    eta = bp0 * base + rhs + dm * ftop / dzk;
+                } else {
+                    bb = bp + dp / dzk;
+                    eta = bp0 * base + rhs + ftop / dzk * dx * dy;
+                }
+            } else if (k < nz) {
+                cc = -dp / dzk;
+                aa = -dm / dzk;
                 bb = bp + (dp + dm) / dzk;
-                eta = bp0 * base + rhs + dp * a.ff_bot[i] / dzk;
+                eta = bp0 * base + rhs;
             } else {
-                bb = bp + dm / dzk;
-                eta = bp0 * base + rhs + a.ff_bot[i] / dzk * dx * dy;
+                cc = 0.0;
+                aa = -dm / dzk;
+                if (igb == 1) {
+                    bb = bp + (dp + dm) / dzk;
+                    eta = bp0 * base + rhs + dp * fbot / dzk;
+                } else {
+                    bb = bp + dm / dzk;
+                    eta = bp0 * base + rhs + fbot / dzk * dx * dy;
+                }
             }
+            if (k == 1) {
+                xm = -cc / bb;
+                ym = eta / bb;
+            } else {
+                const double scr = 1.0 / (aa * xm + bb);
+                ym = (eta - aa * ym) * scr;
+                xm = -cc * scr;
+            }
+            a.ffp_out[o] = xm;
+            a.ff_out[o] = ym;
+        } else if (act) {
+            a.ff_out[o] = st[Q_FF * RW + cs];
+            a.ffp_out[o] = st[Q_FFP0 * RW + cs];
         }
-        if (k == 1) {
-            xm = -cc / bb;
-            ym = eta / bb;
-        } else {
-            const double scr = 1.0 / (aa * xm + bb);
-            ym = (eta - aa * ym) * scr;
-            xm = -cc * scr;
-        }
-        xs[q * TB] = xm;
-        ys[q * TB] = ym;
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[sk]);
     }
-    back_filter(xs, ys, TB, nz, P, i, ym, ts, a.ff, a.ffp, a.ff_out, a.ffp_out);
+    if (!ok) {
+        if (lane == 0) atomicOr(a.flag, 1);
+        return;
+    }
+    // the copy warp's last stage (nz + 1, slot nz % TNS) was waited on above
+    if (ocean) back_filter_inplace(nz, P, i, ym, ts, a.ff, a.ffp, a.ff_out, a.ffp_out);
 }
 
 // :415-429 outside the interior (the ring with the wrapped new tracer,
@@ -853,7 +985,8 @@ int baroclinic_dynamics(const Dom &d, const GridDev &g, const Consts &c, const L
 int tracer_tran_diff(const Dom &d, const GridDev &g, const Consts &c, const Levels &L, const TracerArgs &a,
                      cudaStream_t s)
 {
-    if (L.nz < 2 || L.nz > MAX_NZ || wrap_inside(d)) return -1;
+    // the staged solve's 16-byte segments need an even row pitch and level stride
+    if (L.nz < 2 || L.nz > MAX_NZ || wrap_inside(d) || d.pitch % 2 || L.plane % 2 || !a.flag) return -1;
     const int nxi = d.nx_end - d.nx_start + 1, nyi = d.ny_end - d.ny_start + 1;
     k_tracer_flux<<<dim3((nxi + TB - 1) / TB, nyi, 2), TB, 0, s>>>(d, g, L, a);
     // the x-fluxes wrap in x, the y-fluxes in y (Function/tem_sal.f90:265-277)
@@ -867,10 +1000,10 @@ int tracer_tran_diff(const Dom &d, const GridDev &g, const Consts &c, const Leve
         for (double *f : {a.flux_zy, a.coef_zy, a.sfgm_zy})
             k_cyclize_y3<<<dim3((d.nxa() + 127) / 128, L.nz + 1), 128, 0, s>>>(d, L.plane, f);
     }
-    const size_t smem = 2 * (size_t)L.nz * TB * sizeof(double);
+    const size_t smem = tracer_smem(L.nz);
     if (cudaFuncSetAttribute(k_tracer_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return -1;
-    k_tracer_solve<<<dim3((nxi + TB - 1) / TB, nyi), TB, smem, s>>>(d, g, L, a, c.ts);
+    k_tracer_solve<<<dim3((nxi + CW - 1) / CW, nyi), 3 * 32, smem, s>>>(d, g, L, a, c.ts);
     const int count = d.nxa() * d.nya() - nxi * nyi;
     if (count > 0) k_tracer_border<<<dim3((count + 127) / 128, L.nz), 128, 0, s>>>(d, g, L, a, c.ts, count);
     return 0;

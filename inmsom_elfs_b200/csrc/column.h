@@ -66,6 +66,8 @@ struct TracerArgs {
     // work: lateral fluxes (nz), their vertical parts, coefficients and GM
     // stream functions (nz + 1); zero outside the interior
     double *flux_x, *flux_y, *flux_zx, *flux_zy, *coef_zx, *coef_zy, *sfgm_zx, *sfgm_zy;
+    // set to nonzero when a bounded wait of the solve gave up; zero before the launch
+    int *flag;
 };
 
 // Function/tem_sal.f90:1-422 on one domain (hhq_rest from the grid's rest
