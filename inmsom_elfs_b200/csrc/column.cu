@@ -2,17 +2,16 @@
 // expression keeps the left-to-right order of the Fortran line it cites.
 //
 // baroclinic_dynamics runs as two kernels:
-//  1. k_columns (k_columns_direct above 96 levels): every interior water
-//     column and velocity component is one thread, which builds the
-//     tridiagonal system level by level, runs factor8's forward elimination
-//     as it goes (x, y of the sweep kept in shared memory), then
-//     back-substitutes from the bottom and applies the Robert-Asselin filter
-//     to the new velocity at once, writing uu/uup (vv/vvp) to the output
-//     arrays.  The inputs stay untouched, so the neighbouring columns'
-//     Coriolis and advection reads see the old state.  k_columns stages
-//     every level's rows in shared memory with bulk asynchronous copies (a
-//     copy warp runs ahead of the compute warps through a ring of mbarrier
-//     slots); k_columns_direct loads them per thread.
+//  1. k_columns: every interior water column and velocity component is one
+//     thread, which builds the tridiagonal system level by level, runs
+//     factor8's forward elimination as it goes (x, y of the sweep kept in
+//     the output arrays), then back-substitutes from the bottom and applies
+//     the Robert-Asselin filter to the new velocity at once, writing uu/uup
+//     (vv/vvp) to the output arrays.  The inputs stay untouched, so the
+//     neighbouring columns' Coriolis and advection reads see the old state.
+//     Every level's rows are staged in shared memory by bulk asynchronous
+//     copies (a copy warp runs ahead of the compute warps through a ring of
+//     mbarrier slots).
 //  2. k_border, over every point of the arrays outside the interior: the
 //     filter on the one-point ring with the new velocity the periodic wrap
 //     brings there (zero without a wrap, as the reference's un = 0), a copy
@@ -24,8 +23,8 @@ namespace column {
 
 namespace {
 
-constexpr int TB = 64;          // threads (water columns) per block of k_columns_direct
-constexpr int MAX_NZ = 200;     // 2 * MAX_NZ * TB doubles of shared memory
+constexpr int TB = 64;          // threads (water columns) per block of k_tracer_flux
+constexpr int MAX_NZ = 200;     // levels (dz, hzt in shared memory)
 constexpr int BX = 32, BY = 8;
 
 #define X(m_, n_) ix(D, (m_), (n_))
@@ -114,34 +113,13 @@ __device__ __forceinline__ void level_step(const ColConst &c, const LevelIn &v, 
     s0 = v.s1;
 }
 
-// factor8's back substitution (:517-520) from the bottom, with the filter
-// of :1002-1024 at this point: uup = uu + ts*(un - 2 uu + uup)/2, uu = un.
-// xs, ys: the sweep of levels 1..nz at stride `stride`; r starts as y(nz).
-__device__ __forceinline__ void back_filter(const double *xs, const double *ys, int stride, int nz, long long P,
-                                            long long i, double r, double ts, const double *self,
-                                            const double *selfp, double *out, double *outp)
-{
-    long long o = (long long)(nz - 1) * P + i;
-    double cu = self[o], cp = selfp[o];
-    for (int k = nz; k >= 1; k--) {
-        double cu1 = 0.0, cp1 = 0.0;
-        if (k > 1) {                                      // next level up, one iteration ahead
-            cu1 = self[o - P];
-            cp1 = selfp[o - P];
-        }
-        if (k < nz) r = xs[(k - 1) * stride] * r + ys[(k - 1) * stride];
-        outp[o] = cu + ts * (r - 2.0 * cu + cp) / 2.0;
-        out[o] = r;
-        cu = cu1;
-        cp = cp1;
-        o -= P;
-    }
-}
-
-// The same with the sweep kept in the output arrays: x(k) in outp, y(k) in
-// out at level k, written by this thread in the forward sweep and
-// overwritten here with the filtered values (one level ahead loaded first;
-// no other thread touches these addresses, and the lines stay in L2).
+// factor8's back substitution (Service/oc_algorithms.f90:517-520) from the
+// bottom, with the filter of Function/vel_ssh.f90:1002-1024 at this point:
+// uup = uu + ts*(un - 2 uu + uup)/2, uu = un.  The sweep's x(k), y(k) are
+// in outp, out at level k, written by this thread in the forward sweep and
+// overwritten here with the filtered values (the next level up loaded one
+// iteration ahead; no other thread touches these addresses, and the lines
+// are still in L2); r starts as y(nz).
 __device__ __forceinline__ void back_filter_inplace(int nz, long long P, long long i, double r, double ts,
                                                     const double *self, const double *selfp, double *out,
                                                     double *outp)
@@ -167,79 +145,16 @@ __device__ __forceinline__ void back_filter_inplace(int nz, long long P, long lo
     }
 }
 
-// ---- the direct kernel (any nz up to MAX_NZ): each thread loads its
-// column's values from global memory level by level ----------------------
-template <bool V>
-__device__ __forceinline__ void solve_column(const Dom &D, const GridDev &g, const Levels &L,
-                                             const BaroclinicArgs &a, double ts, int m, int n, double *xs,
-                                             double *ys)
-{
-    const long long i = X(m, n);
-    const long long P = L.plane;
-    const int nz = L.nz;
-    const long long e = far_off<V>(D), p = partner_off<V>(D);
-    const double *self = V ? a.vv : a.uu, *selfp = V ? a.vvp : a.uup, *other = V ? a.uu : a.vv;
-    double *out = V ? a.vv_out : a.uu_out, *outp = V ? a.vvp_out : a.uup_out;
-    const float mask = V ? g.lcv[i] : g.lcu[i];
-    if (!(mask > 0.5f)) {
-        for (int k = 0; k < nz; k++) {
-            const long long o = (long long)k * P + i;
-            out[o] = self[o];
-            outp[o] = selfp[o];
-        }
-        return;
-    }
-    const ColConst c = col_const<V>(D, g, a, i);
-    const double *rhs = V ? a.rhsy : a.rhsx, *rhst = V ? a.rhsy_tran : a.rhsx_tran;
-    double dp = 0.0, fz_p = 0.0, xm = 0.0, ym = 0.0;
-    double s0 = self[i];
-    for (int k = 1; k <= nz; k++) {
-        const long long o = (long long)(k - 1) * P + i;
-        LevelIn v;
-        v.sp = selfp[o];
-        v.r1 = rhs[o];
-        v.r2 = rhst[o];
-        v.oe = other[o + e];
-        v.o0 = other[o];
-        v.ope = other[o + p + e];
-        v.op = other[o + p];
-        if (k < nz) {
-            const long long o1 = o + P;
-            v.nu0 = a.nu[o1];
-            v.nu1 = a.nu[o1 + e];
-            v.w0 = a.ww[o1];
-            v.w1 = a.ww[o1 + e];
-            v.s1 = self[o1];
-        } else {
-            v.nu0 = v.nu1 = v.w0 = v.w1 = v.s1 = 0.0;
-        }
-        level_step<V>(c, v, k, nz, L.dz[k - 1], k < nz ? L.hzt[k] : 1.0, dp, fz_p, xm, ym, s0);
-        xs[(k - 1) * TB] = xm;
-        ys[(k - 1) * TB] = ym;
-    }
-    back_filter(xs, ys, TB, nz, P, i, ym, ts, self, selfp, out, outp);
-}
-
-__global__ void __launch_bounds__(TB) k_columns_direct(Dom D, GridDev g, Levels L, BaroclinicArgs a, double ts)
-{
-    extern __shared__ double sm[];
-    const int m = D.nx_start + blockIdx.x * TB + threadIdx.x;
-    const int n = D.ny_start + blockIdx.y;
-    if (m > D.nx_end) return;
-    double *xs = sm + threadIdx.x, *ys = sm + (size_t)L.nz * TB + threadIdx.x;
-    if (blockIdx.z == 0) solve_column<false>(D, g, L, a, ts, m, n, xs, ys);
-    else solve_column<true>(D, g, L, a, ts, m, n, xs, ys);
-}
-
-// ---- the staged kernel (nz up to NZ_STAGED) -------------------------------
+// ---- the column solve ------------------------------------------------------
 // A CTA owns CW consecutive columns of one row n for both components: warps
 // 0-1 the u columns, warps 2-3 the v columns, warp 4 the copies.  For every
 // level j the copy warp brings the fourteen row segments the level's
 // equations read (CW + 4 columns each, 16-byte aligned) into a ring slot
 // with 1-D bulk asynchronous copies completing on the slot's mbarrier; the
 // compute warps read the slot of level k and of level k + 1, then release
-// slot k.  The sweep's x, y stay in shared memory for the back
-// substitution, which re-reads uu/uup (vv/vvp) from global memory (L2).
+// slot k.  The sweep's x, y go to the output arrays, and the back
+// substitution re-reads them with uu/uup (vv/vvp) from global memory (L2),
+// so shared memory holds only the ring: four CTAs per SM (registers).
 
 constexpr int CW = 64;                   // columns per CTA
 constexpr int NCW = 4;                   // compute warps
@@ -247,7 +162,6 @@ constexpr int NS = 4;                    // ring slots (levels)
 constexpr int NROW = 14;                 // row segments per level
 constexpr int RW = CW + 4;               // doubles per staged segment
 constexpr int SLOT_D = NROW * RW;        // doubles per slot
-constexpr int NZ_STAGED = MAX_NZ;
 constexpr unsigned WAIT_LIMIT = 1u << 20;
 
 // the row segments of a slot: field (level j), row
@@ -552,90 +466,187 @@ __global__ void k_vertical_velocity(Dom D, GridDev g, Levels L, double rho, int 
 
 // ---- Function/tem_sal.f90: one tracer's step ---------------------------
 
-// :101-253 at one u (V = false) or v (V = true) point of the interior: the
-// lateral advective, diffusive and GM fluxes of every level, the vertical
-// parts and coefficients of the isoneutral flux (levels 2..nz; levels 1 and
-// nz + 1 are zero), and the depth-integrated diagnostics.
-template <bool V>
-__device__ __forceinline__ void tracer_flux_point(const Dom &D, const GridDev &g, const Levels &L,
-                                                  const TracerArgs &a, int m, int n)
+// :101-253 at the u (V = false) and v (V = true) points of the interior:
+// the lateral advective, diffusive and GM fluxes of every level, the
+// vertical parts and coefficients of the isoneutral flux (levels 2..nz;
+// levels 1 and nz + 1 are zero), and the depth-integrated diagnostics.
+// Staged like k_columns: warps 0-1 the u points of CW columns of row n,
+// warps 2-3 the v points, warp 4 copies the twelve row segments of each
+// level (ffp, mu, ff on rows n and n+1; uu, vv and the four slopes on row n;
+// no slopes for level 1) into a 4-slot mbarrier ring.
+constexpr int FNROW = 12;
+constexpr int FSLOT_D = FNROW * RW;
+enum { G_FFP0, G_FFP1, G_MU0, G_MU1, G_FF0, G_FF1, G_UU, G_VV, G_SLRX, G_SLZX, G_SLRY, G_SLZY };
+
+size_t flux_smem(int nz)
 {
-    const long long i = X(m, n);
-    const long long P = L.plane;
+    return ((size_t)NS * FSLOT_D + 2 * (size_t)nz + 1) * sizeof(double) + 2 * NS * sizeof(uint64_t);
+}
+
+template <bool V>
+__device__ __forceinline__ bool tracer_flux_column(const Dom &D, const GridDev &g, const Levels &L,
+                                                   const TracerArgs &a, int m, int n, int cs, const double *ring,
+                                                   const double *sdz, uint64_t *full, uint64_t *empty, int lane)
+{
     const int nz = L.nz;
-    const long long e = V ? D.pitch : 1;                 // the far point: u m+1, v n+1
+    const long long P = L.plane;
+    const bool act = m <= D.nx_end;
+    const long long i = act ? X(m, n) : 0;
+    const bool wet = act && (V ? g.lcv[i] : g.lcu[i]) > 0.5f;
     double *flux = V ? a.flux_y : a.flux_x, *fz = V ? a.flux_zy : a.flux_zx;
     double *coef = V ? a.coef_zy : a.coef_zx, *sfgm = V ? a.sfgm_zy : a.sfgm_zx;
     double *ffo = V ? a.flux_f_y : a.flux_f_x;
-    const bool wet = (V ? g.lcv[i] : g.lcu[i]) > 0.5f;
-    if (!wet) {
-        for (int k = 0; k < nz; k++) flux[(long long)k * P + i] = 0.0;
-        for (int k = 0; k <= nz; k++) {
-            const long long o = (long long)k * P + i;
-            fz[o] = 0.0;
-            coef[o] = 0.0;
-            sfgm[o] = 0.0;
-        }
-        for (int c = 0; c < 4; c++) ffo[(long long)c * P + i] = 0.0;
-        return;
+    // the far point (u: m+1 on row n, v: m on row n+1) in the staged rows
+    const int rf_ffp = V ? G_FFP1 : G_FFP0, rf_mu = V ? G_MU1 : G_MU0, rf_ff = V ? G_FF1 : G_FF0;
+    const int cf = V ? cs : cs + 1;
+    const int r_slr = V ? G_SLRY : G_SLRX, r_slz = V ? G_SLZY : G_SLZX, r_vel = V ? G_VV : G_UU;
+    double hh = 0.0, dside = 0.0, dnorm = 0.0;
+    if (wet) {
+        hh = (V ? a.hhv : a.hhu)[i];
+        dside = V ? g.dxh[i] : g.dyh[i];
+        dnorm = V ? g.dyt[i] : g.dxt[i];
     }
-    const double hh = (V ? a.hhv : a.hhu)[i];
-    const double *slr = V ? a.slry : a.slrx, *slz = V ? a.slzy : a.slzx, *vel = V ? a.vv : a.uu;
-    const double dside = V ? g.dxh[i] : g.dyh[i], dnorm = V ? g.dyt[i] : g.dxt[i];
-    double f1d = 0.0, sg = 0.0;                          // flux_1d(k), sfgm(k) of the level in hand
+    if (act) {
+        fz[i] = 0.0;
+        coef[i] = 0.0;
+        sfgm[i] = 0.0;
+    }
+    double f1d = 0.0, sg = 0.0;
     double acc1 = 0.0, acc2 = 0.0, acc3 = 0.0, acc4 = 0.0;
-    fz[i] = 0.0;
-    coef[i] = 0.0;
-    sfgm[i] = 0.0;
-    for (int k = 1; k <= nz; k++) {
-        const long long o = (long long)(k - 1) * P + i;  // level k
-        double f1d1 = 0.0, sg1 = 0.0;                     // level k + 1
-        if (k < nz) {
-            const long long o1 = o + P;
-            const double dfdz = (a.ffp[o1] - a.ffp[o] + a.ffp[o1 + e] - a.ffp[o + e]) / 2.0;
-            const double dfdh = (a.ffp[o1 + e] - a.ffp[o1] + a.ffp[o + e] - a.ffp[o]) / 2.0;
-            const double mu1 = (a.mu[o1] + a.mu[o] + a.mu[o1 + e] + a.mu[o + e]) / 4.0 * a.factor_mu * dside / dnorm;
-            const double slope = a.ar * slr[o1] + a.az * slz[o1];
-            f1d1 = mu1 * (hh * dfdh * L.hzt[k] - slope * dfdz);
-            fz[o1] = mu1 * slope * dfdh;
-            coef[o1] = mu1 * (slope * slope) / hh / L.hzt[k];
-            sg1 = mu1 * (slr[o1] - slz[o1]) * a.alpha_gm;
-            sfgm[o1] = sg1;
+    bool ok = true;
+    for (int k = 1; k <= nz && ok; k++) {
+        const int sk = (k - 1) % NS, sn = k % NS;
+        ok = mbar_wait(&full[sk], (uint32_t)(((k - 1) / NS) & 1));
+        if (ok && k < nz) ok = mbar_wait(&full[sn], (uint32_t)((k / NS) & 1));
+        ok = __all_sync(0xffffffffu, ok);
+        if (!ok) break;
+        const double *st = ring + (size_t)sk * FSLOT_D, *nx = ring + (size_t)sn * FSLOT_D;
+        const long long o = (long long)(k - 1) * P + i;
+        if (wet) {
+            double f1d1 = 0.0, sg1 = 0.0;
+            if (k < nz) {
+                const long long o1 = o + P;
+                const double dfdz = (nx[G_FFP0 * RW + cs] - st[G_FFP0 * RW + cs] + nx[rf_ffp * RW + cf] -
+                                     st[rf_ffp * RW + cf]) / 2.0;
+                const double dfdh = (nx[rf_ffp * RW + cf] - nx[G_FFP0 * RW + cs] + st[rf_ffp * RW + cf] -
+                                     st[G_FFP0 * RW + cs]) / 2.0;
+                const double mu1 = (nx[G_MU0 * RW + cs] + st[G_MU0 * RW + cs] + nx[rf_mu * RW + cf] +
+                                    st[rf_mu * RW + cf]) / 4.0 * a.factor_mu * dside / dnorm;
+                const double slr = nx[r_slr * RW + cs], slz = nx[r_slz * RW + cs];
+                const double slope = a.ar * slr + a.az * slz;
+                f1d1 = mu1 * (hh * dfdh * sdz[nz + k] - slope * dfdz);
+                fz[o1] = mu1 * slope * dfdh;
+                coef[o1] = mu1 * (slope * slope) / hh / sdz[nz + k];
+                sg1 = mu1 * (slr - slz) * a.alpha_gm;
+                sfgm[o1] = sg1;
+            }
+            const double dzk = sdz[k - 1];
+            double fd;
+            if (k == 1) fd = f1d1 / sdz[nz + 1];
+            else if (k < nz) fd = (f1d + f1d1) / dzk / 2.0;
+            else fd = f1d / sdz[nz + k - 1];
+            const double s2 = st[G_FF0 * RW + cs] + st[rf_ff * RW + cf];
+            const double fa = -(st[r_vel * RW + cs] * hh * dside * s2 / 2.0);
+            const double vg = (sg1 - sg) / dzk;
+            const double fg = -(vg * s2 / 2.0);
+            flux[o] = fa + fd + fg;
+            acc1 = acc1 + dzk * (fa + fd + fg);
+            acc2 = acc2 + dzk * fa;
+            acc3 = acc3 + dzk * fd;
+            acc4 = acc4 + dzk * fg;
+            f1d = f1d1;
+            sg = sg1;
+        } else if (act) {
+            flux[o] = 0.0;
+            if (k < nz) {
+                fz[o + P] = 0.0;
+                coef[o + P] = 0.0;
+                sfgm[o + P] = 0.0;
+            }
         }
-        const double dzk = L.dz[k - 1];
-        double fd;
-        if (k == 1) fd = f1d1 / L.hzt[1];
-        else if (k < nz) fd = (f1d + f1d1) / dzk / 2.0;
-        else fd = f1d / L.hzt[k - 1];
-        const double s2 = a.ff[o] + a.ff[o + e];
-        const double fa = -(vel[o] * hh * dside * s2 / 2.0);
-        const double vg = (sg1 - sg) / dzk;
-        const double fg = -(vg * s2 / 2.0);
-        flux[o] = fa + fd + fg;
-        acc1 = acc1 + dzk * (fa + fd + fg);
-        acc2 = acc2 + dzk * fa;
-        acc3 = acc3 + dzk * fd;
-        acc4 = acc4 + dzk * fg;
-        f1d = f1d1;
-        sg = sg1;
+        __syncwarp();
+        if (lane == 0) mbar_arrive(&empty[sk]);
     }
-    const long long ot = (long long)nz * P + i;            // level nz + 1
-    fz[ot] = 0.0;
-    coef[ot] = 0.0;
-    sfgm[ot] = 0.0;
-    ffo[i] = acc1;
-    ffo[P + i] = acc2;
-    ffo[2 * P + i] = acc3;
-    ffo[3 * P + i] = acc4;
+    if (ok && act) {
+        const long long ot = (long long)nz * P + i;        // level nz + 1
+        fz[ot] = 0.0;
+        coef[ot] = 0.0;
+        sfgm[ot] = 0.0;
+        ffo[i] = acc1;
+        ffo[P + i] = acc2;
+        ffo[2 * P + i] = acc3;
+        ffo[3 * P + i] = acc4;
+    }
+    return ok;
 }
 
-__global__ void __launch_bounds__(TB) k_tracer_flux(Dom D, GridDev g, Levels L, TracerArgs a)
+__global__ void __launch_bounds__((NCW + 1) * 32) k_tracer_flux(Dom D, GridDev g, Levels L, TracerArgs a)
 {
-    const int m = D.nx_start + blockIdx.x * TB + threadIdx.x;
-    const int n = D.ny_start + blockIdx.y;
-    if (m > D.nx_end) return;
-    if (blockIdx.z == 0) tracer_flux_point<false>(D, g, L, a, m, n);
-    else tracer_flux_point<true>(D, g, L, a, m, n);
+    extern __shared__ __align__(128) double sm[];
+    const int nz = L.nz;
+    double *ring = sm;
+    double *sdz = ring + (size_t)NS * FSLOT_D;            // dz (nz), hzt (nz + 1)
+    uint64_t *full = reinterpret_cast<uint64_t *>(sdz + 2 * nz + 1);
+    uint64_t *empty = full + NS;
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const int m0 = D.nx_start + blockIdx.x * CW, n = D.ny_start + blockIdx.y;
+    for (int t = threadIdx.x; t < 2 * nz + 1; t += blockDim.x) sdz[t] = L.dz[t];
+    if (threadIdx.x == 0) {
+        for (int s = 0; s < NS; s++) {
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&full[s])), "r"(1) : "memory");
+            asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&empty[s])), "r"(NCW)
+                         : "memory");
+        }
+        asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    }
+    __syncthreads();
+    const int cm0 = m0 - D.bnd_x1 + D.xoff;
+    const int mlast = min(m0 + CW - 1, D.nx_end);
+    const int c0 = (cm0 - 1) & ~1;
+    const int cnt = ((mlast - D.bnd_x1 + D.xoff + 2 - c0) + 1) & ~1;
+    if (warp == NCW) {
+        if (lane != 0) return;
+        const long long P = L.plane;
+        const long long rb = (long long)(n - D.bnd_y1) * D.pitch + c0, pt = D.pitch;
+        const uint32_t seg = (uint32_t)cnt * 8u;
+        int armed = 0;
+        bool ok = true;
+        for (int j = 1; j <= nz; j++) {
+            const int s = (j - 1) % NS;
+            if (j > NS && !mbar_wait(&empty[s], (uint32_t)(((j - 1) / NS - 1) & 1))) {
+                ok = false;
+                break;
+            }
+            double *slot = ring + (size_t)s * FSLOT_D;
+            const long long lv = (long long)(j - 1) * P + rb;
+            mbar_expect(&full[s], seg * (uint32_t)(j == 1 ? G_SLRX : FNROW));
+            bulk_copy(slot + G_FFP0 * RW, a.ffp + lv, seg, &full[s]);
+            bulk_copy(slot + G_FFP1 * RW, a.ffp + lv + pt, seg, &full[s]);
+            bulk_copy(slot + G_MU0 * RW, a.mu + lv, seg, &full[s]);
+            bulk_copy(slot + G_MU1 * RW, a.mu + lv + pt, seg, &full[s]);
+            bulk_copy(slot + G_FF0 * RW, a.ff + lv, seg, &full[s]);
+            bulk_copy(slot + G_FF1 * RW, a.ff + lv + pt, seg, &full[s]);
+            bulk_copy(slot + G_UU * RW, a.uu + lv, seg, &full[s]);
+            bulk_copy(slot + G_VV * RW, a.vv + lv, seg, &full[s]);
+            if (j > 1) {
+                bulk_copy(slot + G_SLRX * RW, a.slrx + lv, seg, &full[s]);
+                bulk_copy(slot + G_SLZX * RW, a.slzx + lv, seg, &full[s]);
+                bulk_copy(slot + G_SLRY * RW, a.slry + lv, seg, &full[s]);
+                bulk_copy(slot + G_SLZY * RW, a.slzy + lv, seg, &full[s]);
+            }
+            armed = j;
+        }
+        if (!ok) atomicOr(a.flag, 1);
+        for (int j = max(1, armed - NS + 1); j <= armed; j++)
+            (void)mbar_wait(&full[(j - 1) % NS], (uint32_t)(((j - 1) / NS) & 1));
+        return;
+    }
+    const bool V = warp >= 2;
+    const int m = m0 + (warp & 1) * 32 + lane;
+    const int cs = (m - D.bnd_x1 + D.xoff) - c0;
+    const bool ok = V ? tracer_flux_column<true>(D, g, L, a, m, n, cs, ring, sdz, full, empty, lane)
+                      : tracer_flux_column<false>(D, g, L, a, m, n, cs, ring, sdz, full, empty, lane);
+    if (!ok && lane == 0) atomicOr(a.flag, 1);
 }
 
 // :279-403 at the T points of the interior (the vertical diffusion system,
@@ -961,22 +972,14 @@ bool wrap_inside(const Dom &d)
 int baroclinic_dynamics(const Dom &d, const GridDev &g, const Consts &c, const Levels &L,
                         const BaroclinicArgs &a, cudaStream_t s)
 {
-    if (L.nz < 2 || L.nz > MAX_NZ || wrap_inside(d)) return -1;
+    // the staged segments need an even row pitch and level stride
+    if (L.nz < 2 || L.nz > MAX_NZ || wrap_inside(d) || d.pitch % 2 || L.plane % 2 || !a.flag) return -1;
     const int nxi = d.nx_end - d.nx_start + 1, nyi = d.ny_end - d.ny_start + 1;
-    // the staged kernel's 16-byte segments need even row pitch and level stride
-    if (L.nz <= NZ_STAGED && d.pitch % 2 == 0 && L.plane % 2 == 0 && a.flag) {
-        const size_t smem = staged_smem(L.nz);
-        // per device: set on every call (the context's device is current)
-        if (cudaFuncSetAttribute(k_columns, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
-            return -1;
-        k_columns<<<dim3((nxi + CW - 1) / CW, nyi), (NCW + 1) * 32, smem, s>>>(d, g, L, a, c.ts);
-    } else {
-        const size_t smem = 2 * (size_t)L.nz * TB * sizeof(double);
-        if (cudaFuncSetAttribute(k_columns_direct, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) !=
-            cudaSuccess)
-            return -1;
-        k_columns_direct<<<dim3((nxi + TB - 1) / TB, nyi, 2), TB, smem, s>>>(d, g, L, a, c.ts);
-    }
+    const size_t smem = staged_smem(L.nz);
+    // per device: set on every call (the context's device is current)
+    if (cudaFuncSetAttribute(k_columns, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return -1;
+    k_columns<<<dim3((nxi + CW - 1) / CW, nyi), (NCW + 1) * 32, smem, s>>>(d, g, L, a, c.ts);
     const int count = d.nxa() * d.nya() - nxi * nyi;
     if (count > 0) k_border<<<dim3((count + 127) / 128, L.nz), 128, 0, s>>>(d, g, L, a, c.ts, count);
     return 0;
@@ -988,7 +991,10 @@ int tracer_tran_diff(const Dom &d, const GridDev &g, const Consts &c, const Leve
     // the staged solve's 16-byte segments need an even row pitch and level stride
     if (L.nz < 2 || L.nz > MAX_NZ || wrap_inside(d) || d.pitch % 2 || L.plane % 2 || !a.flag) return -1;
     const int nxi = d.nx_end - d.nx_start + 1, nyi = d.ny_end - d.ny_start + 1;
-    k_tracer_flux<<<dim3((nxi + TB - 1) / TB, nyi, 2), TB, 0, s>>>(d, g, L, a);
+    const size_t fsm = flux_smem(L.nz);
+    if (cudaFuncSetAttribute(k_tracer_flux, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm) != cudaSuccess)
+        return -1;
+    k_tracer_flux<<<dim3((nxi + CW - 1) / CW, nyi), (NCW + 1) * 32, fsm, s>>>(d, g, L, a);
     // the x-fluxes wrap in x, the y-fluxes in y (Function/tem_sal.f90:265-277)
     if (d.px) {
         k_cyclize_x3<<<dim3((d.nya() + 127) / 128, L.nz), 128, 0, s>>>(d, L.plane, a.flux_x);

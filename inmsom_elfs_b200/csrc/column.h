@@ -31,13 +31,12 @@ struct BaroclinicArgs {
     const double *hhu, *hhup, *hhun, *hhv, *hhvp, *hhvn, *hhh;
     // nz levels: uu, uup, vv, vvp after the step (every point of the arrays)
     double *uu_out, *uup_out, *vv_out, *vvp_out;
-    // set to nonzero when a bounded wait of the staged kernel gave up (its
+    // set to nonzero when a bounded wait of the column kernel gave up (its
     // outputs are then incomplete); must be zero before the launch
     int *flag;
 };
 
-// largest nz the solve supports (its sweep coefficients live in shared
-// memory; up to 96 levels the staged kernel runs, above it the direct one)
+// largest nz the solves support
 int max_levels();
 // true when a periodic wrap column/row lies inside the interior (the filter
 // would then need the wrapped value at an interior point; not supported)
