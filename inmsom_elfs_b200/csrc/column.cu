@@ -16,6 +16,12 @@
 //     filter on the one-point ring with the new velocity the periodic wrap
 //     brings there (zero without a wrap, as the reference's un = 0), a copy
 //     elsewhere.
+//
+// tracer_tran_diff runs the same way in three kernels: k_tracer_flux (the
+// lateral fluxes on the u and v points), the periodic wraps of those
+// fluxes, k_tracer_solve (the vertical diffusion system of every T column
+// with the filter) and k_tracer_border.  vertical_velocity, depth_ave and
+// the barotropic shift are one thread per column or point.
 #include "column.h"
 
 namespace inmsom {
@@ -23,7 +29,6 @@ namespace column {
 
 namespace {
 
-constexpr int TB = 64;          // threads (water columns) per block of k_tracer_flux
 constexpr int MAX_NZ = 200;     // levels (dz, hzt in shared memory)
 constexpr int BX = 32, BY = 8;
 

@@ -1,7 +1,10 @@
-// Per-water-column kernels of the 3-D velocity block: the implicit vertical
-// viscosity solve of baroclinic_dynamics (Function/vel_ssh.f90:794-1027,
-// tridiagonal sweep factor8 of Service/oc_algorithms.f90:494-524) and the
-// continuity integral of vertical_velocity (Function/vel_ssh.f90:1030-1076).
+// Per-water-column kernels of the 3-D part of the mode-split step: the
+// implicit vertical viscosity solve of baroclinic_dynamics
+// (Function/vel_ssh.f90:794-1027, tridiagonal sweep factor8 of
+// Service/oc_algorithms.f90:494-524), the continuity integral of
+// vertical_velocity (:1030-1076), one tracer's step tracer_tran_diff
+// (Function/tem_sal.f90:1-422), depth_ave (Function/depth.f90:223-254) and
+// the barotropic shift of Control/dyncall.f90:170-183, :215-229.
 //
 // 3-D fields are stacks of pitched 2-D levels: level k (0-based) of a field
 // starts plane * k doubles after level 0, and element (m, n) of a level sits
