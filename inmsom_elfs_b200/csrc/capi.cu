@@ -101,6 +101,12 @@ struct inmsom_ctx {
     // levels in one block (col3, colw, col2) and dz, hzt
     double *col = nullptr, *col_lev = nullptr;
     int col_nz = 0;
+    // inmsom_baroclinic_dynamics' copy pipeline: upload and download streams,
+    // events per row band, and the phase times of a pipelined call
+    cudaStream_t s_up = nullptr, s_dn = nullptr;
+    cudaEvent_t bev[4 * 8 + 4] = {};
+    float ph_ms[3] = {};
+    bool ph_direct = false;
     // inmsom_tracer_tran_diff: fields of trc_nz levels in one block and dz, hzt
     double *trc = nullptr, *trc_lev = nullptr;
     int trc_nz = 0;
@@ -407,6 +413,10 @@ int inmsom_gpu_finalize(inmsom_ctx *c)
     cudaFree(c->col_lev);
     cudaFree(c->trc);
     cudaFree(c->trc_lev);
+    for (auto &e : c->bev)
+        if (e) cudaEventDestroy(e);
+    if (c->s_up) cudaStreamDestroy(c->s_up);
+    if (c->s_dn) cudaStreamDestroy(c->s_dn);
     cudaFree(c->d_nbad);
     cudaFree(c->d_rows);
     cudaFree(c->d_out);
@@ -525,6 +535,7 @@ int inmsom_barotropic_dynamics(inmsom_ctx *c, double tau, int nstep, int ksw4, d
     for (int k = 0; k < NSTATE; k++) c->h_state[k] = hs[k];
     for (int k = 0; k < NSCR; k++) c->h_scr[k] = hc[k];
     c->ph_valid = false;
+    c->ph_direct = false;
     CK(cudaEventRecord(c->ph[0], c->stream));
 
     if (!resident || !c->state_on_device) {
@@ -591,6 +602,12 @@ int inmsom_gpu_last_phases(inmsom_ctx *c, float *upload_ms, float *compute_ms, f
 {
     if (!c || !upload_ms || !compute_ms || !download_ms) return set_err(INMSOM_EARG, "NULL argument");
     if (!c->ph_valid) return set_err(INMSOM_EARG, "no completed timed call");
+    if (c->ph_direct) {
+        *upload_ms = c->ph_ms[0];
+        *compute_ms = c->ph_ms[1];
+        *download_ms = c->ph_ms[2];
+        return INMSOM_OK;
+    }
     CK(cudaEventElapsedTime(upload_ms, c->ph[0], c->ph[1]));
     CK(cudaEventElapsedTime(compute_ms, c->ph[1], c->ph[2]));
     CK(cudaEventElapsedTime(download_ms, c->ph[2], c->ph[3]));
@@ -1088,8 +1105,6 @@ int col_alloc(inmsom_ctx *c, int nz)
     if (c->col && c->col_nz == nz) return INMSOM_OK;
     cudaFree(c->col);
     cudaFree(c->col_lev);
-    cudaFree(c->trc);
-    cudaFree(c->trc_lev);
     c->col = c->col_lev = nullptr;
     c->col_nz = 0;
     const size_t planes = (size_t)NC3 * nz + 2 * (size_t)(nz + 1) + NC2;
@@ -1116,6 +1131,29 @@ int d2h3(inmsom_ctx *c, double *host, const double *dev, int nlev)
     const size_t w = (size_t)c->dom.nxa() * sizeof(double);
     CK(cudaMemcpy2DAsync(host, w, dev + c->dom.xoff, (size_t)c->dom.pitch * sizeof(double), w,
                          (size_t)c->dom.nya() * nlev, cudaMemcpyDeviceToHost, c->stream));
+    return INMSOM_OK;
+}
+
+// rows r0..r1 and array columns x0..x1 (0-based from bnd_x1 / bnd_y1) of
+// nlev levels between a host array (bnd_x1:bnd_x2, bnd_y1:bnd_y2, nlev) and
+// its pitched device copy, as one 3-D copy
+int box3(inmsom_ctx *c, double *dev, double *host, int nlev, int r0, int r1, int x0, int x1, bool up,
+         cudaStream_t s)
+{
+    if (r1 < r0 || x1 < x0) return INMSOM_OK;
+    const Dom &d = c->dom;
+    cudaMemcpy3DParms p = {};
+    cudaPitchedPtr hp = make_cudaPitchedPtr(host, (size_t)d.nxa() * sizeof(double), (size_t)d.nxa(), (size_t)d.nya());
+    cudaPitchedPtr dp = make_cudaPitchedPtr(dev + d.xoff, (size_t)d.pitch * sizeof(double), (size_t)d.nxa(),
+                                            (size_t)d.nya());
+    const cudaPos pos = make_cudaPos((size_t)x0 * sizeof(double), (size_t)r0, 0);
+    p.srcPtr = up ? hp : dp;
+    p.dstPtr = up ? dp : hp;
+    p.srcPos = pos;
+    p.dstPos = pos;
+    p.extent = make_cudaExtent((size_t)(x1 - x0 + 1) * sizeof(double), (size_t)(r1 - r0 + 1), (size_t)nlev);
+    p.kind = up ? cudaMemcpyHostToDevice : cudaMemcpyDeviceToHost;
+    CK(cudaMemcpy3DAsync(&p, s));
     return INMSOM_OK;
 }
 
@@ -1156,16 +1194,12 @@ int inmsom_baroclinic_dynamics(inmsom_ctx *c, int nz, const double *dz, const do
     const Dom &d = c->dom;
     if (column::wrap_inside(d)) return set_err(INMSOM_EUNSUPPORTED, "inmsom_baroclinic_dynamics: a periodic wrap column/row lies in the interior");
     CKR(col_alloc(c, nz));
+    if (!c->s_up) CK(cudaStreamCreateWithFlags(&c->s_up, cudaStreamNonBlocking));
+    if (!c->s_dn) CK(cudaStreamCreateWithFlags(&c->s_dn, cudaStreamNonBlocking));
+    for (auto &e : c->bev)
+        if (!e) CK(cudaEventCreate(&e));
     c->ph_valid = false;
-    CK(cudaEventRecord(c->ph[0], c->stream));
-    for (int k = 0; k < 4; k++) CKR(h2d3(c, col3(c, C3_UU + k), io[k], nz));
-    for (int k = 0; k < 4; k++) CKR(h2d3(c, col3(c, C3_RHSX + k), in3[k], nz));
-    CKR(h2d3(c, colw(c, 0), ww, nz + 1));
-    CKR(h2d3(c, colw(c, 1), nu, nz + 1));
-    for (int k = 0; k < NC2; k++) CKR(h2d(c, col2(c, k), in2[k]));
-    CK(cudaMemcpyAsync(c->col_lev, dz, nz * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->col_lev + nz, hzt, (nz + 1) * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaEventRecord(c->ph[1], c->stream));
+    c->ph_direct = false;
     column::BaroclinicArgs a;
     a.tau = tau;
     a.uu = col3(c, C3_UU); a.uup = col3(c, C3_UUP); a.vv = col3(c, C3_VV); a.vvp = col3(c, C3_VVP);
@@ -1178,18 +1212,82 @@ int inmsom_baroclinic_dynamics(inmsom_ctx *c, int nz, const double *dz, const do
     a.hhv = col2(c, 10); a.hhvp = col2(c, 11); a.hhvn = col2(c, 12); a.hhh = col2(c, 13);
     a.uu_out = col3(c, C3_UUO); a.uup_out = col3(c, C3_UUPO); a.vv_out = col3(c, C3_VVO); a.vvp_out = col3(c, C3_VVPO);
     a.flag = reinterpret_cast<int *>(c->col_lev + 2 * nz + 1);
+    const column::Levels L = col_levels(c);
+    const GridDev gd = c->gdev();
+
+    // Row bands, pipelined over three streams: band b's rows are uploaded on
+    // s_up while band b-1 is solved on the context's stream and band b-2's
+    // results go back on s_dn.  Each row is uploaded once: band b brings the
+    // rows from just after band b-1's last upload to one past its own last
+    // interior row (the solves read rows n-1..n+1); the last band brings the
+    // rest of the arrays.  The border (outside the interior) is filtered and
+    // downloaded after the last band.
+    cudaEvent_t *ev_up = c->bev, *ev_k0 = c->bev + 8, *ev_k1 = c->bev + 16, *ev_bd = c->bev + 32;
+    const int nyi = d.ny_end - d.ny_start + 1, nb = std::min(8, nyi);
+    const int nxa = d.nxa(), nya = d.nya();
+    const int ix0 = d.nx_start - d.bnd_x1, ix1 = d.nx_end - d.bnd_x1;      // interior columns, 0-based
+    // the nz-level inputs in the order of the block's fields C3_UU .. C3_RHSYT
+    double *const up3[8] = {uu, uup, vv, vvp, (double *)RHSx, (double *)RHSy, (double *)RHSx_tran,
+                            (double *)RHSy_tran};
+    CK(cudaEventRecord(c->ph[0], c->stream));
+    CK(cudaStreamWaitEvent(c->s_up, c->ph[0], 0));
     CK(cudaMemsetAsync(a.flag, 0, sizeof(int), c->stream));
-    if (column::baroclinic_dynamics(d, c->gdev(), c->c, col_levels(c), a, c->stream))
-        return set_err(INMSOM_ECUDA, "inmsom_baroclinic_dynamics: launch failed: %s",
-                       cudaGetErrorString(cudaGetLastError()));
+    for (int k = 0; k < NC2; k++)
+        CK(cudaMemcpy2DAsync(col2(c, k) + d.xoff, (size_t)d.pitch * sizeof(double), in2[k], nxa * sizeof(double),
+                             nxa * sizeof(double), nya, cudaMemcpyHostToDevice, c->s_up));
+    CK(cudaMemcpyAsync(c->col_lev, dz, nz * sizeof(double), cudaMemcpyHostToDevice, c->s_up));
+    CK(cudaMemcpyAsync(c->col_lev + nz, hzt, (nz + 1) * sizeof(double), cudaMemcpyHostToDevice, c->s_up));
+    int up_next = 0;                                                   // next array row (0-based) to upload
+    for (int b = 0; b < nb; b++) {
+        const int n0 = d.ny_start + (int)((long long)nyi * b / nb);
+        const int n1 = d.ny_start + (int)((long long)nyi * (b + 1) / nb) - 1;
+        const int up_last = b == nb - 1 ? nya - 1 : n1 + 1 - d.bnd_y1;
+        for (int k = 0; k < 8; k++)
+            CKR(box3(c, col3(c, C3_UU + k), up3[k], nz, up_next, up_last, 0, nxa - 1, true, c->s_up));
+        CKR(box3(c, colw(c, 0), (double *)ww, nz + 1, up_next, up_last, 0, nxa - 1, true, c->s_up));
+        CKR(box3(c, colw(c, 1), (double *)nu, nz + 1, up_next, up_last, 0, nxa - 1, true, c->s_up));
+        up_next = up_last + 1;
+        CK(cudaEventRecord(ev_up[b], c->s_up));
+        CK(cudaStreamWaitEvent(c->stream, ev_up[b], 0));
+        CK(cudaEventRecord(ev_k0[b], c->stream));
+        if (column::baroclinic_rows(d, gd, c->c, L, a, n0, n1, c->stream))
+            return set_err(INMSOM_ECUDA, "inmsom_baroclinic_dynamics: launch failed: %s",
+                           cudaGetErrorString(cudaGetLastError()));
+        CK(cudaEventRecord(ev_k1[b], c->stream));
+        CK(cudaStreamWaitEvent(c->s_dn, ev_k1[b], 0));
+        for (int k = 0; k < 4; k++)
+            CKR(box3(c, col3(c, C3_UUO + k), io[k], nz, n0 - d.bnd_y1, n1 - d.bnd_y1, ix0, ix1, false, c->s_dn));
+    }
+    CK(cudaEventRecord(ev_bd[0], c->stream));
+    column::baroclinic_border(d, gd, c->c, L, a, c->stream);
     CK(cudaGetLastError());
-    CK(cudaEventRecord(c->ph[2], c->stream));
+    CK(cudaEventRecord(ev_bd[1], c->stream));
+    CK(cudaStreamWaitEvent(c->s_dn, ev_bd[1], 0));
     int flag = 0;
-    CK(cudaMemcpyAsync(&flag, a.flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    for (int k = 0; k < 4; k++) CKR(d2h3(c, io[k], col3(c, C3_UUO + k), nz));
-    CK(cudaEventRecord(c->ph[3], c->stream));
+    CK(cudaMemcpyAsync(&flag, a.flag, sizeof(int), cudaMemcpyDeviceToHost, c->s_dn));
+    const int iy0 = d.ny_start - d.bnd_y1, iy1 = d.ny_end - d.bnd_y1;
+    for (int k = 0; k < 4; k++) {
+        double *dev = col3(c, C3_UUO + k);
+        CKR(box3(c, dev, io[k], nz, 0, iy0 - 1, 0, nxa - 1, false, c->s_dn));             // rows above
+        CKR(box3(c, dev, io[k], nz, iy1 + 1, nya - 1, 0, nxa - 1, false, c->s_dn));       // rows below
+        CKR(box3(c, dev, io[k], nz, iy0, iy1, 0, ix0 - 1, false, c->s_dn));              // columns left
+        CKR(box3(c, dev, io[k], nz, iy0, iy1, ix1 + 1, nxa - 1, false, c->s_dn));        // columns right
+    }
+    CK(cudaEventRecord(c->ph[3], c->s_dn));
+    CK(cudaStreamWaitEvent(c->stream, c->ph[3], 0));
     CKR(sync_stream(c));
     if (flag) return set_err(INMSOM_ETIMEOUT, "inmsom_baroclinic_dynamics: a bounded wait of the column kernel gave up");
+    // phases: the uploads, the kernels' own time, and from the last kernel to the end
+    float t = 0.0f, sum = 0.0f;
+    CK(cudaEventElapsedTime(&c->ph_ms[0], c->ph[0], ev_up[nb - 1]));
+    for (int b = 0; b < nb; b++) {
+        CK(cudaEventElapsedTime(&t, ev_k0[b], ev_k1[b]));
+        sum += t;
+    }
+    CK(cudaEventElapsedTime(&t, ev_bd[0], ev_bd[1]));
+    c->ph_ms[1] = sum + t;
+    CK(cudaEventElapsedTime(&c->ph_ms[2], ev_bd[1], c->ph[3]));
+    c->ph_direct = true;
     c->ph_valid = true;
     return INMSOM_OK;
 }
@@ -1265,6 +1363,7 @@ int inmsom_tracer_tran_diff(inmsom_ctx *c, int nz, const double *dz, const doubl
         }
     CKR(trc_alloc(c, nz));
     c->ph_valid = false;
+    c->ph_direct = false;
     CK(cudaEventRecord(c->ph[0], c->stream));
     const int f3[6] = {T_FF, T_FFP, T_UU, T_VV, T_MU, T_SRC};
     const int f31[6] = {T_WW, T_NU, T_SLRX, T_SLRY, T_SLZX, T_SLZY};
@@ -1324,6 +1423,7 @@ int inmsom_vertical_velocity(inmsom_ctx *c, int nz, const double *dz, const doub
         return set_err(INMSOM_EARG, "inmsom_vertical_velocity: NULL argument");
     CKR(col_alloc(c, nz));
     c->ph_valid = false;
+    c->ph_direct = false;
     CK(cudaEventRecord(c->ph[0], c->stream));
     CKR(h2d3(c, col3(c, C3_UU), u, nz));
     CKR(h2d3(c, col3(c, C3_VV), v, nz));

@@ -295,7 +295,8 @@ __device__ __forceinline__ bool staged_column(const Dom &D, const GridDev &g, co
     return ok;
 }
 
-__global__ void __launch_bounds__((NCW + 1) * 32, 4) k_columns(Dom D, GridDev g, Levels L, BaroclinicArgs a, double ts)
+__global__ void __launch_bounds__((NCW + 1) * 32, 4) k_columns(Dom D, GridDev g, Levels L, BaroclinicArgs a, double ts,
+                                                               int row0)
 {
     extern __shared__ __align__(128) double sm[];
     const int nz = L.nz;
@@ -304,7 +305,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32, 4) k_columns(Dom D, GridDev g,
     uint64_t *full = reinterpret_cast<uint64_t *>(sdz + 2 * nz + 1);
     uint64_t *empty = full + NS;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = D.nx_start + blockIdx.x * CW, n = D.ny_start + blockIdx.y;
+    const int m0 = D.nx_start + blockIdx.x * CW, n = row0 + blockIdx.y;
 
     for (int t = threadIdx.x; t < 2 * nz + 1; t += blockDim.x) sdz[t] = L.dz[t];
     if (threadIdx.x == 0) {
@@ -974,20 +975,35 @@ bool wrap_inside(const Dom &d)
            (d.py && (in(d.nnn - 1, d.ny_start, d.ny_end) || in(d.nn + 1, d.ny_start, d.ny_end)));
 }
 
-int baroclinic_dynamics(const Dom &d, const GridDev &g, const Consts &c, const Levels &L,
-                        const BaroclinicArgs &a, cudaStream_t s)
+int baroclinic_rows(const Dom &d, const GridDev &g, const Consts &c, const Levels &L, const BaroclinicArgs &a,
+                    int n0, int n1, cudaStream_t s)
 {
     // the staged segments need an even row pitch and level stride
     if (L.nz < 2 || L.nz > MAX_NZ || wrap_inside(d) || d.pitch % 2 || L.plane % 2 || !a.flag) return -1;
-    const int nxi = d.nx_end - d.nx_start + 1, nyi = d.ny_end - d.ny_start + 1;
+    if (n0 < d.ny_start || n1 > d.ny_end || n0 > n1) return -1;
+    const int nxi = d.nx_end - d.nx_start + 1;
     const size_t smem = staged_smem(L.nz);
     // per device: set on every call (the context's device is current)
     if (cudaFuncSetAttribute(k_columns, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return -1;
-    k_columns<<<dim3((nxi + CW - 1) / CW, nyi), (NCW + 1) * 32, smem, s>>>(d, g, L, a, c.ts);
+    k_columns<<<dim3((nxi + CW - 1) / CW, n1 - n0 + 1), (NCW + 1) * 32, smem, s>>>(d, g, L, a, c.ts, n0);
+    return 0;
+}
+
+int baroclinic_border(const Dom &d, const GridDev &g, const Consts &c, const Levels &L, const BaroclinicArgs &a,
+                      cudaStream_t s)
+{
+    const int nxi = d.nx_end - d.nx_start + 1, nyi = d.ny_end - d.ny_start + 1;
     const int count = d.nxa() * d.nya() - nxi * nyi;
     if (count > 0) k_border<<<dim3((count + 127) / 128, L.nz), 128, 0, s>>>(d, g, L, a, c.ts, count);
     return 0;
+}
+
+int baroclinic_dynamics(const Dom &d, const GridDev &g, const Consts &c, const Levels &L,
+                        const BaroclinicArgs &a, cudaStream_t s)
+{
+    if (baroclinic_rows(d, g, c, L, a, d.ny_start, d.ny_end, s)) return -1;
+    return baroclinic_border(d, g, c, L, a, s);
 }
 
 int tracer_tran_diff(const Dom &d, const GridDev &g, const Consts &c, const Levels &L, const TracerArgs &a,

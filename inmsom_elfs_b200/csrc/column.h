@@ -49,6 +49,14 @@ bool wrap_inside(const Dom &d);
 // out of range or a periodic wrap column/row lies inside the interior.
 int baroclinic_dynamics(const Dom &d, const GridDev &g, const Consts &c, const Levels &L,
                         const BaroclinicArgs &a, cudaStream_t s);
+// The same in parts: the column solves of interior rows n0..n1 (they read
+// the inputs of rows n0-1..n1+1 and write the outputs of those interior
+// rows only), then, after every interior row, the border (the ring's filter
+// with the wrapped new velocity, copies elsewhere).
+int baroclinic_rows(const Dom &d, const GridDev &g, const Consts &c, const Levels &L, const BaroclinicArgs &a,
+                    int n0, int n1, cudaStream_t s);
+int baroclinic_border(const Dom &d, const GridDev &g, const Consts &c, const Levels &L, const BaroclinicArgs &a,
+                      cudaStream_t s);
 
 // Function/vel_ssh.f90:1030-1076: w (nz + 1 levels) in place.
 int vertical_velocity(const Dom &d, const GridDev &g, const Consts &c, const Levels &L, const double *u,

@@ -234,3 +234,27 @@ def test_tracer_rejects_bad_arguments(gpu, ora):
             s.tracer_tran_diff(dz, hzt, TAU, f["ff"].copy(order="F"), f["ffp"].copy(order="F"),
                                np.zeros((*b.bounds.shape, 4), order="F"), np.zeros((*b.bounds.shape, 4), order="F"), f)
     assert e.value.code == 2
+
+
+@pytest.mark.gpu
+def test_tracer_and_baroclinic_share_a_context(gpu, ora):
+    """Both blocks on one context, with the level count changing in between:
+    each keeps its own device block and stays bit-exact."""
+    from test_baroclinic import _run_oracle as baro_oracle
+    from test_baroclinic import inputs as baro_inputs
+    b = coastline(ora, nx=60, ny=50)
+    with gpu.BarotropicSolver(b, resident=False) as s:
+        for nz in (NZ, 7, NZ):
+            dz, hzt, f = inputs(b, nz=nz, seed=nz)
+            want = _oracle(ora, b, dz, hzt, f)
+            ff, ffp = f["ff"].copy(order="F"), f["ffp"].copy(order="F")
+            fx, fy = np.zeros((*b.bounds.shape, 4), order="F"), np.zeros((*b.bounds.shape, 4), order="F")
+            got = s.tracer_tran_diff(dz, hzt, TAU, ff, ffp, fx, fy, f)
+            for g_, w_ in zip(got, want):
+                assert np.array_equal(g_, w_)
+            dzb, hztb, fb = baro_inputs(b, nz=nz + 3, seed=nz)
+            wb = baro_oracle(ora, b, dzb, hztb, fb)
+            st = [fb[k].copy(order="F") for k in ("uu", "uup", "vv", "vvp")]
+            s.baroclinic_dynamics(dzb, hztb, TAU, *st, **{k: fb[k] for k in s.BAROCLINIC_FIELDS})
+            for g_, w_ in zip(st, wb):
+                assert np.array_equal(g_, w_)
