@@ -67,6 +67,8 @@ namespace inmsom {
 // Sets the message of inmsom_gpu_last_error() for entry points defined in
 // other source files of the library.
 int record_error(int code, const char *msg) { return set_err(code, "%s", msg); }
+// Service/input_output_data.f90:4-115 fulfname (csrc/dstd.cu)
+std::string full_file_name(const char *path, const char *fname);
 }  // namespace inmsom
 
 namespace {
@@ -1589,10 +1591,7 @@ int inmsom_write_checkpoint(inmsom_ctx *c, const char *path, const inmsom_ctl_ax
             CKR(inmsom_wdstd8(path, f.f8, t + 1, fld, lu, nx, ny, 1, i0 - f.dx, i1, j0 - f.dy, j1, 1, 1));
             CKR(inmsom_wdstd(path, f.f4, t + 1, f4.data(), lu, nx, ny, 1, i0 - f.dx, i1, j0 - f.dy, j1, 1, 1));
         }
-        std::string name = path;
-        while (!name.empty() && name.back() == ' ') name.pop_back();
-        if (!name.empty() && name.back() != '/') name += '/';
-        name += f.ctl;
+        const std::string name = inmsom::full_file_name(path, f.ctl);   // fulfname, as the reference
         CKR(inmsom_ctl_file_write(name.c_str(), -1.0e32f, nx_glob + f.dx, ny_glob + f.dy, 1, 2, ax->xgr_type,
                                   f.dx ? ax->xu : ax->xt, ax->dxst, ax->ygr_type, f.dy ? ax->yv : ax->yt, ax->dyst,
                                   0, &zero, 1.0, ax->calendar, ax->year, ax->month, ax->day, ax->hour, ax->minute,

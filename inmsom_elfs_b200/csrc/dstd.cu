@@ -269,6 +269,15 @@ std::string extname(const std::string &name, const char *ext)
 
 }  // namespace
 
+namespace inmsom {
+// fulfname for callers elsewhere in the library (empty on a missing file name)
+std::string full_file_name(const char *path, const char *fname)
+{
+    std::string out;
+    return fulfname(out, path, fname) ? out : std::string();
+}
+}  // namespace inmsom
+
 extern "C" {
 
 int inmsom_wdstd8(const char *path, const char *fname, int nfield, double *field, const float *lu, int nx, int ny,

@@ -276,7 +276,8 @@ def _gpu_run(gpu, basin, dz, hzt, f, tau=TAU):
 @pytest.mark.parametrize("case,nz", [("coastline", NZ), ("coastline", 2), ("coastline", 57), ("coastline", 96),
                                      ("coastline", 97), ("coastline", 150), ("periodic_xy", NZ), ("channel_x", 7)])
 def test_baroclinic_bitexact(gpu, ora, case, nz):
-    """Up to 96 levels the staged kernel runs, above it the direct one."""
+    """From the smallest nz to one whose column sweep far exceeds a ring
+slot's worth of levels; the drop-in call splits the rows into bands."""
     b = {"coastline": lambda: coastline(ora), "periodic_xy": lambda: periodic(ora),
          "channel_x": lambda: periodic(ora, px=1, py=0)}[case]()
     dz, hzt, f = inputs(b, nz=nz, seed=nz)
