@@ -472,7 +472,7 @@ __global__ void k_vertical_velocity(Dom D, GridDev g, Levels L, double rho, int 
 
 // ---- Function/tem_sal.f90: one tracer's step ---------------------------
 
-// :101-253 at the u (V = false) and v (V = true) points of the interior:
+// :108-251 at the u (V = false) and v (V = true) points of the interior:
 // the lateral advective, diffusive and GM fluxes of every level, the
 // vertical parts and coefficients of the isoneutral flux (levels 2..nz;
 // levels 1 and nz + 1 are zero), and the depth-integrated diagnostics.
@@ -655,8 +655,8 @@ __global__ void __launch_bounds__((NCW + 1) * 32) k_tracer_flux(Dom D, GridDev g
     if (!ok && lane == 0) atomicOr(a.flag, 1);
 }
 
-// :279-403 at the T points of the interior (the vertical diffusion system,
-// factor8), then the filter of :415-429 there.  Staged like k_columns: a CTA
+// :277-392 at the T points of the interior (the vertical diffusion system,
+// factor8), then the filter of :405-419 there.  Staged like k_columns: a CTA
 // owns CW columns of row n (warps 0-1) and a copy warp (2) brings, for
 // every level j, the nineteen row segments the equations of levels j - 1
 // and j read into a 3-slot mbarrier ring; stage nz + 1 holds nu only.  The
@@ -859,7 +859,7 @@ __global__ void __launch_bounds__(3 * 32) k_tracer_solve(Dom D, GridDev g, Level
     if (ocean) back_filter_inplace(nz, P, i, ym, ts, a.ff, a.ffp, a.ff_out, a.ffp_out);
 }
 
-// :415-429 outside the interior (the ring with the wrapped new tracer,
+// :405-419 outside the interior (the ring with the wrapped new tracer,
 // copies elsewhere), one level per grid row
 __global__ void k_tracer_border(Dom D, GridDev g, Levels L, TracerArgs a, double ts, int count)
 {
@@ -1016,7 +1016,7 @@ int tracer_tran_diff(const Dom &d, const GridDev &g, const Consts &c, const Leve
     if (cudaFuncSetAttribute(k_tracer_flux, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm) != cudaSuccess)
         return -1;
     k_tracer_flux<<<dim3((nxi + CW - 1) / CW, nyi), (NCW + 1) * 32, fsm, s>>>(d, g, L, a);
-    // the x-fluxes wrap in x, the y-fluxes in y (Function/tem_sal.f90:265-277)
+    // the x-fluxes wrap in x, the y-fluxes in y (Function/tem_sal.f90:264-274)
     if (d.px) {
         k_cyclize_x3<<<dim3((d.nya() + 127) / 128, L.nz), 128, 0, s>>>(d, L.plane, a.flux_x);
         for (double *f : {a.flux_zx, a.coef_zx, a.sfgm_zx})

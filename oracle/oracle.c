@@ -870,10 +870,10 @@ void ora_shift_barotropic(const ora_grid *g, int nz, double *uu, double *vv, con
 
 /* Function/tem_sal.f90:1-422 tracer_tran_diff: one tracer's step —
  * lateral advection, isoneutral diffusion and Gent-McWilliams fluxes on u
- * and v points (:101-253), the periodic wrap of those fluxes (:255-277),
+ * and v points (:108-251), the periodic wrap of those fluxes (:253-275),
  * the implicit vertical diffusion per water column with vertical
- * advection and the fluxes' vertical parts (:279-403, factor8), and the
- * Robert-Asselin filter (:415-429).  The lateral-boundary arguments of the
+ * advection and the fluxes' vertical parts (:277-392, factor8), and the
+ * Robert-Asselin filter (:405-419).  The lateral-boundary arguments of the
  * reference (ksw_lbc, numlbc, lqpx, lqpy, ind_lbc, flbc) are not read by
  * its body and are not taken here.  ig_top/ig_bot must be 1 or 2 at the
  * ocean points (other values leave the reference's b(1)/eta(1) unset). */
@@ -897,7 +897,7 @@ void ora_tracer_tran_diff(const ora_grid *g, int nz, const double *dz, const dou
     memset(flux_f_x, 0, 4 * nt * sizeof(double));
     memset(flux_f_y, 0, 4 * nt * sizeof(double));
 #define F4(a, m, n, c) (a)[I(m, n) + (size_t)((c) - 1) * nt]
-    /* :101-253 */
+    /* :108-251 */
 #pragma omp parallel for
     for (int n = B->ny_start; n <= B->ny_end; n++) {
         double *flux_1d = malloc((size_t)(nz + 2) * sizeof(double)), *mu_1d = malloc((size_t)(nz + 2) * sizeof(double));
@@ -949,7 +949,7 @@ void ora_tracer_tran_diff(const ora_grid *g, int nz, const double *dz, const dou
         free(flux_1d);
         free(mu_1d);
     }
-    /* :255-277: x-fluxes wrap in x, y-fluxes in y */
+    /* :253-275: x-fluxes wrap in x, y-fluxes in y */
     for (int k = 1; k <= nz + 1; k++) {
         const size_t o = (size_t)(k - 1) * nt;
         if (B->periodicity_x) {
@@ -965,7 +965,7 @@ void ora_tracer_tran_diff(const ora_grid *g, int nz, const double *dz, const dou
             ora_cyclize8_y(B, sfgm_zy + o);
         }
     }
-    /* :279-403 */
+    /* :277-392 */
 #pragma omp parallel for
     for (int n = B->ny_start; n <= B->ny_end; n++) {
         double *a = malloc(6 * (size_t)nz * sizeof(double));
@@ -1044,12 +1044,12 @@ void ora_tracer_tran_diff(const ora_grid *g, int nz, const double *dz, const dou
         free(a);
         free(rksi);
     }
-    /* :405-413 */
+    /* :394-402 */
     for (int k = 1; k <= nz; k++) {
         if (B->periodicity_x) ora_cyclize8_x(B, fn + (size_t)(k - 1) * nt);
         if (B->periodicity_y) ora_cyclize8_y(B, fn + (size_t)(k - 1) * nt);
     }
-    /* :415-429 */
+    /* :405-419 */
     const double ts = g->time_smooth;
 #pragma omp parallel for
     for (int n = B->ny_start - 1; n <= B->ny_end + 1; n++)
