@@ -192,3 +192,19 @@ def test_checkpoint_restart_continues_bit_for_bit(gpu, tmp_path):
         s.sync_to_host(0x1)
     for k in cont:
         assert np.array_equal(fresh.state[k], cont[k]), k
+
+
+def test_format_error_codes(tmp_path):
+    c = CTL_CASES[0]
+    with pytest.raises(InmsomError) as e:
+        dstd.ctl_file_write(str(tmp_path / "a.dat"), -1.0e32, 4, 4, 1, 1, 0, [0.0], 1.0, 0, [0.0], 1.0, 0, [0.0], 1.0,
+                            1, 2000, 13, 1, 0, 0, 86400.0, c["title"], "ssh")
+    assert e.value.code == 2
+    f, lu = _case(7, nx=4, ny=3, nz=2)
+    (tmp_path / "short.dat").write_bytes(b"\0" * 40)          # less than one 96-byte record
+    with pytest.raises(InmsomError) as e:
+        dstd.rdstd8(str(tmp_path), "short.dat", 1, f.copy(order="F"), lu)
+    assert e.value.code == 6
+    with pytest.raises(InmsomError) as e:
+        dstd.wdstd8(str(tmp_path / "no" / "such" / "dir"), "x.dat", 1, f.copy(order="F"), lu)
+    assert e.value.code == 6
