@@ -247,6 +247,27 @@ def test_uncoupled_levels_are_eta_over_bp(ora):
     assert np.array_equal(sh(uu)[~m], sh(f["uu"])[~m])
 
 
+def test_vertical_viscosity_conserves_column_momentum(ora):
+    """With only the vertical viscosity acting (no advection, Coriolis, drag,
+    stress or RHS), each water column keeps sum_k dz*bp*un = sum_k dz*bp0*uup:
+    the implicit diffusion moves momentum between levels only."""
+    b = coastline(ora, nx=50, ny=40)
+    b.rlh_s = np.zeros(b.bounds.shape, order="F")
+    dz, hzt, f = inputs(b, nz=15, seed=4)
+    for k in ("ww", "rdis", "tx_surf", "ty_surf", "tx_bot", "ty_bot", "pgrx", "pgry", "rhsx", "rhsy",
+              "rhsx_tran", "rhsy_tran"):
+        f[k] = np.zeros_like(f[k])
+    uu, uup, vv, vvp = _run_oracle(ora, b, dz, hzt, f)
+    sh = _views(b.bounds)
+    for comp, new, prev, hn, hp, mask in (("u", uu, "uup", "hhun", "hhup", "lcu"), ("v", vv, "vvp", "hhvn", "hhvp", "lcv")):
+        m = sh(b.masks[mask]) > 0.5
+        lhs = np.sum(dz * sh(new), axis=2) * sh(f[hn])
+        rhs = np.sum(dz * sh(f[prev]), axis=2) * sh(f[hp])
+        scale = np.sum(dz * np.abs(sh(f[prev])), axis=2) * sh(f[hp])
+        assert np.max(np.abs(lhs - rhs)[m] / scale[m]) < 1e-12, comp
+        assert not np.allclose(sh(new)[m], sh(f[prev])[m])
+
+
 @pytest.mark.parametrize("case", ["coastline", "periodic_xy"])
 def test_vertical_velocity_oracle_matches_numpy(ora, case):
     b = coastline(ora) if case == "coastline" else periodic(ora)

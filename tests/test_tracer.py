@@ -203,6 +203,29 @@ def test_uniform_tracer_without_fluxes_stays_uniform(ora):
     assert np.all(np.abs(fx) < 1e-9) and np.all(np.abs(fy) < 1e-9)
 
 
+def test_tracer_content_is_conserved(ora):
+    """Closed basin, no source, zero-flux surface and bottom (type 2): the
+    step only moves the tracer, sum over ocean columns and levels of
+    dz*hhqn*dx*dy*ff(new) equals that of dz*hhqp*dx*dy*ffp (the lateral
+    fluxes cancel between neighbours, the vertical parts and the diffusion
+    telescope in the column)."""
+    b = coastline(ora)
+    dz, hzt, f = inputs(b, nz=12, seed=5)
+    f["src"] = np.zeros_like(f["src"])
+    f["ig_top"][:] = 2
+    f["ig_bot"][:] = 2
+    f["ff_top"] = np.zeros_like(f["ff_top"])
+    f["ff_bot"] = np.zeros_like(f["ff_bot"])
+    ff, ffp, _, _ = _oracle(ora, b, dz, hzt, f)
+    sh = _views(b.bounds)
+    m = (sh(b.masks["lu"]) > 0.5)[..., None]
+    area = (sh(b.metrics["dx"]) * sh(b.metrics["dy"]))[..., None]
+    new = np.sum(np.where(m, dz * sh(f["hhqn"])[..., None] * area * sh(ff), 0.0))
+    old = np.sum(np.where(m, dz * sh(f["hhqp"])[..., None] * area * sh(f["ffp"]), 0.0))
+    assert abs(new - old) / abs(old) < 1e-12
+    assert not np.allclose(sh(ff)[m[..., 0]], sh(f["ffp"])[m[..., 0]])   # but it does move
+
+
 # ---- GPU ------------------------------------------------------------------
 
 @pytest.mark.gpu
