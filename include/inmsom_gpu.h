@@ -162,7 +162,7 @@ int inmsom_r_diss(inmsom_ctx *ctx, double r_fric, double *r_diss);
 int inmsom_wind_forcing(inmsom_ctx *ctx, const double *taux, const double *tauy,
                         double *RHSx2d, double *RHSy2d);
 
-/* After barotropic_dynamics, Control/dyncall.f90:186-201 (the 2-D part of
+/* After barotropic_dynamics, Control/dyncall.f90:188-201 (the 2-D part of
  * the mode-split step): at the ocean u points of the interior and its
  * one-point ring uu2d = ubrtr_i/hhu and pgrx = pgrx - (slpr(m+1,n) -
  * slpr(m,n))*hhu*dyh/RefDen; likewise vv2d, pgry at v points.  Host arrays;

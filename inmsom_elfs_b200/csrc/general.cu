@@ -402,7 +402,7 @@ __global__ void k_rhs2d_term(int m0, int m1, int n0, int n1, Dom D, GridDev g, d
     }
 }
 
-// ---- Control/dyncall.f90:186-201: corrected 2-D velocity and the slpr part
+// ---- Control/dyncall.f90:188-201: corrected 2-D velocity and the slpr part
 // of the time-mean pressure gradient (interior and its one-point ring)
 __global__ void k_velocity2d(int m0, int m1, int n0, int n1, Dom D, GridDev g, double rho, double *uu2d,
                              double *vv2d, double *pgrx, double *pgry, const double *ubrtr_i,

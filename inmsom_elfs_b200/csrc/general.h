@@ -77,7 +77,7 @@ void r_diss(const Dom &d, const GridDev &g, double r_fric, double *r, cudaStream
 void wind_forcing(const Dom &d, const GridDev &g, const Consts &c,
                   const double *taux, const double *tauy, double *rhsx,
                   double *rhsy, cudaStream_t s);
-// Control/dyncall.f90:186-201: uu2d = ubrtr_i/hhu, pgrx -= slpr gradient (and v)
+// Control/dyncall.f90:188-201: uu2d = ubrtr_i/hhu, pgrx -= slpr gradient (and v)
 void velocity2d(const Dom &d, const GridDev &g, const Consts &c, double *uu2d, double *vv2d, double *pgrx,
                 double *pgry, const double *ubrtr_i, const double *vbrtr_i, const double *slpr, const double *hhu,
                 const double *hhv, cudaStream_t s);

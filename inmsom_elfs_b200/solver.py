@@ -158,7 +158,7 @@ class BarotropicSolver:
         return rhsx, rhsy
 
     def velocity2d(self, uu2d, vv2d, pgrx, pgry, ubrtr_i, vbrtr_i, slpr, hhu, hhv):
-        """Control/dyncall.f90:186-201 in place (inmsom_velocity2d)."""
+        """Control/dyncall.f90:188-201 in place (inmsom_velocity2d)."""
         check(load().inmsom_velocity2d(self._ctx, dptr(uu2d), dptr(vv2d), dptr(pgrx), dptr(pgry), dptr(ubrtr_i),
                                        dptr(vbrtr_i), dptr(slpr), dptr(hhu), dptr(hhv)))
         return uu2d, vv2d, pgrx, pgry

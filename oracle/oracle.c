@@ -1095,7 +1095,7 @@ void ora_vertical_velocity(const ora_grid *g, int nz, const double *dz, const do
 #undef I3
 }
 
-/* Control/dyncall.f90:186-201: the corrected 2-D velocity from the time
+/* Control/dyncall.f90:188-201: the corrected 2-D velocity from the time
  * means and the sea-level-pressure part of the time-mean pressure gradient,
  * over nx_start-1..nx_end+1 x ny_start-1..ny_end+1 */
 void ora_velocity2d(const ora_grid *g, double *uu2d, double *vv2d, double *pgrx, double *pgry,

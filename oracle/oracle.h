@@ -173,7 +173,7 @@ void ora_depth_ave(const ora_grid *g, int nz, const double *dz, double *u, doubl
 /* Control/dyncall.f90:170-183 (sign < 0) and :215-229 (sign > 0) */
 void ora_shift_barotropic(const ora_grid *g, int nz, double *uu, double *vv, const double *uu2d,
                           const double *vv2d, int sign);
-/* Control/dyncall.f90:186-201: uu2d = ubrtr_i/hhu, pgrx -= slpr gradient
+/* Control/dyncall.f90:188-201: uu2d = ubrtr_i/hhu, pgrx -= slpr gradient
  * (and v), on the interior and its one-point ring. */
 void ora_velocity2d(const ora_grid *g, double *uu2d, double *vv2d, double *pgrx, double *pgry,
                     const double *ubrtr_i, const double *vbrtr_i, const double *slpr, const double *hhu,

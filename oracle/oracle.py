@@ -150,7 +150,7 @@ def rhs2d(basin, rhsx, rhsy, diff_disp=(None, None), tran=(None, None), tran_dis
 
 
 def velocity2d(basin, uu2d, vv2d, pgrx, pgry, ubrtr_i, vbrtr_i, slpr, hhu, hhv):
-    """Control/dyncall.f90:186-201 in place on uu2d, vv2d, pgrx, pgry."""
+    """Control/dyncall.f90:188-201 in place on uu2d, vv2d, pgrx, pgry."""
     g = grid_struct(basin)
     load().ora_velocity2d(ctypes.byref(g), _d(uu2d), _d(vv2d), _d(pgrx), _d(pgry), _d(ubrtr_i), _d(vbrtr_i),
                           _d(slpr), _d(hhu), _d(hhv))

@@ -308,7 +308,7 @@ def test_rhs2d_bitexact(gpu, ora, with_all):
 
 
 def test_velocity2d_bitexact(gpu, ora):
-    """inmsom_velocity2d (Control/dyncall.f90:186-201) against the oracle's
+    """inmsom_velocity2d (Control/dyncall.f90:188-201) against the oracle's
     restatement, bit for bit, after a call of barotropic_dynamics."""
     b = prep(basins.regional_basin(nx=170, ny=140, seed=20), ora)
     with gpu.BarotropicSolver(b, resident=True) as s:
