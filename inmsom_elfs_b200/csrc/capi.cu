@@ -9,6 +9,7 @@
 #include <cstdarg>
 #include <cstdio>
 #include <cstring>
+#include <functional>
 #include <string>
 #include <vector>
 
@@ -1159,6 +1160,89 @@ int box3(inmsom_ctx *c, double *dev, double *host, int nlev, int r0, int r1, int
     return INMSOM_OK;
 }
 
+// A 3-D field of a banded call: its device copy, the host array, its levels
+struct Field3 {
+    double *dev;
+    double *host;
+    int nlev;
+};
+
+// The copy pipeline of the 3-D entry points.  The interior rows are cut into
+// nb bands; band b's rows of the inputs are uploaded on s_up while band b-1
+// runs on the context's stream (run(n0, n1)) and band b-2's interior
+// results go back on s_dn.  Each input row is uploaded once: band b brings
+// the rows from just after band b-1's last to one past its own last
+// interior row (run reads rows n0-1..n1+1), the last band the rest of the
+// arrays.  After every band, border() runs and everything of the outputs
+// outside the interior is downloaded.  pre(s_up) issues the 2-D uploads;
+// flag (4 bytes on the device) is read back at the end.  The phase times
+// are the uploads, the kernels' own time (CUDA events around each run and
+// the border) and from the last kernel to the end.
+int pipelined(inmsom_ctx *c, int nb, const std::vector<Field3> &in, const std::vector<Field3> &out,
+              const std::function<int(cudaStream_t)> &pre, const std::function<int(int, int)> &run,
+              const std::function<int()> &border, const int *flag_dev, int *flag)
+{
+    const Dom &d = c->dom;
+    if (!c->s_up) CK(cudaStreamCreateWithFlags(&c->s_up, cudaStreamNonBlocking));
+    if (!c->s_dn) CK(cudaStreamCreateWithFlags(&c->s_dn, cudaStreamNonBlocking));
+    for (auto &e : c->bev)
+        if (!e) CK(cudaEventCreate(&e));
+    cudaEvent_t *ev_up = c->bev, *ev_k0 = c->bev + 8, *ev_k1 = c->bev + 16, *ev_bd = c->bev + 32;
+    const int nyi = d.ny_end - d.ny_start + 1;
+    nb = std::max(1, std::min(nb, std::min(8, nyi)));
+    const int nxa = d.nxa(), nya = d.nya();
+    const int ix0 = d.nx_start - d.bnd_x1, ix1 = d.nx_end - d.bnd_x1;      // interior, 0-based
+    const int iy0 = d.ny_start - d.bnd_y1, iy1 = d.ny_end - d.bnd_y1;
+    c->ph_valid = false;
+    c->ph_direct = false;
+    CK(cudaEventRecord(c->ph[0], c->stream));
+    CK(cudaStreamWaitEvent(c->s_up, c->ph[0], 0));
+    CKR(pre(c->s_up));
+    int up_next = 0;
+    for (int b = 0; b < nb; b++) {
+        const int n0 = d.ny_start + (int)((long long)nyi * b / nb);
+        const int n1 = d.ny_start + (int)((long long)nyi * (b + 1) / nb) - 1;
+        const int up_last = b == nb - 1 ? nya - 1 : n1 + 1 - d.bnd_y1;
+        for (const Field3 &f : in) CKR(box3(c, f.dev, f.host, f.nlev, up_next, up_last, 0, nxa - 1, true, c->s_up));
+        up_next = up_last + 1;
+        CK(cudaEventRecord(ev_up[b], c->s_up));
+        CK(cudaStreamWaitEvent(c->stream, ev_up[b], 0));
+        CK(cudaEventRecord(ev_k0[b], c->stream));
+        if (run(n0, n1)) return set_err(INMSOM_ECUDA, "launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+        CK(cudaGetLastError());
+        CK(cudaEventRecord(ev_k1[b], c->stream));
+        CK(cudaStreamWaitEvent(c->s_dn, ev_k1[b], 0));
+        for (const Field3 &f : out)
+            CKR(box3(c, f.dev, f.host, f.nlev, n0 - d.bnd_y1, n1 - d.bnd_y1, ix0, ix1, false, c->s_dn));
+    }
+    CK(cudaEventRecord(ev_bd[0], c->stream));
+    if (border()) return set_err(INMSOM_ECUDA, "launch failed: %s", cudaGetErrorString(cudaGetLastError()));
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(ev_bd[1], c->stream));
+    CK(cudaStreamWaitEvent(c->s_dn, ev_bd[1], 0));
+    CK(cudaMemcpyAsync(flag, flag_dev, sizeof(int), cudaMemcpyDeviceToHost, c->s_dn));
+    for (const Field3 &f : out) {
+        CKR(box3(c, f.dev, f.host, f.nlev, 0, iy0 - 1, 0, nxa - 1, false, c->s_dn));             // rows above
+        CKR(box3(c, f.dev, f.host, f.nlev, iy1 + 1, nya - 1, 0, nxa - 1, false, c->s_dn));       // rows below
+        CKR(box3(c, f.dev, f.host, f.nlev, iy0, iy1, 0, ix0 - 1, false, c->s_dn));              // columns left
+        CKR(box3(c, f.dev, f.host, f.nlev, iy0, iy1, ix1 + 1, nxa - 1, false, c->s_dn));        // columns right
+    }
+    CK(cudaEventRecord(c->ph[3], c->s_dn));
+    CK(cudaStreamWaitEvent(c->stream, c->ph[3], 0));
+    CKR(sync_stream(c));
+    float t = 0.0f, sum = 0.0f;
+    CK(cudaEventElapsedTime(&c->ph_ms[0], c->ph[0], ev_up[nb - 1]));
+    for (int b = 0; b < nb; b++) {
+        CK(cudaEventElapsedTime(&t, ev_k0[b], ev_k1[b]));
+        sum += t;
+    }
+    CK(cudaEventElapsedTime(&t, ev_bd[0], ev_bd[1]));
+    c->ph_ms[1] = sum + t;
+    CK(cudaEventElapsedTime(&c->ph_ms[2], ev_bd[1], c->ph[3]));
+    c->ph_direct = true;
+    return INMSOM_OK;
+}
+
 column::Levels col_levels(inmsom_ctx *c)
 {
     column::Levels L;
@@ -1196,12 +1280,6 @@ int inmsom_baroclinic_dynamics(inmsom_ctx *c, int nz, const double *dz, const do
     const Dom &d = c->dom;
     if (column::wrap_inside(d)) return set_err(INMSOM_EUNSUPPORTED, "inmsom_baroclinic_dynamics: a periodic wrap column/row lies in the interior");
     CKR(col_alloc(c, nz));
-    if (!c->s_up) CK(cudaStreamCreateWithFlags(&c->s_up, cudaStreamNonBlocking));
-    if (!c->s_dn) CK(cudaStreamCreateWithFlags(&c->s_dn, cudaStreamNonBlocking));
-    for (auto &e : c->bev)
-        if (!e) CK(cudaEventCreate(&e));
-    c->ph_valid = false;
-    c->ph_direct = false;
     column::BaroclinicArgs a;
     a.tau = tau;
     a.uu = col3(c, C3_UU); a.uup = col3(c, C3_UUP); a.vv = col3(c, C3_VV); a.vvp = col3(c, C3_VVP);
@@ -1216,80 +1294,29 @@ int inmsom_baroclinic_dynamics(inmsom_ctx *c, int nz, const double *dz, const do
     a.flag = reinterpret_cast<int *>(c->col_lev + 2 * nz + 1);
     const column::Levels L = col_levels(c);
     const GridDev gd = c->gdev();
-
-    // Row bands, pipelined over three streams: band b's rows are uploaded on
-    // s_up while band b-1 is solved on the context's stream and band b-2's
-    // results go back on s_dn.  Each row is uploaded once: band b brings the
-    // rows from just after band b-1's last upload to one past its own last
-    // interior row (the solves read rows n-1..n+1); the last band brings the
-    // rest of the arrays.  The border (outside the interior) is filtered and
-    // downloaded after the last band.
-    cudaEvent_t *ev_up = c->bev, *ev_k0 = c->bev + 8, *ev_k1 = c->bev + 16, *ev_bd = c->bev + 32;
-    const int nyi = d.ny_end - d.ny_start + 1, nb = std::min(8, nyi);
-    const int nxa = d.nxa(), nya = d.nya();
-    const int ix0 = d.nx_start - d.bnd_x1, ix1 = d.nx_end - d.bnd_x1;      // interior columns, 0-based
     // the nz-level inputs in the order of the block's fields C3_UU .. C3_RHSYT
     double *const up3[8] = {uu, uup, vv, vvp, (double *)RHSx, (double *)RHSy, (double *)RHSx_tran,
                             (double *)RHSy_tran};
-    CK(cudaEventRecord(c->ph[0], c->stream));
-    CK(cudaStreamWaitEvent(c->s_up, c->ph[0], 0));
+    std::vector<Field3> in, out;
+    for (int k = 0; k < 8; k++) in.push_back({col3(c, C3_UU + k), up3[k], nz});
+    in.push_back({colw(c, 0), (double *)ww, nz + 1});
+    in.push_back({colw(c, 1), (double *)nu, nz + 1});
+    for (int k = 0; k < 4; k++) out.push_back({col3(c, C3_UUO + k), io[k], nz});
     CK(cudaMemsetAsync(a.flag, 0, sizeof(int), c->stream));
-    for (int k = 0; k < NC2; k++)
-        CK(cudaMemcpy2DAsync(col2(c, k) + d.xoff, (size_t)d.pitch * sizeof(double), in2[k], nxa * sizeof(double),
-                             nxa * sizeof(double), nya, cudaMemcpyHostToDevice, c->s_up));
-    CK(cudaMemcpyAsync(c->col_lev, dz, nz * sizeof(double), cudaMemcpyHostToDevice, c->s_up));
-    CK(cudaMemcpyAsync(c->col_lev + nz, hzt, (nz + 1) * sizeof(double), cudaMemcpyHostToDevice, c->s_up));
-    int up_next = 0;                                                   // next array row (0-based) to upload
-    for (int b = 0; b < nb; b++) {
-        const int n0 = d.ny_start + (int)((long long)nyi * b / nb);
-        const int n1 = d.ny_start + (int)((long long)nyi * (b + 1) / nb) - 1;
-        const int up_last = b == nb - 1 ? nya - 1 : n1 + 1 - d.bnd_y1;
-        for (int k = 0; k < 8; k++)
-            CKR(box3(c, col3(c, C3_UU + k), up3[k], nz, up_next, up_last, 0, nxa - 1, true, c->s_up));
-        CKR(box3(c, colw(c, 0), (double *)ww, nz + 1, up_next, up_last, 0, nxa - 1, true, c->s_up));
-        CKR(box3(c, colw(c, 1), (double *)nu, nz + 1, up_next, up_last, 0, nxa - 1, true, c->s_up));
-        up_next = up_last + 1;
-        CK(cudaEventRecord(ev_up[b], c->s_up));
-        CK(cudaStreamWaitEvent(c->stream, ev_up[b], 0));
-        CK(cudaEventRecord(ev_k0[b], c->stream));
-        if (column::baroclinic_rows(d, gd, c->c, L, a, n0, n1, c->stream))
-            return set_err(INMSOM_ECUDA, "inmsom_baroclinic_dynamics: launch failed: %s",
-                           cudaGetErrorString(cudaGetLastError()));
-        CK(cudaEventRecord(ev_k1[b], c->stream));
-        CK(cudaStreamWaitEvent(c->s_dn, ev_k1[b], 0));
-        for (int k = 0; k < 4; k++)
-            CKR(box3(c, col3(c, C3_UUO + k), io[k], nz, n0 - d.bnd_y1, n1 - d.bnd_y1, ix0, ix1, false, c->s_dn));
-    }
-    CK(cudaEventRecord(ev_bd[0], c->stream));
-    column::baroclinic_border(d, gd, c->c, L, a, c->stream);
-    CK(cudaGetLastError());
-    CK(cudaEventRecord(ev_bd[1], c->stream));
-    CK(cudaStreamWaitEvent(c->s_dn, ev_bd[1], 0));
+    auto pre = [&](cudaStream_t su) -> int {
+        for (int k = 0; k < NC2; k++)
+            CK(cudaMemcpy2DAsync(col2(c, k) + d.xoff, (size_t)d.pitch * sizeof(double), in2[k],
+                                 d.nxa() * sizeof(double), d.nxa() * sizeof(double), d.nya(),
+                                 cudaMemcpyHostToDevice, su));
+        CK(cudaMemcpyAsync(c->col_lev, dz, nz * sizeof(double), cudaMemcpyHostToDevice, su));
+        CK(cudaMemcpyAsync(c->col_lev + nz, hzt, (nz + 1) * sizeof(double), cudaMemcpyHostToDevice, su));
+        return INMSOM_OK;
+    };
+    auto run = [&](int n0, int n1) { return column::baroclinic_rows(d, gd, c->c, L, a, n0, n1, c->stream); };
+    auto border = [&]() { return column::baroclinic_border(d, gd, c->c, L, a, c->stream); };
     int flag = 0;
-    CK(cudaMemcpyAsync(&flag, a.flag, sizeof(int), cudaMemcpyDeviceToHost, c->s_dn));
-    const int iy0 = d.ny_start - d.bnd_y1, iy1 = d.ny_end - d.bnd_y1;
-    for (int k = 0; k < 4; k++) {
-        double *dev = col3(c, C3_UUO + k);
-        CKR(box3(c, dev, io[k], nz, 0, iy0 - 1, 0, nxa - 1, false, c->s_dn));             // rows above
-        CKR(box3(c, dev, io[k], nz, iy1 + 1, nya - 1, 0, nxa - 1, false, c->s_dn));       // rows below
-        CKR(box3(c, dev, io[k], nz, iy0, iy1, 0, ix0 - 1, false, c->s_dn));              // columns left
-        CKR(box3(c, dev, io[k], nz, iy0, iy1, ix1 + 1, nxa - 1, false, c->s_dn));        // columns right
-    }
-    CK(cudaEventRecord(c->ph[3], c->s_dn));
-    CK(cudaStreamWaitEvent(c->stream, c->ph[3], 0));
-    CKR(sync_stream(c));
+    CKR(pipelined(c, 8, in, out, pre, run, border, a.flag, &flag));
     if (flag) return set_err(INMSOM_ETIMEOUT, "inmsom_baroclinic_dynamics: a bounded wait of the column kernel gave up");
-    // phases: the uploads, the kernels' own time, and from the last kernel to the end
-    float t = 0.0f, sum = 0.0f;
-    CK(cudaEventElapsedTime(&c->ph_ms[0], c->ph[0], ev_up[nb - 1]));
-    for (int b = 0; b < nb; b++) {
-        CK(cudaEventElapsedTime(&t, ev_k0[b], ev_k1[b]));
-        sum += t;
-    }
-    CK(cudaEventElapsedTime(&t, ev_bd[0], ev_bd[1]));
-    c->ph_ms[1] = sum + t;
-    CK(cudaEventElapsedTime(&c->ph_ms[2], ev_bd[1], c->ph[3]));
-    c->ph_direct = true;
     c->ph_valid = true;
     return INMSOM_OK;
 }
@@ -1364,19 +1391,6 @@ int inmsom_tracer_tran_diff(inmsom_ctx *c, int nz, const double *dz, const doubl
                                m, n);
         }
     CKR(trc_alloc(c, nz));
-    c->ph_valid = false;
-    c->ph_direct = false;
-    CK(cudaEventRecord(c->ph[0], c->stream));
-    const int f3[6] = {T_FF, T_FFP, T_UU, T_VV, T_MU, T_SRC};
-    const int f31[6] = {T_WW, T_NU, T_SLRX, T_SLRY, T_SLZX, T_SLZY};
-    for (int k = 0; k < 6; k++) CKR(h2d3(c, trc3(c, f3[k]), in3[k], nz));
-    for (int k = 0; k < 6; k++) CKR(h2d3(c, trc31(c, f31[k]), in31[k], nz + 1));
-    for (int k = 0; k < 7; k++) CKR(h2d(c, trc2(c, T_TOP + k), in2[k]));
-    CKR(h2d(c, reinterpret_cast<int *>(trc2(c, T_IGT)), ig_top));
-    CKR(h2d(c, reinterpret_cast<int *>(trc2(c, T_IGB)), ig_bot));
-    CK(cudaMemcpyAsync(c->trc_lev, dz, nz * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaMemcpyAsync(c->trc_lev + nz, hzt, (nz + 1) * sizeof(double), cudaMemcpyHostToDevice, c->stream));
-    CK(cudaEventRecord(c->ph[1], c->stream));
     column::TracerArgs a;
     a.tau = tau; a.factor_mu = factor_mu; a.factor_nu = factor_nu; a.az = az; a.ar = ar; a.alpha_gm = alpha_gm;
     a.src_factor = src_factor;
@@ -1393,24 +1407,40 @@ int inmsom_tracer_tran_diff(inmsom_ctx *c, int nz, const double *dz, const doubl
     a.flux_zx = trc31(c, T_FZX); a.flux_zy = trc31(c, T_FZY); a.coef_zx = trc31(c, T_COX); a.coef_zy = trc31(c, T_COY);
     a.sfgm_zx = trc31(c, T_SGX); a.sfgm_zy = trc31(c, T_SGY);
     a.flag = reinterpret_cast<int *>(c->trc_lev + 2 * nz + 1);
-    CK(cudaMemsetAsync(a.flag, 0, sizeof(int), c->stream));
     column::Levels L;
     L.nz = nz;
     L.plane = (long long)col_plane(c);
     L.dz = c->trc_lev;
     L.hzt = c->trc_lev + nz;
-    if (column::tracer_tran_diff(d, c->gdev(), c->c, L, a, c->stream))
-        return set_err(INMSOM_ECUDA, "inmsom_tracer_tran_diff: launch failed: %s", cudaGetErrorString(cudaGetLastError()));
-    CK(cudaGetLastError());
-    CK(cudaEventRecord(c->ph[2], c->stream));
+    const GridDev gd = c->gdev();
+    const int f3[6] = {T_FF, T_FFP, T_UU, T_VV, T_MU, T_SRC};
+    const int f31[6] = {T_WW, T_NU, T_SLRX, T_SLRY, T_SLZX, T_SLZY};
+    std::vector<Field3> in, out;
+    for (int k = 0; k < 6; k++) in.push_back({trc3(c, f3[k]), (double *)in3[k], nz});
+    for (int k = 0; k < 6; k++) in.push_back({trc31(c, f31[k]), (double *)in31[k], nz + 1});
+    out.push_back({trc3(c, T_FFO), ff, nz});
+    out.push_back({trc3(c, T_FFPO), ffp, nz});
+    out.push_back({trc2(c, T_FFX), flux_f_x, 4});
+    out.push_back({trc2(c, T_FFY), flux_f_y, 4});
+    CK(cudaMemsetAsync(a.flag, 0, sizeof(int), c->stream));
+    auto pre = [&](cudaStream_t su) -> int {
+        const size_t w = (size_t)d.nxa() * sizeof(double), dp = (size_t)d.pitch * sizeof(double);
+        for (int k = 0; k < 7; k++)
+            CK(cudaMemcpy2DAsync(trc2(c, T_TOP + k) + d.xoff, dp, in2[k], w, w, d.nya(), cudaMemcpyHostToDevice, su));
+        const size_t wi = (size_t)d.nxa() * sizeof(int), dpi = (size_t)d.pitch * sizeof(int);
+        CK(cudaMemcpy2DAsync(reinterpret_cast<int *>(trc2(c, T_IGT)) + d.xoff, dpi, ig_top, wi, wi, d.nya(),
+                             cudaMemcpyHostToDevice, su));
+        CK(cudaMemcpy2DAsync(reinterpret_cast<int *>(trc2(c, T_IGB)) + d.xoff, dpi, ig_bot, wi, wi, d.nya(),
+                             cudaMemcpyHostToDevice, su));
+        CK(cudaMemcpyAsync(c->trc_lev, dz, nz * sizeof(double), cudaMemcpyHostToDevice, su));
+        CK(cudaMemcpyAsync(c->trc_lev + nz, hzt, (nz + 1) * sizeof(double), cudaMemcpyHostToDevice, su));
+        return INMSOM_OK;
+    };
+    auto run = [&](int n0, int n1) { return column::tracer_rows(d, gd, c->c, L, a, n0, n1, c->stream); };
+    auto border = [&]() { return column::tracer_border(d, gd, c->c, L, a, c->stream); };
     int flag = 0;
-    CK(cudaMemcpyAsync(&flag, a.flag, sizeof(int), cudaMemcpyDeviceToHost, c->stream));
-    CKR(d2h3(c, ff, trc3(c, T_FFO), nz));
-    CKR(d2h3(c, ffp, trc3(c, T_FFPO), nz));
-    CKR(d2h3(c, flux_f_x, trc2(c, T_FFX), 4));
-    CKR(d2h3(c, flux_f_y, trc2(c, T_FFY), 4));
-    CK(cudaEventRecord(c->ph[3], c->stream));
-    CKR(sync_stream(c));
+    // a periodic y wraps the y-fluxes of every row before any solve: one band
+    CKR(pipelined(c, d.py ? 1 : 8, in, out, pre, run, border, a.flag, &flag));
     if (flag) return set_err(INMSOM_ETIMEOUT, "inmsom_tracer_tran_diff: a bounded wait of the solve gave up");
     c->ph_valid = true;
     return INMSOM_OK;

@@ -586,7 +586,7 @@ __device__ __forceinline__ bool tracer_flux_column(const Dom &D, const GridDev &
     return ok;
 }
 
-__global__ void __launch_bounds__((NCW + 1) * 32) k_tracer_flux(Dom D, GridDev g, Levels L, TracerArgs a)
+__global__ void __launch_bounds__((NCW + 1) * 32) k_tracer_flux(Dom D, GridDev g, Levels L, TracerArgs a, int row0)
 {
     extern __shared__ __align__(128) double sm[];
     const int nz = L.nz;
@@ -595,7 +595,7 @@ __global__ void __launch_bounds__((NCW + 1) * 32) k_tracer_flux(Dom D, GridDev g
     uint64_t *full = reinterpret_cast<uint64_t *>(sdz + 2 * nz + 1);
     uint64_t *empty = full + NS;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = D.nx_start + blockIdx.x * CW, n = D.ny_start + blockIdx.y;
+    const int m0 = D.nx_start + blockIdx.x * CW, n = row0 + blockIdx.y;
     for (int t = threadIdx.x; t < 2 * nz + 1; t += blockDim.x) sdz[t] = L.dz[t];
     if (threadIdx.x == 0) {
         for (int s = 0; s < NS; s++) {
@@ -674,7 +674,7 @@ size_t tracer_smem(int nz)
     return ((size_t)TNS * TSLOT_D + 2 * (size_t)nz + 1) * sizeof(double) + 2 * TNS * sizeof(uint64_t);
 }
 
-__global__ void __launch_bounds__(3 * 32) k_tracer_solve(Dom D, GridDev g, Levels L, TracerArgs a, double ts)
+__global__ void __launch_bounds__(3 * 32) k_tracer_solve(Dom D, GridDev g, Levels L, TracerArgs a, double ts, int row0)
 {
     extern __shared__ __align__(128) double sm[];
     const int nz = L.nz;
@@ -683,7 +683,7 @@ __global__ void __launch_bounds__(3 * 32) k_tracer_solve(Dom D, GridDev g, Level
     uint64_t *full = reinterpret_cast<uint64_t *>(sdz + 2 * nz + 1);
     uint64_t *empty = full + TNS;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-    const int m0 = D.nx_start + blockIdx.x * CW, n = D.ny_start + blockIdx.y;
+    const int m0 = D.nx_start + blockIdx.x * CW, n = row0 + blockIdx.y;
     for (int t = threadIdx.x; t < 2 * nz + 1; t += blockDim.x) sdz[t] = L.dz[t];
     if (threadIdx.x == 0) {
         for (int s = 0; s < TNS; s++) {
@@ -1006,17 +1006,21 @@ int baroclinic_dynamics(const Dom &d, const GridDev &g, const Consts &c, const L
     return baroclinic_border(d, g, c, L, a, s);
 }
 
-int tracer_tran_diff(const Dom &d, const GridDev &g, const Consts &c, const Levels &L, const TracerArgs &a,
-                     cudaStream_t s)
+int tracer_rows(const Dom &d, const GridDev &g, const Consts &c, const Levels &L, const TracerArgs &a, int n0, int n1,
+                cudaStream_t s)
 {
-    // the staged solve's 16-byte segments need an even row pitch and level stride
+    // the staged kernels' 16-byte segments need an even row pitch and level stride
     if (L.nz < 2 || L.nz > MAX_NZ || wrap_inside(d) || d.pitch % 2 || L.plane % 2 || !a.flag) return -1;
-    const int nxi = d.nx_end - d.nx_start + 1, nyi = d.ny_end - d.ny_start + 1;
+    if (n0 < d.ny_start || n1 > d.ny_end || n0 > n1) return -1;
+    // the y-fluxes' periodic wrap needs every row's fluxes first
+    if (d.py && (n0 != d.ny_start || n1 != d.ny_end)) return -1;
+    const int nxi = d.nx_end - d.nx_start + 1, rows = n1 - n0 + 1;
     const size_t fsm = flux_smem(L.nz);
     if (cudaFuncSetAttribute(k_tracer_flux, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)fsm) != cudaSuccess)
         return -1;
-    k_tracer_flux<<<dim3((nxi + CW - 1) / CW, nyi), (NCW + 1) * 32, fsm, s>>>(d, g, L, a);
-    // the x-fluxes wrap in x, the y-fluxes in y (Function/tem_sal.f90:264-274)
+    k_tracer_flux<<<dim3((nxi + CW - 1) / CW, rows), (NCW + 1) * 32, fsm, s>>>(d, g, L, a, n0);
+    // the x-fluxes wrap in x, the y-fluxes in y (Function/tem_sal.f90:264-274); the x wrap
+    // copies whole columns, so a band's wrap also rewrites the earlier bands' (final) rows
     if (d.px) {
         k_cyclize_x3<<<dim3((d.nya() + 127) / 128, L.nz), 128, 0, s>>>(d, L.plane, a.flux_x);
         for (double *f : {a.flux_zx, a.coef_zx, a.sfgm_zx})
@@ -1030,10 +1034,24 @@ int tracer_tran_diff(const Dom &d, const GridDev &g, const Consts &c, const Leve
     const size_t smem = tracer_smem(L.nz);
     if (cudaFuncSetAttribute(k_tracer_solve, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return -1;
-    k_tracer_solve<<<dim3((nxi + CW - 1) / CW, nyi), 3 * 32, smem, s>>>(d, g, L, a, c.ts);
+    k_tracer_solve<<<dim3((nxi + CW - 1) / CW, rows), 3 * 32, smem, s>>>(d, g, L, a, c.ts, n0);
+    return 0;
+}
+
+int tracer_border(const Dom &d, const GridDev &g, const Consts &c, const Levels &L, const TracerArgs &a,
+                  cudaStream_t s)
+{
+    const int nxi = d.nx_end - d.nx_start + 1, nyi = d.ny_end - d.ny_start + 1;
     const int count = d.nxa() * d.nya() - nxi * nyi;
     if (count > 0) k_tracer_border<<<dim3((count + 127) / 128, L.nz), 128, 0, s>>>(d, g, L, a, c.ts, count);
     return 0;
+}
+
+int tracer_tran_diff(const Dom &d, const GridDev &g, const Consts &c, const Levels &L, const TracerArgs &a,
+                     cudaStream_t s)
+{
+    if (tracer_rows(d, g, c, L, a, d.ny_start, d.ny_end, s)) return -1;
+    return tracer_border(d, g, c, L, a, s);
 }
 
 int depth_ave(const Dom &d, const Levels &L, double *u, double *utr, const float *mask, int kbcl, cudaStream_t s)

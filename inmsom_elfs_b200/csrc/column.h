@@ -85,6 +85,13 @@ struct TracerArgs {
 // column/row lies inside the interior.
 int tracer_tran_diff(const Dom &d, const GridDev &g, const Consts &c, const Levels &L, const TracerArgs &a,
                      cudaStream_t s);
+// The same in parts: the fluxes and column solves of interior rows n0..n1
+// (the solves read the fluxes of row n0-1, which an earlier call wrote;
+// with a periodic y the whole interior at once), then the border.
+int tracer_rows(const Dom &d, const GridDev &g, const Consts &c, const Levels &L, const TracerArgs &a, int n0, int n1,
+                cudaStream_t s);
+int tracer_border(const Dom &d, const GridDev &g, const Consts &c, const Levels &L, const TracerArgs &a,
+                  cudaStream_t s);
 
 // Function/depth.f90:223-254: utr = sum_k u(k)*dz(k) at the points of mask
 // (all but the arrays' outermost ring), u = u - kbcl*utr there; L.dz only.
