@@ -602,7 +602,7 @@ def run_study_baroclinic(args):
                      "traffic_source": "ncu dram bytes of a 512x512x20 launch scaled by cell-levels",
                      "algorithmic_bytes_per_call": int(alg),
                      "kernels_timed": "k_columns (8 row bands) + k_border, CUDA events around each launch"},
-        "gpu_launches": 2 * len(comp),
+        "gpu_launches": 9 * len(comp),            # per call: k_columns for each of 8 row bands, k_border
         "clocks": clk.summary(),
     }
     if not args.no_cpu:
@@ -676,7 +676,9 @@ def run_study_tracer(args):
                      "algorithmic_bytes_per_call": int(alg),
                      "kernels_timed": "k_tracer_flux, wraps, k_tracer_solve (8 row bands) + k_tracer_border, "
                                       "CUDA events around each band"},
-        "gpu_launches": 3 * len(comp),
+        # per call: k_tracer_flux and k_tracer_solve for each of 8 row bands (and the flux
+        # wraps on a periodic basin), k_tracer_border
+        "gpu_launches": 17 * len(comp),
         "clocks": clk.summary(),
     }
     if not args.no_cpu:
