@@ -184,11 +184,11 @@ std::string fmt_e(double x, int w, int d)
     return right(s, w);
 }
 
-// Fw.d
+// Fw.d (the decimal point is always written, also for d = 0)
 std::string fmt_f(double x, int w, int d)
 {
     char buf[512];
-    std::snprintf(buf, sizeof buf, "%.*f", d, x);
+    std::snprintf(buf, sizeof buf, "%#.*f", d, x);
     std::string s = buf;
     if (s[0] == '-' && s.find_first_not_of("-0.") == std::string::npos) s.erase(0, 1);   // no minus zero
     if ((int)s.size() > w && s.compare(0, 2, "0.") == 0) s.erase(0, 1);

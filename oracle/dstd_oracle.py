@@ -87,7 +87,7 @@ def edit_e(x, w, d):
 
 
 def edit_f(x, w, d):
-    s = f"{x:.{d}f}"
+    s = f"{x:.{d}f}" + ("." if d == 0 else "")     # Fw.0 still writes the point
     if s.startswith("-") and float(s) == 0.0:
         s = s[1:]
     if len(s) > w:

@@ -208,3 +208,24 @@ def test_format_error_codes(tmp_path):
     with pytest.raises(InmsomError) as e:
         dstd.wdstd8(str(tmp_path / "no" / "such" / "dir"), "x.dat", 1, f.copy(order="F"), lu)
     assert e.value.code == 6
+
+
+def test_ctl_number_editing_edge_cases(tmp_path):
+    """G15.8 editing of values at the F/E boundaries (rounding that changes
+    the decade, tiny and huge exponents, negative zero) and random values,
+    through a LEVELS axis: the library's text equals the restatement's."""
+    rng = np.random.default_rng(3)
+    edge = [0.0, -0.0, 1.0, -1.0, 0.1, 0.099999999, 0.0999999999, 9.999999994, 9.999999995, 99999999.4,
+            99999999.5, 1.0e8, 123456789.0, 1.0e-100, -1.0e-100, 1.0e100, 3.0e-5, 0.5, 27.5, -1500.0,
+            np.nextafter(0.1, 0.0), np.nextafter(1.0e8, 0.0)]
+    vals = edge + list(10.0 ** rng.uniform(-12, 12, 60) * rng.choice([-1.0, 1.0], 60))
+    n = len(vals)
+    args = (str(tmp_path / "g.dat"), -1.0e32, n, 1, 1, 1, 1, vals, 0.0, 0, [0.0], 1.0, 0, [0.0], 1.0, 1, 2000, 1, 1,
+            0, 0, 86400.0, "t", "v")
+    dstd.ctl_file_write(*args)
+    _, text = od.ctl_text(*args)
+    assert (tmp_path / "g.ctl").read_text() == text
+    # worked out by hand: G15.8 of 99999999.4 is F11.0 (the point kept) and 4 blanks
+    assert od.edit_g(99999999.4, 15, 8) == "  99999999.    "
+    assert od.edit_g(9.999999995, 15, 8) == "  10.000000    "
+    assert od.edit_g(1.0e100, 15, 8) == " 0.10000000+101"
