@@ -26,12 +26,14 @@ SOURCES = {
     "general.cu": ["--fmad=false"],
     "fused.cu": [],
     "capi.cu": [],
+    "capi_column.cu": [],
+    "capi_io.cu": [],
     "noalloc.cu": [],
     "closure.cu": [],
     "column.cu": ["--fmad=false"],
     "dstd.cu": [],
 }
-HEADERS = ["common.cuh", "general.h", "fused.h", "closure.h", "column.h"]
+HEADERS = ["common.cuh", "general.h", "fused.h", "closure.h", "column.h", "context.h"]
 
 
 def nvcc() -> str:
