@@ -409,6 +409,28 @@ int inmsom_ctl_file_write(const char *fname, float undef, int nx, int ny, int nz
                           int yr_type, int year0, int month0, int day0, int hour0, int minute0, float ht,
                           const char *title, const char *varname);
 
+/* The GrADS descriptor reader of Service/rw_ctl_file.f90:185-566
+ * ctl_file_read, same arguments in the same order, with the capacity of
+ * each array after it: datname (datname_len bytes), x0/y0/z0 (x0_cap ...
+ * values), title (title_len bytes), varname (varname_cap names of
+ * varname_len bytes each, one after another).  Character results are
+ * NUL-terminated without trailing blanks; a name longer than its room is
+ * cut as the Fortran character variable would cut it.  As the reference:
+ * inform counts the definitions read (DSET, TITLE, UNDEF, OPTIONS, XDEF,
+ * YDEF, ZDEF, VARS; TDEF is not counted), yr_type is 1 unless OPTIONS
+ * starts with 365, a LINEAR x or y axis is filled as x0(1) + hx*(i-1) and a
+ * LINEAR z axis as z0(1) + hz*i, LEVELS values may continue over the
+ * following lines, the TDEF step is in seconds (yr = 365 days, mo = 30
+ * days, dy, hr, mn) in single precision, and the read stops at ENDVARS
+ * (at most 512 lines).  title and varname may be NULL.  Errors:
+ * INMSOM_EIO (no such file), INMSOM_EARG (the reference's error messages,
+ * an end of file before ENDVARS, more values than an array holds). */
+int inmsom_ctl_file_read(const char *ctlname, char *datname, int datname_len, float *undef, int *nx, int *ny,
+                         int *nz, int *nt, int *xtype, double *x0, int x0_cap, double *hx, int *ytype, double *y0,
+                         int y0_cap, double *hy, int *ztype, double *z0, int z0_cap, double *hz, int *nvar,
+                         int *yr_type, int *year0, int *month0, int *day0, int *hour0, int *minute0, float *ht,
+                         char *title, int title_len, char *varname, int varname_len, int varname_cap, int *inform);
+
 /* The grid and calendar that the checkpoint's descriptors state
  * (basin_grid's xt, xu, yt, yv, dxst, dyst, xgr_type, ygr_type and the
  * model time of Control/output.f90:1454-1463): for a LINEAR axis (type 0)

@@ -31,7 +31,7 @@ EXPORTS = (
     "inmsom_gpu_stream", "inmsom_gpu_pitch", "inmsom_rhs2d", "inmsom_velocity2d",
     "inmsom_baroclinic_dynamics", "inmsom_vertical_velocity", "inmsom_depth_ave", "inmsom_shift_barotropic",
     "inmsom_wdstd8", "inmsom_wdstd", "inmsom_rdstd8", "inmsom_rdstd", "inmsom_ctl_file_write",
-    "inmsom_write_checkpoint", "inmsom_read_checkpoint", "inmsom_tracer_tran_diff",
+    "inmsom_write_checkpoint", "inmsom_read_checkpoint", "inmsom_tracer_tran_diff", "inmsom_ctl_file_read",
 )
 
 # include/inmsom_gpu.h: INMSOM_MLP_*
@@ -142,6 +142,9 @@ def load() -> ctypes.CDLL:
     lib.inmsom_ctl_file_write.argtypes = [cp, ctypes.c_float, i, i, i, i, i, DP, d, i, DP, d, i, DP, d,
                                           i, i, i, i, i, i, ctypes.c_float, cp, cp]
     lib.inmsom_write_checkpoint.argtypes = [VP, cp, ctypes.POINTER(CCtlAxes)]
+    IP, FPn = ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_float)
+    lib.inmsom_ctl_file_read.argtypes = [cp, cp, i, FPn, IP, IP, IP, IP, IP, DP, i, DP, IP, DP, i, DP, IP, DP, i,
+                                         DP, IP, IP, IP, IP, IP, IP, IP, FPn, cp, i, cp, i, i, IP]
     IPP = ctypes.POINTER(ctypes.c_int)
     lib.inmsom_tracer_tran_diff.argtypes = ([VP, i, DP, DP, DP, DP, d, DP, DP, DP, DP, d, DP, d, DP, DP, DP, DP,
                                              d, d, d, DP, DP, IPP, IPP, DP, DP, DP, i, i, IPP, IPP, cp, FP, DP, d]

@@ -32,6 +32,7 @@ SOURCES = {
     "closure.cu": [],
     "column.cu": ["--fmad=false"],
     "dstd.cu": [],
+    "ctl_read.cu": [],
 }
 HEADERS = ["common.cuh", "general.h", "fused.h", "closure.h", "column.h", "context.h"]
 

@@ -3,9 +3,10 @@
 DIOGIN-standard direct-access files (Service/input_output_data.f90:117-534):
 one record per level of a box of a field, x fastest, FP64 (wdstd8/rdstd8)
 or FP32 (wdstd/rdstd), land points written as undef = -1.0e32 and read as 0.
-GrADS descriptors (Service/rw_ctl_file.f90:1-139 ctl_file_write).  Arrays
-are Fortran-ordered numpy arrays (nx, ny[, nz]); boxes are 1-based inclusive
-(nxb, nxe, nyb, nye, nzb, nze) as in the reference's argument lists.
+GrADS descriptors (Service/rw_ctl_file.f90:1-139 ctl_file_write and
+:185-566 ctl_file_read).  Arrays are Fortran-ordered numpy arrays (nx, ny[,
+nz]); boxes are 1-based inclusive (nxb, nxe, nyb, nye, nzb, nze) as in the
+reference's argument lists.
 """
 from __future__ import annotations
 
@@ -68,3 +69,32 @@ def ctl_file_write(fname, undef, nx, ny, nz, nt, xtype, x0, hx, ytype, y0, hy, z
                                        arrs[0].ctypes.data_as(DP), float(hx), ytype, arrs[1].ctypes.data_as(DP),
                                        float(hy), ztype, arrs[2].ctypes.data_as(DP), float(hz), yr_type, year0,
                                        month0, day0, hour0, minute0, float(ht), title.encode(), varname.encode()))
+
+
+def ctl_file_read(ctlname, x_cap=4096, y_cap=4096, z_cap=1024, var_cap=16, name_len=256):
+    """inmsom_ctl_file_read (Service/rw_ctl_file.f90:185-566): a dict of the
+    reference's output arguments; x0, y0, z0 hold nx, ny, nz values (at
+    least one), varname the nvar names.  Arguments the descriptor does not
+    set come back as 0 (the reference leaves them as they were)."""
+    I, F, D = ctypes.c_int, ctypes.c_float, ctypes.c_double
+    ints = {k: I(0) for k in ("nx", "ny", "nz", "nt", "xtype", "ytype", "ztype", "nvar", "yr_type", "year0",
+                              "month0", "day0", "hour0", "minute0", "inform")}
+    undef, ht, hx, hy, hz = F(0), F(0), D(0), D(0), D(0)
+    x0, y0, z0 = (np.zeros(max(n, 1)) for n in (x_cap, y_cap, z_cap))
+    datname, title = ctypes.create_string_buffer(name_len), ctypes.create_string_buffer(name_len)
+    names = ctypes.create_string_buffer(var_cap * name_len)
+    r = ctypes.byref
+    check(load().inmsom_ctl_file_read(
+        str(ctlname).encode(), datname, name_len, r(undef), r(ints["nx"]), r(ints["ny"]), r(ints["nz"]),
+        r(ints["nt"]), r(ints["xtype"]), x0.ctypes.data_as(DP), len(x0), r(hx), r(ints["ytype"]),
+        y0.ctypes.data_as(DP), len(y0), r(hy), r(ints["ztype"]), z0.ctypes.data_as(DP), len(z0), r(hz),
+        r(ints["nvar"]), r(ints["yr_type"]), r(ints["year0"]), r(ints["month0"]), r(ints["day0"]),
+        r(ints["hour0"]), r(ints["minute0"]), r(ht), title, name_len, names, name_len, var_cap, r(ints["inform"])))
+    out = {k: v.value for k, v in ints.items()}
+    nvar = max(out["nvar"], 0)
+    out.update(datname=datname.value.decode(), title=title.value.decode(), undef=np.float32(undef.value),
+               ht=np.float32(ht.value), hx=hx.value, hy=hy.value, hz=hz.value,
+               x0=x0[:max(out["nx"], 1)].copy(), y0=y0[:max(out["ny"], 1)].copy(), z0=z0[:max(out["nz"], 1)].copy(),
+               varname=[names.raw[k * name_len:(k + 1) * name_len].split(b"\0", 1)[0].decode()
+                        for k in range(min(nvar, var_cap))])
+    return out

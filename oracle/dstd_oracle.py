@@ -8,6 +8,9 @@ restatement of the reference's on-disk formats.
 * ctl_file_write (Service/rw_ctl_file.f90:1-139) with the Fortran 2008
   rules for the Ew.d, Gw.d, Iw and Iw.m edit descriptors it uses
   (10.7.2.3.3, 10.7.5.2.2, 10.7.2.2), and sec_to_yr_mo_hr_mn (:161-183).
+* ctl_file_read (Service/rw_ctl_file.f90:185-566) and nonblank (:568-596),
+  with the list-directed input rules its READ statements use
+  (Fortran 2008 10.10.3).
 
 Parity unpinned: no Fortran compiler exists here, so no file written by the
 reference itself is available; these restate the reference's statements.
@@ -163,3 +166,211 @@ def ctl_text(fname, undef, nx, ny, nz, nt, xtype, x0, hx, ytype, y0, hy, ztype, 
     t += varname + " " * 8 + edit_i(nz, 5) + "  1 VARIABLES \n"
     t += "ENDVARS\n\n"
     return namectl, t
+
+
+# ---- ctl_file_read (Service/rw_ctl_file.f90:185-566, nonblank :568-596) ------
+
+class CtlError(ValueError):
+    """The reference prints an error message and returns, or stops on an
+    end of file."""
+
+
+def _f32(x):
+    return float(np.float32(x))
+
+
+def _values(rec):
+    """The values of one list-directed record (blanks/commas separate,
+    quotes delimit, r*c repeats) and whether a slash ended it.  Null values
+    raise."""
+    vals, i, n = [], 0, len(rec)
+    while i < n:
+        commas = 0
+        while i < n and rec[i] in " \t,":
+            commas += rec[i] == ","
+            i += 1
+        if commas > 1:
+            raise CtlError("null value")
+        if i >= n:
+            return vals, False
+        if rec[i] == "/":
+            return vals, True
+        if rec[i] in "'\"":
+            q, j, tok = rec[i], i + 1, ""
+            while j < n:
+                if rec[j] == q and j + 1 < n and rec[j + 1] == q:
+                    tok, j = tok + q, j + 2
+                elif rec[j] == q:
+                    j += 1
+                    break
+                else:
+                    tok, j = tok + rec[j], j + 1
+            vals.append(tok)
+            i = j
+            continue
+        j = i
+        while j < n and rec[j] not in " \t,/":
+            j += 1
+        tok, i = rec[i:j], j
+        head, star, tail = tok.partition("*")
+        if star and head.isdigit():
+            if not tail:
+                raise CtlError("null value")
+            vals += [tail] * int(head)
+        else:
+            vals.append(tok)
+    return vals, False
+
+
+def _int(t):
+    try:
+        return int(t.strip())
+    except ValueError:
+        raise CtlError(f"not an integer: {t!r}") from None
+
+
+def _real(t):
+    u = t.strip().upper().replace("D", "E").replace("Q", "E")
+    if "E" not in u:
+        for k in range(1, len(u)):
+            if u[k] in "+-" and (u[k - 1].isdigit() or u[k - 1] == "."):
+                u = u[:k] + "E" + u[k:]
+                break
+    try:
+        return float(u)
+    except ValueError:
+        raise CtlError(f"not a real: {t!r}") from None
+
+
+def _spelled(s, word):
+    w = s[:len(word)]
+    return w in (word, word.lower(), word.capitalize())
+
+
+def ctl_read(text, datname_len=255, title_len=255):
+    """The output arguments of ctl_file_read on a descriptor's text, as a
+    dict (arguments it does not set are absent).  Raises CtlError where the
+    reference prints an error or stops."""
+    recs = [ln.rstrip("\r")[:256].ljust(256) for ln in text.split("\n")]
+    if text.endswith("\n"):
+        recs.pop()
+    out = {"inform": 0, "datname": "", "yr_type": 1}
+    nxt = 0
+
+    def ext_read(need):
+        """READ(40, *) from the next record on."""
+        nonlocal nxt
+        vals = []
+        while len(vals) < need:
+            if nxt >= len(recs):
+                raise CtlError("end of file")
+            v, slash = _values(recs[nxt])
+            nxt += 1
+            vals += v
+            if slash:
+                break
+        return vals
+
+    for _line in range(512):
+        if nxt >= len(recs):
+            raise CtlError("exit by eof, not by endvars")
+        s = recs[nxt]
+        nxt += 1
+        stripped = s.lstrip(" ")
+        nb = len(s) - len(stripped) + 1            # nonblank(string, 1)
+        if not stripped or nb > len(s) - 5:
+            continue
+        key = s[nb - 1:]
+        vals, _ = _values(s)
+        if _spelled(key, "ENDVARS"):
+            return out
+        if _spelled(key, "VARS"):
+            if len(vals) < 2:
+                raise CtlError("in definition vars or variable name")
+            out["nvar"] = _int(vals[1])
+            out["varname"] = []
+            for _ in range(out["nvar"]):
+                v = ext_read(2)
+                if len(v) < 2:
+                    raise CtlError("in definition vars or variable name")
+                _int(v[1])
+                out["varname"].append(v[0])
+            out["inform"] += 1
+        if _spelled(key, "DSET"):
+            l1 = nb + 4                           # 1-based positions, as the reference
+            while l1 <= 256 and s[l1 - 1] in " ^":
+                l1 += 1
+            l2 = min(256, datname_len + l1 - 1)
+            while l2 >= nb + 4 and s[l2 - 1] == " ":
+                l2 -= 1
+            if l2 < nb + 4:
+                l2 -= 1
+            if l1 > l2:
+                raise CtlError("in definition name of file with data")
+            out["datname"] = s[l1 - 1:l2]
+            out["inform"] += 1
+        if _spelled(key, "TITLE"):
+            out["title"] = s[nb + 4:][:title_len].rstrip(" ")
+            out["inform"] += 1
+        if _spelled(key, "UNDEF"):
+            if len(vals) < 2:
+                raise CtlError("in definition undefinit value")
+            out["undef"] = _f32(_real(vals[1]))
+            out["inform"] += 1
+        if _spelled(key, "OPTIONS"):
+            if len(vals) < 2:
+                raise CtlError("in definition Options")
+            out["inform"] += 1
+            if vals[1][:32][:3] == "365":
+                out["yr_type"] = 0
+        for tag, a in (("XDEF", "x"), ("YDEF", "y"), ("ZDEF", "z")):
+            if not _spelled(key, tag):
+                continue
+            if len(vals) < 3:
+                raise CtlError(f"in definition {a}-grid")
+            n = out["n" + a] = _int(vals[1])
+            gt = vals[2][:32]
+            if gt in ("linear", "LINEAR", "Linear"):
+                out[a + "type"] = 0
+                if len(vals) < 5:
+                    raise CtlError(f"in definition {a}-grid")
+                v0, h = _real(vals[3]), _real(vals[4])
+                # x0(i) = x0(1) + hx*dfloat(i-1); the z axis: z0(1) + hz*dfloat(i)
+                step = (lambda i: i - 1) if a != "z" else (lambda i: i)
+                out[a + "0"] = [v0] + [v0 + h * float(step(i)) for i in range(2, n + 1)]
+                out["h" + a] = h
+                out["inform"] += 1
+            elif gt in ("levels", "LEVELS", "Levels"):
+                out[a + "type"] = 1
+                nxt -= 1                          # BACKSPACE (40)
+                v = ext_read(3 + max(n, 0))
+                _int(v[1])
+                out[a + "0"] = [_real(t) for t in v[3:3 + n]]
+                out["h" + a] = 0.0
+                out["inform"] += 1
+        if _spelled(key, "TDEF"):
+            if len(vals) < 5:
+                raise CtlError("in definition t-grid")
+            out["nt"] = _int(vals[1])
+            if vals[2][:32] in ("linear", "LINEAR", "Linear"):
+                ti, st = vals[3][:32].ljust(32), vals[4][:32].ljust(32)
+                l2 = len(st.rstrip(" ")) or 1
+                out["hour0"], out["minute0"] = _int(ti[0:2]), _int(ti[3:5])
+                out["day0"], out["year0"] = _int(ti[6:8]), _int(ti[11:15])
+                for k, m in enumerate(MONTHS):
+                    if ti[8:11] in (m, m.lower(), m.capitalize()):
+                        out["month0"] = k + 1
+                if l2 < 3:
+                    raise CtlError("in definition t-grid")
+                f = np.float32
+                ht = f(_real(st[:l2 - 2]))
+                unit = st[l2 - 2:l2]
+                mult = {"yr": (365.0, 24.0, 3600.0), "mo": (30.0, 24.0, 3600.0), "dy": (24.0, 3600.0),
+                        "hr": (3600.0,), "mn": (60.0,)}
+                if unit not in mult:
+                    out["ht"] = ht
+                    raise CtlError("in definition time step for t-grid")
+                for m in mult[unit]:
+                    ht = f(ht * f(m))
+                out["ht"] = ht
+    raise CtlError("in definition undefinit value")

@@ -1,7 +1,8 @@
 """On-disk formats: the DIOGIN-standard direct-access files and GrADS
 descriptors of the reference (Service/input_output_data.f90:117-534,
-Service/rw_ctl_file.f90:1-183) through the C ABI, against the oracle's
-restatement (oracle/dstd_oracle.py), byte for byte; the barotropic
+Service/rw_ctl_file.f90:1-596) through the C ABI, against the oracle's
+restatements (oracle/dstd_oracle.py): the files byte for byte, the
+descriptor reader's outputs value for value; the barotropic
 checkpoint and restart (Control/output.f90:1736-1847,
 Control/init_pars.f90:384-411) on the GPU.
 """
@@ -229,3 +230,157 @@ def test_ctl_number_editing_edge_cases(tmp_path):
     assert od.edit_g(99999999.4, 15, 8) == "  99999999.    "
     assert od.edit_g(9.999999995, 15, 8) == "  10.000000    "
     assert od.edit_g(1.0e100, 15, 8) == " 0.10000000+101"
+
+
+# ---- the descriptor reader (Service/rw_ctl_file.f90:185-566) -----------------
+
+def _read_both(tmp_path, text, name="d.ctl", **kw):
+    """The library's ctl_file_read and the oracle's on the same text: both
+    fail or both give the same outputs (exactly).  Returns the library's."""
+    p = tmp_path / name
+    p.write_text(text)
+    try:
+        want = od.ctl_read(text)
+    except od.CtlError:
+        with pytest.raises(InmsomError) as e:
+            dstd.ctl_file_read(p, **kw)
+        assert e.value.code == 2
+        return None
+    got = dstd.ctl_file_read(p, **kw)
+    for k, v in want.items():
+        if k in ("x0", "y0", "z0"):
+            assert np.array_equal(got[k][:len(v)], np.asarray(v, dtype=np.float64)), k
+        elif k == "undef":
+            assert np.float32(got[k]) == np.float32(v), k
+        else:
+            assert got[k] == v, (k, got[k], v)
+    return got
+
+
+@pytest.mark.parametrize("case", range(len(CTL_CASES)))
+def test_ctl_read_round_trip(tmp_path, case):
+    """What ctl_file_write writes, ctl_file_read reads back: the axes to the
+    eight significant digits of G15.8, the calendar, the step in the unit
+    the writer chose."""
+    c = CTL_CASES[case]
+    fname = str(tmp_path / "cpsshe.dat")
+    y, mo, d, h, mn = c["date"]
+    dstd.ctl_file_write(fname, -1.0e32, c["nx"], c["ny"], c["nz"], c["nt"], c["xtype"], c["x0"], c["hx"],
+                        c["ytype"], c["y0"], c["hy"], c["ztype"], c["z0"], c["hz"], c["yr_type"], y, mo, d, h, mn,
+                        c["ht"], c["title"], c["var"])
+    text = (tmp_path / "cpsshe.ctl").read_text()
+    got = _read_both(tmp_path, text, name="cpsshe.ctl")
+    if c["ht"] < 60.0:
+        assert got is None       # a step under a minute has no unit to read back
+        return
+    assert got["inform"] == 8 - (c["yr_type"] == 1)
+    assert got["datname"] == "cpsshe.dat" and got["title"] == "    " + c["title"]
+    assert got["undef"] == np.float32(-1.0e32)
+    for a, n in (("x", c["nx"]), ("y", c["ny"]), ("z", c["nz"])):
+        assert got["n" + a] == n and got[a + "type"] == c[a + "type"]
+        if c[a + "type"] == 1:
+            np.testing.assert_allclose(got[a + "0"], c[a + "0"], rtol=5e-8, atol=1e-300)
+        else:
+            np.testing.assert_allclose(got[a + "0"][0], c[a + "0"][0], rtol=5e-8)
+            np.testing.assert_allclose(got["h" + a], c["h" + a], rtol=5e-8)
+    assert got["nt"] == c["nt"] and got["yr_type"] == c["yr_type"]
+    assert (got["year0"], got["month0"], got["day0"], got["hour0"], got["minute0"]) == c["date"]
+    assert got["nvar"] == 1 and got["varname"] == [c["var"]]
+    want_ht = {86400.0: 86400.0, 6 * 3600.0: 21600.0, 30 * 86400.0: 2592000.0, 90.0: 60.0}[c["ht"]]
+    assert got["ht"] == np.float32(want_ht)
+
+
+HAND_CTL = """dset ^../data/run 1/temp.dat
+title   Model   output
+undef -9.99e8
+options 365_day_calendar
+xdef 10 linear 0 1.5
+Ydef 3 levels
+  -10.0, 0.0 10.0
+zdef 4 LINEAR 1.0 2.0
+tdef 24 linear 12:30z15jul1999 3hr
+VARS 2
+t  4  99 temperature
+'sal inity'  4  99 salinity
+ENDVARS
+"""
+
+
+def test_ctl_read_by_hand(tmp_path):
+    """A descriptor in lower and capitalised keywords, worked out by hand:
+    the DSET name after '^' with its inner blank, TITLE from the fifth
+    character after the keyword, the LEVELS values on the next line, the
+    z axis filled as z0(1) + hz*i, the month in lower case."""
+    got = _read_both(tmp_path, HAND_CTL)
+    assert got["datname"] == "../data/run 1/temp.dat"
+    assert got["title"] == "   Model   output"
+    assert got["undef"] == np.float32(-9.99e8) and got["yr_type"] == 0
+    assert got["nx"] == 10 and got["xtype"] == 0 and np.array_equal(got["x0"], 1.5 * np.arange(10))
+    assert got["ytype"] == 1 and np.array_equal(got["y0"], [-10.0, 0.0, 10.0]) and got["hy"] == 0.0
+    assert got["ztype"] == 0 and np.array_equal(got["z0"], [1.0, 5.0, 7.0, 9.0])
+    assert (got["nt"], got["hour0"], got["minute0"], got["day0"], got["month0"], got["year0"]) == \
+        (24, 12, 30, 15, 7, 1999)
+    assert got["ht"] == np.float32(10800.0)
+    assert got["nvar"] == 2 and got["varname"] == ["t", "sal inity"] and got["inform"] == 8
+
+
+@pytest.mark.parametrize("text, check", [
+    # the step units in single precision
+    ("TDEF 1 LINEAR 00:00Z01JAN2000 2yr\nENDVARS\n", lambda g: g["ht"] == np.float32(2 * 365 * 86400.0)),
+    ("TDEF 1 LINEAR 00:00Z01Feb2000 1mo\nENDVARS\n", lambda g: g["ht"] == np.float32(2592000.0) and g["month0"] == 2),
+    ("TDEF 1 LINEAR 00:00Z01DEC2000 0.1dy\nENDVARS\n",
+     lambda g: g["ht"] == np.float32(np.float32(np.float32(0.1) * np.float32(24.0)) * np.float32(3600.0))),
+    ("TDEF 1 LINEAR 00:00Z01DEC2000 45mn\nENDVARS\n", lambda g: g["ht"] == np.float32(2700.0)),
+    # TDEF is not counted in inform; a non-linear time axis leaves the calendar unread
+    ("TDEF 5 levels 1 2\nENDVARS\n", lambda g: g["nt"] == 5 and g["inform"] == 0 and g["ht"] == 0),
+    # Fortran real forms: a D exponent, a signed exponent with no letter, r*c repeats
+    ("UNDEF -1.0D+30\nXDEF 3 LEVELS 0.1+101 1.5-3 2*7\nENDVARS\n",
+     lambda g: g["undef"] == np.float32(-1.0e30) and list(g["x0"]) == [1.0e100, 1.5e-3, 7.0]),
+    ("ZDEF 4 LEVELS 4*2.5\nENDVARS\n", lambda g: list(g["z0"]) == [2.5] * 4),
+    # a slash ends the LEVELS read: the values it did not reach stay as they were
+    ("XDEF 5 LEVELS 1 2 3 /\nENDVARS\n", lambda g: list(g["x0"]) == [1.0, 2.0, 3.0, 0.0, 0.0]),
+    # keywords in other spellings are not keywords
+    ("xDef 4 LINEAR 0 1\nENDVARS\n", lambda g: g["nx"] == 0 and g["inform"] == 0),
+    # nonblank: a first non-blank past column 251 makes the record blank
+    (" " * 251 + "UNDEF\nENDVARS\n", lambda g: g["inform"] == 0),
+    # blank lines and '^' runs before the name
+    ("\n\n   DSET  ^^ ^a.dat   \nENDVARS\n", lambda g: g["datname"] == "a.dat" and g["inform"] == 1),
+    # OPTIONS other than 365... keep the leap-year calendar but count
+    ("OPTIONS template\nENDVARS\n", lambda g: g["yr_type"] == 1 and g["inform"] == 1),
+    # ENDVARS in its three spellings ends the read; later lines are not read
+    ("Endvars\nUNDEF 5\n", lambda g: g["inform"] == 0 and g["undef"] == 0),
+])
+def test_ctl_read_rules(tmp_path, text, check):
+    got = _read_both(tmp_path, text)
+    assert got is not None and check(got)
+
+
+@pytest.mark.parametrize("text", [
+    "UNDEF 5\n",                                          # end of file before ENDVARS
+    " " * 250 + "UNDEF\nENDVARS\n",                       # column 251 is read: no value
+    "TDEF 1 LINEAR 00:00Z01JAN2000 3wk\nENDVARS\n",       # no such unit
+    "TDEF 1 LINEAR 00:00Z01JAN2000 hr\nENDVARS\n",        # no count before the unit
+    "XDEF 3 LEVELS 1 2\n",                                # LEVELS runs into the end of file
+    "VARS 2\nt 1\nENDVARS\n",                             # the second name takes ENDVARS; the file ends before its integer
+    "DSET ^^^\nENDVARS\n",                                # no name
+    "XDEF 3 LINEAR 1,,2\nENDVARS\n",                      # a null value
+    "\n" * 512 + "ENDVARS\n",                             # 512 records without ENDVARS
+])
+def test_ctl_read_errors(tmp_path, text):
+    assert _read_both(tmp_path, text) is None
+
+
+def test_ctl_read_limits(tmp_path):
+    # 511 blank records and ENDVARS are within the 512 the reference reads
+    assert _read_both(tmp_path, "\n" * 511 + "ENDVARS\n")["inform"] == 0
+    # the unit's value is kept when the unit is unknown (the reference sets
+    # ht before it checks the unit); a name is cut to its variable's length
+    (tmp_path / "n.ctl").write_text("DSET abcdefghij\nENDVARS\n")
+    assert dstd.ctl_file_read(tmp_path / "n.ctl", name_len=8)["datname"] == "abcdefg"
+    (tmp_path / "n.ctl").write_text("XDEF 9 LEVELS 1 2 3 4 5 6 7 8 9\nENDVARS\n")
+    with pytest.raises(InmsomError) as e:
+        dstd.ctl_file_read(tmp_path / "n.ctl", x_cap=8)
+    assert e.value.code == 2
+    with pytest.raises(InmsomError) as e:
+        dstd.ctl_file_read(tmp_path / "missing.ctl")
+    assert e.value.code == 6
