@@ -400,6 +400,28 @@ int inmsom_rdstd8(const char *path, const char *fname, int nfield, double *field
 int inmsom_rdstd(const char *path, const char *fname, int nfield, float *field, const float *lu, int nx, int ny,
                  int nz, int nxb, int nxe, int nyb, int nye, int nzb, int nze);
 
+/* The MPI-IO forms prdstd / pwdstd (Service/input_output_data.f90:535-652,
+ * :657-819), same arguments with the rank's bounds first (the reference
+ * takes them from mpi_parallel_tools): fild(bnd_x1:bnd_x2, bnd_y1:bnd_y2,
+ * nz) and lu(bnd_x1:bnd_x2, bnd_y1:bnd_y2) are the rank's local FP32
+ * arrays; nx, ny, nz and the box are global.  Each rank transfers only its
+ * interior nx_start..nx_end x ny_start..ny_end of levels nzb..nze, which
+ * must lie inside the box, at the place the single-process wdstd record
+ * layout gives it (field nfild after (nfild-1) * (nze-nzb+1) records of
+ * (nxe-nxb+1)*(nye-nyb+1) values), so the ranks together write or read the
+ * same file as wdstd / rdstd.  Ranks call these independently: the writes
+ * and reads are positioned on disjoint byte ranges, no collective.  As the
+ * reference: pwdstd sets the land points (|lu| < 0.5) of the rank's
+ * interior to undef = -1.0e32 in fild, and writes them so; the file is not
+ * truncated; prdstd reads every point (lu unused) and leaves values past
+ * the end of the file as they were.  Errors (the reference aborts):
+ * INMSOM_EARG (no file name, box outside nx/ny/nz, interior outside the
+ * box), INMSOM_EIO. */
+int inmsom_pwdstd(const inmsom_bounds *b, const char *path, const char *fname, int nfild, float *fild,
+                  const float *lu, int nx, int ny, int nz, int nxb, int nxe, int nyb, int nye, int nzb, int nze);
+int inmsom_prdstd(const inmsom_bounds *b, const char *path, const char *fname, int nfild, float *fild,
+                  const float *lu, int nx, int ny, int nz, int nxb, int nxe, int nyb, int nye, int nzb, int nze);
+
 /* The GrADS descriptor of Service/rw_ctl_file.f90:1-139 ctl_file_write,
  * same arguments: writes <fname with .ctl> describing <fname with .dat>,
  * line by line as the reference's formatted WRITE statements (e12.5,

@@ -32,6 +32,7 @@ EXPORTS = (
     "inmsom_baroclinic_dynamics", "inmsom_vertical_velocity", "inmsom_depth_ave", "inmsom_shift_barotropic",
     "inmsom_wdstd8", "inmsom_wdstd", "inmsom_rdstd8", "inmsom_rdstd", "inmsom_ctl_file_write",
     "inmsom_write_checkpoint", "inmsom_read_checkpoint", "inmsom_tracer_tran_diff", "inmsom_ctl_file_read",
+    "inmsom_pwdstd", "inmsom_prdstd",
 )
 
 # include/inmsom_gpu.h: INMSOM_MLP_*
@@ -139,6 +140,8 @@ def load() -> ctypes.CDLL:
     cp = ctypes.c_char_p
     for nm, ptr in (("inmsom_wdstd8", DP), ("inmsom_wdstd", FP), ("inmsom_rdstd8", DP), ("inmsom_rdstd", FP)):
         getattr(lib, nm).argtypes = [cp, cp, i, ptr, FP] + [i] * 9
+    for nm in ("inmsom_pwdstd", "inmsom_prdstd"):
+        getattr(lib, nm).argtypes = [ctypes.POINTER(CBounds), cp, cp, i, FP, FP] + [i] * 9
     lib.inmsom_ctl_file_write.argtypes = [cp, ctypes.c_float, i, i, i, i, i, DP, d, i, DP, d, i, DP, d,
                                           i, i, i, i, i, i, ctypes.c_float, cp, cp]
     lib.inmsom_write_checkpoint.argtypes = [VP, cp, ctypes.POINTER(CCtlAxes)]

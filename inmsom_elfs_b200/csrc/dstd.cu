@@ -4,6 +4,9 @@
 //    FP64 (wdstd8/rdstd8), record (nfield-1)*(nze-nzb+1) + k-nzb+1, land
 //    points (|lu| < 0.5) written as undef = -1.0e32 and read back as 0
 //    (Service/input_output_data.f90:117-534; Inc/reclen.fi);
+//  * prdstd / pwdstd, the MPI-IO forms (Service/input_output_data.f90:535-819):
+//    each rank reads or writes its own interior of the same FP32 file, by
+//    positioned I/O on disjoint byte ranges instead of a collective;
 //  * the GrADS descriptor ctl_file_write (Service/rw_ctl_file.f90:1-183)
 //    with the Fortran edit descriptors of its WRITE statements;
 //  * the checkpoint of the barotropic state and its restart
@@ -142,6 +145,64 @@ int read_std(const char *path, const char *fname, int nfield, T *field, const fl
     }
     close(fd);
     return rc;
+}
+
+// ---- prdstd / pwdstd: one rank's subdomain of the file ---------------------
+
+// Where one rank's interior (nx_start..nx_end, ny_start..ny_end) of levels
+// nzb..nze sits in the file: the MPI subarray view of
+// Service/input_output_data.f90:583-611 / 706-772 (global sizes = the box,
+// local sizes = the interior, offsets = interior start - box start) after
+// the displacement bx*by*4*(nfild-1)*bz bytes.
+struct SubView {
+    long long bx, by, bz;       // the box
+    long long lx, ly, ox, oy;   // the rank's part of it
+    long long disp;             // bytes before field nfild
+    long long nxa, nya;         // the rank's local arrays (bnd_x1:bnd_x2, bnd_y1:bnd_y2)
+};
+
+int sub_view(const inmsom_bounds *b, int nfild, int nx, int ny, int nz, int nxb, int nxe, int nyb, int nye, int nzb,
+             int nze, SubView &v, const char *who)
+{
+    if (!b || nfild < 1) return fail(INMSOM_EARG, "%s: bad argument", who);
+    if (b->nx_start > b->nx_end || b->ny_start > b->ny_end || b->bnd_x1 > b->nx_start || b->bnd_x2 < b->nx_end ||
+        b->bnd_y1 > b->ny_start || b->bnd_y2 < b->ny_end)
+        return fail(INMSOM_EARG, "%s: interior %d..%d x %d..%d outside the arrays %d..%d x %d..%d", who, b->nx_start,
+                    b->nx_end, b->ny_start, b->ny_end, b->bnd_x1, b->bnd_x2, b->bnd_y1, b->bnd_y2);
+    // ierr = 1, 2, 3 of the reference (then mpi_abort)
+    if (nxe > nx || nxb < 1 || nxb > nxe) return fail(INMSOM_EARG, "%s: error in grid diapason of 1 - coordinate", who);
+    if (nye > ny || nyb < 1 || nyb > nye) return fail(INMSOM_EARG, "%s: error in grid diapason of 2 - coordinate", who);
+    if (nze > nz || nzb < 1 || nzb > nze) return fail(INMSOM_EARG, "%s: error in grid diapason of 3 - coordinate", who);
+    v.bx = nxe - nxb + 1;
+    v.by = nye - nyb + 1;
+    v.bz = nze - nzb + 1;
+    v.lx = b->nx_end - b->nx_start + 1;
+    v.ly = b->ny_end - b->ny_start + 1;
+    v.ox = b->nx_start - nxb;
+    v.oy = b->ny_start - nyb;
+    // MPI_Type_create_subarray refuses a part that leaves the box
+    if (v.ox < 0 || v.oy < 0 || v.ox + v.lx > v.bx || v.oy + v.ly > v.by)
+        return fail(INMSOM_EARG, "%s: the interior %d..%d x %d..%d is not inside the box %d..%d x %d..%d", who,
+                    b->nx_start, b->nx_end, b->ny_start, b->ny_end, nxb, nxe, nyb, nye);
+    // 64-bit: the reference forms this product in default integers
+    v.disp = v.bx * v.by * 4LL * (long long)(nfild - 1) * v.bz;
+    v.nxa = b->bnd_x2 - b->bnd_x1 + 1;
+    v.nya = b->bnd_y2 - b->bnd_y1 + 1;
+    return INMSOM_OK;
+}
+
+// the rank's part of level kr (0-based in the box) as runs of contiguous
+// bytes: one run when the part spans whole rows of the box, else one per row
+template <typename F>
+int for_runs(const SubView &v, long long kr, F &&run)
+{
+    const long long lvl = v.disp + 4LL * kr * v.bx * v.by;
+    if (v.lx == v.bx) return run(lvl + 4LL * v.oy * v.bx, 0LL, v.lx * v.ly);
+    for (long long j = 0; j < v.ly; j++) {
+        const int rc = run(lvl + 4LL * ((v.oy + j) * v.bx + v.ox), j * v.lx, v.lx);
+        if (rc != INMSOM_OK) return rc;
+    }
+    return INMSOM_OK;
 }
 
 // ---- Fortran edit descriptors of ctl_file_write ----------------------------
@@ -306,6 +367,87 @@ int inmsom_rdstd(const char *path, const char *fname, int nfield, float *field, 
 {
     return read_std<float>(path, fname, nfield, field, lu, nx, ny, nz, nxb, nxe, nyb, nye, nzb, nze,
                            "inmsom_rdstd");
+}
+
+int inmsom_pwdstd(const inmsom_bounds *b, const char *path, const char *fname, int nfild, float *fild,
+                  const float *lu, int nx, int ny, int nz, int nxb, int nxe, int nyb, int nye, int nzb, int nze)
+{
+    const char *who = "inmsom_pwdstd";
+    std::string name;
+    if (!fulfname(name, path, fname)) return fail(INMSOM_EARG, "%s: error in full name of file for writing", who);
+    if (!fild || !lu) return fail(INMSOM_EARG, "%s: NULL array", who);
+    SubView v;
+    const int rc0 = sub_view(b, nfild, nx, ny, nz, nxb, nxe, nyb, nye, nzb, nze, v, who);
+    if (rc0 != INMSOM_OK) return rc0;
+    auto at = [&](int i, int j, int k) -> float & {
+        return fild[(size_t)(i - b->bnd_x1) + (size_t)v.nxa * ((size_t)(j - b->bnd_y1) + (size_t)v.nya * (k - 1))];
+    };
+    // the land points of the interior become undef in the caller's array
+    for (int j = b->ny_start; j <= b->ny_end; j++)
+        for (int i = b->nx_start; i <= b->nx_end; i++)
+            if (std::fabs(lu[(size_t)(i - b->bnd_x1) + (size_t)v.nxa * (size_t)(j - b->bnd_y1)]) < 0.5f)
+                for (int k = nzb; k <= nze; k++) at(i, j, k) = UNDEF;
+    const int fd = open(name.c_str(), O_WRONLY | O_CREAT, 0644);    // mpi_mode_wronly + mpi_mode_create
+    if (fd < 0) return fail(INMSOM_EIO, "%s: error in open file for writing: %s", who, name.c_str());
+    std::vector<float> part((size_t)(v.lx * v.ly));
+    int rc = INMSOM_OK;
+    for (int k = nzb; k <= nze && rc == INMSOM_OK; k++) {
+        size_t q = 0;
+        for (int j = b->ny_start; j <= b->ny_end; j++)
+            for (int i = b->nx_start; i <= b->nx_end; i++) part[q++] = at(i, j, k);
+        rc = for_runs(v, k - nzb, [&](long long off, long long first, long long n) {
+            const ssize_t want = (ssize_t)(4 * n);
+            if (pwrite(fd, part.data() + first, (size_t)want, (off_t)off) != want)
+                return fail(INMSOM_EIO, "%s: error in writing level %d of %s", who, k, name.c_str());
+            return (int)INMSOM_OK;
+        });
+    }
+    if (close(fd) != 0 && rc == INMSOM_OK) rc = fail(INMSOM_EIO, "%s: error closing %s", who, name.c_str());
+    return rc;
+}
+
+int inmsom_prdstd(const inmsom_bounds *b, const char *path, const char *fname, int nfild, float *fild,
+                  const float *lu, int nx, int ny, int nz, int nxb, int nxe, int nyb, int nye, int nzb, int nze)
+{
+    (void)lu;   // prdstd takes the mask but reads every point
+    const char *who = "inmsom_prdstd";
+    std::string name;
+    if (!fulfname(name, path, fname)) return fail(INMSOM_EARG, "%s: error in full name of file for reading", who);
+    if (!fild) return fail(INMSOM_EARG, "%s: NULL array", who);
+    SubView v;
+    const int rc0 = sub_view(b, nfild, nx, ny, nz, nxb, nxe, nyb, nye, nzb, nze, v, who);
+    if (rc0 != INMSOM_OK) return rc0;
+    const int fd = open(name.c_str(), O_RDONLY);                    // mpi_mode_rdonly
+    if (fd < 0) return fail(INMSOM_EIO, "%s: error in open file for reading: %s", who, name.c_str());
+    std::vector<float> part((size_t)(v.lx * v.ly));
+    int rc = INMSOM_OK;
+    for (int k = nzb; k <= nze && rc == INMSOM_OK; k++) {
+        // what lies past the end of the file is not read, as MPI-IO reads
+        // (the reference does not look at the count read): keep those values
+        size_t q = 0;
+        for (int j = b->ny_start; j <= b->ny_end; j++)
+            for (int i = b->nx_start; i <= b->nx_end; i++)
+                part[q++] = fild[(size_t)(i - b->bnd_x1) +
+                                 (size_t)v.nxa * ((size_t)(j - b->bnd_y1) + (size_t)v.nya * (k - 1))];
+        rc = for_runs(v, k - nzb, [&](long long off, long long first, long long n) {
+            char *dst = reinterpret_cast<char *>(part.data() + first);
+            long long got = 0;
+            while (got < 4 * n) {
+                const ssize_t r = pread(fd, dst + got, (size_t)(4 * n - got), (off_t)(off + got));
+                if (r < 0) return fail(INMSOM_EIO, "%s: error in reading level %d of %s", who, k, name.c_str());
+                if (r == 0) break;
+                got += r;
+            }
+            return (int)INMSOM_OK;
+        });
+        q = 0;
+        for (int j = b->ny_start; j <= b->ny_end; j++)
+            for (int i = b->nx_start; i <= b->nx_end; i++)
+                fild[(size_t)(i - b->bnd_x1) + (size_t)v.nxa * ((size_t)(j - b->bnd_y1) + (size_t)v.nya * (k - 1))] =
+                    part[q++];
+    }
+    close(fd);
+    return rc;
 }
 
 int inmsom_ctl_file_write(const char *fname, float undef, int nx, int ny, int nz, int nt, int xtype, const double *x0,

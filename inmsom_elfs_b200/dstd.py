@@ -2,7 +2,9 @@
 
 DIOGIN-standard direct-access files (Service/input_output_data.f90:117-534):
 one record per level of a box of a field, x fastest, FP64 (wdstd8/rdstd8)
-or FP32 (wdstd/rdstd), land points written as undef = -1.0e32 and read as 0.
+or FP32 (wdstd/rdstd), land points written as undef = -1.0e32 and read as 0;
+their MPI-IO forms pwdstd/prdstd (:535-819), one rank's subdomain of the
+same FP32 file.
 GrADS descriptors (Service/rw_ctl_file.f90:1-139 ctl_file_write and
 :185-566 ctl_file_read).  Arrays are Fortran-ordered numpy arrays (nx, ny[,
 nz]); boxes are 1-based inclusive (nxb, nxe, nyb, nye, nzb, nze) as in the
@@ -98,3 +100,33 @@ def ctl_file_read(ctlname, x_cap=4096, y_cap=4096, z_cap=1024, var_cap=16, name_
                varname=[names.raw[k * name_len:(k + 1) * name_len].split(b"\0", 1)[0].decode()
                         for k in range(min(nvar, var_cap))])
     return out
+
+
+def _pcall(name, bounds, path, fname, nfild, fild, lu, nx, ny, nz, box):
+    from ._lib import cbounds
+    if fild.dtype != np.float32 or not fild.flags.f_contiguous:
+        raise TypeError(f"{name}: expected a Fortran-ordered float32 array")
+    if fild.shape[:2] != bounds.shape:
+        raise ValueError(f"{name}: the local array must have the bounds' shape {bounds.shape}")
+    lu = np.asfortranarray(lu, dtype=np.float32)
+    if lu.shape != bounds.shape:
+        raise ValueError(f"{name}: lu must have the bounds' shape {bounds.shape}")
+    cb = cbounds(bounds)
+    check(getattr(load(), name)(ctypes.byref(cb), path.encode(), fname.encode(), int(nfild), fild.ctypes.data_as(FP),
+                                lu.ctypes.data_as(FP), int(nx), int(ny), int(nz), *box))
+    return fild
+
+
+def pwdstd(bounds, path, fname, nfild, fild, lu, nx, ny, nz, box):
+    """inmsom_pwdstd (Service/input_output_data.f90:657-819): this rank's
+    interior of the local float32 array fild (bounds.shape[+ (nz,)]) into
+    the file every rank shares; nx, ny, nz and the 1-based box are global.
+    Like the reference, sets the interior's land points of fild to undef."""
+    return _pcall("inmsom_pwdstd", bounds, path, fname, nfild, fild, lu, nx, ny, nz, box)
+
+
+def prdstd(bounds, path, fname, nfild, fild, lu, nx, ny, nz, box):
+    """inmsom_prdstd (Service/input_output_data.f90:535-652): this rank's
+    interior of fild from the shared file (every point; values past the
+    end of the file are left as they were)."""
+    return _pcall("inmsom_prdstd", bounds, path, fname, nfild, fild, lu, nx, ny, nz, box)

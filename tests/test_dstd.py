@@ -1,7 +1,8 @@
 """On-disk formats: the DIOGIN-standard direct-access files and GrADS
 descriptors of the reference (Service/input_output_data.f90:117-534,
 Service/rw_ctl_file.f90:1-596) through the C ABI, against the oracle's
-restatements (oracle/dstd_oracle.py): the files byte for byte, the
+restatements (oracle/dstd_oracle.py): the files byte for byte (the MPI-IO
+forms prdstd/pwdstd through several ranks, gloo processes included), the
 descriptor reader's outputs value for value; the barotropic
 checkpoint and restart (Control/output.f90:1736-1847,
 Control/init_pars.f90:384-411) on the GPU.
@@ -384,3 +385,151 @@ def test_ctl_read_limits(tmp_path):
     with pytest.raises(InmsomError) as e:
         dstd.ctl_file_read(tmp_path / "missing.ctl")
     assert e.value.code == 6
+
+
+# ---- the MPI-IO forms (Service/input_output_data.f90:535-819) ----------------
+
+def _rank_grid(g, xs, ys):
+    """Local bounds of a process grid: interior x ranges xs, y ranges ys
+    (global indices), arrays with the two-point halo."""
+    from dataclasses import replace
+    return [replace(g, nx_start=a, nx_end=b, ny_start=c, ny_end=d, bnd_x1=a - 2, bnd_x2=b + 2, bnd_y1=c - 2,
+                    bnd_y2=d + 2) for (c, d) in ys for (a, b) in xs]
+
+
+def _local(a, g, lb):
+    return np.asfortranarray(a[lb.bnd_x1 - g.bnd_x1:lb.bnd_x2 - g.bnd_x1 + 1,
+                               lb.bnd_y1 - g.bnd_y1:lb.bnd_y2 - g.bnd_y1 + 1].copy())
+
+
+def _pglobal(seed=11, nz=3):
+    from inmsom_elfs_b200.grid import Bounds
+    g = Bounds.serial(11, 9)
+    f, lu = _case(seed, nx=g.shape[0], ny=g.shape[1], nz=nz)
+    return g, np.asfortranarray(f.astype(np.float32)), lu
+
+
+def test_pwdstd_ranks_write_the_wdstd_file(tmp_path):
+    """Four ranks of a 2 x 2 process grid (uneven parts) write fields 1 and
+    2, levels 2..3, of the global interior: the file is byte for byte the
+    one wdstd writes for the global field, the ranks' land points are undef
+    in their arrays and nothing outside their interiors changes."""
+    g, f1, lu = _pglobal(11)
+    _, f2, _ = _pglobal(12)
+    nx, ny, nz = f1.shape
+    box = (g.mmm, g.mm, g.nnn, g.nn, 2, 3)
+    ranks = _rank_grid(g, [(3, 7), (8, 13)], [(3, 6), (7, 11)])
+    for nfild, f in ((2, f2), (1, f1)):             # the ranks and fields in any order
+        for lb in reversed(ranks):
+            loc = _local(f, g, lb)
+            before = loc.copy()
+            dstd.pwdstd(lb, str(tmp_path), "p.dat", nfild, loc, _local(lu, g, lb), nx, ny, nz, box)
+            inner = np.zeros(loc.shape, bool)
+            inner[2:-2, 2:-2, 1:3] = True
+            land = inner & (np.abs(_local(lu, g, lb)) < 0.5)[..., None]
+            assert np.all(loc[land] == od.UNDEF) and np.array_equal(loc[~land], before[~land])
+    assert (tmp_path / "p.dat").read_bytes() == _expected_file([(1, f1), (2, f2)], lu, box, np.float32)
+
+
+def test_prdstd_reads_each_rank_part(tmp_path):
+    """prdstd of each rank gives its interior of the wdstd file (undef at
+    land, not 0 as rdstd gives) and leaves the rest of its array alone;
+    values past the end of a short file stay as they were."""
+    g, f, lu = _pglobal(13)
+    nx, ny, nz = f.shape
+    box = (g.mmm, g.mm, g.nnn, g.nn, 1, 3)
+    dstd.wdstd(str(tmp_path), "w.dat", 1, f.copy(order="F"), lu, box)
+    want = f.copy(order="F")
+    want[np.broadcast_to((np.abs(lu) < 0.5)[..., None], want.shape)] = od.UNDEF
+    for lb in _rank_grid(g, [(3, 13)], [(3, 4), (5, 11)]) + _rank_grid(g, [(3, 9), (10, 13)], [(3, 11)]):
+        loc = np.full(lb.shape + (nz,), 7.0, np.float32, order="F")
+        dstd.prdstd(lb, str(tmp_path), "w.dat", 1, loc, _local(lu, g, lb), nx, ny, nz, box)
+        exp = np.full_like(loc, 7.0)
+        exp[2:-2, 2:-2, :] = _local(want, g, lb)[2:-2, 2:-2, :]
+        assert np.array_equal(loc, exp)
+    # a file that ends inside level 2 of the top strip
+    data = (tmp_path / "w.dat").read_bytes()
+    bx, by = g.mm - g.mmm + 1, g.nn - g.nnn + 1
+    cut = 4 * (bx * by + bx * 7 + 3)                  # level 2, row 8 of the box, three values in
+    (tmp_path / "s.dat").write_bytes(data[:cut])
+    lb = _rank_grid(g, [(3, 13)], [(5, 11)])[0]
+    loc = np.full(lb.shape + (nz,), 7.0, np.float32, order="F")
+    dstd.prdstd(lb, str(tmp_path), "s.dat", 1, loc, _local(lu, g, lb), nx, ny, nz, box)
+    w = _local(want, g, lb)
+    assert np.array_equal(loc[2:-2, 2:-2, 0], w[2:-2, 2:-2, 0])
+    lvl2 = loc[2:-2, 2:-2, 1]                          # box rows 3..9 of this strip; row 8 is local row 5
+    assert np.array_equal(lvl2[:, :5], w[2:-2, 2:7, 1])
+    assert np.array_equal(lvl2[:3, 5], w[2:5, 7, 1]) and np.all(lvl2[3:, 5] == 7.0) and np.all(lvl2[:, 6:] == 7.0)
+    assert np.all(loc[2:-2, 2:-2, 2] == 7.0)
+
+
+def test_parallel_forms_errors(tmp_path):
+    g, f, lu = _pglobal(14)
+    nx, ny, nz = f.shape
+    lb = _rank_grid(g, [(3, 13)], [(3, 11)])[0]
+    loc = _local(f, g, lb)
+    for box in [(4, 13, 3, 11, 1, 1),                 # the interior starts before the box
+                (3, 12, 3, 11, 1, 1),                 # ... and ends after it
+                (3, nx + 1, 3, 11, 1, 1),             # the box leaves the global field
+                (3, 13, 3, 11, 2, 1)]:
+        with pytest.raises(InmsomError) as e:
+            dstd.pwdstd(lb, str(tmp_path), "e.dat", 1, loc.copy(order="F"), _local(lu, g, lb), nx, ny, nz, box)
+        assert e.value.code == 2
+    with pytest.raises(InmsomError) as e:
+        dstd.pwdstd(lb, str(tmp_path), "  ", 1, loc.copy(order="F"), _local(lu, g, lb), nx, ny, nz,
+                    (3, 13, 3, 11, 1, 1))
+    assert e.value.code == 2
+    with pytest.raises(InmsomError) as e:
+        dstd.prdstd(lb, str(tmp_path), "none.dat", 1, loc, _local(lu, g, lb), nx, ny, nz, (3, 13, 3, 11, 1, 1))
+    assert e.value.code == 6
+    assert not (tmp_path / "e.dat").exists()
+
+
+def _pw_rank(rank, world, port, path, q):
+    import os
+    import torch.distributed as dist
+    from inmsom_elfs_b200.strips import strip_bounds
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        g, f, lu = _pglobal(15)
+        nx, ny, nz = f.shape
+        lb = strip_bounds(g, world)[rank]
+        box = (g.mmm, g.mm, g.nnn, g.nn, 1, nz)
+        dstd.pwdstd(lb, path, "cp.dat", 3, _local(f, g, lb), _local(lu, g, lb), nx, ny, nz, box)
+        dist.barrier()
+        loc = np.zeros(lb.shape + (nz,), np.float32, order="F")
+        dstd.prdstd(lb, path, "cp.dat", 3, loc, _local(lu, g, lb), nx, ny, nz, box)
+        q.put((rank, loc[2:-2, 2:-2].copy()))
+    finally:
+        dist.destroy_process_group()
+
+
+@pytest.mark.parametrize("world", [2, 3])
+def test_pwdstd_gloo_ranks(tmp_path, world):
+    """One process per strip (gloo ranks): each writes its strip of field 3
+    with no collective on the data, then reads it back; the file is the
+    wdstd file of the global field."""
+    import socket
+    import torch.multiprocessing as mp
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        port = s.getsockname()[1]
+    ctx = mp.get_context("spawn")
+    q = ctx.Queue()
+    procs = [ctx.Process(target=_pw_rank, args=(r, world, port, str(tmp_path), q)) for r in range(world)]
+    for p in procs:
+        p.start()
+    got = dict(q.get(timeout=120) for _ in range(world))
+    for p in procs:
+        p.join(timeout=60)
+        assert p.exitcode == 0
+    g, f, lu = _pglobal(15)
+    box = (g.mmm, g.mm, g.nnn, g.nn, 1, f.shape[2])
+    want = _expected_file([(3, f)], lu, box, np.float32)
+    assert (tmp_path / "cp.dat").read_bytes() == want
+    from inmsom_elfs_b200.strips import strip_bounds
+    full = f.copy(order="F")
+    full[np.broadcast_to((np.abs(lu) < 0.5)[..., None], full.shape)] = od.UNDEF
+    for r, lb in enumerate(strip_bounds(g, world)):
+        assert np.array_equal(got[r], _local(full, g, lb)[2:-2, 2:-2])
