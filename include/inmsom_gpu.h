@@ -468,6 +468,39 @@ typedef struct inmsom_ctl_axes {
     float tstep;
 } inmsom_ctl_axes;
 
+/* The prognostic fields of the reference's checkpoint: column-major host
+ * arrays over (bnd_x1:bnd_x2, bnd_y1:bnd_y2), with nz levels (tt .. vvp),
+ * nz+1 levels (q2 .. q2lp) or one (the sea surface heights and the
+ * external transports).  A pair left NULL (both time levels) is skipped. */
+typedef struct inmsom_ocean_state {
+    double *tt, *ttp, *ss, *ssp, *uu, *uup, *vv, *vvp;
+    double *q2, *q2p, *q2l, *q2lp;
+    double *ssh_i, *sshp_i, *ssh_e, *sshp_e, *ubrtr_e, *ubrtrp_e, *vbrtr_e, *vbrtrp_e;
+} inmsom_ocean_state;
+
+/* The whole checkpoint ocpwrite (Control/output.f90:1454-1847) from host
+ * arrays, same files: for each pair, cp<name>8.dat (FP64, present then
+ * previous), cp<name>.dat (FP32) and its descriptor, over mmm..mm x
+ * nnn..nn (u-point fields from mmm-1 with mask llu, v-point fields from
+ * nnn-1 with mask llv, the others with lu); the 3-D descriptors carry
+ * z*1000 (nz levels) or zw*1000 (nz+1 levels) as LEVELS.  As the
+ * reference (wdstd8), the land points of the written box are 0 in the
+ * caller's arrays afterwards.  The u transport's FP32 file is cpubi.dat
+ * and its descriptor names cpube.dat, as the reference writes them. */
+int inmsom_ocpwrite(const char *path, const inmsom_bounds *b, int nz, const float *lu, const float *llu,
+                    const float *llv, const double *z, const double *zw, const inmsom_ctl_axes *axes,
+                    inmsom_ocean_state *state);
+
+/* The restart from those files (start_type > 0), which
+ * Control/init_pars.f90:312-417 lists after a stop that leaves it
+ * unimplemented: rdstd8 of every pair (land points of the box 0, the rest
+ * of each array as it was), the periodic wraps (q2 and q2l wrapped in y
+ * over their first nz levels only, as the reference passes nz there), then
+ * q2, q2p, q2l, q2lp = max(., tur_var_min) over the whole arrays
+ * (tur_var_min = 1.0e-8 in Inc/basinpar.fi:102). */
+int inmsom_ocpread(const char *path, const inmsom_bounds *b, int nz, const float *lu, const float *llu,
+                   const float *llv, double tur_var_min, inmsom_ocean_state *state);
+
 /* The barotropic part of the reference's checkpoint ocpwrite
  * (Control/output.f90:1736-1847) from the context's resident state: in
  * `path`, cpsshe8.dat (ssh_e, sshp_e over mmm..mm x nnn..nn, mask lu),

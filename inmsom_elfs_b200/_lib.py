@@ -32,7 +32,7 @@ EXPORTS = (
     "inmsom_baroclinic_dynamics", "inmsom_vertical_velocity", "inmsom_depth_ave", "inmsom_shift_barotropic",
     "inmsom_wdstd8", "inmsom_wdstd", "inmsom_rdstd8", "inmsom_rdstd", "inmsom_ctl_file_write",
     "inmsom_write_checkpoint", "inmsom_read_checkpoint", "inmsom_tracer_tran_diff", "inmsom_ctl_file_read",
-    "inmsom_pwdstd", "inmsom_prdstd",
+    "inmsom_pwdstd", "inmsom_prdstd", "inmsom_ocpwrite", "inmsom_ocpread",
 )
 
 # include/inmsom_gpu.h: INMSOM_MLP_*
@@ -50,6 +50,15 @@ class CCtlAxes(ctypes.Structure):
                 ("dxst", ctypes.c_double), ("dyst", ctypes.c_double),
                 ("calendar", ctypes.c_int), ("year", ctypes.c_int), ("month", ctypes.c_int), ("day", ctypes.c_int),
                 ("hour", ctypes.c_int), ("minute", ctypes.c_int), ("tstep", ctypes.c_float)]
+
+
+OCEAN_STATE_FIELDS = ("tt", "ttp", "ss", "ssp", "uu", "uup", "vv", "vvp", "q2", "q2p", "q2l", "q2lp", "ssh_i",
+                      "sshp_i", "ssh_e", "sshp_e", "ubrtr_e", "ubrtrp_e", "vbrtr_e", "vbrtrp_e")
+
+
+class COceanState(ctypes.Structure):
+    """include/inmsom_gpu.h: inmsom_ocean_state."""
+    _fields_ = [(n, ctypes.POINTER(ctypes.c_double)) for n in OCEAN_STATE_FIELDS]
 
 
 class InmsomError(RuntimeError):
@@ -140,6 +149,9 @@ def load() -> ctypes.CDLL:
     cp = ctypes.c_char_p
     for nm, ptr in (("inmsom_wdstd8", DP), ("inmsom_wdstd", FP), ("inmsom_rdstd8", DP), ("inmsom_rdstd", FP)):
         getattr(lib, nm).argtypes = [cp, cp, i, ptr, FP] + [i] * 9
+    lib.inmsom_ocpwrite.argtypes = [cp, ctypes.POINTER(CBounds), i, FP, FP, FP, DP, DP, ctypes.POINTER(CCtlAxes),
+                                    ctypes.POINTER(COceanState)]
+    lib.inmsom_ocpread.argtypes = [cp, ctypes.POINTER(CBounds), i, FP, FP, FP, d, ctypes.POINTER(COceanState)]
     for nm in ("inmsom_pwdstd", "inmsom_prdstd"):
         getattr(lib, nm).argtypes = [ctypes.POINTER(CBounds), cp, cp, i, FP, FP] + [i] * 9
     lib.inmsom_ctl_file_write.argtypes = [cp, ctypes.c_float, i, i, i, i, i, DP, d, i, DP, d, i, DP, d,

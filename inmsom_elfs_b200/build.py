@@ -33,6 +33,7 @@ SOURCES = {
     "column.cu": ["--fmad=false"],
     "dstd.cu": [],
     "ctl_read.cu": [],
+    "ocean_cp.cu": [],
 }
 HEADERS = ["common.cuh", "general.h", "fused.h", "closure.h", "column.h", "context.h"]
 

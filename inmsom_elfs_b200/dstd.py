@@ -130,3 +130,55 @@ def prdstd(bounds, path, fname, nfild, fild, lu, nx, ny, nz, box):
     interior of fild from the shared file (every point; values past the
     end of the file are left as they were)."""
     return _pcall("inmsom_prdstd", bounds, path, fname, nfild, fild, lu, nx, ny, nz, box)
+
+
+def _ocean_state(state, bounds, nz):
+    """COceanState over the arrays of `state` (a dict by field name; pairs
+    left out are skipped), each checked for its shape."""
+    from ._lib import OCEAN_STATE_FIELDS, COceanState
+    cs = COceanState()
+    for name in OCEAN_STATE_FIELDS:
+        a = state.get(name)
+        if a is None:
+            continue
+        lev = (nz if name in ("tt", "ttp", "ss", "ssp", "uu", "uup", "vv", "vvp")
+               else nz + 1 if name in ("q2", "q2p", "q2l", "q2lp") else 1)
+        want = bounds.shape + ((lev,) if lev > 1 else ())
+        if a.dtype != np.float64 or not a.flags.f_contiguous or a.shape[:len(want)] != want or a.size != np.prod(want):
+            raise ValueError(f"{name}: expected a Fortran-ordered float64 array of shape {want}")
+        setattr(cs, name, a.ctypes.data_as(DP))
+    return cs
+
+
+def ocpwrite(path, bounds, nz, lu, llu, llv, z, zw, axes, state):
+    """inmsom_ocpwrite (Control/output.f90:1454-1847): the checkpoint files
+    of every pair in `state` (a dict: tt, ttp, ..., vbrtrp_e); `axes` is a
+    dict of xt, xu, yt, yv (first values for LINEAR axes), dxst, dyst and
+    optionally xgr_type, ygr_type, calendar, date=(y, mo, d, h, mn), tstep.
+    Like the reference, zeroes the written land points of the arrays."""
+    from ._lib import CCtlAxes, cbounds
+    keep = [np.ascontiguousarray(np.atleast_1d(axes[k]), dtype=np.float64) for k in ("xt", "xu", "yt", "yv")]
+    ax = CCtlAxes(axes.get("xgr_type", 0), axes.get("ygr_type", 0), *[k.ctypes.data_as(DP) for k in keep],
+                  float(axes["dxst"]), float(axes["dyst"]), axes.get("calendar", 1),
+                  *[int(x) for x in axes.get("date", (2000, 1, 1, 0, 0))], float(axes.get("tstep", 86400.0)))
+    zs = [np.ascontiguousarray(v, dtype=np.float64) for v in (z, zw)]
+    if zs[0].size < nz or zs[1].size < nz + 1:
+        raise ValueError("z needs nz values and zw nz+1")
+    masks = [np.asfortranarray(m, dtype=np.float32) for m in (lu, llu, llv)]
+    cb = cbounds(bounds)
+    cs = _ocean_state(state, bounds, nz)
+    check(load().inmsom_ocpwrite(str(path).encode(), ctypes.byref(cb), int(nz), *[m.ctypes.data_as(FP) for m in masks],
+                                 zs[0].ctypes.data_as(DP), zs[1].ctypes.data_as(DP), ctypes.byref(ax),
+                                 ctypes.byref(cs)))
+
+
+def ocpread(path, bounds, nz, lu, llu, llv, state, tur_var_min=1.0e-8):
+    """inmsom_ocpread: the restart of every pair in `state` (arrays filled in
+    place) from the checkpoint files in `path`."""
+    from ._lib import cbounds
+    masks = [np.asfortranarray(m, dtype=np.float32) for m in (lu, llu, llv)]
+    cb = cbounds(bounds)
+    cs = _ocean_state(state, bounds, nz)
+    check(load().inmsom_ocpread(str(path).encode(), ctypes.byref(cb), int(nz),
+                                *[m.ctypes.data_as(FP) for m in masks], float(tur_var_min), ctypes.byref(cs)))
+    return state

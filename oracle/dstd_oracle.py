@@ -374,3 +374,98 @@ def ctl_read(text, datname_len=255, title_len=255):
                     ht = f(ht * f(m))
                 out["ht"] = ht
     raise CtlError("in definition undefinit value")
+
+
+# ---- the ocean checkpoint (Control/output.f90:1454-1847) and its restart ------
+# (Control/init_pars.f90:312-417)
+
+# the groups of ocpwrite in its order: FP64 file, FP32 file, the name the
+# descriptor is made from, mask, box start offsets (dx, dy), levels
+# ("1", "nz", "nz+1"), title, variable, the pair of fields
+CP_GROUPS = [
+    ("cptt8.dat", "cptt.dat", "cptt.dat", "lu", 0, 0, "nz", "Potential temperature, C", "tt", ("tt", "ttp")),
+    ("cpss8.dat", "cpss.dat", "cpss.dat", "lu", 0, 0, "nz", "Salinity, PSU", "ss", ("ss", "ssp")),
+    ("cpuu8.dat", "cpuu.dat", "cpuu.dat", "llu", 1, 0, "nz", "Zonal velocity, m/s", "u", ("uu", "uup")),
+    ("cpvv8.dat", "cpvv.dat", "cpvv.dat", "llv", 0, 1, "nz", "Meridional velocity, m/s", "v", ("vv", "vvp")),
+    ("cpq28.dat", "cpq2.dat", "cpq2.dat", "lu", 0, 0, "nz+1", "turbulent kunetic energy, (m/s)^2", "q2",
+     ("q2", "q2p")),
+    ("cpq2l8.dat", "cpq2l.dat", "cpq2l.dat", "lu", 0, 0, "nz+1",
+     "turbulent kunetic energy by length scale, (m/s)^2*m", "q2l", ("q2l", "q2lp")),
+    ("cpsshi8.dat", "cpsshi.dat", "cpsshi.dat", "lu", 0, 0, "1", "Internal SSH, m", "ssh", ("ssh_i", "sshp_i")),
+    ("cpsshe8.dat", "cpsshe.dat", "cpsshe.dat", "lu", 0, 0, "1", "External SSH, m", "ssh", ("ssh_e", "sshp_e")),
+    ("cpube8.dat", "cpubi.dat", "cpube.dat", "llu", 1, 0, "1", "External UB, m/s", "ub", ("ubrtr_e", "ubrtrp_e")),
+    ("cpvbe8.dat", "cpvbe.dat", "cpvbe.dat", "llv", 0, 1, "1", "External VB, m/s", "vb", ("vbrtr_e", "vbrtrp_e")),
+]
+
+
+def file_bytes(fields, lu, box, dtype):
+    """The bytes of a file holding fields [(nfield, field), ...] of one box,
+    written by wdstd / wdstd8 in that order."""
+    chunks, size = [], 0
+    for nfield, f in fields:
+        for kr, rec in enumerate(records(f, lu, box, dtype), start=1):
+            off = record_offset(nfield, box, kr, np.dtype(dtype).itemsize)
+            chunks.append((off, rec))
+            size = max(size, off + len(rec))
+    buf = bytearray(size)
+    for off, rec in chunks:
+        buf[off:off + len(rec)] = rec
+    return bytes(buf)
+
+
+def _cp_box(b, dx, dy, levels):
+    i0, i1 = b.mmm - b.bnd_x1 + 1, b.mm - b.bnd_x1 + 1
+    j0, j1 = b.nnn - b.bnd_y1 + 1, b.nn - b.bnd_y1 + 1
+    return (i0 - dx, i1, j0 - dy, j1, 1, levels)
+
+
+def ocpwrite_files(path, b, nz, masks, z, zw, axes, state):
+    """{file name: bytes or text} of everything ocpwrite writes for the
+    pairs present in `state` (masks: dict lu/llu/llv; axes as the library's
+    ocpwrite takes them)."""
+    out = {}
+    nx_glob, ny_glob = b.mm - b.mmm + 1, b.nn - b.nnn + 1
+    date = axes.get("date", (2000, 1, 1, 0, 0))
+    for f8, f4, ctl, mk, dx, dy, lev, title, var, (a, ap) in CP_GROUPS:
+        if a not in state:
+            continue
+        L = {"1": 1, "nz": nz, "nz+1": nz + 1}[lev]
+        box = _cp_box(b, dx, dy, L)
+        lu = masks[mk]
+        f, fp = state[a], state[ap]
+        out[f8] = file_bytes([(1, f), (2, fp)], lu, box, np.float64)
+        out[f4] = file_bytes([(1, f.astype(np.float32)), (2, fp.astype(np.float32))], lu, box, np.float32)
+        zv = [0.0] if L == 1 else [float(v) * 1000.0 for v in (z if lev == "nz" else zw)[:L]]
+        name, text = ctl_text(f"{path}/{ctl}", -1.0e32, nx_glob + dx, ny_glob + dy, L, 2, axes.get("xgr_type", 0),
+                              axes["xu"] if dx else axes["xt"], axes["dxst"], axes.get("ygr_type", 0),
+                              axes["yv"] if dy else axes["yt"], axes["dyst"], 0 if L == 1 else 1, zv, 1.0,
+                              axes.get("calendar", 1), *date, axes.get("tstep", 86400.0), title, var)
+        out[name.rsplit("/", 1)[-1]] = text
+    return out
+
+
+def ocpread_state(files, b, nz, masks, state, tur_var_min=1.0e-8):
+    """The arrays of `state` (in place) after the restart reads of
+    Control/init_pars.f90:312-417 from files {name: bytes}: rdstd8 (land of
+    the box 0), the wraps (cyclize8_y of q2/q2l over nz levels), the
+    tur_var_min floor of q2, q2p, q2l, q2lp."""
+    for f8, _, _, mk, dx, dy, lev, _, _, pair in CP_GROUPS:
+        if pair[0] not in state:
+            continue
+        L = {"1": 1, "nz": nz, "nz+1": nz + 1}[lev]
+        box = _cp_box(b, dx, dy, L)
+        for nfield, name in enumerate(pair, start=1):
+            f = state[name]
+            read_field(files[f8], nfield, box, np.float64, masks[mk], f)
+            g = f if f.ndim == 3 else f[:, :, None]
+            i0, i1 = b.mmm - b.bnd_x1, b.mm - b.bnd_x1
+            j0, j1 = b.nnn - b.bnd_y1, b.nn - b.bnd_y1
+            ly = nz if lev == "nz+1" else L
+            if b.periodicity_x:
+                g[i0 - 1, :, :L], g[i1 + 1, :, :L] = g[i1, :, :L].copy(), g[i0, :, :L].copy()
+            if b.periodicity_y:
+                g[:, j0 - 1, :ly], g[:, j1 + 1, :ly] = g[:, j1, :ly].copy(), g[:, j0, :ly].copy()
+    for name in ("q2", "q2p", "q2l", "q2lp"):
+        if name in state:
+            np.maximum(state[name], tur_var_min, out=state[name])
+    return state

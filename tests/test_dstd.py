@@ -533,3 +533,88 @@ def test_pwdstd_gloo_ranks(tmp_path, world):
     full[np.broadcast_to((np.abs(lu) < 0.5)[..., None], full.shape)] = od.UNDEF
     for r, lb in enumerate(strip_bounds(g, world)):
         assert np.array_equal(got[r], _local(full, g, lb)[2:-2, 2:-2])
+
+
+# ---- the whole checkpoint from host arrays (Control/output.f90:1454-1847) ----
+
+def _ocean(seed, b, nz):
+    rng = np.random.default_rng(seed)
+    sh = b.shape
+    st = {}
+    for name in ("tt", "ttp", "ss", "ssp", "uu", "uup", "vv", "vvp"):
+        st[name] = np.asfortranarray(rng.standard_normal(sh + (nz,)))
+    for name in ("q2", "q2p", "q2l", "q2lp"):
+        st[name] = np.asfortranarray(rng.standard_normal(sh + (nz + 1,)) * 1e-6)   # some below tur_var_min
+    for name in ("ssh_i", "sshp_i", "ssh_e", "sshp_e", "ubrtr_e", "ubrtrp_e", "vbrtr_e", "vbrtrp_e"):
+        st[name] = np.asfortranarray(rng.standard_normal(sh))
+    masks = {k: np.asfortranarray((rng.random(sh) > 0.35).astype(np.float32)) for k in ("lu", "llu", "llv")}
+    return st, masks
+
+
+AXES = dict(xt=[27.5], xu=[27.25], yt=[40.9], yv=[40.775], dxst=0.5, dyst=0.25, calendar=0,
+            date=(2001, 7, 15, 6, 0), tstep=21600.0)
+
+
+@pytest.mark.parametrize("px, py", [(0, 0), (1, 0), (0, 1), (1, 1)])
+def test_ocean_checkpoint_files_and_restart(tmp_path, px, py):
+    """ocpwrite from host arrays writes the reference's 30 files (FP64, FP32
+    and descriptor of ten pairs) byte for byte as the restatement does, and
+    zeroes the written land points of its arrays; ocpread brings back what
+    the restart reads give (land 0, the wraps, the q2 floor)."""
+    from inmsom_elfs_b200.grid import Bounds
+    b = Bounds.serial(10, 7, px, py)
+    nz = 4
+    st, masks = _ocean(21 + 2 * px + py, b, nz)
+    z = np.linspace(0.005, 0.9, nz)
+    zw = np.linspace(0.0, 1.0, nz + 1)
+    mine = {k: v.copy(order="F") for k, v in st.items()}
+    dstd.ocpwrite(str(tmp_path), b, nz, masks["lu"], masks["llu"], masks["llv"], z, zw, AXES, mine)
+    want = od.ocpwrite_files(str(tmp_path), b, nz, masks, z, zw, AXES, st)
+    assert len(want) == 30 and sorted(p.name for p in tmp_path.iterdir()) == sorted(want)
+    for name, content in want.items():
+        got = (tmp_path / name).read_bytes()
+        assert got == (content.encode() if isinstance(content, str) else content), name
+    # the written boxes' land points are 0 in the caller's arrays, the rest untouched
+    for f8, _, _, mk, dx, dy, lev, _, _, pair in od.CP_GROUPS:
+        box = od._cp_box(b, dx, dy, 1)
+        land = np.zeros(b.shape, bool)
+        land[box[0] - 1:box[1], box[2] - 1:box[3]] = np.abs(masks[mk][box[0] - 1:box[1], box[2] - 1:box[3]]) < 0.5
+        for name in pair:
+            m = land if mine[name].ndim == 2 else land[..., None] & np.ones(mine[name].shape, bool)
+            assert np.all(mine[name][m] == 0) and np.array_equal(mine[name][~m], st[name][~m]), name
+    # the restart, into arrays that hold something else
+    rng = np.random.default_rng(99)
+    old = {k: np.asfortranarray(rng.standard_normal(v.shape)) for k, v in st.items()}
+    got = {k: v.copy(order="F") for k, v in old.items()}
+    dstd.ocpread(str(tmp_path), b, nz, masks["lu"], masks["llu"], masks["llv"], got)
+    files = {f8: (tmp_path / f8).read_bytes() for f8, *_ in od.CP_GROUPS}
+    exp = od.ocpread_state(files, b, nz, masks, {k: v.copy(order="F") for k, v in old.items()})
+    for k in st:
+        assert np.array_equal(got[k], exp[k]), k
+    # the interior ocean values come back exactly
+    i, j = b.interior
+    ocean = np.abs(masks["lu"][i, j]) >= 0.5
+    assert np.array_equal(got["tt"][i, j][ocean], st["tt"][i, j][ocean])
+    assert np.all(got["q2"] >= 1.0e-8)
+
+
+def test_ocean_checkpoint_pairs_and_errors(tmp_path):
+    """Only the pairs given are written (a barotropic-only state writes the
+    same three groups as the context's checkpoint); half a pair, a missing
+    z or an unreadable file is an error."""
+    from inmsom_elfs_b200.grid import Bounds
+    b = Bounds.serial(6, 5)
+    st, masks = _ocean(5, b, 2)
+    baro = {k: st[k] for k in ("ssh_e", "sshp_e", "ubrtr_e", "ubrtrp_e", "vbrtr_e", "vbrtrp_e")}
+    dstd.ocpwrite(str(tmp_path), b, 2, masks["lu"], masks["llu"], masks["llv"], [0.1, 0.6], [0, 0.5, 1], AXES, baro)
+    assert sorted(p.name for p in tmp_path.iterdir()) == sorted(
+        ["cpsshe8.dat", "cpsshe.dat", "cpsshe.ctl", "cpube8.dat", "cpubi.dat", "cpube.ctl", "cpvbe8.dat",
+         "cpvbe.dat", "cpvbe.ctl"])
+    with pytest.raises(InmsomError) as e:
+        dstd.ocpwrite(str(tmp_path), b, 2, masks["lu"], masks["llu"], masks["llv"], [0.1, 0.6], [0, 0.5, 1], AXES,
+                      {"tt": st["tt"]})
+    assert e.value.code == 2
+    with pytest.raises(InmsomError) as e:
+        dstd.ocpread(str(tmp_path), b, 2, masks["lu"], masks["llu"], masks["llv"],
+                     {"tt": st["tt"].copy(order="F"), "ttp": st["ttp"].copy(order="F")})
+    assert e.value.code == 6
