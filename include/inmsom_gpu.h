@@ -453,6 +453,17 @@ int inmsom_ctl_file_read(const char *ctlname, char *datname, int datname_len, fl
                          int *yr_type, int *year0, int *month0, int *day0, int *hour0, int *minute0, float *ht,
                          char *title, int title_len, char *varname, int varname_len, int varname_cap, int *inform);
 
+/* compare_grids (Service/rw_ctl_file.f90:628-714; the reference calls it
+ * nowhere), same arguments: *ierr = 1 when a grid of descriptor a is longer
+ * than maxgridlen or the x, y, z or t point counts differ, else 2 when an
+ * x, y or z coordinate differs, else 0.  The undefined values, steps and
+ * times are not compared, as in the reference. */
+int inmsom_compare_grids(int maxgridlen, int *ierr, float undefa, int nxa, int nya, int nza, int nta,
+                         const double *xa, double hxa, const double *ya, double hya, float ta, float hta,
+                         const double *za, double hza, float undefb, int nxb, int nyb, int nzb, int ntb,
+                         const double *xb, double hxb, const double *yb, double hyb, float tb, float htb,
+                         const double *zb, double hzb);
+
 /* The grid and calendar that the checkpoint's descriptors state
  * (basin_grid's xt, xu, yt, yv, dxst, dyst, xgr_type, ygr_type and the
  * model time of Control/output.f90:1454-1463): for a LINEAR axis (type 0)

@@ -33,6 +33,7 @@ EXPORTS = (
     "inmsom_wdstd8", "inmsom_wdstd", "inmsom_rdstd8", "inmsom_rdstd", "inmsom_ctl_file_write",
     "inmsom_write_checkpoint", "inmsom_read_checkpoint", "inmsom_tracer_tran_diff", "inmsom_ctl_file_read",
     "inmsom_pwdstd", "inmsom_prdstd", "inmsom_ocpwrite", "inmsom_ocpread",
+    "inmsom_compare_grids",
 )
 
 # include/inmsom_gpu.h: INMSOM_MLP_*
@@ -152,6 +153,8 @@ def load() -> ctypes.CDLL:
     lib.inmsom_ocpwrite.argtypes = [cp, ctypes.POINTER(CBounds), i, FP, FP, FP, DP, DP, ctypes.POINTER(CCtlAxes),
                                     ctypes.POINTER(COceanState)]
     lib.inmsom_ocpread.argtypes = [cp, ctypes.POINTER(CBounds), i, FP, FP, FP, d, ctypes.POINTER(COceanState)]
+    grid = [ctypes.c_float, i, i, i, i, DP, d, DP, d, ctypes.c_float, ctypes.c_float, DP, d]
+    lib.inmsom_compare_grids.argtypes = [i, ctypes.POINTER(ctypes.c_int)] + grid + grid
     for nm in ("inmsom_pwdstd", "inmsom_prdstd"):
         getattr(lib, nm).argtypes = [ctypes.POINTER(CBounds), cp, cp, i, FP, FP] + [i] * 9
     lib.inmsom_ctl_file_write.argtypes = [cp, ctypes.c_float, i, i, i, i, i, DP, d, i, DP, d, i, DP, d,

@@ -1,5 +1,6 @@
-// The GrADS descriptor reader ctl_file_read (Service/rw_ctl_file.f90:185-566)
-// and its helper nonblank (:568-596); host code, no kernels.
+// The GrADS descriptor reader ctl_file_read (Service/rw_ctl_file.f90:185-566),
+// its helper nonblank (:568-596), and compare_grids (:628-714), which
+// compares the grids two descriptors state; host code, no kernels.
 //
 // The reference reads the descriptor record by record (character(256),
 // at most 512 iterations) and dispatches on the keyword at the first
@@ -400,6 +401,34 @@ int inmsom_ctl_file_read(const char *ctlname, char *datname, int datname_len, fl
     // the loop ends without ENDVARS: the reference falls through to its
     // first error label (the undefined-value message)
     return err("in definition undefinit value");
+}
+
+int inmsom_compare_grids(int maxgridlen, int *ierr, float undefa, int nxa, int nya, int nza, int nta,
+                         const double *xa, double hxa, const double *ya, double hya, float ta, float hta,
+                         const double *za, double hza, float undefb, int nxb, int nyb, int nzb, int ntb,
+                         const double *xb, double hxb, const double *yb, double hyb, float tb, float htb,
+                         const double *zb, double hzb)
+{
+    (void)undefa, (void)hxa, (void)hya, (void)ta, (void)hta, (void)hza;
+    (void)undefb, (void)hxb, (void)hyb, (void)tb, (void)htb, (void)hzb;
+    if (!ierr || !xa || !ya || !za || !xb || !yb || !zb)
+        return fail(INMSOM_EARG, "inmsom_compare_grids: NULL argument");
+    *ierr = 0;
+    // ierr = 1: a grid longer than maxgridlen, or different point counts
+    // (the checks of Service/rw_ctl_file.f90:653-692, in their order)
+    if (nxa > maxgridlen || nya > maxgridlen || nza > maxgridlen || nxa != nxb || nya != nyb || nza != nzb ||
+        nta != ntb) {
+        *ierr = 1;
+        return INMSOM_OK;
+    }
+    // ierr = 2: a coordinate that differs (:694-712)
+    for (int i = 0; i < nxa; i++)
+        if (xa[i] != xb[i]) *ierr = 2;
+    for (int i = 0; i < nya; i++)
+        if (ya[i] != yb[i]) *ierr = 2;
+    for (int i = 0; i < nza; i++)
+        if (za[i] != zb[i]) *ierr = 2;
+    return INMSOM_OK;
 }
 
 }  // extern "C"

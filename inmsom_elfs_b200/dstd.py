@@ -182,3 +182,21 @@ def ocpread(path, bounds, nz, lu, llu, llv, state, tur_var_min=1.0e-8):
     check(load().inmsom_ocpread(str(path).encode(), ctypes.byref(cb), int(nz),
                                 *[m.ctypes.data_as(FP) for m in masks], float(tur_var_min), ctypes.byref(cs)))
     return state
+
+
+def compare_grids(a, b, maxgridlen=4096):
+    """inmsom_compare_grids (Service/rw_ctl_file.f90:628-714) on two
+    ctl_file_read results: 0 same grids, 1 too long or different counts,
+    2 different coordinates."""
+    ierr = ctypes.c_int(-1)
+
+    def args(g):
+        arrs = [np.ascontiguousarray(np.resize(np.asarray(g[k], dtype=np.float64), max(len(g[k]), 1)))
+                for k in ("x0", "y0", "z0")]
+        return arrs, [float(g["undef"]), g["nx"], g["ny"], g["nz"], g["nt"], arrs[0].ctypes.data_as(DP), g["hx"],
+                      arrs[1].ctypes.data_as(DP), g["hy"], 0.0, float(g["ht"]), arrs[2].ctypes.data_as(DP), g["hz"]]
+
+    keep_a, la = args(a)
+    keep_b, lb = args(b)
+    check(load().inmsom_compare_grids(int(maxgridlen), ctypes.byref(ierr), *la, *lb))
+    return ierr.value

@@ -618,3 +618,27 @@ def test_ocean_checkpoint_pairs_and_errors(tmp_path):
         dstd.ocpread(str(tmp_path), b, 2, masks["lu"], masks["llu"], masks["llv"],
                      {"tt": st["tt"].copy(order="F"), "ttp": st["ttp"].copy(order="F")})
     assert e.value.code == 6
+
+
+def test_compare_grids(tmp_path):
+    """compare_grids on descriptors read back: 0 for the same grids, 1 for
+    different counts or a grid past maxgridlen, 2 for a coordinate that
+    differs; the undefined value and time step are not compared."""
+    c = CTL_CASES[1]
+
+    def write(name, **over):
+        a = dict(c, **over)
+        y, mo, d, h, mn = a["date"]
+        dstd.ctl_file_write(str(tmp_path / f"{name}.dat"), a.get("undef", -1.0e32), a["nx"], a["ny"], a["nz"],
+                            a["nt"], a["xtype"], a["x0"], a["hx"], a["ytype"], a["y0"], a["hy"], a["ztype"], a["z0"],
+                            a["hz"], a["yr_type"], y, mo, d, h, mn, a["ht"], a["title"], a["var"])
+        return dstd.ctl_file_read(tmp_path / f"{name}.ctl")
+
+    base = write("a")
+    assert dstd.compare_grids(base, write("b", undef=-9.0, ht=3600.0)) == 0
+    assert dstd.compare_grids(base, write("c", nt=13)) == 1
+    z = list(c["z0"])
+    assert dstd.compare_grids(base, write("d", nz=19, z0=z[:19])) == 1
+    assert dstd.compare_grids(base, base, maxgridlen=8) == 1
+    z[4] += 1.0
+    assert dstd.compare_grids(base, write("e", z0=z)) == 2
