@@ -233,6 +233,26 @@ int inmsom_tracer_tran_diff(inmsom_ctx *ctx, int nz, const double *dz, const dou
                             const double *src, double src_factor, const double *hhu, const double *hhv,
                             const double *hhqn, const double *hhqp);
 
+/* Replaces stress_components, Function/mixing.f90:115-168, on nlev levels
+ * (Control/dyncall.f90:38 calls it with nz for uup, vvp): tension str_t at
+ * the lu points and shear str_s at the luu points of the interior, then
+ * the periodic wraps of both; the other points keep the values the caller
+ * passed (the reference's arrays keep theirs).  u, v, str_t, str_s are
+ * (bnd_x1:bnd_x2, bnd_y1:bnd_y2, nlev) host arrays. */
+int inmsom_stress_components(inmsom_ctx *ctx, int nlev, const double *u, const double *v, double *str_t,
+                             double *str_s);
+
+/* Replaces smagorinsky_coeff, Function/mixing.f90:171-219 (called at
+ * Control/dyncall.f90:41-43 when ksw_lat > 0): at the lu points of the
+ * interior on nz levels, mu_smag = (vonkarman/Pi)^2 dx dy sqrt(str_t^2 +
+ * the mean of the four str_s^2 around the point), amuv = visc2 + mu_smag,
+ * amts = dift + 0.1 mu_smag (vonkarman = 0.4, Pi of Inc/basinpar.fi:72,89),
+ * then the periodic wraps of both; other points keep the caller's values.
+ * The barotropic viscosity of that step is then
+ * inmsom_depth_ave(amuv -> amuv2d, kbcl = 0). */
+int inmsom_smagorinsky_coeff(inmsom_ctx *ctx, int nz, double visc2, double dift, const double *str_t,
+                             const double *str_s, double *amts, double *amuv);
+
 /* Replaces depth_ave, Function/depth.f90:223-254 (called at
  * Control/dyncall.f90:101-105 to take the barotropic RHS out of the 3-D
  * one): at the points where mask > 0.5 (all but the arrays' outermost ring)

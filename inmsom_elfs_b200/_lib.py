@@ -33,7 +33,7 @@ EXPORTS = (
     "inmsom_wdstd8", "inmsom_wdstd", "inmsom_rdstd8", "inmsom_rdstd", "inmsom_ctl_file_write",
     "inmsom_write_checkpoint", "inmsom_read_checkpoint", "inmsom_tracer_tran_diff", "inmsom_ctl_file_read",
     "inmsom_pwdstd", "inmsom_prdstd", "inmsom_ocpwrite", "inmsom_ocpread",
-    "inmsom_compare_grids",
+    "inmsom_compare_grids", "inmsom_stress_components", "inmsom_smagorinsky_coeff",
 )
 
 # include/inmsom_gpu.h: INMSOM_MLP_*
@@ -147,6 +147,8 @@ def load() -> ctypes.CDLL:
     lib.inmsom_vertical_velocity.argtypes = [VP, i] + [DP] * 7
     lib.inmsom_depth_ave.argtypes = [VP, i, DP, DP, DP, FP, i]
     lib.inmsom_shift_barotropic.argtypes = [VP, i, DP, DP, DP, DP, i]
+    lib.inmsom_stress_components.argtypes = [VP, i, DP, DP, DP, DP]
+    lib.inmsom_smagorinsky_coeff.argtypes = [VP, i, d, d, DP, DP, DP, DP]
     cp = ctypes.c_char_p
     for nm, ptr in (("inmsom_wdstd8", DP), ("inmsom_wdstd", FP), ("inmsom_rdstd8", DP), ("inmsom_rdstd", FP)):
         getattr(lib, nm).argtypes = [cp, cp, i, ptr, FP] + [i] * 9

@@ -437,4 +437,46 @@ int inmsom_shift_barotropic(inmsom_ctx *c, int nz, double *uu, double *vv, const
     return sync_stream(c);
 }
 
+int inmsom_stress_components(inmsom_ctx *c, int nlev, const double *u, const double *v, double *str_t,
+                             double *str_s)
+{
+    CKR(ensure_grid(c));
+    if (nlev < 1 || nlev > 65535) return set_err(INMSOM_EARG, "inmsom_stress_components: nlev = %d", nlev);
+    if (!u || !v || !str_t || !str_s) return set_err(INMSOM_EARG, "inmsom_stress_components: NULL argument");
+    CKR(col_alloc(c, nlev));
+    CKR(h2d3(c, col3(c, C3_UU), u, nlev));
+    CKR(h2d3(c, col3(c, C3_VV), v, nlev));
+    CKR(h2d3(c, col3(c, C3_RHSX), str_t, nlev));   // points the routine does not set keep the caller's values
+    CKR(h2d3(c, col3(c, C3_RHSY), str_s, nlev));
+    if (column::stress_components(c->dom, c->gdev(), col_levels(c), col3(c, C3_UU), col3(c, C3_VV),
+                                  col3(c, C3_RHSX), col3(c, C3_RHSY), c->stream))
+        return set_err(INMSOM_EARG, "inmsom_stress_components: bad levels");
+    CK(cudaGetLastError());
+    CKR(d2h3(c, str_t, col3(c, C3_RHSX), nlev));
+    CKR(d2h3(c, str_s, col3(c, C3_RHSY), nlev));
+    return sync_stream(c);
+}
+
+int inmsom_smagorinsky_coeff(inmsom_ctx *c, int nz, double visc2, double dift, const double *str_t,
+                             const double *str_s, double *amts, double *amuv)
+{
+    CKR(ensure_grid(c));
+    if (nz < 1 || nz > 65535) return set_err(INMSOM_EARG, "inmsom_smagorinsky_coeff: nz = %d", nz);
+    if (!str_t || !str_s || !amts || !amuv) return set_err(INMSOM_EARG, "inmsom_smagorinsky_coeff: NULL argument");
+    // Inc/basinpar.fi:72,89: Pi, vonkarman
+    const double kp = 0.4 / 3.141592653589793;
+    CKR(col_alloc(c, nz));
+    CKR(h2d3(c, col3(c, C3_UU), str_t, nz));
+    CKR(h2d3(c, col3(c, C3_VV), str_s, nz));
+    CKR(h2d3(c, col3(c, C3_RHSX), amts, nz));      // land points keep the caller's values
+    CKR(h2d3(c, col3(c, C3_RHSY), amuv, nz));
+    if (column::smagorinsky_coeff(c->dom, c->gdev(), col_levels(c), visc2, dift, kp, col3(c, C3_UU),
+                                  col3(c, C3_VV), col3(c, C3_RHSX), col3(c, C3_RHSY), c->stream))
+        return set_err(INMSOM_EARG, "inmsom_smagorinsky_coeff: bad levels");
+    CK(cudaGetLastError());
+    CKR(d2h3(c, amts, col3(c, C3_RHSX), nz));
+    CKR(d2h3(c, amuv, col3(c, C3_RHSY), nz));
+    return sync_stream(c);
+}
+
 }  // extern "C"

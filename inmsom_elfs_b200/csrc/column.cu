@@ -936,6 +936,46 @@ __global__ void k_shift_barotropic(Dom D, GridDev g, Levels L, double *uu, doubl
     }
 }
 
+// Function/mixing.f90:129-153 at one point of the interior, level blockIdx.z
+__global__ void k_stress3(Dom D, GridDev g, Levels L, const double *u, const double *v, double *str_t,
+                          double *str_s)
+{
+    const int m = D.nx_start + blockIdx.x * BX + threadIdx.x;
+    const int n = D.ny_start + blockIdx.y * BY + threadIdx.y;
+    if (m > D.nx_end || n > D.ny_end) return;
+    const long long o = (long long)blockIdx.z * L.plane;
+    const double *uk = u + o, *vk = v + o;
+    const double *dx = g.dx, *dy = g.dy, *dxh = g.dxh, *dyh = g.dyh;
+    const double *dxt = g.dxt, *dyt = g.dyt, *dxb = g.dxb, *dyb = g.dyb;
+    if (g.lu[X(m, n)] > 0.5f)
+        str_t[o + X(m, n)] =
+            dy[X(m, n)] / dx[X(m, n)] * (uk[X(m, n)] / dyh[X(m, n)] - uk[X(m - 1, n)] / dyh[X(m - 1, n)]) -
+            dx[X(m, n)] / dy[X(m, n)] * (vk[X(m, n)] / dxh[X(m, n)] - vk[X(m, n - 1)] / dxh[X(m, n - 1)]);
+    if (g.luu[X(m, n)] > 0.5f)
+        str_s[o + X(m, n)] =
+            dxb[X(m, n)] / dyb[X(m, n)] * (uk[X(m, n + 1)] / dxt[X(m, n + 1)] - uk[X(m, n)] / dxt[X(m, n)]) +
+            dyb[X(m, n)] / dxb[X(m, n)] * (vk[X(m + 1, n)] / dyt[X(m + 1, n)] - vk[X(m, n)] / dyt[X(m, n)]);
+}
+
+// Function/mixing.f90:186-199 at one point of the interior, level
+// blockIdx.z; kp = vonkarman/Pi
+__global__ void k_smagorinsky3(Dom D, GridDev g, Levels L, double visc2, double dift, double kp,
+                               const double *str_t, const double *str_s, double *amts, double *amuv)
+{
+    const int m = D.nx_start + blockIdx.x * BX + threadIdx.x;
+    const int n = D.ny_start + blockIdx.y * BY + threadIdx.y;
+    if (m > D.nx_end || n > D.ny_end) return;
+    if (!(g.lu[X(m, n)] > 0.5f)) return;
+    const long long o = (long long)blockIdx.z * L.plane;
+    const double *sk = str_s + o;
+    const double s0 = sk[X(m, n)], s1 = sk[X(m - 1, n)], s2 = sk[X(m, n - 1)], s3 = sk[X(m - 1, n - 1)];
+    const double str_s2 = (s0 * s0 + s1 * s1 + s2 * s2 + s3 * s3) / 4.0;
+    const double st = str_t[o + X(m, n)];
+    const double mu_smag = kp * kp * g.dx[X(m, n)] * g.dy[X(m, n)] * sqrt(st * st + str_s2);
+    amuv[o + X(m, n)] = visc2 + mu_smag;
+    amts[o + X(m, n)] = dift + mu_smag * 0.1;   // prandtl = 0.1d0 (:177)
+}
+
 // Service/oc_algorithms.f90:50-95 and :118-135 on every level (grid y)
 __global__ void k_cyclize_x3(Dom D, long long plane, double *f)
 {
@@ -1060,6 +1100,30 @@ int depth_ave(const Dom &d, const Levels &L, double *u, double *utr, const float
     const int w = d.nxa() - 2, h = d.nya() - 2;
     if (w < 1 || h < 1) return 0;
     k_depth_ave<<<dim3((w + BX - 1) / BX, (h + BY - 1) / BY), dim3(BX, BY), 0, s>>>(d, L, u, utr, mask, kbcl);
+    return 0;
+}
+
+int stress_components(const Dom &d, const GridDev &g, const Levels &L, const double *u, const double *v,
+                      double *str_t, double *str_s, cudaStream_t s)
+{
+    if (L.nz < 1 || L.nz > 65535) return -1;
+    const int nxi = d.nx_end - d.nx_start + 1, nyi = d.ny_end - d.ny_start + 1;
+    k_stress3<<<dim3((nxi + BX - 1) / BX, (nyi + BY - 1) / BY, L.nz), dim3(BX, BY), 0, s>>>(d, g, L, u, v, str_t,
+                                                                                            str_s);
+    halo3(d, str_t, L.nz, L.plane, s);
+    halo3(d, str_s, L.nz, L.plane, s);
+    return 0;
+}
+
+int smagorinsky_coeff(const Dom &d, const GridDev &g, const Levels &L, double visc2, double dift, double kp,
+                      const double *str_t, const double *str_s, double *amts, double *amuv, cudaStream_t s)
+{
+    if (L.nz < 1 || L.nz > 65535) return -1;
+    const int nxi = d.nx_end - d.nx_start + 1, nyi = d.ny_end - d.ny_start + 1;
+    k_smagorinsky3<<<dim3((nxi + BX - 1) / BX, (nyi + BY - 1) / BY, L.nz), dim3(BX, BY), 0, s>>>(
+        d, g, L, visc2, dift, kp, str_t, str_s, amts, amuv);
+    halo3(d, amuv, L.nz, L.plane, s);
+    halo3(d, amts, L.nz, L.plane, s);
     return 0;
 }
 

@@ -97,6 +97,18 @@ int tracer_border(const Dom &d, const GridDev &g, const Consts &c, const Levels 
 // (all but the arrays' outermost ring), u = u - kbcl*utr there; L.dz only.
 int depth_ave(const Dom &d, const Levels &L, double *u, double *utr, const float *mask, int kbcl, cudaStream_t s);
 
+// Function/mixing.f90:115-168 stress_components on L.nz levels: tension
+// at the lu points and shear at the luu points of the interior (other
+// points keep their values), then the periodic wraps of both.
+int stress_components(const Dom &d, const GridDev &g, const Levels &L, const double *u, const double *v,
+                      double *str_t, double *str_s, cudaStream_t s);
+
+// Function/mixing.f90:171-219 smagorinsky_coeff on L.nz levels (kp =
+// vonkarman/Pi): amuv, amts at the lu points of the interior, then the
+// periodic wraps of both.
+int smagorinsky_coeff(const Dom &d, const GridDev &g, const Levels &L, double visc2, double dift, double kp,
+                      const double *str_t, const double *str_s, double *amts, double *amuv, cudaStream_t s);
+
 // Control/dyncall.f90:170-183 (sign < 0: uu - uu2d) and :215-229 (sign > 0:
 // uu + uu2d) at the ocean u (v) points of the interior and its ring.
 int shift_barotropic(const Dom &d, const GridDev &g, const Levels &L, double *uu, double *vv, const double *uu2d,

@@ -241,6 +241,27 @@ class BarotropicSolver:
                                       fptr(mask), int(kbcl)))
         return u, utr
 
+    def stress_components(self, u, v, str_t, str_s):
+        """Function/mixing.f90:115-168 on the levels of u, v, in place on
+        str_t, str_s (inmsom_stress_components)."""
+        arrs = (u, v, str_t, str_s)
+        if any(a.shape != u.shape or a.shape[:2] != self.basin.bounds.shape for a in arrs):
+            raise ValueError("u, v, str_t, str_s need the array shape and the same levels")
+        nlev = u.shape[2] if u.ndim == 3 else 1
+        check(load().inmsom_stress_components(self._ctx, nlev, *[dptr(a) for a in arrs]))
+        return str_t, str_s
+
+    def smagorinsky_coeff(self, visc2: float, dift: float, str_t, str_s, amts, amuv):
+        """Function/mixing.f90:171-219 in place on amts, amuv
+        (inmsom_smagorinsky_coeff)."""
+        arrs = (str_t, str_s, amts, amuv)
+        if any(a.shape != str_t.shape or a.shape[:2] != self.basin.bounds.shape for a in arrs):
+            raise ValueError("str_t, str_s, amts, amuv need the array shape and the same levels")
+        nz = str_t.shape[2] if str_t.ndim == 3 else 1
+        check(load().inmsom_smagorinsky_coeff(self._ctx, nz, float(visc2), float(dift),
+                                              *[dptr(a) for a in arrs]))
+        return amts, amuv
+
     def shift_barotropic(self, uu, vv, uu2d, vv2d, sign: int):
         """Control/dyncall.f90:170-183 (sign -1) / :215-229 (sign +1) in
         place on uu, vv (inmsom_shift_barotropic)."""

@@ -216,6 +216,29 @@ def depth_ave(basin, dz, u, utr, mask, kbcl):
     return u, utr
 
 
+def _levels(a):
+    return [a] if a.ndim == 2 else [a[:, :, k] for k in range(a.shape[2])]
+
+
+def stress_components(basin, u, v, str_t, str_s):
+    """Function/mixing.f90:115-168 on every level of u, v (the routine's
+    level loop is innermost and the levels do not interact), in place."""
+    g = grid_struct(basin)
+    for uk, vk, tk, sk in zip(*[_levels(a) for a in (u, v, str_t, str_s)]):
+        load().ora_stress_components(ctypes.byref(g), _d(uk), _d(vk), _d(tk), _d(sk))
+    return str_t, str_s
+
+
+def smagorinsky_coeff(basin, visc2, dift, str_t, str_s, amts, amuv, vonkarman=0.4, pi=3.141592653589793):
+    """Function/mixing.f90:171-219 on every level, in place on amts, amuv
+    (vonkarman, Pi: Inc/basinpar.fi:72,89)."""
+    g = grid_struct(basin)
+    for tk, sk, ak, mk in zip(*[_levels(a) for a in (str_t, str_s, amts, amuv)]):
+        load().ora_smagorinsky_coeff(ctypes.byref(g), ctypes.c_double(visc2), ctypes.c_double(dift), _d(tk),
+                                     _d(sk), _d(ak), _d(mk), ctypes.c_double(vonkarman), ctypes.c_double(pi))
+    return amts, amuv
+
+
 def shift_barotropic(basin, nz, uu, vv, uu2d, vv2d, sign):
     """Control/dyncall.f90:170-183 (sign -1) / :215-229 (sign +1) in place."""
     g = grid_struct(basin)
