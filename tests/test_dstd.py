@@ -642,3 +642,36 @@ def test_compare_grids(tmp_path):
     assert dstd.compare_grids(base, base, maxgridlen=8) == 1
     z[4] += 1.0
     assert dstd.compare_grids(base, write("e", z0=z)) == 2
+
+
+def test_ctl_write_read_random(tmp_path):
+    """Random descriptors: the library's text equals the restatement's, and
+    the library's reader and the restatement's reader agree on it."""
+    from hypothesis import HealthCheck, given, settings
+    from hypothesis import strategies as st
+
+    real = st.floats(min_value=-1e12, max_value=1e12, allow_nan=False, allow_infinity=False)
+    axis = st.tuples(st.integers(1, 30), st.sampled_from([0, 1]), st.lists(real, min_size=30, max_size=30), real)
+    word = st.text(alphabet="abcdefghijklmnopqrstuvwxyz_0123456789", min_size=1, max_size=12)
+    title = st.text(alphabet="abcdefghijklmnopqrstuvwxyz ,.()^*/0123456789", min_size=0, max_size=60)
+
+    @settings(max_examples=150, deadline=None, suppress_health_check=[HealthCheck.function_scoped_fixture])
+    @given(ax=axis, ay=axis, az=axis, nt=st.integers(1, 9999), yr=st.sampled_from([0, 1]),
+           date=st.tuples(st.integers(1, 9999), st.integers(1, 12), st.integers(1, 31), st.integers(0, 23),
+                          st.integers(0, 59)),
+           ht=st.floats(min_value=60.0, max_value=5.0e8), title=title, var=word)
+    def run(ax, ay, az, nt, yr, date, ht, title, var):
+        fname = str(tmp_path / "r.dat")
+        args = [fname, -1.0e32]
+        dims = [ax[0], ay[0], az[0], nt]
+        axes = []
+        for n, typ, vals, h in (ax, ay, az):
+            axes += [typ, vals[:n] if typ else vals[:1], h]
+        args += dims + axes + [yr, *date, ht, title, var]
+        dstd.ctl_file_write(*args)
+        _, text = od.ctl_text(*args)
+        assert (tmp_path / "r.ctl").read_text() == text
+        got = _read_both(tmp_path, text, name="r2.ctl")
+        assert got is not None and got["nx"] == ax[0] and got["nt"] == nt and got["varname"] == [var]
+
+    run()
