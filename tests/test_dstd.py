@@ -675,3 +675,68 @@ def test_ctl_write_read_random(tmp_path):
         assert got is not None and got["nx"] == ax[0] and got["nt"] == nt and got["varname"] == [var]
 
     run()
+
+
+def test_field_files_random_boxes(tmp_path):
+    """Random fields, masks, boxes and process grids: wdstd/wdstd8 give the
+    restatement's bytes, rdstd8 reads back the ocean values, and the ranks
+    of a random process grid tiling the box write wdstd's FP32 file with
+    pwdstd and read their parts back with prdstd."""
+    from dataclasses import replace
+
+    from hypothesis import HealthCheck, given, settings
+    from hypothesis import strategies as st
+
+    from inmsom_elfs_b200.grid import Bounds
+
+    @settings(max_examples=60, deadline=None, suppress_health_check=[HealthCheck.function_scoped_fixture])
+    @given(nx=st.integers(6, 20), ny=st.integers(6, 16), nz=st.integers(1, 4), seed=st.integers(0, 10**6),
+           data=st.data())
+    def run(nx, ny, nz, seed, data):
+        rng = np.random.default_rng(seed)
+        g = Bounds.serial(nx - 4, ny - 4)           # arrays 1..nx x 1..ny, interior 3..nx-2 x 3..ny-2
+        f = np.asfortranarray(rng.standard_normal((nx, ny, nz)))
+        lu = np.asfortranarray((rng.random((nx, ny)) > 0.3).astype(np.float32))
+        nzb = data.draw(st.integers(1, nz))
+        nze = data.draw(st.integers(nzb, nz))
+        nfield = data.draw(st.integers(1, 3))
+        box = (data.draw(st.integers(1, 3)), data.draw(st.integers(nx - 2, nx)),
+               data.draw(st.integers(1, 3)), data.draw(st.integers(ny - 2, ny)), nzb, nze)
+        for name, dtype, write in (("a8.dat", np.float64, dstd.wdstd8), ("a4.dat", np.float32, dstd.wdstd)):
+            fx = f.astype(dtype, order="F")
+            p = tmp_path / name
+            if p.exists():
+                p.unlink()
+            write(str(tmp_path), name, nfield, fx.copy(order="F"), lu, box)
+            assert p.read_bytes() == od.file_bytes([(nfield, fx)], lu, box, dtype)   # earlier fields: zeros
+        back = np.zeros_like(f)
+        dstd.rdstd8(str(tmp_path), "a8.dat", nfield, back, lu, box)
+        nxb, nxe, nyb, nye = box[:4]
+        sub = (slice(nxb - 1, nxe), slice(nyb - 1, nye), slice(nzb - 1, nze))
+        ocean = np.broadcast_to((np.abs(lu) >= 0.5)[..., None], f.shape)[sub]
+        assert np.array_equal(back[sub][ocean], f[sub][ocean]) and np.all(back[sub][~ocean] == 0)
+        # a process grid over the interior, with the box equal to the interior
+        xs = sorted(set(data.draw(st.lists(st.integers(g.mmm + 1, g.mm), max_size=2))))
+        ys = sorted(set(data.draw(st.lists(st.integers(g.nnn + 1, g.nn), max_size=2))))
+        xr = list(zip([g.mmm] + xs, [x - 1 for x in xs] + [g.mm]))
+        yr = list(zip([g.nnn] + ys, [y - 1 for y in ys] + [g.nn]))
+        ibox = (g.mmm, g.mm, g.nnn, g.nn, nzb, nze)
+        f4 = f.astype(np.float32, order="F")
+        for p in ("w.dat", "p.dat"):
+            if (tmp_path / p).exists():
+                (tmp_path / p).unlink()
+        dstd.wdstd(str(tmp_path), "w.dat", nfield, f4.copy(order="F"), lu, ibox)
+        ranks = [replace(g, nx_start=a, nx_end=b_, ny_start=c, ny_end=d, bnd_x1=a - 2, bnd_x2=b_ + 2,
+                         bnd_y1=c - 2, bnd_y2=d + 2) for (c, d) in yr for (a, b_) in xr]
+        order = data.draw(st.permutations(range(len(ranks))))
+        for r in order:
+            lb = ranks[r]
+            dstd.pwdstd(lb, str(tmp_path), "p.dat", nfield, _local(f4, g, lb), _local(lu, g, lb), nx, ny, nz, ibox)
+        assert (tmp_path / "p.dat").read_bytes() == (tmp_path / "w.dat").read_bytes()
+        for lb in ranks:
+            loc = np.zeros(lb.shape + (nz,), np.float32, order="F")
+            dstd.prdstd(lb, str(tmp_path), "w.dat", nfield, loc, _local(lu, g, lb), nx, ny, nz, ibox)
+            want = _local(np.where((np.abs(lu) < 0.5)[..., None], od.UNDEF, f4), g, lb)
+            assert np.array_equal(loc[2:-2, 2:-2, nzb - 1:nze], want[2:-2, 2:-2, nzb - 1:nze])
+
+    run()
