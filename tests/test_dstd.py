@@ -740,3 +740,34 @@ def test_field_files_random_boxes(tmp_path):
             assert np.array_equal(loc[2:-2, 2:-2, nzb - 1:nze], want[2:-2, 2:-2, nzb - 1:nze])
 
     run()
+
+
+def test_checkpoint_golden_fixture(tmp_path):
+    """The library writes the committed golden bytes of a seeded checkpoint
+    (tests/golden/make_formats.py) and reads its descriptors as stored."""
+    import importlib.util
+    from pathlib import Path
+    gdir = Path(__file__).resolve().parent / "golden"
+    spec = importlib.util.spec_from_file_location("make_formats", gdir / "make_formats.py")
+    mf = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mf)
+    fix = np.load(gdir / "formats_checkpoint.npz")
+    b, masks, z, zw, st = mf.case()
+    dstd.ocpwrite(str(tmp_path), b, mf.NZ, masks["lu"], masks["llu"], masks["llv"], z, zw, mf.AXES, st)
+    names = sorted(k[5:] for k in fix.files if k.startswith("file:"))
+    assert names == sorted(p.name for p in tmp_path.iterdir()) and len(names) == 30
+    for name in names:
+        assert (tmp_path / name).read_bytes() == fix["file:" + name].tobytes(), name
+    for ctl in ("cptt.ctl", "cpube.ctl"):
+        got = dstd.ctl_file_read(tmp_path / ctl)
+        for key in (k for k in fix.files if k.startswith(f"read:{ctl}:")):
+            name, want = key.split(":")[2], fix[key]
+            g = got[name]
+            if name == "varname":
+                assert "\n".join(g) == str(want)
+            elif name in ("x0", "y0", "z0"):
+                assert np.array_equal(g, want)
+            elif want.dtype.kind in "US":
+                assert g == str(want)
+            else:
+                assert g == want.item(), name
