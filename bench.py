@@ -123,54 +123,125 @@ def config_dict(b, args, nranks):
 
 # ------------------------------------------------------------------ clocks
 class Clocks:
-    def __init__(self, gpu_index: int):
+    """SM clock and clock-event reasons sampled while the timed region runs.
+
+    NVML is polled from a thread every ~1 ms (the timed region of a short
+    run lasts a few milliseconds; the library call releases the GIL), the
+    device found by its PCI bus id so that CUDA and NVML agree on it; if
+    NVML cannot be loaded, nvidia-smi is polled every 100 ms instead.  Only
+    reads: no clock or other setting of the GPU is changed."""
+
+    REASONS = (("hw_slowdown", "nvmlClocksEventReasonHwSlowdown", 0x8),
+               ("hw_thermal_slowdown", "nvmlClocksEventReasonHwThermalSlowdown", 0x40),
+               ("sw_thermal_slowdown", "nvmlClocksEventReasonSwThermalSlowdown", 0x20),
+               ("sw_power_cap", "nvmlClocksEventReasonSwPowerCap", 0x4))
+
+    def __init__(self, cuda_index: int):
+        self.cuda_index = cuda_index
+        self.samples = []          # (sm_mhz, reasons bitmask)
+        self.max_mhz = None
         self.proc = None
-        self.lines = []
-        self.gpu = gpu_index
+        self.stop = threading.Event()
+        self.source = None
+
+    def _nvml_handle(self):
+        import pynvml
+        import torch
+        pynvml.nvmlInit()
+        props = torch.cuda.get_device_properties(self.cuda_index)
+        bus = "%08X:%02X:%02X.0" % (props.pci_domain_id, props.pci_bus_id, props.pci_device_id)
+        try:
+            h = pynvml.nvmlDeviceGetHandleByPciBusId(bus)
+        except Exception:
+            h = pynvml.nvmlDeviceGetHandleByPciBusId(bus[4:])
+        return pynvml, h
 
     def __enter__(self):
+        try:
+            nv, h = self._nvml_handle()
+            self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(h, nv.NVML_CLOCK_SM))
+            get_r = getattr(nv, "nvmlDeviceGetCurrentClocksEventReasons", None) or \
+                nv.nvmlDeviceGetCurrentClocksThrottleReasons
+            self.bits = [(name, getattr(nv, attr, dflt)) for name, attr, dflt in self.REASONS]
+
+            def poll():
+                while not self.stop.is_set():
+                    try:
+                        self.samples.append((float(nv.nvmlDeviceGetClockInfo(h, nv.NVML_CLOCK_SM)),
+                                             int(get_r(h))))
+                    except Exception:
+                        pass
+                    time.sleep(0.001)
+            self.t = threading.Thread(target=poll, daemon=True)
+            self.t.start()
+            self.source = "nvml 1 ms"
+            return self
+        except Exception:
+            pass
         q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
         try:
             self.proc = subprocess.Popen(
                 ["nvidia-smi", f"--query-gpu={q}", "--format=csv,noheader,nounits", "-lms", "100",
-                 "-i", str(self.gpu)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
-            self.t = threading.Thread(target=self._read, daemon=True)
+                 "-i", str(self.cuda_index)], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.t = threading.Thread(target=self._read_smi, daemon=True)
             self.t.start()
+            self.source = "nvidia-smi 100 ms"
         except Exception:
             self.proc = None
         return self
 
-    def _read(self):
+    def _read_smi(self):
+        self.bits = [(name, 1 << i) for i, (name, _, _) in enumerate(self.REASONS)]
         for line in self.proc.stdout:
-            self.lines.append(line.strip())
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                mhz = float(f[1])
+                self.max_mhz = float(f[2])
+            except ValueError:
+                continue
+            mask = 0
+            for i, v in enumerate(f[5:9]):
+                if v.lower().startswith("active"):
+                    mask |= 1 << i
+            self.samples.append((mhz, mask))
 
     def __exit__(self, *exc):
+        self.stop.set()
         if self.proc:
             self.proc.terminate()
             try:
                 self.proc.wait(timeout=5)
             except Exception:
                 self.proc.kill()
+        elif getattr(self, "t", None) is not None:
+            self.t.join(timeout=2)
 
     def summary(self):
-        sm, mx, reasons = [], None, set()
-        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-        for ln in self.lines:
-            f = [x.strip() for x in ln.split(",")]
-            if len(f) < 9:
-                continue
-            try:
-                sm.append(float(f[1]))
-                mx = float(f[2])
-            except ValueError:
-                continue
-            for nm, v in zip(names, f[5:9]):
-                if v.lower().startswith("active"):
-                    reasons.add(nm)
-        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": mx,
-                "reasons": sorted(reasons), "samples": len(sm)}
+        sm = [m for m, _ in self.samples]
+        reasons = set()
+        for _, mask in self.samples:
+            for name, bit in getattr(self, "bits", []):
+                if mask & bit:
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "samples": len(sm), "source": self.source}
+
+
+def gpu_launches(steps: int, fp32_velocity: bool) -> int:
+    """Kernels of one inmsom_run_substeps(steps) on the fused path: one
+    k_minmax3, one fused kernel per step, one k_advance per replayed graph
+    (graphs of min(50, steps rounded down to even) steps); FP32 velocity
+    storage adds three k_to_f32 and one k_vel_from_f32."""
+    n = steps + 1
+    if steps >= 2:
+        n += steps // min(50, steps & ~1)
+    if fp32_velocity:
+        n += 4
+    return n
 
 
 def measured_hbm():
@@ -222,8 +293,11 @@ def run_reference(args):
     b = workload(args, 0)
     basins.finalize(b, ora.OracleBackend())
     ora.hh_init_external(b)
+    # one call advances nstep steps (2*nstep substeps, the second half for
+    # the time means); warm-up and timed calls as many as --warmup and
+    # --steps ask for, the timed ones capped at 20 calls (a bounded sample)
     nstep = 5
-    for _ in range(max(args.warmup, 0) and min(args.warmup, 3)):
+    for _ in range(max(args.warmup, 0)):
         ora.barotropic_dynamics(b, nstep * b.dt, nstep)
     t0 = time.perf_counter()
     ksteps = max(1, min(args.steps, 20))
@@ -234,7 +308,8 @@ def run_reference(args):
     cfg = config_dict(b, args, 1)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
-        "steps": ksteps, "warmup": min(args.warmup, 3), "ms_per_step": el / ksteps * 1e3,
+        "steps": ksteps * nstep, "warmup": max(args.warmup, 0) * nstep,
+        "ms_per_step": el / (ksteps * nstep) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": cfg,
         "cpu_baseline": {"value": v, "unit": METRIC, "cores": threads, "kind": "port",
@@ -367,9 +442,7 @@ def run_ours(args):
                          "bytes_per_cell_step": bpc,
                          "peak_kind": f"{peak_kind} HBM copy bandwidth"},
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
-            # one fused kernel per step, one k_advance per replayed graph of
-            # 50 steps (runs of 100 steps or more), one k_minmax3 per run
-            "gpu_launches": args.steps + (args.steps // 50 if args.steps >= 100 and not args.fp32_velocity else 0) + 1,
+            "gpu_launches": gpu_launches(args.steps, args.fp32_velocity),
             "path": path[1], "guard_bad_points": nbad,
         }
         print(json.dumps(line), flush=True)

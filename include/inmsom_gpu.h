@@ -337,10 +337,18 @@ int inmsom_gpu_diag(inmsom_ctx *ctx, double *volume, double *energy);
  * cleared, but calls whose work overlaps on the GPU (unordered streams)
  * race on that array and may return wrong sums -- order them on one stream
  * or with events.  The first call on each device looks up the array's
- * device address (cudaGetSymbolAddress); make that first call before any
- * stream capture begins.  More than INMSOM_DIAG_NOALLOC_MAX_ROWS interior
- * rows returns INMSOM_EARG without touching the device.  An empty interior
- * gives volume = energy = 0. */
+ * device address (cudaGetSymbolAddress) under the current CUDA context and
+ * caches it for that context (a call under another context of the device,
+ * e.g. after cudaDeviceReset, looks it up again); make that first call
+ * before any stream capture begins.  CUDA loads device code lazily by
+ * default (CUDA_MODULE_LOADING=LAZY), so that first call is also when the
+ * driver loads this part of the library onto the device and reserves the
+ * array there: a caller whose memory pool takes the device's memory makes
+ * its first call before the pool does, or sets CUDA_MODULE_LOADING=EAGER
+ * so that the array is reserved when the CUDA context is created.  More
+ * than INMSOM_DIAG_NOALLOC_MAX_ROWS interior rows returns INMSOM_EARG
+ * without touching the device.  An empty interior gives
+ * volume = energy = 0. */
 int inmsom_diag_noalloc(const inmsom_bounds *b, const inmsom_consts *c, long long ld,
                         const float *lu, const float *lcu, const float *lcv,
                         const double *dx, const double *dy, const double *dxt,

@@ -506,14 +506,83 @@ int inmsom_load_state(inmsom_ctx *c, double *ubrtr_e, double *ubrtrp_e, double *
 
 namespace {
 
-constexpr int RS_GROUP = 50;   // substeps per graph replay (even: the state stays in its set)
+constexpr int RS_GROUP = 50;   // most substeps per graph replay
+
+// substeps per replayed graph for a run of nsub: even, so that a replay
+// leaves the state in the set it started from
+int rs_length(int nsub) { return std::min(RS_GROUP, nsub & ~1); }
+
+bool rs_current(const inmsom_ctx *c, int len, double dt)
+{
+    const fused::Plan &p = c->plan;
+    return c->rs_exec && c->rs_len == len && c->rs_gen == p.generation && c->rs_dt == dt &&
+           c->rs_src == c->state[0] && c->rs_pgen == p.prep_gen && c->rs_mu0 == p.prep_mu0 &&
+           c->rs_rd0 == p.prep_rd0 && c->rs_wq0 == p.prep_wq0;
+}
+
+// capture len fused launches (and the counter advance) as the context's
+// replayed graph, with the forcing mode of the plan's last preparation
+int rs_capture(inmsom_ctx *c, int len, double dt)
+{
+    const bool f32 = (c->flags & INMSOM_FP32_VELOCITY) != 0;
+    fused::Plan &p = c->plan;
+    if (c->rs_exec) cudaGraphExecDestroy(c->rs_exec);
+    c->rs_exec = nullptr;
+    cudaGraph_t g = nullptr;
+    CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
+    const int lrc = f32 ? fused::launch_steps_f32(p, c->dom, c->c, dt, len, c->d_rs, c->d_base, nullptr, c->state,
+                                                  c->stream)
+                        : fused::launch_steps(p, c->dom, c->c, dt, len, c->d_rs, c->d_base, c->state, c->stream);
+    if (lrc == 0) k_advance<<<1, 1, 0, c->stream>>>(c->d_base, len);
+    const cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
+    if (lrc || ce != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return set_err(INMSOM_ECUDA, "fused substeps: graph capture failed: %s", cudaGetErrorString(ce));
+    }
+    const cudaError_t ie = cudaGraphInstantiate(&c->rs_exec, g, 0);
+    cudaGraphDestroy(g);
+    if (ie != cudaSuccess) return set_err(INMSOM_ECUDA, "fused substeps: %s", cudaGetErrorString(ie));
+    c->rs_len = len;
+    c->rs_gen = p.generation;
+    c->rs_dt = dt;
+    c->rs_src = c->state[0];
+    c->rs_pgen = p.prep_gen;
+    c->rs_mu0 = p.prep_mu0;
+    c->rs_rd0 = p.prep_rd0;
+    c->rs_wq0 = p.prep_wq0;
+    return INMSOM_OK;
+}
+
+// Set-up of a graph run that needs no device work: the per-substep scale
+// buffer and, when an earlier graph run prepared the plan, the capture of
+// this run's graph with that run's forcing mode (kept if the preparation
+// of this run finds the same mode).  Host work only, so it stays out of
+// the run's timed region.
+int rs_setup(inmsom_ctx *c, int nsub, double dt)
+{
+    if (!c->d_base) CK(cudaMalloc(&c->d_base, sizeof(int)));
+    if ((size_t)nsub > c->rs_cap) {
+        if (c->rs_exec) cudaGraphExecDestroy(c->rs_exec);
+        c->rs_exec = nullptr;   // it holds the old buffer
+        CK(cudaStreamSynchronize(c->stream));
+        cudaFree(c->d_rs);
+        c->d_rs = nullptr;
+        c->rs_cap = 0;
+        CK(cudaMalloc(&c->d_rs, (size_t)nsub * sizeof(double)));
+        c->rs_cap = (size_t)nsub;
+    }
+    const int len = rs_length(nsub);
+    if (c->rs_pgen >= 0 && c->plan.prepared && !rs_current(c, len, dt)) CKR(rs_capture(c, len, dt));
+    return INMSOM_OK;
+}
 
 // inmsom_run_substeps on the fused path as replays of one captured graph of
-// RS_GROUP launches (launch gaps removed: 2-3 % on the 2048 x 1536 basin);
-// the RHS scale of every substep is read on the device at a counter the
-// graph advances.  The graph is recaptured when dt, the work items or the
-// state's set change.  FP32 velocity storage: the same with its kernel,
-// between the conversions to and from FP32.
+// rs_length(nsub) launches (launch gaps removed: 2-3 % on the 2048 x 1536
+// basin); the RHS scale of every substep is read on the device at a counter
+// the graph advances.  The graph is recaptured when its length, dt, the
+// work items, the state's set or the forcing mode change.  FP32 velocity
+// storage: the same with its kernel, between the conversions to and from
+// FP32.
 int run_substeps_graph(inmsom_ctx *c, int nsub, double dt, const double *rhs_scale)
 {
     const bool f32 = (c->flags & INMSOM_FP32_VELOCITY) != 0;
@@ -532,41 +601,14 @@ int run_substeps_graph(inmsom_ctx *c, int nsub, double dt, const double *rhs_sca
                                              c->stream)
                    : fused::launch_steps(c->plan, c->dom, c->c, dt, n, c->d_rs, c->d_base, c->state, c->stream);
     };
-    if (!c->d_base) CK(cudaMalloc(&c->d_base, sizeof(int)));
-    if ((size_t)nsub > c->rs_cap) {
-        if (c->rs_exec) cudaGraphExecDestroy(c->rs_exec);
-        c->rs_exec = nullptr;   // it holds the old buffer
-        cudaFree(c->d_rs);
-        c->d_rs = nullptr;
-        c->rs_cap = 0;
-        CK(cudaMalloc(&c->d_rs, (size_t)nsub * sizeof(double)));
-        c->rs_cap = (size_t)nsub;
-    }
     std::vector<double> rs((size_t)nsub, 1.0);
     if (rhs_scale)
         for (int k = 0; k < nsub; k++) rs[k] = rhs_scale[k];
     CK(cudaMemcpyAsync(c->d_rs, rs.data(), (size_t)nsub * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(c->d_base, 0, sizeof(int), c->stream));
-    if (!c->rs_exec || c->rs_gen != c->plan.generation || c->rs_dt != dt || c->rs_src != c->state[0]) {
-        if (c->rs_exec) cudaGraphExecDestroy(c->rs_exec);
-        c->rs_exec = nullptr;
-        cudaGraph_t g = nullptr;
-        CK(cudaStreamBeginCapture(c->stream, cudaStreamCaptureModeThreadLocal));
-        const int lrc = launch(RS_GROUP);
-        if (lrc == 0) k_advance<<<1, 1, 0, c->stream>>>(c->d_base, RS_GROUP);
-        const cudaError_t ce = cudaStreamEndCapture(c->stream, &g);
-        if (lrc || ce != cudaSuccess) {
-            if (g) cudaGraphDestroy(g);
-            return set_err(INMSOM_ECUDA, "fused substeps: graph capture failed: %s", cudaGetErrorString(ce));
-        }
-        const cudaError_t ie = cudaGraphInstantiate(&c->rs_exec, g, 0);
-        cudaGraphDestroy(g);
-        if (ie != cudaSuccess) return set_err(INMSOM_ECUDA, "fused substeps: %s", cudaGetErrorString(ie));
-        c->rs_gen = c->plan.generation;
-        c->rs_dt = dt;
-        c->rs_src = c->state[0];
-    }
-    const int groups = nsub / RS_GROUP, rest = nsub % RS_GROUP;
+    const int len = rs_length(nsub);
+    if (!rs_current(c, len, dt)) CKR(rs_capture(c, len, dt));
+    const int groups = nsub / len, rest = nsub % len;
     for (int gi = 0; gi < groups; gi++) CK(cudaGraphLaunch(c->rs_exec, c->stream));
     if (rest && launch(rest)) return set_err(INMSOM_ECUDA, "fused substeps: launch failed");
     const int frc = f32 ? fused::finish_steps_f32(c->plan, c->dom, c->state, c->stream)
@@ -586,8 +628,10 @@ int inmsom_run_substeps(inmsom_ctx *c, int nsub, double dt, const double *rhs_sc
         return set_err(INMSOM_EARG, "no resident state: call inmsom_load_state or barotropic_dynamics first");
     if ((c->flags & INMSOM_FP32_VELOCITY) && !c->fused_ok)
         return set_err(INMSOM_EUNSUPPORTED, "FP32 velocity storage needs the fused path (%s)", c->fused_reason);
+    const bool graph = c->fused_ok && nsub >= 2;
+    if (graph) CKR(rs_setup(c, nsub, dt));
     CK(cudaEventRecord(c->ev0, c->stream));
-    if (c->fused_ok && nsub >= 2 * RS_GROUP) {
+    if (graph) {
         CKR(run_substeps_graph(c, nsub, dt, rhs_scale));
         c->depths_current = false;
         if (c->plan.last_flags & (fused::FLAG_TIMEOUT | fused::FLAG_SMEM)) return fused_flag_error(c, "fused kernel");

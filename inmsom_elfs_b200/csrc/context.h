@@ -104,11 +104,15 @@ struct inmsom_ctx {
     bool scratch_on_device = false;
 
     fused::Plan plan{};              // fused-path layout and eligibility
-    // run_substeps as replays of a graph of RS_GROUP substeps
+    // run_substeps as replays of a graph of rs_len (even, <= RS_GROUP) substeps
     cudaGraphExec_t rs_exec = nullptr;
     unsigned rs_gen = 0;
     const double *rs_src = nullptr;  // state set the graph reads first (an odd run moves the state)
     double rs_dt = 0.0;
+    int rs_len = 0;
+    // the forcing mode the graph's launches were captured with
+    int rs_pgen = -1;
+    double rs_mu0 = 0.0, rs_rd0 = 0.0, rs_wq0 = 0.0;
     double *d_rs = nullptr;          // RHS scale per substep of the run
     size_t rs_cap = 0;
     int *d_base = nullptr;           // first substep of the next replay

@@ -8,8 +8,13 @@
 // the inputs and the two-double output, but it cannot give this library room
 // for the reduction's scratch.  The scratch -- one volume and one energy
 // partial per interior row -- therefore lives in a fixed array that is part
-// of this file's device image: the CUDA runtime reserves it on each GPU that
-// loads the image and keeps it until the process exits.
+// of this file's device image: the CUDA driver reserves it on each GPU when
+// it loads the image there and keeps it until the process exits.  CUDA 12
+// loads device images lazily by default, so on each device that happens at
+// the first call here (the address look-up below), together with the
+// reduction kernels' code -- not when the library is loaded.  A caller whose
+// pool is about to claim the device's memory therefore makes one call (or
+// runs with CUDA_MODULE_LOADING=EAGER) before the pool does.
 //
 // The array is shared by every call on a device and keeps whatever the last
 // call left in it.  The row kernel writes every partial that the final
@@ -38,8 +43,18 @@ namespace {
 
 constexpr int kMaxDevices = 64;
 
+// cuCtxGetCurrent from the driver, reached through the runtime (the library
+// does not link libcuda): the address of the array belongs to one CUDA
+// context, so the cache below keys on the context as well as the device.
+typedef int (*CtxGetCurrentFn)(void **ctx);
+
 std::mutex g_setup_mutex;
-double *g_rows_on_device[kMaxDevices] = {};
+struct Resolved {
+    void *ctx = nullptr;
+    double *rows = nullptr;
+};
+Resolved g_rows_on_device[kMaxDevices];
+CtxGetCurrentFn g_ctx_get_current = nullptr;
 
 int fail(int code, const char *fmt, ...)
 {
@@ -53,8 +68,11 @@ int fail(int code, const char *fmt, ...)
 
 // Device address of g_diag_rows on the current device.  In host code the
 // name g_diag_rows only stands for the array; its address on a given GPU
-// comes from cudaGetSymbolAddress with that GPU current, looked up once per
-// device on its first call here and cached.
+// comes from cudaGetSymbolAddress with that GPU current.  It is looked up
+// once per device, on the first call there, and cached together with the
+// CUDA context that was current; a call under another context of that
+// device (after cudaDeviceReset, or with a context the caller made current
+// through the driver) looks it up again for that context.
 int rows_scratch(double **rows)
 {
     int dev = -1;
@@ -66,17 +84,35 @@ int rows_scratch(double **rows)
         return fail(INMSOM_EUNSUPPORTED, "inmsom_diag_noalloc: device %d beyond %d", dev,
                     kMaxDevices);
     std::lock_guard<std::mutex> lock(g_setup_mutex);
-    if (!g_rows_on_device[dev]) {
-        void *p = nullptr;
-        e = cudaGetSymbolAddress(&p, g_diag_rows);
-        if (e != cudaSuccess || !p)
+    if (!g_ctx_get_current) {
+        void *fn = nullptr;
+        cudaDriverEntryPointQueryResult qr{};
+        e = cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &qr);
+        if (e != cudaSuccess || qr != cudaDriverEntryPointSuccess || !fn)
+            return fail(INMSOM_ECUDA, "inmsom_diag_noalloc: cuCtxGetCurrent not found: %s",
+                        cudaGetErrorString(e));
+        g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(fn);
+    }
+    Resolved &r = g_rows_on_device[dev];
+    void *ctx = nullptr;
+    if (g_ctx_get_current(&ctx) != 0) ctx = nullptr;
+    if (!ctx || r.ctx != ctx) {
+        // first call on this device (or under a new context): the look-up
+        // also makes the runtime's context current when none is yet
+        void *addr = nullptr;
+        e = cudaGetSymbolAddress(&addr, g_diag_rows);
+        if (e != cudaSuccess || !addr)
             return fail(INMSOM_ECUDA,
                         "inmsom_diag_noalloc: cudaGetSymbolAddress of the scratch array on "
                         "device %d failed: %s",
                         dev, cudaGetErrorString(e));
-        g_rows_on_device[dev] = static_cast<double *>(p);
+        if (g_ctx_get_current(&ctx) != 0 || !ctx)
+            return fail(INMSOM_ECUDA, "inmsom_diag_noalloc: no current CUDA context on device %d",
+                        dev);
+        r.ctx = ctx;
+        r.rows = static_cast<double *>(addr);
     }
-    *rows = g_rows_on_device[dev];
+    *rows = r.rows;
     return INMSOM_OK;
 }
 
@@ -136,11 +172,17 @@ extern "C" int inmsom_diag_noalloc(const inmsom_bounds *b, const inmsom_consts *
     k.ts = c->time_smooth; k.g = c->free_fall_acc; k.rho = c->ref_den; k.ffs = c->full_free_surface;
 
     cudaStream_t s = static_cast<cudaStream_t>(stream);
+    // an error left pending by an earlier, unrelated runtime call stays
+    // pending for its owner: only an error these launches raise is taken
+    // (and cleared) as this call's failure
+    const cudaError_t before = cudaPeekAtLastError();
     general::diag_rows(d, g, k, ssh, u, v, hu, hv, rows, s);
     general::diag_final((int)nrows, rows, out, s);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess)
+    const cudaError_t e = cudaPeekAtLastError();
+    if (e != cudaSuccess && e != before) {
+        cudaGetLastError();
         return fail(INMSOM_ECUDA, "inmsom_diag_noalloc: kernel launch failed: %s",
                     cudaGetErrorString(e));
+    }
     return INMSOM_OK;
 }

@@ -7,7 +7,8 @@ through the C ABI on caller-owned device arrays, twice in a row on two
 different basins (the second with fewer rows, so stale partials of the first
 call would show) and once more on the first basin with a padded row pitch,
 and compares each result with inmsom_gpu_diag of a context holding the same
-state, within the diagnostic's tolerance.
+state, within the diagnostic's tolerance; the device's free memory is the
+same before and after each call but the first.
 """
 import ctypes
 
@@ -82,12 +83,18 @@ def test_noalloc_diag_matches_context_diag(gpu):
     nxa_b = b.bounds.bnd_x2 - b.bounds.bnd_x1 + 1
 
     calls = ((a, nxa_a, want_a), (b, nxa_b, want_b), (a, nxa_a + 37, want_a))
-    for basin, ld, (vol, en) in calls:
+    for i, (basin, ld, (vol, en)) in enumerate(calls):
         fields = _fields(torch, basin, ld)
         out = torch.full((2,), float("nan"), dtype=torch.float64, device="cuda:0")
+        torch.cuda.synchronize()
+        free0 = torch.cuda.mem_get_info(0)[0]
         rc = _call(lib, basin.bounds, basin.consts, ld, fields, out, stream.cuda_stream)
         assert rc == 0, lib.inmsom_gpu_last_error().decode()
         got = out.cpu().numpy()          # waits for the stream
+        if i > 0:
+            # after the first call (which may load the device code and the
+            # array), a call takes no device memory at all
+            assert torch.cuda.mem_get_info(0)[0] == free0
         assert abs(got[0] - vol) <= TOL * abs(vol), (got[0], vol)
         assert abs(got[1] - en) <= TOL * abs(en), (got[1], en)
         assert en > 0.0
