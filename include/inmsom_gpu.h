@@ -397,6 +397,21 @@ int inmsom_load_state(inmsom_ctx *ctx, double *ubrtr_e, double *ubrtrp_e,
  * reference rounding), 1 = fused streaming kernel.  *reason receives a
  * static string saying why the fused path is not eligible (or "eligible"). */
 int inmsom_gpu_path(inmsom_ctx *ctx, int *path, const char **reason);
+
+/* Test hook of the fused kernel's bounded waits.  No counterpart in the
+ * reference, which has no wait to bound: its failure path is `stop`
+ * (Control/dyncall.f90:452-516).  Until called again with item = -1, work
+ * item `item` of every fused substep launch on this context does not issue
+ * the copies of its `ring_row`-th input row (0 = the first row it loads;
+ * clamped to its last), so its wait for that row gives up, and every
+ * bounded wait of those launches gives up after `wait_polls` polls of
+ * mbarrier.try_wait (0 = the built-in 2^20).  The CTA that gave up sets a
+ * status bit, waits (bounded) for the copies it did issue and returns; the
+ * call that ran the launch returns INMSOM_ETIMEOUT and leaves its outputs
+ * undefined (reload the state with inmsom_load_state or a copy-in call).
+ * Nothing faults and the context stays usable: with item = -1 the next
+ * calls compute normally. */
+int inmsom_test_hold_copy(inmsom_ctx *ctx, int item, int ring_row, unsigned wait_polls);
 /* Device time of the phases of the last completed
  * inmsom_barotropic_dynamics, inmsom_baroclinic_dynamics,
  * inmsom_vertical_velocity or inmsom_tracer_tran_diff call (CUDA events on the context's stream):

@@ -34,6 +34,7 @@ EXPORTS = (
     "inmsom_write_checkpoint", "inmsom_read_checkpoint", "inmsom_tracer_tran_diff", "inmsom_ctl_file_read",
     "inmsom_pwdstd", "inmsom_prdstd", "inmsom_ocpwrite", "inmsom_ocpread",
     "inmsom_compare_grids", "inmsom_stress_components", "inmsom_smagorinsky_coeff",
+    "inmsom_test_hold_copy",
 )
 
 # include/inmsom_gpu.h: INMSOM_MLP_*
@@ -119,6 +120,7 @@ def load() -> ctypes.CDLL:
     lib.inmsom_run_substeps.argtypes = [VP, i, d, DP, ctypes.POINTER(ctypes.c_float)]
     lib.inmsom_load_state.argtypes = [VP] + [DP] * 12
     lib.inmsom_gpu_path.argtypes = [VP, ctypes.POINTER(i), ctypes.POINTER(ctypes.c_char_p)]
+    lib.inmsom_test_hold_copy.argtypes = [VP, i, i, ctypes.c_uint]
     lib.inmsom_gpu_finalize.argtypes = [VP]
     lib.inmsom_ens_create.argtypes = [ctypes.POINTER(VP), ctypes.POINTER(VP), i, i]
     lib.inmsom_ens_run.argtypes = [VP, i, DP, DP, ctypes.POINTER(ctypes.c_float)]

@@ -13,6 +13,8 @@ Workloads (sizes are significant points):
                      log-normal shallow depth, smooth random wind
   ridge_basin        4096x4096, 2 km, 4000 m with a 200 m-rms ridge
   spherical_basin    lat-lon grid with the reference's spherical metrics
+  williamson2_basin  Williamson et al.'s shallow-water test 2 on a
+                     zonally periodic lat-lon band (analytic steady state)
 """
 from __future__ import annotations
 
@@ -311,6 +313,84 @@ def spherical_basin(nx: int = 48, ny: int = 32, rlon: float = 27.5, rlat: float 
     basin.info.update(workload="spherical_basin", nx=nx, ny=ny, seed=seed,
                       rotation_on_lat=rotation_on_lat)
     return basin.fill_defaults()
+
+
+WILLIAMSON2_DEPTH = 3000.0        # g*h0 = 2.94e4 m^2/s^2 with g = 9.8
+WILLIAMSON2_U0 = 2.0 * math.pi * RAD_EARTH / (12.0 * 86400.0)
+
+
+def williamson2_fields(basin: Basin):
+    """Analytic state of Williamson et al.'s shallow-water test 2 with
+    alpha = 0 (steady zonal geostrophic flow) on the basin's T rows and u
+    points: eta = -(R*Omega*u0 + u0^2/2) sin^2(lat)/g, u = u0 cos(lat),
+    v = 0, with the latitude of each T row as the grid set-up gives it.
+    Returns (eta, u) as full arrays, zero off the lu / lcu masks."""
+    b = basin.bounds
+    info = basin.info
+    n = np.arange(b.bnd_y1, b.bnd_y2 + 1, dtype=np.float64)
+    lat = info["rlat"] + (n - b.nnn) * info["dyst"]
+    s = np.sin(DPIP180 * lat)
+    g = basin.consts.free_fall_acc
+    u0 = WILLIAMSON2_U0
+    eta = -(RAD_EARTH * EARTH_ANG_VEL * u0 + 0.5 * u0 * u0) * s * s / g
+    uu = u0 * np.cos(DPIP180 * lat)
+    m = basin.masks
+    eta2 = np.asfortranarray(np.broadcast_to(eta[None, :], b.shape) * (m["lu"] > 0.5))
+    u2 = np.asfortranarray(np.broadcast_to(uu[None, :], b.shape) * (m["lcu"] > 0.5))
+    return eta2, u2
+
+
+def williamson2_basin(dlon: float = 2.5, dlat: float = 2.0, lat_max: float = 80.0,
+                      dt: Optional[float] = None, backend=None) -> Basin:
+    """Williamson et al.'s shallow-water test 2 (alpha = 0) on the
+    reference's spherical grid: a zonally periodic lat-lon band of dlon x
+    dlat degrees between -lat_max and lat_max, closed by land rows (the
+    exact solution has v = 0, so the walls are consistent with it), flat
+    rest depth 3000 m, no viscosity, drag, wind or water flux; the state
+    starts at the analytic solution (williamson2_fields) at both time
+    levels.  The test the thesis of the reference reports (dipl. p.27):
+    relative max-norm error of the level after 5 days, 6.93e-6 on 2.5 x 2.0
+    degrees and 1.74e-6 on 1.25 x 1.0.  dt defaults to 60 s per degree of
+    latitude spacing (gravity-wave stability number 0.83 for the rest depth
+    at the band's edge, 0.52 for the depth there).  backend (gridcon) derives the masks; the state is set
+    when it is given."""
+    nx = int(round(360.0 / dlon))
+    ny = int(round(2.0 * lat_max / dlat))
+    b = Bounds.serial(nx, ny, periodicity_x=1)
+    basin = Basin(b, Consts())
+    lu = b.zeros(np.float32)
+    lu[:, b.nnn - b.bnd_y1:b.nn - b.bnd_y1 + 1] = 1.0   # every column: the wrap sees ocean
+    basin.masks["lu"] = lu
+    rlon, rlat = 0.5 * dlon, -lat_max + 0.5 * dlat
+    spherical_metrics(basin, rlon, rlat, dlon, dlat)
+    basin.hhq_rest = np.asfortranarray(np.where(lu > 0.5, WILLIAMSON2_DEPTH, 0.0))
+    basin.dt = 60.0 * dlat if dt is None else dt
+    basin.info.update(workload="williamson2", nx=nx, ny=ny, rlon=rlon, rlat=rlat, dxst=dlon,
+                      dyst=dlat, lat_max=lat_max)
+    basin.fill_defaults()
+    if backend is not None:
+        basin.masks.update(backend.gridcon(b, lu))
+        eta, u = williamson2_fields(basin)
+        for k in ("ssh_e", "sshp_e"):
+            basin.state[k][...] = eta
+        for k in ("ubrtr_e", "ubrtrp_e"):
+            basin.state[k][...] = u
+        # the periodic wrap of the initial state (cyclize8_x): gridcon leaves
+        # the u mask of the last ring column at land, the wrap fills it
+        i0, i1 = b.mmm - b.bnd_x1, b.mm - b.bnd_x1
+        for a in basin.state.values():
+            a[i0 - 1], a[i1 + 1] = a[i1].copy(), a[i0].copy()
+    return basin
+
+
+def williamson2_error(basin: Basin) -> float:
+    """max |h - h_T| / max h_T over the ocean points, h = rest depth + level
+    (the thesis's l_inf of the level, normalised by the analytic depth)."""
+    b = basin.bounds
+    eta, _ = williamson2_fields(basin)
+    ocean = basin.masks["lu"][b.interior] > 0.5
+    err = np.abs(basin.state["ssh_e"][b.interior] - eta[b.interior])[ocean].max()
+    return float(err / (basin.hhq_rest[b.interior] + eta[b.interior])[ocean].max())
 
 
 def cfl_number(basin: Basin) -> float:

@@ -382,6 +382,17 @@ int inmsom_gpu_path(inmsom_ctx *c, int *path, const char **reason)
     return INMSOM_OK;
 }
 
+int inmsom_test_hold_copy(inmsom_ctx *c, int item, int ring_row, unsigned wait_polls)
+{
+    if (!c) return set_err(INMSOM_EARG, "NULL context");
+    if (item < -1 || ring_row < 0) return set_err(INMSOM_EARG, "inmsom_test_hold_copy: item < -1 or ring_row < 0");
+    c->plan.hold_item = item;
+    c->plan.hold_row = item < 0 ? -1 : ring_row;
+    c->plan.wait_limit = item < 0 ? 0u : wait_polls;
+    c->plan.generation++;   // captured graphs hold the old parameters
+    return INMSOM_OK;
+}
+
 int inmsom_barotropic_dynamics(inmsom_ctx *c, double tau, int nstep, int ksw4, double *ubrtr_e,
                                double *ubrtrp_e, double *vbrtr_e, double *vbrtrp_e, double *ssh_e,
                                double *sshp_e, double *ubrtr_i, double *vbrtr_i,

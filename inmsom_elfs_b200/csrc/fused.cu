@@ -79,6 +79,12 @@ struct alignas(64) Params {
     const double *rs_dev;
     const int *rs_base;
     int rs_k;
+    // polls of a bounded mbarrier wait before it gives up; and a test hook:
+    // work item hold_item (-1: none) does not issue the copies of its
+    // hold_row-th ring row (counted from its first, clamped to its last),
+    // so that its wait for that row runs out
+    unsigned wait_limit;
+    int hold_item, hold_row;
 };
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
@@ -123,9 +129,9 @@ __device__ __forceinline__ bool mbar_test(uint64_t *bar, uint32_t parity)
     return ok != 0;
 }
 
-__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity)
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, uint32_t parity, unsigned limit)
 {
-    for (unsigned i = 0; i < WAIT_LIMIT; i++)
+    for (unsigned i = 0; i < limit; i++)
         if (mbar_try_wait(bar, parity)) return true;
     return false;
 }
@@ -369,6 +375,7 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
 #define CF(o, x) (reinterpret_cast<const RowCoef *>(ring + (o) + L::COEF_OFF)->x)
 
     auto issue = [&](int row, int slot) {
+        if ((int)blockIdx.x == p.hold_item && row == min(row_lo + p.hold_row, row_hi)) return;   // test hook
         issue_row<GEN, F32>(ring + slot * L::SLOT_B, &mbar[slot], tm_src, &p.tm_stat, &p.tm_ssh, &p.tm_rhs, p.rows + row,
                        p.bits + (size_t)row * p.bm_words + wbase, g0, row);
     };
@@ -395,8 +402,8 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
     uint32_t mk = 0;
     int waited = row_lo - 1;
     bool ready = false;   // row j+1 found complete by a test in the previous iteration
-    bool ok = mbar_wait(&mbar[0], 0);
-    ok = __all_sync(0xffffffffu, ok && mbar_wait(&mbar[1], 0));
+    bool ok = mbar_wait(&mbar[0], 0, p.wait_limit);
+    ok = __all_sync(0xffffffffu, ok && mbar_wait(&mbar[1], 0, p.wait_limit));
     if (ok) waited = row_lo + 1;
 
     S1 A{}, B{};
@@ -419,7 +426,7 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
         const int o_m2 = i_m2 * L::SLOT_B, o_m1 = i_m1 * L::SLOT_B, o_0 = i_0 * L::SLOT_B, o_p1 = i_p1 * L::SLOT_B;
         if constexpr (D1) {   // stage 1 reads row j+1
             if (!__all_sync(0xffffffffu, ready)) {
-                ok = __all_sync(0xffffffffu, mbar_wait(&mbar[i_p1], ph));
+                ok = __all_sync(0xffffffffu, mbar_wait(&mbar[i_p1], ph, p.wait_limit));
                 if (!ok) return;
             }
             waited = j + 1;
@@ -694,7 +701,8 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
             atomicOr(p.flags, FLAG_TIMEOUT);
             // drain this CTA's copies still in flight (bounded) before exiting
             for (int row = waited + 1; row <= issued; row++)
-                (void)mbar_wait(&mbar[(row - row_lo) % RING], (uint32_t)(((row - row_lo) / RING) & 1));
+                (void)mbar_wait(&mbar[(row - row_lo) % RING], (uint32_t)(((row - row_lo) / RING) & 1),
+                                p.wait_limit);
         }
         return false;
     }
@@ -854,6 +862,9 @@ Params base_params(const Plan &p, const Dom &d, const Consts &c, const Forcing &
     q.rhs_scale = 1.0;
     q.vort_zero = p.vort_zero ? 1 : 0;
     q.flags = p.d_flags;
+    q.wait_limit = p.wait_limit ? p.wait_limit : WAIT_LIMIT;
+    q.hold_item = p.hold_item;
+    q.hold_row = p.hold_row;
     q.d = p.d;
     q.inv_d = p.d != 0.0 ? 1.0 / p.d : 0.0;
     q.d4 = p.d / 4.0;

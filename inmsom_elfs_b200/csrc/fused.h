@@ -121,6 +121,10 @@ struct Plan {
     bool vort_zero = false;
     bool buffers_synced = false;    // buf[][] hold the state's land/halo values
     unsigned last_flags = 0;        // status bits of the last run
+    // bounded waits: polls before giving up (0: the built-in 2^20); test
+    // hook: item hold_item withholds the copies of its hold_row-th ring row
+    unsigned wait_limit = 0;
+    int hold_item = -1, hold_row = -1;
     int last_variant = -1;          // 0 uniform, 1 general, 2 uniform with FP32 velocities (last launch)
 };
 
