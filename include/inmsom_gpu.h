@@ -60,6 +60,17 @@ extern "C" {
                                      uniform grid with uniform viscosity, drag
                                      and water flux (else INMSOM_EUNSUPPORTED);
                                      barotropic_dynamics stays FP64.           */
+#define INMSOM_STATIC_COEFFS 0x10u /* with INMSOM_RESIDENT: the coefficient
+                                     fields wflux, mu, rdis (and mu4) are
+                                     copied in by the first barotropic_dynamics
+                                     call that reads them and stay on the
+                                     device; later calls copy in only RHSx and
+                                     RHSy.  INMSOM sets mu and rdis once at
+                                     start-up (Control/init_pars.f90:166-167,
+                                     :459-481); a host that changes them (or
+                                     wflux) calls inmsom_gpu_sync_from_host
+                                     with INMSOM_SYNC_COEFFS, and the next call
+                                     copies them in again.                      */
 
 /* Domain bounds: Modules/mod_mpi_parallel_tools.f90:7-15 (local interior
  * nx_start..ny_end and array bounds bnd_x1..bnd_y2), global significant area
@@ -363,6 +374,9 @@ int inmsom_diag_noalloc(const inmsom_bounds *b, const inmsom_consts *c, long lon
 #define INMSOM_SYNC_STATE   0x1u /* ubrtr_e ubrtrp_e vbrtr_e vbrtrp_e ssh_e sshp_e */
 #define INMSOM_SYNC_DEPTHS  0x2u /* the twelve external depth arrays              */
 #define INMSOM_SYNC_SCRATCH 0x4u /* vort str_t2d str_s2d fx fy RHS*_adv RHS*_dif  */
+#define INMSOM_SYNC_COEFFS  0x8u /* from_host only, INMSOM_STATIC_COEFFS contexts:
+                                    the next barotropic_dynamics call copies
+                                    wflux, mu, rdis and mu4 in again          */
 int inmsom_gpu_sync_to_host(inmsom_ctx *ctx, unsigned what);
 int inmsom_gpu_sync_from_host(inmsom_ctx *ctx, unsigned what);
 

@@ -13,8 +13,8 @@ import numpy as np
 LIB_PATH = Path(__file__).resolve().with_name("libinmsom_gpu.so")
 
 OK, ECUDA, EARG, EGUARD, ETIMEOUT, EUNSUPPORTED = 0, 1, 2, 3, 4, 5
-RESIDENT, FORCE_GENERAL, GUARD, FP32_VELOCITY = 0x1, 0x2, 0x4, 0x8
-SYNC_STATE, SYNC_DEPTHS, SYNC_SCRATCH = 0x1, 0x2, 0x4
+RESIDENT, FORCE_GENERAL, GUARD, FP32_VELOCITY, STATIC_COEFFS = 0x1, 0x2, 0x4, 0x8, 0x10
+SYNC_STATE, SYNC_DEPTHS, SYNC_SCRATCH, SYNC_COEFFS = 0x1, 0x2, 0x4, 0x8
 
 # every exported entry point declared in include/inmsom_gpu.h
 EXPORTS = (

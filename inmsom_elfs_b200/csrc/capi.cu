@@ -355,6 +355,7 @@ int inmsom_gpu_register_grid(inmsom_ctx *c, const float *lu, const float *luu, c
     c->grid_ok = true;
     c->state_on_device = false;
     c->scratch_on_device = false;
+    for (int k = 0; k < NFORC; k++) c->coef_on_device[k] = false;
     // fused-path eligibility and its static tables (host-side checks)
     c->fused_ok = false;
     if (c->flags & INMSOM_FORCE_GENERAL) {
@@ -426,9 +427,13 @@ int inmsom_barotropic_dynamics(inmsom_ctx *c, double tau, int nstep, int ksw4, d
         for (int k = 0; k < NSCR; k++) CKR(h2d(c, c->scr[k], (const double *)hc[k]));
         c->scratch_on_device = true;
     }
+    const bool static_coef = resident && (c->flags & INMSOM_STATIC_COEFFS);
     for (int k = 0; k < NFORC; k++) {
         if (k == F_MU4 && ksw4 <= 0) continue;   // read only by uv_diff4
+        const bool coef = k != F_RHSX && k != F_RHSY;
+        if (static_coef && coef && c->coef_on_device[k]) continue;
         CKR(h2d(c, c->forc[k], hf[k]));
+        c->coef_on_device[k] = static_coef && coef;
     }
     if (!resident) {
         for (int k = 0; k < NDEPTH; k++)
@@ -505,9 +510,11 @@ int inmsom_load_state(inmsom_ctx *c, double *ubrtr_e, double *ubrtrp_e, double *
         CKR(h2d(c, c->state[k], (const double *)hs[k]));
         c->h_state[k] = hs[k];
     }
+    const bool static_coef = (c->flags & INMSOM_RESIDENT) && (c->flags & INMSOM_STATIC_COEFFS);
     for (int k = 0; k < NFORC; k++) {
         if (k == F_MU4 && !mu4) continue;
         CKR(h2d(c, c->forc[k], hf[k]));
+        c->coef_on_device[k] = static_coef && k != F_RHSX && k != F_RHSY;
     }
     c->state_on_device = true;
     fused::mark_state_changed(c->plan);
@@ -1083,6 +1090,8 @@ int inmsom_gpu_sync_from_host(inmsom_ctx *c, unsigned what)
         for (int k = 0; k < NSCR; k++) CKR(h2d(c, c->scr[k], (const double *)c->h_scr[k]));
         c->scratch_on_device = true;
     }
+    if (what & INMSOM_SYNC_COEFFS)
+        for (int k = 0; k < NFORC; k++) c->coef_on_device[k] = false;
     return sync_stream(c);
 }
 

@@ -102,6 +102,7 @@ struct inmsom_ctx {
     bool state_on_device = false;   // resident state has been uploaded
     bool depths_current = false;    // depth[] == hh_init(state) or evolved faithfully
     bool scratch_on_device = false;
+    bool coef_on_device[NFORC] = {};   // INMSOM_STATIC_COEFFS: field copied in and current
 
     fused::Plan plan{};              // fused-path layout and eligibility
     // run_substeps as replays of a graph of rs_len (even, <= RS_GROUP) substeps

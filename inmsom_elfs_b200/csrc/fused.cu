@@ -71,7 +71,9 @@ struct alignas(64) Params {
     long long pitch;
     int bm_words;
     int c_first, c_last;   // interior device columns
-    double two_ti, gam, c4, rhs_scale, mu0, rd0, wq0, inv_rho;
+    double two_ti, gam, rhs_scale, mu0, rd0, wq0, inv_rho;
+    // time means: a substep adds ca * (old level's term) + cb * (new level's)
+    double ca, cb;
     double d, inv_d, d4, gd, d2, tt;   // UNI: d, 1/d, d/4, g*d, d*d, two_ti/d^2
     int vort_zero;
     unsigned *flags;
@@ -590,7 +592,7 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
                 const long long idx = gi - p.pitch;
                 if (ACC && wu) {
                     const double slxn = -(SNr - sn) * (GEN ? CF(o_m1, gdyh) : p.gd) * hun;
-                    double a = (c.U + un * hun) * p.c4, b = (c.slx + slxn) * p.c4;
+                    double a = c.U * p.ca + un * hun * p.cb, b = c.slx * p.ca + slxn * p.cb;
                     if (ACC == 2) { a += qc.au0; b += qc.au2; }
                     p.acc[0][idx] = a;
                     p.acc[2][idx] = b;
@@ -633,7 +635,7 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
                 const long long idx = gi - 2 * p.pitch;
                 if (ACC && wv) {
                     const double slyn = -(sn1 - sn0) * (GEN ? CF(o_m2, gdxh) : p.gd) * hvn;
-                    double a = (qc.V + vn * hvn) * p.c4, b = (qc.sly + slyn) * p.c4;
+                    double a = qc.V * p.ca + vn * hvn * p.cb, b = qc.sly * p.ca + slyn * p.cb;
                     if (ACC == 2) { a += qc.av1; b += qc.av3; }
                     p.acc[1][idx] = a;
                     p.acc[3][idx] = b;
@@ -1410,14 +1412,30 @@ int dynamics(Plan &p, const Dom &d, const Consts &c, double tau, int nstep, doub
     const double ti = tau / (double)nstep;
     set_times(q, 2.0 * ti, p);
     q.gam = c.ts / 2.0 / (double)nstep;
-    q.c4 = 1.0 / (double)(4 * nstep);
     for (int k = 0; k < 4; k++) q.acc[k] = acc[k];
+    // The time means of vel_ssh.f90:549-550, :567-568 add (X(s-1) + X(s)) /
+    // (4*nstep) in every substep s = 1..2*nstep, X being a transport or a
+    // pressure-gradient term of a time level: that is X(0)/(4 nstep) +
+    // sum_{s=1}^{2 nstep-1} X(s)/(2 nstep) + X(2 nstep)/(4 nstep).  The sums
+    // are read and written in substep 1 (X(0)) and the even substeps
+    // (X(s-1) + X(s), the last one's X(s) with half the weight) only; the
+    // odd substeps after the first run the plain kernel.  Same sum, a
+    // different rounding order, half the time-mean traffic.
+    const double c2 = 1.0 / (double)(2 * nstep), c4 = 1.0 / (double)(4 * nstep);
+    // (every odd substep writes the state: only the last, even one does not)
+    auto mode_of = [&](int st, bool write) {
+        if (st == 1) { q.ca = c4; q.cb = 0.0; return 4; }
+        if (st & 1) return 3;
+        q.ca = c2;
+        q.cb = st == 2 * nstep ? c4 : c2;
+        return write ? 5 : 2;
+    };
     // substeps 1..nstep ping-pong between state[] and buf[0]; the state
     // after substep nstep (vel_ssh.f90:638-648) is then swapped into state[]
     for (int step = 1; step <= nstep; step++) {
         const bool odd = step & 1;
         if (set_io(p, q, odd ? state : p.buf[0], odd ? p.buf[0] : state)) return 1;
-        if (launch(p, q, gen, step == 1 ? 4 : 5, s) || cudaGetLastError() != cudaSuccess) return 1;
+        if (launch(p, q, gen, mode_of(step, true), s) || cudaGetLastError() != cudaSuccess) return 1;
     }
     if (nstep & 1)
         for (int k = 0; k < 6; k++) std::swap(state[k], p.buf[0][k]);
@@ -1427,7 +1445,7 @@ int dynamics(Plan &p, const Dom &d, const Consts &c, double tau, int nstep, doub
         double *const *src = k2 == 1 ? state : ((k2 & 1) ? p.buf[1] : p.buf[0]);
         double *const *dst = (k2 & 1) ? p.buf[0] : p.buf[1];
         if (set_io(p, q, src, dst)) return 1;
-        if (launch(p, q, gen, k2 < nstep ? 5 : 2, s) || cudaGetLastError() != cudaSuccess) return 1;
+        if (launch(p, q, gen, mode_of(nstep + k2, k2 < nstep), s) || cudaGetLastError() != cudaSuccess) return 1;
     }
     unsigned flags = 0;
     if (read_flags(p, s, &flags)) return 1;
@@ -1455,7 +1473,6 @@ int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt, co
     Params q = base_params(p, d, c, f, gen);
     set_times(q, 2.0 * dt, p);
     q.gam = c.ts / 2.0;   // nstep = 1
-    q.c4 = 0.25;
     for (int k = 0; k < 4; k++) q.acc[k] = nullptr;
     for (int step = 0; step < nsub; step++) {
         if (set_io(p, q, (step & 1) ? p.buf[0] : state, (step & 1) ? state : p.buf[0])) return 1;
@@ -1495,7 +1512,6 @@ int launch_steps_f32(Plan &p, const Dom &d, const Consts &c, double dt, int nste
     Params q = base_params(p, d, c, f, 0);
     set_times(q, 2.0 * dt, p);
     q.gam = c.ts / 2.0;   // nstep = 1
-    q.c4 = 0.25;
     for (int k = 0; k < 4; k++) q.acc[k] = nullptr;
     q.tm_rhs = p.tm_rhs32;
     q.tm_stat = p.tm_stat_f32;
@@ -1566,7 +1582,6 @@ int launch_steps(Plan &p, const Dom &d, const Consts &c, double dt, int nsteps, 
     Params q = base_params(p, d, c, f, gen);
     set_times(q, 2.0 * dt, p);
     q.gam = c.ts / 2.0;   // nstep = 1
-    q.c4 = 0.25;
     for (int k = 0; k < 4; k++) q.acc[k] = nullptr;
     q.rs_dev = rs_dev;
     q.rs_base = rs_base;

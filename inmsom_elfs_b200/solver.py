@@ -37,12 +37,14 @@ def gridcon(bounds: Bounds, lu: np.ndarray, device: int = 0) -> dict:
 class BarotropicSolver:
     def __init__(self, basin: Basin, device: int = 0, resident: bool = True,
                  force_general: bool = False, guard: bool = False,
-                 register_depths: bool = True, fp32_velocity: bool = False):
+                 register_depths: bool = True, fp32_velocity: bool = False,
+                 static_coeffs: bool = False):
         lib = load()
         self.basin = basin
         self.device = device
         flags = (_lib.RESIDENT if resident else 0) | (_lib.FORCE_GENERAL if force_general else 0) \
-            | (_lib.GUARD if guard else 0) | (_lib.FP32_VELOCITY if fp32_velocity else 0)
+            | (_lib.GUARD if guard else 0) | (_lib.FP32_VELOCITY if fp32_velocity else 0) \
+            | (_lib.STATIC_COEFFS if static_coeffs else 0)
         self._ctx = ctypes.c_void_p()
         cb, cc = cbounds(basin.bounds), cconsts(basin.consts)
         check(lib.inmsom_gpu_init(ctypes.byref(self._ctx), ctypes.byref(cb), ctypes.byref(cc),

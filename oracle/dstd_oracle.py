@@ -281,10 +281,13 @@ def ctl_read(text, datname_len=255, title_len=255):
         if not stripped or nb > len(s) - 5:
             continue
         key = s[nb - 1:]
-        vals, _ = _values(s)
+        # READ(string, *) of the record happens only in the branches of the
+        # keywords that read values (VARS, UNDEF, OPTIONS, XDEF/YDEF/ZDEF,
+        # TDEF); a TITLE or DSET record is never read that way
         if _spelled(key, "ENDVARS"):
             return out
         if _spelled(key, "VARS"):
+            vals, _ = _values(s)
             if len(vals) < 2:
                 raise CtlError("in definition vars or variable name")
             out["nvar"] = _int(vals[1])
@@ -313,11 +316,13 @@ def ctl_read(text, datname_len=255, title_len=255):
             out["title"] = s[nb + 4:][:title_len].rstrip(" ")
             out["inform"] += 1
         if _spelled(key, "UNDEF"):
+            vals, _ = _values(s)
             if len(vals) < 2:
                 raise CtlError("in definition undefinit value")
             out["undef"] = _f32(_real(vals[1]))
             out["inform"] += 1
         if _spelled(key, "OPTIONS"):
+            vals, _ = _values(s)
             if len(vals) < 2:
                 raise CtlError("in definition Options")
             out["inform"] += 1
@@ -326,6 +331,7 @@ def ctl_read(text, datname_len=255, title_len=255):
         for tag, a in (("XDEF", "x"), ("YDEF", "y"), ("ZDEF", "z")):
             if not _spelled(key, tag):
                 continue
+            vals, _ = _values(s)
             if len(vals) < 3:
                 raise CtlError(f"in definition {a}-grid")
             n = out["n" + a] = _int(vals[1])
@@ -349,6 +355,7 @@ def ctl_read(text, datname_len=255, title_len=255):
                 out["h" + a] = 0.0
                 out["inform"] += 1
         if _spelled(key, "TDEF"):
+            vals, _ = _values(s)
             if len(vals) < 5:
                 raise CtlError("in definition t-grid")
             out["nt"] = _int(vals[1])

@@ -771,3 +771,17 @@ def test_checkpoint_golden_fixture(tmp_path):
                 assert g == str(want)
             else:
                 assert g == want.item(), name
+
+
+def test_ctl_title_is_not_read_list_directed(tmp_path):
+    """A TITLE record is taken as text (Service/rw_ctl_file.f90: the title
+    is a substring of the record; only VARS, UNDEF, OPTIONS, the axis and
+    TDEF records are read list-directed), so separators or slashes in a
+    title are no error."""
+    for title in (",,", "a, b / c", "/", "1*,2"):
+        fname = str(tmp_path / "t.dat")
+        dstd.ctl_file_write(fname, -1.0e32, 1, 1, 1, 1, 0, [0.0], 0.0, 0, [0.0], 0.0, 0, [0.0], 0.0,
+                            0, 1, 1, 1, 0, 0, 60.0, title, "v")
+        text = (tmp_path / "t.ctl").read_text()
+        got = _read_both(tmp_path, text, name="t2.ctl")
+        assert got is not None and got["title"].strip() == title

@@ -326,3 +326,28 @@ def test_velocity2d_bitexact(gpu, ora):
     for g_, r_ in zip(got, ref):
         assert np.array_equal(g_, r_)
     assert not np.array_equal(got[0], outs[0])
+
+
+def test_static_coeffs_stay_resident(gpu, ora):
+    # INMSOM_STATIC_COEFFS: wflux, mu and rdis are copied in by the first
+    # call and kept; a change on the host reaches the device only after
+    # inmsom_gpu_sync_from_host(INMSOM_SYNC_COEFFS)
+    from inmsom_elfs_b200 import _lib
+    b = prep(basins.regional_basin(nx=200, ny=120, seed=21), ora)
+    bo, bg = b.copy(), b.copy()
+    with gpu.BarotropicSolver(bg, resident=True, static_coeffs=True) as s:
+        ora.barotropic_dynamics(bo, 4 * b.dt, 4)
+        s.barotropic_dynamics(4 * b.dt, 4)
+        bg.forcing["mu"][...] *= 3.0                    # not seen by the device
+        ora.barotropic_dynamics(bo, 4 * b.dt, 4)
+        s.barotropic_dynamics(4 * b.dt, 4)
+        s.sync_to_host()
+        assert_close(bo, bg, TOL10)
+        bo.forcing["mu"][...] *= 3.0
+        s.sync_from_host(_lib.SYNC_COEFFS)
+        ora.barotropic_dynamics(bo, 4 * b.dt, 4)
+        s.barotropic_dynamics(4 * b.dt, 4)
+        s.sync_to_host()
+    assert_close(bo, bg, TOL10)
+    for k in MEANS:
+        assert rel_err(bg.means[k], bo.means[k]) <= TOL10, k
