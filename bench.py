@@ -48,8 +48,13 @@ same basin and levels (a study line).
 per-field max/RMS differences (a study line, not a benchmark line).
 
 --impl reference runs only the CPU oracle arm (rank 0) and prints its line.
-Multi-GPU (torchrun): every rank runs its own basin replica (seed + rank);
-the time is the max over ranks and value sums the ranks' cells.
+Multi-GPU (torchrun): one basin made of N regional basins stacked along y
+(2048 x 1536 N), cut into 1 x N row strips, one per rank (weak scaling);
+halos of 2*block rows, block substeps per halo exchange (NCCL send/recv of
+the packed rows, dist.run_strip); the time is the max over ranks (CUDA
+events on each rank's stream) and value sums the ranks' cells.  --replicas
+runs independent basins instead; the e2e drop-in call runs one basin per
+rank.
 """
 from __future__ import annotations
 
@@ -96,6 +101,10 @@ def parse():
     p.add_argument("--closure-eval", type=int, default=60000, help="coarse substeps of the comparison")
     p.add_argument("--members", type=int, default=64)
     p.add_argument("--group", type=int, default=20)
+    p.add_argument("--block", type=int, default=4,
+                   help="row strips (--gpus N > 1): substeps per halo exchange (halos of 2*block rows)")
+    p.add_argument("--replicas", action="store_true",
+                   help="--gpus N > 1: independent basin replicas instead of row strips of one basin")
     return p.parse_args()
 
 
@@ -111,6 +120,14 @@ def workload(args, rank):
 
 
 def config_dict(b, args, nranks):
+    if nranks == 1:
+        par = "single"
+    elif getattr(args, "replicas", False):
+        par = f"replicas{nranks} (independent basins, seed + rank)"
+    else:
+        par = (f"strips{nranks}: one {b.bounds.nx}x{b.bounds.ny * nranks} basin of {nranks} stacked regional "
+               f"basins, 1 x {nranks} row strips, halos of {2 * args.block} rows, {args.block} substeps per "
+               f"NCCL halo exchange")
     return {
         "workload": f"regional_basin {b.bounds.nx}x{b.bounds.ny} 1 km FP64 barotropic leap-frog",
         "nx": b.bounds.nx, "ny": b.bounds.ny, "spacing_m": 1000.0, "dt_s": b.dt,
@@ -118,7 +135,7 @@ def config_dict(b, args, nranks):
         "cells_per_rank": b.cells,
         "l2": "inputs larger than L2: 6 state + H + 2 forcing FP64 fields = %.0f MB per step"
               % (9 * 8 * b.cells / 1e6),
-        "parallelism": "replicas" if nranks > 1 else "single",
+        "parallelism": par,
         "step": "one advancing leap-frog substep (barotropic_dynamics(dt,1) state evolution)",
     }
 
@@ -378,8 +395,26 @@ def run_ours(args):
     from inmsom_elfs_b200 import basins, solver
     from inmsom_elfs_b200.grid import MEANS
 
-    b = workload(args, rank)
-    basins.finalize(b, solver.GpuBackend(local))
+    strips = ws > 1 and not args.replicas
+    if strips and args.fp32_velocity:
+        raise SystemExit("row strips keep an FP64 state: --fp32-velocity needs --gpus 1 or --replicas")
+    if strips:
+        # one basin of N stacked regional basins (2048 x 1536 N), one row
+        # strip per rank (weak scaling: each rank's strip is basin `rank`),
+        # halos of 2k rows, k substeps per NCCL exchange
+        from inmsom_elfs_b200.strips import stacked_strip
+        parts = {}
+        for q in (rank - 1, rank, rank + 1):
+            if 0 <= q < ws:
+                parts[q] = workload(args, q)
+                basins.finalize(parts[q], solver.GpuBackend(local))
+        b = stacked_strip(parts, ws, rank, 2 * args.block)
+        own = parts[rank]
+        del parts
+    else:
+        b = workload(args, rank)
+        basins.finalize(b, solver.GpuBackend(local))
+        own = b
     cpu_copy = b.copy() if (rank == 0 and ws == 1 and not args.no_cpu) else None
 
     def barrier():
@@ -401,12 +436,25 @@ def run_ours(args):
     path = s.path()
     s.load_state()
     warm = basins.wind_cycle(args.warmup, b.dt)
-    s.run_substeps(args.warmup, b.dt, warm)
     scale = basins.wind_cycle(args.steps, b.dt, t0=args.warmup * b.dt)
-    barrier()
-    with Clocks(local) as clk:
-        ms = s.run_substeps(args.steps, b.dt, scale)
+    if strips:
+        from inmsom_elfs_b200 import dist as sdist
+        stepper = sdist.GpuStripStepper(s, host_staging=False)
+        sdist.run_strip(stepper, rank, ws, args.warmup, b.dt, warm)
+        ev0, ev1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         barrier()
+        with Clocks(local) as clk:
+            ev0.record(stepper.stream)       # the context's stream: the kernels and the exchanges
+            sdist.run_strip(stepper, rank, ws, args.steps, b.dt, scale)
+            ev1.record(stepper.stream)
+            barrier()
+        ms = ev0.elapsed_time(ev1)
+    else:
+        s.run_substeps(args.warmup, b.dt, warm)
+        barrier()
+        with Clocks(local) as clk:
+            ms = s.run_substeps(args.steps, b.dt, scale)
+            barrier()
     ms = maxall(ms)
     nbad = s.guard()
     s.close()
@@ -420,7 +468,9 @@ def run_ours(args):
     # ---- e2e through the drop-in with pinned host buffers
     e2e = None
     if not args.no_e2e:
-        e2e = e2e_arm(args, b, local, barrier, maxall, ws)
+        # the drop-in call is single-domain: with several ranks each runs it
+        # on its own regional basin (replicas)
+        e2e = e2e_arm(args, own, local, barrier, maxall, ws)
 
     cpu = None
     if cpu_copy is not None:
@@ -448,7 +498,7 @@ def run_ours(args):
                          "bytes_per_cell_step": bpc,
                          "peak_kind": f"{peak_kind} HBM copy bandwidth"},
             "cpu_baseline": cpu, "e2e": e2e, "clocks": clk.summary(),
-            "gpu_launches": gpu_launches(args.steps, args.fp32_velocity),
+            "gpu_launches": args.steps + 1 if strips else gpu_launches(args.steps, args.fp32_velocity),
             "path": path[1], "guard_bad_points": nbad,
         }
         print(json.dumps(line), flush=True)
@@ -475,6 +525,34 @@ def run_study_fp32(args):
             v1, e1 = s.diag()
             s.sync_to_host()
         out[fp32], vol[fp32] = bg, (v1 - v0) / v0
+    # against the FP64 CPU oracle (the reference's scheme) on a 1024 x 1024
+    # part of the same configuration (the oracle would take most of an hour
+    # on the 4096 x 4096 basin): both GPU runs' errors per field
+    vs_oracle = None
+    if not args.no_cpu:
+        from oracle import oracle as ora
+        nso = 1024 if n > 1024 else n
+        so = basins.ridge_basin(n=nso)
+        basins.finalize(so, ora.OracleBackend())
+        ora.hh_init_external(so)
+        steps_o = min(args.steps, 1000)
+        sc = basins.wind_cycle(steps_o, so.dt)
+        ref = so.copy()
+        ora.run_substeps(ref, steps_o, so.dt, sc)
+        oc = so.masks["lu"] > 0.5
+        vs_oracle = {"workload": f"ridge_basin {nso}x{nso} 2 km dt 3 s", "steps": steps_o, "fields": {}}
+        for fp32 in (False, True):
+            bg = so.copy()
+            with solver.BarotropicSolver(bg, resident=True, fp32_velocity=fp32) as s:
+                s.load_state()
+                s.run_substeps(steps_o, so.dt, sc)
+                s.sync_to_host()
+            for k in ref.state:
+                d = (bg.state[k] - ref.state[k])[oc]
+                r = ref.state[k][oc]
+                vs_oracle["fields"].setdefault(k, {})["fp32_velocity" if fp32 else "fp64"] = {
+                    "max_abs": float(np.abs(d).max()), "rms": float(np.sqrt(np.mean(d * d))),
+                    "rel_max": float(np.abs(d).max() / max(np.abs(r).max(), 1e-300))}
     ocean = b.masks["lu"] > 0.5
     errs = {}
     for k in out[False].state:
@@ -485,7 +563,8 @@ def run_study_fp32(args):
                    "rel_max": float(np.abs(d).max() / max(np.abs(r).max(), 1e-300))}
     print(json.dumps({
         "study": "fp32_velocity", "workload": f"ridge_basin {n}x{n} 2 km dt 3 s, wind with a 6 h cycle",
-        "steps": args.steps, "fields": errs, "relative_volume_change": {"fp64": vol[False], "fp32_velocity": vol[True]},
+        "steps": args.steps, "fields": errs, "vs_fp64_oracle": vs_oracle,
+        "relative_volume_change": {"fp64": vol[False], "fp32_velocity": vol[True]},
         "ms_per_step": {"fp64": ms[False] / args.steps, "fp32_velocity": ms[True] / args.steps},
         "cell_steps_per_s": {"fp64": b.cells * args.steps / (ms[False] / 1e3),
                              "fp32_velocity": b.cells * args.steps / (ms[True] / 1e3)},

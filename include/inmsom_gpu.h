@@ -625,8 +625,11 @@ int inmsom_ens_destroy(inmsom_ens *ens);
  * the two rows of the six state fields next to every internal boundary are
  * copied into the neighbour's halo rows (the fused kernel recomputes what
  * it needs in its halo rows, so one exchange per substep gives the
- * single-domain result bit for bit).  Contexts on different devices get
- * peer access. */
+ * single-domain result bit for bit).  With halos of 2k rows between the
+ * strips (the same width on both sides of a boundary, and at most a
+ * strip's rows) the strips advance k substeps per exchange of 2k rows,
+ * computing into their halos as inmsom_step_launch_rows describes.
+ * Contexts on different devices get peer access. */
 typedef struct inmsom_strips inmsom_strips;
 int inmsom_strips_create(inmsom_strips **strips, inmsom_ctx *const *ctxs, int n);
 int inmsom_strips_run(inmsom_strips *strips, int nsub, double dt, const double *rhs_scale, float *ms);
@@ -642,19 +645,34 @@ int inmsom_strips_destroy(inmsom_strips *strips);
  * unpacks what it received into its halo rows.  One exchange per substep
  * gives the single-domain result bit for bit (the fused kernel recomputes
  * its halo rows' intermediates).  FP64 state, fused path only.
+ *
+ * Wide halos (the GPU form of the reference's wide-halo exchange mode): a
+ * strip whose halo on a side it shares with another strip is 2k rows (k
+ * >= 1; its outer sides keep 2) advances k substeps per exchange of 2k
+ * rows.  In substep i = 1..k of such a block it computes 2(k-i) rows into
+ * each shared halo as well (inmsom_step_launch_rows), which the neighbour
+ * computes alike from the same values, so the result stays the
+ * single-domain one bit for bit while the exchanges drop k-fold.
  *   inmsom_step_begin: classify and stage the forcing for a run of substeps
  *     (synchronises the stream);
  *   inmsom_step_launch: enqueue one substep with RHS scale rhs_scale;
- *   inmsom_halo_pack: side 0 the two southernmost interior rows, side 1 the
- *     two northernmost, of the six state fields into buf (device,
- *     INMSOM_HALO_DOUBLES(pitch) doubles, field-major, rows of `pitch`
- *     doubles; pitch from inmsom_gpu_pitch);
- *   inmsom_halo_unpack: buf into the two southern (side 0) or northern
+ *   inmsom_step_launch_rows: the same computing rows_south / rows_north
+ *     rows beyond the interior (each at most the halo width on that side
+ *     minus 2, and 0 on a side that is the basin's edge);
+ *   inmsom_halo_pack: side 0 the w southernmost interior rows, side 1 the w
+ *     northernmost, w the halo width on that side, of the six state fields
+ *     into buf (device, 6 * w * pitch doubles, field-major, rows of `pitch`
+ *     doubles: INMSOM_HALO_DOUBLES(pitch) for w = 2; pitch from
+ *     inmsom_gpu_pitch, w from inmsom_gpu_halo);
+ *   inmsom_halo_unpack: buf into the w southern (side 0) or northern
  *     (side 1) halo rows;
  *   inmsom_step_end: wait for the stream and read the kernel status. */
 #define INMSOM_HALO_DOUBLES(pitch) (12LL * (long long)(pitch))
 int inmsom_step_begin(inmsom_ctx *ctx);
 int inmsom_step_launch(inmsom_ctx *ctx, double dt, double rhs_scale);
+int inmsom_step_launch_rows(inmsom_ctx *ctx, double dt, double rhs_scale, int rows_south, int rows_north);
+/* halo rows of the context south and north of its interior */
+int inmsom_gpu_halo(inmsom_ctx *ctx, int *rows_south, int *rows_north);
 int inmsom_halo_pack(inmsom_ctx *ctx, int side, void *buf);
 int inmsom_halo_unpack(inmsom_ctx *ctx, int side, const void *buf);
 int inmsom_step_end(inmsom_ctx *ctx);

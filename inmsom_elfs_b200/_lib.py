@@ -34,7 +34,7 @@ EXPORTS = (
     "inmsom_write_checkpoint", "inmsom_read_checkpoint", "inmsom_tracer_tran_diff", "inmsom_ctl_file_read",
     "inmsom_pwdstd", "inmsom_prdstd", "inmsom_ocpwrite", "inmsom_ocpread",
     "inmsom_compare_grids", "inmsom_stress_components", "inmsom_smagorinsky_coeff",
-    "inmsom_test_hold_copy",
+    "inmsom_test_hold_copy", "inmsom_step_launch_rows", "inmsom_gpu_halo",
 )
 
 # include/inmsom_gpu.h: INMSOM_MLP_*
@@ -174,6 +174,8 @@ def load() -> ctypes.CDLL:
     lib.inmsom_read_checkpoint.argtypes = [VP, cp] + [DP] * 6
     lib.inmsom_step_begin.argtypes = [VP]
     lib.inmsom_step_launch.argtypes = [VP, d, d]
+    lib.inmsom_step_launch_rows.argtypes = [VP, d, d, i, i]
+    lib.inmsom_gpu_halo.argtypes = [VP, ctypes.POINTER(i), ctypes.POINTER(i)]
     lib.inmsom_halo_pack.argtypes = [VP, i, VP]
     lib.inmsom_halo_unpack.argtypes = [VP, i, VP]
     lib.inmsom_step_end.argtypes = [VP]

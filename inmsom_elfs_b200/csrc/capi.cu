@@ -1347,17 +1347,21 @@ struct inmsom_strips {
 
 namespace {
 
-// copy rows [r, r+1] of the six fields of `from`'s current state set into
+// copy rows [r, r+nrows) of the six fields of `from`'s current state set into
 // rows [h, h+1] of `to`'s, on `to`'s stream... or the stream given
-int copy_rows(const inmsom_ctx *from, int r, inmsom_ctx *to, int h, cudaStream_t s)
+int copy_rows(const inmsom_ctx *from, int r, inmsom_ctx *to, int h, int nrows, cudaStream_t s)
 {
     const size_t pitch_b = (size_t)from->dom.pitch * sizeof(double);
     const size_t fs_from = (size_t)from->dom.pitch * from->dom.nya() * sizeof(double);
     const size_t fs_to = (size_t)to->dom.pitch * to->dom.nya() * sizeof(double);
     CK(cudaMemcpy2DAsync(to->state[0] + (size_t)h * to->dom.pitch, fs_to, from->state[0] + (size_t)r * from->dom.pitch,
-                         fs_from, 2 * pitch_b, NSTATE, cudaMemcpyDefault, s));
+                         fs_from, (size_t)nrows * pitch_b, NSTATE, cudaMemcpyDefault, s));
     return INMSOM_OK;
 }
+
+// halo rows south / north of the interior
+int halo_s(const inmsom_ctx *c) { return c->dom.ny_start - c->dom.bnd_y1; }
+int halo_n(const inmsom_ctx *c) { return c->dom.bnd_y2 - c->dom.ny_end; }
 
 }  // namespace
 
@@ -1375,6 +1379,9 @@ int inmsom_strips_create(inmsom_strips **out, inmsom_ctx *const *ctxs, int n)
             if (a.ny_end + 1 != b.ny_start || a.nx_start != b.nx_start || a.nx_end != b.nx_end ||
                 a.bnd_x1 != b.bnd_x1 || a.bnd_x2 != b.bnd_x2 || a.pitch != b.pitch || a.nnn != b.nnn || a.nn != b.nn)
                 return set_err(INMSOM_EARG, "strips %d and %d are not consecutive row strips of one basin", k - 1, k);
+            if (halo_n(ctxs[k - 1]) != halo_s(c) || halo_s(c) > b.ny_end - b.ny_start + 1 ||
+                halo_n(ctxs[k - 1]) > a.ny_end - a.ny_start + 1)
+                return set_err(INMSOM_EARG, "strips %d and %d: halo widths differ or exceed a strip", k - 1, k);
         }
     }
     if (ctxs[0]->dom.ny_start != ctxs[0]->dom.nnn || ctxs[n - 1]->dom.ny_end != ctxs[n - 1]->dom.nn)
@@ -1433,27 +1440,43 @@ int inmsom_strips_run(inmsom_strips *g, int nsub, double dt, const double *rhs_s
         CK(cudaSetDevice(g->m[k]->device));
         CK(cudaStreamWaitEvent(g->m[k]->stream, g->ev0, 0));
     }
-    for (int step = 0; step < nsub; step++) {
-        const double rs = rhs_scale ? rhs_scale[step] : 1.0;
-        for (int k = 0; k < n; k++) {
-            inmsom_ctx *c = g->m[k];
-            CK(cudaSetDevice(c->device));
-            if (fused::launch_steps(c->plan, c->dom, c->c, dt, 1, nullptr, nullptr, c->state, c->stream, rs))
-                return set_err(INMSOM_ECUDA, "strip %d: launch failed", k);
-            CK(cudaEventRecord(g->done[k], c->stream));
+    // k substeps per exchange, k = half the narrowest halo between strips
+    // (1 with 2-row halos): in substep i of a block each strip also computes
+    // 2(k-i) rows into its halo on the sides it shares with another strip,
+    // which that strip computes alike, so that after k substeps the 2k
+    // halo rows are exchanged once
+    int kb = 1 << 20;
+    for (int k = 0; k + 1 < n; k++) kb = std::min(kb, halo_n(g->m[k]) / 2);
+    if (n == 1) kb = 1;
+    for (int step = 0; step < nsub;) {
+        const int len = std::min(kb, nsub - step);
+        for (int i = 1; i <= len; i++, step++) {
+            const double rs = rhs_scale ? rhs_scale[step] : 1.0;
+            for (int k = 0; k < n; k++) {
+                inmsom_ctx *c = g->m[k];
+                CK(cudaSetDevice(c->device));
+                const int es = k > 0 ? 2 * (len - i) : 0, en = k + 1 < n ? 2 * (len - i) : 0;
+                if (fused::launch_step_ext(c->plan, c->dom, c->c, dt, es, en, c->state, c->stream, rs))
+                    return set_err(INMSOM_ECUDA, "strip %d: launch failed", k);
+            }
         }
-        // halo rows of the new state: strip k's two northernmost interior
-        // rows into k+1's southern halo rows, k+1's two southernmost into
-        // k's northern halo rows
+        for (int k = 0; k < n; k++) {
+            CK(cudaSetDevice(g->m[k]->device));
+            CK(cudaEventRecord(g->done[k], g->m[k]->stream));
+        }
+        // halo rows of the new state: strip k's 2k northernmost interior
+        // rows into k+1's southern halo, k+1's 2k southernmost into k's
+        // northern halo
         for (int k = 0; k + 1 < n; k++) {
             inmsom_ctx *a = g->m[k], *b = g->m[k + 1];
+            const int w = halo_n(a);
             const int a_last = a->dom.ny_end - a->dom.bnd_y1;   // device row of ny_end
             CK(cudaSetDevice(b->device));
             CK(cudaStreamWaitEvent(b->stream, g->done[k], 0));
-            CKR(copy_rows(a, a_last - 1, b, 0, b->stream));
+            CKR(copy_rows(a, a_last - w + 1, b, 0, w, b->stream));
             CK(cudaSetDevice(a->device));
             CK(cudaStreamWaitEvent(a->stream, g->done[k + 1], 0));
-            CKR(copy_rows(b, 2, a, a_last + 1, a->stream));
+            CKR(copy_rows(b, w, a, a_last + 1, w, a->stream));
         }
     }
     // ev1 after every strip's last work
@@ -1491,24 +1514,44 @@ int inmsom_step_begin(inmsom_ctx *c)
 
 int inmsom_step_launch(inmsom_ctx *c, double dt, double rhs_scale)
 {
+    return inmsom_step_launch_rows(c, dt, rhs_scale, 0, 0);
+}
+
+int inmsom_step_launch_rows(inmsom_ctx *c, double dt, double rhs_scale, int rows_south, int rows_north)
+{
     if (!c) return set_err(INMSOM_EARG, "context is NULL");
     if (!c->plan.prepared) return set_err(INMSOM_EARG, "inmsom_step_begin has not been called");
     if (!(dt > 0.0)) return set_err(INMSOM_EARG, "dt must be > 0");
+    if (rows_south < 0 || rows_north < 0 || rows_south > halo_s(c) - 2 || rows_north > halo_n(c) - 2 ||
+        (rows_south && c->dom.ny_start == c->dom.nnn) || (rows_north && c->dom.ny_end == c->dom.nn))
+        return set_err(INMSOM_EARG, "inmsom_step_launch_rows: %d / %d rows beyond the interior need a halo 2 rows "
+                                    "wider on a side shared with another strip (halo %d / %d)",
+                       rows_south, rows_north, halo_s(c), halo_n(c));
     CK(cudaSetDevice(c->device));
-    if (fused::launch_steps(c->plan, c->dom, c->c, dt, 1, nullptr, nullptr, c->state, c->stream, rhs_scale))
+    if (fused::launch_step_ext(c->plan, c->dom, c->c, dt, rows_south, rows_north, c->state, c->stream, rhs_scale))
         return set_err(INMSOM_ECUDA, "substep launch failed: %s", cudaGetErrorString(cudaGetLastError()));
     c->depths_current = false;
     return INMSOM_OK;
 }
 
+int inmsom_gpu_halo(inmsom_ctx *c, int *rows_south, int *rows_north)
+{
+    if (!c || !rows_south || !rows_north) return set_err(INMSOM_EARG, "NULL argument");
+    CKR(ensure_grid(c));
+    *rows_south = halo_s(c);
+    *rows_north = halo_n(c);
+    return INMSOM_OK;
+}
+
 namespace {
-// device row of the first of the two rows a side packs (interior) or
-// unpacks (halo): south 2 / 0, north ny_end-1 / ny_end+1 (relative to bnd_y1)
+// device row of the first of the w rows a side packs (interior) or unpacks
+// (halo), w the side's halo width: south w / 0, north ny_end-w+1 / ny_end+1
+// (relative to bnd_y1)
 int halo_row(const inmsom_ctx *c, int side, bool pack)
 {
     const int last = c->dom.ny_end - c->dom.bnd_y1;
-    if (side == 0) return pack ? 2 : 0;
-    return pack ? last - 1 : last + 1;
+    if (side == 0) return pack ? halo_s(c) : 0;
+    return pack ? last - halo_n(c) + 1 : last + 1;
 }
 }  // namespace
 
@@ -1518,8 +1561,9 @@ int inmsom_halo_pack(inmsom_ctx *c, int side, void *buf)
     if (!buf || (side != 0 && side != 1)) return set_err(INMSOM_EARG, "inmsom_halo_pack: bad argument");
     const size_t row_b = (size_t)c->dom.pitch * sizeof(double);
     const size_t fs = row_b * c->dom.nya();
-    CK(cudaMemcpy2DAsync(buf, 2 * row_b, c->state[0] + (size_t)halo_row(c, side, true) * c->dom.pitch, fs,
-                         2 * row_b, NSTATE, cudaMemcpyDeviceToDevice, c->stream));
+    const size_t w = (size_t)(side ? halo_n(c) : halo_s(c));
+    CK(cudaMemcpy2DAsync(buf, w * row_b, c->state[0] + (size_t)halo_row(c, side, true) * c->dom.pitch, fs,
+                         w * row_b, NSTATE, cudaMemcpyDeviceToDevice, c->stream));
     return INMSOM_OK;
 }
 
@@ -1529,8 +1573,9 @@ int inmsom_halo_unpack(inmsom_ctx *c, int side, const void *buf)
     if (!buf || (side != 0 && side != 1)) return set_err(INMSOM_EARG, "inmsom_halo_unpack: bad argument");
     const size_t row_b = (size_t)c->dom.pitch * sizeof(double);
     const size_t fs = row_b * c->dom.nya();
-    CK(cudaMemcpy2DAsync(c->state[0] + (size_t)halo_row(c, side, false) * c->dom.pitch, fs, buf, 2 * row_b,
-                         2 * row_b, NSTATE, cudaMemcpyDeviceToDevice, c->stream));
+    const size_t w = (size_t)(side ? halo_n(c) : halo_s(c));
+    CK(cudaMemcpy2DAsync(c->state[0] + (size_t)halo_row(c, side, false) * c->dom.pitch, fs, buf, w * row_b,
+                         w * row_b, NSTATE, cudaMemcpyDeviceToDevice, c->stream));
     return INMSOM_OK;
 }
 

@@ -998,44 +998,42 @@ int encode_fields(EncodeTiled enc, CUtensorMap *map, void *base, const Dom &d, l
 constexpr double LAND_COST = 0.7;
 constexpr int MIN_ROWS = 16;
 
-// Ocean flags of the written columns of every strip and interior row
-// (strip-major), from the host T mask.
+// Ocean flags of the written columns of every strip and device row
+// (strip-major, nya rows per strip), from the host T mask.
 std::vector<uint8_t> ocean_rows(const Plan &p, const Dom &d, const float *lu)
 {
-    const int nxa = d.nxa();
-    const int rf = d.ny_start - d.bnd_y1, rl = d.ny_end - d.bnd_y1;   // interior device rows
+    const int nxa = d.nxa(), nya = d.nya();
     const int cf = d.nx_start - d.bnd_x1 + d.xoff, cl = d.nx_end - d.bnd_x1 + d.xoff;
-    const int ny = rl - rf + 1;
-    std::vector<uint8_t> oc((size_t)p.nstrips * ny, 0);
+    std::vector<uint8_t> oc((size_t)p.nstrips * nya, 0);
     for (int s = 0; s < p.nstrips; s++) {
         const int g0 = s * p.outw;
         const int c0 = std::max(g0 + 3, cf), c1 = std::min(g0 + 2 + p.outw, cl);   // written columns
-        for (int r = rf; r <= rl; r++) {
+        for (int r = 0; r < nya; r++) {
             bool ocean = false;
             for (int col = c0; col <= c1 && !ocean; col++) ocean = lu[(size_t)r * nxa + (col - d.xoff)] > 0.5f;
-            oc[(size_t)s * ny + (r - rf)] = ocean;
+            oc[(size_t)s * nya + r] = ocean;
         }
     }
     return oc;
 }
 
-// Work items of one variant: each strip's interior rows cut into chunks of
+// Work items of one variant: each strip's rows rf..rl (device rows; the
+// interior unless a row strip computes into its halo) cut into chunks of
 // about equal cost.  rows_per_item = 0: as many items in all as one wave of
 // resident CTAs holds (`slots`), so that the wave finishes together; else
 // about that many rows per item (several waves).  A row whose written
 // columns are all land skips the momentum stages and costs about LAND_COST
 // of an ocean row; no chunk is shorter than MIN_ROWS rows (each pays three
 // warm-up iterations).
-std::vector<int4> partition(const Plan &p, const Dom &d, int slots, int rows_per_item)
+std::vector<int4> partition(const Plan &p, const Dom &d, int slots, int rows_per_item, int rf, int rl)
 {
-    const int rf = d.ny_start - d.bnd_y1, rl = d.ny_end - d.bnd_y1;
-    const int ny = rl - rf + 1;
+    const int ny = rl - rf + 1, nya = d.nya();
     std::vector<std::vector<double>> cost(p.nstrips, std::vector<double>(ny));
     std::vector<double> total(p.nstrips, 0.0);
     double all = 0.0;
     for (int s = 0; s < p.nstrips; s++) {
         for (int r = 0; r < ny; r++) {
-            cost[s][r] = p.ocean[(size_t)s * ny + r] ? 1.0 : LAND_COST;
+            cost[s][r] = p.ocean[(size_t)s * nya + rf + r] ? 1.0 : LAND_COST;
             total[s] += cost[s][r];
         }
         all += total[s];
@@ -1082,6 +1080,11 @@ std::vector<int4> partition(const Plan &p, const Dom &d, int slots, int rows_per
     return items;
 }
 
+std::vector<int4> partition(const Plan &p, const Dom &d, int slots, int rows_per_item)
+{
+    return partition(p, d, slots, rows_per_item, d.ny_start - d.bnd_y1, d.ny_end - d.bnd_y1);
+}
+
 // waves of work items per table: one for the plain substep (measured on the
 // 2048 x 1536 basin: 2 waves +5.6 %, 1.5 waves +15 %), two for the
 // time-mean substeps (-1.9 % against one)
@@ -1116,6 +1119,8 @@ void release(Plan &p)
         cudaFree(it);
         it = nullptr;
     }
+    for (auto &t : p.ext) cudaFree(t.items);
+    p.ext.clear();
     for (auto &v : p.vset) {
         cudaFree(v);
         v = nullptr;
@@ -1192,18 +1197,21 @@ const char *check_eligible(const Plan &p, const Dom &d, const Consts &c, const f
                            const double *const grid[10])
 {
     (void)p;
-    if (d.bnd_x1 != d.nx_start - 2 || d.bnd_x2 != d.nx_end + 2 || d.bnd_y1 != d.ny_start - 2 ||
-        d.bnd_y2 != d.ny_end + 2)
-        return "array bounds are not the interior plus a 2-point halo";
+    // a row strip of a larger basin: the halo rows next to another strip
+    // hold that strip's values (they may be ocean), and there the halo may
+    // be wider than 2 rows (an even number: a strip that advances k
+    // substeps per exchange computes 2(k-1) rows into it)
+    const bool open_s = d.ny_start > d.nnn, open_n = d.ny_end < d.nn;
+    const int hs = d.ny_start - d.bnd_y1, hn = d.bnd_y2 - d.ny_end;
+    if (d.bnd_x1 != d.nx_start - 2 || d.bnd_x2 != d.nx_end + 2 || (open_s ? hs < 2 || hs % 2 : hs != 2) ||
+        (open_n ? hn < 2 || hn % 2 : hn != 2))
+        return "array bounds are not the interior plus a 2-point halo (an even wider one next to another strip)";
     if (d.px || d.py) return "periodic wrap";
     if (c.ffs != 1) return "full_free_surface != 1";
     if (d.xoff != XOFF) return "device layout without the fused column offset";
     const int nxa = d.nxa(), nya = d.nya();
     auto at = [&](const float *a, int m, int n) { return a[(size_t)(n - d.bnd_y1) * nxa + (m - d.bnd_x1)]; };
     if (d.nx_start != d.mmm || d.nx_end != d.mm) return "domain split along x (only row strips are supported)";
-    // a row strip of a larger basin: the halo rows next to another strip
-    // hold that strip's values (they may be ocean)
-    const bool open_s = d.ny_start > d.nnn, open_n = d.ny_end < d.nn;
     const float *lu = masks[0];
     for (int n = d.bnd_y1; n <= d.bnd_y2; n++)
         for (int m = d.bnd_x1; m <= d.bnd_x2; m++) {
@@ -1236,8 +1244,9 @@ const char *check_eligible(const Plan &p, const Dom &d, const Consts &c, const f
                 return "derived masks differ from gridcon(lu)";
         }
     // metrics and Coriolis constant along rows over the points the step reads
+    // (rows bnd_y1+1..bnd_y2-1: ny_start-1..ny_end+1 with a 2-row halo)
     for (int k = 0; k < 9; k++)
-        for (int n = d.ny_start - 1; n <= d.ny_end + 1; n++) {
+        for (int n = d.bnd_y1 + 1; n <= d.bnd_y2 - 1; n++) {
             const double *g = grid[k] + (size_t)(n - d.bnd_y1) * nxa;
             const double v0 = g[d.nx_start - d.bnd_x1];
             if (!std::isfinite(v0) || (k < 8 && v0 == 0.0)) return "zero or non-finite metric";
@@ -1255,8 +1264,10 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
 {
     release(p);
     const int nxa = d.nxa(), nya = d.nya();
+    // metrics of the rows the step reads: bnd_y1+1..bnd_y2-1 (ny_start-1..
+    // ny_end+1 with a 2-row halo); rows outside repeat the nearest
     auto row_of = [&](int k, int n) {
-        n = std::min(std::max(n, d.ny_start - 1), d.ny_end + 1);
+        n = std::min(std::max(n, d.bnd_y1 + 1), d.bnd_y2 - 1);
         return grid[k][(size_t)(n - d.bnd_y1) * nxa + (d.nx_start - d.bnd_x1)];
     };
     enum { DX, DY, DXT, DYT, DXH, DYH, DXB, DYB, RLH };
@@ -1287,7 +1298,7 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
         q.vt0 = g(DYT, 0) - g(DYB, 0);
         q.vt1 = g(DXT, 1) - g(DXB, 0);
         q.vt2 = g(DXT, 0) - g(DXB, 0);
-        if (n >= d.ny_start - 1 && n <= d.ny_end && (q.vt0 != 0.0 || q.vt1 != 0.0 || q.vt2 != 0.0)) vz = false;
+        if (n >= d.bnd_y1 + 1 && n <= d.bnd_y2 - 2 && (q.vt0 != 0.0 || q.vt1 != 0.0 || q.vt2 != 0.0)) vz = false;
         q.t1 = g(DY, 0) / (g(DX, 0) * g(DYH, 0));
         q.t2 = g(DX, 0) / (g(DY, 0) * g(DXH, 0));
         q.t3 = g(DX, 0) / (g(DY, 0) * g(DXH, -1));
@@ -1313,7 +1324,7 @@ int setup(Plan &p, const Dom &d, const Consts &c, const float *const masks[7], c
     p.uni = true;
     p.d = row_of(DX, d.ny_start);
     for (int k = 0; k < 8 && p.uni; k++)
-        for (int n = d.ny_start - 1; n <= d.ny_end + 1 && p.uni; n++)
+        for (int n = d.bnd_y1 + 1; n <= d.bnd_y2 - 1 && p.uni; n++)
             if (row_of(k, n) != p.d) p.uni = false;
     std::vector<double> cor(nya);
     for (int r = 0; r < nya; r++) cor[r] = row_of(RLH, r + d.bnd_y1) * p.d * p.d;
@@ -1593,6 +1604,54 @@ int launch_steps(Plan &p, const Dom &d, const Consts &c, double dt, int nsteps, 
     }
     if (nsteps & 1)
         for (int k = 0; k < 6; k++) std::swap(state[k], p.buf[0][k]);
+    return 0;
+}
+
+namespace {
+// the plain-substep items over device rows extended es rows south and en
+// rows north of the interior, built (and kept) on first use; nullptr if
+// the halo is too narrow for them (the kernel reads two rows below and two
+// above the rows it computes)
+const Plan::ExtTable *ext_table(Plan &p, const Dom &d, int gen, int es, int en, cudaStream_t s)
+{
+    for (const auto &t : p.ext)
+        if (t.gen == gen && t.s == es && t.n == en) return &t;
+    const int rf = d.ny_start - d.bnd_y1 - es, rl = d.ny_end - d.bnd_y1 + en;
+    if (es < 0 || en < 0 || rf < 2 || rl + 2 > d.nya() - 1) return nullptr;
+    const std::vector<int4> items = partition(p, d, item_waves(gen) * p.nsm * p.occ[gen], 0, rf, rl);
+    Plan::ExtTable t{gen, es, en, (int)items.size(), nullptr};
+    if (cudaMalloc(&t.items, items.size() * sizeof(int4)) != cudaSuccess) return nullptr;
+    p.ext.push_back(t);   // owned by the plan from here on (freed by release)
+    if (cudaMemcpyAsync(t.items, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, s) !=
+            cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)
+        return nullptr;
+    return &p.ext.back();
+}
+}  // namespace
+
+int launch_step_ext(Plan &p, const Dom &d, const Consts &c, double dt, int ext_s, int ext_n, double *state[6],
+                    cudaStream_t s, double rs_host)
+{
+    if (!p.prepared) return 1;
+    if (ext_s == 0 && ext_n == 0) return launch_steps(p, d, c, dt, 1, nullptr, nullptr, state, s, rs_host);
+    const int gen = p.prep_gen;
+    if (p.stat_box[gen] != (gen ? Layout<true>::NS : Layout<false>::NS)) return 1;
+    const Plan::ExtTable *t = ext_table(p, d, gen, ext_s, ext_n, s);
+    if (!t) return 1;
+    Forcing f{true, p.prep_mu0, p.prep_rd0, p.prep_wq0};
+    Params q = base_params(p, d, c, f, gen);
+    set_times(q, 2.0 * dt, p);
+    q.gam = c.ts / 2.0;   // nstep = 1
+    for (int k = 0; k < 4; k++) q.acc[k] = nullptr;
+    q.rhs_scale = rs_host;
+    if (set_io(p, q, state, p.buf[0])) return 1;
+    q.items = t->items;
+    p.last_variant = gen;
+    if (gen) launch_substep<true, 3>(t->nitems, q, s);
+    else launch_substep<false, 3>(t->nitems, q, s);
+    if (cudaGetLastError() != cudaSuccess) return 1;
+    for (int k = 0; k < 6; k++) std::swap(state[k], p.buf[0][k]);
     return 0;
 }
 

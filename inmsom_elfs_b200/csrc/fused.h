@@ -98,6 +98,14 @@ struct Plan {
     int occ[5] = {0, 0, 0, 0, 0};   // resident CTAs per SM, per item table
     std::vector<uint8_t> ocean;     // per strip and interior row: any written column is ocean
     int rows_per_item[2] = {0, 0};  // 0: one wave of items by cost; else rows per item
+    // plain-substep items over rows extended into the halo (a row strip
+    // that advances several substeps per exchange): per variant and number
+    // of rows computed south / north of the interior, built on first use
+    struct ExtTable {
+        int gen, s, n, nitems;
+        int4 *items;
+    };
+    std::vector<ExtTable> ext;
     unsigned generation = 0;        // bumped whenever buffers or work items change
     // prepare_steps: classification of the forcing for launch_steps
     bool prepared = false;
@@ -175,6 +183,13 @@ int prepare_steps(Plan &p, const Dom &d, const Consts &c, double *state[6], doub
 int launch_steps(Plan &p, const Dom &d, const Consts &c, double dt, int nsteps, const double *rs_dev,
                  const int *rs_base, double *state[6], cudaStream_t s, double rs_host = 1.0);
 int finish_steps(Plan &p, cudaStream_t s);
+// One plain substep (prepared by prepare_steps) over the interior rows and
+// ext_s rows south / ext_n rows north of them, in the halo of a row strip
+// whose halo is at least 2 rows wider than that on each side: a strip that
+// advances k substeps per halo exchange of 2k rows computes 2(k-i) rows
+// into its halo in substep i, which its neighbour computes alike.
+int launch_step_ext(Plan &p, const Dom &d, const Consts &c, double dt, int ext_s, int ext_n, double *state[6],
+                    cudaStream_t s, double rs_host);
 // The FP32-velocity run in the same parts: prepare_steps_f32 also converts
 // the state, the other ping-pong set and RHSx/RHSy to FP32 (returns 2 if the
 // grid needs the general variant); launch_steps_f32 enqueues nsteps

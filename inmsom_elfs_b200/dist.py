@@ -10,7 +10,11 @@ northernmost interior rows of the six state fields go to the northern
 neighbour's southern halo rows and the two southernmost to the southern
 neighbour's northern halo rows.  The fused kernel recomputes the
 intermediates it needs in its halo rows, so this gives the single-domain
-result bit for bit.
+result bit for bit.  With halos of 2k rows between the strips (the GPU
+form of the reference's wide-halo exchange mode) a rank advances k
+substeps per exchange of 2k rows, computing 2(k-i) rows into each shared
+halo in substep i of a block, as its neighbour does from the same values:
+the same result with k times fewer exchanges.
 
 Transport: torch.distributed point-to-point (batch_isend_irecv).  With NCCL
 the device buffers go directly, ordered on the context's CUDA stream; with
@@ -38,13 +42,17 @@ class GpuStripStepper:
         self.solver = solver
         ctx = solver._ctx
         lib = load()
-        self.n = 12 * int(lib.inmsom_gpu_pitch(ctx))
+        hs, hn = ctypes.c_int(), ctypes.c_int()
+        check(lib.inmsom_gpu_halo(ctx, ctypes.byref(hs), ctypes.byref(hn)))
+        self.halo = (hs.value, hn.value)
+        pitch = int(lib.inmsom_gpu_pitch(ctx))
+        sizes = [6 * w * pitch for w in (hs.value, hn.value)] * 2   # send s/n, receive s/n
         dev = torch.device("cuda", solver.device)
-        self.dev = [torch.empty(self.n, dtype=torch.float64, device=dev) for _ in range(4)]
+        self.dev = [torch.empty(n, dtype=torch.float64, device=dev) for n in sizes]
         self.stream = torch.cuda.ExternalStream(lib.inmsom_gpu_stream(ctx), device=dev)
         self.host = host_staging
         if host_staging:
-            self.cpu = [torch.empty(self.n, dtype=torch.float64).pin_memory() for _ in range(4)]
+            self.cpu = [torch.empty(n, dtype=torch.float64).pin_memory() for n in sizes]
 
     # buffers: 0 send south, 1 send north, 2 receive south, 3 receive north
     def buffer(self, k: int):
@@ -53,8 +61,9 @@ class GpuStripStepper:
     def begin(self) -> None:
         check(load().inmsom_step_begin(self.solver._ctx))
 
-    def launch(self, dt: float, rs: float) -> None:
-        check(load().inmsom_step_launch(self.solver._ctx, float(dt), float(rs)))
+    def launch(self, dt: float, rs: float, rows_south: int = 0, rows_north: int = 0) -> None:
+        check(load().inmsom_step_launch_rows(self.solver._ctx, float(dt), float(rs), int(rows_south),
+                                             int(rows_north)))
 
     def pack(self, side: int) -> None:
         check(load().inmsom_halo_pack(self.solver._ctx, side, ctypes.c_void_p(self.dev[side].data_ptr())))
@@ -108,26 +117,49 @@ def exchange(stepper, rank: int, world: int, group=None) -> None:
         stepper.unpack(1)
 
 
+def substeps_per_exchange(stepper, rank: int, world: int) -> int:
+    """k of a strip whose halos shared with other strips are 2k rows (every
+    rank computes the same k from the common halo width)."""
+    hs, hn = stepper.halo
+    shared = ([hs] if rank > 0 else []) + ([hn] if rank + 1 < world else [])
+    if not shared:
+        return 1
+    if len(set(shared)) != 1 or shared[0] < 2 or shared[0] % 2:
+        raise ValueError(f"rank {rank}: shared halos {shared} must be one even width >= 2")
+    return shared[0] // 2
+
+
 def run_strip(stepper, rank: int, world: int, nsub: int, dt: float,
               rhs_scale: Optional[Sequence[float]] = None, group=None) -> None:
-    """nsub substeps of this rank's strip with one halo exchange after each."""
+    """nsub substeps of this rank's strip: blocks of k substeps (k from the
+    halo width, 1 with the reference's two rows), the i-th computing 2(k-i)
+    rows into each shared halo, and one halo exchange after each block."""
+    k = substeps_per_exchange(stepper, rank, world)
     stepper.begin()
-    for k in range(nsub):
-        stepper.launch(dt, 1.0 if rhs_scale is None else float(rhs_scale[k]))
+    step = 0
+    while step < nsub:
+        n = min(k, nsub - step)
+        for i in range(1, n + 1):
+            e = 2 * (n - i)
+            stepper.launch(dt, 1.0 if rhs_scale is None else float(rhs_scale[step]),
+                           e if rank > 0 else 0, e if rank + 1 < world else 0)
+            step += 1
         exchange(stepper, rank, world, group)
     stepper.end()
 
 
 class NumpyStripStepper:
     """A stand-in with the same interface for testing the exchange on CPU:
-    six fields on the strip's rows (two halo rows each side), a radius-2
+    six fields on the strip's rows (halo rows each side), a radius-2
     row/column stencil that, like the fused kernel, needs only the state's
     halo rows.  Rows outside the global interior are never written."""
 
     def __init__(self, fields: np.ndarray, local_rows: tuple):
         self.f = fields.copy()                       # [6, nx, rows]
         self.l0, self.l1 = local_rows                # first/last interior rows of this strip (local index)
-        self.buf = [np.zeros((6, self.f.shape[1], 2)) for _ in range(4)]
+        self.halo = (self.l0, self.f.shape[2] - 1 - self.l1)
+        w = self.halo * 2
+        self.buf = [np.zeros((6, self.f.shape[1], w[k])) for k in range(4)]
 
     def buffer(self, k):
         import torch
@@ -136,10 +168,10 @@ class NumpyStripStepper:
     def begin(self):
         pass
 
-    def launch(self, dt, rs):
+    def launch(self, dt, rs, rows_south=0, rows_north=0):
         f = self.f
         new = f.copy()
-        for j in range(self.l0, self.l1 + 1):
+        for j in range(self.l0 - rows_south, self.l1 + rows_north + 1):
             for q in range(6):
                 a = f[q, 2:-2, j]
                 new[q, 2:-2, j] = (0.4 * a + 0.15 * (f[q, 2:-2, j - 1] + f[q, 2:-2, j + 1])
@@ -149,8 +181,9 @@ class NumpyStripStepper:
         self.f = new
 
     def pack(self, side):
-        r = self.l0 if side == 0 else self.l1 - 1
-        self.buf[side][...] = self.f[:, :, r:r + 2]
+        w = self.halo[side]
+        r = self.l0 if side == 0 else self.l1 - w + 1
+        self.buf[side][...] = self.f[:, :, r:r + w]
 
     def sync(self):
         pass
@@ -159,8 +192,9 @@ class NumpyStripStepper:
         pass
 
     def unpack(self, side):
-        r = self.l0 - 2 if side == 0 else self.l1 + 1
-        self.f[:, :, r:r + 2] = self.buf[2 + side]
+        w = self.halo[side]
+        r = self.l0 - w if side == 0 else self.l1 + 1
+        self.f[:, :, r:r + w] = self.buf[2 + side]
 
     def end(self):
         pass

@@ -1,7 +1,9 @@
-"""One process per strip (inmsom_elfs_b200.dist): the per-substep halo
-exchange between gloo ranks on CPU, with a radius-2 numpy stencil standing
-in for the GPU substep, must reproduce the single-domain run bit for bit
-(2 and 3 ranks); the FP64 all-reduce of the diagnostics (dist.diag) must
+"""One process per strip (inmsom_elfs_b200.dist): the halo exchange between
+gloo ranks on CPU, with a radius-2 numpy stencil standing in for the GPU
+substep, must reproduce the single-domain run bit for bit (2 and 3 ranks),
+with the reference's two halo rows (an exchange per substep) and with wide
+halos of 2k rows (k substeps per exchange, computing into the halo, the
+last block of a run shorter); the FP64 all-reduce of the diagnostics (dist.diag) must
 give every rank the single-domain volume and energy.  The GPU side of the
 same exchange is tested in test_dist_gpu.py."""
 import os
@@ -37,30 +39,33 @@ def _split(world):
     return out
 
 
-def _rank(rank, world, port, q):
+def _rank(rank, world, port, q, halo):
     import torch.distributed as dist
-    from inmsom_elfs_b200.dist import NumpyStripStepper, run_strip
+    from inmsom_elfs_b200.dist import NumpyStripStepper, run_strip, substeps_per_exchange
     os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port))
     dist.init_process_group("gloo", rank=rank, world_size=world)
     try:
         a, b = _split(world)[rank]
-        f = _fields()[:, :, a - 2:b + 3]
-        st = NumpyStripStepper(f, (2, b - a + 2))
+        hs = halo if rank > 0 else 2
+        hn = halo if rank + 1 < world else 2
+        f = _fields()[:, :, a - hs:b + hn + 1]
+        st = NumpyStripStepper(f, (hs, b - a + hs))
+        assert substeps_per_exchange(st, rank, world) == halo // 2
         run_strip(st, rank, world, NSUB, 0.5, np.linspace(0.5, 1.5, NSUB))
-        q.put((rank, st.f[:, :, 2:b - a + 3]))
+        q.put((rank, st.f[:, :, hs:b - a + hs + 1]))
     finally:
         dist.destroy_process_group()
 
 
-@pytest.mark.parametrize("world", [2, 3])
-def test_gloo_ranks_reproduce_one_domain(world):
+@pytest.mark.parametrize("world,halo", [(2, 2), (3, 2), (2, 4), (3, 6)])
+def test_gloo_ranks_reproduce_one_domain(world, halo):
     from inmsom_elfs_b200.dist import NumpyStripStepper, run_strip
     ref = NumpyStripStepper(_fields(), (2, ROWS - 3))
     run_strip(ref, 0, 1, NSUB, 0.5, np.linspace(0.5, 1.5, NSUB))
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _port()
-    procs = [ctx.Process(target=_rank, args=(r, world, port, q)) for r in range(world)]
+    procs = [ctx.Process(target=_rank, args=(r, world, port, q, halo)) for r in range(world)]
     for p in procs:
         p.start()
     got = dict(q.get(timeout=300) for _ in range(world))

@@ -1,7 +1,7 @@
 """One process per strip on the GPU (inmsom_step_*, inmsom_halo_*,
 inmsom_elfs_b200.dist): two ranks, each with its own context for its strip,
-advance with one halo exchange per substep (gloo, staged through host
-memory; both ranks on the one GPU this test gets -- their kernels never
+advance with one halo exchange per substep, or with halos of 2k rows k
+substeps per exchange (gloo, staged through host memory; both ranks on the one GPU this test gets -- their kernels never
 wait for each other, the host exchange orders them) and must end bit for
 bit where the single-domain fused run ends; the all-reduced volume and
 energy equal the single-domain diagnostics to 1e-13 / 1e-12 relative."""
@@ -29,7 +29,7 @@ def _basin():
     return b
 
 
-def _rank(rank, world, port, q):
+def _rank(rank, world, port, q, halo):
     import torch
     import torch.distributed as dist
     from inmsom_elfs_b200 import basins, solver
@@ -40,7 +40,7 @@ def _rank(rank, world, port, q):
     try:
         torch.cuda.set_device(0)
         b = _basin()
-        loc = split_basin(b, world)[rank]
+        loc = split_basin(b, world, halo)[rank]
         scale = basins.wind_cycle(NSUB, b.dt, t0=50.0, period=900.0)
         from inmsom_elfs_b200.dist import diag
         with solver.BarotropicSolver(loc, resident=True) as s:
@@ -53,13 +53,14 @@ def _rank(rank, world, port, q):
         dist.destroy_process_group()
 
 
-def test_two_ranks_match_single_domain(gpu):
+@pytest.mark.parametrize("halo", [2, 6])
+def test_two_ranks_match_single_domain(gpu, halo):
     from inmsom_elfs_b200 import basins
     from inmsom_elfs_b200.strips import gather_state, split_basin
     ctx = mp.get_context("spawn")
     q = ctx.Queue()
     port = _port()
-    procs = [ctx.Process(target=_rank, args=(r, 2, port, q)) for r in range(2)]
+    procs = [ctx.Process(target=_rank, args=(r, 2, port, q, halo)) for r in range(2)]
     for p in procs:
         p.start()
     got, dg = {}, {}
@@ -81,7 +82,7 @@ def test_two_ranks_match_single_domain(gpu):
     # sums up to the order of the additions
     assert dg[0] == dg[1]
     assert abs(dg[0][0] - vol) <= 1e-13 * abs(vol) and abs(dg[0][1] - en) <= 1e-12 * abs(en)
-    parts = split_basin(b, 2)
+    parts = split_basin(b, 2, halo)
     for r in range(2):
         parts[r].state.update(got[r])
     merged = gather_state(parts, b)
@@ -102,4 +103,8 @@ def test_step_entry_points_check_their_arguments(gpu):
             _lib.check(lib.inmsom_step_launch(s._ctx, b.dt, 1.0))
         with pytest.raises(InmsomError):
             _lib.check(lib.inmsom_halo_pack(s._ctx, 2, ctypes.c_void_p(1)))
+        _lib.check(lib.inmsom_step_begin(s._ctx))
+        with pytest.raises(InmsomError):           # rows beyond a basin edge
+            _lib.check(lib.inmsom_step_launch_rows(s._ctx, b.dt, 1.0, 2, 0))
+        _lib.check(lib.inmsom_step_end(s._ctx))
         assert lib.inmsom_gpu_pitch(s._ctx) % 32 == 0

@@ -1,8 +1,8 @@
 """FP32 velocity storage (INMSOM_FP32_VELOCITY) for inmsom_run_substeps.
 
 u, up, v, vp live in FP32 on the device during a run; every operation and
-SSH stay FP64.  Tolerances against the FP64 fused run (normwise relative,
-max|a-b|/max|b|), written here:
+SSH stay FP64.  Tolerances against the FP64 fused run and against the FP64
+CPU oracle (normwise relative, max|a-b|/max|b|), written here:
   * after 300 substeps of the 400 x 300 regional basin: SSH <= 1e-6,
     u and v (both levels) <= 2e-6 (measured on a B200: 3.4e-7 and 4.4e-7);
   * the closed-basin volume is conserved to 1e-13 relative, as in FP64:
@@ -49,6 +49,25 @@ def test_fp32_velocity_close_to_fp64(gpu):
     # the velocities came back through FP32
     u = b32.state["ubrtr_e"]
     assert np.array_equal(u, u.astype(np.float32).astype(np.float64))
+
+
+def test_fp32_velocity_against_the_fp64_oracle(gpu, ora):
+    # the errors of the variant against the FP64 CPU oracle (the reference's
+    # scheme): the same bounds as against the FP64 GPU run, which itself
+    # stays within 1e-12 of the oracle over this many steps
+    b = _prep(gpu, basins.regional_basin(nx=400, ny=300, seed=41))
+    ora.hh_init_external(b)
+    scale = basins.wind_cycle(300, b.dt, t0=0.0, period=1800.0)
+    bo = b.copy()
+    ora.run_substeps(bo, 300, b.dt, scale)
+    b32, _, _ = _run(gpu, b, 300, True, scale)
+    ocean = b.masks["lu"] > 0.5
+    errs = {k: rel_err(b32.state[k], bo.state[k]) for k in bo.state}
+    rms = {k: float(np.sqrt(np.mean((b32.state[k] - bo.state[k])[ocean] ** 2))) for k in bo.state}
+    print("fp32 velocity vs FP64 oracle: normwise", errs, "rms", rms)
+    assert errs["ssh_e"] <= TOL_SSH and errs["sshp_e"] <= TOL_SSH, errs
+    for k in ("ubrtr_e", "ubrtrp_e", "vbrtr_e", "vbrtrp_e"):
+        assert errs[k] <= TOL_UV, (k, errs[k])
 
 
 def test_fp32_velocity_conserves_volume(gpu):

@@ -117,3 +117,42 @@ def test_strip_bounds_follow_the_reference_formula():
     assert all(x.nx_start == g.nx_start and x.nx_end == g.nx_end for x in s)
     with pytest.raises(ValueError):
         strip_bounds(Bounds.serial(10, 3), 4)
+
+
+def test_stacked_strip_equals_split_of_the_stack(ora):
+    from inmsom_elfs_b200 import basins
+    """strips.stacked_strip (the multi-GPU benchmark's strips: N basins
+    stacked along y, each finalized on its own) gives exactly what
+    split_basin gives on the explicitly stacked global basin, for the
+    reference's 2-row halos and for wide ones."""
+    from dataclasses import replace
+    from inmsom_elfs_b200.grid import Basin
+    from inmsom_elfs_b200.strips import split_basin, stacked_strip
+    n, ny = 3, 30
+    parts = {q: basins.finalize(basins.regional_basin(nx=40, ny=ny, seed=5 + q), ora.OracleBackend())
+             for q in range(n)}
+    for q, p in parts.items():
+        p.state["ssh_e"][...] = np.random.default_rng(q).standard_normal(p.bounds.shape)
+    own = parts[0]
+    b = own.bounds
+    glob = replace(b, ny_end=b.ny_start + n * ny - 1, bnd_y2=b.ny_start + n * ny + 1, nn=b.nnn + n * ny - 1)
+
+    def stack(get):
+        cols = [get(parts[0])[:, :2]] + [get(parts[q])[:, 2:-2] for q in range(n)] + [get(parts[n - 1])[:, -2:]]
+        return np.asfortranarray(np.concatenate(cols, axis=1))
+
+    def grp(name):
+        return {k: stack(lambda p, k=k: getattr(p, name)[k]) for k in getattr(own, name)}
+
+    g = Basin(glob, own.consts, grp("masks"), grp("metrics"), stack(lambda p: p.rlh_s),
+              stack(lambda p: p.hhq_rest), grp("depths"), grp("state"), grp("means"), grp("forcing"),
+              grp("scratch"), None, None, own.dt)
+    for halo in (2, 6):
+        sp = split_basin(g, n, halo)
+        for r in range(n):
+            loc = stacked_strip({q: parts[q] for q in (r - 1, r, r + 1) if 0 <= q < n}, n, r, halo)
+            assert loc.bounds == sp[r].bounds
+            for name in ("masks", "metrics", "state", "forcing", "depths"):
+                for k, v in getattr(loc, name).items():
+                    assert np.array_equal(v, getattr(sp[r], name)[k]), (name, k, r)
+            assert np.array_equal(loc.hhq_rest, sp[r].hhq_rest) and np.array_equal(loc.rlh_s, sp[r].rlh_s)

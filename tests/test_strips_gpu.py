@@ -1,6 +1,8 @@
 """Row strips on one GPU (inmsom_strips_*): a basin split into strips, one
-context each, advanced with one halo-row exchange per substep, must end bit
-for bit where the single-domain fused run ends (both fused variants)."""
+context each, advanced with one halo-row exchange per substep -- or, with
+halos of 2k rows, k substeps per exchange computing into the halos -- must
+end bit for bit where the single-domain fused run ends (both fused
+variants)."""
 import numpy as np
 import pytest
 
@@ -10,8 +12,9 @@ from inmsom_elfs_b200.strips import gather_state, split_basin
 pytestmark = pytest.mark.gpu
 
 
-@pytest.mark.parametrize("nstrips,general", [(3, False), (2, True), (4, False)])
-def test_strips_match_single_domain(gpu, nstrips, general):
+@pytest.mark.parametrize("nstrips,general,halo", [(3, False, 2), (2, True, 2), (4, False, 2),
+                                                  (3, False, 4), (2, True, 6), (4, False, 8)])
+def test_strips_match_single_domain(gpu, nstrips, general, halo):
     b = basins.regional_basin(nx=180, ny=170, seed=91)
     if general:
         rng = np.random.default_rng(92)
@@ -25,7 +28,7 @@ def test_strips_match_single_domain(gpu, nstrips, general):
         s.run_substeps(nsub, b.dt, scale)
         s.sync_to_host()
         assert s.path()[0] == 1
-    parts = split_basin(b, nstrips)
+    parts = split_basin(b, nstrips, halo)
     solvers = [gpu.BarotropicSolver(p, resident=True) for p in parts]
     for s in solvers:
         assert s.path()[0] == 1, s.path()[1]
