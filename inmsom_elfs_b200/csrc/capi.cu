@@ -290,6 +290,7 @@ int inmsom_gpu_finalize(inmsom_ctx *c)
     cudaFree(c->d_out);
     if (c->rs_exec) cudaGraphExecDestroy(c->rs_exec);
     cudaFree(c->d_rs);
+    cudaFreeHost(c->h_rs);
     cudaFree(c->d_base);
     if (c->cl_exec) cudaGraphExecDestroy(c->cl_exec);
     cudaFree(c->cl_fac[0]);   // one block with cl_fac[1]
@@ -434,6 +435,7 @@ int inmsom_barotropic_dynamics(inmsom_ctx *c, double tau, int nstep, int ksw4, d
         if (static_coef && coef && c->coef_on_device[k]) continue;
         CKR(h2d(c, c->forc[k], hf[k]));
         c->coef_on_device[k] = static_coef && coef;
+        c->forc_gen++;
     }
     if (!resident) {
         for (int k = 0; k < NDEPTH; k++)
@@ -515,6 +517,7 @@ int inmsom_load_state(inmsom_ctx *c, double *ubrtr_e, double *ubrtrp_e, double *
         if (k == F_MU4 && !mu4) continue;
         CKR(h2d(c, c->forc[k], hf[k]));
         c->coef_on_device[k] = static_coef && k != F_RHSX && k != F_RHSY;
+        c->forc_gen++;
     }
     c->state_on_device = true;
     fused::mark_state_changed(c->plan);
@@ -560,6 +563,8 @@ int rs_capture(inmsom_ctx *c, int len, double dt)
     const cudaError_t ie = cudaGraphInstantiate(&c->rs_exec, g, 0);
     cudaGraphDestroy(g);
     if (ie != cudaSuccess) return set_err(INMSOM_ECUDA, "fused substeps: %s", cudaGetErrorString(ie));
+    // put the graph on the device now, not at its first launch
+    CK(cudaGraphUpload(c->rs_exec, c->stream));
     c->rs_len = len;
     c->rs_gen = p.generation;
     c->rs_dt = dt;
@@ -589,6 +594,14 @@ int rs_setup(inmsom_ctx *c, int nsub, double dt)
         CK(cudaMalloc(&c->d_rs, (size_t)nsub * sizeof(double)));
         c->rs_cap = (size_t)nsub;
     }
+    if ((size_t)nsub > c->h_rs_cap) {
+        CK(cudaStreamSynchronize(c->stream));
+        cudaFreeHost(c->h_rs);
+        c->h_rs = nullptr;
+        c->h_rs_cap = 0;
+        CK(cudaMallocHost(&c->h_rs, (size_t)nsub * sizeof(double)));
+        c->h_rs_cap = (size_t)nsub;
+    }
     const int len = rs_length(nsub);
     if (c->rs_pgen >= 0 && c->plan.prepared && !rs_current(c, len, dt)) CKR(rs_capture(c, len, dt));
     return INMSOM_OK;
@@ -601,17 +614,17 @@ int rs_setup(inmsom_ctx *c, int nsub, double dt)
 // work items, the state's set or the forcing mode change.  FP32 velocity
 // storage: the same with its kernel, between the conversions to and from
 // FP32.
-int run_substeps_graph(inmsom_ctx *c, int nsub, double dt, const double *rhs_scale)
+int run_substeps_graph(inmsom_ctx *c, int nsub, double dt, const double *rhs_scale, bool *ev1_recorded)
 {
     const bool f32 = (c->flags & INMSOM_FP32_VELOCITY) != 0;
     if (f32) {
-        const int rc = fused::prepare_steps_f32(c->plan, c->dom, c->c, c->state, c->forc, c->stream);
+        const int rc = fused::prepare_steps_f32(c->plan, c->dom, c->c, c->state, c->forc, c->stream, c->forc_gen);
         if (rc == 2)
             return set_err(INMSOM_EUNSUPPORTED,
                            "FP32 velocity storage needs a square uniform grid with uniform viscosity, drag and "
                            "water flux");
         if (rc) return set_err(INMSOM_ECUDA, "fused substeps: prepare failed: %s", cudaGetErrorString(cudaGetLastError()));
-    } else if (fused::prepare_steps(c->plan, c->dom, c->c, c->state, c->forc, c->stream)) {
+    } else if (fused::prepare_steps(c->plan, c->dom, c->c, c->state, c->forc, c->stream, c->forc_gen)) {
         return set_err(INMSOM_ECUDA, "fused substeps: prepare failed: %s", cudaGetErrorString(cudaGetLastError()));
     }
     auto launch = [&](int n) {
@@ -619,16 +632,22 @@ int run_substeps_graph(inmsom_ctx *c, int nsub, double dt, const double *rhs_sca
                                              c->stream)
                    : fused::launch_steps(c->plan, c->dom, c->c, dt, n, c->d_rs, c->d_base, c->state, c->stream);
     };
-    std::vector<double> rs((size_t)nsub, 1.0);
-    if (rhs_scale)
-        for (int k = 0; k < nsub; k++) rs[k] = rhs_scale[k];
-    CK(cudaMemcpyAsync(c->d_rs, rs.data(), (size_t)nsub * sizeof(double), cudaMemcpyHostToDevice, c->stream));
+    // the scales go through pinned memory (an asynchronous copy); the
+    // previous run ended with a synchronisation, so the buffer is free
+    for (int k = 0; k < nsub; k++) c->h_rs[k] = rhs_scale ? rhs_scale[k] : 1.0;
+    CK(cudaMemcpyAsync(c->d_rs, c->h_rs, (size_t)nsub * sizeof(double), cudaMemcpyHostToDevice, c->stream));
     CK(cudaMemsetAsync(c->d_base, 0, sizeof(int), c->stream));
     const int len = rs_length(nsub);
     if (!rs_current(c, len, dt)) CKR(rs_capture(c, len, dt));
     const int groups = nsub / len, rest = nsub % len;
     for (int gi = 0; gi < groups; gi++) CK(cudaGraphLaunch(c->rs_exec, c->stream));
     if (rest && launch(rest)) return set_err(INMSOM_ECUDA, "fused substeps: launch failed");
+    // the end of the run's device work, before the status read-back waits
+    // for it (the FP32 run's last work is its conversion back to FP64)
+    if (!f32) {
+        CK(cudaEventRecord(c->ev1, c->stream));
+        *ev1_recorded = true;
+    }
     const int frc = f32 ? fused::finish_steps_f32(c->plan, c->dom, c->state, c->stream)
                         : fused::finish_steps(c->plan, c->stream);
     if (frc) return set_err(INMSOM_ECUDA, "fused substeps: %s", cudaGetErrorString(cudaGetLastError()));
@@ -647,10 +666,11 @@ int inmsom_run_substeps(inmsom_ctx *c, int nsub, double dt, const double *rhs_sc
     if ((c->flags & INMSOM_FP32_VELOCITY) && !c->fused_ok)
         return set_err(INMSOM_EUNSUPPORTED, "FP32 velocity storage needs the fused path (%s)", c->fused_reason);
     const bool graph = c->fused_ok && nsub >= 2;
+    bool ev1_recorded = false;
     if (graph) CKR(rs_setup(c, nsub, dt));
     CK(cudaEventRecord(c->ev0, c->stream));
     if (graph) {
-        CKR(run_substeps_graph(c, nsub, dt, rhs_scale));
+        CKR(run_substeps_graph(c, nsub, dt, rhs_scale, &ev1_recorded));
         c->depths_current = false;
         if (c->plan.last_flags & (fused::FLAG_TIMEOUT | fused::FLAG_SMEM)) return fused_flag_error(c, "fused kernel");
     } else if (c->fused_ok) {
@@ -685,7 +705,7 @@ int inmsom_run_substeps(inmsom_ctx *c, int nsub, double dt, const double *rhs_sc
         }
         for (int k = 0; k < NWORK; k++) w[k] = saved[k];
     }
-    CK(cudaEventRecord(c->ev1, c->stream));
+    if (!ev1_recorded) CK(cudaEventRecord(c->ev1, c->stream));
     CKR(sync_stream(c));
     if (ms) CK(cudaEventElapsedTime(ms, c->ev0, c->ev1));
     if (c->flags & INMSOM_GUARD) {

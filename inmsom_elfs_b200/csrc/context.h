@@ -103,6 +103,9 @@ struct inmsom_ctx {
     bool depths_current = false;    // depth[] == hh_init(state) or evolved faithfully
     bool scratch_on_device = false;
     bool coef_on_device[NFORC] = {};   // INMSOM_STATIC_COEFFS: field copied in and current
+    unsigned forc_gen = 1;           // changes whenever forc[] is written (the fused path's staging key)
+    double *h_rs = nullptr;          // pinned staging of the per-substep RHS scales
+    size_t h_rs_cap = 0;
 
     fused::Plan plan{};              // fused-path layout and eligibility
     // run_substeps as replays of a graph of rs_len (even, <= RS_GROUP) substeps

@@ -109,6 +109,7 @@ struct Plan {
     unsigned generation = 0;        // bumped whenever buffers or work items change
     // prepare_steps: classification of the forcing for launch_steps
     bool prepared = false;
+    unsigned staged_key = 0;        // key of the preparation the staged forcing belongs to (0: none)
     int prep_gen = 0;
     double prep_mu0 = 0.0, prep_rd0 = 0.0, prep_wq0 = 0.0;
     // FP32 velocity storage for run_substeps (uniform variant): per state
@@ -172,14 +173,16 @@ int run_substeps(Plan &p, const Dom &d, const Consts &c, int nsub, double dt,
                  const double *rhs_scale, double *state[6], double *forc[6],
                  cudaStream_t s);
 // Capture-friendly form of run_substeps for CUDA graphs (FP64): prepare_steps
-// classifies the forcing and stages it (it synchronises the stream);
+// classifies the forcing and stages it (it synchronises the stream) -- or,
+// given the nonzero key of its last preparation (the caller changes the key
+// whenever it writes the forcing fields), keeps what it found then;
 // launch_steps then only enqueues nsteps kernels, the RHS scale of launch k
 // being rs_dev[*rs_base + k] read on the device, or rs_host when rs_dev is
 // NULL (an even nsteps leaves the
 // state in the same set, so the launches can be replayed); finish_steps
 // reads the status bits.
 int prepare_steps(Plan &p, const Dom &d, const Consts &c, double *state[6], double *forc[6],
-                  cudaStream_t s);
+                  cudaStream_t s, unsigned key = 0);
 int launch_steps(Plan &p, const Dom &d, const Consts &c, double dt, int nsteps, const double *rs_dev,
                  const int *rs_base, double *state[6], cudaStream_t s, double rs_host = 1.0);
 int finish_steps(Plan &p, cudaStream_t s);
@@ -197,7 +200,7 @@ int launch_step_ext(Plan &p, const Dom &d, const Consts &c, double dt, int ext_s
 // rs_host[k] (or 1); finish_steps_f32 writes the velocities back to the
 // FP64 state and reads the status bits.
 int prepare_steps_f32(Plan &p, const Dom &d, const Consts &c, double *state[6], double *forc[6],
-                      cudaStream_t s);
+                      cudaStream_t s, unsigned key = 0);
 int launch_steps_f32(Plan &p, const Dom &d, const Consts &c, double dt, int nsteps, const double *rs_dev,
                      const int *rs_base, const double *rs_host, double *state[6], cudaStream_t s);
 int finish_steps_f32(Plan &p, const Dom &d, double *state[6], cudaStream_t s);

@@ -61,6 +61,9 @@ def test_drop_in_call_times_out_then_recovers(gpu, ora):
         with pytest.raises(_lib.InmsomError, match="timed out"):
             s.barotropic_dynamics(3 * b.dt, 3)
         assert lib.inmsom_test_hold_copy(s._ctx, -1, 0, 0) == _lib.OK
+        # the timed-out call left the resident state undefined; the host
+        # arrays still hold the start state (the call copied nothing out)
+        s.sync_from_host(_lib.SYNC_STATE)
         for _ in range(3):
             ora.barotropic_dynamics(bo, 3 * b.dt, 3)
             s.barotropic_dynamics(3 * b.dt, 3)
