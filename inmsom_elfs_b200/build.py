@@ -30,6 +30,7 @@ SOURCES = {
     "capi_io.cu": [],
     "noalloc.cu": [],
     "closure.cu": [],
+    "closure_tc.cu": [],
     "column.cu": ["--fmad=false"],
     "dstd.cu": [],
     "ctl_read.cu": [],

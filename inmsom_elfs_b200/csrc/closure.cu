@@ -762,9 +762,7 @@ bool smem_ready = false;
 int ensure_smem()
 {
     if (smem_ready) return INMSOM_OK;
-    if (cudaFuncSetAttribute(k_mlp_grad, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sizeof(GSmem)) !=
-        cudaSuccess)
-        return fail(INMSOM_ECUDA, "MLP kernels: shared memory attribute");
+    if (inmsom::closure::grad_tc_setup()) return fail(INMSOM_ECUDA, "MLP kernels: shared memory attribute");
     smem_ready = true;
     return INMSOM_OK;
 }
@@ -833,17 +831,14 @@ int inmsom_mlp_grad(const void *x, const float *targets, const int *idx, int bat
         return fail(INMSOM_EARG, "inmsom_mlp_grad: NULL argument");
     if (batch <= 0 || batch % TILE) return fail(INMSOM_EARG, "inmsom_mlp_grad: batch must be a positive multiple of 128");
     if (ensure_smem()) return INMSOM_ECUDA;
-    // persistent CTAs, at most one per 128 samples (the partial buffer's size)
-    int dev = 0, nsm = 148, occ = 1;
+    // persistent CTAs on the tcgen05 tensor cores, one per SM at most and
+    // at most one per 128 samples (the partial buffer's size)
+    int dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_mlp_grad, GW * 32, sizeof(GSmem)) != cudaSuccess ||
-        occ < 1)
-        occ = 1;
-    const int grid = std::min(batch / TILE, occ * nsm);
-    k_mlp_grad<<<grid, GW * 32, sizeof(GSmem), (cudaStream_t)stream>>>(
-        (const __nv_bfloat16 *)x, targets, idx, batch, params, (const __nv_bfloat16 *)wbf16, partial);
-    if (check_launch("inmsom_mlp_grad")) return INMSOM_ECUDA;
+    const int grid = std::min(batch / TILE, nsm);
+    if (inmsom::closure::grad_tc(x, targets, idx, batch, params, wbf16, partial, grid, (cudaStream_t)stream))
+        return check_launch("inmsom_mlp_grad");
     k_mlp_reduce<<<(NPARAM + 1 + 31) / 32, 256, 0, (cudaStream_t)stream>>>(partial, grid, batch, grad);
     return check_launch("inmsom_mlp_grad reduce");
 }

@@ -33,5 +33,14 @@ int features(const Args &a, int nsm, cudaStream_t s);
 int factors(const Args &a, const float *lcu, const float *lcv, const double *dxt, const double *dyh,
             const double *dyt, const double *dxh, double *fac_u, double *fac_v, cudaStream_t s);
 
+// The training gradient on the tcgen05 tensor cores (closure_tc.cu):
+// per-CTA partial sums (INMSOM_MLP_PARTIAL floats each) of grid persistent
+// CTAs, one per SM at most, over the batch's tiles of 128 samples;
+// grad_tc_setup sets the kernel's shared-memory size once.
+size_t grad_tc_smem();
+int grad_tc_setup();
+int grad_tc(const void *x, const float *targets, const int *idx, int batch, const float *params, const void *wbf16,
+            float *partial, int grid, cudaStream_t s);
+
 }  // namespace closure
 }  // namespace inmsom

@@ -67,6 +67,7 @@ def test_drop_in_call_times_out_then_recovers(gpu, ora):
         for _ in range(3):
             ora.barotropic_dynamics(bo, 3 * b.dt, 3)
             s.barotropic_dynamics(3 * b.dt, 3)
+        s.sync_to_host()                        # the resident state to the host arrays
     for k in ("ssh_e", "ubrtr_e", "vbrtr_e"):
         assert rel_err(bg.state[k], bo.state[k]) <= 1e-12, k
     for k in ("ubrtr_i", "vbrtr_i"):
