@@ -1,6 +1,8 @@
 // Learned subgrid momentum closure: a 45 -> 64 -> 64 -> 2 MLP with GELU,
-// BF16 weights and activations on the tensor cores (mma.sync m16n8k16,
-// FP32 accumulate), FP32 master weights and Adam.  No counterpart in the
+// BF16 weights and activations on the tensor cores (FP32 accumulate), FP32
+// master weights and Adam.  Inference (fused into the step's forcing, and
+// on feature rows) chains the layers through registers with mma.sync
+// m16n8k16; the training gradient is closure_tc.cu's tcgen05 kernel.  No counterpart in the
 // reference: it stands in for the Laplacian viscosity of uv_diff2
 // (Function/vel_ssh.f90:117-184) on coarse grids.
 //
@@ -52,7 +54,8 @@ __device__ __forceinline__ void mma16816(float c[4], const uint32_t a[4], const 
 // GELU in the tanh form of Hendrycks & Gimpel (2016),
 // 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))), with the hardware tanh
 // (tanh.approx.f32, relative error about 2^-11: below the BF16 rounding of
-// the activations); training and inference use this one definition.
+// the activations); training (closure_tc.cu) and inference use this one
+// definition.
 constexpr float GC0 = 0.7978845608028654f, GC1 = 0.7978845608028654f * 0.044715f;
 __device__ __forceinline__ float tanh_hw(float x)
 {
@@ -64,11 +67,6 @@ __device__ __forceinline__ float gelu(float x)
 {
     const float h = 0.5f * x;
     return fmaf(h, tanh_hw(x * fmaf(GC1, x * x, GC0)), h);
-}
-__device__ __forceinline__ float gelu_d(float x)
-{
-    const float x2 = x * x, t = tanh_hw(x * fmaf(GC1, x2, GC0));
-    return fmaf(0.5f, 1.0f + t, 0.5f * x * (1.0f - t * t) * fmaf(3.0f * GC1, x2, GC0));
 }
 
 // grad[p] = sum over CTAs of partial[c][p] in CTA order (deterministic);
@@ -346,345 +344,23 @@ __global__ void k_closure_factors(inmsom::closure::Args a, const float *lcu, con
     }
 }
 
-// ============================================================ training
-// Gradient of the mean squared error, 64 samples per tile, one warp per 16
-// samples.  Forward: layer outputs chained through registers as MMA
-// fragments (like k_closure_apply), pre-activations z1, z2 kept in registers
-// for the backward pass, activations a1, a2 stored to shared memory.
-// Backward, per warp: output gradient, d(a2) = d3 W3^T, d(z2), d(a1) =
-// d(z2) W2^T, d(z1), again chained through registers; then the weight
-// gradients (K = the tile's samples, across the warps) from transposed
-// ldmatrix fragments.  CTAs loop over tiles; each warp owns a fixed set of
-// weight-gradient tiles and adds to them in shared memory, so the per-CTA
-// sums, like their reduction over CTAs, do not depend on timing.
+// ======================================================= feature rows
+// The training gradient runs on the tcgen05 tensor cores (closure_tc.cu).
+// Here: the network of k_closure_apply on rows of features, 64 samples per
+// tile, one warp per 16.
 constexpr int GT = 64, GW = 4;            // samples per tile, warps per CTA
-constexpr int XS = KIN + 8, HS = HID + 8, OS = 24;   // padded row strides (16-byte rows, conflict-free)
-
-struct GSmem {
-    alignas(16) __nv_bfloat16 w1t[HID][XS];            // W1^T [out][in]
-    alignas(16) __nv_bfloat16 w2t[HID][HS];   // W2^T
-    alignas(16) __nv_bfloat16 w3t[16][HS];             // W3^T, outputs padded to 16 (rows 8..15 zero)
-    float b1[HID], b2[HID], b3[N3];
-    alignas(16) __nv_bfloat16 x[2][GT][XS];   // this tile's inputs and the next one's
-    alignas(16) float tg[2][GT][NOUT];       // targets, likewise
-    alignas(16) __nv_bfloat16 a1[GT][HS], a2[GT][HS];
-    alignas(16) __nv_bfloat16 d1[GT][HS], d2[GT][HS];
-    alignas(16) __nv_bfloat16 d3[GT][OS];              // output gradients, columns 8..15 zero
-    float bw[GW][2 * HID + N3];            // per-warp bias-gradient sums (b1, b2, b3)
-    float lw[GW];                          // per-warp squared-error sums
-    float dw[OFF_B3];                      // weight-gradient sums (the parameter layout, biases unused)
-};
+constexpr int XS = KIN + 8, HS = HID + 8;  // padded row strides (16-byte rows, conflict-free)
 
 __device__ __forceinline__ uint32_t smem_addr(const void *p)
 {
     return (uint32_t)__cvta_generic_to_shared(p);
 }
-__device__ __forceinline__ void cp_async16(void *dst, const void *src)
-{
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async8(void *dst, const void *src)
-{
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"(smem_addr(dst)), "l"(src) : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait1() { asm volatile("cp.async.wait_group 1;" ::: "memory"); }
 
 __device__ __forceinline__ void ldsm4(uint32_t r[4], const void *p)
 {
     asm volatile("ldmatrix.sync.aligned.m8n8.x4.shared.b16 {%0,%1,%2,%3}, [%4];"
                  : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
                  : "r"(smem_addr(p)));
-}
-__device__ __forceinline__ void ldsm4t(uint32_t r[4], const void *p)
-{
-    asm volatile("ldmatrix.sync.aligned.m8n8.x4.trans.shared.b16 {%0,%1,%2,%3}, [%4];"
-                 : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3])
-                 : "r"(smem_addr(p)));
-}
-__device__ __forceinline__ void ldsm2t(uint32_t r[2], const void *p)
-{
-    asm volatile("ldmatrix.sync.aligned.m8n8.x2.trans.shared.b16 {%0,%1}, [%2];"
-                 : "=r"(r[0]), "=r"(r[1])
-                 : "r"(smem_addr(p)));
-}
-
-// B fragments of n-tiles nt, nt+1 for k-block kb from a [n][k] array
-// (row stride S): b[0], b[1] of nt, b[2], b[3] of nt+1
-template <int S>
-__device__ __forceinline__ void frag_b_nk(uint32_t b[4], const __nv_bfloat16 *base, int n0, int k0)
-{
-    const int l = threadIdx.x & 31;
-    ldsm4(b, base + (n0 + (l & 7) + 8 * (l >> 4)) * S + k0 + 8 * ((l >> 3) & 1));
-}
-// the same from a [k][n] array (transposed load)
-template <int S>
-__device__ __forceinline__ void frag_b_kn(uint32_t b[4], const __nv_bfloat16 *base, int n0, int k0)
-{
-    const int l = threadIdx.x & 31;
-    ldsm4t(b, base + (k0 + (l & 7) + 8 * ((l >> 3) & 1)) * S + n0 + 8 * (l >> 4));
-}
-
-// C fragments (16 x 64, 8 n-tiles) to the A fragments of a K = 64 product
-__device__ __forceinline__ void c_to_a(uint32_t a[4][4], const float c[8][4])
-{
-#pragma unroll
-    for (int kb = 0; kb < 4; kb++) {
-        a[kb][0] = pack2(c[2 * kb][0], c[2 * kb][1]);
-        a[kb][1] = pack2(c[2 * kb][2], c[2 * kb][3]);
-        a[kb][2] = pack2(c[2 * kb + 1][0], c[2 * kb + 1][1]);
-        a[kb][3] = pack2(c[2 * kb + 1][2], c[2 * kb + 1][3]);
-    }
-}
-// store C fragments (16 rows from m0, 64 columns) as BF16 to a [row][HS] array
-__device__ __forceinline__ void c_store(__nv_bfloat16 (*dst)[HS], int m0, const float c[8][4])
-{
-    const int l = threadIdx.x & 31, g = l >> 2, t = l & 3;
-#pragma unroll
-    for (int nt = 0; nt < 8; nt++) {
-        *reinterpret_cast<uint32_t *>(&dst[m0 + g][8 * nt + 2 * t]) = pack2(c[nt][0], c[nt][1]);
-        *reinterpret_cast<uint32_t *>(&dst[m0 + g + 8][8 * nt + 2 * t]) = pack2(c[nt][2], c[nt][3]);
-    }
-}
-// per-warp column sums of C fragments (16 rows) added to sums[64]
-__device__ __forceinline__ void c_colsum(float *sums, const float c[8][4])
-{
-    const int l = threadIdx.x & 31, t = l & 3;
-#pragma unroll
-    for (int nt = 0; nt < 8; nt++) {
-        float s0 = c[nt][0] + c[nt][2], s1 = c[nt][1] + c[nt][3];
-#pragma unroll
-        for (int o = 4; o < 32; o <<= 1) {
-            s0 += __shfl_xor_sync(0xffffffffu, s0, o);
-            s1 += __shfl_xor_sync(0xffffffffu, s1, o);
-        }
-        if (l < 4) {
-            sums[8 * nt + 2 * t] += s0;
-            sums[8 * nt + 2 * t + 1] += s1;
-        }
-    }
-}
-
-__global__ void __launch_bounds__(GW * 32) k_mlp_grad(const __nv_bfloat16 *x, const float *tgt, const int *idx,
-                                                     int batch, const float *prm, const __nv_bfloat16 *wb,
-                                                     float *partial)
-{
-    extern __shared__ __align__(16) unsigned char raw[];
-    GSmem &s = *reinterpret_cast<GSmem *>(raw);
-    const int w = threadIdx.x >> 5, l = threadIdx.x & 31, g = l >> 2, t = l & 3;
-    for (int i = threadIdx.x; i < KIN * HID; i += blockDim.x) s.w1t[i % HID][i / HID] = wb[BOFF_W1 + i];
-    for (int i = threadIdx.x; i < HID * HID; i += blockDim.x) s.w2t[i % HID][i / HID] = wb[BOFF_W2 + i];
-    for (int i = threadIdx.x; i < 16 * HS; i += blockDim.x) {
-        const int o = i / HS, c = i % HS;
-        s.w3t[o][c] = o < N3 && c < HID ? wb[BOFF_W3 + c * N3 + o] : __float2bfloat16(0.f);
-    }
-    for (int i = threadIdx.x; i < HID; i += blockDim.x) {
-        s.b1[i] = prm[OFF_B1 + i];
-        s.b2[i] = prm[OFF_B2 + i];
-    }
-    if (threadIdx.x < N3) s.b3[threadIdx.x] = prm[OFF_B3 + threadIdx.x];
-    for (int i = threadIdx.x; i < GT * OS; i += blockDim.x) s.d3[i / OS][i % OS] = __float2bfloat16(0.f);
-    for (int i = threadIdx.x; i < OFF_B3; i += blockDim.x) s.dw[i] = 0.f;
-    for (int i = threadIdx.x; i < GW * (2 * HID + N3); i += blockDim.x) (&s.bw[0][0])[i] = 0.f;
-    if (threadIdx.x < GW) s.lw[threadIdx.x] = 0.f;
-    const float scale = 2.0f / ((float)batch * NOUT);
-    const int m0 = 16 * w;
-    const int ntiles = batch / GT;
-    // the inputs (64 rows of 6 x 16 bytes) and targets of a tile into buffer b
-    auto fetch = [&](int tile, int b) {
-        if (tile < ntiles) {
-            for (int i = threadIdx.x; i < GT * 7; i += blockDim.x) {
-                const int r = i / 7, q = i % 7;
-                const long long row = idx ? idx[tile * GT + r] : (long long)tile * GT + r;
-                if (q < 6) cp_async16(&s.x[b][r][8 * q], x + row * KIN + 8 * q);
-                else cp_async8(&s.tg[b][r][0], tgt + row * NOUT);
-            }
-        }
-        cp_async_commit();   // an empty group past the last tile keeps the count
-    };
-    fetch(blockIdx.x, 0);
-    int cur = 0;
-    for (int tile = blockIdx.x; tile < ntiles; tile += gridDim.x, cur ^= 1) {
-        __syncthreads();   // the previous tile's shared arrays are no longer read
-        fetch(tile + gridDim.x, cur ^ 1);
-        cp_async_wait1();  // this tile's group has landed (for this thread)
-        __syncthreads();   // ... and for every thread
-        // ---- forward (this warp's 16 samples)
-        float z1[8][4], z2[8][4], acc[8][4];
-        uint32_t a[4][4];
-#pragma unroll
-        for (int nt = 0; nt < 8; nt++) {
-            z1[nt][0] = z1[nt][2] = s.b1[8 * nt + 2 * t];
-            z1[nt][1] = z1[nt][3] = s.b1[8 * nt + 2 * t + 1];
-        }
-#pragma unroll
-        for (int kb = 0; kb < 3; kb++) {
-            uint32_t af[4];
-            ldsm4(af, &s.x[cur][m0 + (l & 7) + 8 * ((l >> 3) & 1)][16 * kb + 8 * (l >> 4)]);
-#pragma unroll
-            for (int np = 0; np < 4; np++) {
-                uint32_t b[4];
-                frag_b_nk<XS>(b, &s.w1t[0][0], 16 * np, 16 * kb);
-                mma16816(z1[2 * np], af, b);
-                mma16816(z1[2 * np + 1], af, b + 2);
-            }
-        }
-#pragma unroll
-        for (int nt = 0; nt < 8; nt++)
-#pragma unroll
-            for (int q = 0; q < 4; q++) acc[nt][q] = gelu(z1[nt][q]);
-        c_to_a(a, acc);
-        c_store(s.a1, m0, acc);
-#pragma unroll
-        for (int nt = 0; nt < 8; nt++) {
-            z2[nt][0] = z2[nt][2] = s.b2[8 * nt + 2 * t];
-            z2[nt][1] = z2[nt][3] = s.b2[8 * nt + 2 * t + 1];
-        }
-#pragma unroll
-        for (int kb = 0; kb < 4; kb++)
-#pragma unroll
-            for (int np = 0; np < 4; np++) {
-                uint32_t b[4];
-                frag_b_nk<HS>(b, &s.w2t[0][0], 16 * np, 16 * kb);
-                mma16816(z2[2 * np], a[kb], b);
-                mma16816(z2[2 * np + 1], a[kb], b + 2);
-            }
-#pragma unroll
-        for (int nt = 0; nt < 8; nt++)
-#pragma unroll
-            for (int q = 0; q < 4; q++) acc[nt][q] = gelu(z2[nt][q]);
-        c_to_a(a, acc);
-        c_store(s.a2, m0, acc);
-        float o[4];
-        o[0] = o[2] = s.b3[2 * t];
-        o[1] = o[3] = s.b3[2 * t + 1];
-#pragma unroll
-        for (int kb = 0; kb < 4; kb += 2) {
-            uint32_t b[4];
-            ldsm4(b, &s.w3t[l & 7][16 * kb + 8 * (l >> 3)]);
-            mma16816(o, a[kb], b);
-            mma16816(o, a[kb + 1], b + 2);
-        }
-        // ---- loss and output gradient (outputs 0, 1 live in lanes t = 0)
-        float d3[4] = {0.f, 0.f, 0.f, 0.f}, lsum = 0.f;
-        if (t == 0) {
-#pragma unroll
-            for (int h = 0; h < 2; h++) {
-#pragma unroll
-                for (int j = 0; j < NOUT; j++) {
-                    const float e = o[2 * h + j] - s.tg[cur][m0 + g + 8 * h][j];
-                    lsum += e * e;
-                    d3[2 * h + j] = scale * e;
-                }
-            }
-        }
-        *reinterpret_cast<uint32_t *>(&s.d3[m0 + g][2 * t]) = pack2(d3[0], d3[1]);
-        *reinterpret_cast<uint32_t *>(&s.d3[m0 + g + 8][2 * t]) = pack2(d3[2], d3[3]);
-        {
-            float s0 = d3[0] + d3[2], s1 = d3[1] + d3[3];
-#pragma unroll
-            for (int q = 4; q < 32; q <<= 1) {
-                s0 += __shfl_xor_sync(0xffffffffu, s0, q);
-                s1 += __shfl_xor_sync(0xffffffffu, s1, q);
-                lsum += __shfl_xor_sync(0xffffffffu, lsum, q);
-            }
-            if (l < 4) {
-                s.bw[w][2 * HID + 2 * t] += s0;
-                s.bw[w][2 * HID + 2 * t + 1] += s1;
-            }
-            if (l == 0) s.lw[w] += lsum;
-        }
-        // ---- d(a2) = d3 W3^T (K = 16 padded outputs), d(z2) = d(a2) GELU'(z2)
-        {
-            const uint32_t ad[4] = {pack2(d3[0], d3[1]), pack2(d3[2], d3[3]), 0u, 0u};
-#pragma unroll
-            for (int nt = 0; nt < 8; nt++)
-#pragma unroll
-                for (int q = 0; q < 4; q++) acc[nt][q] = 0.f;
-#pragma unroll
-            for (int np = 0; np < 4; np++) {
-                uint32_t b[4];
-                frag_b_kn<HS>(b, &s.w3t[0][0], 16 * np, 0);
-                mma16816(acc[2 * np], ad, b);
-                mma16816(acc[2 * np + 1], ad, b + 2);
-            }
-        }
-#pragma unroll
-        for (int nt = 0; nt < 8; nt++)
-#pragma unroll
-            for (int q = 0; q < 4; q++) acc[nt][q] *= gelu_d(z2[nt][q]);
-        c_colsum(&s.bw[w][HID], acc);
-        c_to_a(a, acc);
-        c_store(s.d2, m0, acc);
-        // ---- d(a1) = d(z2) W2^T, d(z1) = d(a1) GELU'(z1)
-#pragma unroll
-        for (int nt = 0; nt < 8; nt++)
-#pragma unroll
-            for (int q = 0; q < 4; q++) acc[nt][q] = 0.f;
-#pragma unroll
-        for (int kb = 0; kb < 4; kb++)
-#pragma unroll
-            for (int np = 0; np < 4; np++) {
-                uint32_t b[4];
-                frag_b_kn<HS>(b, &s.w2t[0][0], 16 * np, 16 * kb);
-                mma16816(acc[2 * np], a[kb], b);
-                mma16816(acc[2 * np + 1], a[kb], b + 2);
-            }
-#pragma unroll
-        for (int nt = 0; nt < 8; nt++)
-#pragma unroll
-            for (int q = 0; q < 4; q++) acc[nt][q] *= gelu_d(z1[nt][q]);
-        c_colsum(&s.bw[w][0], acc);
-        c_store(s.d1, m0, acc);
-        __syncthreads();
-        // ---- weight gradients over the tile's samples: dW1 (3 x 8 tiles),
-        // dW2 (4 x 8), dW3 (4 x 1); tile q of 60 belongs to warp q % 4
-        for (int q = w; q < 60; q += GW) {
-            const __nv_bfloat16 *A, *B;
-            int sa, sb, m0w, n0w, off, ldw;
-            if (q < 24) {
-                A = &s.x[cur][0][0], sa = XS, B = &s.d1[0][0], sb = HS;
-                m0w = 16 * (q >> 3), n0w = 8 * (q & 7), off = OFF_W1, ldw = HID;
-            } else if (q < 56) {
-                const int r = q - 24;
-                A = &s.a1[0][0], sa = HS, B = &s.d2[0][0], sb = HS;
-                m0w = 16 * (r >> 3), n0w = 8 * (r & 7), off = OFF_W2, ldw = HID;
-            } else {
-                A = &s.a2[0][0], sa = HS, B = &s.d3[0][0], sb = OS;
-                m0w = 16 * (q - 56), n0w = 0, off = OFF_W3, ldw = N3;
-            }
-            float c[4] = {0.f, 0.f, 0.f, 0.f};
-#pragma unroll
-            for (int kb = 0; kb < GT / 16; kb++) {
-                uint32_t af[4], bf[2];
-                const int i = l >> 3, r = l & 7;
-                ldsm4t(af, A + (16 * kb + r + 8 * (i >> 1)) * sa + m0w + 8 * (i & 1));
-                ldsm2t(bf, B + (16 * kb + r + 8 * (i & 1)) * sb + n0w);
-                mma16816(c, af, bf);
-            }
-            float *dw = s.dw + off;
-            dw[(m0w + g) * ldw + n0w + 2 * t] += c[0];
-            dw[(m0w + g) * ldw + n0w + 2 * t + 1] += c[1];
-            dw[(m0w + g + 8) * ldw + n0w + 2 * t] += c[2];
-            dw[(m0w + g + 8) * ldw + n0w + 2 * t + 1] += c[3];
-        }
-    }
-    __syncthreads();
-    float *pg = partial + (size_t)blockIdx.x * NPART;
-    for (int i = threadIdx.x; i < OFF_B3; i += blockDim.x) {
-        const bool bias = (i >= OFF_B1 && i < OFF_W2) || (i >= OFF_B2 && i < OFF_W3);
-        if (!bias) pg[i] = s.dw[i];
-    }
-    for (int i = threadIdx.x; i < 2 * HID + N3; i += blockDim.x) {
-        float v = 0.f;
-        for (int k = 0; k < GW; k++) v += s.bw[k][i];
-        pg[i < HID ? OFF_B1 + i : (i < 2 * HID ? OFF_B2 + i - HID : OFF_B3 + i - 2 * HID)] = v;
-    }
-    if (threadIdx.x == 0) {
-        float v = 0.f;
-        for (int k = 0; k < GW; k++) v += s.lw[k];
-        pg[NPARAM] = v;
-    }
 }
 
 // y[n][0..1] = MLP(x[n]) for n < count: the network of k_closure_apply

@@ -4,8 +4,12 @@
 // No counterpart in the reference (the closure stands in for the Laplacian
 // viscosity of uv_diff2, Function/vel_ssh.f90:117-184, on coarse grids).
 //
-// One CTA of four warps per SM, persistent over tiles of 128 samples.
-// Thread r owns sample r of a tile and tensor-memory lane r.  Per tile:
+// One CTA of sixteen warps per SM, persistent over tiles of 128 samples.
+// Warp w reads tensor-memory lanes 32 (w % 4) .. +31 (the lane quarter it
+// may access), so each thread owns one sample (its lane) and 16 of the 64
+// columns of every layer's output (w / 4 picks which); the next tile's
+// inputs are fetched while a tile computes.  One thread issues the MMAs.
+// Per tile:
 //   forward   Z1 = X W1, A1 = GELU(Z1 + b1); Z2 = A1 W2, A2 = GELU(Z2 + b2);
 //             O = A2 W3 (+ b3)                        (M = 128 samples)
 //   backward  D3 = 2 (O - T) / (batch * 2); DA2 = D3 W3^T;
@@ -43,7 +47,8 @@ constexpr int OFF_W1 = 0, OFF_B1 = OFF_W1 + KIN * HID, OFF_W2 = OFF_B1 + HID, OF
 constexpr int BOFF_W1 = 0, BOFF_W2 = KIN * HID, BOFF_W3 = BOFF_W2 + HID * HID;
 static_assert(NPARAM == INMSOM_MLP_NPARAM, "parameter block size");
 constexpr int NPART = NPARAM + 1;
-constexpr int TILE = 128, THREADS = 128;
+constexpr int TILE = 128, THREADS = 512;
+constexpr int SLICE = 16;                 // columns of a 64-column block per thread (4 warps per lane quarter)
 constexpr int NO = 16;                    // output columns of the MMAs (2 used)
 constexpr int XC = 64, AC = 128;          // columns of the X and A1/A2 tiles (data, a ones column, zeros)
 constexpr unsigned WAIT_POLLS = 1u << 24;
@@ -65,7 +70,7 @@ struct __align__(128) Smem {
     __nv_bfloat16 dz2[TILE * HID];
     __nv_bfloat16 dz1[TILE * HID];
     float b1[HID], b2[HID], b3[NO];
-    float loss[THREADS / 32];
+    float loss[4];
     uint64_t mbar;
     uint32_t tmem_base;
     int gave_up;
@@ -124,23 +129,7 @@ __device__ __forceinline__ void fence_after() { asm volatile("tcgen05.fence::aft
 __device__ __forceinline__ void fence_smem_async() { asm volatile("fence.proxy.async.shared::cta;" ::: "memory"); }
 __device__ __forceinline__ void wait_ld() { asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory"); }
 
-// 32 consecutive FP32 columns of this thread's tensor-memory lane
-__device__ __forceinline__ void ld32(uint32_t taddr, float (&v)[32])
-{
-    uint32_t r[32];
-    asm volatile(
-        "tcgen05.ld.sync.aligned.32x32b.x32.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
-        "%15, %16, %17, %18, %19, %20, %21, %22, %23, %24, %25, %26, %27, %28, %29, %30, %31}, [%32];"
-        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
-          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15]),
-          "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
-          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
-        : "r"(taddr));
-    wait_ld();
-#pragma unroll
-    for (int k = 0; k < 32; k++) v[k] = __uint_as_float(r[k]);
-}
-
+// 16 consecutive FP32 columns of this thread's tensor-memory lane
 __device__ __forceinline__ void ld16(uint32_t taddr, float (&v)[16])
 {
     uint32_t r[16];
@@ -205,8 +194,10 @@ __global__ void __launch_bounds__(THREADS, 1)
 {
     extern __shared__ __align__(1024) unsigned char raw[];
     Smem &s = *reinterpret_cast<Smem *>(raw);
-    const int r = threadIdx.x, w = r >> 5;
-    const bool issuer = r == 0;
+    const int t = threadIdx.x, w = t >> 5, q = w & 3, cs = w >> 2;
+    const int r = 32 * q + (t & 31);       // this thread's sample row and tensor-memory lane
+    const int c0 = SLICE * cs;             // its columns of a 64-column block
+    const bool issuer = t == 0;
 
     if (issuer) {
         asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;" ::"r"(saddr(&s.mbar)) : "memory");
@@ -219,25 +210,26 @@ __global__ void __launch_bounds__(THREADS, 1)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    // weights (transposed into the K-major operands), biases, constant columns
-    for (int i = r; i < HID * XC; i += THREADS) {
-        const int o = i / XC, k = i % XC;   // row = output, column = input
+    // weights transposed into the K-major operands (coalesced reads of the
+    // [in][out] layout), biases, constant columns
+    for (int i = t; i < HID * XC; i += THREADS) {
+        const int k = i / HID, o = i % HID;   // W1[k][o], k = input
         s.w1t[blk(o, k, XC)] = k < KIN ? wb[BOFF_W1 + k * HID + o] : __float2bfloat16(0.f);
     }
-    for (int i = r; i < HID * HID; i += THREADS) {
-        const int o = i / HID, k = i % HID;
+    for (int i = t; i < HID * HID; i += THREADS) {
+        const int k = i / HID, o = i % HID;
         s.w2t[blk(o, k, HID)] = wb[BOFF_W2 + k * HID + o];
     }
-    for (int i = r; i < NO * HID; i += THREADS) {
-        const int o = i / HID, k = i % HID;
+    for (int i = t; i < NO * HID; i += THREADS) {
+        const int k = i / NO, o = i % NO;
         s.w3t[blk(o, k, HID)] = o < N3 ? wb[BOFF_W3 + k * N3 + o] : __float2bfloat16(0.f);
     }
-    if (r < HID) {
-        s.b1[r] = prm[OFF_B1 + r];
-        s.b2[r] = prm[OFF_B2 + r];
+    if (t < HID) {
+        s.b1[t] = prm[OFF_B1 + t];
+        s.b2[t] = prm[OFF_B2 + t];
     }
-    if (r < NO) s.b3[r] = r < N3 ? prm[OFF_B3 + r] : 0.f;
-    {
+    if (t < NO) s.b3[t] = t < N3 ? prm[OFF_B3 + t] : 0.f;
+    if (cs == 0) {
         float one[8] = {1.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, zero[8] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
         st_chunk(s.x, r, 48, XC, one);
         st_chunk(s.x, r, 56, XC, zero);
@@ -251,7 +243,7 @@ __global__ void __launch_bounds__(THREADS, 1)
     __syncthreads();
     fence_after();
     const uint32_t tb = s.tmem_base;
-    const uint32_t lane = tb + ((uint32_t)(32 * w) << 16);   // this warp's lanes
+    const uint32_t lane = tb + ((uint32_t)(32 * q) << 16);   // this warp's lane quarter
     const float scale = 2.0f / ((float)batch * NOUT);
     const int ntiles = batch / TILE;
     uint32_t ph = 0;
@@ -268,28 +260,44 @@ __global__ void __launch_bounds__(THREADS, 1)
         fence_after();
         return s.gave_up == 0;
     };
-
-    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
-        // ---- this thread's sample into row r of X
+    // this thread's part of a sample: 16-byte chunks cs and cs + 4 (of 6),
+    // and (slice 0) the two targets
+    uint4 xa = make_uint4(0u, 0u, 0u, 0u), xb = xa;
+    float t0 = 0.f, t1 = 0.f;
+    auto fetch = [&](int tile) {
+        if (tile >= ntiles) return;
         const long long row = idx ? (long long)idx[tile * TILE + r] : (long long)tile * TILE + r;
         const uint4 *src = reinterpret_cast<const uint4 *>(x + row * KIN);
-#pragma unroll
-        for (int q = 0; q < 6; q++) *reinterpret_cast<uint4 *>(s.x + blk(r, 8 * q, XC)) = src[q];
-        const float t0 = tgt[row * NOUT], t1 = tgt[row * NOUT + 1];
+        xa = src[cs];
+        if (cs + 4 < 6) xb = src[cs + 4];
+        if (cs == 0) {
+            t0 = tgt[row * NOUT];
+            t1 = tgt[row * NOUT + 1];
+        }
+    };
+    fetch(blockIdx.x);
+
+    for (int tile = blockIdx.x; tile < ntiles && ok; tile += gridDim.x) {
+        // ---- this tile's samples into X; the next tile's are fetched while
+        // this one computes
+        *reinterpret_cast<uint4 *>(s.x + blk(r, 8 * cs, XC)) = xa;
+        if (cs + 4 < 6) *reinterpret_cast<uint4 *>(s.x + blk(r, 8 * (cs + 4), XC)) = xb;
+        const float tg0 = t0, tg1 = t1;
         handoff();
+        fetch(tile + gridDim.x);
         // ---- Z1 = X W1 (K = 48)
         if (issuer)
             for (int ks = 0; ks < 3; ks++)
                 mma(tb + C_Z1, sdesc(s.x + 128 * ks, 128, 1024), sdesc(s.w1t + 128 * ks, 128, 1024),
                     idesc(128, 64, false, false), ks > 0);
         if (!(ok = sync_mma())) break;
-        for (int h = 0; h < 2; h++) {
-            float z[32];
-            ld32(lane + C_Z1 + 32 * h, z);
+        {
+            float z[16];
+            ld16(lane + C_Z1 + c0, z);
 #pragma unroll
-            for (int k = 0; k < 32; k++) z[k] = gelu(z[k] + s.b1[32 * h + k]);
-#pragma unroll
-            for (int q = 0; q < 4; q++) st_chunk(s.a1, r, 32 * h + 8 * q, AC, z + 8 * q);
+            for (int k = 0; k < 16; k++) z[k] = gelu(z[k] + s.b1[c0 + k]);
+            st_chunk(s.a1, r, c0, AC, z);
+            st_chunk(s.a1, r, c0 + 8, AC, z + 8);
         }
         handoff();
         // ---- Z2 = A1 W2 (K = 64)
@@ -298,13 +306,13 @@ __global__ void __launch_bounds__(THREADS, 1)
                 mma(tb + C_Z2, sdesc(s.a1 + 128 * ks, 128, 2048), sdesc(s.w2t + 128 * ks, 128, 1024),
                     idesc(128, 64, false, false), ks > 0);
         if (!(ok = sync_mma())) break;
-        for (int h = 0; h < 2; h++) {
-            float z[32];
-            ld32(lane + C_Z2 + 32 * h, z);
+        {
+            float z[16];
+            ld16(lane + C_Z2 + c0, z);
 #pragma unroll
-            for (int k = 0; k < 32; k++) z[k] = gelu(z[k] + s.b2[32 * h + k]);
-#pragma unroll
-            for (int q = 0; q < 4; q++) st_chunk(s.a2, r, 32 * h + 8 * q, AC, z + 8 * q);
+            for (int k = 0; k < 16; k++) z[k] = gelu(z[k] + s.b2[c0 + k]);
+            st_chunk(s.a2, r, c0, AC, z);
+            st_chunk(s.a2, r, c0 + 8, AC, z + 8);
         }
         handoff();
         // ---- O = A2 W3 (N = 16, 2 used)
@@ -313,16 +321,16 @@ __global__ void __launch_bounds__(THREADS, 1)
                 mma(tb + C_O, sdesc(s.a2 + 128 * ks, 128, 2048), sdesc(s.w3t + 128 * ks, 128, 1024),
                     idesc(128, NO, false, false), ks > 0);
         if (!(ok = sync_mma())) break;
-        {
+        if (cs == 0) {
             float o[16];
             ld16(lane + C_O, o);
-            const float e0 = o[0] + s.b3[0] - t0, e1 = o[1] + s.b3[1] - t1;
+            const float e0 = o[0] + s.b3[0] - tg0, e1 = o[1] + s.b3[1] - tg1;
             lsum += e0 * e0 + e1 * e1;
             float d[8] = {scale * e0, scale * e1, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
             st_chunk(s.d3, r, 0, NO, d);
         }
         handoff();
-        // ---- DA2 = D3 W3^T (K = 16); dW3 += A2^T D3 (M = 128 rows of A2, K = 128 samples)
+        // ---- DA2 = D3 W3^T (K = 16); dW3 += A2^T D3 (M = 128 columns of A2, K = 128 samples)
         if (issuer) {
             mma(tb + C_DA2, sdesc(s.d3, 128, 256), sdesc(s.w3t, 1024, 128), idesc(128, 64, false, true), 0);
             for (int ks = 0; ks < 8; ks++)
@@ -330,14 +338,14 @@ __global__ void __launch_bounds__(THREADS, 1)
                     idesc(128, NO, true, true), !(first && ks == 0));
         }
         if (!(ok = sync_mma())) break;
-        for (int h = 0; h < 2; h++) {
-            float da[32], z[32];
-            ld32(lane + C_DA2 + 32 * h, da);
-            ld32(lane + C_Z2 + 32 * h, z);
+        {
+            float da[16], z[16];
+            ld16(lane + C_DA2 + c0, da);
+            ld16(lane + C_Z2 + c0, z);
 #pragma unroll
-            for (int k = 0; k < 32; k++) da[k] *= gelu_d(z[k] + s.b2[32 * h + k]);
-#pragma unroll
-            for (int q = 0; q < 4; q++) st_chunk(s.dz2, r, 32 * h + 8 * q, HID, da + 8 * q);
+            for (int k = 0; k < 16; k++) da[k] *= gelu_d(z[k] + s.b2[c0 + k]);
+            st_chunk(s.dz2, r, c0, HID, da);
+            st_chunk(s.dz2, r, c0 + 8, HID, da + 8);
         }
         handoff();
         // ---- DA1 = DZ2 W2^T (K = 64); dW2 += A1^T DZ2
@@ -350,14 +358,14 @@ __global__ void __launch_bounds__(THREADS, 1)
                     idesc(128, 64, true, true), !(first && ks == 0));
         }
         if (!(ok = sync_mma())) break;
-        for (int h = 0; h < 2; h++) {
-            float da[32], z[32];
-            ld32(lane + C_DA1 + 32 * h, da);
-            ld32(lane + C_Z1 + 32 * h, z);
+        {
+            float da[16], z[16];
+            ld16(lane + C_DA1 + c0, da);
+            ld16(lane + C_Z1 + c0, z);
 #pragma unroll
-            for (int k = 0; k < 32; k++) da[k] *= gelu_d(z[k] + s.b1[32 * h + k]);
-#pragma unroll
-            for (int q = 0; q < 4; q++) st_chunk(s.dz1, r, 32 * h + 8 * q, HID, da + 8 * q);
+            for (int k = 0; k < 16; k++) da[k] *= gelu_d(z[k] + s.b1[c0 + k]);
+            st_chunk(s.dz1, r, c0, HID, da);
+            st_chunk(s.dz1, r, c0 + 8, HID, da + 8);
         }
         handoff();
         // ---- dW1 += X^T DZ1 (M = 64 columns of X)
@@ -371,46 +379,46 @@ __global__ void __launch_bounds__(THREADS, 1)
 
     if (ok && !first) {
         float *out = partial + (size_t)blockIdx.x * NPART;
-        // dW1: M = 64 rows in lanes 32 w + (0..15) of warp w: row 16 w + lane
-        const int lr = r & 31, m64 = 16 * w + lr;
-        for (int h = 0; h < 2; h++) {
-            float v[32];
-            ld32(lane + C_DW1 + 32 * h, v);
+        {
+            // dW1: M = 64 rows in lanes 32 q + (0..15) of quarter q: row 16 q + lane
+            const int lr = t & 31, m64 = 16 * q + lr;
+            float v[16];
+            ld16(lane + C_DW1 + c0, v);
             if (lr < 16) {
                 if (m64 < KIN)
-                    for (int k = 0; k < 32; k++) out[OFF_W1 + m64 * HID + 32 * h + k] = v[k];
+                    for (int k = 0; k < 16; k++) out[OFF_W1 + m64 * HID + c0 + k] = v[k];
                 else if (m64 == KIN)
-                    for (int k = 0; k < 32; k++) out[OFF_B1 + 32 * h + k] = v[k];
+                    for (int k = 0; k < 16; k++) out[OFF_B1 + c0 + k] = v[k];
             }
         }
-        for (int h = 0; h < 2; h++) {
-            float v[32];
-            ld32(lane + C_DW2 + 32 * h, v);
-            if (r < HID)
-                for (int k = 0; k < 32; k++) out[OFF_W2 + r * HID + 32 * h + k] = v[k];
-            else if (r == HID)
-                for (int k = 0; k < 32; k++) out[OFF_B2 + 32 * h + k] = v[k];
-        }
         {
+            float v[16];
+            ld16(lane + C_DW2 + c0, v);
+            if (r < HID)
+                for (int k = 0; k < 16; k++) out[OFF_W2 + r * HID + c0 + k] = v[k];
+            else if (r == HID)
+                for (int k = 0; k < 16; k++) out[OFF_B2 + c0 + k] = v[k];
+        }
+        if (cs == 0) {
             float v[16];
             ld16(lane + C_DW3, v);
             if (r < HID)
                 for (int k = 0; k < N3; k++) out[OFF_W3 + r * N3 + k] = v[k];
             else if (r == HID)
                 for (int k = 0; k < N3; k++) out[OFF_B3 + k] = v[k];
-        }
 #pragma unroll
-        for (int q = 16; q > 0; q >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, q);
-        if ((r & 31) == 0) s.loss[w] = lsum;
+            for (int m = 16; m > 0; m >>= 1) lsum += __shfl_xor_sync(0xffffffffu, lsum, m);
+            if ((t & 31) == 0) s.loss[q] = lsum;
+        }
         __syncthreads();
-        if (r == 0) out[NPARAM] = (s.loss[0] + s.loss[1]) + (s.loss[2] + s.loss[3]);
+        if (t == 0) out[NPARAM] = (s.loss[0] + s.loss[1]) + (s.loss[2] + s.loss[3]);
     }
     if (!ok) {
         // a wait gave up: the CTA's partial sums are NaN (so the gradient
         // and the loss are), and the MMAs of the step that timed out are
         // waited for (bounded) before the tensor memory is freed
         float *out = partial + (size_t)blockIdx.x * NPART;
-        for (int i = r; i < NPART; i += THREADS) out[i] = __int_as_float(0x7fc00000);
+        for (int i = t; i < NPART; i += THREADS) out[i] = __int_as_float(0x7fc00000);
         if (issuer) (void)wait_bar(&s.mbar, ph ^ 1u);
     }
     fence_before();
