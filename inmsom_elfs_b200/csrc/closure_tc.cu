@@ -210,19 +210,30 @@ __global__ void __launch_bounds__(THREADS, 1)
                      : "memory");
         asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
     }
-    // weights transposed into the K-major operands (coalesced reads of the
-    // [in][out] layout), biases, constant columns
-    for (int i = t; i < HID * XC; i += THREADS) {
-        const int k = i / HID, o = i % HID;   // W1[k][o], k = input
-        s.w1t[blk(o, k, XC)] = k < KIN ? wb[BOFF_W1 + k * HID + o] : __float2bfloat16(0.f);
-    }
-    for (int i = t; i < HID * HID; i += THREADS) {
-        const int k = i / HID, o = i % HID;
-        s.w2t[blk(o, k, HID)] = wb[BOFF_W2 + k * HID + o];
-    }
-    for (int i = t; i < NO * HID; i += THREADS) {
-        const int k = i / NO, o = i % NO;
-        s.w3t[blk(o, k, HID)] = o < N3 ? wb[BOFF_W3 + k * N3 + o] : __float2bfloat16(0.f);
+    // weights transposed into the K-major operands: 16-byte reads of 8
+    // consecutive outputs of one input row of the [in][out] layout, all
+    // issued before any is stored; biases, constant columns
+    {
+        constexpr int N1 = KIN * HID / 8, N2 = HID * HID / 8, NW3 = HID * N3 / 8;   // 16-byte pieces
+        static_assert(N1 <= THREADS && N2 <= THREADS && NW3 <= THREADS, "one piece per thread");
+        const uint4 *w16 = reinterpret_cast<const uint4 *>(wb);
+        uint4 p1 = make_uint4(0u, 0u, 0u, 0u), p2 = p1, p3 = p1;
+        if (t < N1) p1 = w16[(BOFF_W1 / 8) + t];
+        if (t < N2) p2 = w16[(BOFF_W2 / 8) + t];
+        if (t < NW3) p3 = w16[(BOFF_W3 / 8) + t];
+        auto put = [&](__nv_bfloat16 *dst, int C, int k, int o0, const uint4 &v) {
+            const __nv_bfloat16 *e = reinterpret_cast<const __nv_bfloat16 *>(&v);
+#pragma unroll
+            for (int j = 0; j < 8; j++) dst[blk(o0 + j, k, C)] = e[j];
+        };
+        if (t < N1) put(s.w1t, XC, t / (HID / 8), 8 * (t % (HID / 8)), p1);
+        if (t < N2) put(s.w2t, HID, t / (HID / 8), 8 * (t % (HID / 8)), p2);
+        if (t < NW3) put(s.w3t, HID, t, 0, p3);   // W3 row k = t: outputs 0..7
+        // W1^T columns 48..63 and W3^T rows 8..15 are zero
+        for (int i = t; i < HID * (XC - KIN); i += THREADS)
+            s.w1t[blk(i / (XC - KIN), KIN + i % (XC - KIN), XC)] = __float2bfloat16(0.f);
+        for (int i = t; i < (NO - N3) * HID; i += THREADS)
+            s.w3t[blk(N3 + i / HID, i % HID, HID)] = __float2bfloat16(0.f);
     }
     if (t < HID) {
         s.b1[t] = prm[OFF_B1 + t];
