@@ -609,8 +609,10 @@ def run_study_fp32(args):
 
 
 def run_study_ensemble(args):
-    """64 independent basins: graph ensemble (tuned, untuned) against the
-    members run one after another with inmsom_run_substeps."""
+    """64 independent basins: the ensemble as a CUDA graph of one launch per
+    member and substep and as one persistent launch per group of substeps
+    (tuned and untuned work items), against the members run one after
+    another with inmsom_run_substeps."""
     import torch
     from inmsom_elfs_b200 import basins, solver
     torch.cuda.set_device(0)
@@ -638,9 +640,10 @@ def run_study_ensemble(args):
         t += s.run_substeps(args.steps, b.dt, scale)
     res["sequential_members"] = {"ms": t, "cell_steps_per_s": cells * args.steps / (t / 1e3)}
     with solver.Ensemble(solvers, group=args.group) as e:
-        for tag in ("graph_untuned", "graph_tuned"):
+        for tag in ("graph_untuned", "persistent_untuned", "graph_tuned", "persistent_tuned"):
             if tag == "graph_tuned":
                 rows = e.tune(dts, trial_groups=2)
+            e.set_persistent(tag.startswith("persistent"))
             for s in solvers:
                 s.load_state()
             e.run(2 * args.group, dts)

@@ -611,6 +611,16 @@ int inmsom_ens_run(inmsom_ens *ens, int nsub, const double *dt, const double *rh
  * chunk) and keeps the fastest; rows_per_item[i] receives member i's
  * choice (0 = one wave).  The trial runs advance the members' states. */
 int inmsom_ens_tune(inmsom_ens *ens, const double *dt, int trial_groups, int *rows_per_item);
+/* on != 0: inmsom_ens_run advances each group of substeps of all members
+ * with ONE persistent cooperative launch (still replayed as a CUDA graph)
+ * instead of one launch per member and substep: one wave of CTAs claims the
+ * members' work items in the order (substep, member, item), and an item of
+ * a member starts once that member's items of the previous substep are
+ * done (per-member completion counters, bounded waits), so members never
+ * wait for one another and the substeps of a group have no launch
+ * boundary.  The same work items and arithmetic: the same values bit for
+ * bit.  on = 0 returns to the per-member graph. */
+int inmsom_ens_persistent(inmsom_ens *ens, int on);
 int inmsom_ens_destroy(inmsom_ens *ens);
 
 /* Row strips of one basin on several contexts (one per GPU, or several on

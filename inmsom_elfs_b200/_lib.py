@@ -34,7 +34,7 @@ EXPORTS = (
     "inmsom_write_checkpoint", "inmsom_read_checkpoint", "inmsom_tracer_tran_diff", "inmsom_ctl_file_read",
     "inmsom_pwdstd", "inmsom_prdstd", "inmsom_ocpwrite", "inmsom_ocpread",
     "inmsom_compare_grids", "inmsom_stress_components", "inmsom_smagorinsky_coeff",
-    "inmsom_test_hold_copy", "inmsom_step_launch_rows", "inmsom_gpu_halo",
+    "inmsom_test_hold_copy", "inmsom_step_launch_rows", "inmsom_gpu_halo", "inmsom_ens_persistent",
 )
 
 # include/inmsom_gpu.h: INMSOM_MLP_*
@@ -126,6 +126,7 @@ def load() -> ctypes.CDLL:
     lib.inmsom_ens_run.argtypes = [VP, i, DP, DP, ctypes.POINTER(ctypes.c_float)]
     lib.inmsom_ens_tune.argtypes = [VP, DP, i, ctypes.POINTER(i)]
     lib.inmsom_ens_destroy.argtypes = [VP]
+    lib.inmsom_ens_persistent.argtypes = [VP, i]
     lib.inmsom_strips_create.argtypes = [ctypes.POINTER(VP), ctypes.POINTER(VP), i]
     lib.inmsom_strips_run.argtypes = [VP, i, d, DP, ctypes.POINTER(ctypes.c_float)]
     lib.inmsom_strips_destroy.argtypes = [VP]

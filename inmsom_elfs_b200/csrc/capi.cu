@@ -1129,9 +1129,12 @@ struct inmsom_ens {
     std::vector<double> graph_dt;          // dt per member the graph was captured with
     std::vector<unsigned> graph_gen;       // plan generation per member at capture
     std::vector<const double *> graph_src; // state set per member at capture (an odd run moves the state)
+    std::vector<double> graph_prep;        // forcing mode per member at capture (variant, mu0, rd0, wq0)
     double *d_rs = nullptr;                // RHS scale per substep of the run
     size_t rs_cap = 0;
     int *d_base = nullptr;                 // first substep of the next group
+    bool persistent = false;               // one persistent launch per group (fused::ens_launch)
+    fused::EnsTable table;                 // its device tables (rebuilt with the graph)
 };
 
 namespace {
@@ -1140,19 +1143,32 @@ void ens_drop_graph(inmsom_ens *e)
 {
     if (e->exec) cudaGraphExecDestroy(e->exec);
     e->exec = nullptr;
+    fused::ens_free(e->table);
     e->graph_dt.clear();
     e->graph_gen.clear();
     e->graph_src.clear();
+    e->graph_prep.clear();
 }
 
 int ens_capture(inmsom_ens *e, const double *dt)
 {
     ens_drop_graph(e);
+    if (e->persistent) {
+        std::vector<fused::EnsMemberIn> in;
+        for (size_t i = 0; i < e->m.size(); i++) {
+            inmsom_ctx *c = e->m[i];
+            in.push_back({&c->plan, &c->dom, &c->c, dt[i], c->state});
+        }
+        if (fused::ens_table(in, e->group, e->d_rs, e->d_base, e->table, e->origin))
+            return set_err(INMSOM_ECUDA, "persistent ensemble tables: %s", cudaGetErrorString(cudaGetLastError()));
+    }
     cudaGraph_t g = nullptr;
     CK(cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeThreadLocal));
     int rc = INMSOM_OK;
     cudaError_t ce = cudaEventRecord(e->fork, e->origin);
-    for (size_t i = 0; i < e->m.size() && ce == cudaSuccess && rc == INMSOM_OK; i++) {
+    if (e->persistent && ce == cudaSuccess && fused::ens_launch(e->table, e->origin))
+        rc = set_err(INMSOM_ECUDA, "persistent ensemble launch failed during graph capture");
+    for (size_t i = 0; i < e->m.size() && !e->persistent && ce == cudaSuccess && rc == INMSOM_OK; i++) {
         inmsom_ctx *c = e->m[i];
         ce = cudaStreamWaitEvent(c->stream, e->fork, 0);
         if (ce == cudaSuccess &&
@@ -1181,6 +1197,9 @@ int ens_capture(inmsom_ens *e, const double *dt)
     e->graph_dt.assign(dt, dt + e->m.size());
     for (auto *c : e->m) e->graph_gen.push_back(c->plan.generation);
     for (auto *c : e->m) e->graph_src.push_back(c->state[0]);
+    for (auto *c : e->m)
+        e->graph_prep.insert(e->graph_prep.end(),
+                             {(double)c->plan.prep_gen, c->plan.prep_mu0, c->plan.prep_rd0, c->plan.prep_wq0});
     return INMSOM_OK;
 }
 
@@ -1191,6 +1210,11 @@ bool ens_graph_current(const inmsom_ens *e, const double *dt)
         if (e->graph_dt[i] != dt[i] || e->graph_gen[i] != e->m[i]->plan.generation ||
             e->graph_src[i] != e->m[i]->state[0])
             return false;
+    for (size_t i = 0; i < e->m.size(); i++) {
+        const fused::Plan &p = e->m[i]->plan;
+        const double *g = &e->graph_prep[4 * i];
+        if (g[0] != (double)p.prep_gen || g[1] != p.prep_mu0 || g[2] != p.prep_rd0 || g[3] != p.prep_wq0) return false;
+    }
     return true;
 }
 
@@ -1226,6 +1250,17 @@ int inmsom_ens_create(inmsom_ens **out, inmsom_ctx *const *members, int n, int g
         return set_err(INMSOM_ECUDA, "inmsom_ens_create: %s", cudaGetErrorString(ce));
     }
     *out = e;
+    return INMSOM_OK;
+}
+
+int inmsom_ens_persistent(inmsom_ens *e, int on)
+{
+    if (!e) return set_err(INMSOM_EARG, "NULL ensemble");
+    if (e->persistent != (on != 0)) {
+        CK(cudaSetDevice(e->device));
+        ens_drop_graph(e);
+        e->persistent = on != 0;
+    }
     return INMSOM_OK;
 }
 

@@ -741,6 +741,94 @@ __global__ void __launch_bounds__(NL, min_ctas<GEN, MODE, F32>()) k_substep(cons
     (void)substep_item<GEN, MODE, F32>(p, &p.tm_src, p.dst, rs, p.items[blockIdx.x], ring, mbar);
 }
 
+// ---------------------------------------------------------------------
+// Persistent ensemble kernel: ONE cooperative launch advances every member
+// of an ensemble by a group of plain substeps.  Its CTAs (one wave, all
+// resident) claim work items from one counter in the order (substep, member,
+// item); an item of member m at substep s starts once member m's items of
+// substep s - 1 are all done (a per-member, per-substep completion counter),
+// so members never wait for each other and a member's substeps follow one
+// another with no launch boundary.  Claims are monotonic and every claimed
+// item's dependencies were claimed earlier by resident CTAs, so the waits
+// always end; they are bounded all the same (a wait that gives up sets the
+// member's timeout bit and the item runs anyway, its result then wrong).
+// The items and their arithmetic are those of k_substep: the same values
+// bit for bit.
+struct EnsItem {
+    Params q[2];          // parity 0: reads the state set, writes the first ping-pong set; 1: back
+    const int4 *items;
+    int nitems, gen;
+};
+static_assert(sizeof(EnsItem) % 64 == 0, "tensor maps of consecutive members stay 64-byte aligned");
+
+__device__ __forceinline__ unsigned ld_acquire(const unsigned *a)
+{
+    unsigned v;
+    asm volatile("ld.acquire.gpu.global.u32 %0, [%1];" : "=r"(v) : "l"(a) : "memory");
+    return v;
+}
+
+constexpr int ENS_CTAS = 11;   // resident CTAs per SM the kernel is cut for (the general variant's)
+
+__global__ void __launch_bounds__(NL, ENS_CTAS)
+    k_ens_persistent(const EnsItem *__restrict__ mem, const int *__restrict__ moff, int nmem, int total,
+                     int group, unsigned *ctr, unsigned *done)
+{
+    extern __shared__ __align__(128) unsigned char smem_raw[];
+    unsigned char *ring = smem_raw;
+    const int l = threadIdx.x;
+    if (smem_addr(smem_raw) & 127u) {
+        if (l == 0) atomicOr(mem[0].q[0].flags, FLAG_SMEM);
+        return;
+    }
+    const unsigned work = (unsigned)total * (unsigned)group;
+    for (;;) {
+        unsigned c = 0;
+        if (l == 0) c = atomicAdd(ctr, 1u);
+        c = __shfl_sync(0xffffffffu, c, 0);
+        if (c >= work) break;
+        const int st = (int)(c / (unsigned)total), j = (int)(c % (unsigned)total);
+        int lo = 0, hi = nmem - 1;   // the member whose items hold flat index j
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (moff[mid] <= j) lo = mid;
+            else hi = mid - 1;
+        }
+        const int m = lo;
+        const EnsItem &em = mem[m];
+        const Params &q = em.q[st & 1];
+        if (st > 0) {
+            if (l == 0) {
+                unsigned polls = 0;
+                while (ld_acquire(&done[m * group + st - 1]) < (unsigned)em.nitems) {
+                    if (++polls > q.wait_limit) {
+                        atomicOr(q.flags, FLAG_TIMEOUT);
+                        break;
+                    }
+                    __nanosleep(64);
+                }
+            }
+            __syncwarp();
+            // the bulk copies below read what other CTAs stored
+            asm volatile("fence.proxy.async;" ::: "memory");
+        }
+        const double rs = q.rs_dev[*q.rs_base + st];
+        const int4 item = em.items[j - moff[m]];
+        if (em.gen) {
+            uint64_t *mbar = reinterpret_cast<uint64_t *>(ring + ring_slots<true, 3>() * Layout<true>::SLOT_B);
+            (void)substep_item<true, 3>(q, &q.tm_src, q.dst, rs, item, ring, mbar);
+        } else {
+            uint64_t *mbar = reinterpret_cast<uint64_t *>(ring + ring_slots<false, 3>() * Layout<false>::SLOT_B);
+            (void)substep_item<false, 3>(q, &q.tm_src, q.dst, rs, item, ring, mbar);
+        }
+        // this item's stores, visible to the bulk copies of later items, then counted
+        asm volatile("fence.proxy.async;" ::: "memory");
+        __threadfence();
+        __syncwarp();
+        if (l == 0) atomicAdd(&done[m * group + st], 1u);
+    }
+}
+
 // min/max over the ocean points of three fields, for the uniform-forcing test
 __global__ void k_minmax3(Dom D, const float *lu, const double *a, const double *b, const double *c3, double *out)
 {
@@ -1664,6 +1752,95 @@ int launch_step_ext(Plan &p, const Dom &d, const Consts &c, double dt, int ext_s
     if (cudaGetLastError() != cudaSuccess) return 1;
     for (int k = 0; k < 6; k++) std::swap(state[k], p.buf[0][k]);
     return 0;
+}
+
+int ens_table(const std::vector<EnsMemberIn> &mem, int group, const double *rs_dev, const int *rs_base, EnsTable &t,
+              cudaStream_t s)
+{
+    ens_free(t);
+    if (mem.empty() || group < 2 || group % 2) return 1;
+    std::vector<EnsItem> h(mem.size());
+    std::vector<int> off(mem.size());
+    int total = 0;
+    for (size_t i = 0; i < mem.size(); i++) {
+        Plan &p = *mem[i].p;
+        if (!p.prepared) return 1;
+        const int gen = p.prep_gen;
+        if (p.stat_box[gen] != (gen ? Layout<true>::NS : Layout<false>::NS)) return 1;
+        Forcing f{true, p.prep_mu0, p.prep_rd0, p.prep_wq0};
+        for (int par = 0; par < 2; par++) {
+            Params q = base_params(p, *mem[i].d, *mem[i].c, f, gen);
+            set_times(q, 2.0 * mem[i].dt, p);
+            q.gam = mem[i].c->ts / 2.0;   // nstep = 1
+            for (int k = 0; k < 4; k++) q.acc[k] = nullptr;
+            q.rs_dev = rs_dev;
+            q.rs_base = rs_base;
+            q.rhs_scale = 1.0;
+            double *const *state = mem[i].state;
+            if (set_io(p, q, par ? p.buf[0] : state, par ? state : p.buf[0])) return 1;
+            q.items = p.items[gen];
+            h[i].q[par] = q;
+        }
+        h[i].items = p.items[gen];
+        h[i].nitems = p.nitems[gen];
+        h[i].gen = gen;
+        off[i] = total;
+        total += p.nitems[gen];
+    }
+    const size_t smem = ring_bytes<true, 3>();
+    if (cudaFuncSetAttribute(k_ens_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return 1;
+    int occ = 0, dev = 0, nsm = 148;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ens_persistent, NL, smem) != cudaSuccess || occ < 1)
+        return 1;
+    EnsItem *dm = nullptr;
+    if (cudaMalloc(&dm, h.size() * sizeof(EnsItem)) != cudaSuccess) return 1;
+    t.d_mem = dm;
+    if (cudaMalloc(&t.d_moff, off.size() * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&t.d_ctr, sizeof(unsigned)) != cudaSuccess ||
+        cudaMalloc(&t.d_done, mem.size() * (size_t)group * sizeof(unsigned)) != cudaSuccess)
+        return 1;
+    if (cudaMemcpyAsync(dm, h.data(), h.size() * sizeof(EnsItem), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaMemcpyAsync(t.d_moff, off.data(), off.size() * sizeof(int), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess)   // the host vectors go out of scope
+        return 1;
+    t.nmem = (int)mem.size();
+    t.total = total;
+    t.group = group;
+    t.grid = occ * nsm;
+    t.smem = smem;
+    return 0;
+}
+
+int ens_launch(const EnsTable &t, cudaStream_t s)
+{
+    if (!t.d_mem) return 1;
+    if (cudaMemsetAsync(t.d_ctr, 0, sizeof(unsigned), s) != cudaSuccess ||
+        cudaMemsetAsync(t.d_done, 0, (size_t)t.nmem * t.group * sizeof(unsigned), s) != cudaSuccess)
+        return 1;
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(t.grid);
+    cfg.blockDim = dim3(NL);
+    cfg.dynamicSmemBytes = t.smem;
+    cfg.stream = s;
+    cudaLaunchAttribute at[1];
+    at[0].id = cudaLaunchAttributeCooperative;   // every CTA resident: the completion waits end
+    at[0].val.cooperative = 1;
+    cfg.attrs = at;
+    cfg.numAttrs = 1;
+    return cudaLaunchKernelEx(&cfg, k_ens_persistent, (const EnsItem *)t.d_mem, (const int *)t.d_moff, t.nmem,
+                              t.total, t.group, t.d_ctr, t.d_done) != cudaSuccess;
+}
+
+void ens_free(EnsTable &t)
+{
+    cudaFree(t.d_mem);
+    cudaFree(t.d_moff);
+    cudaFree(t.d_ctr);
+    cudaFree(t.d_done);
+    t = EnsTable{};
 }
 
 int finish_steps(Plan &p, cudaStream_t s)

@@ -206,6 +206,32 @@ int launch_steps_f32(Plan &p, const Dom &d, const Consts &c, double dt, int nste
 int finish_steps_f32(Plan &p, const Dom &d, double *state[6], cudaStream_t s);
 // re-cut the work items: rows_per_item = 0 for one wave of items by cost
 int repartition(Plan &p, const Dom &d, int rows_per_item, cudaStream_t s);
+// Persistent ensemble launch: one cooperative launch of one wave of CTAs
+// advances every member by `group` plain substeps (prepared by
+// prepare_steps, RHS scale of substep k read at rs_dev[*rs_base + k]); its
+// CTAs claim the members' work items in the order (substep, member, item),
+// an item of a member waiting (bounded) until that member's items of the
+// previous substep are done.  ens_table builds the device tables (the
+// members' source/destination sets of both parities and item tables);
+// ens_launch enqueues the counter resets and the launch (capturable).
+struct EnsMemberIn {
+    Plan *p;
+    const Dom *d;
+    const Consts *c;
+    double dt;
+    double *const *state;
+};
+struct EnsTable {
+    void *d_mem = nullptr;
+    int *d_moff = nullptr;
+    unsigned *d_ctr = nullptr, *d_done = nullptr;
+    int nmem = 0, total = 0, group = 0, grid = 0;
+    size_t smem = 0;
+};
+int ens_table(const std::vector<EnsMemberIn> &mem, int group, const double *rs_dev, const int *rs_base, EnsTable &t,
+              cudaStream_t s);
+int ens_launch(const EnsTable &t, cudaStream_t s);
+void ens_free(EnsTable &t);
 void free_plan(Plan &p);
 
 }  // namespace fused

@@ -336,11 +336,18 @@ class Ensemble:
     BarotropicSolver with its state resident; `group` substeps of all
     members per CUDA-graph launch."""
 
-    def __init__(self, members: Sequence["BarotropicSolver"], group: int = 10):
+    def __init__(self, members: Sequence["BarotropicSolver"], group: int = 10, persistent: bool = False):
         self.members = list(members)
         arr = (ctypes.c_void_p * len(self.members))(*[m._ctx.value for m in self.members])
         self._ens = ctypes.c_void_p()
         check(load().inmsom_ens_create(ctypes.byref(self._ens), arr, len(self.members), int(group)))
+        if persistent:
+            self.set_persistent(True)
+
+    def set_persistent(self, on: bool) -> None:
+        """One persistent cooperative launch per group of substeps
+        (inmsom_ens_persistent) instead of one launch per member and substep."""
+        check(load().inmsom_ens_persistent(self._ens, 1 if on else 0))
 
     def _dt(self, dt):
         a = np.ascontiguousarray(dt, dtype=np.float64)

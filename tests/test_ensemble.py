@@ -1,8 +1,9 @@
 """Ensemble runs (inmsom_ens_*): members of different sizes and both fused
-variants advanced by CUDA-graph launches must end bit for bit where each
-member run alone with inmsom_run_substeps ends -- the same kernels on the
-same data; the work partition (changed by the autotuner) does not change
-any value."""
+variants advanced by CUDA-graph launches -- one launch per member and
+substep, or one persistent launch per group of substeps -- must end bit for
+bit where each member run alone with inmsom_run_substeps ends: the same
+work items and arithmetic on the same data; the work partition (changed by
+the autotuner) does not change any value."""
 import numpy as np
 import pytest
 
@@ -33,13 +34,13 @@ def _alone(gpu, b, nsub, scale):
     return bg
 
 
-def _ensemble(gpu, bs, nsub, scale, group, tune=False):
+def _ensemble(gpu, bs, nsub, scale, group, tune=False, persistent=False):
     cps = [b.copy() for b in bs]
     solvers = [gpu.BarotropicSolver(b, resident=True) for b in cps]
     for s in solvers:
         s.load_state()
     dts = [b.dt for b in cps]
-    with gpu.Ensemble(solvers, group=group) as e:
+    with gpu.Ensemble(solvers, group=group, persistent=persistent) as e:
         rows = None
         if tune:
             rows = e.tune(dts, trial_groups=1)
@@ -52,13 +53,13 @@ def _ensemble(gpu, bs, nsub, scale, group, tune=False):
     return cps, rows
 
 
-@pytest.mark.parametrize("tune", [False, True])
-def test_ensemble_matches_members_run_alone(gpu, tune):
+@pytest.mark.parametrize("tune,persistent", [(False, False), (True, False), (False, True), (True, True)])
+def test_ensemble_matches_members_run_alone(gpu, tune, persistent):
     bs = _members(gpu)
     nsub = 22                                   # 5 graph launches of 4 and 2 direct substeps
     scale = basins.wind_cycle(nsub, 2.0, t0=300.0, period=600.0)
     ref = [_alone(gpu, b, nsub, scale) for b in bs]
-    got, rows = _ensemble(gpu, bs, nsub, scale, group=4, tune=tune)
+    got, rows = _ensemble(gpu, bs, nsub, scale, group=4, tune=tune, persistent=persistent)
     for r, g in zip(ref, got):
         for k in r.state:
             assert np.array_equal(r.state[k], g.state[k]), k
@@ -75,7 +76,8 @@ def test_ensemble_rejects_odd_group(gpu):
             gpu.Ensemble([s], group=3)
 
 
-def test_ensemble_odd_runs_back_to_back(gpu):
+@pytest.mark.parametrize("persistent", [False, True])
+def test_ensemble_odd_runs_back_to_back(gpu, persistent):
     """An odd run moves each member's state to its other ping-pong set; the
     next run must notice (recapture) and continue from there."""
     bs = _members(gpu)
@@ -86,7 +88,7 @@ def test_ensemble_odd_runs_back_to_back(gpu):
     for s in solvers:
         s.load_state()
     dts = [b.dt for b in cps]
-    with gpu.Ensemble(solvers, group=4) as e:
+    with gpu.Ensemble(solvers, group=4, persistent=persistent) as e:
         e.run(5, dts, scale[:5])       # one graph launch and one direct substep
         e.run(5, dts, scale[5:])
     for s in solvers:
