@@ -769,6 +769,7 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *a)
 }
 
 constexpr int ENS_CTAS = 11;   // resident CTAs per SM the kernel is cut for (the general variant's)
+constexpr unsigned ENS_WAIT_POLLS = 1u << 16;
 
 __global__ void __launch_bounds__(NL, ENS_CTAS)
     k_ens_persistent(const EnsItem *__restrict__ mem, const int *__restrict__ moff, int nmem, int total,
@@ -799,13 +800,15 @@ __global__ void __launch_bounds__(NL, ENS_CTAS)
         const Params &q = em.q[st & 1];
         if (st > 0) {
             if (l == 0) {
+                // an item lasts well under a millisecond: 2^16 polls of at
+                // least 128 ns each are ample
                 unsigned polls = 0;
                 while (ld_acquire(&done[m * group + st - 1]) < (unsigned)em.nitems) {
-                    if (++polls > q.wait_limit) {
+                    if (++polls > ENS_WAIT_POLLS) {
                         atomicOr(q.flags, FLAG_TIMEOUT);
                         break;
                     }
-                    __nanosleep(64);
+                    __nanosleep(128);
                 }
             }
             __syncwarp();
