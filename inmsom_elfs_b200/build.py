@@ -36,7 +36,7 @@ SOURCES = {
     "ctl_read.cu": [],
     "ocean_cp.cu": [],
 }
-HEADERS = ["common.cuh", "general.h", "fused.h", "closure.h", "column.h", "context.h"]
+HEADERS = ["common.cuh", "general.h", "fused.h", "closure.h", "column.h", "context.h", "gelu.cuh"]
 
 
 def nvcc() -> str:

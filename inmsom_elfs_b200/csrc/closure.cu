@@ -12,6 +12,7 @@
 // the same layout.  A sample is 48 BF16 features (45 used).
 #include "inmsom_gpu.h"
 #include "closure.h"
+#include "gelu.cuh"
 
 #include <cuda_bf16.h>
 
@@ -24,6 +25,8 @@ int record_error(int code, const char *msg);
 }
 
 namespace {
+
+using namespace inmsom::closure;
 
 constexpr int KIN = 48, HID = 64, NOUT = 2, N3 = 8;
 constexpr int OFF_W1 = 0, OFF_B1 = OFF_W1 + KIN * HID, OFF_W2 = OFF_B1 + HID, OFF_B2 = OFF_W2 + HID * HID,
@@ -49,24 +52,6 @@ __device__ __forceinline__ void mma16816(float c[4], const uint32_t a[4], const 
         "{%0,%1,%2,%3};"
         : "+f"(c[0]), "+f"(c[1]), "+f"(c[2]), "+f"(c[3])
         : "r"(a[0]), "r"(a[1]), "r"(a[2]), "r"(a[3]), "r"(b[0]), "r"(b[1]));
-}
-
-// GELU in the tanh form of Hendrycks & Gimpel (2016),
-// 0.5 x (1 + tanh(sqrt(2/pi) (x + 0.044715 x^3))), with the hardware tanh
-// (tanh.approx.f32, relative error about 2^-11: below the BF16 rounding of
-// the activations); training (closure_tc.cu) and inference use this one
-// definition.
-constexpr float GC0 = 0.7978845608028654f, GC1 = 0.7978845608028654f * 0.044715f;
-__device__ __forceinline__ float tanh_hw(float x)
-{
-    float y;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-__device__ __forceinline__ float gelu(float x)
-{
-    const float h = 0.5f * x;
-    return fmaf(h, tanh_hw(x * fmaf(GC1, x * x, GC0)), h);
 }
 
 // grad[p] = sum over CTAs of partial[c][p] in CTA order (deterministic);
@@ -203,10 +188,11 @@ __device__ __forceinline__ void mlp16(const S &s, const uint32_t a1[3][4], float
     uint32_t a2[4][4];
 #pragma unroll
     for (int kb = 0; kb < 4; kb++) {
-        a2[kb][0] = pack2(gelu(acc[2 * kb][0]), gelu(acc[2 * kb][1]));
-        a2[kb][1] = pack2(gelu(acc[2 * kb][2]), gelu(acc[2 * kb][3]));
-        a2[kb][2] = pack2(gelu(acc[2 * kb + 1][0]), gelu(acc[2 * kb + 1][1]));
-        a2[kb][3] = pack2(gelu(acc[2 * kb + 1][2]), gelu(acc[2 * kb + 1][3]));
+        // columns 16 kb .. +7 (an even 8-column block) and 16 kb + 8 .. +15
+        a2[kb][0] = pack2(gelu_t(acc[2 * kb][0]), gelu_t(acc[2 * kb][1]));
+        a2[kb][1] = pack2(gelu_t(acc[2 * kb][2]), gelu_t(acc[2 * kb][3]));
+        a2[kb][2] = pack2(gelu_p(acc[2 * kb + 1][0]), gelu_p(acc[2 * kb + 1][1]));
+        a2[kb][3] = pack2(gelu_p(acc[2 * kb + 1][2]), gelu_p(acc[2 * kb + 1][3]));
     }
 #pragma unroll
     for (int nt = 0; nt < 8; nt++) {
@@ -222,10 +208,11 @@ __device__ __forceinline__ void mlp16(const S &s, const uint32_t a1[3][4], float
         }
 #pragma unroll
     for (int kb = 0; kb < 4; kb++) {
-        a2[kb][0] = pack2(gelu(acc[2 * kb][0]), gelu(acc[2 * kb][1]));
-        a2[kb][1] = pack2(gelu(acc[2 * kb][2]), gelu(acc[2 * kb][3]));
-        a2[kb][2] = pack2(gelu(acc[2 * kb + 1][0]), gelu(acc[2 * kb + 1][1]));
-        a2[kb][3] = pack2(gelu(acc[2 * kb + 1][2]), gelu(acc[2 * kb + 1][3]));
+        // columns 16 kb .. +7 (an even 8-column block) and 16 kb + 8 .. +15
+        a2[kb][0] = pack2(gelu_t(acc[2 * kb][0]), gelu_t(acc[2 * kb][1]));
+        a2[kb][1] = pack2(gelu_t(acc[2 * kb][2]), gelu_t(acc[2 * kb][3]));
+        a2[kb][2] = pack2(gelu_p(acc[2 * kb + 1][0]), gelu_p(acc[2 * kb + 1][1]));
+        a2[kb][3] = pack2(gelu_p(acc[2 * kb + 1][2]), gelu_p(acc[2 * kb + 1][3]));
     }
     o[0] = o[2] = s.b3[2 * t];
     o[1] = o[3] = s.b3[2 * t + 1];

@@ -34,12 +34,15 @@
 // frees its tensor memory and returns.
 #include "inmsom_gpu.h"
 #include "closure.h"
+#include "gelu.cuh"
 
 #include <cuda_bf16.h>
 
 #include <cstdint>
 
 namespace {
+
+using namespace inmsom::closure;
 
 constexpr int KIN = 48, HID = 64, NOUT = 2, N3 = 8;
 constexpr int OFF_W1 = 0, OFF_B1 = OFF_W1 + KIN * HID, OFF_W2 = OFF_B1 + HID, OFF_B2 = OFF_W2 + HID * HID,
@@ -142,26 +145,6 @@ __device__ __forceinline__ void ld16(uint32_t taddr, float (&v)[16])
     wait_ld();
 #pragma unroll
     for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
-}
-
-// GELU in the tanh form (Hendrycks & Gimpel 2016) with the hardware tanh,
-// the definition of the other closure kernels
-constexpr float GC0 = 0.7978845608028654f, GC1 = 0.7978845608028654f * 0.044715f;
-__device__ __forceinline__ float tanh_hw(float x)
-{
-    float y;
-    asm("tanh.approx.f32 %0, %1;" : "=f"(y) : "f"(x));
-    return y;
-}
-__device__ __forceinline__ float gelu(float x)
-{
-    const float h = 0.5f * x;
-    return fmaf(h, tanh_hw(x * fmaf(GC1, x * x, GC0)), h);
-}
-__device__ __forceinline__ float gelu_d(float x)
-{
-    const float x2 = x * x, t = tanh_hw(x * fmaf(GC1, x2, GC0));
-    return fmaf(0.5f, 1.0f + t, 0.5f * x * (1.0f - t * t) * fmaf(3.0f * GC1, x2, GC0));
 }
 
 __device__ __forceinline__ uint32_t pack2(float lo, float hi)
@@ -306,7 +289,8 @@ __global__ void __launch_bounds__(THREADS, 1)
             float z[16];
             ld16(lane + C_Z1 + c0, z);
 #pragma unroll
-            for (int k = 0; k < 16; k++) z[k] = gelu(z[k] + s.b1[c0 + k]);
+            for (int k = 0; k < 16; k++)   // columns c0..c0+7: an even 8-column block
+                z[k] = k < 8 ? gelu_t(z[k] + s.b1[c0 + k]) : gelu_p(z[k] + s.b1[c0 + k]);
             st_chunk(s.a1, r, c0, AC, z);
             st_chunk(s.a1, r, c0 + 8, AC, z + 8);
         }
@@ -321,7 +305,8 @@ __global__ void __launch_bounds__(THREADS, 1)
             float z[16];
             ld16(lane + C_Z2 + c0, z);
 #pragma unroll
-            for (int k = 0; k < 16; k++) z[k] = gelu(z[k] + s.b2[c0 + k]);
+            for (int k = 0; k < 16; k++)
+                z[k] = k < 8 ? gelu_t(z[k] + s.b2[c0 + k]) : gelu_p(z[k] + s.b2[c0 + k]);
             st_chunk(s.a2, r, c0, AC, z);
             st_chunk(s.a2, r, c0 + 8, AC, z + 8);
         }
@@ -354,7 +339,8 @@ __global__ void __launch_bounds__(THREADS, 1)
             ld16(lane + C_DA2 + c0, da);
             ld16(lane + C_Z2 + c0, z);
 #pragma unroll
-            for (int k = 0; k < 16; k++) da[k] *= gelu_d(z[k] + s.b2[c0 + k]);
+            for (int k = 0; k < 16; k++)
+                da[k] *= k < 8 ? gelu_dt(z[k] + s.b2[c0 + k]) : gelu_dp(z[k] + s.b2[c0 + k]);
             st_chunk(s.dz2, r, c0, HID, da);
             st_chunk(s.dz2, r, c0 + 8, HID, da + 8);
         }
@@ -374,7 +360,8 @@ __global__ void __launch_bounds__(THREADS, 1)
             ld16(lane + C_DA1 + c0, da);
             ld16(lane + C_Z1 + c0, z);
 #pragma unroll
-            for (int k = 0; k < 16; k++) da[k] *= gelu_d(z[k] + s.b1[c0 + k]);
+            for (int k = 0; k < 16; k++)
+                da[k] *= k < 8 ? gelu_dt(z[k] + s.b1[c0 + k]) : gelu_dp(z[k] + s.b1[c0 + k]);
             st_chunk(s.dz1, r, c0, HID, da);
             st_chunk(s.dz1, r, c0 + 8, HID, da + 8);
         }
