@@ -258,13 +258,14 @@ def gpu_launches(steps: int, fp32_velocity: bool) -> int:
     one fused kernel per step and one k_advance per replayed graph (graphs
     of min(50, steps rounded down to even) steps); the forcing
     classification (k_minmax3) ran in the warm-up run and is kept, the
-    forcing being unchanged.  FP32 velocity storage adds three k_to_f32 and
-    one k_vel_from_f32 per run."""
+    forcing being unchanged.  FP32 velocity storage adds one k_to_f32 (the
+    state's velocities; the partner set and the forcing were converted in
+    the warm-up run) and one k_vel_from_f32 per run."""
     n = steps
     if steps >= 2:
         n += steps // min(50, steps & ~1)
     if fp32_velocity:
-        n += 4
+        n += 2
     return n
 
 
@@ -540,8 +541,40 @@ def run_study_general(args):
         ms = s.run_substeps(steps, w.dt) / steps
         out["williamson2_1.25x1.0"] = {"path": s.path()[1], "cells": w.cells, "ms_per_step": ms,
                                        "cell_steps_per_s": w.cells / (ms / 1e3)}
+    out["beta_plane_256"] = beta_plane_256(args)
     print(json.dumps({"study": "general", "workload": f"regional_basin {b.bounds.nx}x{b.bounds.ny} 1 km FP64",
                       "steps": steps, "results": out}), flush=True)
+
+
+def beta_plane_256(args):
+    """The 256 x 256 beta-plane basin (10 km, dt = 15 s: 20 s breaks the
+    gravity-wave limit there), 1000 steps: the fused path (L2-resident, so
+    bound by launches and the one wave of small work items, not HBM), its
+    largest normwise error against the oracle after the 1000 steps, and the
+    oracle's own rate on all host threads (barotropic_dynamics calls of 50
+    steps)."""
+    from oracle import oracle as ora
+    from inmsom_elfs_b200 import basins, solver
+    nsteps = 1000
+    b = basins.beta_plane_basin(n=256)
+    basins.finalize(b, ora.OracleBackend())
+    ora.hh_init_external(b)
+    bo, bg = b.copy(), b.copy()
+    with solver.BarotropicSolver(bg, resident=True) as s:
+        s.load_state()
+        path = s.path()[1]
+        s.run_substeps(max(args.warmup, 2), b.dt)
+        s.load_state()
+        ms = s.run_substeps(nsteps, b.dt) / nsteps
+        s.sync_to_host()
+    ora.run_substeps(bo, nsteps, b.dt)
+    err = max(float(np.abs(bg.state[k] - bo.state[k]).max() / max(np.abs(bo.state[k]).max(), 1e-300))
+              for k in ("ssh_e", "ubrtr_e", "vbrtr_e", "sshp_e", "ubrtrp_e", "vbrtrp_e"))
+    threads = os.cpu_count() or 1
+    cpu, calls, el = cpu_arm(basins.beta_plane_basin(n=256), 50, min(args.cpu_seconds, 10.0), threads)
+    return {"path": path, "cells": b.cells, "steps": nsteps, "dt": b.dt, "ms_per_step": ms,
+            "cell_steps_per_s": b.cells / (ms / 1e3), "rel_err_vs_oracle_1000": err,
+            "cpu_oracle": {"cell_steps_per_s": cpu, "cores": threads, "sample": f"{calls} calls of 50 steps"}}
 
 
 def run_study_fp32(args):

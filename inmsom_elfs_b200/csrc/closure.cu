@@ -188,11 +188,10 @@ __device__ __forceinline__ void mlp16(const S &s, const uint32_t a1[3][4], float
     uint32_t a2[4][4];
 #pragma unroll
     for (int kb = 0; kb < 4; kb++) {
-        // columns 16 kb .. +7 (an even 8-column block) and 16 kb + 8 .. +15
-        a2[kb][0] = pack2(gelu_t(acc[2 * kb][0]), gelu_t(acc[2 * kb][1]));
-        a2[kb][1] = pack2(gelu_t(acc[2 * kb][2]), gelu_t(acc[2 * kb][3]));
-        a2[kb][2] = pack2(gelu_p(acc[2 * kb + 1][0]), gelu_p(acc[2 * kb + 1][1]));
-        a2[kb][3] = pack2(gelu_p(acc[2 * kb + 1][2]), gelu_p(acc[2 * kb + 1][3]));
+        a2[kb][0] = pack2(gelu(acc[2 * kb][0]), gelu(acc[2 * kb][1]));
+        a2[kb][1] = pack2(gelu(acc[2 * kb][2]), gelu(acc[2 * kb][3]));
+        a2[kb][2] = pack2(gelu(acc[2 * kb + 1][0]), gelu(acc[2 * kb + 1][1]));
+        a2[kb][3] = pack2(gelu(acc[2 * kb + 1][2]), gelu(acc[2 * kb + 1][3]));
     }
 #pragma unroll
     for (int nt = 0; nt < 8; nt++) {
@@ -208,11 +207,10 @@ __device__ __forceinline__ void mlp16(const S &s, const uint32_t a1[3][4], float
         }
 #pragma unroll
     for (int kb = 0; kb < 4; kb++) {
-        // columns 16 kb .. +7 (an even 8-column block) and 16 kb + 8 .. +15
-        a2[kb][0] = pack2(gelu_t(acc[2 * kb][0]), gelu_t(acc[2 * kb][1]));
-        a2[kb][1] = pack2(gelu_t(acc[2 * kb][2]), gelu_t(acc[2 * kb][3]));
-        a2[kb][2] = pack2(gelu_p(acc[2 * kb + 1][0]), gelu_p(acc[2 * kb + 1][1]));
-        a2[kb][3] = pack2(gelu_p(acc[2 * kb + 1][2]), gelu_p(acc[2 * kb + 1][3]));
+        a2[kb][0] = pack2(gelu(acc[2 * kb][0]), gelu(acc[2 * kb][1]));
+        a2[kb][1] = pack2(gelu(acc[2 * kb][2]), gelu(acc[2 * kb][3]));
+        a2[kb][2] = pack2(gelu(acc[2 * kb + 1][0]), gelu(acc[2 * kb + 1][1]));
+        a2[kb][3] = pack2(gelu(acc[2 * kb + 1][2]), gelu(acc[2 * kb + 1][3]));
     }
     o[0] = o[2] = s.b3[2 * t];
     o[1] = o[3] = s.b3[2 * t + 1];

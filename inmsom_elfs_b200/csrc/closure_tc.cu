@@ -289,8 +289,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             float z[16];
             ld16(lane + C_Z1 + c0, z);
 #pragma unroll
-            for (int k = 0; k < 16; k++)   // columns c0..c0+7: an even 8-column block
-                z[k] = k < 8 ? gelu_t(z[k] + s.b1[c0 + k]) : gelu_p(z[k] + s.b1[c0 + k]);
+            for (int k = 0; k < 16; k++) z[k] = gelu(z[k] + s.b1[c0 + k]);
             st_chunk(s.a1, r, c0, AC, z);
             st_chunk(s.a1, r, c0 + 8, AC, z + 8);
         }
@@ -305,8 +304,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             float z[16];
             ld16(lane + C_Z2 + c0, z);
 #pragma unroll
-            for (int k = 0; k < 16; k++)
-                z[k] = k < 8 ? gelu_t(z[k] + s.b2[c0 + k]) : gelu_p(z[k] + s.b2[c0 + k]);
+            for (int k = 0; k < 16; k++) z[k] = gelu(z[k] + s.b2[c0 + k]);
             st_chunk(s.a2, r, c0, AC, z);
             st_chunk(s.a2, r, c0 + 8, AC, z + 8);
         }
@@ -340,7 +338,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             ld16(lane + C_Z2 + c0, z);
 #pragma unroll
             for (int k = 0; k < 16; k++)
-                da[k] *= k < 8 ? gelu_dt(z[k] + s.b2[c0 + k]) : gelu_dp(z[k] + s.b2[c0 + k]);
+                da[k] *= gelu_d(z[k] + s.b2[c0 + k]);
             st_chunk(s.dz2, r, c0, HID, da);
             st_chunk(s.dz2, r, c0 + 8, HID, da + 8);
         }
@@ -361,7 +359,7 @@ __global__ void __launch_bounds__(THREADS, 1)
             ld16(lane + C_Z1 + c0, z);
 #pragma unroll
             for (int k = 0; k < 16; k++)
-                da[k] *= k < 8 ? gelu_dt(z[k] + s.b1[c0 + k]) : gelu_dp(z[k] + s.b1[c0 + k]);
+                da[k] *= gelu_d(z[k] + s.b1[c0 + k]);
             st_chunk(s.dz1, r, c0, HID, da);
             st_chunk(s.dz1, r, c0 + 8, HID, da + 8);
         }

@@ -160,12 +160,12 @@ struct Layout {
 };
 
 // ring slots: rows j-2..j+1 in use plus one row in flight for the plain
-// substep (16 CTAs per SM fit), two in flight where the registers hold the
-// CTAs per SM to 12 (time-mean sums) or the slots are small (FP32 velocities)
+// substep (16 CTAs per SM fit, 20 with FP32 velocities), two in flight where
+// the registers hold the CTAs per SM to 12 (time-mean sums)
 template <bool GEN, int MODE, bool F32 = false>
 __host__ __device__ constexpr int ring_slots()
 {
-    return (MODE % 3 != 0 || F32) ? 6 : 5;
+    return (MODE % 3 != 0) ? 6 : 5;
 }
 template <bool GEN, int MODE, bool F32 = false>
 constexpr size_t ring_bytes()
@@ -174,11 +174,12 @@ constexpr size_t ring_bytes()
 }
 
 // resident CTAs per SM the register budget is cut for: 16 one-warp CTAs
-// (4 warps per SM sub-partition, 128 registers) for the plain substep, 12
-// where the time-mean sums need more registers, 11 for the general variant,
-// and never more than the shared memory holds (228 KB per SM, 1 KB of it
-// reserved per CTA): 16 for the FP64 uniform ring of 5 slots, 11 for the
-// general one.  (A 6-slot ring holds 13 uniform CTAs: 6 % slower on the
+// (4 warps per SM sub-partition, 128 registers) for the plain substep, 20
+// (5 warps per sub-partition, 96 registers) for its FP32-velocity form with
+// FP32 momentum arithmetic, 12 where the time-mean sums need more registers,
+// 11 for the general variant, and never more than the shared memory holds
+// (228 KB per SM, 1 KB of it reserved per CTA): 16 for the FP64 uniform ring
+// of 5 slots, 20 for the FP32 one, 11 for the general one.  (A 6-slot ring holds 13 uniform CTAs: 6 % slower on the
 // 2048 x 1536 basin; 128 bytes of alignment slack per CTA leave room for 15:
 // 2 % slower; reading the forcing from global memory instead of the ring
 // exposes the load latency: 5 % slower.)
@@ -186,7 +187,7 @@ template <bool GEN, int MODE, bool F32 = false>
 constexpr int min_ctas()
 {
     constexpr int by_smem = (int)(233472 / (ring_bytes<GEN, MODE, F32>() + 1024));
-    constexpr int want = GEN ? 11 : (MODE % 3 ? 12 : 16);
+    constexpr int want = GEN ? 11 : (MODE % 3 ? 12 : (F32 ? 20 : 16));
     return by_smem < want ? by_smem : want;
 }
 static_assert(NSET * SEG * 8 <= 1792, "state segment overlaps the static segment");
@@ -270,11 +271,13 @@ __device__ __forceinline__ void issue_row(unsigned char *slot, uint64_t *bar, co
 }
 
 __device__ __forceinline__ double sel(int m, double x) { return m ? x : 0.0; }
+__device__ __forceinline__ float sel(int m, float x) { return m ? x : 0.0f; }
 
 // 1 / (number of ocean T points) for the mask-weighted depth averages
-__device__ __forceinline__ double rcount(int n)
+template <class R>
+__device__ __forceinline__ R rcount(int n)
 {
-    return n == 4 ? 0.25 : (n == 3 ? 1.0 / 3.0 : (n == 2 ? 0.5 : (n == 1 ? 1.0 : 0.0)));
+    return n == 4 ? R(0.25) : (n == 3 ? R(1.0 / 3.0) : (n == 2 ? R(0.5) : (n == 1 ? R(1.0) : R(0.0))));
 }
 
 // 1/x by two Newton-Raphson steps r <- r + r*(1 - x*r) (quadratic
@@ -288,6 +291,8 @@ __device__ __forceinline__ double rcp_nr(double x)
     e = fma(-x, r, 1.0);
     return fma(r, e, r);
 }
+// the FP32 reciprocal, rounded to nearest
+__device__ __forceinline__ float rcp_nr(float x) { return __frcp_rn(x); }
 
 // state field F of the slot at byte offset o, at the lane's column + dk:
 // FP64, or FP32 velocities widened to FP64
@@ -303,9 +308,34 @@ __device__ __forceinline__ double ld_state(const unsigned char *lane, const unsi
         return *reinterpret_cast<const double *>(lane + o + (F * SEG + dk) * 8);
 }
 
+// a velocity field (u, up, v, vp) in the arithmetic type of the variant:
+// FP64, or the FP32 values as stored
+template <bool GEN, bool F32, int F>
+__device__ __forceinline__ std::conditional_t<F32, float, double> ld_vel(const unsigned char *lane,
+                                                                       const unsigned char *lane32, int o, int dk)
+{
+    using L = Layout<GEN, F32>;
+    static_assert(F < S_SSH, "velocity fields only");
+    if constexpr (F32)
+        return *reinterpret_cast<const float *>(lane32 + o + (F * L::VSEG + dk) * 4);
+    else
+        return *reinterpret_cast<const double *>(lane + o + (F * SEG + dk) * 8);
+}
+
+// a constant in the momentum arithmetic's type: the FP64 value, or its
+// FP32 copy
+template <bool F32>
+__device__ __forceinline__ std::conditional_t<F32, float, double> pick_real(double pv, float fv)
+{
+    if constexpr (F32)
+        return fv;
+    else
+        return pv;
+}
+
 // store a new state value; FP32 velocities are rounded to nearest
-template <bool F32, int F>
-__device__ __forceinline__ void st_state(float *const *vdst, double *const *dst, long long idx, double v)
+template <bool F32, int F, class T>
+__device__ __forceinline__ void st_state(float *const *vdst, double *const *dst, long long idx, T v)
 {
     if constexpr (F32 && F < S_SSH)
         vdst[F][idx] = (float)v;
@@ -316,27 +346,32 @@ __device__ __forceinline__ void st_state(float *const *vdst, double *const *dst,
 #define SHFL_UP(x) __shfl_up_sync(0xffffffffu, (x), 1)
 #define SHFL_DN(x) __shfl_down_sync(0xffffffffu, (x), 1)
 
+// R: the arithmetic type of the momentum terms (FP64, or FP32 in the
+// FP32-velocity variant); SSH levels and the continuity stay FP64
+template <class R>
 struct HQ {          // H + ssh of a row at columns k, k+1
-    double a, b;
+    R a, b;
 };
 // values of row j from stage 1, carried to the next iteration
+template <class R>
 struct S1 {
-    double U, Ul, V, Vr;     // U = u*hu at k, k-1; V = v*hv at k, k+1
-    double Ru;               // u equation of row j: forcing + pressure gradient - drag
-    double Rv;               // v equation of row j: forcing + pressure gradient - drag
-    double cor;              // uniform variant: Coriolis factor of row j
-    double slx, sly;         // pressure-gradient terms (time means only)
-    HQ hq;                   // H + ssh of row j+1
+    R U, Ul, V, Vr;          // U = u*hu at k, k-1; V = v*hv at k, k+1
+    R Ru;                    // u equation of row j: forcing + pressure gradient - drag
+    R Rv;                    // v equation of row j: forcing + pressure gradient - drag
+    R cor;                   // uniform variant: Coriolis factor of row j
+    R slx, sly;              // pressure-gradient terms (time means only)
+    HQ<R> hq;                // H + ssh of row j+1
 };
 // values of row j-1 from stage 2 (and of stage 1 routed on), carried on
+template <class R>
 struct S2 {
     double sn;               // new SSH of the row
-    double V, Uo;            // V and U of the row
-    double vs;               // v(k) + v(k+1) of the row
-    double Cu;               // the row's part of the u equation of the row above
-    double Pv;               // the row's part of its own v equation, less the GX flux
-    double sly;              // pressure-gradient term of the row (time means only)
-    HQ hqm;                  // H + ssh of row j
+    R V, Uo;                 // V and U of the row
+    R vs;                    // v(k) + v(k+1) of the row
+    R Cu;                    // the row's part of the u equation of the row above
+    R Pv;                    // the row's part of its own v equation, less the GX flux
+    R sly;                   // pressure-gradient term of the row (time means only)
+    HQ<R> hqm;               // H + ssh of row j
     double au0, au2;         // time-mean sums (u, pgrx) of row j, for the next iteration's stage 3u
     double av1, av3;         // time-mean sums (v, pgry) of row j-1, for its stage 3v
 };
@@ -373,6 +408,7 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
 
     // field f of the state / static segment of the slot at byte offset o
 #define AS(o, f, dk) ld_state<GEN, F32, (f)>(lane, lane32, (o), (dk))
+#define AV(o, f, dk) ld_vel<GEN, F32, (f)>(lane, lane32, (o), (dk))
 #define AT(o, f, dk) (*reinterpret_cast<const double *>(lane + (o) + L::STAT_OFF + ((f) * SEG + (dk)) * 8))
 #define CF(o, x) (reinterpret_cast<const RowCoef *>(ring + (o) + L::COEF_OFF)->x)
 
@@ -396,6 +432,13 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
 
     const bool out = l >= 1 && l <= NL - 2 && k >= p.c_first && k <= p.c_last;
     const double gam = p.gam, two_ti = p.two_ti;
+    // the momentum arithmetic's type, and FP32 copies of the uniform
+    // variant's constants for it (the FP64 kernel reads the parameters)
+    using R = std::conditional_t<F32, float, double>;
+    const float f_gam = (float)p.gam, f_rs = (float)rs, f_d4 = (float)p.d4, f_d = (float)p.d,
+                f_inv_d = (float)p.inv_d, f_gd = (float)p.gd, f_tt = (float)p.tt, f_d2 = (float)p.d2,
+                f_rd0 = (float)p.rd0, f_mu0 = (float)p.mu0;
+#define RK(pv, fv) pick_real<F32>((pv), (fv))
 
     // slots of rows j-2, j-1, j, j+1 and the fill parity of row j+1
     int i_m2 = RING - 1, i_m1 = 0, i_0 = 1, i_p1 = 2;
@@ -408,20 +451,20 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
     ok = __all_sync(0xffffffffu, ok && mbar_wait(&mbar[1], 0, p.wait_limit));
     if (ok) waited = row_lo + 1;
 
-    S1 A{}, B{};
-    S2 X{}, Y{};
+    S1<R> A{}, B{};
+    S2<R> X{}, Y{};
     if (ok) {
         mk = (mask2(0) << 2) | mask2(L::SLOT_B);
         // H + ssh of row r0-1, the "current" row of the first iteration
-        B.hq.a = AT(L::SLOT_B, T_H, 0) + AS(L::SLOT_B, S_SSH, 0);
-        B.hq.b = AT(L::SLOT_B, T_H, 1) + AS(L::SLOT_B, S_SSH, 1);
+        B.hq.a = (R)(AT(L::SLOT_B, T_H, 0) + AS(L::SLOT_B, S_SSH, 0));
+        B.hq.b = (R)(AT(L::SLOT_B, T_H, 1) + AS(L::SLOT_B, S_SSH, 1));
     }
     long long gi = (long long)(r0 - 1) * p.pitch + k;   // element (row j, column k)
 
     // One iteration of the row loop; the flags say which stages are valid
     // for row j (the first three and the last iteration lack some).
-    auto step = [&](const int j, auto on1, auto on2, auto on3u, auto on3v, S1 &n, const S1 &c, S2 &q,
-                    const S2 &qc) {
+    auto step = [&](const int j, auto on1, auto on2, auto on3u, auto on3v, S1<R> &n, const S1<R> &c, S2<R> &q,
+                    const S2<R> &qc) {
         constexpr bool D1 = decltype(on1)::value, D2 = decltype(on2)::value;
         constexpr bool D3U = decltype(on3u)::value, D3V = decltype(on3v)::value;
         if (!ok) return;
@@ -453,25 +496,25 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
         // ---------------- stage 1: row j (independent of stage 2) -------
         if constexpr (D1) {
             const uint32_t mj = (mk >> 2) & 3u, mn = mk & 3u;
-            n.hq.a = AT(o_p1, T_H, 0) + AS(o_p1, S_SSH, 0);
-            n.hq.b = AT(o_p1, T_H, 1) + AS(o_p1, S_SSH, 1);
+            n.hq.a = (R)(AT(o_p1, T_H, 0) + AS(o_p1, S_SSH, 0));
+            n.hq.b = (R)(AT(o_p1, T_H, 1) + AS(o_p1, S_SSH, 1));
             const int a = mj & 1, b = (mj >> 1) & 1, cc = mn & 1;
             // Function/depth.f90:127-139 mask-weighted averages to u and v points
-            double hu, hv;
+            R hu, hv;
             if constexpr (GEN) {
                 hu = (sel(a, c.hq.a) + sel(b, c.hq.b)) * (a & b ? CF(o_0, ku2) : (a | b ? CF(o_0, ku) : 0.0));
                 hv = (sel(a, c.hq.a * CF(o_0, wv0)) + sel(cc, n.hq.a * CF(o_0, wv1))) *
                      (a & cc ? 0.5 : (a | cc ? 1.0 : 0.0));
             } else {
-                hu = (sel(a, c.hq.a) + sel(b, c.hq.b)) * (a & b ? 0.5 : (a | b ? 1.0 : 0.0));
-                hv = (sel(a, c.hq.a) + sel(cc, n.hq.a)) * (a & cc ? 0.5 : (a | cc ? 1.0 : 0.0));
+                hu = (sel(a, c.hq.a) + sel(b, c.hq.b)) * (a & b ? R(0.5) : (a | b ? R(1.0) : R(0.0)));
+                hv = (sel(a, c.hq.a) + sel(cc, n.hq.a)) * (a & cc ? R(0.5) : (a | cc ? R(1.0) : R(0.0)));
             }
-            n.U = AS(o_0, S_U, 0) * hu;
-            n.V = AS(o_0, S_V, 0) * hv;
+            n.U = AV(o_0, S_U, 0) * hu;
+            n.V = AV(o_0, S_V, 0) * hv;
             // vel_ssh.f90:536-545, :554-565: forcing, pressure gradient of
             // the current level and Rayleigh drag of the previous level
             const double e0 = AS(o_0, S_SSH, 0), e1 = AS(o_0, S_SSH, 1), e1v = AS(o_p1, S_SSH, 0);
-            double slx, sly, rdu, rdv, au, av;
+            R slx, sly, rdu, rdv, au, av;
             if constexpr (GEN) {
                 slx = -(e1 - e0) * CF(o_0, gdyh) * hu;
                 sly = -(e1v - e0) * CF(o_0, gdxh) * hv;
@@ -480,19 +523,18 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
                 au = CF(o_0, au);
                 av = CF(o_0, av);
             } else {
-                slx = -(e1 - e0) * p.gd * hu;
-                sly = -(e1v - e0) * p.gd * hv;
-                rdu = rdv = p.rd0;
-                au = av = p.d2;
-                n.cor = p.cor[j];
+                slx = -(R)(e1 - e0) * RK(p.gd, f_gd) * hu;
+                sly = -(R)(e1v - e0) * RK(p.gd, f_gd) * hv;
+                rdu = rdv = RK(p.rd0, f_rd0);
+                au = av = RK(p.d2, f_d2);
+                n.cor = (R)p.cor[j];
             }
             // RHS: from the ring (FP64 state) or from the FP32 copy
-            const double rx = F32 ? (double)*reinterpret_cast<const float *>(lane32 + o_0 + L::RHS_OFF)
-                                  : AT(o_0, T_RX, 0);
-            const double ry = F32 ? (double)*reinterpret_cast<const float *>(lane32 + o_0 + L::RHS_OFF + L::VSEG * 4)
-                                  : AT(o_0, T_RY, 0);
-            n.Ru = rx * rs + slx - rdu * AS(o_0, S_UP, 0) * au * hu;
-            n.Rv = ry * rs + sly - rdv * AS(o_0, S_VP, 0) * av * hv;
+            const R rx = F32 ? (R)*reinterpret_cast<const float *>(lane32 + o_0 + L::RHS_OFF) : (R)AT(o_0, T_RX, 0);
+            const R ry = F32 ? (R)*reinterpret_cast<const float *>(lane32 + o_0 + L::RHS_OFF + L::VSEG * 4)
+                             : (R)AT(o_0, T_RY, 0);
+            n.Ru = rx * RK(rs, f_rs) + slx - rdu * AV(o_0, S_UP, 0) * au * hu;
+            n.Rv = ry * RK(rs, f_rs) + sly - rdv * AV(o_0, S_VP, 0) * av * hv;
             if (ACC) {
                 n.slx = slx;
                 n.sly = sly;
@@ -502,40 +544,43 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
         // forcing of the rows that stage 3 updates, loaded early
 
         // ---------------- stage 2: row rho = j-1 -------------------------
-        double FX, FY, GY, ST, SS, QU, QV, sn, vs, u_r, up_r, v_m, vp_m;
+        double sn;
+        R FX, FY, GY, ST, SS, QU, QV, vs, u_r, up_r, v_m, vp_m;
         if constexpr (D2) {
             const uint32_t mr = (mk >> 4) & 3u, mu_ = (mk >> 2) & 3u;   // rows rho, rho+1
             const int lc = mr & 1, lr = (mr >> 1) & 1, lu = mu_ & 1, lur = (mu_ >> 1) & 1;
             const int luu = lc & lr & lu & lur;
-            u_r = AS(o_m1, S_U, 0);
-            up_r = AS(o_m1, S_UP, 0);
-            v_m = AS(o_m2, S_V, 0);
-            vp_m = AS(o_m2, S_VP, 0);
-            const double u_l = AS(o_m1, S_U, -1), u_u = AS(o_0, S_U, 0);
-            const double v_r = AS(o_m1, S_V, 0), v_rr = AS(o_m1, S_V, 1);
-            const double up_l = AS(o_m1, S_UP, -1), up_u = AS(o_0, S_UP, 0);
-            const double vp_r = AS(o_m1, S_VP, 0), vp_rr = AS(o_m1, S_VP, 1);
-            double mu_t = p.mu0, mu_h = p.mu0, wq = p.wq0;
+            u_r = AV(o_m1, S_U, 0);
+            up_r = AV(o_m1, S_UP, 0);
+            v_m = AV(o_m2, S_V, 0);
+            vp_m = AV(o_m2, S_VP, 0);
+            const R u_l = AV(o_m1, S_U, -1), u_u = AV(o_0, S_U, 0);
+            const R v_r = AV(o_m1, S_V, 0), v_rr = AV(o_m1, S_V, 1);
+            const R up_l = AV(o_m1, S_UP, -1), up_u = AV(o_0, S_UP, 0);
+            const R vp_r = AV(o_m1, S_VP, 0), vp_rr = AV(o_m1, S_VP, 1);
+            R mu_t = RK(p.mu0, f_mu0), mu_h = RK(p.mu0, f_mu0);
+            double wq = p.wq0;
             if constexpr (GEN) {
                 mu_t = AT(o_m1, T_MU, 0);
                 mu_h = (mu_t + AT(o_m1, T_MU, 1) + AT(o_0, T_MU, 0) + AT(o_0, T_MU, 1)) * 0.25;
                 wq = AT(o_m1, T_WF, 0) * p.inv_rho;
             }
-            // vel_ssh.f90:491-494 continuity over 2*tau_inner
+            // vel_ssh.f90:491-494 continuity over 2*tau_inner, in FP64 (the
+            // FP32 transports widened: their differences are exact)
             const double div = GEN ? (c.U - c.Ul) * CF(o_m1, c_u) + c.V * CF(o_m1, c_v0) - qc.V * CF(o_m1, c_v1)
-                                   : ((c.U - c.Ul) + (c.V - qc.V)) * p.inv_d;
+                                   : (((double)c.U - (double)c.Ul) + ((double)c.V - (double)qc.V)) * p.inv_d;
             sn = sel(lc, AS(o_m1, S_SSHP, 0) + two_ti * (wq - div));
             // vel_ssh.f90:63-73, :88-98 advective fluxes on T and h faces
             vs = v_r + v_rr;
-            FX = (c.Ul + c.U) * (u_l + u_r) * (GEN ? CF(o_m1, fx) : p.d4);
-            FY = sel(luu, (c.V + c.Vr) * (u_r + u_u) * (GEN ? CF(o_m1, fy) : p.d4));
-            GY = (GEN ? qc.V * CF(o_m1, gy0) + c.V * CF(o_m1, gy1) : (qc.V + c.V) * p.d4) * (v_m + v_r);
+            FX = (c.Ul + c.U) * (u_l + u_r) * (GEN ? (R)CF(o_m1, fx) : RK(p.d4, f_d4));
+            FY = sel(luu, (c.V + c.Vr) * (u_r + u_u) * (GEN ? (R)CF(o_m1, fy) : RK(p.d4, f_d4)));
+            GY = (GEN ? (R)(qc.V * CF(o_m1, gy0) + c.V * CF(o_m1, gy1)) : (qc.V + c.V) * RK(p.d4, f_d4)) * (v_m + v_r);
             // depth.f90:141-147 depth on the h point
-            const double sa = sel(lc, qc.hqm.a) + sel(lr, qc.hqm.b);
-            const double sb = sel(lu, c.hq.a) + sel(lur, c.hq.b);
-            const double hh = (GEN ? sa * CF(o_m1, wh0) + sb * CF(o_m1, wh1) : sa + sb) * rcount(lc + lr + lu + lur);
+            const R sa = sel(lc, qc.hqm.a) + sel(lr, qc.hqm.b);
+            const R sb = sel(lu, c.hq.a) + sel(lur, c.hq.b);
+            const R hh = (GEN ? (R)(sa * CF(o_m1, wh0) + sb * CF(o_m1, wh1)) : sa + sb) * rcount<R>(lc + lr + lu + lur);
             // vel_ssh.f90:35-37 metric vorticity (zero on uniform grids) + Coriolis
-            double cor;
+            R cor;
             if constexpr (GEN) {
                 cor = CF(o_m1, cor);
                 if (!p.vort_zero)
@@ -543,18 +588,19 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
             } else {
                 cor = c.cor;
             }
-            const double Wh = hh * cor;
+            const R Wh = hh * cor;
             QU = Wh * vs;
             QV = Wh * (u_r + u_u);
             // mixing.f90:134-148 stresses from the previous level
-            const double str_t = GEN ? sel(lc, CF(o_m1, t1) * (up_r - up_l) - (CF(o_m1, t2) * vp_r - CF(o_m1, t3) * vp_m))
-                                     : sel(lc, ((up_r - up_l) - (vp_r - vp_m)) * p.inv_d);
-            const double str_s = GEN ? sel(luu, CF(o_m1, s1) * up_u - CF(o_m1, s2) * up_r + CF(o_m1, s3) * (vp_rr - vp_r))
-                                     : sel(luu, ((up_u - up_r) + (vp_rr - vp_r)) * p.inv_d);
+            const R str_t = GEN ? (R)sel(lc, CF(o_m1, t1) * (up_r - up_l) - (CF(o_m1, t2) * vp_r - CF(o_m1, t3) * vp_m))
+                                : sel(lc, ((up_r - up_l) - (vp_r - vp_m)) * RK(p.inv_d, f_inv_d));
+            const R str_s = GEN ? (R)sel(luu, CF(o_m1, s1) * up_u - CF(o_m1, s2) * up_r + CF(o_m1, s3) * (vp_rr - vp_r))
+                                : sel(luu, ((up_u - up_r) + (vp_rr - vp_r)) * RK(p.inv_d, f_inv_d));
             ST = mu_t * qc.hqm.a * str_t;
             SS = mu_h * hh * str_s;
         }
-        double FXr, STr, SNr, QVl, SSl;
+        R FXr, STr, QVl, SSl;
+        double SNr;
         if constexpr (D2) {
             FXr = SHFL_DN(FX);
             STr = SHFL_DN(ST);
@@ -583,12 +629,12 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
                 const double sp0 = AS(o_m1, S_SSHP, 0), sp1 = AS(o_m1, S_SSHP, 1);
                 const double h0 = AT(o_m1, T_H, 0), h1 = AT(o_m1, T_H, 1);
                 // vel_ssh.f90:536-551
-                const double ku2 = GEN ? CF(o_m1, ku2) : 0.5;
-                const double hup = ((h0 + sp0) + (h1 + sp1)) * ku2;
-                const double hun = ((h0 + sn) + (h1 + SNr)) * ku2;
-                const double difx = GEN ? (STr - ST) * CF(o_m1, dux) + SS * CF(o_m1, dus0) : ((STr - ST) + SS) * p.d;
-                const double grx = c.Ru + qc.Cu - ((FXr - FX) + FY) + difx + QU * 0.25;
-                const double un = (up_r * hup + grx * (GEN ? two_ti * CF(o_m1, rau) : p.tt)) * rcp_nr(hun);
+                const R ku2 = GEN ? (R)CF(o_m1, ku2) : R(0.5);
+                const R hup = (R)((h0 + sp0) + (h1 + sp1)) * ku2;
+                const R hun = (R)((h0 + sn) + (h1 + SNr)) * ku2;
+                const R difx = GEN ? (R)((STr - ST) * CF(o_m1, dux) + SS * CF(o_m1, dus0)) : ((STr - ST) + SS) * RK(p.d, f_d);
+                const R grx = c.Ru + qc.Cu - ((FXr - FX) + FY) + difx + QU * R(0.25);
+                const R un = (up_r * hup + grx * (GEN ? (R)(two_ti * CF(o_m1, rau)) : RK(p.tt, f_tt))) * rcp_nr(hun);
                 const long long idx = gi - p.pitch;
                 if (ACC && wu) {
                     const double slxn = -(SNr - sn) * (GEN ? CF(o_m1, gdyh) : p.gd) * hun;
@@ -598,7 +644,7 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
                     p.acc[2][idx] = b;
                 }
                 if (WRITE && wu) {
-                    st_state<F32, S_UP>(p.vdst, dst, idx, u_r + gam * (un - 2.0 * u_r + up_r));
+                    st_state<F32, S_UP>(p.vdst, dst, idx, u_r + RK(gam, f_gam) * (un - R(2.0) * u_r + up_r));
                     st_state<F32, S_U>(p.vdst, dst, idx, un);
                 }
                 if (WRITE && wt) {   // vel_ssh.f90:593-596
@@ -612,26 +658,26 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
         if constexpr (D3V) {
             // vel_ssh.f90:88-98 the x flux of v on the h point of row R,
             // from the transports of rows R and R+1
-            const double GX = (GEN ? qc.Uo * CF(o_m2, gx0) + c.U * CF(o_m2, gx1) : (qc.Uo + c.U) * p.d4) * qc.vs;
-            const double GXl = SHFL_UP(GX);
+            const R GX = (GEN ? (R)(qc.Uo * CF(o_m2, gx0) + c.U * CF(o_m2, gx1)) : (qc.Uo + c.U) * RK(p.d4, f_d4)) * qc.vs;
+            const R GXl = SHFL_UP(GX);
             const uint32_t mR = (mk >> 6) & 3u, mU = (mk >> 4) & 3u;   // rows R, R+1
             if (__any_sync(0xffffffffu, out && (mR & mU & 1u))) {
                 const bool wv = out && (mR & mU & 1u);
                 const double sp0 = AS(o_m2, S_SSHP, 0), sp1 = AS(o_m1, S_SSHP, 0);
                 const double h0 = AT(o_m2, T_H, 0), h1 = AT(o_m1, T_H, 0);
-                const double v0 = v_m, vp0 = vp_m;
+                const R v0 = v_m, vp0 = vp_m;
                 const double sn0 = qc.sn, sn1 = sn;
                 // vel_ssh.f90:554-569
-                double hvp, hvn;
+                R hvp, hvn;
                 if constexpr (GEN) {
                     hvp = ((h0 + sp0) * CF(o_m2, wv0) + (h1 + sp1) * CF(o_m2, wv1)) * 0.5;
                     hvn = ((h0 + sn0) * CF(o_m2, wv0) + (h1 + sn1) * CF(o_m2, wv1)) * 0.5;
                 } else {
-                    hvp = ((h0 + sp0) + (h1 + sp1)) * 0.5;
-                    hvn = ((h0 + sn0) + (h1 + sn1)) * 0.5;
+                    hvp = (R)((h0 + sp0) + (h1 + sp1)) * R(0.5);
+                    hvn = (R)((h0 + sn0) + (h1 + sn1)) * R(0.5);
                 }
-                const double gry = qc.Pv - (GX - GXl) - GY - ST * (GEN ? CF(o_m2, dvt1) : p.d);
-                const double vn = (vp0 * hvp + gry * (GEN ? two_ti * CF(o_m2, rav) : p.tt)) * rcp_nr(hvn);
+                const R gry = qc.Pv - (GX - GXl) - GY - ST * (GEN ? (R)CF(o_m2, dvt1) : RK(p.d, f_d));
+                const R vn = (vp0 * hvp + gry * (GEN ? (R)(two_ti * CF(o_m2, rav)) : RK(p.tt, f_tt))) * rcp_nr(hvn);
                 const long long idx = gi - 2 * p.pitch;
                 if (ACC && wv) {
                     const double slyn = -(sn1 - sn0) * (GEN ? CF(o_m2, gdxh) : p.gd) * hvn;
@@ -641,7 +687,7 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
                     p.acc[3][idx] = b;
                 }
                 if (WRITE && wv) {
-                    st_state<F32, S_VP>(p.vdst, dst, idx, v0 + gam * (vn - 2.0 * v0 + vp0));
+                    st_state<F32, S_VP>(p.vdst, dst, idx, v0 + RK(gam, f_gam) * (vn - R(2.0) * v0 + vp0));
                     st_state<F32, S_V>(p.vdst, dst, idx, vn);
                 }
             }
@@ -651,12 +697,12 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
         if constexpr (D2) {
             // its part of the u equation of row rho+1 (vel_ssh.f90:539-541):
             // +FY(rho), -SS(rho)*dxb(rho)^2/dxt(rho+1), +QU(rho)/4
-            q.Cu = FY + QU * 0.25 - SS * (GEN ? CF(o_0, dus1) : p.d);
+            q.Cu = FY + QU * R(0.25) - SS * (GEN ? (R)CF(o_0, dus1) : RK(p.d, f_d));
             // its part of its own v equation (vel_ssh.f90:557-560); the
             // next iteration adds -(GX - GX(k-1)), -GY(rho+1) and
             // -ST(rho+1)*dx(rho+1)^2/dxh(rho)
-            const double dify = GEN ? ST * CF(o_m1, dvt0) + (SS - SSl) * CF(o_m1, dvs) : (ST + (SS - SSl)) * p.d;
-            q.Pv = c.Rv + GY + dify - (QV + QVl) * 0.25;
+            const R dify = GEN ? (R)(ST * CF(o_m1, dvt0) + (SS - SSl) * CF(o_m1, dvs)) : (ST + (SS - SSl)) * RK(p.d, f_d);
+            q.Pv = c.Rv + GY + dify - (QV + QVl) * R(0.25);
             q.sn = sn;
             q.vs = vs;
         }
@@ -715,6 +761,8 @@ __device__ __forceinline__ bool substep_item(const Params &p, const CUtensorMap 
     __syncwarp();
     return true;
 #undef AS
+#undef AV
+#undef RK
 #undef AT
 #undef CF
 }
@@ -768,10 +816,19 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *a)
     return v;
 }
 
-constexpr int ENS_CTAS = 11;   // resident CTAs per SM the kernel is cut for (the general variant's)
+// resident CTAs per SM the kernel is cut for: the general variant's where
+// some member takes it, else 12 (the uniform plain substep's 16 leave the
+// claim loop 128 registers and spill; 12 ran 24 % faster than 16 and 10 %
+// faster than 11 on 64 regional basins)
+template <bool ANYGEN>
+constexpr int ens_ctas()
+{
+    return ANYGEN ? min_ctas<true, 3>() : 12;
+}
 constexpr unsigned ENS_WAIT_POLLS = 1u << 16;
 
-__global__ void __launch_bounds__(NL, ENS_CTAS)
+template <bool ANYGEN>
+__global__ void __launch_bounds__(NL, ens_ctas<ANYGEN>())
     k_ens_persistent(const EnsItem *__restrict__ mem, const int *__restrict__ moff, int nmem, int total,
                      int group, unsigned *ctr, unsigned *done)
 {
@@ -817,7 +874,7 @@ __global__ void __launch_bounds__(NL, ENS_CTAS)
         }
         const double rs = q.rs_dev[*q.rs_base + st];
         const int4 item = em.items[j - moff[m]];
-        if (em.gen) {
+        if (ANYGEN && em.gen) {
             uint64_t *mbar = reinterpret_cast<uint64_t *>(ring + ring_slots<true, 3>() * Layout<true>::SLOT_B);
             (void)substep_item<true, 3>(q, &q.tm_src, q.dst, rs, item, ring, mbar);
         } else {
@@ -927,6 +984,7 @@ int forcing_mode(Plan &p, const Dom &d, const Consts &c, double *forc[6], cudaSt
 // copy the forcing fields the variant reads into the static block
 int stage_forcing(Plan &p, double *forc[6], int gen, cudaStream_t s)
 {
+    p.f32_rhs_key = 0;   // the FP32 copy of RHSx, RHSy is stale
     const size_t fb = (size_t)p.fstride * sizeof(double);
     const int src_of[NSTAT] = {-1, 0, 1, 3, 5, 2};   // T_* <- forc index (RHSx RHSy wflux mu mu4 rdis)
     for (int t = 1; t < NSTAT; t++)
@@ -1042,6 +1100,7 @@ int sync_buffers(Plan &p, double *state[6], cudaStream_t s)
     for (int b = 0; b < 2; b++)
         if (cudaMemcpyAsync(p.buf[b][0], state[0], bytes, cudaMemcpyDeviceToDevice, s) != cudaSuccess) return 1;
     p.buffers_synced = true;
+    for (bool &f : p.f32_land) f = false;
     return 0;
 }
 
@@ -1244,6 +1303,8 @@ EncodeTiled encoder()
 int ensure_f32(Plan &p, const Dom &d, cudaStream_t s)
 {
     if (p.vset[0]) return 0;
+    for (bool &f : p.f32_land) f = false;
+    p.f32_rhs_key = 0;
     EncodeTiled enc = encoder();
     if (!enc) return 1;
     const size_t fb = (size_t)p.fstride * sizeof(float);
@@ -1602,9 +1663,20 @@ int prepare_steps_f32(Plan &p, const Dom &d, const Consts &c, double *state[6], 
     const int blocks = 4 * p.nsm;
     const int a = set_index(p, state[0]), b = set_index(p, p.buf[0][0]);
     if (a < 0 || b < 0) return 1;
+    // the state's velocities every run (the FP64 state may have changed);
+    // the partner set's only for the values at the points the kernel does
+    // not write, once after they were synchronised; RHSx, RHSy once per
+    // staging of the forcing
     k_to_f32<<<blocks, 256, 0, s>>>(p.set[a], p.vset[a], 4 * p.fstride);
-    k_to_f32<<<blocks, 256, 0, s>>>(p.set[b], p.vset[b], 4 * p.fstride);
-    k_to_f32<<<blocks, 256, 0, s>>>(p.stat + T_RX * p.fstride, p.stat32, 2 * p.fstride);
+    p.f32_land[a] = true;
+    if (!p.f32_land[b]) {
+        k_to_f32<<<blocks, 256, 0, s>>>(p.set[b], p.vset[b], 4 * p.fstride);
+        p.f32_land[b] = true;
+    }
+    if (key == 0 || p.f32_rhs_key != key) {
+        k_to_f32<<<blocks, 256, 0, s>>>(p.stat + T_RX * p.fstride, p.stat32, 2 * p.fstride);
+        p.f32_rhs_key = key;
+    }
     return cudaGetLastError() != cudaSuccess;
 }
 
@@ -1790,13 +1862,16 @@ int ens_table(const std::vector<EnsMemberIn> &mem, int group, const double *rs_d
         off[i] = total;
         total += p.nitems[gen];
     }
-    const size_t smem = ring_bytes<true, 3>();
-    if (cudaFuncSetAttribute(k_ens_persistent, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+    bool anygen = false;
+    for (const EnsItem &e : h) anygen = anygen || e.gen;
+    const size_t smem = anygen ? ring_bytes<true, 3>() : ring_bytes<false, 3>();
+    const void *kern = anygen ? (const void *)k_ens_persistent<true> : (const void *)k_ens_persistent<false>;
+    if (cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
         return 1;
     int occ = 0, dev = 0, nsm = 148;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, dev);
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, k_ens_persistent, NL, smem) != cudaSuccess || occ < 1)
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ, kern, NL, smem) != cudaSuccess || occ < 1)
         return 1;
     EnsItem *dm = nullptr;
     if (cudaMalloc(&dm, h.size() * sizeof(EnsItem)) != cudaSuccess) return 1;
@@ -1813,6 +1888,7 @@ int ens_table(const std::vector<EnsMemberIn> &mem, int group, const double *rs_d
     t.total = total;
     t.group = group;
     t.grid = occ * nsm;
+    t.anygen = anygen;
     t.smem = smem;
     return 0;
 }
@@ -1833,8 +1909,9 @@ int ens_launch(const EnsTable &t, cudaStream_t s)
     at[0].val.cooperative = 1;
     cfg.attrs = at;
     cfg.numAttrs = 1;
-    return cudaLaunchKernelEx(&cfg, k_ens_persistent, (const EnsItem *)t.d_mem, (const int *)t.d_moff, t.nmem,
-                              t.total, t.group, t.d_ctr, t.d_done) != cudaSuccess;
+    return cudaLaunchKernelEx(&cfg, t.anygen ? k_ens_persistent<true> : k_ens_persistent<false>,
+                              (const EnsItem *)t.d_mem, (const int *)t.d_moff, t.nmem, t.total, t.group, t.d_ctr,
+                              t.d_done) != cudaSuccess;
 }
 
 void ens_free(EnsTable &t)

@@ -121,6 +121,8 @@ struct Plan {
     CUtensorMap tm_ssh[3];          // box {36, 1, 2} over the SSH fields of each state set
     CUtensorMap tm_stat_f32;        // box {36, 1, 1}: H alone, for the FP32-velocity ring
     CUtensorMap tm_rhs32;           // box {40, 1, 2} FP32 over stat32: RHSx, RHSy
+    bool f32_land[3] = {false, false, false};   // vset[b] holds set b's values where the kernel does not write
+    unsigned f32_rhs_key = 0;       // forcing key stat32 was converted for (0: stale)
     int stat_box[2] = {0, 0};       // static fields in tm_stat[v], checked against the ring layout
     int stat_box_f32 = 0;
     double *d_uniform = nullptr;    // per-block min/max of mu, rdis, wflux
@@ -226,6 +228,7 @@ struct EnsTable {
     int *d_moff = nullptr;
     unsigned *d_ctr = nullptr, *d_done = nullptr;
     int nmem = 0, total = 0, group = 0, grid = 0;
+    bool anygen = false;   // some member takes the general variant (fewer CTAs per SM)
     size_t smem = 0;
 };
 int ens_table(const std::vector<EnsMemberIn> &mem, int group, const double *rs_dev, const int *rs_base, EnsTable &t,

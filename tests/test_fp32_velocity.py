@@ -1,13 +1,16 @@
 """FP32 velocity storage (INMSOM_FP32_VELOCITY) for inmsom_run_substeps.
 
-u, up, v, vp live in FP32 on the device during a run; every operation and
-SSH stay FP64.  Tolerances against the FP64 fused run and against the FP64
-CPU oracle (normwise relative, max|a-b|/max|b|), written here:
+u, up, v, vp live in FP32 on the device during a run and the momentum
+arithmetic is FP32; SSH, its time levels and the continuity stay FP64.
+Tolerances against the FP64 fused run and against the FP64 CPU oracle
+(normwise relative, max|a-b|/max|b|), written here:
   * after 300 substeps of the 400 x 300 regional basin: SSH <= 1e-6,
-    u and v (both levels) <= 2e-6 (measured on a B200: 3.4e-7 and 4.4e-7);
+    u and v (both levels) <= 2e-6;
   * the closed-basin volume is conserved to 1e-13 relative, as in FP64:
-    the continuity fluxes are FP64 products shared by both cells of a face;
-  * land and halo points of the FP64 state are never written.
+    the continuity differences the FP32 transports in FP64 (exactly), so
+    each face's flux leaves one cell and enters the other;
+  * land and halo points of the FP64 state are never written;
+  * runs split by a change of the forcing continue as one run does.
 """
 import numpy as np
 import pytest
@@ -65,6 +68,33 @@ def test_fp32_velocity_against_the_fp64_oracle(gpu, ora):
     errs = {k: rel_err(b32.state[k], bo.state[k]) for k in bo.state}
     rms = {k: float(np.sqrt(np.mean((b32.state[k] - bo.state[k])[ocean] ** 2))) for k in bo.state}
     print("fp32 velocity vs FP64 oracle: normwise", errs, "rms", rms)
+    assert errs["ssh_e"] <= TOL_SSH and errs["sshp_e"] <= TOL_SSH, errs
+    for k in ("ubrtr_e", "ubrtrp_e", "vbrtr_e", "vbrtrp_e"):
+        assert errs[k] <= TOL_UV, (k, errs[k])
+
+
+def test_fp32_velocity_runs_split_by_a_forcing_change(gpu):
+    """An odd run (the state moves to the other ping-pong set), a new
+    forcing, then two runs with it unchanged: against the FP64 runs of the
+    same sequence, within the tolerances of one run -- a stale FP32 copy of
+    the forcing or of either set would be far outside them."""
+    b = _prep(gpu, basins.regional_basin(nx=400, ny=300, seed=45))
+    out = {}
+    for fp32 in (False, True):
+        bg = b.copy()
+        with gpu.BarotropicSolver(bg, resident=True, fp32_velocity=fp32) as s:
+            s.load_state()
+            s.run_substeps(7, b.dt)
+            s.sync_to_host()
+            for k in ("RHSx", "RHSy"):
+                bg.forcing[k] *= 1.3
+            s.load_state()
+            s.run_substeps(6, b.dt)
+            s.run_substeps(5, b.dt)
+            s.sync_to_host()
+        out[fp32] = bg
+    errs = {k: rel_err(out[True].state[k], out[False].state[k]) for k in b.state}
+    print("fp32 velocity split runs:", errs)
     assert errs["ssh_e"] <= TOL_SSH and errs["sshp_e"] <= TOL_SSH, errs
     for k in ("ubrtr_e", "ubrtrp_e", "vbrtr_e", "vbrtrp_e"):
         assert errs[k] <= TOL_UV, (k, errs[k])
