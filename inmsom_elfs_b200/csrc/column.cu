@@ -482,11 +482,13 @@ __global__ void k_vertical_velocity(Dom D, GridDev g, Levels L, double rho, int 
 // no slopes for level 1) into a 4-slot mbarrier ring.
 constexpr int FNROW = 12;
 constexpr int FSLOT_D = FNROW * RW;
+constexpr int FNS = 4;                   // ring slots (levels) of the flux kernel
+constexpr int FLUX_CTAS = 6;             // resident CTAs per SM its registers are cut for
 enum { G_FFP0, G_FFP1, G_MU0, G_MU1, G_FF0, G_FF1, G_UU, G_VV, G_SLRX, G_SLZX, G_SLRY, G_SLZY };
 
 size_t flux_smem(int nz)
 {
-    return ((size_t)NS * FSLOT_D + 2 * (size_t)nz + 1) * sizeof(double) + 2 * NS * sizeof(uint64_t);
+    return ((size_t)FNS * FSLOT_D + 2 * (size_t)nz + 1) * sizeof(double) + 2 * FNS * sizeof(uint64_t);
 }
 
 template <bool V>
@@ -521,9 +523,9 @@ __device__ __forceinline__ bool tracer_flux_column(const Dom &D, const GridDev &
     double acc1 = 0.0, acc2 = 0.0, acc3 = 0.0, acc4 = 0.0;
     bool ok = true;
     for (int k = 1; k <= nz && ok; k++) {
-        const int sk = (k - 1) % NS, sn = k % NS;
-        ok = mbar_wait(&full[sk], (uint32_t)(((k - 1) / NS) & 1));
-        if (ok && k < nz) ok = mbar_wait(&full[sn], (uint32_t)((k / NS) & 1));
+        const int sk = (k - 1) % FNS, sn = k % FNS;
+        ok = mbar_wait(&full[sk], (uint32_t)(((k - 1) / FNS) & 1));
+        if (ok && k < nz) ok = mbar_wait(&full[sn], (uint32_t)((k / FNS) & 1));
         ok = __all_sync(0xffffffffu, ok);
         if (!ok) break;
         const double *st = ring + (size_t)sk * FSLOT_D, *nx = ring + (size_t)sn * FSLOT_D;
@@ -586,19 +588,19 @@ __device__ __forceinline__ bool tracer_flux_column(const Dom &D, const GridDev &
     return ok;
 }
 
-__global__ void __launch_bounds__((NCW + 1) * 32) k_tracer_flux(Dom D, GridDev g, Levels L, TracerArgs a, int row0)
+__global__ void __launch_bounds__((NCW + 1) * 32, FLUX_CTAS) k_tracer_flux(Dom D, GridDev g, Levels L, TracerArgs a, int row0)
 {
     extern __shared__ __align__(128) double sm[];
     const int nz = L.nz;
     double *ring = sm;
-    double *sdz = ring + (size_t)NS * FSLOT_D;            // dz (nz), hzt (nz + 1)
+    double *sdz = ring + (size_t)FNS * FSLOT_D;            // dz (nz), hzt (nz + 1)
     uint64_t *full = reinterpret_cast<uint64_t *>(sdz + 2 * nz + 1);
-    uint64_t *empty = full + NS;
+    uint64_t *empty = full + FNS;
     const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
     const int m0 = D.nx_start + blockIdx.x * CW, n = row0 + blockIdx.y;
     for (int t = threadIdx.x; t < 2 * nz + 1; t += blockDim.x) sdz[t] = L.dz[t];
     if (threadIdx.x == 0) {
-        for (int s = 0; s < NS; s++) {
+        for (int s = 0; s < FNS; s++) {
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&full[s])), "r"(1) : "memory");
             asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_addr(&empty[s])), "r"(NCW)
                          : "memory");
@@ -618,8 +620,8 @@ __global__ void __launch_bounds__((NCW + 1) * 32) k_tracer_flux(Dom D, GridDev g
         int armed = 0;
         bool ok = true;
         for (int j = 1; j <= nz; j++) {
-            const int s = (j - 1) % NS;
-            if (j > NS && !mbar_wait(&empty[s], (uint32_t)(((j - 1) / NS - 1) & 1))) {
+            const int s = (j - 1) % FNS;
+            if (j > FNS && !mbar_wait(&empty[s], (uint32_t)(((j - 1) / FNS - 1) & 1))) {
                 ok = false;
                 break;
             }
@@ -643,8 +645,8 @@ __global__ void __launch_bounds__((NCW + 1) * 32) k_tracer_flux(Dom D, GridDev g
             armed = j;
         }
         if (!ok) atomicOr(a.flag, 1);
-        for (int j = max(1, armed - NS + 1); j <= armed; j++)
-            (void)mbar_wait(&full[(j - 1) % NS], (uint32_t)(((j - 1) / NS) & 1));
+        for (int j = max(1, armed - FNS + 1); j <= armed; j++)
+            (void)mbar_wait(&full[(j - 1) % FNS], (uint32_t)(((j - 1) / FNS) & 1));
         return;
     }
     const bool V = warp >= 2;
