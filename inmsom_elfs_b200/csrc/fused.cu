@@ -921,22 +921,31 @@ __global__ void k_minmax3(Dom D, const float *lu, const double *a, const double 
 }
 
 // FP64 -> FP32 (round to nearest), n values
+// FP64 -> FP32, rounded to nearest; four values per thread and iteration
+// (two 16-byte loads, one 16-byte store) where the arrays allow it
 __global__ void k_to_f32(const double *a, float *b, long long n)
 {
-    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        b[i] = (float)a[i];
+    const long long t0 = blockIdx.x * (long long)blockDim.x + threadIdx.x, st = (long long)gridDim.x * blockDim.x;
+    const bool vec = ((reinterpret_cast<uintptr_t>(a) | reinterpret_cast<uintptr_t>(b)) & 15u) == 0;
+    const long long n4 = vec ? n / 4 : 0;
+    for (long long i = t0; i < n4; i += st) {
+        const double2 x = reinterpret_cast<const double2 *>(a)[2 * i], y = reinterpret_cast<const double2 *>(a)[2 * i + 1];
+        reinterpret_cast<float4 *>(b)[i] = make_float4((float)x.x, (float)x.y, (float)y.x, (float)y.y);
+    }
+    for (long long i = 4 * n4 + t0; i < n; i += st) b[i] = (float)a[i];
 }
 
 // FP32 velocities back into an FP64 set at the points the FP32 kernel
 // writes: u, up on lcu, v, vp on lcv (interior); every other point of the
 // FP64 set keeps its value
+// (one thread per column of a row: blockIdx.y strides the rows)
 __global__ void k_vel_from_f32(const float *vs, double *set, const float *lu, long long pitch, long long fs, int r0,
                                int r1, int c0, int c1)
 {
-    const int w = c1 - c0 + 1;
-    const long long tot = (long long)w * (r1 - r0 + 1);
-    for (long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x; t < tot; t += (long long)gridDim.x * blockDim.x) {
-        const long long i = (long long)(r0 + t / w) * pitch + c0 + t % w;
+    const int c = c0 + blockIdx.x * blockDim.x + threadIdx.x;
+    if (c > c1) return;
+    for (int row = r0 + blockIdx.y; row <= r1; row += gridDim.y) {
+        const long long i = (long long)row * pitch + c;
         const bool o = lu[i] > 0.5f;
         if (o && lu[i + 1] > 0.5f) {
             set[S_U * fs + i] = (double)vs[0 * fs + i];
@@ -1720,10 +1729,13 @@ int finish_steps_f32(Plan &p, const Dom &d, double *state[6], cudaStream_t s)
 {
     const int fi = set_index(p, state[0]);
     if (fi < 0) return 1;
-    k_vel_from_f32<<<4 * p.nsm, 256, 0, s>>>(p.vset[fi], p.set[fi], p.lu, d.pitch, p.fstride,
-                                             d.ny_start - d.bnd_y1, d.ny_end - d.bnd_y1,
-                                             d.nx_start - d.bnd_x1 + d.xoff, d.nx_end - d.bnd_x1 + d.xoff);
-    if (cudaGetLastError() != cudaSuccess) return 1;
+    const int c0 = d.nx_start - d.bnd_x1 + d.xoff, c1 = d.nx_end - d.bnd_x1 + d.xoff;
+    const int r0 = d.ny_start - d.bnd_y1, r1 = d.ny_end - d.bnd_y1;
+    if (c1 >= c0 && r1 >= r0) {
+        const dim3 grid((unsigned)((c1 - c0 + 1 + 127) / 128), (unsigned)std::min(r1 - r0 + 1, 65535));
+        k_vel_from_f32<<<grid, 128, 0, s>>>(p.vset[fi], p.set[fi], p.lu, d.pitch, p.fstride, r0, r1, c0, c1);
+        if (cudaGetLastError() != cudaSuccess) return 1;
+    }
     return finish_steps(p, s);
 }
 
