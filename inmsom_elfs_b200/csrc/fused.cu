@@ -817,9 +817,9 @@ __device__ __forceinline__ unsigned ld_acquire(const unsigned *a)
 }
 
 // resident CTAs per SM the kernel is cut for: the general variant's where
-// some member takes it, else 12 (the uniform plain substep's 16 leave the
-// claim loop 128 registers and spill; 12 ran 24 % faster than 16 and 10 %
-// faster than 11 on 64 regional basins)
+// some member takes it, else 12 (on 64 regional basins 16 CTAs, at 128
+// registers with a few bytes spilled, ran 8 % slower, 11 CTAs 10 % slower,
+// and 8, 10 and 12 alike)
 template <bool ANYGEN>
 constexpr int ens_ctas()
 {
