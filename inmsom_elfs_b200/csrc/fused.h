@@ -225,7 +225,7 @@ struct EnsMemberIn {
 };
 struct EnsTable {
     void *d_mem = nullptr;
-    int *d_moff = nullptr;
+    int2 *d_order = nullptr;   // {member, item} per claim within a substep
     unsigned *d_ctr = nullptr, *d_done = nullptr;
     int nmem = 0, total = 0, group = 0, grid = 0;
     bool anygen = false;   // some member takes the general variant (fewer CTAs per SM)
