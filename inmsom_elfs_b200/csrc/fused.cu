@@ -28,7 +28,7 @@
 // holds a 36-column segment of the six state fields and of the static
 // fields (rest depth, forcing; in the general variant also viscosity, drag
 // and water flux), brought by two 3-D tiled TMA loads from field-blocked
-// arrays (cp.async.bulk.tensor, no multicast), plus the row's T-mask bits
+// arrays (cp.async.bulk.tensor, each copy for one CTA), plus the row's T-mask bits
 // (and, in the general variant, its metric coefficients) by 1-D bulk copies.
 // One elected lane refills the slot of row j-2 with row j-2+RING once every
 // lane is past it.  Every wait is bounded: on timeout the CTA sets a status bit,

@@ -6,7 +6,7 @@
 // time-mean accumulation and Robert-Asselin filter with time shift) for the
 // whole basin.  Each CTA owns a strip of columns and marches down a chunk of
 // rows; input rows arrive through a ring of shared-memory slots filled by
-// 3-D tiled TMA copies (cp.async.bulk.tensor, no multicast) of field-blocked
+// 3-D tiled TMA copies (cp.async.bulk.tensor, each copy for one CTA) of field-blocked
 // arrays, tracked by mbarriers.
 //
 // Device layout of the fused path: a state set is ONE allocation holding the
