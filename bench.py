@@ -333,7 +333,9 @@ def run_reference(args):
     cfg = config_dict(b, args, 1)
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": METRIC, "n_gpus": args.gpus,
-        "steps": ksteps * nstep, "warmup": max(args.warmup, 0) * nstep,
+        # steps and warmup as run: calls of barotropic_dynamics, each a bounded
+        # sample of nstep advancing steps; value and ms_per_step per advancing step
+        "steps": ksteps, "warmup": max(args.warmup, 0), "advancing_steps_per_step": nstep,
         "ms_per_step": el / (ksteps * nstep) * 1e3,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": cfg,
