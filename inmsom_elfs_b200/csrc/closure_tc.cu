@@ -147,6 +147,39 @@ __device__ __forceinline__ void ld16(uint32_t taddr, float (&v)[16])
     for (int k = 0; k < 16; k++) v[k] = __uint_as_float(r[k]);
 }
 
+// 2 x 16 consecutive FP32 columns of this thread's lane (two blocks of
+// tensor memory), both loads in flight before one wait; the registers are
+// operands of the wait, so nothing reads them before it
+__device__ __forceinline__ void ld16x2(uint32_t ta, uint32_t tb, float (&a)[16], float (&b)[16])
+{
+    uint32_t r[32];
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+          "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+        : "r"(ta));
+    asm volatile(
+        "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+        "%15}, [%16];"
+        : "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]), "=r"(r[22]), "=r"(r[23]),
+          "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]), "=r"(r[29]), "=r"(r[30]), "=r"(r[31])
+        : "r"(tb));
+    asm volatile("tcgen05.wait::ld.sync.aligned;"
+                 : "+r"(r[0]), "+r"(r[1]), "+r"(r[2]), "+r"(r[3]), "+r"(r[4]), "+r"(r[5]), "+r"(r[6]), "+r"(r[7]),
+                   "+r"(r[8]), "+r"(r[9]), "+r"(r[10]), "+r"(r[11]), "+r"(r[12]), "+r"(r[13]), "+r"(r[14]),
+                   "+r"(r[15]), "+r"(r[16]), "+r"(r[17]), "+r"(r[18]), "+r"(r[19]), "+r"(r[20]), "+r"(r[21]),
+                   "+r"(r[22]), "+r"(r[23]), "+r"(r[24]), "+r"(r[25]), "+r"(r[26]), "+r"(r[27]), "+r"(r[28]),
+                   "+r"(r[29]), "+r"(r[30]), "+r"(r[31])
+                 :
+                 : "memory");
+#pragma unroll
+    for (int k = 0; k < 16; k++) {
+        a[k] = __uint_as_float(r[k]);
+        b[k] = __uint_as_float(r[16 + k]);
+    }
+}
+
 __device__ __forceinline__ uint32_t pack2(float lo, float hi)
 {
     const __nv_bfloat162 v = __floats2bfloat162_rn(lo, hi);
@@ -334,8 +367,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         if (!(ok = sync_mma())) break;
         {
             float da[16], z[16];
-            ld16(lane + C_DA2 + c0, da);
-            ld16(lane + C_Z2 + c0, z);
+            ld16x2(lane + C_DA2 + c0, lane + C_Z2 + c0, da, z);
 #pragma unroll
             for (int k = 0; k < 16; k++)
                 da[k] *= gelu_d(z[k] + s.b2[c0 + k]);
@@ -355,8 +387,7 @@ __global__ void __launch_bounds__(THREADS, 1)
         if (!(ok = sync_mma())) break;
         {
             float da[16], z[16];
-            ld16(lane + C_DA1 + c0, da);
-            ld16(lane + C_Z1 + c0, z);
+            ld16x2(lane + C_DA1 + c0, lane + C_Z1 + c0, da, z);
 #pragma unroll
             for (int k = 0; k < 16; k++)
                 da[k] *= gelu_d(z[k] + s.b1[c0 + k]);
