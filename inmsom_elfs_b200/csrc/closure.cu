@@ -167,7 +167,9 @@ __device__ __forceinline__ uint32_t pack2(float lo, float hi)
 }
 
 // y (outputs 0, 1 of cells g and g+8 in o[0..3] of lanes t == 0) of the
-// 16 cells whose layer-1 A fragments are a1
+// 16 cells whose layer-1 A fragments are a1.  The hidden activations are
+// kept as 2 GELU (gelu2) and s.w2t, s.w3t hold the halved weights: the same
+// products, one multiplication fewer per activation.
 template <class S>
 __device__ __forceinline__ void mlp16(const S &s, const uint32_t a1[3][4], float o[4])
 {
@@ -188,10 +190,10 @@ __device__ __forceinline__ void mlp16(const S &s, const uint32_t a1[3][4], float
     uint32_t a2[4][4];
 #pragma unroll
     for (int kb = 0; kb < 4; kb++) {
-        a2[kb][0] = pack2(gelu(acc[2 * kb][0]), gelu(acc[2 * kb][1]));
-        a2[kb][1] = pack2(gelu(acc[2 * kb][2]), gelu(acc[2 * kb][3]));
-        a2[kb][2] = pack2(gelu(acc[2 * kb + 1][0]), gelu(acc[2 * kb + 1][1]));
-        a2[kb][3] = pack2(gelu(acc[2 * kb + 1][2]), gelu(acc[2 * kb + 1][3]));
+        a2[kb][0] = pack2(gelu2(acc[2 * kb][0]), gelu2(acc[2 * kb][1]));
+        a2[kb][1] = pack2(gelu2(acc[2 * kb][2]), gelu2(acc[2 * kb][3]));
+        a2[kb][2] = pack2(gelu2(acc[2 * kb + 1][0]), gelu2(acc[2 * kb + 1][1]));
+        a2[kb][3] = pack2(gelu2(acc[2 * kb + 1][2]), gelu2(acc[2 * kb + 1][3]));
     }
 #pragma unroll
     for (int nt = 0; nt < 8; nt++) {
@@ -207,10 +209,10 @@ __device__ __forceinline__ void mlp16(const S &s, const uint32_t a1[3][4], float
         }
 #pragma unroll
     for (int kb = 0; kb < 4; kb++) {
-        a2[kb][0] = pack2(gelu(acc[2 * kb][0]), gelu(acc[2 * kb][1]));
-        a2[kb][1] = pack2(gelu(acc[2 * kb][2]), gelu(acc[2 * kb][3]));
-        a2[kb][2] = pack2(gelu(acc[2 * kb + 1][0]), gelu(acc[2 * kb + 1][1]));
-        a2[kb][3] = pack2(gelu(acc[2 * kb + 1][2]), gelu(acc[2 * kb + 1][3]));
+        a2[kb][0] = pack2(gelu2(acc[2 * kb][0]), gelu2(acc[2 * kb][1]));
+        a2[kb][1] = pack2(gelu2(acc[2 * kb][2]), gelu2(acc[2 * kb][3]));
+        a2[kb][2] = pack2(gelu2(acc[2 * kb + 1][0]), gelu2(acc[2 * kb + 1][1]));
+        a2[kb][3] = pack2(gelu2(acc[2 * kb + 1][2]), gelu2(acc[2 * kb + 1][3]));
     }
     o[0] = o[2] = s.b3[2 * t];
     o[1] = o[3] = s.b3[2 * t + 1];
@@ -227,8 +229,12 @@ __global__ void __launch_bounds__(WARPS * 32, 2) k_closure_apply(const __grid_co
     __shared__ __align__(16) ClSmem s;
     const __nv_bfloat16 *wb = (const __nv_bfloat16 *)a.wb;
     for (int i = threadIdx.x; i < KIN * HID; i += blockDim.x) s.w1t[i % HID][i / HID] = wb[BOFF_W1 + i];
-    for (int i = threadIdx.x; i < HID * HID; i += blockDim.x) s.w2t[i % HID][i / HID] = wb[BOFF_W2 + i];
-    for (int i = threadIdx.x; i < HID * N3; i += blockDim.x) s.w3t[i % N3][i / N3] = wb[BOFF_W3 + i];
+    // layers 2 and 3 take 2 GELU (gelu2) as their input: their weights are
+    // halved here (exact in BF16), so that every product is the network's
+    for (int i = threadIdx.x; i < HID * HID; i += blockDim.x)
+        s.w2t[i % HID][i / HID] = __float2bfloat16(0.5f * __bfloat162float(wb[BOFF_W2 + i]));
+    for (int i = threadIdx.x; i < HID * N3; i += blockDim.x)
+        s.w3t[i % N3][i / N3] = __float2bfloat16(0.5f * __bfloat162float(wb[BOFF_W3 + i]));
     for (int i = threadIdx.x; i < HID; i += blockDim.x) {
         s.b1[i] = a.prm[OFF_B1 + i];
         s.b2[i] = a.prm[OFF_B2 + i];
@@ -364,10 +370,13 @@ __global__ void __launch_bounds__(GW * 32) k_mlp_forward(const __nv_bfloat16 *x,
     __shared__ FSmem s;
     const int w = threadIdx.x >> 5, l = threadIdx.x & 31, g = l >> 2, t = l & 3;
     for (int i = threadIdx.x; i < KIN * HID; i += blockDim.x) s.w1t[i % HID][i / HID] = wb[BOFF_W1 + i];
-    for (int i = threadIdx.x; i < HID * HID; i += blockDim.x) s.w2t[i % HID][i / HID] = wb[BOFF_W2 + i];
+    // layers 2 and 3 take 2 GELU (mlp16's gelu2): their weights halved (exact)
+    for (int i = threadIdx.x; i < HID * HID; i += blockDim.x)
+        s.w2t[i % HID][i / HID] = __float2bfloat16(0.5f * __bfloat162float(wb[BOFF_W2 + i]));
     for (int i = threadIdx.x; i < 16 * HS; i += blockDim.x) {
         const int o = i / HS, c = i % HS;
-        s.w3t[o][c] = o < N3 && c < HID ? wb[BOFF_W3 + c * N3 + o] : __float2bfloat16(0.f);
+        s.w3t[o][c] = o < N3 && c < HID ? __float2bfloat16(0.5f * __bfloat162float(wb[BOFF_W3 + c * N3 + o]))
+                                        : __float2bfloat16(0.f);
     }
     for (int i = threadIdx.x; i < HID; i += blockDim.x) {
         s.b1[i] = prm[OFF_B1 + i];

@@ -26,6 +26,15 @@ __device__ __forceinline__ float gelu(float x)
     return fmaf(h, tanh_hw(x * fmaf(GELU_C1, x * x, GELU_C0)), h);
 }
 
+// 2 GELU(x) = x (1 + t), one multiplication fewer than GELU itself and
+// bit for bit twice its value (a power-of-two scale commutes with the
+// rounding): the inference kernel feeds it to the next layer with that
+// layer's weights halved, which leaves every product a * w unchanged
+__device__ __forceinline__ float gelu2(float x)
+{
+    return fmaf(x, tanh_hw(x * fmaf(GELU_C1, x * x, GELU_C0)), x);
+}
+
 __device__ __forceinline__ float gelu_d(float x)
 {
     const float x2 = x * x, t = tanh_hw(x * fmaf(GELU_C1, x2, GELU_C0));
