@@ -114,3 +114,26 @@ def test_ensemble_members_match_the_oracle(gpu, ora):
         ora.run_substeps(bo, nsub, b.dt, scale)
         for k in ("ssh_e", "ubrtr_e", "vbrtr_e", "sshp_e", "ubrtrp_e", "vbrtrp_e"):
             assert rel_err(g.state[k], bo.state[k]) <= 1e-12, (b.bounds.nx, k)
+
+
+@pytest.mark.parametrize("persistent", [False, True])
+def test_sixty_four_members_match_members_run_alone(gpu, persistent):
+    """The configuration's member count: 64 regional basins of sides drawn
+    from 64..256 in steps of 64 (seeded), wind amplitude +-20 %, 10 substeps
+    (two replays of a group of 4 and two direct substeps), every member bit
+    for bit its run alone."""
+    rng = np.random.default_rng(64)
+    bs = []
+    for i, (n, a) in enumerate(zip(rng.choice([64, 128, 192, 256], size=64), rng.uniform(0.8, 1.2, size=64))):
+        b = basins.regional_basin(nx=int(n), ny=int(n), seed=200 + i)
+        b.taux *= a
+        b.tauy *= a
+        basins.finalize(b, gpu.GpuBackend(0))
+        bs.append(b)
+    nsub = 10
+    scale = basins.wind_cycle(nsub, 2.0, t0=50.0, period=600.0)
+    ref = [_alone(gpu, b, nsub, scale) for b in bs]
+    got, _ = _ensemble(gpu, bs, nsub, scale, group=4, persistent=persistent)
+    for r, g in zip(ref, got):
+        for k in r.state:
+            assert np.array_equal(r.state[k], g.state[k]), k

@@ -100,6 +100,37 @@ def test_fp32_velocity_runs_split_by_a_forcing_change(gpu):
         assert errs[k] <= TOL_UV, (k, errs[k])
 
 
+def test_fp32_velocity_at_the_4096_ridge_basin_size(gpu):
+    """The configuration's own case: the 4096 x 4096 double-gyre ridge basin
+    (2 km, dt 3 s, wind with a 6-hour cycle), 5000 steps of the FP32-velocity
+    variant against the FP64 run.  Bounds (max over ocean points of |diff| /
+    max |FP64|): u 1e-4, v 2e-4, SSH 1e-4 (measured on a B200: 3.7e-5, 1.0e-4,
+    4.6e-5); the volume change as small as the FP64 run's (1e-13)."""
+    b = _prep(gpu, basins.ridge_basin(n=4096))
+    steps = 5000
+    scale = basins.wind_cycle(steps, b.dt)
+    out, dvol = {}, {}
+    for fp32 in (False, True):
+        bg = b.copy()
+        with gpu.BarotropicSolver(bg, resident=True, fp32_velocity=fp32) as s:
+            s.load_state()
+            v0, _ = s.diag()
+            s.run_substeps(steps, b.dt, scale)
+            v1, _ = s.diag()
+            s.sync_to_host()
+        out[fp32], dvol[fp32] = bg, abs(v1 - v0) / v0
+    ocean = b.masks["lu"] > 0.5
+    err = {}
+    for k in b.state:
+        d = (out[True].state[k] - out[False].state[k])[ocean]
+        err[k] = float(np.abs(d).max() / np.abs(out[False].state[k][ocean]).max())
+    print("4096^2 ridge basin, 5000 steps, FP32 velocity vs FP64:", err, "volume change", dvol)
+    assert err["ubrtr_e"] <= 1e-4 and err["ubrtrp_e"] <= 1e-4, err
+    assert err["vbrtr_e"] <= 2e-4 and err["vbrtrp_e"] <= 2e-4, err
+    assert err["ssh_e"] <= 1e-4 and err["sshp_e"] <= 1e-4, err
+    assert dvol[True] <= 1e-13 and dvol[False] <= 1e-13, dvol
+
+
 def test_fp32_velocity_conserves_volume(gpu):
     b = _prep(gpu, basins.beta_plane_basin(n=200, seed=42))
     lu = b.masks["lu"] > 0.5
