@@ -139,3 +139,25 @@ def test_regional_2048x1536_volume_over_10000_steps(gpu, regional):
         assert s.guard() == 0
     assert e1 > 0.0
     assert abs(v1 - v0) <= 1e-12 * abs(v0), (v1 - v0) / v0
+
+
+@pytest.mark.gpu
+def test_regional_2048x1536_drop_in_call_with_time_means(gpu, ora, regional):
+    """The call the end-to-end measurement makes, at the benchmark basin's
+    size: barotropic_dynamics(tau = 10 dt, nstep = 10) through the drop-in
+    entry point (20 substeps, the state saved at the tenth, the four time
+    means over all of them), twice, on a resident context with static
+    coefficients, against the oracle: state and time means within 1e-12."""
+    b, _ = regional
+    bo, bg = b.copy(), b.copy()
+    for _ in range(2):
+        ora.barotropic_dynamics(bo, 10 * b.dt, 10)
+    with gpu.BarotropicSolver(bg, resident=True, static_coeffs=True) as s:
+        for _ in range(2):
+            s.barotropic_dynamics(10 * b.dt, 10)
+        s.sync_to_host(0x1 | 0x2)
+        assert s.path() == (1, "eligible")
+    _close(bo, bg, TOL10)
+    for k in ("ubrtr_i", "vbrtr_i", "ssh4gradx", "ssh4grady"):
+        e = rel_err(bg.means[k], bo.means[k])
+        assert e <= TOL10, f"{k}: {e:.3e}"
