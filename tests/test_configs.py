@@ -161,3 +161,22 @@ def test_regional_2048x1536_drop_in_call_with_time_means(gpu, ora, regional):
     for k in ("ubrtr_i", "vbrtr_i", "ssh4gradx", "ssh4grady"):
         e = rel_err(bg.means[k], bo.means[k])
         assert e <= TOL10, f"{k}: {e:.3e}"
+
+
+@pytest.mark.gpu
+def test_ridge_4096_fp64_parity_10(gpu, ora):
+    """The 4096 x 4096 double-gyre ridge basin (2 km, dt 3 s), the FP32
+    variant's reference run, in FP64 on the fused path against the oracle
+    after 10 steps (1e-12); 16.8 M cells, the largest configuration."""
+    b = basins.ridge_basin(n=4096)
+    basins.finalize(b, ora.OracleBackend())
+    ora.hh_init_external(b)
+    bo, bg = b.copy(), b.copy()
+    scale = basins.wind_cycle(10, b.dt)
+    ora.run_substeps(bo, 10, b.dt, scale)
+    with gpu.BarotropicSolver(bg, resident=True) as s:
+        assert s.path() == (1, "eligible")
+        s.load_state()
+        s.run_substeps(10, b.dt, scale)
+        s.sync_to_host()
+    _close(bo, bg, TOL10)
