@@ -351,3 +351,18 @@ def test_static_coeffs_stay_resident(gpu, ora):
     assert_close(bo, bg, TOL10)
     for k in MEANS:
         assert rel_err(bg.means[k], bo.means[k]) <= TOL10, k
+
+
+@pytest.mark.parametrize("nx,ny", [(3, 3), (5, 4), (17, 9), (29, 6), (31, 5), (61, 3), (7, 40)])
+def test_tiny_and_ragged_basins(gpu, ora, nx, ny):
+    """Basins smaller than a strip (30 columns) or a work item (16 rows), one
+    ocean cell upward, and strips cut one or two columns into the next: the
+    fused path against the oracle after 10 steps (1e-12) and the per-loop
+    path bit for bit."""
+    b = prep(basins.beta_plane_basin(n=nx, ny=ny, seed=nx * 100 + ny), ora)
+    bo, bg, path = run_pair(gpu, ora, b, 10, b.dt, 1)
+    assert path[0] == 1, path
+    assert_close(bo, bg, TOL10)
+    bo, bg, path = run_pair(gpu, ora, b, 10, b.dt, 1, force_general=True)
+    assert path[0] == 0
+    assert_bitexact(bo, bg, groups=("state",))
