@@ -366,3 +366,18 @@ def test_tiny_and_ragged_basins(gpu, ora, nx, ny):
     bo, bg, path = run_pair(gpu, ora, b, 10, b.dt, 1, force_general=True)
     assert path[0] == 0
     assert_bitexact(bo, bg, groups=("state",))
+
+
+@pytest.mark.parametrize("force_general", [False, True])
+def test_all_land_basin_keeps_its_state(gpu, ora, force_general):
+    """An empty ocean (every point land): both paths run and leave every
+    state array as it was, as the oracle does."""
+    b = basins.beta_plane_basin(n=40, ny=30, seed=5)
+    b.masks["lu"][...] = 0.0
+    b.hhq_rest[...] = 0.0
+    prep(b, ora)
+    bo, bg, path = run_pair(gpu, ora, b, 5, b.dt, 1, force_general=force_general)
+    assert path[0] == (0 if force_general else 1), path
+    for k in STATE:
+        assert np.array_equal(bg.state[k], b.state[k]), k
+        assert np.array_equal(bo.state[k], b.state[k]), k
