@@ -381,3 +381,25 @@ def test_all_land_basin_keeps_its_state(gpu, ora, force_general):
     for k in STATE:
         assert np.array_equal(bg.state[k], b.state[k]), k
         assert np.array_equal(bo.state[k], b.state[k]), k
+
+
+@pytest.mark.parametrize("force_general", [False, True])
+def test_land_values_do_not_reach_the_ocean(gpu, ora, force_general):
+    """Random values at every land and halo point of the state (the
+    reference never writes them, and its stencils weight them by masks):
+    the ocean points match the oracle (fused 1e-12, per-loop bit for bit)
+    and the land points keep their values."""
+    b = basins.regional_basin(nx=120, ny=90, seed=23)
+    prep(b, ora)
+    rng = np.random.default_rng(24)
+    land = b.masks["lu"] < 0.5
+    for k in STATE:
+        b.state[k] = np.asfortranarray(np.where(land, rng.standard_normal(b.bounds.shape), b.state[k]))
+    bo, bg, path = run_pair(gpu, ora, b, 10, b.dt, 1, force_general=force_general)
+    assert path[0] == (0 if force_general else 1), path
+    if force_general:
+        assert_bitexact(bo, bg, groups=("state",))
+    else:
+        assert_close(bo, bg, TOL10)
+    for k in STATE:
+        assert np.array_equal(bg.state[k][land], b.state[k][land]), k
