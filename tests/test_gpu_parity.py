@@ -403,3 +403,53 @@ def test_land_values_do_not_reach_the_ocean(gpu, ora, force_general):
         assert_close(bo, bg, TOL10)
     for k in STATE:
         assert np.array_equal(bg.state[k][land], b.state[k][land]), k
+
+
+def test_fixed_depth_free_surface_off(gpu, ora):
+    """full_free_surface = 0 (Inc/basinpar.fi: the depths stay at the rest
+    depth and the water flux leaves the continuity): the fused path refuses
+    it and the per-loop path follows the oracle bit for bit, time means and
+    depths included."""
+    import dataclasses
+    b = basins.regional_basin(nx=90, ny=70, seed=29)
+    b.consts = dataclasses.replace(b.consts, full_free_surface=0)
+    b.forcing["wflux"] = np.asfortranarray(1e-4 * np.random.default_rng(30).standard_normal(b.bounds.shape))
+    prep(b, ora)
+    bo, bg, path = run_pair(gpu, ora, b, 4, 3 * b.dt, 3)
+    assert path[0] == 0 and "full_free_surface" in path[1], path
+    assert_bitexact(bo, bg, groups=("state", "means", "depths"))
+
+
+@pytest.mark.parametrize("px,py", [(1, 0), (0, 1), (1, 1)])
+def test_general_bitexact_periodic(gpu, ora, px, py):
+    """Periodic wraps of the barotropic step (Service/oc_algorithms.f90:50-135
+    after every field update) in x, y and both, on a basin with a seeded
+    island and a non-uniform Coriolis field: the per-loop path bit for bit
+    with the oracle, time means and depths included."""
+    from inmsom_elfs_b200.grid import Basin, Consts
+    rng = np.random.default_rng(40 + 2 * px + py)
+    nx, ny = 36, 28
+    bd = Bounds.serial(nx, ny, periodicity_x=px, periodicity_y=py)
+    b = Basin(bd, Consts())
+    lu = np.ones(bd.shape, dtype=np.float32, order="F")
+    if not py:
+        lu[:, : bd.nnn - bd.bnd_y1] = 0.0
+        lu[:, bd.nn - bd.bnd_y1 + 1:] = 0.0
+    if not px:
+        lu[: bd.mmm - bd.bnd_x1, :] = 0.0
+        lu[bd.mm - bd.bnd_x1 + 1:, :] = 0.0
+    i0, j0 = bd.mmm - bd.bnd_x1 + nx // 3, bd.nnn - bd.bnd_y1 + ny // 3
+    lu[i0:i0 + 3, j0:j0 + 2] = 0.0
+    b.masks["lu"] = np.asfortranarray(lu)
+    basins.uniform_metrics(b, 5.0e3)
+    b.rlh_s = np.asfortranarray(1.0e-4 + 1.0e-5 * rng.standard_normal(bd.shape))
+    b.hhq_rest = np.asfortranarray(np.where(lu > 0.5, 200.0 * (0.8 + 0.4 * rng.random(bd.shape)), 0.0))
+    b.taux = np.asfortranarray(0.1 * rng.standard_normal(bd.shape))
+    b.tauy = np.asfortranarray(0.1 * rng.standard_normal(bd.shape))
+    b.forcing["mu"] = np.full(bd.shape, 300.0, order="F")
+    b.forcing["rdis"] = np.full(bd.shape, 1.0e-6, order="F")
+    b.dt = 20.0
+    prep(b.fill_defaults(), ora)
+    bo, bg, path = run_pair(gpu, ora, b, 5, 2 * b.dt, 2)
+    assert path[0] == 0 and "periodic" in path[1], path
+    assert_bitexact(bo, bg, groups=("state", "means", "depths"))
