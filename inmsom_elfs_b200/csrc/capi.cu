@@ -1119,6 +1119,8 @@ int inmsom_gpu_sync_from_host(inmsom_ctx *c, unsigned what)
 
 // ===========================================================================
 // Ensemble of contexts advanced by one CUDA graph per group of substeps.
+constexpr int ENS_MIN_ROWS = 16;   // shortest work item of an ensemble member
+
 struct inmsom_ens {
     std::vector<inmsom_ctx *> m;
     int device = 0, group = 2;
@@ -1245,6 +1247,17 @@ int inmsom_ens_create(inmsom_ens **out, inmsom_ctx *const *members, int n, int g
     e->join.assign(n, nullptr);
     for (int i = 0; i < n && ce == cudaSuccess; i++) ce = cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming);
     if (ce == cudaSuccess) ce = cudaMalloc(&e->d_base, sizeof(int));
+    // members share the device: items of 16 rows at least (a basin alone
+    // cuts down to 4 to spread a small basin over more SMs)
+    for (int i = 0; i < n && ce == cudaSuccess; i++) {
+        inmsom_ctx *c = members[i];
+        if (c->plan.min_rows == ENS_MIN_ROWS) continue;
+        c->plan.min_rows = ENS_MIN_ROWS;
+        if (fused::repartition(c->plan, c->dom, c->plan.rows_per_item[0], c->stream)) {
+            ce = cudaGetLastError();
+            if (ce == cudaSuccess) ce = cudaErrorUnknown;
+        }
+    }
     if (ce != cudaSuccess) {
         inmsom_ens_destroy(e);
         return set_err(INMSOM_ECUDA, "inmsom_ens_create: %s", cudaGetErrorString(ce));

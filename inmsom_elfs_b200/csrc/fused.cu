@@ -1151,7 +1151,6 @@ int encode_fields(EncodeTiled enc, CUtensorMap *map, void *base, const Dom &d, l
 }
 
 constexpr double LAND_COST = 0.7;
-constexpr int MIN_ROWS = 16;
 
 // Ocean flags of the written columns of every strip and device row
 // (strip-major, nya rows per strip), from the host T mask.
@@ -1178,8 +1177,10 @@ std::vector<uint8_t> ocean_rows(const Plan &p, const Dom &d, const float *lu)
 // resident CTAs holds (`slots`), so that the wave finishes together; else
 // about that many rows per item (several waves).  A row whose written
 // columns are all land skips the momentum stages and costs about LAND_COST
-// of an ocean row; no chunk is shorter than MIN_ROWS rows (each pays three
-// warm-up iterations).
+// of an ocean row; no chunk is shorter than p.min_rows rows (each pays
+// three warm-up iterations: 4 rows for a basin alone, where the items of a
+// small basin would otherwise fill few SMs; 16 for an ensemble member, whose
+// neighbours fill the rest).
 std::vector<int4> partition(const Plan &p, const Dom &d, int slots, int rows_per_item, int rf, int rl)
 {
     const int ny = rl - rf + 1, nya = d.nya();
@@ -1193,7 +1194,7 @@ std::vector<int4> partition(const Plan &p, const Dom &d, int slots, int rows_per
         }
         all += total[s];
     }
-    const int maxc = std::max(1, ny / MIN_ROWS);
+    const int maxc = std::max(1, ny / std::max(1, p.min_rows));
     std::vector<int> n(p.nstrips);
     if (rows_per_item > 0) {
         for (int s = 0; s < p.nstrips; s++)

@@ -98,6 +98,7 @@ struct Plan {
     int occ[5] = {0, 0, 0, 0, 0};   // resident CTAs per SM, per item table
     std::vector<uint8_t> ocean;     // per strip and interior row: any written column is ocean
     int rows_per_item[2] = {0, 0};  // 0: one wave of items by cost; else rows per item
+    int min_rows = 4;               // no work item is shorter (an ensemble member: 16)
     // plain-substep items over rows extended into the halo (a row strip
     // that advances several substeps per exchange): per variant and number
     // of rows computed south / north of the interior, built on first use

@@ -355,7 +355,7 @@ def test_static_coeffs_stay_resident(gpu, ora):
 
 @pytest.mark.parametrize("nx,ny", [(3, 3), (5, 4), (17, 9), (29, 6), (31, 5), (61, 3), (7, 40)])
 def test_tiny_and_ragged_basins(gpu, ora, nx, ny):
-    """Basins smaller than a strip (30 columns) or a work item (16 rows), one
+    """Basins smaller than a strip (30 columns) or a work item (4 rows), one
     ocean cell upward, and strips cut one or two columns into the next: the
     fused path against the oracle after 10 steps (1e-12) and the per-loop
     path bit for bit."""
