@@ -601,7 +601,10 @@ int inmsom_read_checkpoint(inmsom_ctx *ctx, const char *path, double *ubrtr_e, d
  * is paid once per group.  rhs_scale (nsub values, or NULL for 1) scales
  * every member's RHS at each substep.  group must be even (it keeps each
  * member's state in its set, so the graph can be replayed).  *ms receives
- * the device time of the run. */
+ * the device time of the run.  Creation re-cuts each member's work items
+ * to 16 rows at least (a context alone cuts down to 4, which spreads a
+ * small basin over more SMs; in an ensemble the other members fill them),
+ * and the members keep that cut after the ensemble is destroyed. */
 typedef struct inmsom_ens inmsom_ens;
 int inmsom_ens_create(inmsom_ens **ens, inmsom_ctx *const *members, int nmembers, int group);
 int inmsom_ens_run(inmsom_ens *ens, int nsub, const double *dt, const double *rhs_scale, float *ms);
@@ -609,7 +612,8 @@ int inmsom_ens_run(inmsom_ens *ens, int nsub, const double *dt, const double *rh
  * times `trial_groups` graph launches with each candidate chunk height
  * (one wave of cost-balanced chunks, or about 96, 64, 48 or 32 rows per
  * chunk) and keeps the fastest; rows_per_item[i] receives member i's
- * choice (0 = one wave).  The trial runs advance the members' states. */
+ * choice (0 = one wave), which the members keep.  The trial runs advance
+ * the members' states. */
 int inmsom_ens_tune(inmsom_ens *ens, const double *dt, int trial_groups, int *rows_per_item);
 /* on != 0: inmsom_ens_run advances each group of substeps of all members
  * with ONE persistent cooperative launch (still replayed as a CUDA graph)
