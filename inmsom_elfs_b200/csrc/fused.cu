@@ -1246,18 +1246,23 @@ std::vector<int4> partition(const Plan &p, const Dom &d, int slots, int rows_per
 // time-mean substeps (-1.9 % against one)
 int item_waves(int table) { return table == 2 || table == 3 ? 2 : 1; }
 
+// Replaces table v.  On failure the plan keeps its previous table (a
+// launch never sees a count without its items).
 int upload_items(Plan &p, int v, const std::vector<int4> &items, cudaStream_t s)
 {
+    int4 *t = nullptr;
+    if (cudaMalloc(&t, items.size() * sizeof(int4)) != cudaSuccess) return 1;
+    // the item table is a host vector: finish its copy before returning
+    if (cudaMemcpyAsync(t, items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, s) != cudaSuccess ||
+        cudaStreamSynchronize(s) != cudaSuccess) {
+        cudaFree(t);
+        return 1;
+    }
     p.generation++;
     cudaFree(p.items[v]);
-    p.items[v] = nullptr;
+    p.items[v] = t;
     p.nitems[v] = (int)items.size();
-    if (cudaMalloc(&p.items[v], items.size() * sizeof(int4)) != cudaSuccess) return 1;
-    if (cudaMemcpyAsync(p.items[v], items.data(), items.size() * sizeof(int4), cudaMemcpyHostToDevice, s) !=
-        cudaSuccess)
-        return 1;
-    // the item table is a host vector: finish its copy before returning
-    return cudaStreamSynchronize(s) != cudaSuccess;
+    return 0;
 }
 
 void release(Plan &p)

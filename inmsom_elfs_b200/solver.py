@@ -334,7 +334,9 @@ class BarotropicSolver:
 class Ensemble:
     """Independent basins advanced together (inmsom_ens_*): each member is a
     BarotropicSolver with its state resident; `group` substeps of all
-    members per CUDA-graph launch."""
+    members per CUDA-graph launch.  Creation re-cuts each member's work
+    items to 16 rows at least (a solver alone cuts down to 4), and the
+    members keep that cut, as they keep what tune() chooses."""
 
     def __init__(self, members: Sequence["BarotropicSolver"], group: int = 10, persistent: bool = False):
         self.members = list(members)
