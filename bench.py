@@ -674,11 +674,13 @@ def run_study_ensemble(args):
         s.run_substeps(10, b.dt)
         t += s.run_substeps(args.steps, b.dt, scale)
     res["sequential_members"] = {"ms": t, "cell_steps_per_s": cells * args.steps / (t / 1e3)}
+    rows = {}
     with solver.Ensemble(solvers, group=args.group) as e:
         for tag in ("graph_untuned", "persistent_untuned", "graph_tuned", "persistent_tuned"):
-            if tag == "graph_tuned":
-                rows = e.tune(dts, trial_groups=2)
-            e.set_persistent(tag.startswith("persistent"))
+            form = tag.split("_")[0]
+            e.set_persistent(form == "persistent")
+            if tag.endswith("_tuned"):
+                rows[form] = e.tune(dts, trial_groups=2)   # each form tuned in that form
             for s in solvers:
                 s.load_state()
             e.run(2 * args.group, dts)

@@ -609,11 +609,13 @@ typedef struct inmsom_ens inmsom_ens;
 int inmsom_ens_create(inmsom_ens **ens, inmsom_ctx *const *members, int nmembers, int group);
 int inmsom_ens_run(inmsom_ens *ens, int nsub, const double *dt, const double *rhs_scale, float *ms);
 /* Autotuner: for each size class of members (side length rounded to 256),
- * times `trial_groups` graph launches with each candidate chunk height
- * (one wave of cost-balanced chunks, or about 96, 64, 48 or 32 rows per
- * chunk) and keeps the fastest; rows_per_item[i] receives member i's
- * choice (0 = one wave), which the members keep.  The trial runs advance
- * the members' states. */
+ * times `trial_groups` groups of substeps in the ensemble's current form
+ * (graph or persistent: tune each form for itself) with each candidate
+ * chunk height (one wave of cost-balanced chunks, or about 96, 64, 48 or 32
+ * rows per chunk) and keeps the fastest; the combination is then timed
+ * against the members' cut before tuning, which stays if it is faster.
+ * rows_per_item[i] receives member i's choice (0 = one wave), which the
+ * members keep.  The trial runs advance the members' states. */
 int inmsom_ens_tune(inmsom_ens *ens, const double *dt, int trial_groups, int *rows_per_item);
 /* on != 0: inmsom_ens_run advances each group of substeps of all members
  * with ONE persistent cooperative launch (still replayed as a CUDA graph)

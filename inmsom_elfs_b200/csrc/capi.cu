@@ -1355,7 +1355,14 @@ int inmsom_ens_tune(inmsom_ens *e, const double *dt, int trial_groups, int *rows
         cls[i] = (int)std::lround(side / 256.0);
         ncls = std::max(ncls, cls[i] + 1);
     }
-    std::vector<int> chosen(n, 0);
+    // the members' cut before tuning, timed like the candidates: kept unless
+    // the tuned combination (chosen class by class, the other classes as
+    // they stand) is faster as a whole
+    std::vector<int> start(n), chosen(n);
+    for (size_t i = 0; i < n; i++) chosen[i] = start[i] = e->m[i]->plan.rows_per_item[0];
+    float base = 0.0f, tuned = 0.0f;
+    CKR(inmsom_ens_run(e, e->group * trial_groups, dt, nullptr, &base));   // warm-up, captures
+    CKR(inmsom_ens_run(e, e->group * trial_groups, dt, nullptr, &base));
     for (int k = 0; k < ncls; k++) {
         bool any = false;
         for (size_t i = 0; i < n; i++) any |= cls[i] == k;
@@ -1381,6 +1388,14 @@ int inmsom_ens_tune(inmsom_ens *e, const double *dt, int trial_groups, int *rows
                 chosen[i] = best_c;
             }
     }
+    CKR(inmsom_ens_run(e, e->group * trial_groups, dt, nullptr, &tuned));
+    CKR(inmsom_ens_run(e, e->group * trial_groups, dt, nullptr, &tuned));
+    if (tuned > base)
+        for (size_t i = 0; i < n; i++) {
+            if (fused::repartition(e->m[i]->plan, e->m[i]->dom, start[i], e->m[i]->stream))
+                return set_err(INMSOM_ECUDA, "member %zu: repartition failed", i);
+            chosen[i] = start[i];
+        }
     if (rows_out)
         for (size_t i = 0; i < n; i++) rows_out[i] = chosen[i];
     return INMSOM_OK;

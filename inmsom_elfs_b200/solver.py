@@ -371,8 +371,10 @@ class Ensemble:
         return float(ms.value)
 
     def tune(self, dt, trial_groups: int = 2):
-        """Autotune chunk heights per size class; returns rows per item per
-        member (0 = one wave of cost-balanced chunks).  Advances the states."""
+        """Autotune chunk heights per size class in the ensemble's current
+        form (graph or persistent); the cut before tuning stays unless the
+        tuned one is faster.  Returns rows per item per member (0 = one wave
+        of cost-balanced chunks).  Advances the states."""
         d = self._dt(dt)
         out = (ctypes.c_int * len(self.members))()
         check(load().inmsom_ens_tune(self._ens, dptr(d), int(trial_groups), out))
