@@ -1234,6 +1234,8 @@ int inmsom_ens_create(inmsom_ens **out, inmsom_ctx *const *members, int n, int g
         if (c->flags & INMSOM_FP32_VELOCITY)
             return set_err(INMSOM_EUNSUPPORTED, "member %d: the ensemble runs FP64 state only", i);
         if (c->device != members[0]->device) return set_err(INMSOM_EARG, "member %d on another device", i);
+        for (int j = 0; j < i; j++)
+            if (members[j] == c) return set_err(INMSOM_EARG, "member %d is member %d again", i, j);
     }
     CK(cudaSetDevice(members[0]->device));
     inmsom_ens *e = new inmsom_ens();

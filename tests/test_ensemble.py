@@ -76,6 +76,16 @@ def test_ensemble_rejects_odd_group(gpu):
             gpu.Ensemble([s], group=3)
 
 
+def test_ensemble_rejects_a_member_given_twice(gpu):
+    """Both entries would advance the same state in the same group."""
+    from inmsom_elfs_b200 import InmsomError
+    b = _members(gpu)[0]
+    with gpu.BarotropicSolver(b.copy(), resident=True) as s:
+        s.load_state()
+        with pytest.raises(InmsomError, match="again"):
+            gpu.Ensemble([s, s], group=4)
+
+
 @pytest.mark.parametrize("persistent", [False, True])
 def test_ensemble_odd_runs_back_to_back(gpu, persistent):
     """An odd run moves each member's state to its other ping-pong set; the
